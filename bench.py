@@ -1,0 +1,388 @@
+"""Benchmark of the steady implicit step (residual, Jacobians, LU, multi-colour
+SGS, Newton update) on the 128^3 split-tet Taylor-Green grid.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fpsi|reference]
+
+One step = one implicit pseudo-time step over every cell: FP64 residual
+(MUSCL + Venkatakrishnan + Roe), FP32 Jacobian blocks and LU, 8 symmetric
+multi-colour SGS sweeps in FP32 (defect correction), FP64 Newton update.
+Metric: cell-iterations per second.  Under torchrun each rank runs an
+independent replica of the grid on its own GPU (the path is not partitioned
+across GPUs); timing is CUDA events on the library's stream, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cell-iters/s"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler over the timed region"""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().splitlines() if r.strip()]
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def dist_max(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def sgs_bytes_per_step(nc, nfi, nbf, sweeps, tb, tx):
+    """algorithmic bytes of all SGS colour launches of one step: per cell
+    LU 25*tb + B 5*tb + x write 5*tx; per interior face side block 25*tb +
+    face index 4 + neighbour x 5*tx; two directions per sweep"""
+    per_dir = nc * (30 * tb + 5 * tx) + 2 * nfi * (25 * tb + 4 + 5 * tx)
+    return 2 * sweeps * per_dir
+
+
+def kernel_bytes(name, nc, nfi, nbf, sweeps, tb, tx):
+    """algorithmic bytes of one step of each kernel (every array the kernel
+    must touch counted once: FP64 8 B, FP32 4 B, index 4 B)"""
+    nf = nfi + nbf
+    geo_face = 8 + 32 + 48  # cl,cr + n*A + rL,rR
+    return {
+        "bc_state": nbf * (4 + 24 + 40 + 40),
+        # q + Minv + vol + grad/limiter writes; face geometry and indices
+        "grad_limiter": nc * (40 + 48 + 8 + 120 + 40) + nf * (8 + 48),
+        # survey K3: q 40 + grad 120 + phi 40 per cell, 88 per face, flux write 40 + mev 8
+        "face_flux": nc * (40 + 120 + 40) + nf * (geo_face + 48),
+        "cell_residual": nc * (40 + 8 + 40 + 8) + nf * 48,
+        "face_jacobian": nc * (40 + 120 + 40) + nf * geo_face + (nfi * 2 + nbf) * 25 * tb,
+        "assemble_lu": nc * (40 + 40 + 8 + 8 + 32 * tb + 5 * tx) + (2 * nfi + nbf) * 25 * tb,
+        "sgs_colour": sgs_bytes_per_step(nc, nfi, nbf, sweeps, tb, tx),
+        "update": nc * (80 + 5 * tx),
+    }.get(name)
+
+
+def build_case(args):
+    from flowpsi_b200 import cases
+
+    return cases.taylor_green_tets(args.n, seed=args.seed, sweeps=args.sweeps,
+                                   precision=args.precision)
+
+
+class OracleSample:
+    """the oracle (the C++ restatement) on a smaller grid of the same
+    workload, multi-colour SGS order, every requested host thread"""
+
+    def __init__(self, args, threads: int, n_sample: int):
+        from flowpsi_b200 import cases
+        from oracle import Oracle
+        from oracle.oracle import set_threads
+
+        self.threads = set_threads(threads)
+        case = cases.taylor_green_tets(n_sample, seed=args.seed, sweeps=args.sweeps,
+                                       precision=args.precision)
+        self.case = case
+        self.o = Oracle(case.mesh, case.params)
+        T, p, u = case.initial_state(self.o.geometry()["cellcenter"])
+        self.o.set_state(T, p, u)
+        self.colour = greedy_colours(case.mesh)
+        self.ncells = self.o.ncells
+
+    def step(self) -> float:
+        t0 = time.perf_counter()
+        self.o.newton_step(colour=self.colour)
+        return time.perf_counter() - t0
+
+
+def cpu_oracle_rate(args, threads: int, n_sample: int, steps: int):
+    s = OracleSample(args, threads, n_sample)
+    s.step()  # warm-up
+    dt = sum(s.step() for _ in range(steps))
+    return s.ncells * steps / dt, s.ncells, dt
+
+
+def greedy_colours(mesh) -> np.ndarray:
+    a = mesh.arrays()
+    nc = a.ncells
+    inner = a.cr >= 0
+    cl, cr = a.cl[inner], a.cr[inner]
+    nbr = [[] for _ in range(nc)]
+    for x, y in zip(cl.tolist(), cr.tolist()):
+        nbr[x].append(y)
+        nbr[y].append(x)
+    col = np.full(nc, -1, np.int32)
+    for c in range(nc):
+        used = {col[m] for m in nbr[c] if col[m] >= 0}
+        k = 0
+        while k in used:
+            k += 1
+        col[c] = k
+    return col
+
+
+def run_reference(args, ws, rank):
+    """reference arm: the CPU restatement of the reference path (oracle port)
+    with every host thread, one bounded sample per step"""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    smp = OracleSample(args, threads, args.cpu_n)
+    for _ in range(args.warmup):
+        smp.step()
+    times = [smp.step() for _ in range(args.steps)]
+    total_dt = sum(times)
+    rates = [smp.ncells / t for t in times]
+    value = statistics.median(rates)
+    sample = (f"taylor_green_tets {args.cpu_n}^3 x 6 = {6 * args.cpu_n ** 3} cells, "
+              f"one implicit step per timed step, {args.sweeps} multi-colour SGS sweeps")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-iters/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total_dt / max(args.steps, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+        "config": {"workload": f"taylor_green_tets_{args.n}", "sample_cells": 6 * args.cpu_n ** 3,
+                   "precision": args.precision, "sgs_sweeps": args.sweeps},
+        "cpu_baseline": {"value": value, "unit": "cell-iters/s", "cores": threads,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "cell-iters/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_fpsi(args, ws, rank, local):
+    from flowpsi_b200 import FlowPsi
+    from flowpsi_b200 import _native as N
+
+    if not N.lib().fpsi_device_available():
+        raise SystemExit("no CUDA device: the fpsi arm has no CPU fallback")
+    t0 = time.perf_counter()
+    case = build_case(args)
+    solver = FlowPsi(case.mesh, case.params)
+    solver.keep_blocks(False)
+    log(f"[rank {rank}] setup {time.perf_counter() - t0:.1f}s: {solver.ncells} cells, "
+        f"{solver.nfaces} faces, {solver.ncolours} colours, "
+        f"{solver.device_bytes / 1e9:.2f} GB device")
+    geo = solver.geometry()
+    T0, p0, u0 = case.initial_state(geo["cellcenter"])
+    solver.set_state(T0, p0, u0)
+    nc, nf = solver.ncells, solver.nfaces
+    nfi = nf  # periodic grid: every face is interior
+    hist_w = solver.run(args.warmup) if args.warmup > 0 else []
+    dist_barrier(ws)
+    with Clocks(local) as clk:
+        hist, ms = solver.run_timed(args.steps)
+    ms = dist_max(ms, ws)
+    clocks = clk.summary()
+    value = nc * args.steps * ws / (ms / 1e3)
+
+    # per-kernel device times (separate run, events around every launch)
+    kt = solver.kernel_times(args.profile_steps)
+    tb = 4 if args.precision in ("ref", "mixed") else 8
+    tx = 4 if args.precision == "mixed" else 8
+    peaks, src = load_peaks()
+    peak = float(peaks["hbm_gbs"])
+    kernels = {}
+    for name, (kms, launches) in kt.items():
+        b = kernel_bytes(name, nc, nfi, 0, args.sweeps, tb, tx)
+        if b is None:
+            continue
+        per_step_ms = kms / args.profile_steps
+        kernels[name] = {"ms_per_step": per_step_ms, "launches_per_step": launches / args.profile_steps,
+                         "gbs": b / (per_step_ms / 1e3) / 1e9}
+    dom = max(kernels, key=lambda k: kernels[k]["ms_per_step"])
+    dk = kernels[dom]
+    b_launch = kernel_bytes(dom, nc, nfi, 0, args.sweeps, tb, tx) / dk["launches_per_step"]
+    avg_launch_s = dk["ms_per_step"] / dk["launches_per_step"] / 1e3
+    achieved = b_launch / avg_launch_s / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get(f"{dom}:{args.precision}:{args.n}")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "kernel": dom,
+                "peak_source": src, "bytes_per_launch": b_launch}
+
+    # end to end through the public API: per step the state goes host ->
+    # device from pinned memory, one implicit step runs, the new state and the
+    # residual norms come back
+    import torch
+
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    Th, ph, uh = pin(T0), pin(p0), pin(u0)
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    dist_barrier(ws)
+    t1 = time.perf_counter()
+    for _ in range(e2e_steps):
+        solver.set_state(Th, ph, uh)
+        solver.newton_step()
+        Tn, pn, un = solver.get_state()
+    e2e_s = dist_max(time.perf_counter() - t1, ws)
+    e2e = {"value": nc * e2e_steps * ws / e2e_s, "unit": "cell-iters/s",
+           "h2d_bytes_per_step": 5 * 8 * nc, "d2h_bytes_per_step": 5 * 8 * nc + 64,
+           "steps": e2e_steps, "timer": "host wall clock, synchronous API"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        r, ncs, dt = cpu_oracle_rate(args, threads, args.cpu_n, args.cpu_steps)
+        cpu = {"value": r, "unit": "cell-iters/s", "cores": threads, "kind": "port",
+               "sample": f"taylor_green_tets {args.cpu_n}^3 x 6 = {ncs} cells, "
+                         f"{args.cpu_steps} implicit steps ({dt:.1f} s), multi-colour SGS"}
+
+    launches = sum(v[1] for v in kt.values()) / args.profile_steps * args.steps
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-iters/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 residual + f32 blocks/sweeps" if args.precision == "mixed" else args.precision,
+        "data": "synthetic (seeded Taylor-Green on a jittered split-tet grid)",
+        "config": {"workload": f"taylor_green_tets_{args.n}", "cells": nc, "faces": nf,
+                   "colours": solver.ncolours, "precision": args.precision,
+                   "flux": "roe", "limiter": "venkatakrishnan", "sgs_sweeps": args.sweeps,
+                   "parallelism": f"replicas{ws}",
+                   "l2": "inputs larger than L2 (%.1f GB resident)" % (solver.device_bytes / 1e9)},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": int(round(launches)),
+        "clocks": clocks,
+        "kernels": kernels,
+        "resid_first": hist[0]["rtrms"] if hist else None,
+        "resid_last": hist[-1]["rtrms"] if hist else None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    solver.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fpsi", choices=["fpsi", "reference"])
+    ap.add_argument("--n", type=int, default=128, help="hexes per direction (x6 tets)")
+    ap.add_argument("--sweeps", type=int, default=8)
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "ref", "mixed"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--profile-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-n", type=int, default=40)
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        log("warning: fewer than 3 warm-up steps")
+    ws, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_fpsi(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,158 @@
+"""Synthetic workloads: grids, initial conditions and options.
+
+All random numbers come from a counter-based generator (SplitMix64 followed
+by Box-Muller) evaluated on the host, so every run, CPU or GPU, sees the same
+inputs for the same seed.
+
+* ``farfield_cube``: inviscid Euler, n^3 hex cube [0,1]^3, farfield on all
+  sides at M=0.5 along +x, p=1e5 Pa, T=300 K; initial state the freestream
+  with 1% Gaussian noise in rho, u, v, w and p; Roe flux, MUSCL with the
+  Venkatakrishnan limiter, 5 SGS sweeps per step, CFL 50 (32^3: the
+  CPU-runnable case).
+* ``taylor_green_tets``: n^3 hexes split into 6 Kuhn tetrahedra on the
+  periodic box [0,2pi]^3, nodes jittered by +-10% of the spacing; Taylor-Green
+  vortex at M=0.1 (initial form of examples/taylor/ic_module/
+  taylorGreenIC.loci:26-31: constant density, pressure from the analytic
+  field); Roe + MUSCL + Venkatakrishnan, 8 multi-colour SGS sweeps (128^3:
+  12.58M cells, 25.2M faces).
+* ``oblique_shock_cube``: n^3 hex cube, Mach-2 flow with a Rankine-Hugoniot
+  jump across a plane tilted 30 degrees, 0.5% noise, supersonic inflow /
+  outflow, HLLE + Barth.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .solver import GeneratedMesh, bc, default_params
+
+RTILDE = 8314.4621 / 28.96
+GAMMA = 1.4
+
+_M64 = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+
+def splitmix64(x: np.ndarray) -> np.ndarray:
+    x = (x + np.uint64(0x9E3779B97F4A7C15)) & _M64
+    x = ((x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)) & _M64
+    x = ((x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)) & _M64
+    return x ^ (x >> np.uint64(31))
+
+
+def uniform(seed: int, stream: int, n: int) -> np.ndarray:
+    """n doubles in (0,1) from counter (seed, stream, i)."""
+    with np.errstate(over="ignore"):
+        base = np.uint64((seed * 0x100000001B3 + stream * 0x9E3779B1) & 0xFFFFFFFFFFFFFFFF)
+        i = np.arange(n, dtype=np.uint64)
+        r = splitmix64((base + i * np.uint64(0x632BE59BD9B4E019)) & _M64)
+    return ((r >> np.uint64(11)).astype(np.float64) + 0.5) * (1.0 / 9007199254740992.0)
+
+
+def normal(seed: int, stream: int, n: int) -> np.ndarray:
+    u1 = uniform(seed, 2 * stream, n)
+    u2 = uniform(seed, 2 * stream + 1, n)
+    return np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * math.pi * u2)
+
+
+class Case:
+    def __init__(self, name, mesh, params, steps, init):
+        self.name = name
+        self.mesh = mesh
+        self.params = params
+        self.steps = steps
+        self._init = init
+
+    def initial_state(self, cellcenter: np.ndarray):
+        """(T, pg, u[nc,3]) at the given cell centroids (caller order)."""
+        return self._init(cellcenter)
+
+
+def farfield_cube(n: int = 32, seed: int = 0, sweeps: int = 5, flux: str = "roe",
+                  limiter: str = "venkatakrishnan", precision: str = "ref") -> Case:
+    T0, p0, M = 300.0, 1e5, 0.5
+    a0 = math.sqrt(GAMMA * RTILDE * T0)
+    U0 = M * a0
+    ff = bc("farfield", T=T0, pg=p0, u=(U0, 0.0, 0.0))
+    mesh = GeneratedMesh("hex", n=(n, n, n), L=(1.0, 1.0, 1.0), bc_side=(0,) * 6, bcs=[ff])
+    params = default_params(flux=flux, limiter=limiter, Kl=1.0, solver="sgs",
+                            gauss_seidel_iter=sweeps, cflmax=50.0, precision=precision)
+
+    def init(cc):
+        nc = cc.shape[0]
+        rho0 = p0 / (RTILDE * T0)
+        rho = rho0 * (1.0 + 0.01 * normal(seed, 0, nc))
+        p = p0 * (1.0 + 0.01 * normal(seed, 1, nc))
+        u = np.empty((nc, 3))
+        u[:, 0] = U0 + 0.01 * U0 * normal(seed, 2, nc)
+        u[:, 1] = 0.01 * U0 * normal(seed, 3, nc)
+        u[:, 2] = 0.01 * U0 * normal(seed, 4, nc)
+        T = p / (RTILDE * rho)
+        return T, p, u
+
+    return Case(f"farfield_cube_{n}", mesh, params, 20, init)
+
+
+def taylor_green_tets(n: int = 128, seed: int = 0, sweeps: int = 8, jitter: float = 0.1,
+                      amplitude: float = 1.0, precision: str = "mixed", flux: str = "roe",
+                      limiter: str = "venkatakrishnan") -> Case:
+    L = 2.0 * math.pi
+    mesh = GeneratedMesh("kuhn", n=(n, n, n), L=(L, L, L), jitter=jitter, seed=seed)
+    params = default_params(flux=flux, limiter=limiter, Kl=1.0, solver="sgs",
+                            gauss_seidel_iter=sweeps, cflmax=50.0, precision=precision)
+    T0, p0, M = 300.0, 1e5, 0.1
+    rho0 = p0 / (RTILDE * T0)
+    U0 = amplitude * M * math.sqrt(GAMMA * RTILDE * T0)
+
+    def init(cc):
+        x, y, z = cc[:, 0], cc[:, 1], cc[:, 2]
+        u = np.empty((cc.shape[0], 3))
+        u[:, 0] = U0 * np.sin(x) * np.cos(y) * np.cos(z)
+        u[:, 1] = -U0 * np.cos(x) * np.sin(y) * np.cos(z)
+        u[:, 2] = 0.0
+        p = p0 + rho0 * U0 * U0 / 16.0 * (np.cos(2 * x) + np.cos(2 * y)) * (np.cos(2 * z) + 2.0)
+        T = p / (rho0 * RTILDE)
+        return T, p, u
+
+    return Case(f"taylor_green_tets_{n}", mesh, params, 200, init)
+
+
+def oblique_shock_cube(n: int = 256, seed: int = 0, sweeps: int = 8, precision: str = "mixed",
+                       flux: str = "hlle", limiter: str = "barth") -> Case:
+    T1, p1, M1 = 300.0, 1e5, 2.0
+    a1 = math.sqrt(GAMMA * RTILDE * T1)
+    U1 = M1 * a1
+    inflow = bc("supersonicInflow", T=T1, pg=p1, u=(U1, 0.0, 0.0))
+    outflow = bc("supersonicOutflow", T=T1, pg=p1, u=(U1, 0.0, 0.0))
+    # x-min supersonic inflow, the rest supersonic outflow
+    mesh = GeneratedMesh("hex", n=(n, n, n), L=(1.0, 1.0, 1.0),
+                         bc_side=(0, 1, 1, 1, 1, 1), bcs=[inflow, outflow])
+    params = default_params(flux=flux, limiter=limiter, solver="sgs", gauss_seidel_iter=sweeps,
+                            cflmax=50.0, precision=precision)
+    # shock plane through the centre, normal tilted 30 degrees from x in x-y
+    th = math.radians(30.0)
+    nrm = np.array([math.cos(th), math.sin(th), 0.0])
+    Mn = M1 * nrm[0]
+    g = GAMMA
+    p2 = p1 * (1 + 2 * g / (g + 1) * (Mn * Mn - 1))
+    r1 = p1 / (RTILDE * T1)
+    r2 = r1 * (g + 1) * Mn * Mn / ((g - 1) * Mn * Mn + 2)
+    T2 = p2 / (RTILDE * r2)
+    u1 = np.array([U1, 0.0, 0.0])
+    un1 = float(u1 @ nrm)
+    un2 = un1 * r1 / r2
+    u2 = u1 + (un2 - un1) * nrm
+
+    def init(cc):
+        nc = cc.shape[0]
+        s = (cc - 0.5) @ nrm
+        down = s > 0
+        T = np.where(down, T2, T1)
+        p = np.where(down, p2, p1)
+        u = np.where(down[:, None], u2[None, :], u1[None, :])
+        T = T * (1.0 + 0.005 * normal(seed, 0, nc))
+        p = p * (1.0 + 0.005 * normal(seed, 1, nc))
+        u = u * (1.0 + 0.005 * normal(seed, 2, nc))[:, None]
+        return T, p, u
+
+    return Case(f"oblique_shock_cube_{n}", mesh, params, 200, init)

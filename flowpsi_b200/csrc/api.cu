@@ -1,0 +1,761 @@
+// api.cu -- the C ABI (include/fpsi.h) over the device path.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "fpsi_internal.h"
+#include "kernels.cuh"
+
+using fpsi::HostMesh;
+
+namespace fpsi {
+static cudaEvent_t prof_event(fpsi_ctx* x) {
+  if (x->evnext == x->evpool.size()) {
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    x->evpool.push_back(e);
+  }
+  return x->evpool[x->evnext++];
+}
+void prof_begin(fpsi_ctx* x, const char* name) {
+  if (!x->profiling) return;
+  fpsi_prof_rec r;
+  r.name = name;
+  r.a = prof_event(x);
+  r.b = prof_event(x);
+  cudaEventRecord(r.a, x->stream);
+  x->prof.push_back(r);
+}
+void prof_end(fpsi_ctx* x) {
+  if (!x->profiling || x->prof.empty()) return;
+  cudaEventRecord(x->prof.back().b, x->stream);
+}
+}  // namespace fpsi
+
+namespace {
+
+template <class T>
+int dalloc(fpsi_ctx* x, T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    fpsi::set_error("cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+    *p = nullptr;
+    return e == cudaErrorMemoryAllocation ? FPSI_E_NOMEM : FPSI_E_CUDA;
+  }
+  x->device_bytes += int64_t(n * sizeof(T));
+  return FPSI_OK;
+}
+
+template <class T>
+int upload(fpsi_ctx* x, T** p, const std::vector<T>& h) {
+  int rc = dalloc(x, p, h.size());
+  if (rc) return rc;
+  if (!h.empty()) FPSI_CUDA_TRY(cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return FPSI_OK;
+}
+
+// AoS [n][3] -> SoA [3][n]
+std::vector<double> soa3(const std::vector<double>& a, int64_t n) {
+  std::vector<double> r(3 * n);
+  for (int64_t i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) r[d * n + i] = a[3 * i + d];
+  return r;
+}
+
+void free_system(fpsi_ctx* x) {
+  void* ps[] = {x->d_fjp, x->d_fjm, x->d_cellblk, x->d_D, x->d_x};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  x->d_fjp = x->d_fjm = x->d_cellblk = x->d_D = x->d_x = nullptr;
+}
+
+int alloc_system(fpsi_ctx* x) {
+  if (x->alloc_prec == x->P.precision) return FPSI_OK;
+  free_system(x);
+  const int tb = x->P.precision == FPSI_PREC_FP64 ? 8 : 4;
+  const int tx = x->P.precision == FPSI_PREC_MIXED ? 4 : 8;
+  x->blk_bytes = tb;
+  x->x_bytes = tx;
+  const size_t nf = size_t(x->H.nf), nc = size_t(x->H.nc);
+  int rc;
+  if ((rc = dalloc(x, (char**)&x->d_fjp, nf * 25 * tb))) return rc;
+  if ((rc = dalloc(x, (char**)&x->d_fjm, nf * 25 * tb))) return rc;
+  if ((rc = dalloc(x, (char**)&x->d_cellblk, nc * 32 * tb))) return rc;
+  if (x->keep_D)
+    if ((rc = dalloc(x, (char**)&x->d_D, nc * 25 * tb))) return rc;
+  if ((rc = dalloc(x, (char**)&x->d_x, nc * 5 * tx))) return rc;
+  x->alloc_prec = x->P.precision;
+  x->have_asm = x->have_dq = false;
+  return FPSI_OK;
+}
+
+int check_params(const fpsi_params* p) {
+  if (!p) return FPSI_E_INVALID;
+  if (!(p->gamma > 1.0) || !(p->Rtilde > 0) || p->flux < 0 || p->flux > 2 || p->limiter < 0 ||
+      p->limiter > 3 || p->precision < 0 || p->precision > 2 || p->gauss_seidel_iter < 0) {
+    fpsi::set_error("invalid parameter value");
+    return FPSI_E_INVALID;
+  }
+  if (p->Minf < 0.5) {
+    fpsi::set_error("low-Mach preconditioning (Minf < 0.5) is not on the device path");
+    return FPSI_E_UNSUPPORTED;
+  }
+  if (p->solver != FPSI_SOLVER_SGS) {
+    fpsi::set_error("fluidLinearSolver: only 'sgs' is available on this build");
+    return FPSI_E_UNSUPPORTED;
+  }
+  if (p->viscous != 0) {
+    fpsi::set_error("viscous fluxes are not available on this build");
+    return FPSI_E_UNSUPPORTED;
+  }
+  return FPSI_OK;
+}
+
+int sync(fpsi_ctx* x) {
+  FPSI_CUDA_TRY(cudaStreamSynchronize(x->stream));
+  return FPSI_OK;
+}
+
+void fill_norms(const fpsi_ctx* x, const double* r, fpsi_resid* n) {
+  std::memset(n, 0, sizeof(*n));
+  n->rtrms = r[0];
+  n->etrms = r[1];
+  n->mtrms = r[2];
+  n->rtmax = r[3];
+  n->etmax = r[5];
+  n->mtmax = r[7];
+  const int64_t cr = int64_t(r[4]), ce = int64_t(r[6]);
+  if (cr >= 0 && cr < x->H.nc)
+    for (int d = 0; d < 3; ++d) n->ccmaxr_center[d] = x->H.cc[3 * cr + d];
+  if (ce >= 0 && ce < x->H.nc)
+    for (int d = 0; d < 3; ++d) n->ccmaxe_center[d] = x->H.cc[3 * ce + d];
+}
+
+bool has_nan(const double* r) { return r[0] != r[0] || r[1] != r[1] || r[2] != r[2]; }
+
+template <class T>
+void unpermute_cells(const fpsi_ctx* x, const T* dev_order, int w, T* caller) {
+  const int64_t nc = x->H.nc;
+  for (int64_t i = 0; i < nc; ++i) {
+    const int64_t c = x->H.perm[i];
+    for (int k = 0; k < w; ++k) caller[w * c + k] = dev_order[w * i + k];
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void fpsi_default_params(fpsi_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->gamma = 1.4;
+  p->Rtilde = 8314.4621 / 28.96;
+  p->Pambient = 0.0;
+  p->Minf = 1.0;
+  p->flux = FPSI_FLUX_HLLC;
+  p->limiter = FPSI_LIMITER_VENKATAKRISHNAN;
+  p->Kl = 1.0;
+  p->urelax = 0.2;
+  p->dtmax = 1.0;
+  p->cflmax = 0.0;
+  p->solver = FPSI_SOLVER_LSGS;
+  p->gauss_seidel_iter = 6;
+  p->lsgs_relaxation = 0.25;
+  p->lsgs_abs_tol = 1e-10;
+  p->lsgs_rel_tol = 0.1;
+  p->lsgs_max_iter = 10;
+  p->precision = FPSI_PREC_REF;
+  p->viscous = 0;
+  p->Pr = 0.72;
+  p->Prt = 0.9;
+  p->sutherland_mu0 = 1.716e-5;
+  p->sutherland_T0 = 273.15;
+  p->sutherland_S = 110.4;
+}
+
+const char* fpsi_strerror(int code) {
+  switch (code) {
+    case FPSI_OK: return "ok";
+    case FPSI_E_INVALID: return "invalid argument";
+    case FPSI_E_CUDA: return "CUDA error";
+    case FPSI_E_NOMEM: return "out of memory";
+    case FPSI_E_UNSUPPORTED: return "unsupported option";
+    case FPSI_E_SINGULAR: return "singular diagonal block";
+    case FPSI_E_NAN: return "NaN residual";
+    case FPSI_E_TIMEOUT: return "device wait timed out";
+    case FPSI_E_STATE: return "call out of order";
+    default: return "unknown error";
+  }
+}
+
+const char* fpsi_last_error(void) { return fpsi::last_error(); }
+
+int fpsi_device_available(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n > 0;
+}
+
+int fpsi_destroy(fpsi_ctx* x) {
+  if (!x) return FPSI_OK;
+  free_system(x);
+  void* ps[] = {x->d_cl, x->d_cr, x->d_n, x->d_area, x->d_rL, x->d_rR, x->d_vol, x->d_cc,
+                x->d_Minv, x->d_cf_off, x->d_cf, x->d_colour_cells, x->d_bcs, x->d_q,
+                x->d_qb, x->d_grad, x->d_phi, x->d_F, x->d_mev, x->d_src, x->d_dtau,
+                x->d_part, x->d_resid, x->d_amin, x->d_err, x->d_perm, x->d_stage};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  if (x->h_resid) cudaFreeHost(x->h_resid);
+  for (cudaEvent_t e : x->evpool) cudaEventDestroy(e);
+  if (x->stream) cudaStreamDestroy(x->stream);
+  delete x;
+  return FPSI_OK;
+}
+
+int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params) {
+  if (!out || !mesh || !params) return FPSI_E_INVALID;
+  *out = nullptr;
+  int rc = check_params(params);
+  if (rc) return rc;
+  if (!fpsi_device_available()) {
+    fpsi::set_error("no CUDA device");
+    return FPSI_E_CUDA;
+  }
+  fpsi_ctx* x = new (std::nothrow) fpsi_ctx();
+  if (!x) return FPSI_E_NOMEM;
+  x->P = *params;
+  try {
+    rc = fpsi::build_host_mesh(mesh, x->H);
+  } catch (const std::bad_alloc&) {
+    rc = FPSI_E_NOMEM;
+  }
+  if (rc) {
+    delete x;
+    return rc;
+  }
+  x->bcs.assign(mesh->bcs, mesh->bcs + mesh->nbc);
+  for (const fpsi_bc& b : x->bcs)
+    if (b.kind < FPSI_BC_FARFIELD || b.kind > FPSI_BC_REFLECTING) {
+      fpsi::set_error("boundary condition kind %d is not on the device path", b.kind);
+      delete x;
+      return FPSI_E_UNSUPPORTED;
+    }
+  const HostMesh& H = x->H;
+  const int64_t nc = H.nc, nf = H.nf;
+#define TRY(e)                \
+  do {                        \
+    int rc_ = (e);            \
+    if (rc_) {                \
+      fpsi_destroy(x);        \
+      return rc_;             \
+    }                         \
+  } while (0)
+  if (cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    fpsi::set_error("cudaStreamCreate failed");
+    delete x;
+    return FPSI_E_CUDA;
+  }
+  TRY(upload(x, &x->d_cl, H.cl));
+  TRY(upload(x, &x->d_cr, H.cr));
+  TRY(upload(x, &x->d_n, soa3(H.n, nf)));
+  TRY(upload(x, &x->d_area, H.area));
+  TRY(upload(x, &x->d_rL, soa3(H.rL, nf)));
+  TRY(upload(x, &x->d_rR, soa3(H.rR, nf)));
+  TRY(upload(x, &x->d_vol, H.vol));
+  TRY(upload(x, &x->d_cc, soa3(H.cc, nc)));
+  {
+    std::vector<double> m(6 * nc);
+    for (int64_t c = 0; c < nc; ++c)
+      for (int k = 0; k < 6; ++k) m[k * nc + c] = H.Minv[6 * c + k];
+    TRY(upload(x, &x->d_Minv, m));
+  }
+  TRY(upload(x, &x->d_cf_off, H.cf_off));
+  TRY(upload(x, &x->d_cf, H.cf));
+  TRY(upload(x, &x->d_colour_cells, H.colour_cells));
+  TRY(upload(x, &x->d_perm, H.perm));
+  TRY(dalloc(x, &x->d_stage, nc * 5));
+  TRY(upload(x, &x->d_bcs, x->bcs));
+  TRY(dalloc(x, &x->d_q, nc * 5));
+  TRY(dalloc(x, &x->d_qb, std::max<int64_t>(H.nbf, 1) * 5));
+  TRY(dalloc(x, &x->d_grad, nc * 15));
+  TRY(dalloc(x, &x->d_phi, nc * 5));
+  TRY(dalloc(x, &x->d_F, nf * 5));
+  TRY(dalloc(x, &x->d_mev, nf));
+  TRY(dalloc(x, &x->d_src, nc * 5));
+  TRY(dalloc(x, &x->d_dtau, nc));
+  x->nblk_norm = int((nc + 255) / 256);
+  TRY(dalloc(x, &x->d_part, size_t(x->nblk_norm) * 8));
+  TRY(dalloc(x, &x->d_resid, 16));
+  TRY(dalloc(x, &x->d_amin, size_t(x->nblk_norm)));
+  TRY(dalloc(x, &x->d_err, 4));
+  if (cudaMallocHost((void**)&x->h_resid, 16 * sizeof(double)) != cudaSuccess) {
+    fpsi_destroy(x);
+    return FPSI_E_NOMEM;
+  }
+  if (cudaMemset(x->d_err, 0, 4 * sizeof(int32_t)) != cudaSuccess) {
+    fpsi_destroy(x);
+    return FPSI_E_CUDA;
+  }
+  TRY(alloc_system(x));
+#undef TRY
+  *out = x;
+  return FPSI_OK;
+}
+
+int fpsi_set_params(fpsi_ctx* x, const fpsi_params* p) {
+  if (!x) return FPSI_E_INVALID;
+  int rc = check_params(p);
+  if (rc) return rc;
+  x->P = *p;
+  x->have_asm = x->have_dq = false;
+  return alloc_system(x);
+}
+
+int fpsi_info(fpsi_ctx* x, int64_t* nc, int64_t* nf, int32_t* ncol, int64_t* bytes) {
+  if (!x) return FPSI_E_INVALID;
+  if (nc) *nc = x->H.nc;
+  if (nf) *nf = x->H.nf;
+  if (ncol) *ncol = x->H.ncolours;
+  if (bytes) *bytes = x->device_bytes;
+  return FPSI_OK;
+}
+
+int fpsi_get_geometry(fpsi_ctx* x, double* vol, double* cellcenter, double* face_an,
+                      double* face_area, double* facecenter) {
+  if (!x) return FPSI_E_INVALID;
+  if (vol) unpermute_cells(x, x->H.vol.data(), 1, vol);
+  if (cellcenter) unpermute_cells(x, x->H.cc.data(), 3, cellcenter);
+  if (face_an) std::memcpy(face_an, x->H.an_caller.data(), sizeof(double) * 3 * x->H.nf);
+  if (face_area) std::memcpy(face_area, x->H.area_caller.data(), sizeof(double) * x->H.nf);
+  if (facecenter) std::memcpy(facecenter, x->H.fc_caller.data(), sizeof(double) * 3 * x->H.nf);
+  return FPSI_OK;
+}
+
+int fpsi_get_colours(fpsi_ctx* x, int32_t* colour) {
+  if (!x || !colour) return FPSI_E_INVALID;
+  unpermute_cells(x, x->H.colour.data(), 1, colour);
+  return FPSI_OK;
+}
+
+int fpsi_set_state(fpsi_ctx* x, const double* T, const double* pg, const double* u) {
+  if (!x || !T || !pg || !u) return FPSI_E_INVALID;
+  const int64_t nc = x->H.nc;
+  const size_t b = size_t(nc) * sizeof(double);
+  FPSI_CUDA_TRY(cudaMemcpyAsync(x->d_stage, T, b, cudaMemcpyHostToDevice, x->stream));
+  FPSI_CUDA_TRY(cudaMemcpyAsync(x->d_stage + nc, pg, b, cudaMemcpyHostToDevice, x->stream));
+  FPSI_CUDA_TRY(cudaMemcpyAsync(x->d_stage + 2 * nc, u, 3 * b, cudaMemcpyHostToDevice, x->stream));
+  int rc = fpsi::launch_state(x, true);
+  if (rc) return rc;
+  x->have_resid = x->have_asm = x->have_dq = false;
+  return sync(x);
+}
+
+int fpsi_get_state(fpsi_ctx* x, double* T, double* pg, double* u) {
+  if (!x || !T || !pg || !u) return FPSI_E_INVALID;
+  const int64_t nc = x->H.nc;
+  const size_t b = size_t(nc) * sizeof(double);
+  int rc = fpsi::launch_state(x, false);
+  if (rc) return rc;
+  FPSI_CUDA_TRY(cudaMemcpyAsync(T, x->d_stage, b, cudaMemcpyDeviceToHost, x->stream));
+  FPSI_CUDA_TRY(cudaMemcpyAsync(pg, x->d_stage + nc, b, cudaMemcpyDeviceToHost, x->stream));
+  FPSI_CUDA_TRY(cudaMemcpyAsync(u, x->d_stage + 2 * nc, 3 * b, cudaMemcpyDeviceToHost, x->stream));
+  return sync(x);
+}
+
+int fpsi_keep_blocks(fpsi_ctx* x, int32_t keep) {
+  if (!x) return FPSI_E_INVALID;
+  if (bool(keep) == x->keep_D) return FPSI_OK;
+  x->keep_D = keep != 0;
+  x->alloc_prec = -1;  // reallocate the system arrays
+  return alloc_system(x);
+}
+
+int fpsi_residual(fpsi_ctx* x, double* src, fpsi_resid* norms) {
+  if (!x) return FPSI_E_INVALID;
+  int rc = fpsi::launch_residual(x, x->d_resid);
+  if (rc) return rc;
+  FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid, x->d_resid, 8 * sizeof(double),
+                                cudaMemcpyDeviceToHost, x->stream));
+  std::vector<double> s;
+  if (src) {
+    s.resize(5 * x->H.nc);
+    FPSI_CUDA_TRY(cudaMemcpyAsync(s.data(), x->d_src, s.size() * sizeof(double),
+                                  cudaMemcpyDeviceToHost, x->stream));
+  }
+  if ((rc = sync(x))) return rc;
+  if (src) unpermute_cells(x, s.data(), 5, src);
+  if (norms) fill_norms(x, x->h_resid, norms);
+  x->have_resid = true;
+  x->have_asm = x->have_dq = false;
+  return has_nan(x->h_resid) ? FPSI_E_NAN : FPSI_OK;
+}
+
+int fpsi_get_reconstruction(fpsi_ctx* x, double* grad, double* limiter) {
+  if (!x) return FPSI_E_INVALID;
+  if (!x->have_resid) return FPSI_E_STATE;
+  const int64_t nc = x->H.nc;
+  std::vector<double> g;
+  if (grad) {
+    g.resize(15 * nc);
+    FPSI_CUDA_TRY(cudaMemcpy(g.data(), x->d_grad, g.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    unpermute_cells(x, g.data(), 15, grad);
+  }
+  if (limiter) {
+    g.resize(5 * nc);
+    FPSI_CUDA_TRY(cudaMemcpy(g.data(), x->d_phi, 5 * nc * sizeof(double), cudaMemcpyDeviceToHost));
+    unpermute_cells(x, g.data(), 5, limiter);
+  }
+  return FPSI_OK;
+}
+
+int fpsi_get_dtau(fpsi_ctx* x, double* dtau) {
+  if (!x || !dtau) return FPSI_E_INVALID;
+  if (!x->have_resid) return FPSI_E_STATE;
+  std::vector<double> d(x->H.nc);
+  FPSI_CUDA_TRY(cudaMemcpy(d.data(), x->d_dtau, d.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  unpermute_cells(x, d.data(), 1, dtau);
+  return FPSI_OK;
+}
+
+static int finish_assemble(fpsi_ctx* x) {
+  int32_t err = 0;
+  FPSI_CUDA_TRY(cudaMemcpyAsync(&err, x->d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, x->stream));
+  int rc = sync(x);
+  if (rc) return rc;
+  if (err) {
+    FPSI_CUDA_TRY(cudaMemset(x->d_err, 0, sizeof(int32_t)));
+    fpsi::set_error("zero pivot in a diagonal block LU");
+    return FPSI_E_SINGULAR;
+  }
+  return FPSI_OK;
+}
+
+int fpsi_assemble(fpsi_ctx* x) {
+  if (!x) return FPSI_E_INVALID;
+  if (!x->have_resid) return FPSI_E_STATE;
+  int rc = fpsi::launch_assemble(x, nullptr);
+  if (rc) return rc;
+  if ((rc = finish_assemble(x))) return rc;
+  x->have_asm = true;
+  x->have_dq = false;
+  return FPSI_OK;
+}
+
+int fpsi_get_blocks(fpsi_ctx* x, void* D, void* fjp, void* fjm, void* B) {
+  if (!x) return FPSI_E_INVALID;
+  if (!x->have_asm) return FPSI_E_STATE;
+  const int tb = x->blk_bytes;
+  const int64_t nc = x->H.nc, nf = x->H.nf;
+  std::vector<char> h;
+  if (D) {
+    if (!x->d_D) return FPSI_E_STATE;
+    h.resize(size_t(nc) * 25 * tb);
+    FPSI_CUDA_TRY(cudaMemcpy(h.data(), x->d_D, h.size(), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < nc; ++i)
+      std::memcpy((char*)D + size_t(x->H.perm[i]) * 25 * tb, h.data() + size_t(i) * 25 * tb, 25 * tb);
+  }
+  for (int w = 0; w < 2; ++w) {
+    void* dst = w ? fjm : fjp;
+    if (!dst) continue;
+    h.resize(size_t(nf) * 25 * tb);
+    FPSI_CUDA_TRY(cudaMemcpy(h.data(), w ? x->d_fjm : x->d_fjp, h.size(), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < nf; ++i) {
+      char* o = (char*)dst + size_t(x->H.fperm[i]) * 25 * tb;
+      if (w && i >= x->H.nfi)
+        std::memset(o, 0, 25 * tb);  // no fjm on boundary faces
+      else
+        std::memcpy(o, h.data() + size_t(i) * 25 * tb, 25 * tb);
+    }
+  }
+  if (B) {
+    h.resize(size_t(nc) * 32 * tb);
+    FPSI_CUDA_TRY(cudaMemcpy(h.data(), x->d_cellblk, h.size(), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < nc; ++i)
+      std::memcpy((char*)B + size_t(x->H.perm[i]) * 5 * tb, h.data() + (size_t(i) * 32 + 25) * tb,
+                  5 * tb);
+  }
+  return FPSI_OK;
+}
+
+static int upload_x(fpsi_ctx* x, const double* x0) {
+  const int64_t nc = x->H.nc;
+  if (x->x_bytes == 8) {
+    std::vector<double> v(5 * nc);
+    for (int64_t i = 0; i < nc; ++i)
+      for (int k = 0; k < 5; ++k) v[5 * i + k] = x0[5 * int64_t(x->H.perm[i]) + k];
+    FPSI_CUDA_TRY(cudaMemcpy(x->d_x, v.data(), v.size() * 8, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> v(5 * nc);
+    for (int64_t i = 0; i < nc; ++i)
+      for (int k = 0; k < 5; ++k) v[5 * i + k] = float(x0[5 * int64_t(x->H.perm[i]) + k]);
+    FPSI_CUDA_TRY(cudaMemcpy(x->d_x, v.data(), v.size() * 4, cudaMemcpyHostToDevice));
+  }
+  return FPSI_OK;
+}
+
+static int download_x(fpsi_ctx* x, double* dq) {
+  const int64_t nc = x->H.nc;
+  std::vector<double> v(5 * nc);
+  if (x->x_bytes == 8) {
+    FPSI_CUDA_TRY(cudaMemcpy(v.data(), x->d_x, v.size() * 8, cudaMemcpyDeviceToHost));
+  } else {
+    std::vector<float> f(5 * nc);
+    FPSI_CUDA_TRY(cudaMemcpy(f.data(), x->d_x, f.size() * 4, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < f.size(); ++i) v[i] = f[i];
+  }
+  unpermute_cells(x, v.data(), 5, dq);
+  return FPSI_OK;
+}
+
+int fpsi_linear_solve(fpsi_ctx* x, const double* x0, double* dq, fpsi_lsinfo* info) {
+  if (!x) return FPSI_E_INVALID;
+  if (!x->have_asm) return FPSI_E_STATE;
+  int rc;
+  if (x0) {
+    if ((rc = upload_x(x, x0))) return rc;
+  } else if (x->have_dq) {
+    // iterate was consumed by an earlier solve: rebuild the block Jacobi start
+    if ((rc = fpsi::launch_assemble(x, nullptr))) return rc;
+    if ((rc = finish_assemble(x))) return rc;
+  }
+  if ((rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter))) return rc;
+  if ((rc = sync(x))) return rc;
+  x->have_dq = true;
+  if (dq && (rc = download_x(x, dq))) return rc;
+  if (info) {
+    info->iterations = x->P.gauss_seidel_iter;
+    info->status = FPSI_OK;
+    info->resid0 = info->resid = 0;
+  }
+  return FPSI_OK;
+}
+
+int fpsi_linear_residual(fpsi_ctx* x, double* norm_b, double* norm_r) {
+  if (!x) return FPSI_E_INVALID;
+  if (!x->have_asm || !x->d_D) return FPSI_E_STATE;
+  int rc = fpsi::launch_linres(x, x->d_resid + 8);
+  if (rc) return rc;
+  FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid + 8, x->d_resid + 8, 2 * sizeof(double),
+                                cudaMemcpyDeviceToHost, x->stream));
+  if ((rc = sync(x))) return rc;
+  if (norm_b) *norm_b = x->h_resid[8];
+  if (norm_r) *norm_r = x->h_resid[9];
+  return FPSI_OK;
+}
+
+int fpsi_update(fpsi_ctx* x, double* min_alpha) {
+  if (!x) return FPSI_E_INVALID;
+  if (!x->have_dq) return FPSI_E_STATE;
+  int rc = fpsi::launch_update(x);
+  if (rc) return rc;
+  std::vector<double> a(x->nblk_norm);
+  FPSI_CUDA_TRY(cudaMemcpyAsync(a.data(), x->d_amin, a.size() * sizeof(double),
+                                cudaMemcpyDeviceToHost, x->stream));
+  if ((rc = sync(x))) return rc;
+  if (min_alpha) *min_alpha = *std::min_element(a.begin(), a.end());
+  x->have_resid = x->have_asm = x->have_dq = false;
+  return FPSI_OK;
+}
+
+int fpsi_newton_step(fpsi_ctx* x, fpsi_stepinfo* info) {
+  if (!x) return FPSI_E_INVALID;
+  int rc;
+  if ((rc = fpsi::launch_residual(x, x->d_resid))) return rc;
+  if ((rc = fpsi::launch_assemble(x, nullptr))) return rc;
+  if ((rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter))) return rc;
+  if ((rc = fpsi::launch_update(x))) return rc;
+  FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid, x->d_resid, 8 * sizeof(double),
+                                cudaMemcpyDeviceToHost, x->stream));
+  std::vector<double> a(x->nblk_norm);
+  FPSI_CUDA_TRY(cudaMemcpyAsync(a.data(), x->d_amin, a.size() * sizeof(double),
+                                cudaMemcpyDeviceToHost, x->stream));
+  if ((rc = finish_assemble(x))) return rc;
+  x->have_resid = x->have_asm = x->have_dq = false;
+  if (info) {
+    std::memset(info, 0, sizeof(*info));
+    fill_norms(x, x->h_resid, &info->resid);
+    info->ls.iterations = x->P.gauss_seidel_iter;
+    info->min_alpha = *std::min_element(a.begin(), a.end());
+  }
+  return has_nan(x->h_resid) ? FPSI_E_NAN : FPSI_OK;
+}
+
+int fpsi_run(fpsi_ctx* x, int32_t nsteps, fpsi_resid* norms) {
+  if (!x || nsteps < 0) return FPSI_E_INVALID;
+  if (nsteps == 0) return FPSI_OK;
+  double* hist = nullptr;
+  if (cudaMalloc((void**)&hist, size_t(nsteps) * 8 * sizeof(double)) != cudaSuccess) {
+    fpsi::set_error("cudaMalloc of the residual history failed");
+    return FPSI_E_NOMEM;
+  }
+  int rc = FPSI_OK;
+  for (int32_t s = 0; s < nsteps && !rc; ++s) {
+    rc = fpsi::launch_residual(x, hist + 8 * s);
+    if (!rc) rc = fpsi::launch_assemble(x, nullptr);
+    if (!rc) rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter);
+    if (!rc) rc = fpsi::launch_update(x);
+  }
+  std::vector<double> h(size_t(nsteps) * 8);
+  if (!rc && cudaMemcpyAsync(h.data(), hist, h.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                             x->stream) != cudaSuccess)
+    rc = FPSI_E_CUDA;
+  if (!rc) rc = finish_assemble(x);
+  cudaFree(hist);
+  x->have_resid = x->have_asm = x->have_dq = false;
+  if (rc) return rc;
+  bool nan = false;
+  for (int32_t s = 0; s < nsteps; ++s) {
+    if (norms) fill_norms(x, &h[8 * s], &norms[s]);
+    nan = nan || has_nan(&h[8 * s]);
+  }
+  return nan ? FPSI_E_NAN : FPSI_OK;
+}
+
+static int run_steps(fpsi_ctx* x, int32_t nsteps, double* hist) {
+  int rc = FPSI_OK;
+  for (int32_t s = 0; s < nsteps && !rc; ++s) {
+    rc = fpsi::launch_residual(x, hist + 8 * s);
+    if (!rc) rc = fpsi::launch_assemble(x, nullptr);
+    if (!rc) rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter);
+    if (!rc) rc = fpsi::launch_update(x);
+  }
+  return rc;
+}
+
+int fpsi_run_timed(fpsi_ctx* x, int32_t nsteps, fpsi_resid* norms, double* device_ms) {
+  if (!x || nsteps <= 0 || !device_ms) return FPSI_E_INVALID;
+  double* hist = nullptr;
+  if (cudaMalloc((void**)&hist, size_t(nsteps) * 8 * sizeof(double)) != cudaSuccess) {
+    fpsi::set_error("cudaMalloc of the residual history failed");
+    return FPSI_E_NOMEM;
+  }
+  cudaEvent_t a = nullptr, b = nullptr;
+  int rc = FPSI_OK;
+  if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) rc = FPSI_E_CUDA;
+  if (!rc && cudaEventRecord(a, x->stream) != cudaSuccess) rc = FPSI_E_CUDA;
+  if (!rc) rc = run_steps(x, nsteps, hist);
+  if (!rc && cudaEventRecord(b, x->stream) != cudaSuccess) rc = FPSI_E_CUDA;
+  std::vector<double> h(size_t(nsteps) * 8);
+  if (!rc && cudaMemcpyAsync(h.data(), hist, h.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                             x->stream) != cudaSuccess)
+    rc = FPSI_E_CUDA;
+  if (!rc) rc = finish_assemble(x);
+  float ms = 0;
+  if (!rc && cudaEventElapsedTime(&ms, a, b) != cudaSuccess) rc = FPSI_E_CUDA;
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  cudaFree(hist);
+  x->have_resid = x->have_asm = x->have_dq = false;
+  if (rc) return rc;
+  *device_ms = ms;
+  bool nan = false;
+  for (int32_t s = 0; s < nsteps; ++s) {
+    if (norms) fill_norms(x, &h[8 * s], &norms[s]);
+    nan = nan || has_nan(&h[8 * s]);
+  }
+  return nan ? FPSI_E_NAN : FPSI_OK;
+}
+
+int fpsi_kernel_times(fpsi_ctx* x, int32_t nsteps, int32_t cap, char* names, double* ms,
+                      int64_t* launches, int32_t* count) {
+  if (!x || nsteps <= 0 || cap < 0 || !count) return FPSI_E_INVALID;
+  double* hist = nullptr;
+  if (cudaMalloc((void**)&hist, size_t(nsteps) * 8 * sizeof(double)) != cudaSuccess)
+    return FPSI_E_NOMEM;
+  x->prof.clear();
+  x->evnext = 0;
+  x->profiling = true;
+  int rc = run_steps(x, nsteps, hist);
+  x->profiling = false;
+  if (!rc) rc = sync(x);
+  cudaFree(hist);
+  x->have_resid = x->have_asm = x->have_dq = false;
+  if (rc) return rc;
+  std::vector<std::string> keys;
+  std::vector<double> tot;
+  std::vector<int64_t> cnt;
+  for (const fpsi_prof_rec& r : x->prof) {
+    float t = 0;
+    FPSI_CUDA_TRY(cudaEventElapsedTime(&t, r.a, r.b));
+    size_t k = 0;
+    while (k < keys.size() && keys[k] != r.name) ++k;
+    if (k == keys.size()) {
+      keys.push_back(r.name);
+      tot.push_back(0);
+      cnt.push_back(0);
+    }
+    tot[k] += t;
+    cnt[k] += 1;
+  }
+  x->prof.clear();
+  *count = int32_t(keys.size());
+  for (size_t k = 0; k < keys.size() && int32_t(k) < cap; ++k) {
+    if (names) {
+      std::memset(names + 32 * k, 0, 32);
+      std::strncpy(names + 32 * k, keys[k].c_str(), 31);
+    }
+    if (ms) ms[k] = tot[k];
+    if (launches) launches[k] = cnt[k];
+  }
+  return FPSI_OK;
+}
+
+// ---- batched face functions ----------------------------------------------
+static int batch_common(int64_t n, const double* qL, const double* qR, const double* an,
+                        const double* area, double** dL, double** dR, double** dA,
+                        double** dS) {
+  if (n <= 0 || !qL || !qR || !an || !area) return FPSI_E_INVALID;
+  if (!fpsi_device_available()) {
+    fpsi::set_error("no CUDA device");
+    return FPSI_E_CUDA;
+  }
+  FPSI_CUDA_TRY(cudaMalloc((void**)dL, n * 5 * sizeof(double)));
+  FPSI_CUDA_TRY(cudaMalloc((void**)dR, n * 5 * sizeof(double)));
+  FPSI_CUDA_TRY(cudaMalloc((void**)dA, n * 3 * sizeof(double)));
+  FPSI_CUDA_TRY(cudaMalloc((void**)dS, n * sizeof(double)));
+  FPSI_CUDA_TRY(cudaMemcpy(*dL, qL, n * 5 * sizeof(double), cudaMemcpyHostToDevice));
+  FPSI_CUDA_TRY(cudaMemcpy(*dR, qR, n * 5 * sizeof(double), cudaMemcpyHostToDevice));
+  FPSI_CUDA_TRY(cudaMemcpy(*dA, an, n * 3 * sizeof(double), cudaMemcpyHostToDevice));
+  FPSI_CUDA_TRY(cudaMemcpy(*dS, area, n * sizeof(double), cudaMemcpyHostToDevice));
+  return FPSI_OK;
+}
+
+int fpsi_face_flux(int32_t kind, int64_t n, const double* qL, const double* qR,
+                   const double* an, const double* area, double pambient, double Rt,
+                   double gamma, double us_n, double eta, double* flux) {
+  if (kind < 0 || kind > 2 || !flux) return FPSI_E_INVALID;
+  double *dL = nullptr, *dR = nullptr, *dA = nullptr, *dS = nullptr, *dF = nullptr;
+  int rc = batch_common(n, qL, qR, an, area, &dL, &dR, &dA, &dS);
+  if (!rc && cudaMalloc((void**)&dF, n * 5 * sizeof(double)) != cudaSuccess) rc = FPSI_E_NOMEM;
+  if (!rc) rc = fpsi::launch_batch_flux(kind, n, dL, dR, dA, dS, pambient, Rt, gamma, us_n, eta, dF, 0);
+  if (!rc && cudaMemcpy(flux, dF, n * 5 * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = FPSI_E_CUDA;
+  cudaFree(dL), cudaFree(dR), cudaFree(dA), cudaFree(dS), cudaFree(dF);
+  return rc;
+}
+
+int fpsi_face_jacobian(int64_t n, const double* qL, const double* qR, const double* an,
+                       const double* area, double pambient, double Rt, double gamma,
+                       double us_n, double eta, int32_t dir, int32_t as_double, void* out) {
+  if (!out || (dir != 1 && dir != -1)) return FPSI_E_INVALID;
+  double *dL = nullptr, *dR = nullptr, *dA = nullptr, *dS = nullptr;
+  void* dO = nullptr;
+  const size_t ob = size_t(n) * 25 * (as_double ? 8 : 4);
+  int rc = batch_common(n, qL, qR, an, area, &dL, &dR, &dA, &dS);
+  if (!rc && cudaMalloc(&dO, ob) != cudaSuccess) rc = FPSI_E_NOMEM;
+  if (!rc)
+    rc = fpsi::launch_batch_jac(n, dL, dR, dA, dS, pambient, Rt, gamma, us_n, eta, dir, as_double,
+                                dO, 0);
+  if (!rc && cudaMemcpy(out, dO, ob, cudaMemcpyDeviceToHost) != cudaSuccess) rc = FPSI_E_CUDA;
+  cudaFree(dL), cudaFree(dR), cudaFree(dA), cudaFree(dS), cudaFree(dO);
+  return rc;
+}
+
+}  // extern "C"

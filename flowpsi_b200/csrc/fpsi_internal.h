@@ -1,0 +1,117 @@
+// fpsi_internal.h -- device context of the B200 implicit path (not part of the ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/fpsi.h"
+
+namespace fpsi {
+
+void set_error(const char* fmt, ...);
+
+#define FPSI_CUDA_TRY(expr)                                                          \
+  do {                                                                               \
+    cudaError_t e_ = (expr);                                                         \
+    if (e_ != cudaSuccess) {                                                         \
+      ::fpsi::set_error("%s:%d %s: %s", __FILE__, __LINE__, #expr, cudaGetErrorString(e_)); \
+      return FPSI_E_CUDA;                                                            \
+    }                                                                                \
+  } while (0)
+
+// Host-side mesh after setup: RCM cell order, faces sorted by (cl, cr) with
+// interior faces first and boundary faces last.
+struct HostMesh {
+  int64_t nc = 0, nf = 0, nfi = 0, nbf = 0;
+  std::vector<int32_t> perm;     // new cell id -> caller cell id
+  std::vector<int32_t> iperm;    // caller cell id -> new cell id
+  std::vector<int64_t> fperm;    // new face id -> caller face id
+  std::vector<int32_t> cl, cr;   // new numbering; cr < 0 = -(bc)-1
+  std::vector<double> n, area;   // n: nf*3 (AoS on host)
+  std::vector<double> rL, rR;    // nf*3
+  std::vector<double> vol, cc;   // nc, nc*3
+  std::vector<double> Minv;      // nc*6
+  std::vector<double> an_caller, area_caller, fc_caller;  // caller order, for export
+  std::vector<int32_t> cf_off;   // nc+1
+  std::vector<int32_t> cf;       // (face << 1) | side ; upper, lower, boundary order
+  std::vector<int32_t> colour;   // nc (new numbering)
+  int ncolours = 0;
+  std::vector<int32_t> colour_off;   // ncolours+1 into colour_cells
+  std::vector<int32_t> colour_cells; // cells of each colour, increasing
+  double vol_tot = 0;
+};
+
+int build_host_mesh(const fpsi_mesh* m, HostMesh& h);
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+};
+
+}  // namespace fpsi
+
+struct fpsi_prof_rec {
+  const char* name;
+  cudaEvent_t a, b;
+};
+
+struct fpsi_ctx {
+  fpsi_params P;
+  fpsi::HostMesh H;
+  std::vector<fpsi_bc> bcs;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  // ---- device arrays (new numbering) ----
+  // geometry
+  int32_t *d_cl = nullptr, *d_cr = nullptr;
+  double *d_n = nullptr, *d_area = nullptr;      // SoA: n[3][nf], area[nf]
+  double *d_rL = nullptr, *d_rR = nullptr;       // SoA: [3][nf]
+  double *d_vol = nullptr, *d_cc = nullptr;      // vol[nc], cc[3][nc]
+  double* d_Minv = nullptr;                      // [6][nc]
+  int32_t *d_cf_off = nullptr, *d_cf = nullptr;
+  int32_t* d_colour_cells = nullptr;
+  fpsi_bc* d_bcs = nullptr;
+  // state and residual
+  double* d_q = nullptr;       // [nc][5]  T,u,v,w,pg
+  double* d_qb = nullptr;      // [nbf][5] boundary face states
+  double* d_grad = nullptr;    // [nc][15]
+  double* d_phi = nullptr;     // [nc][5]
+  double* d_F = nullptr;       // [nf][5] face fluxes
+  double* d_mev = nullptr;     // [nf] maxev_f * area
+  double* d_src = nullptr;     // [nc][5]
+  double* d_dtau = nullptr;    // [nc]
+  double* d_part = nullptr;    // per-block partial norms
+  double* d_resid = nullptr;   // 16 doubles: final norms
+  double* h_resid = nullptr;   // pinned mirror
+  int nblk_norm = 0;
+  // implicit system (block type depends on precision)
+  void* d_fjp = nullptr;       // [nf][25] TB
+  void* d_fjm = nullptr;       // [nf][25] TB
+  void* d_cellblk = nullptr;   // [nc][32] TB : LU(25) B(5) piv(1) pad(1)
+  void* d_D = nullptr;         // [nc][25] TB (only when keep_D)
+  void* d_x = nullptr;         // [nc][5] TX
+  double* d_amin = nullptr;    // per-block min alpha
+  int32_t* d_err = nullptr;    // error flags (singular pivots, ...)
+  int blk_bytes = 4;           // sizeof(TB)
+  int x_bytes = 8;             // sizeof(TX)
+  int alloc_prec = -1;
+  bool keep_D = true;
+  bool have_resid = false, have_asm = false, have_dq = false;
+  int64_t device_bytes = 0;
+  // caller-order staging for state transfers (T, pg, u) and the permutation
+  int32_t* d_perm = nullptr;   // new cell id -> caller cell id
+  double* d_stage = nullptr;   // [nc] T, [nc] pg, [3 nc] u (caller order)
+  // per-kernel timing (fpsi_kernel_times)
+  bool profiling = false;
+  std::vector<fpsi_prof_rec> prof;
+  std::vector<cudaEvent_t> evpool;
+  size_t evnext = 0;
+};
+
+namespace fpsi {
+void prof_begin(fpsi_ctx* x, const char* name);
+void prof_end(fpsi_ctx* x);
+}  // namespace fpsi

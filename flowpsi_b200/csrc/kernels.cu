@@ -1,0 +1,1054 @@
+// kernels.cu -- sm_100a kernels of the steady implicit step.
+//
+// Data layout in HBM (RCM cell order, faces sorted by cl, interior first):
+//   q      [nc][5]  FP64  T,u,v,w,pg          (AoS: every gather is one 40 B record)
+//   grad   [nc][15] FP64  dT/dx.. dpg/dz
+//   phi    [nc][5]  FP64  limiter per variable
+//   F      [nf][5]  FP64  face flux, mev [nf] maxev_f*area
+//   src    [nc][5]  FP64, dtau [nc]
+//   fjp/fjm [nf][25] TB   (TB = float in REF/MIXED precision, double in FP64)
+//   cellblk [nc][32] TB   LU(25) B(5) pivots(1) pad(1)  -- one 128 B line in FP32
+//   x      [nc][5]  TX    iterate (TX = double in FP64/REF, float in MIXED)
+// geometry is SoA: n[3][nf], area[nf], rL[3][nf], rR[3][nf], Minv[6][nc].
+//
+// Every reduction has a fixed order (per-cell loops over a fixed face list,
+// fixed-shape block trees), so results are bitwise reproducible run to run.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "fpsi_internal.h"
+#include "kernels.cuh"
+#include "physics.cuh"
+
+namespace fpsi {
+namespace dev {
+
+struct MeshView {
+  int64_t nc, nf, nfi;
+  const int32_t* cl;
+  const int32_t* cr;
+  const double* n;     // [3][nf]
+  const double* area;  // [nf]
+  const double* rL;    // [3][nf]
+  const double* rR;    // [3][nf]
+  const double* vol;
+  const double* Minv;  // [6][nc]
+  const int32_t* cf_off;
+  const int32_t* cf;
+};
+
+__device__ __forceinline__ Q5 load_q(const double* q, int64_t c) {
+  const double* p = q + 5 * c;
+  Q5 r;
+  r.T = __ldg(p + 0);
+  r.u = __ldg(p + 1);
+  r.v = __ldg(p + 2);
+  r.w = __ldg(p + 3);
+  r.p = __ldg(p + 4);
+  return r;
+}
+__device__ __forceinline__ void q_arr(const Q5& q, double a[5]) {
+  a[0] = q.T, a[1] = q.u, a[2] = q.v, a[3] = q.w, a[4] = q.p;
+}
+
+// ---------------------------------------------------------------------------
+// boundary face states (bcInflow.loci:270-344, bcOutflow.loci:84-142,
+// bcImpermeable.loci:48-140); eta == 1
+// ---------------------------------------------------------------------------
+__global__ void k_bc_state(MeshView M, const double* __restrict__ q, const fpsi_bc* __restrict__ bcs,
+                           Gas g, double* __restrict__ qb) {
+  const int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t nbf = M.nf - M.nfi;
+  if (b >= nbf) return;
+  const int64_t f = M.nfi + b;
+  const int32_t c = M.cl[f];
+  const fpsi_bc bc = bcs[-M.cr[f] - 1];
+  const double nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
+  const Q5 qi = load_q(q, c);
+  Q5 q0;
+  q0.T = bc.T, q0.u = bc.u[0], q0.v = bc.u[1], q0.w = bc.u[2], q0.p = bc.pg;
+  Q5 r = qi;
+  switch (bc.kind) {
+    case FPSI_BC_FARFIELD: {
+      const double uit = qi.u * nx + qi.v * ny + qi.w * nz;
+      const double ai = sqrt(g.gamma * g.Rt * qi.T);
+      const double a0 = sqrt(g.gamma * g.Rt * q0.T);
+      if (uit > 0) {
+        if (!(uit > ai)) cv_state(true, qi, q0, nx, ny, nz, 0.0, g, 1.0, r);
+      } else {
+        if (-uit > a0)
+          r = q0;
+        else
+          cv_state(false, qi, q0, nx, ny, nz, 0.0, g, 1.0, r);
+      }
+      break;
+    }
+    case FPSI_BC_SUPERSONIC_INFLOW:
+      r = q0;
+      break;
+    case FPSI_BC_SUPERSONIC_OUTFLOW: {
+      const double ai = sqrt(g.gamma * g.Rt * qi.T);
+      const double ut = qi.u * nx + qi.v * ny + qi.w * nz;
+      if (ut < ai) r.p -= (qi.p + g.pamb) * 0.1;
+      break;
+    }
+    case FPSI_BC_REFLECTING: {
+      const double un = qi.u * nx + qi.v * ny + qi.w * nz;
+      r.u = qi.u - 2.0 * un * nx;
+      r.v = qi.v - 2.0 * un * ny;
+      r.w = qi.w - 2.0 * un * nz;
+      break;
+    }
+    default:
+      break;
+  }
+  double* o = qb + 5 * b;
+  o[0] = r.T, o[1] = r.u, o[2] = r.v, o[3] = r.w, o[4] = r.p;
+}
+
+// ---------------------------------------------------------------------------
+// least-squares gradient + limiter, one thread per cell
+// ---------------------------------------------------------------------------
+__global__ void k_grad_limiter(MeshView M, const double* __restrict__ q,
+                               const double* __restrict__ qb, int limiter, double Kl,
+                               double* __restrict__ grad, double* __restrict__ phi) {
+  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c >= M.nc) return;
+  double qc[5];
+  q_arr(load_q(q, c), qc);
+  double b[15];
+  double qmax[5], qmin[5];
+#pragma unroll
+  for (int k = 0; k < 15; ++k) b[k] = 0.0;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) qmax[k] = qmin[k] = qc[k];
+  const int32_t e0 = M.cf_off[c], e1 = M.cf_off[c + 1];
+  const int64_t nf = M.nf;
+  for (int32_t e = e0; e < e1; ++e) {
+    const int32_t ent = M.cf[e];
+    const int64_t f = ent >> 1;
+    const int side = ent & 1;
+    double qn[5];
+    double d[3];
+    if (f >= M.nfi) {
+      const double* p = qb + 5 * (f - M.nfi);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) qn[k] = __ldg(p + k);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) d[k] = M.rL[k * nf + f];
+    } else {
+      const int32_t o = side ? M.cl[f] : M.cr[f];
+      q_arr(load_q(q, o), qn);
+      const double sg = side ? -1.0 : 1.0;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) d[k] = sg * (M.rL[k * nf + f] - M.rR[k * nf + f]);
+    }
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const double dq = qn[k] - qc[k];
+      b[3 * k] += d[0] * dq;
+      b[3 * k + 1] += d[1] * dq;
+      b[3 * k + 2] += d[2] * dq;
+      qmax[k] = dmax(qmax[k], qn[k]);
+      qmin[k] = dmin(qmin[k], qn[k]);
+    }
+  }
+  const double m0 = M.Minv[c], m1 = M.Minv[M.nc + c], m2 = M.Minv[2 * M.nc + c],
+               m3 = M.Minv[3 * M.nc + c], m4 = M.Minv[4 * M.nc + c], m5 = M.Minv[5 * M.nc + c];
+  double g[15];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const double bx = b[3 * k], by = b[3 * k + 1], bz = b[3 * k + 2];
+    g[3 * k] = m0 * bx + m1 * by + m2 * bz;
+    g[3 * k + 1] = m1 * bx + m3 * by + m4 * bz;
+    g[3 * k + 2] = m2 * bx + m4 * by + m5 * bz;
+  }
+  double ph[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) ph[k] = limiter == FPSI_LIMITER_ZERO ? 0.0 : 1.0;
+  if (limiter == FPSI_LIMITER_VENKATAKRISHNAN || limiter == FPSI_LIMITER_BARTH) {
+    const double h = cbrt(M.vol[c]);
+    const double kh = Kl * h;
+    const double eps2 = kh * kh * kh;
+    for (int32_t e = e0; e < e1; ++e) {
+      const int32_t ent = M.cf[e];
+      const int64_t f = ent >> 1;
+      const double* r = (ent & 1) ? M.rR : M.rL;
+      const double rx = r[f], ry = r[nf + f], rz = r[2 * nf + f];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        const double d2 = g[3 * k] * rx + g[3 * k + 1] * ry + g[3 * k + 2] * rz;
+        double p = 1.0;
+        if (d2 != 0.0) {
+          const double d1 = d2 > 0 ? qmax[k] - qc[k] : qmin[k] - qc[k];
+          if (limiter == FPSI_LIMITER_BARTH) {
+            p = dmin(1.0, d1 / d2);
+          } else {
+            const double num = (d1 * d1 + eps2) + 2.0 * d2 * d1;
+            const double den = d1 * d1 + 2.0 * d2 * d2 + d1 * d2 + eps2;
+            p = dmin(1.0, num / den);
+          }
+        }
+        ph[k] = dmin(ph[k], p);
+      }
+    }
+  }
+  double* go = grad + 15 * c;
+#pragma unroll
+  for (int k = 0; k < 15; ++k) go[k] = g[k];
+  double* po = phi + 5 * c;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) po[k] = ph[k];
+}
+
+// MUSCL states of one face: q_c + phi*grad.(x_f - x_c), floors 0.1*min(T),
+// 0.1*min(pg) - 0.9*Pambient (the form of fluxLowDiss.loci:338-356).
+struct FaceStates {
+  Q5 L, R;
+  double ql[5], qr[5];  // cell-centre (unreconstructed) values of both sides
+};
+
+__device__ __forceinline__ void reconstruct(const MeshView& M, const double* __restrict__ q,
+                                            const double* __restrict__ qb,
+                                            const double* __restrict__ grad,
+                                            const double* __restrict__ phi, int64_t f,
+                                            double pamb, FaceStates& s) {
+  const int64_t nf = M.nf;
+  const int32_t a = M.cl[f];
+  const bool bnd = f >= M.nfi;
+  q_arr(load_q(q, a), s.ql);
+  if (bnd) {
+    const double* p = qb + 5 * (f - M.nfi);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) s.qr[k] = __ldg(p + k);
+  } else {
+    q_arr(load_q(q, M.cr[f]), s.qr);
+  }
+  const double tlim = 0.1 * dmin(s.ql[0], s.qr[0]);
+  const double plim = 0.1 * dmin(s.ql[4], s.qr[4]) - 0.9 * pamb;
+  double l[5], r[5];
+  {
+    const double rx = M.rL[f], ry = M.rL[nf + f], rz = M.rL[2 * nf + f];
+    const double* g = grad + 15 * int64_t(a);
+    const double* ph = phi + 5 * int64_t(a);
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+      l[k] = s.ql[k] + __ldg(ph + k) * (__ldg(g + 3 * k) * rx + __ldg(g + 3 * k + 1) * ry +
+                                        __ldg(g + 3 * k + 2) * rz);
+  }
+  l[0] = dmax(l[0], tlim);
+  l[4] = dmax(l[4], plim);
+  if (bnd) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) r[k] = s.qr[k];
+  } else {
+    const int64_t d = M.cr[f];
+    const double rx = M.rR[f], ry = M.rR[nf + f], rz = M.rR[2 * nf + f];
+    const double* g = grad + 15 * d;
+    const double* ph = phi + 5 * d;
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+      r[k] = s.qr[k] + __ldg(ph + k) * (__ldg(g + 3 * k) * rx + __ldg(g + 3 * k + 1) * ry +
+                                        __ldg(g + 3 * k + 2) * rz);
+    r[0] = dmax(r[0], tlim);
+    r[4] = dmax(r[4], plim);
+  }
+  s.L.T = l[0], s.L.u = l[1], s.L.v = l[2], s.L.w = l[3], s.L.p = l[4];
+  s.R.T = r[0], s.R.u = r[1], s.R.v = r[2], s.R.w = r[3], s.R.p = r[4];
+}
+
+// ---------------------------------------------------------------------------
+// face flux + spectral radius, one thread per face
+// ---------------------------------------------------------------------------
+__global__ void k_face_flux(MeshView M, const double* __restrict__ q,
+                            const double* __restrict__ qb, const double* __restrict__ grad,
+                            const double* __restrict__ phi, Gas g, int kind,
+                            double* __restrict__ F, double* __restrict__ mev) {
+  const int64_t f = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (f >= M.nf) return;
+  FaceStates s;
+  reconstruct(M, q, qb, grad, phi, f, g.pamb, s);
+  const double nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
+  const double A = M.area[f];
+  double fl[5];
+  riemann(kind, s.L, s.R, nx, ny, nz, A, g, 0.0, 1.0, fl);
+  double* o = F + 5 * f;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) o[k] = fl[k];
+  // maxev_f (solverSetup.loci:81-105), eta == 1: |u.n| + a of each side
+  const double utr = s.qr[1] * nx + s.qr[2] * ny + s.qr[3] * nz;
+  const double ar = sqrt(g.gamma * g.Rt * s.qr[0]);
+  const double sr = sqrt(4.0 * ar * ar);
+  double m = 0.5 * dmax(fabs(2.0 * utr - sr), fabs(2.0 * utr + sr));
+  if (f < M.nfi) {
+    const double utl = s.ql[1] * nx + s.ql[2] * ny + s.ql[3] * nz;
+    const double al = sqrt(g.gamma * g.Rt * s.ql[0]);
+    const double sl = sqrt(4.0 * al * al);
+    m = dmax(0.5 * dmax(fabs(2.0 * utl - sl), fabs(2.0 * utl + sl)), m);
+  }
+  mev[f] = m * A;
+}
+
+// ---------------------------------------------------------------------------
+// per-cell residual gather, local time step and norm partials
+// ---------------------------------------------------------------------------
+constexpr int NORM_THREADS = 256;
+
+__global__ void __launch_bounds__(NORM_THREADS)
+k_cell_residual(MeshView M, const double* __restrict__ q, const double* __restrict__ F,
+                const double* __restrict__ mev, Gas g, double urelax, double dtmax,
+                double cflmax, double vol_tot, double* __restrict__ src,
+                double* __restrict__ dtau, double* __restrict__ part) {
+  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  double rt = 0, et = 0, mt = 0, rmax = 0, emax = 0, mmax = 0;
+  double rloc = -1, eloc = -1;
+  if (c < M.nc) {
+    double s[5] = {0, 0, 0, 0, 0};
+    double meva = 0;
+    for (int32_t e = M.cf_off[c]; e < M.cf_off[c + 1]; ++e) {
+      const int32_t ent = M.cf[e];
+      const int64_t f = ent >> 1;
+      const double* p = F + 5 * f;
+      if (ent & 1) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) s[k] += p[k];
+      } else {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) s[k] -= p[k];
+      }
+      meva += mev[f];
+    }
+    double* so = src + 5 * c;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) so[k] = s[k];
+    const double V = M.vol[c];
+    const double cflpdt = 0.5 * meva / V;
+    double dt = dtmax;
+    if (cflmax > 0) dt = dmin(dt, cflmax / cflpdt);
+    const Q5 qc = load_q(q, c);
+    // dtau, solverTimestep.loci:302-329 with eta == 1
+    const double rvol = 1.0 / V;
+    const double p = qc.p + g.pamb, T = qc.T;
+    const double rP = 1.0 / (g.Rt * T);
+    const double rho = p * rP;
+    const double rT = -rho / T;
+    const double qk = 0.5 * (qc.u * qc.u + qc.v * qc.v + qc.w * qc.w);
+    const double fT = rT * qk, fP = 1.0 / (g.gamma - 1.0) + rP * qk;
+    const double cterm = fP * rT - fT * rP;
+    const double dsu = s[1] * qc.u + s[2] * qc.v + s[3] * qc.w;
+    const double dtemp =
+        rvol * (s[0] * (fP * rT) + (dsu - s[4] - 2.0 * qk * s[0]) * (rT * rP)) / (cterm * rT);
+    dt = dmin(dt, urelax * T / (fabs(dtemp) + 1e-30));
+    const double dp = rvol * (rT * (2.0 * qk * s[0] - dsu + s[4]) - fT * s[0]);
+    dt = dmin(dt, urelax * p / (fabs(dp) + 1e-30));
+    dtau[c] = dt;
+    // norms (solverResidual.loci:74-112)
+    const double w = V / vol_tot;
+    const double a0 = rvol * s[0], a4 = rvol * s[4];
+    rt = w * (a0 * a0);
+    et = w * (a4 * a4);
+    double mm = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const double a = rvol * s[1 + i];
+      if (fabs(mmax) < fabs(a)) mmax = a;
+      mm += a * a;
+    }
+    mt = mm * (w / 3.0);
+    rmax = a0, emax = a4;
+    rloc = double(c), eloc = double(c);
+  }
+  // fixed-shape block tree: sums and signed max-abs with lowest-index ties
+  __shared__ double sh[8][NORM_THREADS];
+  const int t = threadIdx.x;
+  sh[0][t] = rt, sh[1][t] = et, sh[2][t] = mt;
+  sh[3][t] = rmax, sh[4][t] = rloc, sh[5][t] = emax, sh[6][t] = eloc, sh[7][t] = mmax;
+  __syncthreads();
+  for (int st = NORM_THREADS / 2; st > 0; st >>= 1) {
+    if (t < st) {
+      sh[0][t] += sh[0][t + st];
+      sh[1][t] += sh[1][t + st];
+      sh[2][t] += sh[2][t + st];
+      if (fabs(sh[3][t + st]) > fabs(sh[3][t]) ||
+          (fabs(sh[3][t + st]) == fabs(sh[3][t]) && sh[4][t] < 0)) {
+        sh[3][t] = sh[3][t + st];
+        sh[4][t] = sh[4][t + st];
+      }
+      if (fabs(sh[5][t + st]) > fabs(sh[5][t]) ||
+          (fabs(sh[5][t + st]) == fabs(sh[5][t]) && sh[6][t] < 0)) {
+        sh[5][t] = sh[5][t + st];
+        sh[6][t] = sh[6][t + st];
+      }
+      if (fabs(sh[7][t + st]) > fabs(sh[7][t])) sh[7][t] = sh[7][t + st];
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    double* o = part + 8 * int64_t(blockIdx.x);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) o[k] = sh[k][0];
+  }
+}
+
+// out[0..2] = rms (sqrt of sums), out[3..4] rtmax/loc, out[5..6] etmax/loc,
+// out[7] mtmax; written to slot `step` of a per-run history
+__global__ void k_norm_final(const double* __restrict__ part, int nblk,
+                             double* __restrict__ out) {
+  __shared__ double sh[8][NORM_THREADS];
+  const int t = threadIdx.x;
+  double a[8] = {0, 0, 0, 0, -1, 0, -1, 0};
+  for (int i = t; i < nblk; i += NORM_THREADS) {
+    const double* p = part + 8 * int64_t(i);
+    a[0] += p[0], a[1] += p[1], a[2] += p[2];
+    if (fabs(p[3]) > fabs(a[3]) || (fabs(p[3]) == fabs(a[3]) && a[4] < 0)) a[3] = p[3], a[4] = p[4];
+    if (fabs(p[5]) > fabs(a[5]) || (fabs(p[5]) == fabs(a[5]) && a[6] < 0)) a[5] = p[5], a[6] = p[6];
+    if (fabs(p[7]) > fabs(a[7])) a[7] = p[7];
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) sh[k][t] = a[k];
+  __syncthreads();
+  for (int st = NORM_THREADS / 2; st > 0; st >>= 1) {
+    if (t < st) {
+      sh[0][t] += sh[0][t + st];
+      sh[1][t] += sh[1][t + st];
+      sh[2][t] += sh[2][t + st];
+      if (fabs(sh[3][t + st]) > fabs(sh[3][t]) ||
+          (fabs(sh[3][t + st]) == fabs(sh[3][t]) && sh[4][t + st] >= 0 &&
+           (sh[4][t] < 0 || sh[4][t + st] < sh[4][t]))) {
+        sh[3][t] = sh[3][t + st];
+        sh[4][t] = sh[4][t + st];
+      }
+      if (fabs(sh[5][t + st]) > fabs(sh[5][t]) ||
+          (fabs(sh[5][t + st]) == fabs(sh[5][t]) && sh[6][t + st] >= 0 &&
+           (sh[6][t] < 0 || sh[6][t + st] < sh[6][t]))) {
+        sh[5][t] = sh[5][t + st];
+        sh[6][t] = sh[6][t + st];
+      }
+      if (fabs(sh[7][t + st]) > fabs(sh[7][t])) sh[7][t] = sh[7][t + st];
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    out[0] = sqrt(sh[0][0]);
+    out[1] = sqrt(sh[1][0]);
+    out[2] = sqrt(sh[2][0]);
+#pragma unroll
+    for (int k = 3; k < 8; ++k) out[k] = sh[k][0];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// face Jacobians fjp (dir +1) and fjm (dir -1), one thread per face
+// ---------------------------------------------------------------------------
+template <class TB>
+__global__ void k_face_jacobian(MeshView M, const double* __restrict__ q,
+                                const double* __restrict__ qb, const double* __restrict__ grad,
+                                const double* __restrict__ phi, Gas g, TB* __restrict__ fjp,
+                                TB* __restrict__ fjm) {
+  const int64_t f = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (f >= M.nf) return;
+  FaceStates s;
+  reconstruct(M, q, qb, grad, phi, f, g.pamb, s);
+  const double nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
+  const double A = M.area[f];
+  const RoeAvg ra = roe_average(s.L, s.R, nx, ny, nz, g, 0.0, 1.0);
+  TB blk[25];
+  jac_roe<TB>(ra, nx, ny, nz, A, g, +1, blk);
+  TB* o = fjp + 25 * f;
+#pragma unroll
+  for (int k = 0; k < 25; ++k) o[k] = blk[k];
+  if (f < M.nfi) {
+    jac_roe<TB>(ra, nx, ny, nz, A, g, -1, blk);
+    o = fjm + 25 * f;
+#pragma unroll
+    for (int k = 0; k < 25; ++k) o[k] = blk[k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 5x5 LU with partial pivoting and its solve
+// ---------------------------------------------------------------------------
+template <class TB>
+__device__ __forceinline__ bool lu5(TB* A, int* piv) {
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    int p = k;
+    TB best = fabs(A[5 * k + k]);
+#pragma unroll
+    for (int i = k + 1; i < 5; ++i) {
+      const TB v = fabs(A[5 * i + k]);
+      if (v > best) best = v, p = i;
+    }
+    piv[k] = p;
+    if (p != k) {
+#pragma unroll
+      for (int j = 0; j < 5; ++j) {
+        // pivot rows are selected with p known only at run time: swap via
+        // a predicated pass over the candidate rows to keep A in registers
+        TB tk = A[5 * k + j];
+        TB tp = tk;
+#pragma unroll
+        for (int i = k + 1; i < 5; ++i)
+          if (i == p) tp = A[5 * i + j];
+#pragma unroll
+        for (int i = k + 1; i < 5; ++i)
+          if (i == p) A[5 * i + j] = tk;
+        A[5 * k + j] = tp;
+      }
+    }
+    const TB d = A[5 * k + k];
+    if (d == TB(0)) {
+      ok = false;
+      continue;
+    }
+#pragma unroll
+    for (int i = k + 1; i < 5; ++i) {
+      A[5 * i + k] /= d;
+      const TB l = A[5 * i + k];
+#pragma unroll
+      for (int j = k + 1; j < 5; ++j) A[5 * i + j] -= l * A[5 * k + j];
+    }
+  }
+  return ok;
+}
+
+template <class TB, class TX>
+__device__ __forceinline__ void lu5_solve(const TB* A, int pv, TX* y) {
+  // pivots packed 3 bits each
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const int p = (pv >> (3 * k)) & 7;
+    if (p != k) {
+      TX tk = y[k], tp = tk;
+#pragma unroll
+      for (int i = k + 1; i < 5; ++i)
+        if (i == p) tp = y[i];
+#pragma unroll
+      for (int i = k + 1; i < 5; ++i)
+        if (i == p) y[i] = tk;
+      y[k] = tp;
+    }
+  }
+#pragma unroll
+  for (int i = 1; i < 5; ++i)
+#pragma unroll
+    for (int j = 0; j < i; ++j) y[i] -= TX(A[5 * i + j]) * y[j];
+#pragma unroll
+  for (int i = 4; i >= 0; --i) {
+#pragma unroll
+    for (int j = i + 1; j < 5; ++j) y[i] -= TX(A[5 * i + j]) * y[j];
+    y[i] /= TX(A[5 * i + i]);
+  }
+}
+
+template <class TB>
+struct PivSlot;
+template <>
+struct PivSlot<float> {
+  __device__ static float pack(int v) { return __int_as_float(v); }
+  __device__ static int unpack(float v) { return __float_as_int(v); }
+};
+template <>
+struct PivSlot<double> {
+  __device__ static double pack(int v) { return __longlong_as_double((long long)v); }
+  __device__ static int unpack(double v) { return int(__double_as_longlong(v)); }
+};
+
+// ---------------------------------------------------------------------------
+// diagonal block assembly (srcJ sum, steady fluid_D), LU, B and the block
+// Jacobi start x0 = D^-1 B; one thread per cell
+// ---------------------------------------------------------------------------
+template <class TB, class TX>
+__global__ void k_assemble(MeshView M, const double* __restrict__ q,
+                           const double* __restrict__ src, const double* __restrict__ dtau,
+                           const TB* __restrict__ fjp, const TB* __restrict__ fjm, Gas g,
+                           TB* __restrict__ cellblk, TB* __restrict__ Dout, TX* __restrict__ x,
+                           const double* __restrict__ x0, int32_t* __restrict__ err) {
+  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c >= M.nc) return;
+  TB sJ[25];
+#pragma unroll
+  for (int i = 0; i < 25; ++i) sJ[i] = TB(0);
+  for (int32_t e = M.cf_off[c]; e < M.cf_off[c + 1]; ++e) {
+    const int32_t ent = M.cf[e];
+    const int64_t f = ent >> 1;
+    if (ent & 1) {
+      const TB* p = fjm + 25 * f;
+#pragma unroll
+      for (int i = 0; i < 25; ++i) sJ[i] += p[i];
+    } else {
+      const TB* p = fjp + 25 * f;
+#pragma unroll
+      for (int i = 0; i < 25; ++i) sJ[i] -= p[i];
+    }
+  }
+  TB D[25];
+#pragma unroll
+  for (int i = 0; i < 25; ++i) D[i] = -sJ[i];
+  const Q5 qc = load_q(q, c);
+  const double coef = M.vol[c] / dtau[c];
+  const double T = qc.T, rP = 1.0 / (g.Rt * T);
+  const double rho = (qc.p + g.pamb) * rP;
+  const double rT = -rho / T;
+  const double qk = 0.5 * (qc.u * qc.u + qc.v * qc.v + qc.w * qc.w);
+  const double fT = rT * qk, fP = 1.0 / (g.gamma - 1.0) + rP * qk;
+  // M P^-1 (solverLinearSystem.loci:176-215) with reta == 1, pterm == 0
+  const double U[3] = {qc.u, qc.v, qc.w};
+  D[0] = TB(double(D[0]) + coef * rT);
+#pragma unroll
+  for (int r = 0; r < 3; ++r) D[5 * (1 + r)] = TB(double(D[5 * (1 + r)]) + coef * rT * U[r]);
+  D[20] = TB(double(D[20]) + coef * fT);
+  D[4] = TB(double(D[4]) + coef * rP);
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+    D[5 * (1 + r) + 4] = TB(double(D[5 * (1 + r) + 4]) + coef * rP * U[r]);
+  D[24] = TB(double(D[24]) + coef * fP);
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    D[6 * (1 + r)] = TB(double(D[6 * (1 + r)]) + coef * rho);
+    D[21 + r] = TB(double(D[21 + r]) + coef * rho * U[r]);
+  }
+  if (Dout) {
+    TB* o = Dout + 25 * c;
+#pragma unroll
+    for (int i = 0; i < 25; ++i) o[i] = D[i];
+  }
+  int piv[5];
+  if (!lu5<TB>(D, piv)) atomicOr(err, 1);
+  int pv = 0;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) pv |= piv[k] << (3 * k);
+  TB* o = cellblk + 32 * c;
+  TB Bv[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) Bv[k] = TB(src[5 * c + k]);
+#pragma unroll
+  for (int i = 0; i < 25; ++i) o[i] = D[i];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) o[25 + k] = Bv[k];
+  o[30] = PivSlot<TB>::pack(pv);
+  o[31] = TB(0);
+  TX y[5];
+  if (x0) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) y[k] = TX(x0[5 * c + k]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) y[k] = TX(Bv[k]);
+    lu5_solve<TB, TX>(D, pv, y);
+  }
+  TX* xo = x + 5 * c;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) xo[k] = y[k];
+}
+
+// ---------------------------------------------------------------------------
+// one colour of a Gauss-Seidel sweep (gseidel_forward/backward,
+// linearSolverSGS.loci:186-207, 277-298):
+//   x_c = D^-1 (B - sum_upper fjm x_cr + sum_lower fjp x_cl)
+// ---------------------------------------------------------------------------
+template <class TB, class TX>
+__global__ void k_sgs_colour(MeshView M, const int32_t* __restrict__ cells, int32_t ncell,
+                             const TB* __restrict__ cellblk, const TB* __restrict__ fjp,
+                             const TB* __restrict__ fjm, TX* __restrict__ x) {
+  const int32_t i = int32_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= ncell) return;
+  const int64_t c = cells[i];
+  const TB* blk = cellblk + 32 * c;
+  TX t[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) t[k] = -TX(blk[25 + k]);
+  for (int32_t e = M.cf_off[c]; e < M.cf_off[c + 1]; ++e) {
+    const int32_t ent = M.cf[e];
+    const int64_t f = ent >> 1;
+    if (f >= M.nfi) continue;
+    const TX* xn;
+    const TB* A;
+    TX xv[5];
+    if (ent & 1) {
+      xn = x + 5 * int64_t(M.cl[f]);
+      A = fjp + 25 * f;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) xv[k] = -xn[k];
+    } else {
+      xn = x + 5 * int64_t(M.cr[f]);
+      A = fjm + 25 * f;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) xv[k] = xn[k];
+    }
+#pragma unroll
+    for (int r = 0; r < 5; ++r)
+#pragma unroll
+      for (int j = 0; j < 5; ++j) t[r] += TX(__ldg(A + 5 * r + j)) * xv[j];
+  }
+  TB LU[25];
+#pragma unroll
+  for (int k = 0; k < 25; ++k) LU[k] = __ldg(blk + k);
+  const int pv = PivSlot<TB>::unpack(blk[30]);
+  TX y[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) y[k] = -t[k];
+  lu5_solve<TB, TX>(LU, pv, y);
+  TX* xo = x + 5 * c;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) xo[k] = y[k];
+}
+
+// ||B - A x||^2 and ||B||^2 per block (A from the unfactored D kept by
+// k_assemble and the face blocks)
+template <class TB, class TX>
+__global__ void __launch_bounds__(NORM_THREADS)
+k_linres(MeshView M, const TB* __restrict__ D, const TB* __restrict__ cellblk,
+         const TB* __restrict__ fjp, const TB* __restrict__ fjm, const TX* __restrict__ x,
+         double* __restrict__ part) {
+  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  double sb = 0, sr = 0;
+  if (c < M.nc) {
+    double r[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) r[k] = double(cellblk[32 * c + 25 + k]);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) sb += r[k] * r[k];
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+#pragma unroll
+      for (int j = 0; j < 5; ++j) r[i] -= double(D[25 * c + 5 * i + j]) * double(x[5 * c + j]);
+    for (int32_t e = M.cf_off[c]; e < M.cf_off[c + 1]; ++e) {
+      const int32_t ent = M.cf[e];
+      const int64_t f = ent >> 1;
+      if (f >= M.nfi) continue;
+      if (ent & 1) {
+        const TX* xn = x + 5 * int64_t(M.cl[f]);
+#pragma unroll
+        for (int i = 0; i < 5; ++i)
+#pragma unroll
+          for (int j = 0; j < 5; ++j) r[i] += double(fjp[25 * f + 5 * i + j]) * double(xn[j]);
+      } else {
+        const TX* xn = x + 5 * int64_t(M.cr[f]);
+#pragma unroll
+        for (int i = 0; i < 5; ++i)
+#pragma unroll
+          for (int j = 0; j < 5; ++j) r[i] -= double(fjm[25 * f + 5 * i + j]) * double(xn[j]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 5; ++k) sr += r[k] * r[k];
+  }
+  __shared__ double sh[2][NORM_THREADS];
+  const int t = threadIdx.x;
+  sh[0][t] = sb, sh[1][t] = sr;
+  __syncthreads();
+  for (int st = NORM_THREADS / 2; st > 0; st >>= 1) {
+    if (t < st) sh[0][t] += sh[0][t + st], sh[1][t] += sh[1][t + st];
+    __syncthreads();
+  }
+  if (t == 0) part[2 * blockIdx.x] = sh[0][0], part[2 * blockIdx.x + 1] = sh[1][0];
+}
+
+__global__ void k_sum2(const double* __restrict__ part, int nblk, double* __restrict__ out) {
+  __shared__ double sh[2][NORM_THREADS];
+  const int t = threadIdx.x;
+  double a = 0, b = 0;
+  for (int i = t; i < nblk; i += NORM_THREADS) a += part[2 * i], b += part[2 * i + 1];
+  sh[0][t] = a, sh[1][t] = b;
+  __syncthreads();
+  for (int st = NORM_THREADS / 2; st > 0; st >>= 1) {
+    if (t < st) sh[0][t] += sh[0][t + st], sh[1][t] += sh[1][t + st];
+    __syncthreads();
+  }
+  if (t == 0) out[0] = sqrt(sh[0][0]), out[1] = sqrt(sh[1][0]);
+}
+
+// ---------------------------------------------------------------------------
+// clipped Newton update (solverNewton.loci:62-78)
+// ---------------------------------------------------------------------------
+template <class TX>
+__global__ void __launch_bounds__(NORM_THREADS)
+k_update(int64_t nc, double pamb, const TX* __restrict__ x, double* __restrict__ q,
+         double* __restrict__ amin_part) {
+  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  double alpha = 1.0;
+  if (c < nc) {
+    double* qc = q + 5 * c;
+    const TX* d = x + 5 * c;
+    const double dT = double(d[0]), dp = double(d[4]);
+    alpha = dmin(alpha, 0.9 * qc[0] / (fabs(dT) + 1e-30));
+    alpha = dmin(alpha, 0.9 * (qc[4] + pamb) / (fabs(dp) + 1e-30));
+    qc[0] += alpha * dT;
+    qc[1] += alpha * double(d[1]);
+    qc[2] += alpha * double(d[2]);
+    qc[3] += alpha * double(d[3]);
+    qc[4] += alpha * dp;
+  }
+  __shared__ double sh[NORM_THREADS];
+  const int t = threadIdx.x;
+  sh[t] = alpha;
+  __syncthreads();
+  for (int st = NORM_THREADS / 2; st > 0; st >>= 1) {
+    if (t < st) sh[t] = dmin(sh[t], sh[t + st]);
+    __syncthreads();
+  }
+  if (t == 0) amin_part[blockIdx.x] = sh[0];
+}
+
+// caller-order state (T[nc], pg[nc], u[3nc]) <-> device q[nc][5] (RCM order)
+__global__ void k_state_in(int64_t nc, const int32_t* __restrict__ perm,
+                           const double* __restrict__ stage, double* __restrict__ q) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= nc) return;
+  const int64_t c = perm[i];
+  double* o = q + 5 * i;
+  o[0] = stage[c];
+  o[1] = stage[2 * nc + 3 * c];
+  o[2] = stage[2 * nc + 3 * c + 1];
+  o[3] = stage[2 * nc + 3 * c + 2];
+  o[4] = stage[nc + c];
+}
+__global__ void k_state_out(int64_t nc, const int32_t* __restrict__ perm,
+                            const double* __restrict__ q, double* __restrict__ stage) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= nc) return;
+  const int64_t c = perm[i];
+  const double* p = q + 5 * i;
+  stage[c] = p[0];
+  stage[2 * nc + 3 * c] = p[1];
+  stage[2 * nc + 3 * c + 1] = p[2];
+  stage[2 * nc + 3 * c + 2] = p[3];
+  stage[nc + c] = p[4];
+}
+
+// batched face functions (inviscidFlux.h entry points)
+__global__ void k_batch_flux(int kind, int64_t n, const double* __restrict__ qL,
+                             const double* __restrict__ qR, const double* __restrict__ an,
+                             const double* __restrict__ area, Gas g, double us_n, double eta,
+                             double* __restrict__ F) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Q5 L, R;
+  L.p = qL[5 * i], L.T = qL[5 * i + 1], L.u = qL[5 * i + 2], L.v = qL[5 * i + 3], L.w = qL[5 * i + 4];
+  R.p = qR[5 * i], R.T = qR[5 * i + 1], R.u = qR[5 * i + 2], R.v = qR[5 * i + 3], R.w = qR[5 * i + 4];
+  double f[5];
+  riemann(kind, L, R, an[3 * i], an[3 * i + 1], an[3 * i + 2], area[i], g, us_n, eta, f);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) F[5 * i + k] = f[k];
+}
+
+template <class TB>
+__global__ void k_batch_jac(int64_t n, const double* __restrict__ qL,
+                            const double* __restrict__ qR, const double* __restrict__ an,
+                            const double* __restrict__ area, Gas g, double us_n, double eta,
+                            int dir, TB* __restrict__ out) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Q5 L, R;
+  L.p = qL[5 * i], L.T = qL[5 * i + 1], L.u = qL[5 * i + 2], L.v = qL[5 * i + 3], L.w = qL[5 * i + 4];
+  R.p = qR[5 * i], R.T = qR[5 * i + 1], R.u = qR[5 * i + 2], R.v = qR[5 * i + 3], R.w = qR[5 * i + 4];
+  const double nx = an[3 * i], ny = an[3 * i + 1], nz = an[3 * i + 2];
+  const RoeAvg s = roe_average(L, R, nx, ny, nz, g, us_n, eta);
+  TB blk[25];
+  jac_roe<TB>(s, nx, ny, nz, area[i], g, dir, blk);
+#pragma unroll
+  for (int k = 0; k < 25; ++k) out[25 * i + k] = blk[k];
+}
+
+}  // namespace dev
+
+// ===========================================================================
+// host launchers
+// ===========================================================================
+namespace {
+inline unsigned blocks_for(int64_t n, int t) { return unsigned((n + t - 1) / t); }
+
+dev::MeshView view(const fpsi_ctx* x) {
+  dev::MeshView M;
+  M.nc = x->H.nc;
+  M.nf = x->H.nf;
+  M.nfi = x->H.nfi;
+  M.cl = x->d_cl;
+  M.cr = x->d_cr;
+  M.n = x->d_n;
+  M.area = x->d_area;
+  M.rL = x->d_rL;
+  M.rR = x->d_rR;
+  M.vol = x->d_vol;
+  M.Minv = x->d_Minv;
+  M.cf_off = x->d_cf_off;
+  M.cf = x->d_cf;
+  return M;
+}
+dev::Gas gas(const fpsi_ctx* x) {
+  dev::Gas g;
+  g.gamma = x->P.gamma;
+  g.Rt = x->P.Rtilde;
+  g.pamb = x->P.Pambient;
+  return g;
+}
+}  // namespace
+
+int launch_residual(fpsi_ctx* x, double* resid_slot) {
+  const dev::MeshView M = view(x);
+  const dev::Gas g = gas(x);
+  cudaStream_t s = x->stream;
+  const int T = 256;
+  if (x->H.nbf > 0) {
+    prof_begin(x, "bc_state");
+    dev::k_bc_state<<<blocks_for(x->H.nbf, T), T, 0, s>>>(M, x->d_q, x->d_bcs, g, x->d_qb);
+    prof_end(x);
+  }
+  prof_begin(x, "grad_limiter");
+  dev::k_grad_limiter<<<blocks_for(M.nc, 128), 128, 0, s>>>(M, x->d_q, x->d_qb, x->P.limiter,
+                                                             x->P.Kl, x->d_grad, x->d_phi);
+  prof_end(x);
+  prof_begin(x, "face_flux");
+  dev::k_face_flux<<<blocks_for(M.nf, 128), 128, 0, s>>>(M, x->d_q, x->d_qb, x->d_grad,
+                                                          x->d_phi, g, x->P.flux, x->d_F,
+                                                          x->d_mev);
+  prof_end(x);
+  prof_begin(x, "cell_residual");
+  dev::k_cell_residual<<<x->nblk_norm, dev::NORM_THREADS, 0, s>>>(
+      M, x->d_q, x->d_F, x->d_mev, g, x->P.urelax, x->P.dtmax, x->P.cflmax, x->H.vol_tot,
+      x->d_src, x->d_dtau, x->d_part);
+  dev::k_norm_final<<<1, dev::NORM_THREADS, 0, s>>>(x->d_part, x->nblk_norm, resid_slot);
+  prof_end(x);
+  FPSI_CUDA_TRY(cudaGetLastError());
+  return FPSI_OK;
+}
+
+template <class TB, class TX>
+static int launch_assemble_t(fpsi_ctx* x, const double* d_x0) {
+  const dev::MeshView M = view(x);
+  const dev::Gas g = gas(x);
+  cudaStream_t s = x->stream;
+  TB* fjp = (TB*)x->d_fjp;
+  TB* fjm = (TB*)x->d_fjm;
+  prof_begin(x, "face_jacobian");
+  dev::k_face_jacobian<TB><<<blocks_for(M.nf, 128), 128, 0, s>>>(M, x->d_q, x->d_qb, x->d_grad,
+                                                                  x->d_phi, g, fjp, fjm);
+  prof_end(x);
+  prof_begin(x, "assemble_lu");
+  dev::k_assemble<TB, TX><<<blocks_for(M.nc, 128), 128, 0, s>>>(
+      M, x->d_q, x->d_src, x->d_dtau, fjp, fjm, g, (TB*)x->d_cellblk,
+      x->keep_D ? (TB*)x->d_D : nullptr, (TX*)x->d_x, d_x0, x->d_err);
+  prof_end(x);
+  FPSI_CUDA_TRY(cudaGetLastError());
+  return FPSI_OK;
+}
+
+int launch_assemble(fpsi_ctx* x, const double* d_x0) {
+  switch (x->P.precision) {
+    case FPSI_PREC_FP64:
+      return launch_assemble_t<double, double>(x, d_x0);
+    case FPSI_PREC_MIXED:
+      return launch_assemble_t<float, float>(x, d_x0);
+    default:
+      return launch_assemble_t<float, double>(x, d_x0);
+  }
+}
+
+template <class TB, class TX>
+static int launch_sgs_t(fpsi_ctx* x, int sweeps) {
+  const dev::MeshView M = view(x);
+  cudaStream_t s = x->stream;
+  const int T = 128;
+  const auto& off = x->H.colour_off;
+  const int K = x->H.ncolours;
+  for (int it = 0; it < sweeps; ++it) {
+    for (int pass = 0; pass < 2; ++pass)
+      for (int kk = 0; kk < K; ++kk) {
+        const int k = pass == 0 ? kk : K - 1 - kk;
+        const int32_t n = off[k + 1] - off[k];
+        if (n == 0) continue;
+        prof_begin(x, "sgs_colour");
+        dev::k_sgs_colour<TB, TX><<<blocks_for(n, T), T, 0, s>>>(
+            M, x->d_colour_cells + off[k], n, (const TB*)x->d_cellblk, (const TB*)x->d_fjp,
+            (const TB*)x->d_fjm, (TX*)x->d_x);
+        prof_end(x);
+      }
+  }
+  FPSI_CUDA_TRY(cudaGetLastError());
+  return FPSI_OK;
+}
+
+int launch_sgs(fpsi_ctx* x, int sweeps) {
+  switch (x->P.precision) {
+    case FPSI_PREC_FP64:
+      return launch_sgs_t<double, double>(x, sweeps);
+    case FPSI_PREC_MIXED:
+      return launch_sgs_t<float, float>(x, sweeps);
+    default:
+      return launch_sgs_t<float, double>(x, sweeps);
+  }
+}
+
+template <class TB, class TX>
+static int launch_linres_t(fpsi_ctx* x, double* out2) {
+  const dev::MeshView M = view(x);
+  dev::k_linres<TB, TX><<<x->nblk_norm, dev::NORM_THREADS, 0, x->stream>>>(
+      M, (const TB*)x->d_D, (const TB*)x->d_cellblk, (const TB*)x->d_fjp, (const TB*)x->d_fjm,
+      (const TX*)x->d_x, x->d_part);
+  dev::k_sum2<<<1, dev::NORM_THREADS, 0, x->stream>>>(x->d_part, x->nblk_norm, out2);
+  FPSI_CUDA_TRY(cudaGetLastError());
+  return FPSI_OK;
+}
+
+int launch_linres(fpsi_ctx* x, double* out2) {
+  switch (x->P.precision) {
+    case FPSI_PREC_FP64:
+      return launch_linres_t<double, double>(x, out2);
+    case FPSI_PREC_MIXED:
+      return launch_linres_t<float, float>(x, out2);
+    default:
+      return launch_linres_t<float, double>(x, out2);
+  }
+}
+
+int launch_update(fpsi_ctx* x) {
+  const int64_t nc = x->H.nc;
+  prof_begin(x, "update");
+  if (x->P.precision == FPSI_PREC_MIXED)
+    dev::k_update<float><<<x->nblk_norm, dev::NORM_THREADS, 0, x->stream>>>(
+        nc, x->P.Pambient, (const float*)x->d_x, x->d_q, x->d_amin);
+  else
+    dev::k_update<double><<<x->nblk_norm, dev::NORM_THREADS, 0, x->stream>>>(
+        nc, x->P.Pambient, (const double*)x->d_x, x->d_q, x->d_amin);
+  prof_end(x);
+  FPSI_CUDA_TRY(cudaGetLastError());
+  return FPSI_OK;
+}
+
+int launch_state(fpsi_ctx* x, bool in) {
+  const int64_t nc = x->H.nc;
+  if (in)
+    dev::k_state_in<<<blocks_for(nc, 256), 256, 0, x->stream>>>(nc, x->d_perm, x->d_stage, x->d_q);
+  else
+    dev::k_state_out<<<blocks_for(nc, 256), 256, 0, x->stream>>>(nc, x->d_perm, x->d_q, x->d_stage);
+  FPSI_CUDA_TRY(cudaGetLastError());
+  return FPSI_OK;
+}
+
+int launch_batch_flux(int kind, int64_t n, const double* qL, const double* qR, const double* an,
+                      const double* area, double pamb, double Rt, double gamma, double us_n,
+                      double eta, double* F, cudaStream_t s) {
+  dev::Gas g{gamma, Rt, pamb};
+  dev::k_batch_flux<<<blocks_for(n, 128), 128, 0, s>>>(kind, n, qL, qR, an, area, g, us_n, eta, F);
+  FPSI_CUDA_TRY(cudaGetLastError());
+  return FPSI_OK;
+}
+
+int launch_batch_jac(int64_t n, const double* qL, const double* qR, const double* an,
+                     const double* area, double pamb, double Rt, double gamma, double us_n,
+                     double eta, int dir, int as_double, void* out, cudaStream_t s) {
+  dev::Gas g{gamma, Rt, pamb};
+  if (as_double)
+    dev::k_batch_jac<double><<<blocks_for(n, 128), 128, 0, s>>>(n, qL, qR, an, area, g, us_n,
+                                                                  eta, dir, (double*)out);
+  else
+    dev::k_batch_jac<float><<<blocks_for(n, 128), 128, 0, s>>>(n, qL, qR, an, area, g, us_n, eta,
+                                                                 dir, (float*)out);
+  FPSI_CUDA_TRY(cudaGetLastError());
+  return FPSI_OK;
+}
+
+}  // namespace fpsi

@@ -1,0 +1,35 @@
+// kernels.cuh -- host launchers of the device path (internal).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+struct fpsi_ctx;
+
+namespace fpsi {
+
+// residual chain: boundary states, gradient+limiter, face flux, per-cell
+// gather (src, dtau), norms into resid_slot[8] (device)
+int launch_residual(fpsi_ctx* x, double* resid_slot);
+// face Jacobians, diagonal blocks, LU, B and the starting iterate
+// (d_x0 == nullptr: block Jacobi start D^-1 B)
+int launch_assemble(fpsi_ctx* x, const double* d_x0);
+// `sweeps` symmetric multi-colour Gauss-Seidel sweeps on the device iterate
+int launch_sgs(fpsi_ctx* x, int sweeps);
+// out2[0] = ||B||, out2[1] = ||B - A x|| (device)
+int launch_linres(fpsi_ctx* x, double* out2);
+// clipped Newton update; per-block minimum alpha into d_amin
+int launch_update(fpsi_ctx* x);
+// caller-order staging buffer <-> device state (in = staging -> q)
+int launch_state(fpsi_ctx* x, bool in);
+
+int launch_batch_flux(int kind, int64_t n, const double* qL, const double* qR, const double* an,
+                      const double* area, double pamb, double Rt, double gamma, double us_n,
+                      double eta, double* F, cudaStream_t s);
+int launch_batch_jac(int64_t n, const double* qL, const double* qR, const double* an,
+                     const double* area, double pamb, double Rt, double gamma, double us_n,
+                     double eta, int dir, int as_double, void* out, cudaStream_t s);
+
+const char* last_error();
+
+}  // namespace fpsi

@@ -1,0 +1,379 @@
+// physics.cuh -- device face physics of the implicit path (FP64 arithmetic).
+//
+// Primitive states are q = [T, u, v, w, pg] (pg = gauge pressure).  The
+// preconditioned Roe scheme of flowPsi is written here around one object,
+// the 5x5 matrix K(l1,l2,l3) of RoeJacobian (fluxInviscid.loci:1019-1090):
+//   * roeCT_flux  (:869-1014)  = central flux - area/2 * K(|l|) dq
+//   * roeCT_jacobian (:1092-1168) = area * K(l+-) with smoothed eigenvalues
+// so the flux dissipation and the flux Jacobians share one coefficient set.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace fpsi {
+namespace dev {
+
+struct Gas {
+  double gamma, Rt, pamb;
+};
+
+struct Q5 {
+  double T, u, v, w, p;
+};
+
+__device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
+
+// Roe-averaged state of roeCT_flux / roeCT_jacobian (:875-915, :1098-1139)
+struct RoeAvg {
+  double rl, rr, rel, rer;   // densities and total energies per volume
+  double r, U, V, W, h0;     // Roe density, velocity, total enthalpy
+  double un, unA;            // U.n - us_n, U.n
+  double a, sigma, eta;
+};
+
+__device__ __forceinline__ RoeAvg roe_average(const Q5& L, const Q5& R, double nx, double ny,
+                                              double nz, const Gas& g, double us_n,
+                                              double eta) {
+  RoeAvg s;
+  const double gm1 = g.gamma - 1.0;
+  const double pl = L.p + g.pamb, pr = R.p + g.pamb;
+  s.rl = pl / (g.Rt * L.T);
+  s.rr = pr / (g.Rt * R.T);
+  s.rel = s.rl * (g.Rt * L.T / gm1 + 0.5 * (L.u * L.u + L.v * L.v + L.w * L.w));
+  s.rer = s.rr * (g.Rt * R.T / gm1 + 0.5 * (R.u * R.u + R.v * R.v + R.w * R.w));
+  const double h0l = (s.rel + pl) / s.rl;
+  const double h0r = (s.rer + pr) / s.rr;
+  s.r = sqrt(s.rl * s.rr);
+  const double wl = sqrt(s.rl), wr = sqrt(s.rr);
+  const double iw = 1.0 / (wl + wr);
+  s.U = (L.u * wl + R.u * wr) * iw;
+  s.V = (L.v * wl + R.v * wr) * iw;
+  s.W = (L.w * wl + R.w * wr) * iw;
+  s.unA = s.U * nx + s.V * ny + s.W * nz;
+  s.un = s.unA - us_n;
+  s.h0 = (h0l * wl + h0r * wr) * iw;
+  const double h = s.h0 - 0.5 * (s.U * s.U + s.V * s.V + s.W * s.W);
+  // strong pressure jumps switch preconditioning off (:914-915)
+  if (fabs(pl - pr) / (pl + pr + 1e-33) > 0.1) eta = 1.0;
+  s.eta = eta;
+  s.a = sqrt(dmax(gm1 * h, 1e-30));
+  const double em = eta - 1.0;
+  s.sigma = sqrt(s.un * s.un * em * em + 4.0 * eta * s.a * s.a);
+  return s;
+}
+
+// Coefficients of K for eigenvalues (l1, l2, l3): the entries are
+//   K[0][T]=l1*rT  K[0][m]=n_m*c7          K[0][p]=c8
+//   K[r][T]=l1*rT*U_r   K[r][m]=n_m*(c7*U_r+n_r*c4)+l1*rho*delta_rm
+//   K[r][p]=c8*U_r-n_r*c1
+//   K[e][T]=l1*c9  K[e][m]=n_m*c10+l1*rho*U_m   K[e][p]=c11
+struct RoeK {
+  double l1, rT, c7, c8, c9, c10, c11, c4, c1, rho, t4, d23;
+};
+
+__device__ __forceinline__ RoeK roe_k(double l1, double l2, double l3, const RoeAvg& s,
+                                      const Gas& g) {
+  const double beta = s.eta, sg = s.sigma, un = s.un;
+  const double bm = beta - 1.0;
+  const double d23 = l2 - l3;
+  const double s23 = l2 + l3 - 2.0 * l1;
+  const double t3 = s.r * (bm * bm * un * un - sg * sg) / (4.0 * sg);
+  const double t4 = s23 * sg + bm * d23 * un;
+  const double t5 = (s23 * sg - bm * d23 * un) / (2.0 * sg);
+  const double t6 = ((l2 + l3) * sg - bm * d23 * un) / (2.0 * sg);
+  const double gm1 = g.gamma - 1.0;
+  const double cp = g.gamma * g.Rt / gm1;
+  const double rT = -g.gamma * g.Rt * s.r /
+                    ((s.h0 - 0.5 * (s.U * s.U + s.V * s.V + s.W * s.W)) * gm1);
+  const double ib = 1.0 / beta;
+  const double ia2 = 1.0 / (s.a * s.a);
+  RoeK k;
+  k.l1 = l1;
+  k.rT = rT;
+  k.rho = s.r;
+  k.c7 = ib * d23 * t3 * ia2;
+  k.c8 = (((ib - 1.0) + g.gamma) * t6 - gm1 * t5) * ia2;
+  k.c9 = cp * s.r + s.h0 * rT;
+  const double x1 = g.gamma * s.h0 * d23 * t3 * ia2 * ib;
+  const double x2 = -ib * gm1 * d23 * t3 * k.c9 * ia2 / rT;
+  const double x3 = -d23 * t3 * ib;
+  const double x4 = 0.5 * s.r * t4 * s.unA / sg;
+  k.c10 = (x1 + x2 + x3 + x4);
+  k.c11 = (ib * ia2 * s.h0 + (k.c9 - s.r * ib * cp) * ia2 * gm1 / rT - ib) * t6 -
+          gm1 * ia2 * k.c9 * t5 / rT - s.unA * d23 / sg;
+  k.c4 = s.r * t4 / (2.0 * sg);
+  k.c1 = d23 / sg;
+  k.t4 = t4;
+  k.d23 = d23;
+  return k;
+}
+
+// y = K dq
+__device__ __forceinline__ void roe_k_apply(const RoeK& k, const RoeAvg& s, double nx,
+                                            double ny, double nz, const double dq[5],
+                                            double y[5]) {
+  const double dun = nx * dq[1] + ny * dq[2] + nz * dq[3];
+  const double Ud = s.U * dq[1] + s.V * dq[2] + s.W * dq[3];
+  const double a1 = k.l1 * k.rT * dq[0];
+  y[0] = a1 + k.c7 * dun + k.c8 * dq[4];
+  y[1] = a1 * s.U + (k.c7 * s.U + nx * k.c4) * dun + k.l1 * k.rho * dq[1] +
+         (k.c8 * s.U - nx * k.c1) * dq[4];
+  y[2] = a1 * s.V + (k.c7 * s.V + ny * k.c4) * dun + k.l1 * k.rho * dq[2] +
+         (k.c8 * s.V - ny * k.c1) * dq[4];
+  y[3] = a1 * s.W + (k.c7 * s.W + nz * k.c4) * dun + k.l1 * k.rho * dq[3] +
+         (k.c8 * s.W - nz * k.c1) * dq[4];
+  y[4] = k.l1 * k.c9 * dq[0] + k.c10 * dun + k.l1 * k.rho * Ud + k.c11 * dq[4];
+}
+
+// M = area * K, row-major
+template <class TB>
+__device__ __forceinline__ void roe_k_matrix(const RoeK& k, const RoeAvg& s, double nx,
+                                             double ny, double nz, double area, TB* M) {
+  const double n[3] = {nx, ny, nz};
+  const double U[3] = {s.U, s.V, s.W};
+  M[0] = TB(area * (k.l1 * k.rT));
+#pragma unroll
+  for (int m = 0; m < 3; ++m) M[1 + m] = TB(area * (n[m] * k.c7));
+  M[4] = TB(area * k.c8);
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    M[5 * (1 + r)] = TB(area * (k.l1 * k.rT * U[r]));
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      double v = n[m] * (k.c7 * U[r] + n[r] * k.c4);
+      if (r == m) v += k.l1 * k.rho;
+      M[5 * (1 + r) + 1 + m] = TB(area * v);
+    }
+    M[5 * (1 + r) + 4] = TB(area * (k.c8 * U[r] - n[r] * k.c1));
+  }
+  M[20] = TB(area * (k.l1 * k.c9));
+#pragma unroll
+  for (int m = 0; m < 3; ++m) M[21 + m] = TB(area * (n[m] * k.c10 + k.l1 * k.rho * U[m]));
+  M[24] = TB(area * k.c11);
+}
+
+// roeCT_flux: central part plus K(|l|) dissipation with the Harten-Hyman
+// entropy fix on the acoustic waves (:918-962).
+__device__ __forceinline__ void flux_roe(const Q5& L, const Q5& R, double nx, double ny,
+                                         double nz, double area, const Gas& g, double us_n,
+                                         double eta, double F[5]) {
+  const RoeAvg s = roe_average(L, R, nx, ny, nz, g, us_n, eta);
+  const double ep = s.eta + 1.0, em = s.eta - 1.0;
+  const double l2s = 0.5 * (s.un * ep - s.sigma);
+  const double l3s = 0.5 * (s.un * ep + s.sigma);
+  double l1 = fabs(s.un), l2 = fabs(l2s), l3 = fabs(l3s);
+  const double unlA = L.u * nx + L.v * ny + L.w * nz, unrA = R.u * nx + R.v * ny + R.w * nz;
+  const double unl = unlA - us_n, unr = unrA - us_n;
+  const double sl = sqrt(unl * unl * em * em + 4.0 * s.eta * g.gamma * g.Rt * L.T);
+  const double sr = sqrt(unr * unr * em * em + 4.0 * s.eta * g.gamma * g.Rt * R.T);
+  const double w2 = dmax(0.0, dmax(l2s - 0.5 * (unl * ep - sl), 0.5 * (unr * ep - sr) - l2s));
+  const double w3 = dmax(0.0, dmax(l3s - 0.5 * (unl * ep + sl), 0.5 * (unr * ep + sr) - l3s));
+  if (l2 < w2) l2 = 0.5 * ((l2s * l2s) / w2 + w2);
+  if (l3 < w3) l3 = 0.5 * ((l3s * l3s) / w3 + w3);
+  const RoeK k = roe_k(l1, l2, l3, s, g);
+  // K(|l|) dq with the association of fluxInviscid.loci:985-1004 so the
+  // FP64 flux agrees with the reference to rounding
+  const double dT = R.T - L.T, dp = R.p - L.p;
+  const double du = R.u - L.u, dv = R.v - L.v, dw = R.w - L.w;
+  const double uj = du * nx + dv * ny + dw * nz;
+  const double i2s = 2.0 * s.sigma;
+  double d[5];
+  d[0] = dp * k.c8 + uj * k.c7 + l1 * dT * k.rT;
+  d[1] = s.U * k.c7 * uj + l1 * (s.U * dT * k.rT + s.r * du) + dp * (k.c8 * s.U - nx * k.d23 / s.sigma) +
+         nx * s.r * k.t4 * uj / i2s;
+  d[2] = s.V * k.c7 * uj + l1 * (s.V * dT * k.rT + s.r * dv) + dp * (k.c8 * s.V - ny * k.d23 / s.sigma) +
+         ny * s.r * k.t4 * uj / i2s;
+  d[3] = s.W * k.c7 * uj + l1 * (s.W * dT * k.rT + s.r * dw) + dp * (k.c8 * s.W - nz * k.d23 / s.sigma) +
+         nz * s.r * k.t4 * uj / i2s;
+  d[4] = dp * k.c11 + k.c10 * uj + l1 * (k.c9 * dT + s.r * (s.U * du + s.V * dv + s.W * dw));
+  const double ah = 0.5 * area;
+  const double ml = s.rl * unl, mr = s.rr * unr;
+  const double pl = L.p + g.pamb, pr = R.p + g.pamb;
+  F[0] = ah * (ml + mr - d[0]);
+  F[1] = ah * (L.u * ml + R.u * mr + nx * (L.p + R.p) - d[1]);
+  F[2] = ah * (L.v * ml + R.v * mr + ny * (L.p + R.p) - d[2]);
+  F[3] = ah * (L.w * ml + R.w * mr + nz * (L.p + R.p) - d[3]);
+  F[4] = ah * ((s.rel * unl + pl * unlA) + (s.rer * unr + pr * unrA) - d[4]);
+}
+
+// Smoothed one-sided eigenvalue Jacobian, roeCT_jacobian (:1141-1167):
+// l -> (l +- sqrt(l^2 + (0.02 (lmax - lmin))^2)) / 2.
+template <class TB>
+__device__ __forceinline__ void jac_roe(const RoeAvg& s, double nx, double ny, double nz,
+                                        double area, const Gas& g, int dir, TB* M) {
+  const double ep = s.eta + 1.0;
+  double l1 = s.un;
+  double l2 = 0.5 * (s.un * ep - s.sigma);
+  double l3 = 0.5 * (s.un * ep + s.sigma);
+  const double hi = dmax(l1, dmax(l2, l3)), lo = dmin(l1, dmin(l2, l3));
+  const double e = 0.02 * (hi - lo);
+  const double e2 = e * e;
+  const double d = dir < 0 ? -1.0 : 1.0;
+  l1 = 0.5 * (l1 + d * sqrt(l1 * l1 + e2));
+  l2 = 0.5 * (l2 + d * sqrt(l2 * l2 + e2));
+  l3 = 0.5 * (l3 + d * sqrt(l3 * l3 + e2));
+  const RoeK k = roe_k(l1, l2, l3, s, g);
+  roe_k_matrix<TB>(k, s, nx, ny, nz, area, M);
+}
+
+// hllc_flux (fluxInviscid.loci:157-256) and the HLL two-wave flux built on
+// the same SL/SR estimates.
+struct Waves {
+  double rl, rr, el, er, unlA, unrA, unl, unr, SL, SR;
+};
+__device__ __forceinline__ Waves hll_waves(const Q5& L, const Q5& R, double nx, double ny,
+                                           double nz, const Gas& g, double us_n, double eta) {
+  Waves w;
+  const double gm1 = g.gamma - 1.0;
+  w.rl = (L.p + g.pamb) / (g.Rt * L.T);
+  w.rr = (R.p + g.pamb) / (g.Rt * R.T);
+  const double h0l = g.Rt * L.T * g.gamma / gm1 + 0.5 * (L.u * L.u + L.v * L.v + L.w * L.w);
+  const double h0r = g.Rt * R.T * g.gamma / gm1 + 0.5 * (R.u * R.u + R.v * R.v + R.w * R.w);
+  w.el = h0l - g.Rt * L.T;
+  w.er = h0r - g.Rt * R.T;
+  const double wl = sqrt(w.rl), wr = sqrt(w.rr), iw = 1.0 / (wl + wr);
+  const double U = (L.u * wl + R.u * wr) * iw, V = (L.v * wl + R.v * wr) * iw,
+               W = (L.w * wl + R.w * wr) * iw;
+  const double un = U * nx + V * ny + W * nz - us_n;
+  const double h0 = (h0l * wl + h0r * wr) * iw;
+  const double a = sqrt(dmax(gm1 * (h0 - 0.5 * (U * U + V * V + W * W)), 0.0));
+  const double ep = eta + 1.0, em = eta - 1.0;
+  const double sg = sqrt(dmax(un * un * em * em + 4.0 * eta * a * a, 1e-30));
+  w.unlA = L.u * nx + L.v * ny + L.w * nz;
+  w.unrA = R.u * nx + R.v * ny + R.w * nz;
+  w.unl = w.unlA - us_n;
+  w.unr = w.unrA - us_n;
+  const double sr = sqrt(dmax(w.unr * w.unr * em * em + 4.0 * eta * g.gamma * g.Rt * R.T, 0.0));
+  const double sl = sqrt(dmax(w.unl * w.unl * em * em + 4.0 * eta * g.gamma * g.Rt * L.T, 0.0));
+  w.SL = dmin(0.5 * (un * ep - sg), 0.5 * (w.unl * ep - sl));
+  w.SR = dmax(0.5 * (un * ep + sg), 0.5 * (w.unr * ep + sr));
+  return w;
+}
+
+__device__ __forceinline__ void flux_hllc(const Q5& L, const Q5& R, double nx, double ny,
+                                          double nz, double area, const Gas& g, double us_n,
+                                          double eta, double F[5]) {
+  const Waves w = hll_waves(L, R, nx, ny, nz, g, us_n, eta);
+  const double SL = w.SL, SR = w.SR, rl = w.rl, rr = w.rr;
+  const double ml = rl * w.unl, mr = rr * w.unr;
+  const double pl = L.p + g.pamb, pr = R.p + g.pamb;
+  const double c = 0.5 * area;
+  const double AL = c * ((SL > 0) ? (SR < 0 ? 1. : 2.) : (SR < 0 ? 0. : 1.));
+  const double AR = c * ((SR < 0) ? (SL > 0 ? 1. : 2.) : (SL > 0 ? 0. : 1.));
+  const double AM = c * ((SL > 0 || SR < 0) ? 0. : 1.);
+  F[0] = AL * ml + AR * mr;
+  F[1] = AL * ml * L.u + AR * mr * R.u + nx * (AL * L.p + AR * R.p);
+  F[2] = AL * ml * L.v + AR * mr * R.v + ny * (AL * L.p + AR * R.p);
+  F[3] = AL * ml * L.w + AR * mr * R.w + nz * (AL * L.p + AR * R.p);
+  F[4] = AL * (ml * w.el + pl * w.unlA) + AR * (mr * w.er + pr * w.unrA);
+  F[0] -= AM * (SL * rl + SR * rr);
+  F[1] -= AM * (SL * rl * L.u + SR * rr * R.u);
+  F[2] -= AM * (SL * rl * L.v + SR * rr * R.v);
+  F[3] -= AM * (SL * rl * L.w + SR * rr * R.w);
+  F[4] -= AM * (SL * rl * w.el + SR * rr * w.er);
+  const double unl = w.unl, unr = w.unr;
+  const double SM = ((rr * unr * (SR - unr) - rl * unl * (SL - unl) + L.p - R.p) /
+                     (rr * (SR - unr) - rl * (SL - unl)));
+  const double il = 1.0 / (SL - SM), ir = 1.0 / (SR - SM);
+  const double pgs = rl * (unl - SL) * (unl - SM) + L.p;
+  const double ps = pgs + g.pamb;
+  const double CR = SR - fabs(SM), CL = SL + fabs(SM);
+  const double fl = (SL - unl) * rl, fr = (SR - unr) * rr;
+  // star states U*_L, U*_R (conserved), weighted by CL, CR
+  F[0] += AM * (CR * (fr / (SR - SM)) + CL * (fl / (SL - SM)));
+  F[1] += AM * (CR * ((fr * R.u + (pgs - R.p) * nx) / (SR - SM)) +
+                CL * ((fl * L.u + (pgs - L.p) * nx) / (SL - SM)));
+  F[2] += AM * (CR * ((fr * R.v + (pgs - R.p) * ny) / (SR - SM)) +
+                CL * ((fl * L.v + (pgs - L.p) * ny) / (SL - SM)));
+  F[3] += AM * (CR * ((fr * R.w + (pgs - R.p) * nz) / (SR - SM)) +
+                CL * ((fl * L.w + (pgs - L.p) * nz) / (SL - SM)));
+  F[4] += AM * (CR * ((fr * w.er - pr * unr + ps * SM) / (SR - SM)) +
+                CL * ((fl * w.el - pl * unl + ps * SM) / (SL - SM)));
+  (void)il;
+  (void)ir;
+}
+
+__device__ __forceinline__ void analytic_flux(const Q5& q, double rho, double e0, double unA,
+                                              double un, double nx, double ny, double nz,
+                                              double area, const Gas& g, double f[5]) {
+  const double m = area * rho * un;
+  f[0] = m;
+  f[1] = m * q.u + area * q.p * nx;
+  f[2] = m * q.v + area * q.p * ny;
+  f[3] = m * q.w + area * q.p * nz;
+  f[4] = m * e0 + area * (q.p + g.pamb) * unA;
+}
+
+__device__ __forceinline__ void flux_hlle(const Q5& L, const Q5& R, double nx, double ny,
+                                          double nz, double area, const Gas& g, double us_n,
+                                          double eta, double F[5]) {
+  const Waves w = hll_waves(L, R, nx, ny, nz, g, us_n, eta);
+  double fl[5], fr[5];
+  analytic_flux(L, w.rl, w.el, w.unlA, w.unl, nx, ny, nz, area, g, fl);
+  analytic_flux(R, w.rr, w.er, w.unrA, w.unr, nx, ny, nz, area, g, fr);
+  if (w.SL >= 0) {
+#pragma unroll
+    for (int i = 0; i < 5; ++i) F[i] = fl[i];
+    return;
+  }
+  if (w.SR <= 0) {
+#pragma unroll
+    for (int i = 0; i < 5; ++i) F[i] = fr[i];
+    return;
+  }
+  const double ql[5] = {w.rl, w.rl * L.u, w.rl * L.v, w.rl * L.w, w.rl * w.el};
+  const double qr[5] = {w.rr, w.rr * R.u, w.rr * R.v, w.rr * R.w, w.rr * w.er};
+  const double id = 1.0 / (w.SR - w.SL);
+  const double ss = area * w.SL * w.SR;
+#pragma unroll
+  for (int i = 0; i < 5; ++i) F[i] = (w.SR * fl[i] - w.SL * fr[i] + ss * (qr[i] - ql[i])) * id;
+}
+
+__device__ __forceinline__ void riemann(int kind, const Q5& L, const Q5& R, double nx,
+                                        double ny, double nz, double area, const Gas& g,
+                                        double us_n, double eta, double F[5]) {
+  if (kind == 1)
+    flux_roe(L, R, nx, ny, nz, area, g, us_n, eta, F);
+  else if (kind == 2)
+    flux_hlle(L, R, nx, ny, nz, area, g, us_n, eta, F);
+  else
+    flux_hllc(L, R, nx, ny, nz, area, g, us_n, eta, F);
+}
+
+// Characteristic boundary states, cv_inflow / cv_outflow (bcTools.h:25-81).
+__device__ __forceinline__ void cv_state(bool outflow, const Q5& qi, const Q5& q0, double nx,
+                                         double ny, double nz, double us_n, const Gas& g,
+                                         double beta, Q5& qb) {
+  const double uit = qi.u * nx + qi.v * ny + qi.w * nz - us_n;
+  const double u0t = q0.u * nx + q0.v * ny + q0.w * nz - us_n;
+  const double a02 = g.gamma * g.Rt * q0.T;
+  const double r0 = (q0.p + g.pamb) / (g.Rt * q0.T);
+  const double bm = 0.5 * (1.0 - beta);
+  const double ub = uit * (1.0 - beta);
+  const double sg = sqrt(ub * ub + 4.0 * beta * a02);
+  const double rel = ((qi.p - q0.p) + r0 * (uit - u0t) * uit * bm) * uit * bm / (2.0 * sg);
+  double pb;
+  if (outflow) {
+    pb = 0.5 * (qi.p + q0.p - 0.5 * r0 * sg * (u0t - uit)) + rel;
+    pb = dmax(pb, 0.1 * (qi.p + g.pamb) - g.pamb);
+    const double s = 2.0 * (qi.p - pb) / (r0 * (sg + uit * bm));
+    qb.u = qi.u + s * nx;
+    qb.v = qi.v + s * ny;
+    qb.w = qi.w + s * nz;
+    const double rb = r0 + (pb - qi.p) * (sg - uit * bm) / (beta * a02 * (sg + uit * bm));
+    qb.T = (pb + g.pamb) / (g.Rt * rb);
+  } else {
+    pb = 0.5 * (q0.p + qi.p - 0.5 * r0 * sg * (u0t - uit)) - rel;
+    pb = dmax(pb, 0.1 * (q0.p + g.pamb) - g.pamb);
+    const double s = 2.0 * (pb - q0.p) / (r0 * (sg + uit * bm));
+    qb.u = q0.u + s * nx;
+    qb.v = q0.v + s * ny;
+    qb.w = q0.w + s * nz;
+    const double rb = r0 + (pb - q0.p) * (sg - uit * bm) / (beta * a02 * (sg + uit * bm));
+    qb.T = (pb + g.pamb) / (g.Rt * rb);
+  }
+  qb.p = pb;
+}
+
+}  // namespace dev
+}  // namespace fpsi

@@ -1,0 +1,379 @@
+// setup.cpp -- host-side preparation of a mesh for the device path.
+//
+//  * geometry in FP64 (Loci FVM's area, facecenter, vol, cellcenter):
+//    fan triangulation of each face about its node average; cell volume and
+//    centroid from the pyramids on those triangles (divergence theorem);
+//  * reverse Cuthill-McKee renumbering of the cells;
+//  * faces sorted by (cl, cr) in the new numbering, interior faces first;
+//  * cell -> face lists (upper, lower, boundary) and least-squares normal
+//    matrices of the cell gradient;
+//  * greedy distance-1 colouring of the cell graph for the multi-colour
+//    Gauss-Seidel sweeps.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+
+#include "fpsi_internal.h"
+
+namespace fpsi {
+
+namespace {
+thread_local char g_err[512] = "";
+}
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+const char* last_error() { return g_err; }
+
+namespace {
+
+struct P3 {
+  double v[3];
+};
+inline P3 p3(const double* a) { return P3{{a[0], a[1], a[2]}}; }
+
+// Cuthill-McKee from a pseudo-peripheral start in every connected component,
+// neighbours visited by increasing degree; reversed at the end.
+std::vector<int32_t> rcm_order(int64_t n, const std::vector<int64_t>& off,
+                               const std::vector<int32_t>& adj) {
+  std::vector<int32_t> order;
+  order.reserve(size_t(n));
+  std::vector<char> seen(size_t(n), 0);
+  std::vector<int32_t> level(size_t(n), -1);
+  auto deg = [&](int32_t c) { return int32_t(off[c + 1] - off[c]); };
+  auto bfs_far = [&](int32_t s, std::vector<int32_t>& comp) {
+    // returns a node of the last BFS level with minimum degree
+    comp.clear();
+    comp.push_back(s);
+    level[s] = 0;
+    size_t h = 0;
+    while (h < comp.size()) {
+      int32_t c = comp[h++];
+      for (int64_t k = off[c]; k < off[c + 1]; ++k) {
+        int32_t m = adj[k];
+        if (level[m] < 0) {
+          level[m] = level[c] + 1;
+          comp.push_back(m);
+        }
+      }
+    }
+    int32_t last = level[comp.back()];
+    int32_t best = comp.back();
+    for (size_t i = comp.size(); i-- > 0;) {
+      if (level[comp[i]] != last) break;
+      if (deg(comp[i]) < deg(best)) best = comp[i];
+    }
+    for (int32_t c : comp) level[c] = -1;
+    return std::make_pair(best, last);
+  };
+  std::vector<int32_t> comp, nb;
+  for (int64_t s0 = 0; s0 < n; ++s0) {
+    if (seen[s0]) continue;
+    int32_t start = int32_t(s0);
+    auto r = bfs_far(start, comp);
+    for (int it = 0; it < 2; ++it) {
+      auto r2 = bfs_far(r.first, comp);
+      if (r2.second <= r.second && it > 0) break;
+      start = r.first;
+      r = r2;
+    }
+    size_t h = order.size();
+    order.push_back(start);
+    seen[start] = 1;
+    while (h < order.size()) {
+      int32_t c = order[h++];
+      nb.clear();
+      for (int64_t k = off[c]; k < off[c + 1]; ++k)
+        if (!seen[adj[k]]) {
+          seen[adj[k]] = 1;
+          nb.push_back(adj[k]);
+        }
+      std::stable_sort(nb.begin(), nb.end(),
+                       [&](int32_t a, int32_t b) { return deg(a) < deg(b); });
+      order.insert(order.end(), nb.begin(), nb.end());
+    }
+  }
+  std::reverse(order.begin(), order.end());
+  return order;
+}
+
+}  // namespace
+
+int build_host_mesh(const fpsi_mesh* m, HostMesh& h) {
+  const int64_t nc = m->ncells, nf = m->nfaces;
+  if (nc <= 0 || nf <= 0 || !m->xyz || !m->face_off || !m->face_nodes || !m->cl || !m->cr) {
+    set_error("mesh: empty or missing arrays");
+    return FPSI_E_INVALID;
+  }
+  if (nc >= (int64_t(1) << 31) || 2 * nf >= (int64_t(1) << 30)) {
+    set_error("mesh: too large for 32-bit indices");
+    return FPSI_E_INVALID;
+  }
+  for (int64_t f = 0; f < nf; ++f) {
+    int32_t a = m->cl[f], b = m->cr[f];
+    if (a < 0 || a >= nc || b >= nc || (b < 0 && -b - 1 >= m->nbc) || a == b) {
+      set_error("mesh: face %lld has invalid cl/cr (%d, %d)", (long long)f, a, b);
+      return FPSI_E_INVALID;
+    }
+    int64_t k = m->face_off[f + 1] - m->face_off[f];
+    if (k < 3) {
+      set_error("mesh: face %lld has %lld nodes", (long long)f, (long long)k);
+      return FPSI_E_INVALID;
+    }
+  }
+  h.nc = nc;
+  h.nf = nf;
+  // ---- geometry in caller order ----
+  std::vector<double> A(nf * 3), fc(nf * 3), ar(nf);
+  for (int64_t f = 0; f < nf; ++f) {
+    const int64_t b = m->face_off[f], e = m->face_off[f + 1];
+    const int k = int(e - b);
+    double xa[3] = {0, 0, 0};
+    for (int64_t i = b; i < e; ++i)
+      for (int d = 0; d < 3; ++d) xa[d] += m->xyz[3 * int64_t(m->face_nodes[i]) + d];
+    for (int d = 0; d < 3; ++d) xa[d] /= k;
+    double Av[3] = {0, 0, 0}, C[3] = {0, 0, 0}, W = 0;
+    for (int i = 0; i < k; ++i) {
+      const double* p0 = m->xyz + 3 * int64_t(m->face_nodes[b + i]);
+      const double* p1 = m->xyz + 3 * int64_t(m->face_nodes[b + (i + 1) % k]);
+      double u[3], v[3];
+      for (int d = 0; d < 3; ++d) u[d] = p0[d] - xa[d], v[d] = p1[d] - xa[d];
+      double t[3] = {0.5 * (u[1] * v[2] - u[2] * v[1]), 0.5 * (u[2] * v[0] - u[0] * v[2]),
+                     0.5 * (u[0] * v[1] - u[1] * v[0])};
+      double w = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+      for (int d = 0; d < 3; ++d) {
+        Av[d] += t[d];
+        C[d] += (w / 3.0) * (xa[d] + p0[d] + p1[d]);
+      }
+      W += w;
+    }
+    double s = std::sqrt(Av[0] * Av[0] + Av[1] * Av[1] + Av[2] * Av[2]);
+    if (!(s > 0)) {
+      set_error("mesh: face %lld has zero area", (long long)f);
+      return FPSI_E_INVALID;
+    }
+    ar[f] = s;
+    for (int d = 0; d < 3; ++d) {
+      A[3 * f + d] = Av[d];
+      fc[3 * f + d] = C[d] / W;
+    }
+  }
+  auto shift = [&](int64_t f, int d) { return m->pshift ? m->pshift[3 * f + d] : 0.0; };
+  std::vector<double> xr(nc * 3, 0.0), vol(nc, 0.0), cc(nc * 3, 0.0);
+  std::vector<int32_t> nfc(nc, 0);
+  for (int64_t f = 0; f < nf; ++f) {
+    int32_t a = m->cl[f], b = m->cr[f];
+    for (int d = 0; d < 3; ++d) xr[3 * a + d] += fc[3 * f + d];
+    nfc[a]++;
+    if (b >= 0) {
+      for (int d = 0; d < 3; ++d) xr[3 * b + d] += fc[3 * f + d] - shift(f, d);
+      nfc[b]++;
+    }
+  }
+  for (int64_t c = 0; c < nc; ++c)
+    for (int d = 0; d < 3; ++d) xr[3 * c + d] /= nfc[c];
+  for (int64_t f = 0; f < nf; ++f) {
+    const int64_t b = m->face_off[f], e = m->face_off[f + 1];
+    const int k = int(e - b);
+    double xa[3] = {0, 0, 0};
+    for (int64_t i = b; i < e; ++i)
+      for (int d = 0; d < 3; ++d) xa[d] += m->xyz[3 * int64_t(m->face_nodes[i]) + d];
+    for (int d = 0; d < 3; ++d) xa[d] /= k;
+    for (int side = 0; side < 2; ++side) {
+      int32_t c = side ? m->cr[f] : m->cl[f];
+      if (c < 0) continue;
+      double sg = side ? -1.0 : 1.0;
+      double sh[3] = {side ? shift(f, 0) : 0, side ? shift(f, 1) : 0, side ? shift(f, 2) : 0};
+      const double* x0 = &xr[3 * c];
+      for (int i = 0; i < k; ++i) {
+        const double* q0 = m->xyz + 3 * int64_t(m->face_nodes[b + i]);
+        const double* q1 = m->xyz + 3 * int64_t(m->face_nodes[b + (i + 1) % k]);
+        double pa[3], p0[3], p1[3];
+        for (int d = 0; d < 3; ++d) {
+          pa[d] = xa[d] - sh[d] - x0[d];
+          p0[d] = q0[d] - sh[d] - x0[d];
+          p1[d] = q1[d] - sh[d] - x0[d];
+        }
+        double cr3[3] = {p0[1] * p1[2] - p0[2] * p1[1], p0[2] * p1[0] - p0[0] * p1[2],
+                         p0[0] * p1[1] - p0[1] * p1[0]};
+        double v = sg * (pa[0] * cr3[0] + pa[1] * cr3[1] + pa[2] * cr3[2]) / 6.0;
+        vol[c] += v;
+        for (int d = 0; d < 3; ++d)
+          cc[3 * c + d] += v * 0.25 * (4 * x0[d] + pa[d] + p0[d] + p1[d]);
+      }
+    }
+  }
+  for (int64_t c = 0; c < nc; ++c) {
+    if (!(vol[c] > 0)) {
+      set_error("mesh: cell %lld has non-positive volume %g", (long long)c, vol[c]);
+      return FPSI_E_INVALID;
+    }
+    for (int d = 0; d < 3; ++d) cc[3 * c + d] /= vol[c];
+  }
+  h.an_caller = A;
+  h.area_caller = ar;
+  h.fc_caller = fc;
+
+  // ---- RCM ----
+  std::vector<int64_t> aoff(nc + 1, 0);
+  for (int64_t f = 0; f < nf; ++f)
+    if (m->cr[f] >= 0) {
+      aoff[m->cl[f] + 1]++;
+      aoff[m->cr[f] + 1]++;
+    }
+  for (int64_t c = 0; c < nc; ++c) aoff[c + 1] += aoff[c];
+  std::vector<int32_t> adj(aoff[nc]);
+  {
+    std::vector<int64_t> pos(aoff.begin(), aoff.end() - 1);
+    for (int64_t f = 0; f < nf; ++f)
+      if (m->cr[f] >= 0) {
+        adj[pos[m->cl[f]]++] = m->cr[f];
+        adj[pos[m->cr[f]]++] = m->cl[f];
+      }
+  }
+  h.perm = rcm_order(nc, aoff, adj);
+  h.iperm.assign(nc, 0);
+  for (int64_t i = 0; i < nc; ++i) h.iperm[h.perm[i]] = int32_t(i);
+
+  // ---- faces: interior by (cl, cr) then boundary by (cl, bc) ----
+  std::vector<int64_t> fo(nf);
+  std::iota(fo.begin(), fo.end(), 0);
+  auto key = [&](int64_t f) {
+    int64_t a = h.iperm[m->cl[f]];
+    int64_t b = m->cr[f] >= 0 ? int64_t(h.iperm[m->cr[f]]) : (int64_t(1) << 40) - m->cr[f];
+    int64_t bnd = m->cr[f] < 0 ? 1 : 0;
+    return std::make_tuple(bnd, a, b, f);
+  };
+  std::sort(fo.begin(), fo.end(), [&](int64_t x, int64_t y) { return key(x) < key(y); });
+  h.fperm = fo;
+  h.cl.resize(nf);
+  h.cr.resize(nf);
+  h.n.resize(nf * 3);
+  h.area.resize(nf);
+  h.rL.assign(nf * 3, 0.0);
+  h.rR.assign(nf * 3, 0.0);
+  h.nfi = 0;
+  for (int64_t i = 0; i < nf; ++i) {
+    int64_t f = fo[i];
+    int32_t a = m->cl[f], b = m->cr[f];
+    h.cl[i] = h.iperm[a];
+    h.cr[i] = b >= 0 ? h.iperm[b] : b;
+    if (b >= 0) h.nfi++;
+    h.area[i] = ar[f];
+    for (int d = 0; d < 3; ++d) {
+      h.n[3 * i + d] = A[3 * f + d] / ar[f];
+      h.rL[3 * i + d] = fc[3 * f + d] - cc[3 * a + d];
+      if (b >= 0) h.rR[3 * i + d] = fc[3 * f + d] - (cc[3 * b + d] + shift(f, d));
+    }
+  }
+  h.nbf = nf - h.nfi;
+  h.vol.resize(nc);
+  h.cc.resize(nc * 3);
+  h.vol_tot = 0;
+  for (int64_t i = 0; i < nc; ++i) {
+    int32_t c = h.perm[i];
+    h.vol[i] = vol[c];
+    for (int d = 0; d < 3; ++d) h.cc[3 * i + d] = cc[3 * c + d];
+  }
+  for (int64_t c = 0; c < nc; ++c) h.vol_tot += vol[c];
+
+  // ---- cell -> faces (upper, lower, boundary; each in face order) ----
+  std::vector<int32_t> nu(nc, 0), nl(nc, 0), nb(nc, 0);
+  for (int64_t f = 0; f < nf; ++f) {
+    if (h.cr[f] >= 0) {
+      nu[h.cl[f]]++;
+      nl[h.cr[f]]++;
+    } else {
+      nb[h.cl[f]]++;
+    }
+  }
+  h.cf_off.assign(nc + 1, 0);
+  for (int64_t c = 0; c < nc; ++c) h.cf_off[c + 1] = h.cf_off[c] + nu[c] + nl[c] + nb[c];
+  h.cf.assign(h.cf_off[nc], 0);
+  {
+    std::vector<int32_t> pu(nc), pl(nc), pb(nc);
+    for (int64_t c = 0; c < nc; ++c) {
+      pu[c] = h.cf_off[c];
+      pl[c] = h.cf_off[c] + nu[c];
+      pb[c] = h.cf_off[c] + nu[c] + nl[c];
+    }
+    for (int64_t f = 0; f < nf; ++f) {
+      int32_t e = int32_t(f) << 1;
+      if (h.cr[f] >= 0) {
+        h.cf[pu[h.cl[f]]++] = e;
+        h.cf[pl[h.cr[f]]++] = e | 1;
+      } else {
+        h.cf[pb[h.cl[f]]++] = e;
+      }
+    }
+  }
+  // ---- least-squares normal matrices (inverse, symmetric 6 entries) ----
+  h.Minv.assign(nc * 6, 0.0);
+  for (int64_t c = 0; c < nc; ++c) {
+    double M[6] = {0, 0, 0, 0, 0, 0};
+    for (int32_t k = h.cf_off[c]; k < h.cf_off[c + 1]; ++k) {
+      int64_t f = h.cf[k] >> 1;
+      int side = h.cf[k] & 1;
+      double dv[3];
+      for (int d = 0; d < 3; ++d) {
+        if (h.cr[f] < 0)
+          dv[d] = h.rL[3 * f + d];
+        else
+          dv[d] = side ? h.rR[3 * f + d] - h.rL[3 * f + d] : h.rL[3 * f + d] - h.rR[3 * f + d];
+      }
+      M[0] += dv[0] * dv[0], M[1] += dv[0] * dv[1], M[2] += dv[0] * dv[2];
+      M[3] += dv[1] * dv[1], M[4] += dv[1] * dv[2], M[5] += dv[2] * dv[2];
+    }
+    double a = M[0], b = M[1], cq = M[2], d = M[3], e = M[4], ff = M[5];
+    double A00 = d * ff - e * e, A01 = cq * e - b * ff, A02 = b * e - cq * d;
+    double A11 = a * ff - cq * cq, A12 = b * cq - a * e, A22 = a * d - b * b;
+    double det = a * A00 + b * A01 + cq * A02;
+    if (!(std::fabs(det) > 0)) {
+      set_error("mesh: singular least-squares matrix in cell %lld", (long long)c);
+      return FPSI_E_INVALID;
+    }
+    double r = 1.0 / det;
+    double* mi = &h.Minv[6 * c];
+    mi[0] = A00 * r, mi[1] = A01 * r, mi[2] = A02 * r;
+    mi[3] = A11 * r, mi[4] = A12 * r, mi[5] = A22 * r;
+  }
+  // ---- greedy colouring in the new order ----
+  h.colour.assign(nc, -1);
+  int ncol = 0;
+  std::vector<int64_t> mark(64, -1);
+  for (int64_t c = 0; c < nc; ++c) {
+    for (int32_t k = h.cf_off[c]; k < h.cf_off[c + 1]; ++k) {
+      int64_t f = h.cf[k] >> 1;
+      if (h.cr[f] < 0) continue;
+      int32_t o = (h.cf[k] & 1) ? h.cl[f] : h.cr[f];
+      int32_t col = h.colour[o];
+      if (col >= 0) {
+        if (col >= (int)mark.size()) mark.resize(col + 1, -1);
+        mark[col] = c;
+      }
+    }
+    int col = 0;
+    while (col < (int)mark.size() && mark[col] == c) ++col;
+    h.colour[c] = col;
+    ncol = std::max(ncol, col + 1);
+  }
+  h.ncolours = ncol;
+  h.colour_off.assign(ncol + 1, 0);
+  for (int64_t c = 0; c < nc; ++c) h.colour_off[h.colour[c] + 1]++;
+  for (int k = 0; k < ncol; ++k) h.colour_off[k + 1] += h.colour_off[k];
+  h.colour_cells.assign(nc, 0);
+  {
+    std::vector<int32_t> pos(h.colour_off.begin(), h.colour_off.end() - 1);
+    for (int64_t c = 0; c < nc; ++c) h.colour_cells[pos[h.colour[c]]++] = int32_t(c);
+  }
+  return FPSI_OK;
+}
+
+}  // namespace fpsi

@@ -1,0 +1,314 @@
+"""Host-side mirror of flowPsi's hot-path rules over the device library.
+
+Each method corresponds to the Loci rule(s) it replaces (reference file:line
+in the docstring) and keeps the reference's names, argument meaning and
+error behaviour (a NaN residual raises, as solverResidual.loci:203-208
+aborts).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+
+
+def default_params(**kw) -> N.Params:
+    """Reference defaults (solverEoS.loci:27-47, solverTimestep.loci:281-287,
+    linearSolverSGS.loci:39-41, linearSolverLSGS.loci:96-108,
+    solverNewton.loci:222-228), overridden by keyword (strings accepted for
+    flux, limiter, fluidLinearSolver/solver and precision)."""
+    p = N.Params()
+    N.lib().fpsi_default_params(C.byref(p))
+    alias = {"fluidLinearSolver": "solver", "inviscidFlux": "flux"}
+    for k, v in kw.items():
+        k = alias.get(k, k)
+        if k == "flux" and isinstance(v, str):
+            v = N.FLUX[v]
+        elif k == "limiter" and isinstance(v, str):
+            v = N.LIMITER[v]
+        elif k == "solver" and isinstance(v, str):
+            v = N.SOLVER[v]
+        elif k == "precision" and isinstance(v, str):
+            v = N.PRECISION[v]
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+def bc(kind: str, T: float = 300.0, pg: float = 1e5, u=(0.0, 0.0, 0.0)) -> N.BCSpec:
+    b = N.BCSpec()
+    b.kind = N.BC[kind]
+    b.T, b.pg = T, pg
+    for i in range(3):
+        b.u[i] = u[i]
+    return b
+
+
+@dataclass
+class MeshArrays:
+    """numpy views of a generated mesh (caller/Loci numbering)."""
+    ncells: int
+    nfaces: int
+    xyz: np.ndarray
+    face_off: np.ndarray
+    face_nodes: np.ndarray
+    cl: np.ndarray
+    cr: np.ndarray
+    pshift: np.ndarray | None
+    bcs: list = field(default_factory=list)
+
+
+class GeneratedMesh:
+    """A synthetic grid owned by the library (fpsi_mesh_generate)."""
+
+    def __init__(self, kind: str, n=(8, 8, 8), L=(1.0, 1.0, 1.0), jitter=0.0, seed=0,
+                 bc_side=(-1, -1, -1, -1, -1, -1), bcs=(), dy0=1e-3, growth=1.1):
+        s = N.MeshSpec()
+        s.kind = {"hex": 0, "kuhn": 1, "bl": 2}[kind]
+        s.nx, s.ny, s.nz = n
+        s.Lx, s.Ly, s.Lz = L
+        s.jitter = jitter
+        s.seed = seed
+        s.dy0, s.growth = dy0, growth
+        for i in range(6):
+            s.bc_side[i] = bc_side[i]
+        s.nbc = len(bcs)
+        for i, b in enumerate(bcs):
+            s.bcs[i] = b
+        p = C.POINTER(N.Mesh)()
+        N.check(N.lib().fpsi_mesh_generate(C.byref(s), C.byref(p)), "fpsi_mesh_generate")
+        self._p = p
+        self.spec = s
+
+    @property
+    def ptr(self):
+        return self._p
+
+    @property
+    def m(self) -> N.Mesh:
+        return self._p.contents
+
+    def arrays(self) -> MeshArrays:
+        m = self.m
+        nf = m.nfaces
+        nfn = np.ctypeslib.as_array(m.face_off, shape=(nf + 1,))[-1]
+        pshift = (np.ctypeslib.as_array(m.pshift, shape=(nf * 3,)) if bool(m.pshift) else None)
+        return MeshArrays(
+            ncells=m.ncells, nfaces=nf,
+            xyz=np.ctypeslib.as_array(m.xyz, shape=(m.nnodes * 3,)),
+            face_off=np.ctypeslib.as_array(m.face_off, shape=(nf + 1,)),
+            face_nodes=np.ctypeslib.as_array(m.face_nodes, shape=(int(nfn),)),
+            cl=np.ctypeslib.as_array(m.cl, shape=(nf,)),
+            cr=np.ctypeslib.as_array(m.cr, shape=(nf,)),
+            pshift=pshift,
+            bcs=[m.bcs[i] for i in range(m.nbc)],
+        )
+
+    def __del__(self):
+        if getattr(self, "_p", None):
+            N.lib().fpsi_mesh_free(self._p)
+            self._p = None
+
+
+class FlowPsi:
+    """One steady implicit solver instance on the GPU (fpsi_ctx)."""
+
+    def __init__(self, mesh: GeneratedMesh | N.Mesh, params: N.Params | None = None):
+        self._mesh = mesh  # keep the arrays alive
+        self.params = params if params is not None else default_params()
+        mp = mesh.ptr if isinstance(mesh, GeneratedMesh) else C.pointer(mesh)
+        ctx = C.c_void_p()
+        N.check(N.lib().fpsi_create(C.byref(ctx), mp, C.byref(self.params)), "fpsi_create")
+        self._ctx = ctx
+        nc, nf, ncol, nb = C.c_int64(), C.c_int64(), C.c_int32(), C.c_int64()
+        N.lib().fpsi_info(ctx, C.byref(nc), C.byref(nf), C.byref(ncol), C.byref(nb))
+        self.ncells, self.nfaces, self.ncolours = nc.value, nf.value, ncol.value
+        self.device_bytes = nb.value
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            N.lib().fpsi_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- parameters / geometry --------------------------------------------
+    def set_params(self, params: N.Params) -> None:
+        N.check(N.lib().fpsi_set_params(self._ctx, C.byref(params)), "fpsi_set_params")
+        self.params = params
+
+    @property
+    def block_dtype(self):
+        return np.float64 if self.params.precision == N.PRECISION["fp64"] else np.float32
+
+    def geometry(self) -> dict:
+        nc, nf = self.ncells, self.nfaces
+        vol, cc = np.empty(nc), np.empty(nc * 3)
+        an, ar, fc = np.empty(nf * 3), np.empty(nf), np.empty(nf * 3)
+        N.check(N.lib().fpsi_get_geometry(self._ctx, N.dptr(vol), N.dptr(cc), N.dptr(an),
+                                          N.dptr(ar), N.dptr(fc)), "fpsi_get_geometry")
+        return {"vol": vol, "cellcenter": cc.reshape(nc, 3), "area_vec": an.reshape(nf, 3),
+                "area": ar, "facecenter": fc.reshape(nf, 3)}
+
+    def colours(self) -> np.ndarray:
+        c = np.empty(self.ncells, np.int32)
+        N.check(N.lib().fpsi_get_colours(self._ctx, N.iptr(c)), "fpsi_get_colours")
+        return c
+
+    # -- state -------------------------------------------------------------
+    def set_state(self, T, pg, u) -> None:
+        T = np.ascontiguousarray(T, np.float64)
+        pg = np.ascontiguousarray(pg, np.float64)
+        u = np.ascontiguousarray(u, np.float64).reshape(-1)
+        assert T.size == self.ncells and pg.size == self.ncells and u.size == 3 * self.ncells
+        N.check(N.lib().fpsi_set_state(self._ctx, N.dptr(T), N.dptr(pg), N.dptr(u)),
+                "fpsi_set_state")
+
+    def get_state(self):
+        nc = self.ncells
+        T, pg, u = np.empty(nc), np.empty(nc), np.empty(nc * 3)
+        N.check(N.lib().fpsi_get_state(self._ctx, N.dptr(T), N.dptr(pg), N.dptr(u)),
+                "fpsi_get_state")
+        return T, pg, u.reshape(nc, 3)
+
+    # -- rules ---------------------------------------------------------------
+    def residual(self, want_src: bool = True):
+        """'src' store and 'residual' norms (fluxInviscid.loci:1253-1268,
+        solverResidual.loci:74-112)."""
+        src = np.empty(self.ncells * 5) if want_src else None
+        r = N.Resid()
+        N.check(N.lib().fpsi_residual(self._ctx, N.dptr(src), C.byref(r)), "fpsi_residual")
+        return (src.reshape(-1, 5) if want_src else None), r.as_dict()
+
+    def reconstruction(self):
+        g, l = np.empty(self.ncells * 15), np.empty(self.ncells * 5)
+        N.check(N.lib().fpsi_get_reconstruction(self._ctx, N.dptr(g), N.dptr(l)),
+                "fpsi_get_reconstruction")
+        return g.reshape(-1, 15), l.reshape(-1, 5)
+
+    def dtau(self) -> np.ndarray:
+        """local pseudo time step, solverTimestep.loci:302-329"""
+        d = np.empty(self.ncells)
+        N.check(N.lib().fpsi_get_dtau(self._ctx, N.dptr(d)), "fpsi_get_dtau")
+        return d
+
+    def assemble(self) -> None:
+        """fjp/fjm, srcJ, fluid_D, fluid_B and the LU of fluid_D
+        (fluxInviscid.loci:1190-1221, solverLinearSystem.loci:45-224,
+        linearSolverSGS.loci:43-50)."""
+        N.check(N.lib().fpsi_assemble(self._ctx), "fpsi_assemble")
+
+    def blocks(self) -> dict:
+        dt = self.block_dtype
+        nc, nf = self.ncells, self.nfaces
+        D, fjp, fjm, B = (np.empty((nc, 5, 5), dt), np.empty((nf, 5, 5), dt),
+                          np.empty((nf, 5, 5), dt), np.empty((nc, 5), dt))
+        N.check(N.lib().fpsi_get_blocks(self._ctx, N.vptr(D), N.vptr(fjp), N.vptr(fjm),
+                                        N.vptr(B)), "fpsi_get_blocks")
+        return {"fluid_D": D, "fjp": fjp, "fjm": fjm, "fluid_B": B}
+
+    def linear_solve(self, x0: np.ndarray | None = None) -> np.ndarray:
+        """SGSBlockedSSolve(fluid) -> dfluid (linearSolverSGS.loci:57-329,
+        solverNewton.loci:252-259); x0 None = block Jacobi start."""
+        dq = np.empty(self.ncells * 5)
+        x0p = None if x0 is None else np.ascontiguousarray(x0, np.float64).reshape(-1)
+        info = N.LsInfo()
+        N.check(N.lib().fpsi_linear_solve(self._ctx, N.dptr(x0p), N.dptr(dq), C.byref(info)),
+                "fpsi_linear_solve")
+        return dq.reshape(-1, 5)
+
+    def linear_residual(self):
+        nb, nr = C.c_double(), C.c_double()
+        N.check(N.lib().fpsi_linear_residual(self._ctx, C.byref(nb), C.byref(nr)),
+                "fpsi_linear_residual")
+        return nb.value, nr.value
+
+    def update(self) -> float:
+        """clipped Newton update, solverNewton.loci:62-78"""
+        a = C.c_double()
+        N.check(N.lib().fpsi_update(self._ctx, C.byref(a)), "fpsi_update")
+        return a.value
+
+    def newton_step(self) -> dict:
+        si = N.StepInfo()
+        N.check(N.lib().fpsi_newton_step(self._ctx, C.byref(si)), "fpsi_newton_step")
+        d = si.resid.as_dict()
+        d["min_alpha"] = si.min_alpha
+        return d
+
+    def run(self, nsteps: int) -> list[dict]:
+        arr = (N.Resid * max(nsteps, 1))()
+        N.check(N.lib().fpsi_run(self._ctx, nsteps, arr), "fpsi_run")
+        return [arr[i].as_dict() for i in range(nsteps)]
+
+    def run_timed(self, nsteps: int):
+        """(norm history, device milliseconds) of nsteps steps, timed with
+        CUDA events on the library's stream"""
+        arr = (N.Resid * max(nsteps, 1))()
+        ms = C.c_double()
+        N.check(N.lib().fpsi_run_timed(self._ctx, nsteps, arr, C.byref(ms)), "fpsi_run_timed")
+        return [arr[i].as_dict() for i in range(nsteps)], ms.value
+
+    def kernel_times(self, nsteps: int = 1) -> dict:
+        """{kernel: (total ms, launches)} over nsteps steps"""
+        cap = 64
+        names = C.create_string_buffer(32 * cap)
+        ms = np.zeros(cap)
+        lc = np.zeros(cap, np.int64)
+        cnt = C.c_int32()
+        N.check(N.lib().fpsi_kernel_times(self._ctx, nsteps, cap, names, N.dptr(ms),
+                                          lc.ctypes.data_as(C.POINTER(C.c_int64)), C.byref(cnt)),
+                "fpsi_kernel_times")
+        raw = names.raw
+        out = {}
+        for k in range(cnt.value):
+            nm = raw[32 * k:32 * k + 32].split(b"\0")[0].decode()
+            out[nm] = (float(ms[k]), int(lc[k]))
+        return out
+
+    def keep_blocks(self, keep: bool) -> None:
+        N.check(N.lib().fpsi_keep_blocks(self._ctx, 1 if keep else 0), "fpsi_keep_blocks")
+
+
+# -- inviscidFlux.h entry points on batches ---------------------------------
+def inviscid_riemann_flux(kind, qL, qR, an, area, pambient=0.0, Rt=8314.4621 / 28.96,
+                          gamma=1.4, us_n=0.0, eta=1.0) -> np.ndarray:
+    """Batched inviscidRiemannFlux / roeCT_flux / HLLE; states packed
+    [pg, T, u, v, w] per face."""
+    kind = N.FLUX[kind] if isinstance(kind, str) else kind
+    qL = np.ascontiguousarray(qL, np.float64)
+    qR = np.ascontiguousarray(qR, np.float64)
+    an = np.ascontiguousarray(an, np.float64)
+    area = np.ascontiguousarray(area, np.float64)
+    n = area.size
+    out = np.empty((n, 5))
+    N.check(N.lib().fpsi_face_flux(kind, n, N.dptr(qL), N.dptr(qR), N.dptr(an), N.dptr(area),
+                                   pambient, Rt, gamma, us_n, eta, N.dptr(out)), "fpsi_face_flux")
+    return out
+
+
+def roe_jacobian(qL, qR, an, area, direction, pambient=0.0, Rt=8314.4621 / 28.96, gamma=1.4,
+                 us_n=0.0, eta=1.0, as_double=False) -> np.ndarray:
+    """Batched roeCT_jacobian (fjp for direction=+1, fjm for -1)."""
+    qL = np.ascontiguousarray(qL, np.float64)
+    qR = np.ascontiguousarray(qR, np.float64)
+    an = np.ascontiguousarray(an, np.float64)
+    area = np.ascontiguousarray(area, np.float64)
+    n = area.size
+    out = np.empty((n, 5, 5), np.float64 if as_double else np.float32)
+    N.check(N.lib().fpsi_face_jacobian(n, N.dptr(qL), N.dptr(qR), N.dptr(an), N.dptr(area),
+                                       pambient, Rt, gamma, us_n, eta, direction,
+                                       1 if as_double else 0, N.vptr(out)),
+            "fpsi_face_jacobian")
+    return out

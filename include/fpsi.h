@@ -1,0 +1,259 @@
+/*
+ * fpsi.h -- C ABI of the B200-native implicit residual-and-relaxation path.
+ *
+ * The library replaces, on one GPU, the chain of Loci rules that flowPsi runs
+ * once per Newton iteration of a steady implicit step:
+ *
+ *   residual      src = -sum(iflux)                 fluxInviscid.loci:1170-1188,1253-1268
+ *   time step     cflpdt, dtcfl, dtau, rhs = src    solverSetup.loci:81-119,
+ *                                                   solverTimestep.loci:289-338
+ *   Jacobians     fjp / fjm (smoothed Roe)          fluxInviscid.loci:1190-1221
+ *   assembly      fluid_L/U/D/B                     solverLinearSystem.loci:45-224
+ *   relaxation    SGSBlockedSSolve / LSGS           linearSolverSGS.loci:43-329,
+ *                                                   linearSolverLSGS.loci:1692-1954
+ *   update        clipped Newton update             solverNewton.loci:62-91
+ *   norms         residual (rtrms, etrms, ...)      solverResidual.loci:74-112
+ *
+ * Conventions (all shared with the reference):
+ *   - primitive variables q = [T, u, v, w, p_g] (column order of every 5x5
+ *     block; rows are the rho, rho u, rho v, rho w, rho e0 equations);
+ *   - blocks are row-major, 25 contiguous values per entity;
+ *   - interior face normals point from cl to cr; boundary faces have cr < 0
+ *     and name boundary condition -cr-1;
+ *   - host arrays are in the caller's (Loci) entity order and AoS layout; the
+ *     library keeps its own RCM order and SoA layout on the device and
+ *     translates at this boundary.
+ *
+ * Every function returns 0 on success or a negative FPSI_E_* code; no C++
+ * exception crosses the ABI.  There is no CPU fallback: without a usable CUDA
+ * device every compute entry point returns FPSI_E_CUDA.
+ */
+#ifndef FPSI_H
+#define FPSI_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes -------------------------------------------------------- */
+#define FPSI_OK              0
+#define FPSI_E_INVALID      -1   /* bad argument or inconsistent mesh        */
+#define FPSI_E_CUDA         -2   /* CUDA runtime failure / no device          */
+#define FPSI_E_NOMEM        -3   /* device or host allocation failed          */
+#define FPSI_E_UNSUPPORTED  -4   /* option not implemented on this path       */
+#define FPSI_E_SINGULAR     -5   /* zero pivot in a 5x5 block LU              */
+#define FPSI_E_NAN          -6   /* NaN residual (solverResidual.loci:203-208)*/
+#define FPSI_E_TIMEOUT      -7   /* a bounded device wait gave up             */
+#define FPSI_E_STATE        -8   /* call out of order (e.g. solve before assemble) */
+
+/* ---- options (names and defaults follow the reference's vars) ----------- */
+enum fpsi_flux_kind {          /* inviscidRiemannFlux, inviscidFlux.h:82-90 */
+  FPSI_FLUX_HLLC = 0,          /* hllc_flux, fluxInviscid.loci:157-256 (reference default) */
+  FPSI_FLUX_ROE  = 1,          /* roeCT_flux, fluxInviscid.loci:869-1014 */
+  FPSI_FLUX_HLLE = 2           /* two-wave HLL with hllc_flux's SL/SR (no reference counterpart) */
+};
+enum fpsi_limiter_kind {       /* vars 'limiter' (guide.tex:495-518) */
+  FPSI_LIMITER_VENKATAKRISHNAN = 0,
+  FPSI_LIMITER_BARTH = 1,
+  FPSI_LIMITER_NONE = 2,
+  FPSI_LIMITER_ZERO = 3
+};
+enum fpsi_solver_kind {        /* vars 'fluidLinearSolver' (solverNewton.loci:222-249) */
+  FPSI_SOLVER_SGS = 0,         /* multi-colour block SGS */
+  FPSI_SOLVER_LSGS = 1         /* line SGS (batched block-tridiagonal lines) */
+};
+enum fpsi_precision {
+  FPSI_PREC_FP64 = 0,          /* every block and iterate in FP64 */
+  FPSI_PREC_REF = 1,           /* reference precision: FP32 blocks and B, FP64 iterate */
+  FPSI_PREC_MIXED = 2          /* FP32 blocks, LU and sweeps (defect correction) */
+};
+enum fpsi_bc_kind {
+  FPSI_BC_FARFIELD = 1,            /* bcInflow.loci:311-375 */
+  FPSI_BC_SUPERSONIC_INFLOW = 2,   /* bcInflow.loci:270-309 */
+  FPSI_BC_SUPERSONIC_OUTFLOW = 3,  /* bcOutflow.loci:127-165 */
+  FPSI_BC_EXTRAPOLATE = 4,         /* bcOutflow.loci:84-120 */
+  FPSI_BC_REFLECTING = 5,          /* symmetry / slip wall, bcImpermeable.loci:48-140 */
+  FPSI_BC_VISCOUS_WALL = 6         /* adiabatic no-slip wall, bcViscousWall.loci:146-240 */
+};
+
+typedef struct fpsi_params {
+  double gamma;            /* 1.4                                  solverEoS.loci:31 */
+  double Rtilde;           /* 8314.4621/28.96                      solverEoS.loci:34-37 */
+  double Pambient;         /* p0 = 0                               solverEoS.loci:39-47 */
+  double Minf;             /* 1; eta == 1 for Minf >= 0.5          fluxInviscid.loci:97-112 */
+  int32_t flux;            /* fpsi_flux_kind, default HLLC */
+  int32_t limiter;         /* fpsi_limiter_kind, default venkatakrishnan */
+  double Kl;               /* Venkatakrishnan threshold, default 1 */
+  double urelax;           /* 0.2                                  solverTimestep.loci:281-283 */
+  double dtmax;            /* 1.0                                  solverTimestep.loci:285-287 */
+  double cflmax;           /* <= 0 disables the CFL time step      solverTimestep.loci:294-297 */
+  int32_t solver;          /* fpsi_solver_kind, default LSGS */
+  int32_t gauss_seidel_iter; /* 6                                  linearSolverSGS.loci:39-41 */
+  double lsgs_relaxation;  /* 0.25                                 linearSolverLSGS.loci:96-108 */
+  double lsgs_abs_tol;     /* 1e-10 */
+  double lsgs_rel_tol;     /* 0.1 */
+  int32_t lsgs_max_iter;   /* 10 */
+  int32_t precision;       /* fpsi_precision, default FPSI_PREC_REF */
+  int32_t viscous;         /* 0 inviscid, 1 laminar (Sutherland), 2 turbulent (needs tmu) */
+  int32_t reserved0;
+  double Pr;               /* 0.72 laminar Prandtl */
+  double Prt;              /* 0.9 turbulent Prandtl */
+  double sutherland_mu0, sutherland_T0, sutherland_S; /* air: 1.716e-5, 273.15, 110.4 */
+} fpsi_params;
+
+typedef struct fpsi_bc {
+  int32_t kind;            /* fpsi_bc_kind */
+  int32_t reserved;
+  double T, pg, u[3];      /* reference state (temperatureRef, gagePressureRef, uRef) */
+} fpsi_bc;
+
+/* Unstructured mesh in the caller's numbering.  Face nodes are ordered so
+ * that the right-hand-rule normal points from cl to cr.  For periodic faces
+ * (translation only) pshift[3f..3f+2] is the vector that moves cell cr next to
+ * cl (x_cr_image = x_cr + pshift); NULL means no periodic faces. */
+typedef struct fpsi_mesh {
+  int64_t nnodes, ncells, nfaces;
+  const double*  xyz;          /* nnodes*3 */
+  const int64_t* face_off;     /* nfaces+1 */
+  const int32_t* face_nodes;   /* face_off[nfaces] */
+  const int32_t* cl;           /* nfaces */
+  const int32_t* cr;           /* nfaces; < 0 => boundary condition -cr-1 */
+  const double*  pshift;       /* nfaces*3 or NULL */
+  int32_t nbc;
+  int32_t reserved;
+  const fpsi_bc* bcs;          /* nbc */
+} fpsi_mesh;
+
+typedef struct fpsi_resid {    /* flowPsi::residual, flowTypes.h:421-427 (rms already square-rooted) */
+  double rtrms, etrms, mtrms;  /* volume-weighted RMS of src/V: density, energy, momentum */
+  double rtmax, etmax, mtmax;  /* signed L-inf values */
+  double ccmaxr_center[3];
+  double ccmaxe_center[3];
+  uint64_t bcErrorCode;
+} fpsi_resid;
+
+typedef struct fpsi_lsinfo {
+  int32_t iterations;          /* symmetric sweeps (SGS) or line iterations (LSGS) */
+  int32_t status;
+  double resid0, resid;        /* ||B - A x|| before / after (if measured) */
+} fpsi_lsinfo;
+
+typedef struct fpsi_stepinfo {
+  fpsi_resid resid;            /* norms of the residual the step started from */
+  fpsi_lsinfo ls;
+  double min_alpha;            /* smallest Newton clip factor applied */
+  double dtau_min, dtau_max;
+} fpsi_stepinfo;
+
+typedef struct fpsi_ctx fpsi_ctx;
+
+/* ---- parameters / errors -------------------------------------------------- */
+void        fpsi_default_params(fpsi_params* p);
+const char* fpsi_strerror(int code);
+const char* fpsi_last_error(void);   /* detail of the last failure in this thread */
+int         fpsi_device_available(void);
+
+/* ---- synthetic meshes (host memory, caller frees with fpsi_mesh_free) ------
+ * kind 0: nx*ny*nz hex box [0,Lx]x[0,Ly]x[0,Lz], boundary condition of the six
+ *         sides bc_side[0..5] = (xmin, xmax, ymin, ymax, zmin, zmax); an entry
+ *         of -1 makes that direction periodic (both sides).
+ * kind 1: nx*ny*nz hexes each split into 6 Kuhn tetrahedra on the periodic
+ *         box [0,Lx]x[0,Ly]x[0,Lz]; nodes jittered by U(-jitter,+jitter)*h.
+ * kind 2: boundary-layer hex block: y spacing dy0*growth^j.
+ * Returns an fpsi_mesh whose arrays are owned by the library. */
+typedef struct fpsi_mesh_spec {
+  int32_t kind;
+  int32_t nx, ny, nz;
+  double Lx, Ly, Lz;
+  double jitter;              /* fraction of the spacing */
+  double dy0, growth;         /* kind 2 */
+  uint64_t seed;
+  int32_t bc_side[6];         /* index into bcs, or -1 (periodic) */
+  int32_t nbc;
+  int32_t reserved;
+  fpsi_bc bcs[8];
+} fpsi_mesh_spec;
+int  fpsi_mesh_generate(const fpsi_mesh_spec* spec, fpsi_mesh** out);
+void fpsi_mesh_free(fpsi_mesh* m);
+
+/* ---- context -------------------------------------------------------------- */
+int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params);
+int fpsi_destroy(fpsi_ctx* ctx);
+int fpsi_set_params(fpsi_ctx* ctx, const fpsi_params* params);
+int fpsi_info(fpsi_ctx* ctx, int64_t* ncells, int64_t* nfaces, int32_t* ncolours,
+              int64_t* device_bytes);
+
+/* geometry as the library computed it (caller order): cell volumes and
+ * centroids, face area vectors (n*|A|) and centroids; any pointer may be NULL */
+int fpsi_get_geometry(fpsi_ctx* ctx, double* vol, double* cellcenter,
+                      double* face_an, double* face_area, double* facecenter);
+/* keep (1, default) or drop (0) the unfactored diagonal blocks after the LU;
+ * fpsi_linear_residual and the D export of fpsi_get_blocks need them */
+int fpsi_keep_blocks(fpsi_ctx* ctx, int32_t keep);
+/* cell colour used by the multi-colour sweeps (caller order) */
+int fpsi_get_colours(fpsi_ctx* ctx, int32_t* colour);
+
+/* state in Loci layout: T[nc], pg[nc], u[nc*3] (AoS) */
+int fpsi_set_state(fpsi_ctx* ctx, const double* T, const double* pg, const double* u);
+int fpsi_get_state(fpsi_ctx* ctx, double* T, double* pg, double* u);
+
+/* residual of the current state.  src (nc*5, AoS, may be NULL) receives
+ * the reference's 'src' store; norms may be NULL.  grad (nc*15: dT/dx..,
+ * du/dx.., dv/dx.., dw/dx.., dp/dx..) and limiter (nc*5) are optional views
+ * of the reconstruction inputs. */
+int fpsi_residual(fpsi_ctx* ctx, double* src, fpsi_resid* norms);
+int fpsi_get_reconstruction(fpsi_ctx* ctx, double* grad, double* limiter);
+
+/* local pseudo time step from the last residual (solverTimestep.loci:302-329) */
+int fpsi_get_dtau(fpsi_ctx* ctx, double* dtau);
+
+/* Jacobians and diagonal blocks for the last residual's state and dtau,
+ * followed by the batched LU of the diagonal blocks. */
+int fpsi_assemble(fpsi_ctx* ctx);
+/* optional export of the assembled blocks (caller order, row-major 25 per
+ * entity, as float in REF/MIXED and as double in FP64 precision):
+ * D (nc*25, before factorisation), fjp and fjm (nfaces*25), B (nc*5). */
+int fpsi_get_blocks(fpsi_ctx* ctx, void* D, void* fjp, void* fjm, void* B);
+
+/* relaxation of  A dq = B.  x0 (nc*5 AoS) NULL selects the reference start
+ * (block Jacobi D^-1 B).  dq (nc*5 AoS) may be NULL (result stays on the
+ * device for fpsi_update). */
+int fpsi_linear_solve(fpsi_ctx* ctx, const double* x0, double* dq, fpsi_lsinfo* info);
+/* || B - A x || (2-norm over all cells) of the device iterate */
+int fpsi_linear_residual(fpsi_ctx* ctx, double* norm_b, double* norm_r);
+/* clipped Newton update with the device dq (solverNewton.loci:62-78) */
+int fpsi_update(fpsi_ctx* ctx, double* min_alpha);
+
+/* one steady implicit step: residual -> dtau -> assemble -> solve -> update */
+int fpsi_newton_step(fpsi_ctx* ctx, fpsi_stepinfo* info);
+/* nsteps steps without host round trips; norms[k] of each step (may be NULL) */
+int fpsi_run(fpsi_ctx* ctx, int32_t nsteps, fpsi_resid* norms);
+/* fpsi_run timed on the device: CUDA events recorded on the library's
+ * stream around the nsteps steps; device_ms receives the elapsed time. */
+int fpsi_run_timed(fpsi_ctx* ctx, int32_t nsteps, fpsi_resid* norms, double* device_ms);
+/* Per-kernel device time of nsteps steps (CUDA events around every launch
+ * group on the library's stream).  Fills up to cap entries of names (32
+ * chars each), total ms and launch counts; *count receives the number of
+ * kernel kinds. */
+int fpsi_kernel_times(fpsi_ctx* ctx, int32_t nsteps, int32_t cap, char* names, double* ms,
+                      int64_t* launches, int32_t* count);
+
+/* ---- face functions on batches (inviscidFlux.h entry points) --------------
+ * States are packed per face as [pg, T, u, v, w] (n*5), normals n*3 (unit),
+ * area n.  Host pointers; copies and one kernel launch inside. */
+int fpsi_face_flux(int32_t kind, int64_t n, const double* qL, const double* qR,
+                   const double* an, const double* area, double pambient,
+                   double Rt, double gamma, double us_n, double eta, double* flux);
+/* roeCT_jacobian (fluxInviscid.loci:1092-1168); dir = +1 (fjp) or -1 (fjm).
+ * out is n*25 float (real_fj) or double when as_double != 0. */
+int fpsi_face_jacobian(int64_t n, const double* qL, const double* qR,
+                       const double* an, const double* area, double pambient,
+                       double Rt, double gamma, double us_n, double eta,
+                       int32_t dir, int32_t as_double, void* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FPSI_H */

@@ -1,0 +1,1373 @@
+// oracle.cpp -- CPU restatement of flowPsi's steady implicit hot path.
+//
+// TEST INFRASTRUCTURE ONLY (the checker): called by tests/, the smoke check
+// and the CPU-baseline leg of bench.py; never linked by the product library.
+//
+// Scalar C++ that follows the reference rule by rule, in the reference's own
+// evaluation order where the order changes rounding (face-order scatter,
+// upper-then-lower accumulation, FP32 stores for real_fj blocks).
+#include "oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+struct V3 {
+  double x, y, z;
+};
+inline V3 mk(double x, double y, double z) { return V3{x, y, z}; }
+inline V3 operator+(V3 a, V3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline V3 operator-(V3 a, V3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+inline V3 operator*(double s, V3 a) { return mk(s * a.x, s * a.y, s * a.z); }
+inline V3 operator*(V3 a, double s) { return mk(s * a.x, s * a.y, s * a.z); }
+inline double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 cross(V3 a, V3 b) {
+  return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+inline double norm(V3 a) { return std::sqrt(dot(a, a)); }
+
+// ---------------------------------------------------------------------------
+// Face physics
+// ---------------------------------------------------------------------------
+
+// inviscidFlux, inviscidFlux.h:25-45: analytic flux of one state.
+void analytic_flux(double f[5], double pg, double T, V3 U, V3 an, double area,
+                   double pamb, double Rt, double gamma, double Us_n) {
+  double gm1 = gamma - 1;
+  double rho = (pg + pamb) / (Rt * T);
+  double h0 = Rt * T * gamma / gm1 + 0.5 * dot(U, U);
+  double e0 = h0 - Rt * T;
+  double uta = dot(U, an);
+  double ut = uta - Us_n;
+  double mdot = area * rho * ut;
+  double p = pg + pamb;
+  f[0] = mdot;
+  f[1] = mdot * U.x + area * pg * an.x;
+  f[2] = mdot * U.y + area * pg * an.y;
+  f[3] = mdot * U.z + area * pg * an.z;
+  f[4] = mdot * e0 + area * p * uta;
+}
+
+// hllc_flux, fluxInviscid.loci:157-256.
+void hllc_flux(double F[5], double pgl, double Tl, V3 Ul, double pgr, double Tr, V3 Ur,
+               V3 an, double area, double pamb, double Rt, double gamma, double Us_n,
+               double Eta) {
+  double gm1 = gamma - 1;
+  double rl = (pgl + pamb) / (Rt * Tl);
+  double rr = (pgr + pamb) / (Rt * Tr);
+  double h0l = Rt * Tl * gamma / gm1 + 0.5 * dot(Ul, Ul);
+  double h0r = Rt * Tr * gamma / gm1 + 0.5 * dot(Ur, Ur);
+  double e0l = h0l - Rt * Tl;
+  double e0r = h0r - Rt * Tr;
+  double srl = std::sqrt(rl), srr = std::sqrt(rr);
+  double rf = 1. / (srl + srr);
+  V3 U_ = (Ul * srl + Ur * srr) * rf;
+  double ut_ = dot(U_, an) - Us_n;
+  double h0_ = (h0l * srl + h0r * srr) * rf;
+  double a_ = std::sqrt(std::max(gm1 * (h0_ - 0.5 * dot(U_, U_)), 0.0));
+  double EtaP = Eta + 1., EtaM = Eta - 1.;
+  double sigma = std::sqrt(std::max(ut_ * ut_ * EtaM * EtaM + 4. * Eta * a_ * a_, 1e-30));
+  double evl_ = 0.5 * (ut_ * EtaP - sigma);
+  double evr_ = 0.5 * (ut_ * EtaP + sigma);
+  double utla = dot(Ul, an), utra = dot(Ur, an);
+  double utl = utla - Us_n, utr = utra - Us_n;
+  double al2 = gamma * Rt * Tl, ar2 = gamma * Rt * Tr;
+  double sigmar = std::sqrt(std::max(utr * utr * EtaM * EtaM + 4. * Eta * ar2, 0.0));
+  double sigmal = std::sqrt(std::max(utl * utl * EtaM * EtaM + 4. * Eta * al2, 0.0));
+  double SL = std::min(evl_, .5 * (utl * EtaP - sigmal));
+  double SR = std::max(evr_, .5 * (utr * EtaP + sigmar));
+  double lmdot = rl * utl, rmdot = rr * utr;
+  double pl = pgl + pamb, pr = pgr + pamb;
+  double coef = 0.5 * area;
+  double AL = coef * ((SL > 0) ? (SR < 0 ? 1. : 2.) : (SR < 0 ? 0. : 1.));
+  double AR = coef * ((SR < 0) ? (SL > 0 ? 1. : 2.) : (SL > 0 ? 0. : 1.));
+  double AM = coef * ((SL > 0 || SR < 0) ? 0. : 1.);
+  F[0] = AL * lmdot + AR * rmdot;
+  F[1] = AL * lmdot * Ul.x + AR * rmdot * Ur.x + an.x * (AL * pgl + AR * pgr);
+  F[2] = AL * lmdot * Ul.y + AR * rmdot * Ur.y + an.y * (AL * pgl + AR * pgr);
+  F[3] = AL * lmdot * Ul.z + AR * rmdot * Ur.z + an.z * (AL * pgl + AR * pgr);
+  F[4] = AL * (lmdot * e0l + pl * utla) + AR * (rmdot * e0r + pr * utra);
+  F[0] -= AM * (SL * rl + SR * rr);
+  F[1] -= AM * (SL * rl * Ul.x + SR * rr * Ur.x);
+  F[2] -= AM * (SL * rl * Ul.y + SR * rr * Ur.y);
+  F[3] -= AM * (SL * rl * Ul.z + SR * rr * Ur.z);
+  F[4] -= AM * (SL * rl * e0l + SR * rr * e0r);
+  double SM = ((rr * utr * (SR - utr) - rl * utl * (SL - utl) + pgl - pgr) /
+               (rr * (SR - utr) - rl * (SL - utl)));
+  double rl_s = rl * (SL - utl) / (SL - SM);
+  double rr_s = rr * (SR - utr) / (SR - SM);
+  double pg_s = rl * (utl - SL) * (utl - SM) + pgl;
+  double p_s = pg_s + pamb;
+  double rul = ((SL - utl) * rl * Ul.x + (pg_s - pgl) * an.x) / (SL - SM);
+  double rvl = ((SL - utl) * rl * Ul.y + (pg_s - pgl) * an.y) / (SL - SM);
+  double rwl = ((SL - utl) * rl * Ul.z + (pg_s - pgl) * an.z) / (SL - SM);
+  double rur = ((SR - utr) * rr * Ur.x + (pg_s - pgr) * an.x) / (SR - SM);
+  double rvr = ((SR - utr) * rr * Ur.y + (pg_s - pgr) * an.y) / (SR - SM);
+  double rwr = ((SR - utr) * rr * Ur.z + (pg_s - pgr) * an.z) / (SR - SM);
+  double rel = ((SL - utl) * rl * e0l - pl * utl + p_s * SM) / (SL - SM);
+  double rer = ((SR - utr) * rr * e0r - pr * utr + p_s * SM) / (SR - SM);
+  double CR = SR - std::fabs(SM), CL = SL + std::fabs(SM);
+  F[0] += AM * (CR * rr_s + CL * rl_s);
+  F[1] += AM * (CR * rur + CL * rul);
+  F[2] += AM * (CR * rvr + CL * rvl);
+  F[3] += AM * (CR * rwr + CL * rwl);
+  F[4] += AM * (CR * rer + CL * rel);
+}
+
+// HLLE: no counterpart in the reference.  Two-wave HLL flux whose wave
+// speeds are hllc_flux's SL/SR (fluxInviscid.loci:173-204).
+void hlle_flux(double F[5], double pgl, double Tl, V3 Ul, double pgr, double Tr, V3 Ur,
+               V3 an, double area, double pamb, double Rt, double gamma, double Us_n,
+               double Eta) {
+  double gm1 = gamma - 1;
+  double rl = (pgl + pamb) / (Rt * Tl);
+  double rr = (pgr + pamb) / (Rt * Tr);
+  double h0l = Rt * Tl * gamma / gm1 + 0.5 * dot(Ul, Ul);
+  double h0r = Rt * Tr * gamma / gm1 + 0.5 * dot(Ur, Ur);
+  double srl = std::sqrt(rl), srr = std::sqrt(rr);
+  double rf = 1. / (srl + srr);
+  V3 U_ = (Ul * srl + Ur * srr) * rf;
+  double ut_ = dot(U_, an) - Us_n;
+  double h0_ = (h0l * srl + h0r * srr) * rf;
+  double a_ = std::sqrt(std::max(gm1 * (h0_ - 0.5 * dot(U_, U_)), 0.0));
+  double EtaP = Eta + 1., EtaM = Eta - 1.;
+  double sigma = std::sqrt(std::max(ut_ * ut_ * EtaM * EtaM + 4. * Eta * a_ * a_, 1e-30));
+  double utl = dot(Ul, an) - Us_n, utr = dot(Ur, an) - Us_n;
+  double al2 = gamma * Rt * Tl, ar2 = gamma * Rt * Tr;
+  double sigmar = std::sqrt(std::max(utr * utr * EtaM * EtaM + 4. * Eta * ar2, 0.0));
+  double sigmal = std::sqrt(std::max(utl * utl * EtaM * EtaM + 4. * Eta * al2, 0.0));
+  double SL = std::min(0.5 * (ut_ * EtaP - sigma), .5 * (utl * EtaP - sigmal));
+  double SR = std::max(0.5 * (ut_ * EtaP + sigma), .5 * (utr * EtaP + sigmar));
+  double fl[5], fr[5];
+  analytic_flux(fl, pgl, Tl, Ul, an, area, pamb, Rt, gamma, Us_n);
+  analytic_flux(fr, pgr, Tr, Ur, an, area, pamb, Rt, gamma, Us_n);
+  if (SL >= 0) {
+    for (int i = 0; i < 5; ++i) F[i] = fl[i];
+    return;
+  }
+  if (SR <= 0) {
+    for (int i = 0; i < 5; ++i) F[i] = fr[i];
+    return;
+  }
+  double e0l = h0l - Rt * Tl, e0r = h0r - Rt * Tr;
+  double ql[5] = {rl, rl * Ul.x, rl * Ul.y, rl * Ul.z, rl * e0l};
+  double qr[5] = {rr, rr * Ur.x, rr * Ur.y, rr * Ur.z, rr * e0r};
+  double rd = 1. / (SR - SL);
+  for (int i = 0; i < 5; ++i)
+    F[i] = (SR * fl[i] - SL * fr[i] + area * SL * SR * (qr[i] - ql[i])) * rd;
+}
+
+// The 5x5 matrix of the preconditioned Roe scheme, RoeJacobian in
+// fluxInviscid.loci:1019-1090.  roeCT_flux (:869-1014) applies the same
+// coefficients, with |eigenvalues|, to the primitive jumps.
+struct RoeCoef {
+  double ev1, rT, T7, T8, T9, T10, T11, T4s, rho, T1s;
+};
+RoeCoef roe_coef(double ev1, double ev2, double ev3, V3 U, double un, double a,
+                 double beta, double sigma, double gamma, double Rt, double rho, double h0,
+                 V3 n) {
+  const double BM = beta - 1.;
+  const double una = dot(U, n);
+  const double T1 = ev2 - ev3;
+  const double T2 = (ev2 + ev3 - 2 * ev1);
+  const double T3 = rho * (BM * BM * un * un - sigma * sigma) / (4. * sigma);
+  const double T4 = T2 * sigma + BM * T1 * un;
+  const double T5 = (T2 * sigma - BM * T1 * un) / (2. * sigma);
+  const double T6 = ((ev2 + ev3) * sigma - BM * T1 * un) / (2. * sigma);
+  const double gm1 = gamma - 1.0;
+  const double Cp = gamma * Rt / gm1;
+  const double rT = -gamma * Rt * rho / ((h0 - 0.5 * dot(U, U)) * gm1);
+  const double rbeta = 1. / beta;
+  const double ra2 = 1. / (a * a);
+  const double T7 = rbeta * T1 * T3 * ra2;
+  const double T8 = (((rbeta - 1) + gamma) * T6 - gm1 * T5) * ra2;
+  const double T9 = Cp * rho + h0 * rT;
+  const double x1 = gamma * h0 * T1 * T3 * ra2 * rbeta;
+  const double x2 = -rbeta * gm1 * T1 * T3 * T9 * ra2 / rT;
+  const double x3 = -T1 * T3 * rbeta;
+  const double x4 = .5 * rho * T4 * una / sigma;
+  const double T10 = (x1 + x2 + x3 + x4);
+  const double T11 = (rbeta * ra2 * h0 + (T9 - rho * rbeta * Cp) * ra2 * gm1 / rT - rbeta) * T6 -
+                     gm1 * ra2 * T9 * T5 / rT - una * T1 / sigma;
+  RoeCoef c;
+  c.ev1 = ev1;
+  c.rT = rT;
+  c.T7 = T7;
+  c.T8 = T8;
+  c.T9 = T9;
+  c.T10 = T10;
+  c.T11 = T11;
+  c.T4s = rho * T4 / (2. * sigma);
+  c.rho = rho;
+  c.T1s = T1 / sigma;
+  return c;
+}
+
+// RoeJacobian (fluxInviscid.loci:1019-1090): Fj += area*K, accumulated in TB.
+template <class TB>
+void roe_matrix_accum(TB Fj[25], const RoeCoef& c, V3 U, V3 n, double area) {
+  const int Ti = 0, Pi = 4, mi = 1, ei = 4;
+  double u[3] = {U.x, U.y, U.z}, nn[3] = {n.x, n.y, n.z};
+#define FJ(i, j) Fj[(i)*5 + (j)]
+  FJ(0, Ti) += area * c.ev1 * c.rT;
+  for (int k = 0; k < 3; ++k) FJ(0, mi + k) += area * nn[k] * c.T7;
+  FJ(0, Pi) += area * c.T8;
+  for (int k = 0; k < 3; ++k) FJ(mi + k, Ti) += area * c.ev1 * c.rT * u[k];
+  for (int r = 0; r < 3; ++r)
+    for (int k = 0; k < 3; ++k) {
+      double v = nn[k] * (c.T7 * u[r] + nn[r] * c.T4s);
+      if (r == k) v += c.ev1 * c.rho;
+      FJ(mi + r, mi + k) += area * v;
+    }
+  for (int r = 0; r < 3; ++r) FJ(mi + r, Pi) += area * (c.T8 * u[r] - nn[r] * c.T1s);
+  FJ(ei, Ti) += area * c.ev1 * c.T9;
+  for (int k = 0; k < 3; ++k) FJ(ei, mi + k) += area * (nn[k] * c.T10 + c.ev1 * c.rho * u[k]);
+  FJ(ei, Pi) += area * c.T11;
+#undef FJ
+}
+
+struct RoeState {
+  double rl, rr, re0l, re0r, pl, pr, r_, srl, srr, h0_, h_, ut_, uta_, a_, sigma, Eta;
+  V3 U_;
+};
+// Roe averages shared by roeCT_flux (:875-915) and roeCT_jacobian (:1098-1139).
+RoeState roe_state(double pgl, double Tl, V3 Ul, double pgr, double Tr, V3 Ur, V3 an,
+                   double pamb, double Rt, double gamma, double Us_n, double Eta) {
+  RoeState s;
+  double gm1 = gamma - 1.;
+  s.pl = pgl + pamb;
+  s.pr = pgr + pamb;
+  s.rl = s.pl / (Rt * Tl);
+  s.rr = s.pr / (Rt * Tr);
+  s.re0l = s.rl * (Rt * Tl / gm1 + 0.5 * dot(Ul, Ul));
+  s.re0r = s.rr * (Rt * Tr / gm1 + 0.5 * dot(Ur, Ur));
+  double h0l = (s.re0l + s.pl) / s.rl;
+  double h0r = (s.re0r + s.pr) / s.rr;
+  s.r_ = std::sqrt(s.rl * s.rr);
+  s.srl = std::sqrt(s.rl);
+  s.srr = std::sqrt(s.rr);
+  double rf = 1. / (s.srl + s.srr);
+  s.U_ = (Ul * s.srl + Ur * s.srr) * rf;
+  s.ut_ = dot(s.U_, an) - Us_n;
+  s.uta_ = dot(s.U_, an);
+  double q2_ = dot(s.U_, s.U_);
+  s.h0_ = (h0l * s.srl + h0r * s.srr) * rf;
+  s.h_ = s.h0_ - 0.5 * q2_;
+  if (std::fabs(s.pl - s.pr) / (s.pl + s.pr + 1e-33) > .1) Eta = 1.;
+  s.Eta = Eta;
+  double af2 = std::max(gm1 * s.h_, 1e-30);
+  s.a_ = std::sqrt(af2);
+  double EtaM = Eta - 1.;
+  s.sigma = std::sqrt(s.ut_ * s.ut_ * EtaM * EtaM + 4. * Eta * s.a_ * s.a_);
+  return s;
+}
+
+// roeCT_flux, fluxInviscid.loci:869-1014 (with the Harten-Hyman fix :940-962).
+void roe_flux(double F[5], double pgl, double Tl, V3 Ul, double pgr, double Tr, V3 Ur, V3 an,
+              double area, double pamb, double Rt, double gamma, double Us_n, double Eta) {
+  RoeState s = roe_state(pgl, Tl, Ul, pgr, Tr, Ur, an, pamb, Rt, gamma, Us_n, Eta);
+  Eta = s.Eta;
+  const double EtaP = Eta + 1., EtaM = Eta - 1.;
+  const double ut_ = s.ut_, sigma = s.sigma;
+  double ev1 = std::fabs(ut_);
+  double ev2 = std::fabs(ut_ * EtaP - sigma) / 2.;
+  double ev3 = std::fabs(ut_ * EtaP + sigma) / 2.;
+  const double al2 = gamma * Rt * Tl, ar2 = gamma * Rt * Tr;
+  const double utla = dot(Ul, an), utra = dot(Ur, an);
+  const double utl = utla - Us_n, utr = utra - Us_n;
+  double sigmal = std::sqrt(utl * utl * EtaM * EtaM + 4. * Eta * al2);
+  double sigmar = std::sqrt(utr * utr * EtaM * EtaM + 4. * Eta * ar2);
+  const double e2l = (utl * EtaP - sigmal) / 2., e2r = (utr * EtaP - sigmar) / 2.;
+  const double e3l = (utl * EtaP + sigmal) / 2., e3r = (utr * EtaP + sigmar) / 2.;
+  const double ev2s = (ut_ * EtaP - sigma) / 2., ev3s = (ut_ * EtaP + sigma) / 2.;
+  const double eps2 = std::max(0.0, std::max(ev2s - e2l, e2r - ev2s));
+  const double eps3 = std::max(0.0, std::max(ev3s - e3l, e3r - ev3s));
+  ev2 = ev2 < eps2 ? 0.5 * ((ev2s * ev2s) / eps2 + eps2) : ev2;
+  ev3 = ev3 < eps3 ? 0.5 * ((ev3s * ev3s) / eps3 + eps3) : ev3;
+  // dissipation, written with the association of :985-1004
+  const V3 U_ = s.U_;
+  const double r_ = s.r_, h0_ = s.h0_, uta_ = s.uta_;
+  const V3 Uj = Ur - Ul;
+  const double utj = dot(Uj, an);
+  const double pj = pgr - pgl, Tj = Tr - Tl;
+  const double BM = EtaM;
+  const double T1 = ev2 - ev3;
+  const double T2 = (ev2 + ev3 - 2 * ev1);
+  const double T3 = r_ * (BM * BM * ut_ * ut_ - sigma * sigma) / (4. * sigma);
+  const double T4 = T2 * sigma + BM * T1 * ut_;
+  const double T5 = (T2 * sigma - BM * T1 * ut_) / (2. * sigma);
+  const double T6 = ((ev2 + ev3) * sigma - BM * T1 * ut_) / (2. * sigma);
+  const double gm1 = gamma - 1.;
+  const double Cp = gamma * Rt / gm1;
+  const double rT_ = -gamma * Rt * r_ / (s.h_ * gm1);
+  const double rbeta = 1. / Eta;
+  const double ra2 = 1. / (s.a_ * s.a_);
+  const double T7 = rbeta * T1 * T3 * ra2;
+  const double T8 = (((rbeta - 1) + gamma) * T6 - gm1 * T5) * ra2;
+  const double T9 = Cp * r_ + h0_ * rT_;
+  const double x1 = gamma * h0_ * T1 * T3 * ra2 * rbeta;
+  const double x2 = -rbeta * gm1 * T1 * T3 * T9 * ra2 / rT_;
+  const double x3 = -T1 * T3 * rbeta;
+  const double x4 = .5 * r_ * T4 * uta_ / sigma;
+  const double T10 = (x1 + x2 + x3 + x4);
+  const double T11 = (rbeta * ra2 * h0_ + (T9 - r_ * rbeta * Cp) * ra2 * gm1 / rT_ - rbeta) * T6 -
+                     gm1 * ra2 * T9 * T5 / rT_ - uta_ * T1 / sigma;
+  double d[5];
+  d[0] = pj * T8 + utj * T7 + ev1 * Tj * rT_;
+  d[1] = U_.x * T7 * utj + ev1 * (U_.x * Tj * rT_ + r_ * Uj.x) + pj * (T8 * U_.x - an.x * T1 / sigma) +
+         an.x * r_ * T4 * utj / (2. * sigma);
+  d[2] = U_.y * T7 * utj + ev1 * (U_.y * Tj * rT_ + r_ * Uj.y) + pj * (T8 * U_.y - an.y * T1 / sigma) +
+         an.y * r_ * T4 * utj / (2. * sigma);
+  d[3] = U_.z * T7 * utj + ev1 * (U_.z * Tj * rT_ + r_ * Uj.z) + pj * (T8 * U_.z - an.z * T1 / sigma) +
+         an.z * r_ * T4 * utj / (2. * sigma);
+  d[4] = pj * T11 + T10 * utj + ev1 * (T9 * Tj + r_ * dot(U_, Uj));
+  const double Ah = 0.5 * area;
+  F[0] = Ah * (s.rl * utl + s.rr * utr - d[0]);
+  F[1] = Ah * (Ul.x * s.rl * utl + Ur.x * s.rr * utr + an.x * (pgl + pgr) - d[1]);
+  F[2] = Ah * (Ul.y * s.rl * utl + Ur.y * s.rr * utr + an.y * (pgl + pgr) - d[2]);
+  F[3] = Ah * (Ul.z * s.rl * utl + Ur.z * s.rr * utr + an.z * (pgl + pgr) - d[3]);
+  F[4] = Ah * ((s.re0l * utl + s.pl * utla) + (s.re0r * utr + s.pr * utra) - d[4]);
+}
+
+// roeCT_jacobian, fluxInviscid.loci:1092-1168 (eigenvalue smoothing :1141-1164).
+template <class TB>
+void roe_jacobian(TB Fj[25], double pgl, double Tl, V3 Ul, double pgr, double Tr, V3 Ur,
+                  V3 an, double area, double pamb, double Rt, double gamma, double Us_n,
+                  double Eta, int dir) {
+  RoeState s = roe_state(pgl, Tl, Ul, pgr, Tr, Ur, an, pamb, Rt, gamma, Us_n, Eta);
+  Eta = s.Eta;
+  const double EtaP = Eta + 1.;
+  double ev1 = s.ut_;
+  double ev2 = (s.ut_ * EtaP - s.sigma) / 2.;
+  double ev3 = (s.ut_ * EtaP + s.sigma) / 2.;
+  double d = (dir < 0) ? -1 : 1;
+  const double mxv = std::max(ev1, std::max(ev2, ev3));
+  const double mnv = std::min(ev1, std::min(ev2, ev3));
+  const double eps = 0.02 * (mxv - mnv);
+  const double eps2 = eps * eps;
+  ev1 = .5 * (ev1 + d * std::sqrt(ev1 * ev1 + eps2));
+  ev2 = .5 * (ev2 + d * std::sqrt(ev2 * ev2 + eps2));
+  ev3 = .5 * (ev3 + d * std::sqrt(ev3 * ev3 + eps2));
+  RoeCoef c = roe_coef(ev1, ev2, ev3, s.U_, s.ut_, s.a_, Eta, s.sigma, gamma, Rt, s.r_, s.h0_, an);
+  roe_matrix_accum<TB>(Fj, c, s.U_, an, area);
+}
+
+void riemann_flux(int kind, double F[5], double pgl, double Tl, V3 Ul, double pgr, double Tr,
+                  V3 Ur, V3 an, double area, double pamb, double Rt, double gamma, double Us_n,
+                  double Eta) {
+  if (kind == FPSI_FLUX_ROE)
+    roe_flux(F, pgl, Tl, Ul, pgr, Tr, Ur, an, area, pamb, Rt, gamma, Us_n, Eta);
+  else if (kind == FPSI_FLUX_HLLE)
+    hlle_flux(F, pgl, Tl, Ul, pgr, Tr, Ur, an, area, pamb, Rt, gamma, Us_n, Eta);
+  else
+    hllc_flux(F, pgl, Tl, Ul, pgr, Tr, Ur, an, area, pamb, Rt, gamma, Us_n, Eta);
+}
+
+// cv_inflow / cv_outflow, bcTools.h:25-81.
+void cv_inflow(double& pgb, double& Tb, V3& ub, double pgi, double Ti, V3 ui, double pg0,
+               double T0, V3 u0, V3 n, double us_n, double pamb, double gamma, double Rt,
+               double Beta) {
+  (void)Ti;
+  const double uit = dot(ui, n) - us_n, u0t = dot(u0, n) - us_n;
+  const double a0 = std::sqrt(gamma * Rt * T0);
+  const double r0 = (pg0 + pamb) / (Rt * T0);
+  const double MinP = 0.1 * (pg0 + pamb) - pamb;
+  const double BetaM = 0.5 * (1.0 - Beta);
+  const double uitBeta = uit * (1. - Beta);
+  const double sigma = std::sqrt(uitBeta * uitBeta + 4. * Beta * a0 * a0);
+  pgb = 0.5 * (pg0 + pgi - 0.5 * r0 * sigma * (u0t - uit)) -
+        ((pgi - pg0) + r0 * (uit - u0t) * uit * BetaM) * uit * BetaM / (2. * sigma);
+  pgb = std::max(pgb, MinP);
+  ub = u0 + 2. * n * (pgb - pg0) * (1.0 / (r0 * (sigma + uit * BetaM)));
+  double rhob = r0 + (pgb - pg0) * (sigma - uit * BetaM) / (Beta * a0 * a0 * (sigma + uit * BetaM));
+  Tb = (pgb + pamb) / (Rt * rhob);
+}
+void cv_outflow(double& pgb, double& Tb, V3& ub, double pgi, double Ti, V3 ui, double pg0,
+                double T0, V3 u0, V3 n, double us_n, double pamb, double gamma, double Rt,
+                double Beta) {
+  (void)Ti;
+  const double uit = dot(ui, n) - us_n, u0t = dot(u0, n) - us_n;
+  const double a0 = std::sqrt(gamma * Rt * T0);
+  const double r0 = (pg0 + pamb) / (Rt * T0);
+  const double MinP = 0.1 * (pgi + pamb) - pamb;
+  const double BetaM = 0.5 * (1.0 - Beta);
+  const double uitBeta = uit * (1. - Beta);
+  const double sigma = std::sqrt(uitBeta * uitBeta + 4. * Beta * a0 * a0);
+  pgb = .5 * (pgi + pg0 - 0.5 * r0 * sigma * (u0t - uit)) +
+        ((pgi - pg0) + r0 * (uit - u0t) * uit * BetaM) * uit * BetaM / (2. * sigma);
+  pgb = std::max(pgb, MinP);
+  ub = ui + 2. * n * (pgi - pgb) * (1.0 / (r0 * (sigma + uit * BetaM)));
+  const double rhob = r0 + (pgb - pgi) * (sigma - uit * BetaM) / (Beta * a0 * a0 * (sigma + uit * BetaM));
+  Tb = (pgb + pamb) / (Rt * rhob);
+}
+
+// ---------------------------------------------------------------------------
+// 5x5 LU with partial pivoting (textbook Doolittle; Loci's decompose_lu_pivot
+// is not vendored) and the solve used by linearSolverSGS.loci:43-69.
+// ---------------------------------------------------------------------------
+template <class TB>
+bool lu5(TB A[25], int piv[5]) {
+  bool ok = true;
+  for (int k = 0; k < 5; ++k) {
+    int p = k;
+    TB best = std::fabs(A[k * 5 + k]);
+    for (int i = k + 1; i < 5; ++i)
+      if (std::fabs(A[i * 5 + k]) > best) {
+        best = std::fabs(A[i * 5 + k]);
+        p = i;
+      }
+    piv[k] = p;
+    if (p != k)
+      for (int j = 0; j < 5; ++j) std::swap(A[k * 5 + j], A[p * 5 + j]);
+    if (A[k * 5 + k] == TB(0)) {
+      ok = false;
+      continue;
+    }
+    for (int i = k + 1; i < 5; ++i) {
+      A[i * 5 + k] /= A[k * 5 + k];
+      TB l = A[i * 5 + k];
+      for (int j = k + 1; j < 5; ++j) A[i * 5 + j] -= l * A[k * 5 + j];
+    }
+  }
+  return ok;
+}
+template <class TB, class TX>
+void lu5_solve(const TB A[25], const int piv[5], const TX b[5], TX x[5]) {
+  TX y[5];
+  for (int i = 0; i < 5; ++i) y[i] = b[i];
+  for (int k = 0; k < 5; ++k)
+    if (piv[k] != k) std::swap(y[k], y[piv[k]]);
+  for (int i = 1; i < 5; ++i)
+    for (int j = 0; j < i; ++j) y[i] -= TX(A[i * 5 + j]) * y[j];
+  for (int i = 4; i >= 0; --i) {
+    for (int j = i + 1; j < 5; ++j) y[i] -= TX(A[i * 5 + j]) * y[j];
+    y[i] /= TX(A[i * 5 + i]);
+  }
+  for (int i = 0; i < 5; ++i) x[i] = y[i];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Mesh-level oracle
+// ---------------------------------------------------------------------------
+struct orc_ctx {
+  fpsi_params P;
+  int64_t nc = 0, nf = 0;
+  std::vector<int32_t> cl, cr;
+  std::vector<fpsi_bc> bcs;
+  // geometry
+  std::vector<double> vol, cc;          // nc, nc*3
+  std::vector<double> an, area, fc;     // nf*3, nf, nf*3
+  std::vector<double> rL, rR;           // nf*3: x_f - x_cl, x_f - x_cr(image)
+  std::vector<double> Minv;             // nc*6 LSQ inverse (xx,xy,xz,yy,yz,zz)
+  double vol_tot = 0;
+  // cell -> faces (upper = faces with cl==c, lower = cr==c, bnd = boundary)
+  std::vector<int64_t> up_off, lo_off, bd_off;
+  std::vector<int64_t> up, lo, bd;
+  // state & results
+  std::vector<double> T, pg, u;         // nc, nc, nc*3
+  std::vector<double> qb;               // nbf... stored per face (nf*5): boundary face state
+  std::vector<double> grad, phi;        // nc*15, nc*5
+  std::vector<double> F, maxev;         // nf*5, nf
+  std::vector<double> src, dtau;        // nc*5, nc
+  bool have_resid = false, have_asm = false, have_dq = false;
+  // blocks (both precisions kept; the active one is selected by P.precision)
+  std::vector<float> fjp32, fjm32, D32, LU32, B32;
+  std::vector<double> fjp64, fjm64, D64, LU64, B64;
+  std::vector<int> piv;                 // nc*5
+  std::vector<double> dq;               // nc*5 (FP64 copy of the result)
+};
+
+static int g_threads = 1;
+
+extern "C" int orc_set_threads(int n) {
+  g_threads = n < 1 ? 1 : n;
+#ifdef _OPENMP
+  omp_set_num_threads(g_threads);
+#endif
+  return g_threads;
+}
+
+static inline V3 v3(const double* p) { return mk(p[0], p[1], p[2]); }
+
+// Face and cell geometry (Loci FVM's area, facecenter, vol, cellcenter;
+// restated: fan triangulation about the node average, divergence theorem).
+static void compute_geometry(orc_ctx* o, const fpsi_mesh* m) {
+  const int64_t nc = m->ncells, nf = m->nfaces;
+  o->an.assign(nf * 3, 0);
+  o->area.assign(nf, 0);
+  o->fc.assign(nf * 3, 0);
+  std::vector<double> Avec(nf * 3);
+  for (int64_t f = 0; f < nf; ++f) {
+    int64_t b = m->face_off[f], e = m->face_off[f + 1];
+    int k = int(e - b);
+    V3 xa = mk(0, 0, 0);
+    for (int64_t i = b; i < e; ++i) xa = xa + v3(m->xyz + 3 * m->face_nodes[i]);
+    xa = (1.0 / k) * xa;
+    V3 A = mk(0, 0, 0), C = mk(0, 0, 0);
+    double W = 0;
+    for (int i = 0; i < k; ++i) {
+      V3 p0 = v3(m->xyz + 3 * m->face_nodes[b + i]);
+      V3 p1 = v3(m->xyz + 3 * m->face_nodes[b + (i + 1) % k]);
+      V3 a = 0.5 * cross(p0 - xa, p1 - xa);
+      A = A + a;
+      double w = norm(a);
+      C = C + (w / 3.0) * (xa + p0 + p1);
+      W += w;
+    }
+    C = (1.0 / W) * C;
+    double s = norm(A);
+    o->area[f] = s;
+    o->an[3 * f] = A.x / s;
+    o->an[3 * f + 1] = A.y / s;
+    o->an[3 * f + 2] = A.z / s;
+    o->fc[3 * f] = C.x;
+    o->fc[3 * f + 1] = C.y;
+    o->fc[3 * f + 2] = C.z;
+    Avec[3 * f] = A.x;
+    Avec[3 * f + 1] = A.y;
+    Avec[3 * f + 2] = A.z;
+  }
+  // reference point per cell: mean of its face centres (in its own frame)
+  std::vector<double> xr(nc * 3, 0);
+  std::vector<int> cnt(nc, 0);
+  for (int64_t f = 0; f < nf; ++f) {
+    V3 x = v3(&o->fc[3 * f]);
+    int c = m->cl[f];
+    xr[3 * c] += x.x, xr[3 * c + 1] += x.y, xr[3 * c + 2] += x.z, cnt[c]++;
+    if (m->cr[f] >= 0) {
+      int d = m->cr[f];
+      V3 s = m->pshift ? v3(m->pshift + 3 * f) : mk(0, 0, 0);
+      V3 y = x - s;
+      xr[3 * d] += y.x, xr[3 * d + 1] += y.y, xr[3 * d + 2] += y.z, cnt[d]++;
+    }
+  }
+  for (int64_t c = 0; c < nc; ++c)
+    for (int i = 0; i < 3; ++i) xr[3 * c + i] /= cnt[c];
+  o->vol.assign(nc, 0);
+  o->cc.assign(nc * 3, 0);
+  // pyramids on the fan triangles of every face, seen from each adjacent cell
+  for (int64_t f = 0; f < nf; ++f) {
+    int64_t b = m->face_off[f], e = m->face_off[f + 1];
+    int k = int(e - b);
+    V3 xa = mk(0, 0, 0);
+    for (int64_t i = b; i < e; ++i) xa = xa + v3(m->xyz + 3 * m->face_nodes[i]);
+    xa = (1.0 / k) * xa;
+    for (int side = 0; side < 2; ++side) {
+      int c = side == 0 ? m->cl[f] : m->cr[f];
+      if (c < 0) continue;
+      V3 s = (side == 1 && m->pshift) ? v3(m->pshift + 3 * f) : mk(0, 0, 0);
+      double sg = side == 0 ? 1.0 : -1.0;
+      V3 x0 = v3(&xr[3 * c]);
+      for (int i = 0; i < k; ++i) {
+        V3 p0 = v3(m->xyz + 3 * m->face_nodes[b + i]) - s;
+        V3 p1 = v3(m->xyz + 3 * m->face_nodes[b + (i + 1) % k]) - s;
+        V3 pa = xa - s;
+        double v = sg * dot(pa - x0, cross(p0 - x0, p1 - x0)) / 6.0;
+        V3 cen = 0.25 * (x0 + pa + p0 + p1);
+        o->vol[c] += v;
+        o->cc[3 * c] += v * cen.x;
+        o->cc[3 * c + 1] += v * cen.y;
+        o->cc[3 * c + 2] += v * cen.z;
+      }
+    }
+  }
+  for (int64_t c = 0; c < nc; ++c)
+    for (int i = 0; i < 3; ++i) o->cc[3 * c + i] /= o->vol[c];
+  o->vol_tot = 0;
+  for (int64_t c = 0; c < nc; ++c) o->vol_tot += o->vol[c];
+  o->rL.assign(nf * 3, 0);
+  o->rR.assign(nf * 3, 0);
+  for (int64_t f = 0; f < nf; ++f) {
+    V3 x = v3(&o->fc[3 * f]);
+    V3 a = x - v3(&o->cc[3 * m->cl[f]]);
+    o->rL[3 * f] = a.x, o->rL[3 * f + 1] = a.y, o->rL[3 * f + 2] = a.z;
+    if (m->cr[f] >= 0) {
+      V3 s = m->pshift ? v3(m->pshift + 3 * f) : mk(0, 0, 0);
+      V3 bb = x - (v3(&o->cc[3 * m->cr[f]]) + s);
+      o->rR[3 * f] = bb.x, o->rR[3 * f + 1] = bb.y, o->rR[3 * f + 2] = bb.z;
+    }
+  }
+}
+
+extern "C" int orc_create(orc_ctx** out, const fpsi_mesh* m, const fpsi_params* p) {
+  if (!out || !m || !p) return FPSI_E_INVALID;
+  orc_ctx* o = new orc_ctx();
+  o->P = *p;
+  o->nc = m->ncells;
+  o->nf = m->nfaces;
+  o->cl.assign(m->cl, m->cl + m->nfaces);
+  o->cr.assign(m->cr, m->cr + m->nfaces);
+  o->bcs.assign(m->bcs, m->bcs + m->nbc);
+  compute_geometry(o, m);
+  const int64_t nc = o->nc, nf = o->nf;
+  // cell -> face lists in face order (the order Loci's upper/lower maps keep)
+  o->up_off.assign(nc + 1, 0);
+  o->lo_off.assign(nc + 1, 0);
+  o->bd_off.assign(nc + 1, 0);
+  for (int64_t f = 0; f < nf; ++f) {
+    if (o->cr[f] >= 0) {
+      o->up_off[o->cl[f] + 1]++;
+      o->lo_off[o->cr[f] + 1]++;
+    } else {
+      o->bd_off[o->cl[f] + 1]++;
+    }
+  }
+  for (int64_t c = 0; c < nc; ++c) {
+    o->up_off[c + 1] += o->up_off[c];
+    o->lo_off[c + 1] += o->lo_off[c];
+    o->bd_off[c + 1] += o->bd_off[c];
+  }
+  o->up.resize(o->up_off[nc]);
+  o->lo.resize(o->lo_off[nc]);
+  o->bd.resize(o->bd_off[nc]);
+  {
+    std::vector<int64_t> pu(o->up_off.begin(), o->up_off.end() - 1),
+        pl(o->lo_off.begin(), o->lo_off.end() - 1), pb(o->bd_off.begin(), o->bd_off.end() - 1);
+    for (int64_t f = 0; f < nf; ++f) {
+      if (o->cr[f] >= 0) {
+        o->up[pu[o->cl[f]]++] = f;
+        o->lo[pl[o->cr[f]]++] = f;
+      } else {
+        o->bd[pb[o->cl[f]]++] = f;
+      }
+    }
+  }
+  // LSQ normal matrices M = sum d d^T over face neighbours (boundary: face centre)
+  o->Minv.assign(nc * 6, 0);
+  for (int64_t c = 0; c < nc; ++c) {
+    double M[6] = {0, 0, 0, 0, 0, 0};
+    auto add = [&](V3 d) {
+      M[0] += d.x * d.x, M[1] += d.x * d.y, M[2] += d.x * d.z;
+      M[3] += d.y * d.y, M[4] += d.y * d.z, M[5] += d.z * d.z;
+    };
+    for (int64_t k = o->up_off[c]; k < o->up_off[c + 1]; ++k) {
+      int64_t f = o->up[k];
+      add(v3(&o->rL[3 * f]) - v3(&o->rR[3 * f]));
+    }
+    for (int64_t k = o->lo_off[c]; k < o->lo_off[c + 1]; ++k) {
+      int64_t f = o->lo[k];
+      add(v3(&o->rR[3 * f]) - v3(&o->rL[3 * f]));
+    }
+    for (int64_t k = o->bd_off[c]; k < o->bd_off[c + 1]; ++k) add(v3(&o->rL[3 * o->bd[k]]));
+    double a = M[0], b = M[1], cc = M[2], d = M[3], e = M[4], f = M[5];
+    double A00 = d * f - e * e, A01 = cc * e - b * f, A02 = b * e - cc * d;
+    double A11 = a * f - cc * cc, A12 = b * cc - a * e, A22 = a * d - b * b;
+    double det = a * A00 + b * A01 + cc * A02;
+    double r = 1.0 / det;
+    double* mi = &o->Minv[6 * c];
+    mi[0] = A00 * r, mi[1] = A01 * r, mi[2] = A02 * r;
+    mi[3] = A11 * r, mi[4] = A12 * r, mi[5] = A22 * r;
+  }
+  o->T.assign(nc, 0);
+  o->pg.assign(nc, 0);
+  o->u.assign(nc * 3, 0);
+  *out = o;
+  return FPSI_OK;
+}
+
+extern "C" void orc_destroy(orc_ctx* o) { delete o; }
+
+extern "C" int orc_set_params(orc_ctx* o, const fpsi_params* p) {
+  o->P = *p;
+  o->have_asm = false;
+  return FPSI_OK;
+}
+
+extern "C" int orc_get_geometry(orc_ctx* o, double* vol, double* cellcenter, double* face_an,
+                                double* face_area, double* facecenter) {
+  if (vol) std::memcpy(vol, o->vol.data(), sizeof(double) * o->nc);
+  if (cellcenter) std::memcpy(cellcenter, o->cc.data(), sizeof(double) * o->nc * 3);
+  if (face_an)
+    for (int64_t f = 0; f < o->nf; ++f)
+      for (int i = 0; i < 3; ++i) face_an[3 * f + i] = o->an[3 * f + i] * o->area[f];
+  if (face_area) std::memcpy(face_area, o->area.data(), sizeof(double) * o->nf);
+  if (facecenter) std::memcpy(facecenter, o->fc.data(), sizeof(double) * o->nf * 3);
+  return FPSI_OK;
+}
+
+extern "C" int orc_set_state(orc_ctx* o, const double* T, const double* pg, const double* u) {
+  std::memcpy(o->T.data(), T, sizeof(double) * o->nc);
+  std::memcpy(o->pg.data(), pg, sizeof(double) * o->nc);
+  std::memcpy(o->u.data(), u, sizeof(double) * o->nc * 3);
+  o->have_resid = o->have_asm = o->have_dq = false;
+  return FPSI_OK;
+}
+extern "C" int orc_get_state(orc_ctx* o, double* T, double* pg, double* u) {
+  std::memcpy(T, o->T.data(), sizeof(double) * o->nc);
+  std::memcpy(pg, o->pg.data(), sizeof(double) * o->nc);
+  std::memcpy(u, o->u.data(), sizeof(double) * o->nc * 3);
+  return FPSI_OK;
+}
+
+// boundary face state (gagePressure_f, temperature_f, u_f) from the cell
+// centre state: farfield bcInflow.loci:311-344, supersonicInflow :270-278,
+// extrapolate bcOutflow.loci:84-95, supersonicOutflow :127-142, reflecting
+// (mirror of the normal velocity) bcImpermeable.loci:48-140.
+static void bc_face_state(const orc_ctx* o, int64_t f, double q[5]) {
+  const fpsi_params& P = o->P;
+  int c = o->cl[f];
+  const fpsi_bc& bc = o->bcs[-o->cr[f] - 1];
+  V3 n = v3(&o->an[3 * f]);
+  double Ti = o->T[c], pgi = o->pg[c];
+  V3 ui = v3(&o->u[3 * c]);
+  V3 u0 = v3(bc.u);
+  double pgb = pgi, Tb = Ti;
+  V3 ub = ui;
+  const double us_n = 0, Eta = 1.0;
+  switch (bc.kind) {
+    case FPSI_BC_FARFIELD: {
+      double uit = dot(ui, n) - us_n;
+      double ai = std::sqrt(P.gamma * P.Rtilde * Ti);
+      double a0 = std::sqrt(P.gamma * P.Rtilde * bc.T);
+      if (uit > 0) {
+        if (uit > ai) {
+          pgb = pgi, Tb = Ti, ub = ui;
+        } else {
+          cv_outflow(pgb, Tb, ub, pgi, Ti, ui, bc.pg, bc.T, u0, n, us_n, P.Pambient, P.gamma,
+                     P.Rtilde, Eta);
+        }
+      } else {
+        if (-uit > a0) {
+          pgb = bc.pg, Tb = bc.T, ub = u0;
+        } else {
+          cv_inflow(pgb, Tb, ub, pgi, Ti, ui, bc.pg, bc.T, u0, n, us_n, P.Pambient, P.gamma,
+                    P.Rtilde, Eta);
+        }
+      }
+      break;
+    }
+    case FPSI_BC_SUPERSONIC_INFLOW:
+      pgb = bc.pg, Tb = bc.T, ub = u0;
+      break;
+    case FPSI_BC_SUPERSONIC_OUTFLOW: {
+      double ai = std::sqrt(P.gamma * P.Rtilde * Ti);
+      double ut = dot(n, ui) - us_n;
+      pgb = pgi;
+      if (ut < ai) pgb -= (pgi + P.Pambient) * .1;
+      Tb = Ti, ub = ui;
+      break;
+    }
+    case FPSI_BC_REFLECTING: {
+      double un = dot(ui, n);
+      ub = ui - 2.0 * un * n;
+      break;
+    }
+    default:  // extrapolate
+      break;
+  }
+  q[0] = Tb, q[1] = ub.x, q[2] = ub.y, q[3] = ub.z, q[4] = pgb;
+}
+
+static inline void cell_q(const orc_ctx* o, int64_t c, double q[5]) {
+  q[0] = o->T[c], q[1] = o->u[3 * c], q[2] = o->u[3 * c + 1], q[3] = o->u[3 * c + 2],
+  q[4] = o->pg[c];
+}
+
+// Least-squares cell gradients (Loci FVM grads/gradv3d; method named in
+// guide/inviscidFlux.tex:234-236) and per-variable limiters (Loci FVM
+// limiters/limiterv3d; options guide/guide.tex:495-518).
+static void gradients_and_limiters(orc_ctx* o) {
+  const int64_t nc = o->nc;
+  const int lim = o->P.limiter;
+  const double Kl = o->P.Kl;
+  o->grad.assign(nc * 15, 0);
+  o->phi.assign(nc * 5, 0);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < nc; ++c) {
+    double qc[5];
+    cell_q(o, c, qc);
+    double b[15] = {0};
+    double qmax[5], qmin[5];
+    for (int k = 0; k < 5; ++k) qmax[k] = qmin[k] = qc[k];
+    auto nb = [&](V3 d, const double* qn) {
+      for (int k = 0; k < 5; ++k) {
+        double dq = qn[k] - qc[k];
+        b[3 * k] += d.x * dq, b[3 * k + 1] += d.y * dq, b[3 * k + 2] += d.z * dq;
+        qmax[k] = std::max(qmax[k], qn[k]);
+        qmin[k] = std::min(qmin[k], qn[k]);
+      }
+    };
+    for (int64_t k = o->up_off[c]; k < o->up_off[c + 1]; ++k) {
+      int64_t f = o->up[k];
+      double qn[5];
+      cell_q(o, o->cr[f], qn);
+      nb(v3(&o->rL[3 * f]) - v3(&o->rR[3 * f]), qn);
+    }
+    for (int64_t k = o->lo_off[c]; k < o->lo_off[c + 1]; ++k) {
+      int64_t f = o->lo[k];
+      double qn[5];
+      cell_q(o, o->cl[f], qn);
+      nb(v3(&o->rR[3 * f]) - v3(&o->rL[3 * f]), qn);
+    }
+    for (int64_t k = o->bd_off[c]; k < o->bd_off[c + 1]; ++k) {
+      int64_t f = o->bd[k];
+      nb(v3(&o->rL[3 * f]), &o->qb[5 * f]);
+    }
+    const double* mi = &o->Minv[6 * c];
+    double* g = &o->grad[15 * c];
+    for (int k = 0; k < 5; ++k) {
+      double bx = b[3 * k], by = b[3 * k + 1], bz = b[3 * k + 2];
+      g[3 * k] = mi[0] * bx + mi[1] * by + mi[2] * bz;
+      g[3 * k + 1] = mi[1] * bx + mi[3] * by + mi[4] * bz;
+      g[3 * k + 2] = mi[2] * bx + mi[4] * by + mi[5] * bz;
+    }
+    double* ph = &o->phi[5 * c];
+    if (lim == FPSI_LIMITER_NONE) {
+      for (int k = 0; k < 5; ++k) ph[k] = 1.0;
+      continue;
+    }
+    if (lim == FPSI_LIMITER_ZERO) {
+      for (int k = 0; k < 5; ++k) ph[k] = 0.0;
+      continue;
+    }
+    const double h = std::cbrt(o->vol[c]);
+    const double eps2 = (Kl * h) * (Kl * h) * (Kl * h);
+    for (int k = 0; k < 5; ++k) ph[k] = 1.0;
+    auto face = [&](V3 r) {
+      for (int k = 0; k < 5; ++k) {
+        double d2 = g[3 * k] * r.x + g[3 * k + 1] * r.y + g[3 * k + 2] * r.z;
+        double p = 1.0;
+        if (d2 != 0.0) {
+          double d1 = d2 > 0 ? qmax[k] - qc[k] : qmin[k] - qc[k];
+          if (lim == FPSI_LIMITER_BARTH) {
+            p = std::min(1.0, d1 / d2);
+          } else {
+            double num = (d1 * d1 + eps2) + 2.0 * d2 * d1;
+            double den = d1 * d1 + 2.0 * d2 * d2 + d1 * d2 + eps2;
+            p = std::min(1.0, num / den);
+          }
+        }
+        ph[k] = std::min(ph[k], p);
+      }
+    };
+    for (int64_t k = o->up_off[c]; k < o->up_off[c + 1]; ++k) face(v3(&o->rL[3 * o->up[k]]));
+    for (int64_t k = o->lo_off[c]; k < o->lo_off[c + 1]; ++k) face(v3(&o->rR[3 * o->lo[k]]));
+    for (int64_t k = o->bd_off[c]; k < o->bd_off[c + 1]; ++k) face(v3(&o->rL[3 * o->bd[k]]));
+  }
+}
+
+// MUSCL states leftsP/rightsP/leftv3d/rightv3d (Loci FVM), restated in the
+// form flowPsi itself writes out at fluxLowDiss.loci:338-356: q_c + phi *
+// grad.(x_f - x_c), with floors 0.1*min(T) and 0.1*min(pg) - 0.9*Pambient.
+static void face_states(const orc_ctx* o, int64_t f, double qL[5], double qR[5]) {
+  int c = o->cl[f];
+  double qc[5];
+  cell_q(o, c, qc);
+  double qo[5];
+  const bool bnd = o->cr[f] < 0;
+  if (bnd) {
+    for (int k = 0; k < 5; ++k) qo[k] = o->qb[5 * f + k];
+  } else {
+    cell_q(o, o->cr[f], qo);
+  }
+  const double tlim = 0.1 * std::min(qc[0], qo[0]);
+  const double plim = 0.1 * std::min(qc[4], qo[4]) - 0.9 * o->P.Pambient;
+  V3 r = v3(&o->rL[3 * f]);
+  const double* g = &o->grad[15 * c];
+  const double* ph = &o->phi[5 * c];
+  for (int k = 0; k < 5; ++k)
+    qL[k] = qc[k] + ph[k] * (g[3 * k] * r.x + g[3 * k + 1] * r.y + g[3 * k + 2] * r.z);
+  qL[0] = std::max(qL[0], tlim);
+  qL[4] = std::max(qL[4], plim);
+  if (bnd) {
+    for (int k = 0; k < 5; ++k) qR[k] = qo[k];
+    return;
+  }
+  int d = o->cr[f];
+  V3 s = v3(&o->rR[3 * f]);
+  const double* gr = &o->grad[15 * d];
+  const double* pr = &o->phi[5 * d];
+  for (int k = 0; k < 5; ++k)
+    qR[k] = qo[k] + pr[k] * (gr[3 * k] * s.x + gr[3 * k + 1] * s.y + gr[3 * k + 2] * s.z);
+  qR[0] = std::max(qR[0], tlim);
+  qR[4] = std::max(qR[4], plim);
+}
+
+extern "C" int orc_residual(orc_ctx* o, double* src_out, fpsi_resid* norms) {
+  const int64_t nc = o->nc, nf = o->nf;
+  const fpsi_params& P = o->P;
+  if (P.Minf < 0.5) return FPSI_E_UNSUPPORTED;
+  o->qb.assign(nf * 5, 0);
+  for (int64_t f = 0; f < nf; ++f)
+    if (o->cr[f] < 0) bc_face_state(o, f, &o->qb[5 * f]);
+  gradients_and_limiters(o);
+  o->F.assign(nf * 5, 0);
+  o->maxev.assign(nf, 0);
+#pragma omp parallel for schedule(static)
+  for (int64_t f = 0; f < nf; ++f) {
+    double qL[5], qR[5];
+    face_states(o, f, qL, qR);
+    V3 n = v3(&o->an[3 * f]);
+    riemann_flux(P.flux, &o->F[5 * f], qL[4], qL[0], mk(qL[1], qL[2], qL[3]), qR[4], qR[0],
+                 mk(qR[1], qR[2], qR[3]), n, o->area[f], P.Pambient, P.Rtilde, P.gamma, 0.0,
+                 1.0);
+    // maxev_f, solverSetup.loci:81-105 (eta == 1)
+    double ql[5], qr[5];
+    cell_q(o, o->cl[f], ql);
+    if (o->cr[f] >= 0)
+      cell_q(o, o->cr[f], qr);
+    else
+      for (int k = 0; k < 5; ++k) qr[k] = o->qb[5 * f + k];
+    const double eta = 1.0, EP = eta + 1., EM = eta - 1.;
+    double utl = ql[1] * n.x + ql[2] * n.y + ql[3] * n.z;
+    double utr = qr[1] * n.x + qr[2] * n.y + qr[3] * n.z;
+    double al = std::sqrt(P.gamma * P.Rtilde * ql[0]);
+    double ar = std::sqrt(P.gamma * P.Rtilde * qr[0]);
+    double sl = std::sqrt(utl * utl * EM * EM + 4. * eta * al * al);
+    double sr = std::sqrt(utr * utr * EM * EM + 4. * eta * ar * ar);
+    double ml = 0.5 * std::max(std::fabs(utl * EP - sl), std::fabs(utl * EP + sl));
+    double mr = 0.5 * std::max(std::fabs(utr * EP - sr), std::fabs(utr * EP + sr));
+    o->maxev[f] = (o->cr[f] >= 0) ? std::max(ml, mr) : mr;
+  }
+  // scatter in face order: src[cl] -= F, src[cr] += F (fluxInviscid.loci:1253-1268),
+  // done as a per-cell gather over the cell's faces in increasing face order.
+  o->src.assign(nc * 5, 0);
+  o->dtau.assign(nc, 0);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < nc; ++c) {
+    // merge upper, lower, boundary lists by face index
+    int64_t iu = o->up_off[c], il = o->lo_off[c], ib = o->bd_off[c];
+    double s[5] = {0, 0, 0, 0, 0};
+    double meva = 0;
+    while (true) {
+      int64_t fu = iu < o->up_off[c + 1] ? o->up[iu] : INT64_MAX;
+      int64_t fl = il < o->lo_off[c + 1] ? o->lo[il] : INT64_MAX;
+      int64_t fb = ib < o->bd_off[c + 1] ? o->bd[ib] : INT64_MAX;
+      int64_t f = std::min(fu, std::min(fl, fb));
+      if (f == INT64_MAX) break;
+      if (f == fl) {
+        for (int k = 0; k < 5; ++k) s[k] += o->F[5 * f + k];
+        ++il;
+      } else {
+        for (int k = 0; k < 5; ++k) s[k] -= o->F[5 * f + k];
+        if (f == fu)
+          ++iu;
+        else
+          ++ib;
+      }
+    }
+    // cflpdt (solverSetup.loci:107-119): lower, upper, boundary order
+    for (int64_t k = o->lo_off[c]; k < o->lo_off[c + 1]; ++k)
+      meva += o->maxev[o->lo[k]] * o->area[o->lo[k]];
+    for (int64_t k = o->up_off[c]; k < o->up_off[c + 1]; ++k)
+      meva += o->maxev[o->up[k]] * o->area[o->up[k]];
+    for (int64_t k = o->bd_off[c]; k < o->bd_off[c + 1]; ++k)
+      meva += o->maxev[o->bd[k]] * o->area[o->bd[k]];
+    for (int k = 0; k < 5; ++k) o->src[5 * c + k] = s[k];
+    double cflpdt = 0.5 * meva / o->vol[c];
+    // dtcfl + dtau (solverTimestep.loci:289-329), eta == 1
+    double dt = P.dtmax;
+    if (P.cflmax > 0) dt = std::min(dt, P.cflmax / cflpdt);
+    const double rvol = 1. / o->vol[c];
+    const double p = o->pg[c] + P.Pambient, T = o->T[c], Rt = P.Rtilde;
+    const double rP = 1. / (Rt * T);
+    const double rho = (o->pg[c] + P.Pambient) * rP;
+    const double rT = -rho / T, g = P.gamma;
+    V3 U = v3(&o->u[3 * c]);
+    const double q = 0.5 * dot(U, U);
+    const double fT = rT * q, fP = (1. / (g - 1) + rP * q);
+    const double reta = 1.0, a2 = g * Rt * T;
+    const double pterm = (1. - reta) * (g - 1.) / a2;
+    const double cterm = fP * rT * reta - fT * rP * reta;
+    const double q2 = 2. * q;
+    const double dsu = s[1] * U.x + s[2] * U.y + s[3] * U.z;
+    const double dtemp = rvol * (s[0] * (fP * rT * reta + fT * pterm) +
+                                 (dsu - s[4] - q2 * s[0]) * (rT * (pterm + rP * reta))) /
+                         (cterm * rT);
+    dt = std::min(dt, P.urelax * T / (std::fabs(dtemp) + 1e-30));
+    const double dp = rvol * (rT * (q2 * s[0] - dsu + s[4]) - fT * s[0]);
+    dt = std::min(dt, P.urelax * p / (std::fabs(dp) + 1e-30));
+    o->dtau[c] = dt;
+  }
+  // residual norms, solverResidual.loci:74-112 joined in cell order
+  fpsi_resid r;
+  std::memset(&r, 0, sizeof(r));
+  double rt = 0, et = 0, mt = 0;
+  for (int64_t c = 0; c < nc; ++c) {
+    const double* s = &o->src[5 * c];
+    double rvol = 1. / o->vol[c];
+    double w = o->vol[c] / o->vol_tot;
+    double a0 = rvol * s[0];
+    rt += w * (a0 * a0);
+    double mm = 0, mmax = 0;
+    for (int i = 0; i < 3; ++i) {
+      double a = rvol * s[1 + i];
+      if (std::fabs(mmax) < std::fabs(a)) mmax = a;
+      mm += a * a;
+    }
+    mt += mm * (w / 3.0);
+    double a4 = rvol * s[4];
+    et += w * (a4 * a4);
+    if (std::fabs(r.rtmax) < std::fabs(a0)) {
+      r.rtmax = a0;
+      for (int i = 0; i < 3; ++i) r.ccmaxr_center[i] = o->cc[3 * c + i];
+    }
+    if (std::fabs(r.etmax) < std::fabs(a4)) {
+      r.etmax = a4;
+      for (int i = 0; i < 3; ++i) r.ccmaxe_center[i] = o->cc[3 * c + i];
+    }
+    if (std::fabs(r.mtmax) < std::fabs(mmax)) r.mtmax = mmax;
+  }
+  r.rtrms = std::sqrt(rt);
+  r.etrms = std::sqrt(et);
+  r.mtrms = std::sqrt(mt);
+  o->have_resid = true;
+  o->have_asm = false;
+  if (src_out) std::memcpy(src_out, o->src.data(), sizeof(double) * nc * 5);
+  if (norms) *norms = r;
+  if (r.rtrms != r.rtrms || r.etrms != r.etrms || r.mtrms != r.mtrms) return FPSI_E_NAN;
+  return FPSI_OK;
+}
+
+extern "C" int orc_get_reconstruction(orc_ctx* o, double* grad, double* limiter) {
+  if (!o->have_resid) return FPSI_E_STATE;
+  if (grad) std::memcpy(grad, o->grad.data(), sizeof(double) * o->nc * 15);
+  if (limiter) std::memcpy(limiter, o->phi.data(), sizeof(double) * o->nc * 5);
+  return FPSI_OK;
+}
+extern "C" int orc_get_dtau(orc_ctx* o, double* dtau) {
+  if (!o->have_resid) return FPSI_E_STATE;
+  std::memcpy(dtau, o->dtau.data(), sizeof(double) * o->nc);
+  return FPSI_OK;
+}
+
+// Jacobians (fluxInviscid.loci:1190-1221, BC srcJ e.g. bcInflow.loci:357-375),
+// srcJ sum (solverLinearSystem.loci:106-121), steady fluid_D (:176-224),
+// fluid_B (:45-55) and the LU (linearSolverSGS.loci:43-50).
+template <class TB>
+static int assemble_t(orc_ctx* o, std::vector<TB>& fjp, std::vector<TB>& fjm,
+                      std::vector<TB>& D, std::vector<TB>& LU, std::vector<TB>& B) {
+  const int64_t nc = o->nc, nf = o->nf;
+  const fpsi_params& P = o->P;
+  fjp.assign(nf * 25, TB(0));
+  fjm.assign(nf * 25, TB(0));
+#pragma omp parallel for schedule(static)
+  for (int64_t f = 0; f < nf; ++f) {
+    double qL[5], qR[5];
+    face_states(o, f, qL, qR);
+    V3 n = v3(&o->an[3 * f]);
+    roe_jacobian<TB>(&fjp[25 * f], qL[4], qL[0], mk(qL[1], qL[2], qL[3]), qR[4], qR[0],
+                     mk(qR[1], qR[2], qR[3]), n, o->area[f], P.Pambient, P.Rtilde, P.gamma,
+                     0.0, 1.0, 1);
+    if (o->cr[f] >= 0)
+      roe_jacobian<TB>(&fjm[25 * f], qL[4], qL[0], mk(qL[1], qL[2], qL[3]), qR[4], qR[0],
+                       mk(qR[1], qR[2], qR[3]), n, o->area[f], P.Pambient, P.Rtilde, P.gamma,
+                       0.0, 1.0, -1);
+  }
+  D.assign(nc * 25, TB(0));
+  LU.assign(nc * 25, TB(0));
+  B.assign(nc * 5, TB(0));
+  o->piv.assign(nc * 5, 0);
+  int bad = 0;
+#pragma omp parallel for schedule(static) reduction(+ : bad)
+  for (int64_t c = 0; c < nc; ++c) {
+    TB sJ[25];
+    for (int i = 0; i < 25; ++i) sJ[i] = TB(0);
+    for (int64_t k = o->up_off[c]; k < o->up_off[c + 1]; ++k)
+      for (int i = 0; i < 25; ++i) sJ[i] -= fjp[25 * o->up[k] + i];
+    for (int64_t k = o->lo_off[c]; k < o->lo_off[c + 1]; ++k)
+      for (int i = 0; i < 25; ++i) sJ[i] += fjm[25 * o->lo[k] + i];
+    for (int64_t k = o->bd_off[c]; k < o->bd_off[c + 1]; ++k)
+      for (int i = 0; i < 25; ++i) sJ[i] -= fjp[25 * o->bd[k] + i];
+    TB* d = &D[25 * c];
+    for (int i = 0; i < 25; ++i) d[i] = -sJ[i];
+    const double coef = o->vol[c] / o->dtau[c];
+    const double Rt = P.Rtilde, T = o->T[c];
+    const double rP = 1. / (Rt * T);
+    const double rho = (o->pg[c] + P.Pambient) * rP;
+    const double rT = -rho / T;
+    V3 U = v3(&o->u[3 * c]);
+    const double q = 0.5 * dot(U, U);
+    const double fT = rT * q, g = P.gamma, fP = (1. / (g - 1) + rP * q);
+    const double reta = 1.0, a2 = g * Rt * T;
+    const double pterm = (1. - reta) * (g - 1.) / a2;
+#define DD(i, j) d[(i)*5 + (j)]
+    DD(0, 0) += coef * rT;
+    DD(1, 0) += coef * rT * U.x;
+    DD(2, 0) += coef * rT * U.y;
+    DD(3, 0) += coef * rT * U.z;
+    DD(4, 0) += coef * fT;
+    DD(0, 4) += coef * (pterm + rP * reta);
+    DD(1, 4) += coef * (pterm + rP * reta) * U.x;
+    DD(2, 4) += coef * (pterm + rP * reta) * U.y;
+    DD(3, 4) += coef * (pterm + rP * reta) * U.z;
+    DD(4, 4) += coef * (fT * pterm / rT + fP * reta);
+    DD(1, 1) += coef * rho;
+    DD(4, 1) += coef * rho * U.x;
+    DD(2, 2) += coef * rho;
+    DD(4, 2) += coef * rho * U.y;
+    DD(3, 3) += coef * rho;
+    DD(4, 3) += coef * rho * U.z;
+#undef DD
+    for (int i = 0; i < 25; ++i) LU[25 * c + i] = d[i];
+    if (!lu5<TB>(&LU[25 * c], &o->piv[5 * c])) bad += 1;
+    for (int k = 0; k < 5; ++k) B[5 * c + k] = TB(o->src[5 * c + k]);
+  }
+  o->have_asm = true;
+  return bad ? FPSI_E_SINGULAR : FPSI_OK;
+}
+
+extern "C" int orc_assemble(orc_ctx* o) {
+  if (!o->have_resid) return FPSI_E_STATE;
+  if (o->P.precision == FPSI_PREC_FP64)
+    return assemble_t<double>(o, o->fjp64, o->fjm64, o->D64, o->LU64, o->B64);
+  return assemble_t<float>(o, o->fjp32, o->fjm32, o->D32, o->LU32, o->B32);
+}
+
+extern "C" int orc_get_blocks(orc_ctx* o, void* D, void* fjp, void* fjm, void* B) {
+  if (!o->have_asm) return FPSI_E_STATE;
+  const bool d64 = o->P.precision == FPSI_PREC_FP64;
+  const size_t es = d64 ? 8 : 4;
+  if (D) std::memcpy(D, d64 ? (void*)o->D64.data() : (void*)o->D32.data(), es * o->nc * 25);
+  if (fjp) std::memcpy(fjp, d64 ? (void*)o->fjp64.data() : (void*)o->fjp32.data(), es * o->nf * 25);
+  if (fjm) std::memcpy(fjm, d64 ? (void*)o->fjm64.data() : (void*)o->fjm32.data(), es * o->nf * 25);
+  if (B) std::memcpy(B, d64 ? (void*)o->B64.data() : (void*)o->B32.data(), es * o->nc * 5);
+  return FPSI_OK;
+}
+
+// One cell of a Gauss-Seidel sweep (gseidel_forward::calculate,
+// linearSolverSGS.loci:186-207): t = -B + sum_upper U x(cr) + sum_lower L x(cl),
+// x_c = D^-1 (-t), with U = fjm and L = -fjp (solverLinearSystem.loci:57-77).
+template <class TB, class TX>
+static inline void gs_cell(const orc_ctx* o, int64_t c, const std::vector<TB>& fjp,
+                           const std::vector<TB>& fjm, const std::vector<TB>& LU,
+                           const std::vector<TB>& B, TX* x) {
+  TX t[5];
+  for (int i = 0; i < 5; ++i) t[i] = -TX(B[5 * c + i]);
+  for (int64_t k = o->up_off[c]; k < o->up_off[c + 1]; ++k) {
+    int64_t f = o->up[k];
+    const TB* U = &fjm[25 * f];
+    const TX* xn = &x[5 * o->cr[f]];
+    for (int i = 0; i < 5; ++i)
+      for (int j = 0; j < 5; ++j) t[i] += TX(U[5 * i + j]) * xn[j];
+  }
+  for (int64_t k = o->lo_off[c]; k < o->lo_off[c + 1]; ++k) {
+    int64_t f = o->lo[k];
+    const TB* Lp = &fjp[25 * f];
+    const TX* xn = &x[5 * o->cl[f]];
+    for (int i = 0; i < 5; ++i)
+      for (int j = 0; j < 5; ++j) t[i] += TX(-Lp[5 * i + j]) * xn[j];
+  }
+  TX v[5];
+  for (int i = 0; i < 5; ++i) v[i] = -t[i];
+  lu5_solve<TB, TX>(&LU[25 * c], &o->piv[5 * c], v, &x[5 * c]);
+}
+
+template <class TB, class TX>
+static int solve_t(orc_ctx* o, const int32_t* colour, const double* x0,
+                   const std::vector<TB>& fjp, const std::vector<TB>& fjm,
+                   const std::vector<TB>& LU, const std::vector<TB>& B) {
+  const int64_t nc = o->nc;
+  std::vector<TX> x(nc * 5);
+  if (x0) {
+    for (int64_t i = 0; i < nc * 5; ++i) x[i] = TX(x0[i]);
+  } else {
+    // block Jacobi start D x = B (linearSolverSGS.loci:57-69)
+    for (int64_t c = 0; c < nc; ++c) {
+      TX b[5];
+      for (int i = 0; i < 5; ++i) b[i] = TX(B[5 * c + i]);
+      lu5_solve<TB, TX>(&LU[25 * c], &o->piv[5 * c], b, &x[5 * c]);
+    }
+  }
+  const int nit = o->P.gauss_seidel_iter;
+  if (!colour) {
+    for (int it = 0; it < nit; ++it) {
+      for (int64_t c = 0; c < nc; ++c) gs_cell<TB, TX>(o, c, fjp, fjm, LU, B, x.data());
+      for (int64_t c = nc - 1; c >= 0; --c) gs_cell<TB, TX>(o, c, fjp, fjm, LU, B, x.data());
+    }
+  } else {
+    int ncol = 0;
+    for (int64_t c = 0; c < nc; ++c) ncol = std::max(ncol, colour[c] + 1);
+    std::vector<std::vector<int64_t>> byc(ncol);
+    for (int64_t c = 0; c < nc; ++c) byc[colour[c]].push_back(c);
+    for (int it = 0; it < nit; ++it) {
+      for (int k = 0; k < ncol; ++k) {
+        const auto& L = byc[k];
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < (int64_t)L.size(); ++i)
+          gs_cell<TB, TX>(o, L[i], fjp, fjm, LU, B, x.data());
+      }
+      for (int k = ncol - 1; k >= 0; --k) {
+        const auto& L = byc[k];
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < (int64_t)L.size(); ++i)
+          gs_cell<TB, TX>(o, L[i], fjp, fjm, LU, B, x.data());
+      }
+    }
+  }
+  o->dq.resize(nc * 5);
+  for (int64_t i = 0; i < nc * 5; ++i) o->dq[i] = double(x[i]);
+  o->have_dq = true;
+  return FPSI_OK;
+}
+
+extern "C" int orc_linear_solve(orc_ctx* o, const int32_t* colour, const double* x0,
+                                double* dq, fpsi_lsinfo* info) {
+  if (!o->have_asm) return FPSI_E_STATE;
+  int rc;
+  switch (o->P.precision) {
+    case FPSI_PREC_FP64:
+      rc = solve_t<double, double>(o, colour, x0, o->fjp64, o->fjm64, o->LU64, o->B64);
+      break;
+    case FPSI_PREC_MIXED:
+      rc = solve_t<float, float>(o, colour, x0, o->fjp32, o->fjm32, o->LU32, o->B32);
+      break;
+    default:
+      rc = solve_t<float, double>(o, colour, x0, o->fjp32, o->fjm32, o->LU32, o->B32);
+  }
+  if (dq) std::memcpy(dq, o->dq.data(), sizeof(double) * o->nc * 5);
+  if (info) {
+    info->iterations = o->P.gauss_seidel_iter;
+    info->status = rc;
+    info->resid0 = info->resid = 0;
+  }
+  return rc;
+}
+
+// ||B - A dq|| with A from the unfactored blocks
+template <class TB>
+static void linres_t(orc_ctx* o, const std::vector<TB>& fjp, const std::vector<TB>& fjm,
+                     const std::vector<TB>& D, const std::vector<TB>& B, double* nb, double* nr) {
+  double sb = 0, sr = 0;
+  for (int64_t c = 0; c < o->nc; ++c) {
+    double r[5];
+    for (int i = 0; i < 5; ++i) r[i] = double(B[5 * c + i]);
+    const double* x = &o->dq[5 * c];
+    for (int i = 0; i < 5; ++i)
+      for (int j = 0; j < 5; ++j) r[i] -= double(D[25 * c + 5 * i + j]) * x[j];
+    for (int64_t k = o->up_off[c]; k < o->up_off[c + 1]; ++k) {
+      int64_t f = o->up[k];
+      const double* xn = &o->dq[5 * o->cr[f]];
+      for (int i = 0; i < 5; ++i)
+        for (int j = 0; j < 5; ++j) r[i] -= double(fjm[25 * f + 5 * i + j]) * xn[j];
+    }
+    for (int64_t k = o->lo_off[c]; k < o->lo_off[c + 1]; ++k) {
+      int64_t f = o->lo[k];
+      const double* xn = &o->dq[5 * o->cl[f]];
+      for (int i = 0; i < 5; ++i)
+        for (int j = 0; j < 5; ++j) r[i] += double(fjp[25 * f + 5 * i + j]) * xn[j];
+    }
+    for (int i = 0; i < 5; ++i) {
+      sb += double(B[5 * c + i]) * double(B[5 * c + i]);
+      sr += r[i] * r[i];
+    }
+  }
+  *nb = std::sqrt(sb);
+  *nr = std::sqrt(sr);
+}
+
+extern "C" int orc_linear_residual(orc_ctx* o, double* norm_b, double* norm_r) {
+  if (!o->have_dq) return FPSI_E_STATE;
+  double nb, nr;
+  if (o->P.precision == FPSI_PREC_FP64)
+    linres_t<double>(o, o->fjp64, o->fjm64, o->D64, o->B64, &nb, &nr);
+  else
+    linres_t<float>(o, o->fjp32, o->fjm32, o->D32, o->B32, &nb, &nr);
+  if (norm_b) *norm_b = nb;
+  if (norm_r) *norm_r = nr;
+  return FPSI_OK;
+}
+
+// Steady Newton update with positivity clip, solverNewton.loci:62-78.
+extern "C" int orc_update(orc_ctx* o, double* min_alpha) {
+  if (!o->have_dq) return FPSI_E_STATE;
+  double amin = 1.0;
+  for (int64_t c = 0; c < o->nc; ++c) {
+    const double* d = &o->dq[5 * c];
+    double alpha = 1.0;
+    alpha = std::min(alpha, 0.9 * o->T[c] / (std::fabs(d[0]) + 1e-30));
+    alpha = std::min(alpha, 0.9 * (o->pg[c] + o->P.Pambient) / (std::fabs(d[4]) + 1e-30));
+    o->T[c] += alpha * d[0];
+    o->pg[c] += alpha * d[4];
+    for (int i = 0; i < 3; ++i) o->u[3 * c + i] += alpha * d[1 + i];
+    amin = std::min(amin, alpha);
+  }
+  if (min_alpha) *min_alpha = amin;
+  o->have_resid = o->have_asm = o->have_dq = false;
+  return FPSI_OK;
+}
+
+extern "C" int orc_newton_step(orc_ctx* o, const int32_t* colour, fpsi_stepinfo* info) {
+  fpsi_stepinfo si;
+  std::memset(&si, 0, sizeof(si));
+  int rc = orc_residual(o, nullptr, &si.resid);
+  if (rc) return rc;
+  si.dtau_min = *std::min_element(o->dtau.begin(), o->dtau.end());
+  si.dtau_max = *std::max_element(o->dtau.begin(), o->dtau.end());
+  rc = orc_assemble(o);
+  if (rc) return rc;
+  rc = orc_linear_solve(o, colour, nullptr, nullptr, &si.ls);
+  if (rc) return rc;
+  rc = orc_update(o, &si.min_alpha);
+  if (info) *info = si;
+  return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Batched face functions
+// ---------------------------------------------------------------------------
+extern "C" int orc_face_flux(int32_t kind, int64_t n, const double* qL, const double* qR,
+                             const double* an, const double* area, double pamb, double Rt,
+                             double gamma, double us_n, double eta, double* flux) {
+  for (int64_t i = 0; i < n; ++i) {
+    const double* l = qL + 5 * i;
+    const double* r = qR + 5 * i;
+    riemann_flux(kind, flux + 5 * i, l[0], l[1], mk(l[2], l[3], l[4]), r[0], r[1],
+                 mk(r[2], r[3], r[4]), v3(an + 3 * i), area[i], pamb, Rt, gamma, us_n, eta);
+  }
+  return FPSI_OK;
+}
+
+extern "C" int orc_face_jacobian(int64_t n, const double* qL, const double* qR,
+                                 const double* an, const double* area, double pamb, double Rt,
+                                 double gamma, double us_n, double eta, int32_t dir,
+                                 int32_t as_double, void* out) {
+  for (int64_t i = 0; i < n; ++i) {
+    const double* l = qL + 5 * i;
+    const double* r = qR + 5 * i;
+    if (as_double) {
+      double* J = (double*)out + 25 * i;
+      for (int k = 0; k < 25; ++k) J[k] = 0;
+      roe_jacobian<double>(J, l[0], l[1], mk(l[2], l[3], l[4]), r[0], r[1],
+                           mk(r[2], r[3], r[4]), v3(an + 3 * i), area[i], pamb, Rt, gamma,
+                           us_n, eta, dir);
+    } else {
+      float* J = (float*)out + 25 * i;
+      for (int k = 0; k < 25; ++k) J[k] = 0;
+      roe_jacobian<float>(J, l[0], l[1], mk(l[2], l[3], l[4]), r[0], r[1],
+                          mk(r[2], r[3], r[4]), v3(an + 3 * i), area[i], pamb, Rt, gamma, us_n,
+                          eta, dir);
+    }
+  }
+  return FPSI_OK;
+}
+
+extern "C" int orc_cv_state(int32_t outflow, int64_t n, const double* qi, const double* q0,
+                            const double* an, double us_n, double pamb, double gamma, double Rt,
+                            double beta, double* out) {
+  for (int64_t i = 0; i < n; ++i) {
+    const double* a = qi + 5 * i;
+    const double* b = q0 + 5 * i;
+    double pgb, Tb;
+    V3 ub;
+    if (outflow)
+      cv_outflow(pgb, Tb, ub, a[0], a[1], mk(a[2], a[3], a[4]), b[0], b[1], mk(b[2], b[3], b[4]),
+                 v3(an + 3 * i), us_n, pamb, gamma, Rt, beta);
+    else
+      cv_inflow(pgb, Tb, ub, a[0], a[1], mk(a[2], a[3], a[4]), b[0], b[1], mk(b[2], b[3], b[4]),
+                v3(an + 3 * i), us_n, pamb, gamma, Rt, beta);
+    double* o = out + 5 * i;
+    o[0] = pgb, o[1] = Tb, o[2] = ub.x, o[3] = ub.y, o[4] = ub.z;
+  }
+  return FPSI_OK;
+}

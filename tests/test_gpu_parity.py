@@ -1,0 +1,229 @@
+"""Parity of the CUDA path with the oracle, through the C ABI.  GPU only.
+
+Tolerances (stated per quantity):
+  * face fluxes and the residual 'src': 1e-12 of the flux scale (the
+    magnitude of the flux terms; see tests.helpers.flux_scale);
+  * FP32 (real_fj) Jacobian blocks: 1e-6 of the block's largest entry; FP64
+    blocks 1e-12;
+  * gradients 1e-10 of the field's largest gradient, limiter values 1e-9;
+  * relaxation result dq with the same colouring: 1e-10 of max|dq| (FP64),
+    1e-4 (FP32 blocks);
+  * Newton states after 3 steps: 1e-10 relative (FP64), 1e-6 (FP32 blocks).
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from flowpsi_b200 import (FlowPsi, FpsiError, cases, inviscid_riemann_flux, roe_jacobian)
+from oracle import Oracle, OracleFunctions
+from tests.helpers import block_rel, face_states, flux_scale, rel_to_scale
+
+pytestmark = pytest.mark.gpu
+
+GOLD = np.load(Path(__file__).resolve().parent / "golden" / "face_functions.npz")
+RT, GAMMA = 8314.4621 / 28.96, 1.4
+
+
+# --------------------------------------------------------------------------
+# face functions
+# --------------------------------------------------------------------------
+@pytest.mark.parametrize("name", ["mild", "strong", "rest"])
+@pytest.mark.parametrize("eta", [1.0, 0.3])
+def test_face_functions_golden(need_gpu, name, eta):
+    qL, qR, an, area = (GOLD[f"{name}_{k}"] for k in ("qL", "qR", "an", "area"))
+    sc = flux_scale(qL, qR, an, area)
+    for kind in ("hllc", "roe"):
+        got = inviscid_riemann_flux(kind, qL, qR, an, area, eta=eta)
+        assert rel_to_scale(got, GOLD[f"{name}_eta{eta:g}_{kind}"], sc) < 1e-12
+    for d, key in ((1, "fjp"), (-1, "fjm")):
+        got = roe_jacobian(qL, qR, an, area, d, eta=eta)
+        assert block_rel(got, GOLD[f"{name}_eta{eta:g}_{key}"]) < 1e-6
+
+
+def test_face_functions_vs_oracle(need_gpu):
+    qL, qR, an, area = face_states(20000, 21, jump=0.4, speed=300.0)
+    O = OracleFunctions()
+    sc = flux_scale(qL, qR, an, area)
+    for kind in ("hllc", "roe", "hlle"):
+        assert rel_to_scale(inviscid_riemann_flux(kind, qL, qR, an, area),
+                            O.flux(kind, qL, qR, an, area), sc) < 1e-12
+    for d in (1, -1):
+        a = roe_jacobian(qL, qR, an, area, d, as_double=True)
+        b = O.jacobian(qL, qR, an, area, d, as_double=True)
+        assert block_rel(a, b) < 1e-12
+
+
+# --------------------------------------------------------------------------
+# mesh level
+# --------------------------------------------------------------------------
+CASES = {
+    "farfield_hex": lambda prec: cases.farfield_cube(8, precision=prec),
+    "tgv_tets": lambda prec: cases.taylor_green_tets(5, precision=prec),
+    "shock_hex": lambda prec: cases.oblique_shock_cube(8, precision=prec),
+    "farfield_hllc": lambda prec: cases.farfield_cube(6, precision=prec, flux="hllc",
+                                                      limiter="barth"),
+}
+
+
+def _pair(case):
+    g = FlowPsi(case.mesh, case.params)
+    o = Oracle(case.mesh, case.params)
+    T, p, u = case.initial_state(o.geometry()["cellcenter"])
+    g.set_state(T, p, u)
+    o.set_state(T, p, u)
+    return g, o
+
+
+def cell_scale(o, T, p, u):
+    """per cell: flux-term magnitude times the cell's total face area"""
+    a = o._mesh.arrays()
+    area = o.geometry()["area"]
+    asum = np.zeros(o.ncells)
+    np.add.at(asum, a.cl, area)
+    inner = a.cr >= 0
+    np.add.at(asum, a.cr[inner], area[inner])
+    rho = p / (RT * T)
+    c = np.sqrt(GAMMA * RT * T)
+    s = np.linalg.norm(u, axis=1) + c
+    e0 = RT * T / (GAMMA - 1) + 0.5 * (u * u).sum(1)
+    out = np.empty((o.ncells, 5))
+    out[:, 0] = rho * s
+    out[:, 1:4] = (rho * s * np.abs(u).max(1) + np.abs(p))[:, None]
+    out[:, 4] = rho * s * e0 + np.abs(p) * s
+    return out * asum[:, None]
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_geometry_matches_oracle(need_gpu, name):
+    g, o = _pair(CASES[name]("ref"))
+    G, O = g.geometry(), o.geometry()
+    np.testing.assert_allclose(G["vol"], O["vol"], rtol=1e-13)
+    np.testing.assert_allclose(G["cellcenter"], O["cellcenter"], rtol=0,
+                               atol=1e-13 * np.abs(O["cellcenter"]).max())
+    np.testing.assert_allclose(G["area"], O["area"], rtol=1e-13)
+    np.testing.assert_allclose(G["facecenter"], O["facecenter"], rtol=0,
+                               atol=1e-13 * np.abs(O["facecenter"]).max())
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_residual_matches_oracle(need_gpu, name):
+    case = CASES[name]("ref")
+    g, o = _pair(case)
+    T, p, u = o.get_state()
+    sg, ng = g.residual()
+    so, no = o.residual()
+    assert np.max(np.abs(sg - so) / cell_scale(o, T, p, u)) < 1e-12
+    for k in ("rtrms", "etrms", "mtrms", "rtmax", "etmax", "mtmax"):
+        assert abs(ng[k] - no[k]) <= 1e-9 * abs(no[k]) + 1e-300, k
+    gg, lg = g.reconstruction()
+    go, lo = o.reconstruction()
+    for v in range(5):
+        sl = slice(3 * v, 3 * v + 3)
+        assert np.abs(gg[:, sl] - go[:, sl]).max() <= 1e-10 * np.abs(go[:, sl]).max() + 1e-300
+    assert np.abs(lg - lo).max() < 1e-9
+    np.testing.assert_allclose(g.dtau(), o.dtau(), rtol=1e-10)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "ref", "mixed"])
+@pytest.mark.parametrize("name", ["farfield_hex", "tgv_tets", "shock_hex"])
+def test_blocks_match_oracle(need_gpu, name, prec):
+    g, o = _pair(CASES[name](prec))
+    g.residual()
+    o.residual()
+    g.assemble()
+    o.assemble()
+    bg, bo = g.blocks(), o.blocks()
+    tol = 1e-12 if prec == "fp64" else 1e-6
+    for k in ("fluid_D", "fjp", "fjm"):
+        assert bg[k].dtype == bo[k].dtype
+        inner = np.abs(bo[k]).reshape(len(bo[k]), -1).max(1) > 0
+        assert block_rel(bg[k][inner], bo[k][inner]) < tol, k
+    np.testing.assert_allclose(bg["fluid_B"], bo["fluid_B"], rtol=tol,
+                               atol=tol * np.abs(bo["fluid_B"]).max())
+
+
+@pytest.mark.parametrize("prec", ["fp64", "ref", "mixed"])
+@pytest.mark.parametrize("name", ["farfield_hex", "tgv_tets"])
+def test_multicolour_sgs_matches_oracle(need_gpu, name, prec):
+    g, o = _pair(CASES[name](prec))
+    g.residual()
+    o.residual()
+    g.assemble()
+    o.assemble()
+    dg = g.linear_solve()
+    do = o.linear_solve(colour=g.colours())
+    tol = 1e-10 if prec == "fp64" else 1e-4
+    for k in range(5):
+        assert np.abs(dg[:, k] - do[:, k]).max() <= tol * np.abs(do[:, k]).max(), k
+    nb, nr = g.linear_residual()
+    assert nr < nb
+
+
+def test_sgs_converges_on_gpu(need_gpu):
+    case = CASES["farfield_hex"]("fp64")
+    g, _ = _pair(case)
+    g.residual()
+    res = []
+    for sweeps in (1, 4, 16):
+        p = case.params
+        p.gauss_seidel_iter = sweeps
+        g.set_params(p)
+        g.assemble()
+        g.linear_solve()
+        res.append(g.linear_residual()[1])
+    assert res[2] < res[1] < res[0]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "ref"])
+@pytest.mark.parametrize("name", ["farfield_hex", "tgv_tets", "shock_hex"])
+def test_newton_steps_match_oracle(need_gpu, name, prec):
+    case = CASES[name](prec)
+    g, o = _pair(case)
+    col = g.colours()
+    for _ in range(3):
+        rg = g.newton_step()
+        ro = o.newton_step(colour=col)
+        assert abs(rg["rtrms"] - ro["rtrms"]) <= 1e-6 * ro["rtrms"]
+    Tg, pg_, ug = g.get_state()
+    To, po, uo = o.get_state()
+    tol = 1e-10 if prec == "fp64" else 1e-6
+    np.testing.assert_allclose(Tg, To, rtol=tol)
+    np.testing.assert_allclose(pg_, po, rtol=tol)
+    assert np.abs(ug - uo).max() <= tol * np.abs(uo).max()
+
+
+def test_run_is_deterministic_and_equals_steps(need_gpu):
+    case = CASES["tgv_tets"]("mixed")
+    g, o = _pair(case)
+    T0, p0, u0 = g.get_state()
+    h1 = g.run(3)
+    s1 = g.get_state()
+    g.set_state(T0, p0, u0)
+    h2 = [g.newton_step() for _ in range(3)]
+    s2 = g.get_state()
+    for a, b in zip(s1, s2):
+        np.testing.assert_array_equal(a, b)
+    for a, b in zip(h1, h2):
+        assert a["rtrms"] == b["rtrms"] and a["etrms"] == b["etrms"]
+
+
+def test_nan_state_is_reported(need_gpu):
+    case = CASES["farfield_hex"]("ref")
+    g, o = _pair(case)
+    T, p, u = g.get_state()
+    T[3] = np.nan
+    g.set_state(T, p, u)
+    with pytest.raises(FpsiError) as e:
+        g.residual()
+    assert e.value.code == -6  # FPSI_E_NAN, as solverResidual.loci:203-208 aborts
+
+
+def test_call_order_enforced(need_gpu):
+    case = CASES["farfield_hex"]("ref")
+    g, _ = _pair(case)
+    with pytest.raises(FpsiError) as e:
+        g.assemble()
+    assert e.value.code == -8
+    with pytest.raises(FpsiError):
+        g.linear_solve()

@@ -1,0 +1,123 @@
+"""Mesh-level checks of the oracle (CPU): geometry closure, free-stream
+preservation, exact gradients of linear fields, SGS convergence and Newton
+residual decrease."""
+import numpy as np
+import pytest
+
+from flowpsi_b200 import GeneratedMesh, bc, cases, default_params
+from oracle import Oracle
+
+
+def _closure(orc, mesh):
+    a = mesh.arrays()
+    g = orc.geometry()
+    s = np.zeros((orc.ncells, 3))
+    np.add.at(s, a.cl, g["area_vec"])
+    inner = a.cr >= 0
+    np.add.at(s, a.cr[inner], -g["area_vec"][inner])
+    return np.abs(s).max() / g["area"].max()
+
+
+@pytest.mark.parametrize("kind", ["hex", "kuhn", "bl"])
+def test_geometry_closed_and_volume(kind):
+    if kind == "hex":
+        m = GeneratedMesh("hex", n=(5, 4, 3), L=(2.0, 1.0, 0.5), bc_side=(0,) * 6,
+                          bcs=[bc("farfield")])
+        vol = 1.0
+    elif kind == "kuhn":
+        m = GeneratedMesh("kuhn", n=(5, 4, 6), L=(1.0, 2.0, 3.0), jitter=0.1, seed=5)
+        vol = 6.0
+    else:
+        m = GeneratedMesh("bl", n=(4, 6, 3), L=(1.0, 1.0, 1.0), dy0=1e-3, growth=1.3,
+                          bc_side=(0, 0, 0, 0, -1, -1), bcs=[bc("farfield")])
+        vol = sum(1e-3 * 1.3 ** j for j in range(6))
+    o = Oracle(m, default_params(solver="sgs"))
+    assert _closure(o, m) < 1e-12
+    assert abs(o.geometry()["vol"].sum() - vol) < 1e-12 * vol
+
+
+def test_freestream_preserved():
+    case = cases.farfield_cube(6)
+    o = Oracle(case.mesh, case.params)
+    b = case.mesh.arrays().bcs[0]
+    nc = o.ncells
+    o.set_state(np.full(nc, b.T), np.full(nc, b.pg), np.tile(list(b.u), (nc, 1)))
+    src, r = o.residual()
+    assert np.abs(src).max() < 1e-9 * 1e5 * o.geometry()["area"].max()
+
+
+def test_periodic_uniform_state_zero_residual():
+    case = cases.taylor_green_tets(5)
+    o = Oracle(case.mesh, case.params)
+    nc = o.ncells
+    o.set_state(np.full(nc, 300.0), np.full(nc, 1e5), np.tile([30.0, -20.0, 10.0], (nc, 1)))
+    src, _ = o.residual()
+    # energy flux scale rho*(|u|+a)*e0*area ~ 1e7 here: round-off only
+    rho, a = 1e5 / (287.05 * 300.0), 347.0
+    scale = rho * (40.0 + a) * (287.05 * 300.0 / 0.4) * o.geometry()["area"].max()
+    assert np.abs(src).max() < 1e-14 * scale
+
+
+def test_linear_field_gradient_exact():
+    case = cases.taylor_green_tets(6)
+    p = default_params(solver="sgs", limiter="none")
+    o = Oracle(case.mesh, p)
+    cc = o.geometry()["cellcenter"]
+    # periodic box: use a field linear inside the box interior only and check
+    # cells whose neighbours do not wrap
+    L = 2 * np.pi
+    T = 300.0 + 3.0 * cc[:, 0] - 2.0 * cc[:, 1] + 1.0 * cc[:, 2]
+    o.set_state(T, np.full(len(T), 1e5), np.zeros((len(T), 3)))
+    o.residual()
+    g, phi = o.reconstruction()
+    inner = np.all((cc > 0.25 * L) & (cc < 0.75 * L), axis=1)
+    np.testing.assert_allclose(g[inner, 0:3], np.tile([3.0, -2.0, 1.0], (inner.sum(), 1)),
+                               rtol=0, atol=1e-9)
+    assert np.all(phi == 1.0)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "ref", "mixed"])
+def test_sgs_reduces_linear_residual(precision):
+    case = cases.farfield_cube(6, precision=precision)
+    o = Oracle(case.mesh, case.params)
+    T, p, u = case.initial_state(o.geometry()["cellcenter"])
+    o.set_state(T, p, u)
+    o.residual()
+    o.assemble()
+    res = []
+    for sweeps in (0, 1, 3, 6):
+        prm = case.params
+        prm.gauss_seidel_iter = sweeps
+        o.set_params(prm)
+        o.assemble()
+        o.linear_solve()
+        res.append(o.linear_residual()[1])
+    assert res[1] < res[0] and res[3] < res[2] < res[1]
+
+
+def test_multicolour_and_sequential_agree_at_convergence():
+    case = cases.farfield_cube(5, precision="fp64")
+    o = Oracle(case.mesh, case.params)
+    T, p, u = case.initial_state(o.geometry()["cellcenter"])
+    o.set_state(T, p, u)
+    o.residual()
+    prm = case.params
+    prm.gauss_seidel_iter = 60
+    o.set_params(prm)
+    o.assemble()
+    seq = o.linear_solve()
+    # red/black-like colouring of the structured hex grid
+    idx = np.arange(o.ncells)
+    i, j, k = idx % 5, (idx // 5) % 5, idx // 25
+    colour = ((i + j + k) % 2).astype(np.int32)
+    mc = o.linear_solve(colour=colour)
+    assert np.abs(seq - mc).max() < 1e-8 * np.abs(seq).max()
+
+
+def test_newton_decreases_residual():
+    case = cases.farfield_cube(8)
+    o = Oracle(case.mesh, case.params)
+    T, p, u = case.initial_state(o.geometry()["cellcenter"])
+    o.set_state(T, p, u)
+    r = [o.newton_step()["rtrms"] for _ in range(8)]
+    assert r[-1] < 0.1 * r[0]
