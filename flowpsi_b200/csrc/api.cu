@@ -69,10 +69,11 @@ std::vector<double> soa3(const std::vector<double>& a, int64_t n) {
 }
 
 void free_system(fpsi_ctx* x) {
-  void* ps[] = {x->d_fjp, x->d_fjm, x->d_cellblk, x->d_D, x->d_x};
+  void* ps[] = {x->d_fjp, x->d_fjm, x->d_D, x->d_x, x->d_luc, x->d_bc, x->d_pv, x->d_aoff};
   for (void* p : ps)
     if (p) cudaFree(p);
-  x->d_fjp = x->d_fjm = x->d_cellblk = x->d_D = x->d_x = nullptr;
+  x->d_fjp = x->d_fjm = x->d_D = x->d_x = x->d_luc = x->d_bc = x->d_aoff = nullptr;
+  x->d_pv = nullptr;
 }
 
 int alloc_system(fpsi_ctx* x) {
@@ -86,7 +87,10 @@ int alloc_system(fpsi_ctx* x) {
   int rc;
   if ((rc = dalloc(x, (char**)&x->d_fjp, nf * 25 * tb))) return rc;
   if ((rc = dalloc(x, (char**)&x->d_fjm, nf * 25 * tb))) return rc;
-  if ((rc = dalloc(x, (char**)&x->d_cellblk, nc * 32 * tb))) return rc;
+  if ((rc = dalloc(x, (char**)&x->d_luc, nc * 25 * tb))) return rc;
+  if ((rc = dalloc(x, (char**)&x->d_bc, nc * 5 * tb))) return rc;
+  if ((rc = dalloc(x, &x->d_pv, nc))) return rc;
+  if ((rc = dalloc(x, (char**)&x->d_aoff, size_t(x->H.nslots) * 25 * tb))) return rc;
   if (x->keep_D)
     if ((rc = dalloc(x, (char**)&x->d_D, nc * 25 * tb))) return rc;
   if ((rc = dalloc(x, (char**)&x->d_x, nc * 5 * tx))) return rc;
@@ -209,7 +213,8 @@ int fpsi_destroy(fpsi_ctx* x) {
   void* ps[] = {x->d_cl, x->d_cr, x->d_n, x->d_area, x->d_rL, x->d_rR, x->d_vol, x->d_cc,
                 x->d_Minv, x->d_cf_off, x->d_cf, x->d_colour_cells, x->d_bcs, x->d_q,
                 x->d_qb, x->d_grad, x->d_phi, x->d_F, x->d_mev, x->d_src, x->d_dtau,
-                x->d_part, x->d_resid, x->d_amin, x->d_err, x->d_perm, x->d_stage};
+                x->d_part, x->d_resid, x->d_amin, x->d_err, x->d_perm, x->d_stage, x->d_ci, x->d_ccol,
+                x->d_nbr, x->d_colinfo};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (x->h_resid) cudaFreeHost(x->h_resid);
@@ -280,6 +285,15 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
   TRY(upload(x, &x->d_cf, H.cf));
   TRY(upload(x, &x->d_colour_cells, H.colour_cells));
   TRY(upload(x, &x->d_perm, H.perm));
+  TRY(upload(x, &x->d_ci, H.ci_of));
+  TRY(upload(x, &x->d_ccol, H.colour));
+  TRY(upload(x, &x->d_nbr, H.nbr));
+  {
+    std::vector<fpsi::ColInfo> ci(H.ncolours);
+    for (int k = 0; k < H.ncolours; ++k)
+      ci[k] = fpsi::ColInfo{H.col_cb[k], H.col_n[k], H.col_eb[k], H.col_m[k]};
+    TRY(upload(x, &x->d_colinfo, ci));
+  }
   TRY(dalloc(x, &x->d_stage, nc * 5));
   TRY(upload(x, &x->d_bcs, x->bcs));
   TRY(dalloc(x, &x->d_q, nc * 5));
@@ -440,7 +454,7 @@ static int finish_assemble(fpsi_ctx* x) {
 int fpsi_assemble(fpsi_ctx* x) {
   if (!x) return FPSI_E_INVALID;
   if (!x->have_resid) return FPSI_E_STATE;
-  int rc = fpsi::launch_assemble(x, nullptr);
+  int rc = fpsi::launch_assemble(x);
   if (rc) return rc;
   if ((rc = finish_assemble(x))) return rc;
   x->have_asm = true;
@@ -475,11 +489,16 @@ int fpsi_get_blocks(fpsi_ctx* x, void* D, void* fjp, void* fjm, void* B) {
     }
   }
   if (B) {
-    h.resize(size_t(nc) * 32 * tb);
-    FPSI_CUDA_TRY(cudaMemcpy(h.data(), x->d_cellblk, h.size(), cudaMemcpyDeviceToHost));
-    for (int64_t i = 0; i < nc; ++i)
-      std::memcpy((char*)B + size_t(x->H.perm[i]) * 5 * tb, h.data() + (size_t(i) * 32 + 25) * tb,
-                  5 * tb);
+    h.resize(size_t(nc) * 5 * tb);
+    FPSI_CUDA_TRY(cudaMemcpy(h.data(), x->d_bc, h.size(), cudaMemcpyDeviceToHost));
+    const HostMesh& H = x->H;
+    for (int k = 0; k < H.ncolours; ++k)
+      for (int64_t i = 0; i < H.col_n[k]; ++i) {
+        const int64_t c = H.colour_cells[H.col_cb[k] + i];
+        char* o = (char*)B + size_t(H.perm[c]) * 5 * tb;
+        for (int j = 0; j < 5; ++j)
+          std::memcpy(o + j * tb, h.data() + (size_t(5 * H.col_cb[k]) + j * H.col_n[k] + i) * tb, tb);
+      }
   }
   return FPSI_OK;
 }
@@ -489,12 +508,14 @@ static int upload_x(fpsi_ctx* x, const double* x0) {
   if (x->x_bytes == 8) {
     std::vector<double> v(5 * nc);
     for (int64_t i = 0; i < nc; ++i)
-      for (int k = 0; k < 5; ++k) v[5 * i + k] = x0[5 * int64_t(x->H.perm[i]) + k];
+      for (int k = 0; k < 5; ++k)
+        v[5 * int64_t(x->H.ci_of[i]) + k] = x0[5 * int64_t(x->H.perm[i]) + k];
     FPSI_CUDA_TRY(cudaMemcpy(x->d_x, v.data(), v.size() * 8, cudaMemcpyHostToDevice));
   } else {
     std::vector<float> v(5 * nc);
     for (int64_t i = 0; i < nc; ++i)
-      for (int k = 0; k < 5; ++k) v[5 * i + k] = float(x0[5 * int64_t(x->H.perm[i]) + k]);
+      for (int k = 0; k < 5; ++k)
+        v[5 * int64_t(x->H.ci_of[i]) + k] = float(x0[5 * int64_t(x->H.perm[i]) + k]);
     FPSI_CUDA_TRY(cudaMemcpy(x->d_x, v.data(), v.size() * 4, cudaMemcpyHostToDevice));
   }
   return FPSI_OK;
@@ -510,7 +531,9 @@ static int download_x(fpsi_ctx* x, double* dq) {
     FPSI_CUDA_TRY(cudaMemcpy(f.data(), x->d_x, f.size() * 4, cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < f.size(); ++i) v[i] = f[i];
   }
-  unpermute_cells(x, v.data(), 5, dq);
+  for (int64_t i = 0; i < nc; ++i)
+    for (int k = 0; k < 5; ++k)
+      dq[5 * int64_t(x->H.perm[i]) + k] = v[5 * int64_t(x->H.ci_of[i]) + k];
   return FPSI_OK;
 }
 
@@ -522,8 +545,7 @@ int fpsi_linear_solve(fpsi_ctx* x, const double* x0, double* dq, fpsi_lsinfo* in
     if ((rc = upload_x(x, x0))) return rc;
   } else if (x->have_dq) {
     // iterate was consumed by an earlier solve: rebuild the block Jacobi start
-    if ((rc = fpsi::launch_assemble(x, nullptr))) return rc;
-    if ((rc = finish_assemble(x))) return rc;
+    if ((rc = fpsi::launch_jacobi_start(x))) return rc;
   }
   if ((rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter))) return rc;
   if ((rc = sync(x))) return rc;
@@ -568,7 +590,7 @@ int fpsi_newton_step(fpsi_ctx* x, fpsi_stepinfo* info) {
   if (!x) return FPSI_E_INVALID;
   int rc;
   if ((rc = fpsi::launch_residual(x, x->d_resid))) return rc;
-  if ((rc = fpsi::launch_assemble(x, nullptr))) return rc;
+  if ((rc = fpsi::launch_assemble(x))) return rc;
   if ((rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter))) return rc;
   if ((rc = fpsi::launch_update(x))) return rc;
   FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid, x->d_resid, 8 * sizeof(double),
@@ -598,7 +620,7 @@ int fpsi_run(fpsi_ctx* x, int32_t nsteps, fpsi_resid* norms) {
   int rc = FPSI_OK;
   for (int32_t s = 0; s < nsteps && !rc; ++s) {
     rc = fpsi::launch_residual(x, hist + 8 * s);
-    if (!rc) rc = fpsi::launch_assemble(x, nullptr);
+    if (!rc) rc = fpsi::launch_assemble(x);
     if (!rc) rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter);
     if (!rc) rc = fpsi::launch_update(x);
   }
@@ -622,7 +644,7 @@ static int run_steps(fpsi_ctx* x, int32_t nsteps, double* hist) {
   int rc = FPSI_OK;
   for (int32_t s = 0; s < nsteps && !rc; ++s) {
     rc = fpsi::launch_residual(x, hist + 8 * s);
-    if (!rc) rc = fpsi::launch_assemble(x, nullptr);
+    if (!rc) rc = fpsi::launch_assemble(x);
     if (!rc) rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter);
     if (!rc) rc = fpsi::launch_update(x);
   }

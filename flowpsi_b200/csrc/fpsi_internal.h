@@ -40,7 +40,21 @@ struct HostMesh {
   int ncolours = 0;
   std::vector<int32_t> colour_off;   // ncolours+1 into colour_cells
   std::vector<int32_t> colour_cells; // cells of each colour, increasing
+  // colour order: ci = position in colour_cells.  The sweeps keep every
+  // per-cell array of one colour contiguous (structure of arrays inside the
+  // colour) and the off-diagonal blocks in slots: slot s of colour k holds,
+  // for each of its n_k cells, the block coupling to the s-th interior
+  // neighbour (upper faces first, then lower faces, as the cell's face list).
+  std::vector<int32_t> ci_of;        // RCM cell -> colour-order index
+  std::vector<int64_t> col_n, col_cb, col_eb, col_m;  // per colour: cells, first ci, first slot, slots
+  std::vector<int32_t> nbr;          // [sum m_k n_k]: ci of the slot's neighbour, -1 = empty
+  int64_t nslots = 0;                // sum m_k n_k
   double vol_tot = 0;
+};
+
+// per-colour description passed to the kernels
+struct ColInfo {
+  int64_t cb, n, eb, m;
 };
 
 int build_host_mesh(const fpsi_mesh* m, HostMesh& h);
@@ -90,9 +104,17 @@ struct fpsi_ctx {
   // implicit system (block type depends on precision)
   void* d_fjp = nullptr;       // [nf][25] TB
   void* d_fjm = nullptr;       // [nf][25] TB
-  void* d_cellblk = nullptr;   // [nc][32] TB : LU(25) B(5) piv(1) pad(1)
   void* d_D = nullptr;         // [nc][25] TB (only when keep_D)
-  void* d_x = nullptr;         // [nc][5] TX
+  // colour-order arrays of the sweeps (see HostMesh)
+  void* d_luc = nullptr;       // per colour [25][n_k] TB: LU factors of fluid_D
+  void* d_bc = nullptr;        // per colour [5][n_k] TB: fluid_B
+  int32_t* d_pv = nullptr;     // [nc] packed pivots, colour order
+  void* d_aoff = nullptr;      // per colour [m_k][25][n_k] TB: off-diagonal blocks
+  int32_t* d_nbr = nullptr;    // per colour [m_k][n_k] neighbour ci
+  int32_t* d_ci = nullptr;     // RCM cell -> ci
+  int32_t* d_ccol = nullptr;   // RCM cell -> colour
+  fpsi::ColInfo* d_colinfo = nullptr;
+  void* d_x = nullptr;         // [nc][5] TX, colour order
   double* d_amin = nullptr;    // per-block min alpha
   int32_t* d_err = nullptr;    // error flags (singular pivots, ...)
   int blk_bytes = 4;           // sizeof(TB)

@@ -7,8 +7,11 @@
 //   F      [nf][5]  FP64  face flux, mev [nf] maxev_f*area
 //   src    [nc][5]  FP64, dtau [nc]
 //   fjp/fjm [nf][25] TB   (TB = float in REF/MIXED precision, double in FP64)
-//   cellblk [nc][32] TB   LU(25) B(5) pivots(1) pad(1)  -- one 128 B line in FP32
-//   x      [nc][5]  TX    iterate (TX = double in FP64/REF, float in MIXED)
+//   sweeps, colour order (ci = position of the cell in its colour's list):
+//     luc  [25][n_k] TB per colour   LU of fluid_D;   bc [5][n_k] TB  fluid_B
+//     aoff [m_k][25][n_k] TB per colour: off-diagonal block of each slot
+//     nbr  [m_k][n_k] int32 per colour: ci of the slot's neighbour
+//     x    [nc][5]  TX (ci order)   (TX = double in FP64/REF, float in MIXED)
 // geometry is SoA: n[3][nf], area[nf], rL[3][nf], rR[3][nf], Minv[6][nc].
 //
 // Every reduction has a fixed order (per-cell loops over a fixed face list,
@@ -441,29 +444,40 @@ __global__ void k_norm_final(const double* __restrict__ part, int nblk,
 // ---------------------------------------------------------------------------
 // face Jacobians fjp (dir +1) and fjm (dir -1), one thread per face
 // ---------------------------------------------------------------------------
+// The 25 entries of each thread's block are staged in shared memory and the
+// CTA's contiguous range of blocks is written back with consecutive threads
+// on consecutive addresses (a thread storing its own 100/200 B block would
+// touch 25 cache lines per instruction across the warp).
+constexpr int JAC_THREADS = 128;
+
 template <class TB>
-__global__ void k_face_jacobian(MeshView M, const double* __restrict__ q,
-                                const double* __restrict__ qb, const double* __restrict__ grad,
-                                const double* __restrict__ phi, Gas g, TB* __restrict__ fjp,
-                                TB* __restrict__ fjm) {
-  const int64_t f = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (f >= M.nf) return;
-  FaceStates s;
-  reconstruct(M, q, qb, grad, phi, f, g.pamb, s);
-  const double nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
-  const double A = M.area[f];
-  const RoeAvg ra = roe_average(s.L, s.R, nx, ny, nz, g, 0.0, 1.0);
-  TB blk[25];
-  jac_roe<TB>(ra, nx, ny, nz, A, g, +1, blk);
-  TB* o = fjp + 25 * f;
-#pragma unroll
-  for (int k = 0; k < 25; ++k) o[k] = blk[k];
-  if (f < M.nfi) {
-    jac_roe<TB>(ra, nx, ny, nz, A, g, -1, blk);
-    o = fjm + 25 * f;
-#pragma unroll
-    for (int k = 0; k < 25; ++k) o[k] = blk[k];
+__global__ void __launch_bounds__(JAC_THREADS)
+k_face_jacobian(MeshView M, const double* __restrict__ q, const double* __restrict__ qb,
+                const double* __restrict__ grad, const double* __restrict__ phi, Gas g,
+                TB* __restrict__ fjp, TB* __restrict__ fjm) {
+  __shared__ TB stage[JAC_THREADS * 25];
+  const int64_t f0 = int64_t(blockIdx.x) * JAC_THREADS;
+  const int64_t f = f0 + threadIdx.x;
+  const int64_t cnt = min(int64_t(JAC_THREADS), M.nf - f0) * 25;
+  const bool live = f < M.nf;
+  RoeAvg ra;
+  double nx = 0, ny = 0, nz = 0, A = 0;
+  if (live) {
+    FaceStates s;
+    reconstruct(M, q, qb, grad, phi, f, g.pamb, s);
+    nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
+    A = M.area[f];
+    ra = roe_average(s.L, s.R, nx, ny, nz, g, 0.0, 1.0);
+    jac_roe<TB>(ra, nx, ny, nz, A, g, +1, stage + 25 * threadIdx.x);
   }
+  __syncthreads();
+  for (int64_t k = threadIdx.x; k < cnt; k += JAC_THREADS) fjp[25 * f0 + k] = stage[k];
+  __syncthreads();
+  if (live && f < M.nfi) jac_roe<TB>(ra, nx, ny, nz, A, g, -1, stage + 25 * threadIdx.x);
+  __syncthreads();
+  // boundary faces have no fjm; their slots are written with whatever the
+  // stage holds and never read
+  for (int64_t k = threadIdx.x; k < cnt; k += JAC_THREADS) fjm[25 * f0 + k] = stage[k];
 }
 
 // ---------------------------------------------------------------------------
@@ -543,45 +557,61 @@ __device__ __forceinline__ void lu5_solve(const TB* A, int pv, TX* y) {
   }
 }
 
-template <class TB>
-struct PivSlot;
-template <>
-struct PivSlot<float> {
-  __device__ static float pack(int v) { return __int_as_float(v); }
-  __device__ static int unpack(float v) { return __float_as_int(v); }
-};
-template <>
-struct PivSlot<double> {
-  __device__ static double pack(int v) { return __longlong_as_double((long long)v); }
-  __device__ static int unpack(double v) { return int(__double_as_longlong(v)); }
-};
-
 // ---------------------------------------------------------------------------
 // diagonal block assembly (srcJ sum, steady fluid_D), LU, B and the block
 // Jacobi start x0 = D^-1 B; one thread per cell
 // ---------------------------------------------------------------------------
+struct SweepView {
+  const int32_t* ci;     // RCM cell -> colour-order index
+  const int32_t* ccol;   // RCM cell -> colour
+  const ColInfo* col;    // per colour
+};
+
+// Also scatters the off-diagonal blocks into the colour-order slots: row c
+// couples to its upper neighbour with U = fjm and to its lower neighbour
+// with L = -fjp (solverLinearSystem.loci:57-77).  Threads run in RCM order;
+// the cells of one colour inside a warp have consecutive colour positions,
+// so every slot store fills whole 32 B sectors.
 template <class TB, class TX>
-__global__ void k_assemble(MeshView M, const double* __restrict__ q,
+__global__ void k_assemble(MeshView M, SweepView S, const double* __restrict__ q,
                            const double* __restrict__ src, const double* __restrict__ dtau,
                            const TB* __restrict__ fjp, const TB* __restrict__ fjm, Gas g,
-                           TB* __restrict__ cellblk, TB* __restrict__ Dout, TX* __restrict__ x,
-                           const double* __restrict__ x0, int32_t* __restrict__ err) {
+                           TB* __restrict__ luc, TB* __restrict__ bcv, int32_t* __restrict__ pvv,
+                           TB* __restrict__ aoff, TB* __restrict__ Dout, TX* __restrict__ x,
+                           int32_t* __restrict__ err) {
   const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (c >= M.nc) return;
+  const int64_t ci = S.ci[c];
+  const ColInfo ck = S.col[S.ccol[c]];
+  const int64_t i = ci - ck.cb, n = ck.n;
   TB sJ[25];
 #pragma unroll
-  for (int i = 0; i < 25; ++i) sJ[i] = TB(0);
+  for (int k = 0; k < 25; ++k) sJ[k] = TB(0);
+  int64_t slot = 0;
   for (int32_t e = M.cf_off[c]; e < M.cf_off[c + 1]; ++e) {
     const int32_t ent = M.cf[e];
     const int64_t f = ent >> 1;
+    const bool interior = f < M.nfi;
+    TB* ao = aoff + 25 * ck.eb + slot * 25 * n + i;
     if (ent & 1) {
       const TB* p = fjm + 25 * f;
+      const TB* l = fjp + 25 * f;
 #pragma unroll
-      for (int i = 0; i < 25; ++i) sJ[i] += p[i];
+      for (int k = 0; k < 25; ++k) {
+        sJ[k] += p[k];
+        ao[k * n] = -l[k];
+      }
+      ++slot;
     } else {
       const TB* p = fjp + 25 * f;
 #pragma unroll
-      for (int i = 0; i < 25; ++i) sJ[i] -= p[i];
+      for (int k = 0; k < 25; ++k) sJ[k] -= p[k];
+      if (interior) {
+        const TB* u = fjm + 25 * f;
+#pragma unroll
+        for (int k = 0; k < 25; ++k) ao[k * n] = u[k];
+        ++slot;
+      }
     }
   }
   TB D[25];
@@ -620,28 +650,42 @@ __global__ void k_assemble(MeshView M, const double* __restrict__ q,
   int pv = 0;
 #pragma unroll
   for (int k = 0; k < 5; ++k) pv |= piv[k] << (3 * k);
-  TB* o = cellblk + 32 * c;
   TB Bv[5];
 #pragma unroll
   for (int k = 0; k < 5; ++k) Bv[k] = TB(src[5 * c + k]);
+  TB* lo = luc + 25 * ck.cb + i;
 #pragma unroll
-  for (int i = 0; i < 25; ++i) o[i] = D[i];
+  for (int k = 0; k < 25; ++k) lo[k * n] = D[k];
+  TB* bo = bcv + 5 * ck.cb + i;
 #pragma unroll
-  for (int k = 0; k < 5; ++k) o[25 + k] = Bv[k];
-  o[30] = PivSlot<TB>::pack(pv);
-  o[31] = TB(0);
+  for (int k = 0; k < 5; ++k) bo[k * n] = Bv[k];
+  pvv[ci] = pv;
+  // block Jacobi start D x = B (linearSolverSGS.loci:57-69)
   TX y[5];
-  if (x0) {
 #pragma unroll
-    for (int k = 0; k < 5; ++k) y[k] = TX(x0[5 * c + k]);
-  } else {
-#pragma unroll
-    for (int k = 0; k < 5; ++k) y[k] = TX(Bv[k]);
-    lu5_solve<TB, TX>(D, pv, y);
-  }
-  TX* xo = x + 5 * c;
+  for (int k = 0; k < 5; ++k) y[k] = TX(Bv[k]);
+  lu5_solve<TB, TX>(D, pv, y);
+  TX* xo = x + 5 * ci;
 #pragma unroll
   for (int k = 0; k < 5; ++k) xo[k] = y[k];
+}
+
+// block Jacobi start alone (a second solve on an assembled system)
+template <class TB, class TX>
+__global__ void k_jacobi_start(int64_t cb, int64_t n, const TB* __restrict__ luc,
+                               const TB* __restrict__ bcv, const int32_t* __restrict__ pvv,
+                               TX* __restrict__ x) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  TB LU[25];
+#pragma unroll
+  for (int k = 0; k < 25; ++k) LU[k] = luc[25 * cb + k * n + i];
+  TX y[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) y[k] = TX(bcv[5 * cb + k * n + i]);
+  lu5_solve<TB, TX>(LU, pvv[cb + i], y);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) x[5 * (cb + i) + k] = y[k];
 }
 
 // ---------------------------------------------------------------------------
@@ -649,49 +693,40 @@ __global__ void k_assemble(MeshView M, const double* __restrict__ q,
 // linearSolverSGS.loci:186-207, 277-298):
 //   x_c = D^-1 (B - sum_upper fjm x_cr + sum_lower fjp x_cl)
 // ---------------------------------------------------------------------------
+// One thread per cell of colour k; every per-cell stream (slots, LU, B,
+// pivots, own iterate) is read with consecutive threads on consecutive
+// addresses; only the neighbours' iterates are gathered.
 template <class TB, class TX>
-__global__ void k_sgs_colour(MeshView M, const int32_t* __restrict__ cells, int32_t ncell,
-                             const TB* __restrict__ cellblk, const TB* __restrict__ fjp,
-                             const TB* __restrict__ fjm, TX* __restrict__ x) {
-  const int32_t i = int32_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= ncell) return;
-  const int64_t c = cells[i];
-  const TB* blk = cellblk + 32 * c;
+__global__ void k_sgs_colour(ColInfo ck, const int32_t* __restrict__ nbr,
+                             const TB* __restrict__ aoff, const TB* __restrict__ luc,
+                             const TB* __restrict__ bcv, const int32_t* __restrict__ pvv,
+                             TX* __restrict__ x) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t n = ck.n;
+  if (i >= n) return;
   TX t[5];
 #pragma unroll
-  for (int k = 0; k < 5; ++k) t[k] = -TX(blk[25 + k]);
-  for (int32_t e = M.cf_off[c]; e < M.cf_off[c + 1]; ++e) {
-    const int32_t ent = M.cf[e];
-    const int64_t f = ent >> 1;
-    if (f >= M.nfi) continue;
-    const TX* xn;
-    const TB* A;
+  for (int k = 0; k < 5; ++k) t[k] = -TX(__ldg(bcv + 5 * ck.cb + k * n + i));
+  for (int64_t s = 0; s < ck.m; ++s) {
+    const int32_t o = __ldg(nbr + ck.eb + s * n + i);
+    if (o < 0) break;
     TX xv[5];
-    if (ent & 1) {
-      xn = x + 5 * int64_t(M.cl[f]);
-      A = fjp + 25 * f;
 #pragma unroll
-      for (int k = 0; k < 5; ++k) xv[k] = -xn[k];
-    } else {
-      xn = x + 5 * int64_t(M.cr[f]);
-      A = fjm + 25 * f;
-#pragma unroll
-      for (int k = 0; k < 5; ++k) xv[k] = xn[k];
-    }
+    for (int k = 0; k < 5; ++k) xv[k] = x[5 * int64_t(o) + k];
+    const TB* A = aoff + 25 * ck.eb + s * 25 * n + i;
 #pragma unroll
     for (int r = 0; r < 5; ++r)
 #pragma unroll
-      for (int j = 0; j < 5; ++j) t[r] += TX(__ldg(A + 5 * r + j)) * xv[j];
+      for (int j = 0; j < 5; ++j) t[r] += TX(__ldg(A + (5 * r + j) * n)) * xv[j];
   }
   TB LU[25];
 #pragma unroll
-  for (int k = 0; k < 25; ++k) LU[k] = __ldg(blk + k);
-  const int pv = PivSlot<TB>::unpack(blk[30]);
+  for (int k = 0; k < 25; ++k) LU[k] = __ldg(luc + 25 * ck.cb + k * n + i);
   TX y[5];
 #pragma unroll
   for (int k = 0; k < 5; ++k) y[k] = -t[k];
-  lu5_solve<TB, TX>(LU, pv, y);
-  TX* xo = x + 5 * c;
+  lu5_solve<TB, TX>(LU, __ldg(pvv + ck.cb + i), y);
+  TX* xo = x + 5 * (ck.cb + i);
 #pragma unroll
   for (int k = 0; k < 5; ++k) xo[k] = y[k];
 }
@@ -700,33 +735,35 @@ __global__ void k_sgs_colour(MeshView M, const int32_t* __restrict__ cells, int3
 // k_assemble and the face blocks)
 template <class TB, class TX>
 __global__ void __launch_bounds__(NORM_THREADS)
-k_linres(MeshView M, const TB* __restrict__ D, const TB* __restrict__ cellblk,
+k_linres(MeshView M, SweepView S, const TB* __restrict__ D, const TB* __restrict__ bcv,
          const TB* __restrict__ fjp, const TB* __restrict__ fjm, const TX* __restrict__ x,
          double* __restrict__ part) {
   const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   double sb = 0, sr = 0;
   if (c < M.nc) {
+    const int64_t ci = S.ci[c];
+    const ColInfo ck = S.col[S.ccol[c]];
     double r[5];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) r[k] = double(cellblk[32 * c + 25 + k]);
+    for (int k = 0; k < 5; ++k) r[k] = double(bcv[5 * ck.cb + k * ck.n + (ci - ck.cb)]);
 #pragma unroll
     for (int k = 0; k < 5; ++k) sb += r[k] * r[k];
 #pragma unroll
     for (int i = 0; i < 5; ++i)
 #pragma unroll
-      for (int j = 0; j < 5; ++j) r[i] -= double(D[25 * c + 5 * i + j]) * double(x[5 * c + j]);
+      for (int j = 0; j < 5; ++j) r[i] -= double(D[25 * c + 5 * i + j]) * double(x[5 * ci + j]);
     for (int32_t e = M.cf_off[c]; e < M.cf_off[c + 1]; ++e) {
       const int32_t ent = M.cf[e];
       const int64_t f = ent >> 1;
       if (f >= M.nfi) continue;
       if (ent & 1) {
-        const TX* xn = x + 5 * int64_t(M.cl[f]);
+        const TX* xn = x + 5 * int64_t(S.ci[M.cl[f]]);
 #pragma unroll
         for (int i = 0; i < 5; ++i)
 #pragma unroll
           for (int j = 0; j < 5; ++j) r[i] += double(fjp[25 * f + 5 * i + j]) * double(xn[j]);
       } else {
-        const TX* xn = x + 5 * int64_t(M.cr[f]);
+        const TX* xn = x + 5 * int64_t(S.ci[M.cr[f]]);
 #pragma unroll
         for (int i = 0; i < 5; ++i)
 #pragma unroll
@@ -766,13 +803,13 @@ __global__ void k_sum2(const double* __restrict__ part, int nblk, double* __rest
 // ---------------------------------------------------------------------------
 template <class TX>
 __global__ void __launch_bounds__(NORM_THREADS)
-k_update(int64_t nc, double pamb, const TX* __restrict__ x, double* __restrict__ q,
+k_update(int64_t nc, double pamb, const int32_t* __restrict__ ci, const TX* __restrict__ x, double* __restrict__ q,
          double* __restrict__ amin_part) {
   const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   double alpha = 1.0;
   if (c < nc) {
     double* qc = q + 5 * c;
-    const TX* d = x + 5 * c;
+    const TX* d = x + 5 * int64_t(ci[c]);
     const double dT = double(d[0]), dp = double(d[4]);
     alpha = dmin(alpha, 0.9 * qc[0] / (fabs(dT) + 1e-30));
     alpha = dmin(alpha, 0.9 * (qc[4] + pamb) / (fabs(dp) + 1e-30));
@@ -916,54 +953,87 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
   return FPSI_OK;
 }
 
+static dev::SweepView sweep_view(const fpsi_ctx* x) {
+  dev::SweepView S;
+  S.ci = x->d_ci;
+  S.ccol = x->d_ccol;
+  S.col = x->d_colinfo;
+  return S;
+}
+
 template <class TB, class TX>
-static int launch_assemble_t(fpsi_ctx* x, const double* d_x0) {
+static int launch_assemble_t(fpsi_ctx* x) {
   const dev::MeshView M = view(x);
   const dev::Gas g = gas(x);
   cudaStream_t s = x->stream;
   TB* fjp = (TB*)x->d_fjp;
   TB* fjm = (TB*)x->d_fjm;
   prof_begin(x, "face_jacobian");
-  dev::k_face_jacobian<TB><<<blocks_for(M.nf, 128), 128, 0, s>>>(M, x->d_q, x->d_qb, x->d_grad,
-                                                                  x->d_phi, g, fjp, fjm);
+  dev::k_face_jacobian<TB><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
+      M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, fjp, fjm);
   prof_end(x);
   prof_begin(x, "assemble_lu");
   dev::k_assemble<TB, TX><<<blocks_for(M.nc, 128), 128, 0, s>>>(
-      M, x->d_q, x->d_src, x->d_dtau, fjp, fjm, g, (TB*)x->d_cellblk,
-      x->keep_D ? (TB*)x->d_D : nullptr, (TX*)x->d_x, d_x0, x->d_err);
+      M, sweep_view(x), x->d_q, x->d_src, x->d_dtau, fjp, fjm, g, (TB*)x->d_luc, (TB*)x->d_bc,
+      x->d_pv, (TB*)x->d_aoff, x->keep_D ? (TB*)x->d_D : nullptr, (TX*)x->d_x, x->d_err);
   prof_end(x);
   FPSI_CUDA_TRY(cudaGetLastError());
   return FPSI_OK;
 }
 
-int launch_assemble(fpsi_ctx* x, const double* d_x0) {
+int launch_assemble(fpsi_ctx* x) {
   switch (x->P.precision) {
     case FPSI_PREC_FP64:
-      return launch_assemble_t<double, double>(x, d_x0);
+      return launch_assemble_t<double, double>(x);
     case FPSI_PREC_MIXED:
-      return launch_assemble_t<float, float>(x, d_x0);
+      return launch_assemble_t<float, float>(x);
     default:
-      return launch_assemble_t<float, double>(x, d_x0);
+      return launch_assemble_t<float, double>(x);
+  }
+}
+
+template <class TB, class TX>
+static int launch_jacobi_t(fpsi_ctx* x) {
+  for (int k = 0; k < x->H.ncolours; ++k) {
+    const int64_t n = x->H.col_n[k];
+    if (n == 0) continue;
+    dev::k_jacobi_start<TB, TX><<<blocks_for(n, 128), 128, 0, x->stream>>>(
+        x->H.col_cb[k], n, (const TB*)x->d_luc, (const TB*)x->d_bc, x->d_pv, (TX*)x->d_x);
+  }
+  FPSI_CUDA_TRY(cudaGetLastError());
+  return FPSI_OK;
+}
+
+int launch_jacobi_start(fpsi_ctx* x) {
+  switch (x->P.precision) {
+    case FPSI_PREC_FP64:
+      return launch_jacobi_t<double, double>(x);
+    case FPSI_PREC_MIXED:
+      return launch_jacobi_t<float, float>(x);
+    default:
+      return launch_jacobi_t<float, double>(x);
   }
 }
 
 template <class TB, class TX>
 static int launch_sgs_t(fpsi_ctx* x, int sweeps) {
-  const dev::MeshView M = view(x);
   cudaStream_t s = x->stream;
   const int T = 128;
-  const auto& off = x->H.colour_off;
   const int K = x->H.ncolours;
   for (int it = 0; it < sweeps; ++it) {
     for (int pass = 0; pass < 2; ++pass)
       for (int kk = 0; kk < K; ++kk) {
         const int k = pass == 0 ? kk : K - 1 - kk;
-        const int32_t n = off[k + 1] - off[k];
-        if (n == 0) continue;
+        ColInfo ck;
+        ck.cb = x->H.col_cb[k];
+        ck.n = x->H.col_n[k];
+        ck.eb = x->H.col_eb[k];
+        ck.m = x->H.col_m[k];
+        if (ck.n == 0) continue;
         prof_begin(x, "sgs_colour");
-        dev::k_sgs_colour<TB, TX><<<blocks_for(n, T), T, 0, s>>>(
-            M, x->d_colour_cells + off[k], n, (const TB*)x->d_cellblk, (const TB*)x->d_fjp,
-            (const TB*)x->d_fjm, (TX*)x->d_x);
+        dev::k_sgs_colour<TB, TX><<<blocks_for(ck.n, T), T, 0, s>>>(
+            ck, x->d_nbr, (const TB*)x->d_aoff, (const TB*)x->d_luc, (const TB*)x->d_bc, x->d_pv,
+            (TX*)x->d_x);
         prof_end(x);
       }
   }
@@ -986,8 +1056,8 @@ template <class TB, class TX>
 static int launch_linres_t(fpsi_ctx* x, double* out2) {
   const dev::MeshView M = view(x);
   dev::k_linres<TB, TX><<<x->nblk_norm, dev::NORM_THREADS, 0, x->stream>>>(
-      M, (const TB*)x->d_D, (const TB*)x->d_cellblk, (const TB*)x->d_fjp, (const TB*)x->d_fjm,
-      (const TX*)x->d_x, x->d_part);
+      M, sweep_view(x), (const TB*)x->d_D, (const TB*)x->d_bc, (const TB*)x->d_fjp,
+      (const TB*)x->d_fjm, (const TX*)x->d_x, x->d_part);
   dev::k_sum2<<<1, dev::NORM_THREADS, 0, x->stream>>>(x->d_part, x->nblk_norm, out2);
   FPSI_CUDA_TRY(cudaGetLastError());
   return FPSI_OK;
@@ -1009,10 +1079,10 @@ int launch_update(fpsi_ctx* x) {
   prof_begin(x, "update");
   if (x->P.precision == FPSI_PREC_MIXED)
     dev::k_update<float><<<x->nblk_norm, dev::NORM_THREADS, 0, x->stream>>>(
-        nc, x->P.Pambient, (const float*)x->d_x, x->d_q, x->d_amin);
+        nc, x->P.Pambient, x->d_ci, (const float*)x->d_x, x->d_q, x->d_amin);
   else
     dev::k_update<double><<<x->nblk_norm, dev::NORM_THREADS, 0, x->stream>>>(
-        nc, x->P.Pambient, (const double*)x->d_x, x->d_q, x->d_amin);
+        nc, x->P.Pambient, x->d_ci, (const double*)x->d_x, x->d_q, x->d_amin);
   prof_end(x);
   FPSI_CUDA_TRY(cudaGetLastError());
   return FPSI_OK;

@@ -12,8 +12,10 @@ namespace fpsi {
 // gather (src, dtau), norms into resid_slot[8] (device)
 int launch_residual(fpsi_ctx* x, double* resid_slot);
 // face Jacobians, diagonal blocks, LU, B and the starting iterate
-// (d_x0 == nullptr: block Jacobi start D^-1 B)
-int launch_assemble(fpsi_ctx* x, const double* d_x0);
+// (the starting iterate is the block Jacobi start D^-1 B)
+int launch_assemble(fpsi_ctx* x);
+// block Jacobi start x = D^-1 B on an assembled system
+int launch_jacobi_start(fpsi_ctx* x);
 // `sweeps` symmetric multi-colour Gauss-Seidel sweeps on the device iterate
 int launch_sgs(fpsi_ctx* x, int sweeps);
 // out2[0] = ||B||, out2[1] = ||B - A x|| (device)

@@ -373,6 +373,44 @@ int build_host_mesh(const fpsi_mesh* m, HostMesh& h) {
     std::vector<int32_t> pos(h.colour_off.begin(), h.colour_off.end() - 1);
     for (int64_t c = 0; c < nc; ++c) h.colour_cells[pos[h.colour[c]]++] = int32_t(c);
   }
+  // ---- colour-order slot structure for the sweeps ----
+  h.ci_of.assign(nc, 0);
+  for (int64_t j = 0; j < nc; ++j) h.ci_of[h.colour_cells[j]] = int32_t(j);
+  h.col_n.assign(ncol, 0);
+  h.col_cb.assign(ncol, 0);
+  h.col_eb.assign(ncol, 0);
+  h.col_m.assign(ncol, 0);
+  auto ninterior = [&](int64_t c) {
+    int32_t k = 0;
+    for (int32_t e = h.cf_off[c]; e < h.cf_off[c + 1]; ++e)
+      if (h.cr[h.cf[e] >> 1] >= 0) ++k;
+    return k;
+  };
+  int64_t eb = 0;
+  for (int k = 0; k < ncol; ++k) {
+    h.col_cb[k] = h.colour_off[k];
+    h.col_n[k] = h.colour_off[k + 1] - h.colour_off[k];
+    int64_t m = 0;
+    for (int32_t j = h.colour_off[k]; j < h.colour_off[k + 1]; ++j)
+      m = std::max<int64_t>(m, ninterior(h.colour_cells[j]));
+    h.col_m[k] = m;
+    h.col_eb[k] = eb;
+    eb += m * h.col_n[k];
+  }
+  h.nslots = eb;
+  h.nbr.assign(size_t(eb), -1);
+  for (int k = 0; k < ncol; ++k)
+    for (int64_t i = 0; i < h.col_n[k]; ++i) {
+      const int32_t c = h.colour_cells[h.col_cb[k] + i];
+      int64_t s = 0;
+      for (int32_t e = h.cf_off[c]; e < h.cf_off[c + 1]; ++e) {
+        const int64_t f = h.cf[e] >> 1;
+        if (h.cr[f] < 0) continue;
+        const int32_t o = (h.cf[e] & 1) ? h.cl[f] : h.cr[f];
+        h.nbr[h.col_eb[k] + s * h.col_n[k] + i] = h.ci_of[o];
+        ++s;
+      }
+    }
   return FPSI_OK;
 }
 
