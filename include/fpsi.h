@@ -240,6 +240,24 @@ int fpsi_run_timed(fpsi_ctx* ctx, int32_t nsteps, fpsi_resid* norms, double* dev
 int fpsi_kernel_times(fpsi_ctx* ctx, int32_t nsteps, int32_t cap, char* names, double* ms,
                       int64_t* launches, int32_t* count);
 
+/* ---- residual norms without allocation -----------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (a host code that hands out device buffers from its own pool and forbids
+ * allocations behind it, or a step that must not block or fail on an
+ * allocation): the norms of fpsi_residual computed from caller-owned device
+ * buffers -- d_src (nc*5 doubles, the 'src' store), d_vol (nc doubles) --
+ * into d_out (8 doubles: rtrms, etrms, mtrms, rtmax, cell of rtmax, etmax,
+ * cell of etmax, mtmax).  stream is a cudaStream_t or NULL.
+ * Allocates nothing: the block partials live in a static 1 MiB __device__
+ * array that every GPU loading the library keeps until exit, so nc is
+ * limited to 16,777,216 cells (larger sizes return FPSI_E_INVALID).  The
+ * first call on a device looks the array's address up (no allocation);
+ * make that first call before any stream capture.  Every call overwrites
+ * the partials it reads, so nothing must start at zero; calls that overlap
+ * on the GPU share the array and race. */
+int fpsi_residual_norms_noalloc(const double* d_src, const double* d_vol, int64_t nc,
+                                double vol_tot, double* d_out, void* stream);
+
 /* ---- face functions on batches (inviscidFlux.h entry points) --------------
  * States are packed per face as [pg, T, u, v, w] (n*5), normals n*3 (unit),
  * area n.  Host pointers; copies and one kernel launch inside. */
