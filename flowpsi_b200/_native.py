@@ -106,6 +106,8 @@ _SIGS = {
                             C.POINTER(C.c_int64)]),
     "fpsi_get_geometry": (C.c_int, [_ctx, _dp, _dp, _dp, _dp, _dp]),
     "fpsi_get_colours": (C.c_int, [_ctx, _ip]),
+    "fpsi_set_lines": (C.c_int, [_ctx, C.c_int64, C.POINTER(C.c_int64), _ip]),
+    "fpsi_get_lines": (C.c_int, [_ctx, _ip, _ip, _ip, C.POINTER(C.c_int64)]),
     "fpsi_set_state": (C.c_int, [_ctx, _dp, _dp, _dp]),
     "fpsi_get_state": (C.c_int, [_ctx, _dp, _dp, _dp]),
     "fpsi_residual": (C.c_int, [_ctx, _dp, C.POINTER(Resid)]),

@@ -117,6 +117,38 @@ def taylor_green_tets(n: int = 128, seed: int = 0, sweeps: int = 8, jitter: floa
     return Case(f"taylor_green_tets_{n}", mesh, params, 200, init)
 
 
+def boundary_layer_block(nx: int = 256, ny: int = 128, nz: int = 64, dy0: float = 1e-6,
+                         growth: float = 1.15, seed: int = 0,
+                         precision: str = "mixed", solver: str = "lsgs",
+                         wall: str = "reflecting", Lx: float = 1.0, Lz: float = 0.25) -> Case:
+    """Flat-plate block: x streamwise, y wall-normal (first spacing dy0,
+    geometric growth), z spanwise periodic; wall at y = 0, farfield at the
+    top, inflow and outflow sides.  M=0.3, T=300 K, p=1e5 Pa.  The
+    wall-normal columns are the LSGS lines (case.lines)."""
+    T0, p0, M = 300.0, 1e5, 0.3
+    U0 = M * math.sqrt(GAMMA * RTILDE * T0)
+    ff = bc("farfield", T=T0, pg=p0, u=(U0, 0.0, 0.0))
+    wl = bc(wall, T=T0, pg=p0)
+    mesh = GeneratedMesh("bl", n=(nx, ny, nz), L=(Lx, 1.0, Lz), dy0=dy0, growth=growth,
+                         bc_side=(0, 0, 1, 0, -1, -1), bcs=[ff, wl])
+    params = default_params(flux="roe", limiter="venkatakrishnan", solver=solver,
+                            gauss_seidel_iter=8, cflmax=50.0, precision=precision)
+
+    def init(cc):
+        nc = cc.shape[0]
+        u = np.zeros((nc, 3))
+        u[:, 0] = U0 * (1.0 + 0.01 * normal(seed, 2, nc))
+        u[:, 1] = 0.01 * U0 * normal(seed, 3, nc)
+        u[:, 2] = 0.01 * U0 * normal(seed, 4, nc)
+        p = p0 * (1.0 + 0.01 * normal(seed, 1, nc))
+        T = T0 * (1.0 + 0.01 * normal(seed, 0, nc))
+        return T, p, u
+
+    c = Case(f"boundary_layer_{nx}x{ny}x{nz}", mesh, params, 100, init)
+    c.lines = mesh.lines_along(1)
+    return c
+
+
 def oblique_shock_cube(n: int = 256, seed: int = 0, sweeps: int = 8, precision: str = "mixed",
                        flux: str = "hlle", limiter: str = "barth") -> Case:
     T1, p1, M1 = 300.0, 1e5, 2.0

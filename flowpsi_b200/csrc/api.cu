@@ -87,8 +87,9 @@ int alloc_system(fpsi_ctx* x) {
   int rc;
   if ((rc = dalloc(x, (char**)&x->d_fjp, nf * 25 * tb))) return rc;
   if ((rc = dalloc(x, (char**)&x->d_fjm, nf * 25 * tb))) return rc;
-  if ((rc = dalloc(x, (char**)&x->d_luc, nc * 25 * tb))) return rc;
-  if ((rc = dalloc(x, (char**)&x->d_bc, nc * 5 * tb))) return rc;
+  const size_t ncp = size_t(x->H.ncp);
+  if ((rc = dalloc(x, (char**)&x->d_luc, ncp * 25 * tb))) return rc;
+  if ((rc = dalloc(x, (char**)&x->d_bc, ncp * 5 * tb))) return rc;
   if ((rc = dalloc(x, &x->d_pv, nc))) return rc;
   if ((rc = dalloc(x, (char**)&x->d_aoff, size_t(x->H.nslots) * 25 * tb))) return rc;
   if (x->keep_D)
@@ -98,6 +99,58 @@ int alloc_system(fpsi_ctx* x) {
   x->have_asm = x->have_dq = false;
   return FPSI_OK;
 }
+
+void free_lsgs(fpsi_ctx* x) {
+  void* ps[] = {x->d_lt, x->d_lonbr, x->d_llen, x->d_lrole, x->d_lrow0, x->d_lD, x->d_lL,
+                x->d_lU, x->d_lF, x->d_lB, x->d_lrhs, x->d_lx, x->d_lxt, x->d_lctl, x->d_lpart};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  x->d_lt = x->d_lonbr = x->d_llen = nullptr;
+  x->d_lrole = nullptr;
+  x->d_lrow0 = nullptr;
+  x->d_lD = x->d_lL = x->d_lU = x->d_lF = x->d_lB = x->d_lrhs = x->d_lx = x->d_lxt = nullptr;
+  x->d_lctl = nullptr;
+  x->d_lpart = nullptr;
+  x->lsgs_prec = -1;
+}
+
+// device arrays of the line solver for the current line layout and precision
+int alloc_lsgs(fpsi_ctx* x) {
+  if (x->P.solver != FPSI_SOLVER_LSGS) return FPSI_OK;
+  int rc;
+  if (!x->LY.built && (rc = fpsi::build_lines(x, nullptr))) return rc;
+  if (x->lsgs_prec == x->P.precision && x->d_lt) return FPSI_OK;
+  free_lsgs(x);
+  const fpsi::LineLayout& Y = x->LY;
+  const int tb = x->P.precision == FPSI_PREC_FP64 ? 8 : 4;
+  const int td = x->P.precision == FPSI_PREC_MIXED ? 4 : 8;
+  const int tx = td;
+  const size_t nt = size_t(Y.nrows) * 32;
+  if ((rc = upload(x, &x->d_lt, Y.t_of))) return rc;
+  if ((rc = upload(x, &x->d_lrole, Y.role))) return rc;
+  if ((rc = upload(x, &x->d_lonbr, Y.onbr))) return rc;
+  if ((rc = upload(x, &x->d_llen, Y.lane_len))) return rc;
+  if ((rc = upload(x, &x->d_lrow0, Y.grp_row0))) return rc;
+  if ((rc = dalloc(x, (char**)&x->d_lD, nt * 25 * td))) return rc;
+  if ((rc = dalloc(x, (char**)&x->d_lL, nt * 25 * tb))) return rc;
+  if ((rc = dalloc(x, (char**)&x->d_lU, nt * 25 * tb))) return rc;
+  if ((rc = dalloc(x, (char**)&x->d_lF, nt * size_t(Y.mout) * 25 * tb))) return rc;
+  if ((rc = dalloc(x, (char**)&x->d_lB, nt * 5 * tb))) return rc;
+  if ((rc = dalloc(x, (char**)&x->d_lrhs, nt * 5 * tx))) return rc;
+  if ((rc = dalloc(x, (char**)&x->d_lx, nt * 5 * tx))) return rc;
+  if ((rc = dalloc(x, (char**)&x->d_lxt, nt * 5 * tx))) return rc;
+  if ((rc = dalloc(x, (char**)&x->d_lctl, 64))) return rc;
+  if ((rc = dalloc(x, &x->d_lpart, (nt + 255) / 256 + 1))) return rc;
+  // padding cells must read as zero in the relaxation and the residual
+  FPSI_CUDA_TRY(cudaMemset(x->d_lx, 0, nt * 5 * tx));
+  FPSI_CUDA_TRY(cudaMemset(x->d_lxt, 0, nt * 5 * tx));
+  FPSI_CUDA_TRY(cudaMemset(x->d_lB, 0, nt * 5 * tb));
+  x->lsgs_prec = x->P.precision;
+  x->keep_D = true;  // the line preprocessing starts from the unfactored blocks
+  return FPSI_OK;
+}
+
+bool is_lsgs(const fpsi_ctx* x) { return x->P.solver == FPSI_SOLVER_LSGS; }
 
 int check_params(const fpsi_params* p) {
   if (!p) return FPSI_E_INVALID;
@@ -110,9 +163,13 @@ int check_params(const fpsi_params* p) {
     fpsi::set_error("low-Mach preconditioning (Minf < 0.5) is not on the device path");
     return FPSI_E_UNSUPPORTED;
   }
-  if (p->solver != FPSI_SOLVER_SGS) {
-    fpsi::set_error("fluidLinearSolver: only 'sgs' is available on this build");
-    return FPSI_E_UNSUPPORTED;
+  if (p->solver != FPSI_SOLVER_SGS && p->solver != FPSI_SOLVER_LSGS) {
+    fpsi::set_error("fluidLinearSolver: 'sgs' or 'lsgs'");
+    return FPSI_E_INVALID;
+  }
+  if (p->solver == FPSI_SOLVER_LSGS && (p->lsgs_max_iter < 0 || !(p->lsgs_relaxation > 0))) {
+    fpsi::set_error("LSGS controls out of range");
+    return FPSI_E_INVALID;
   }
   if (p->viscous != 0) {
     fpsi::set_error("viscous fluxes are not available on this build");
@@ -210,6 +267,7 @@ int fpsi_device_available(void) {
 int fpsi_destroy(fpsi_ctx* x) {
   if (!x) return FPSI_OK;
   free_system(x);
+  free_lsgs(x);
   void* ps[] = {x->d_cl, x->d_cr, x->d_n, x->d_area, x->d_rL, x->d_rR, x->d_vol, x->d_cc,
                 x->d_Minv, x->d_cf_off, x->d_cf, x->d_colour_cells, x->d_bcs, x->d_q,
                 x->d_qb, x->d_grad, x->d_phi, x->d_F, x->d_mev, x->d_src, x->d_dtau,
@@ -291,7 +349,8 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
   {
     std::vector<fpsi::ColInfo> ci(H.ncolours);
     for (int k = 0; k < H.ncolours; ++k)
-      ci[k] = fpsi::ColInfo{H.col_cb[k], H.col_n[k], H.col_eb[k], H.col_m[k]};
+      ci[k] = fpsi::ColInfo{H.col_cb[k], H.col_n[k], H.col_m[k], H.col_ld[k], H.col_cbp[k],
+                            H.col_ebp[k]};
     TRY(upload(x, &x->d_colinfo, ci));
   }
   TRY(dalloc(x, &x->d_stage, nc * 5));
@@ -317,7 +376,9 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
     fpsi_destroy(x);
     return FPSI_E_CUDA;
   }
+  if (params->solver == FPSI_SOLVER_LSGS) x->keep_D = true;
   TRY(alloc_system(x));
+  TRY(alloc_lsgs(x));
 #undef TRY
   *out = x;
   return FPSI_OK;
@@ -329,7 +390,13 @@ int fpsi_set_params(fpsi_ctx* x, const fpsi_params* p) {
   if (rc) return rc;
   x->P = *p;
   x->have_asm = x->have_dq = false;
-  return alloc_system(x);
+  if (is_lsgs(x) && !x->keep_D) {
+    x->keep_D = true;
+    x->alloc_prec = -1;
+  }
+  rc = alloc_system(x);
+  if (rc) return rc;
+  return alloc_lsgs(x);
 }
 
 int fpsi_info(fpsi_ctx* x, int64_t* nc, int64_t* nf, int32_t* ncol, int64_t* bytes) {
@@ -355,6 +422,53 @@ int fpsi_get_geometry(fpsi_ctx* x, double* vol, double* cellcenter, double* face
 int fpsi_get_colours(fpsi_ctx* x, int32_t* colour) {
   if (!x || !colour) return FPSI_E_INVALID;
   unpermute_cells(x, x->H.colour.data(), 1, colour);
+  return FPSI_OK;
+}
+
+int fpsi_set_lines(fpsi_ctx* x, int64_t nlines, const int64_t* line_off,
+                   const int32_t* line_cells) {
+  if (!x || nlines < 0 || (nlines > 0 && (!line_off || !line_cells))) return FPSI_E_INVALID;
+  std::vector<std::vector<int32_t>> lines(nlines);
+  for (int64_t l = 0; l < nlines; ++l) {
+    if (line_off[l + 1] < line_off[l]) return FPSI_E_INVALID;
+    for (int64_t k = line_off[l]; k < line_off[l + 1]; ++k) {
+      const int32_t c = line_cells[k];
+      if (c < 0 || c >= x->H.nc) {
+        fpsi::set_error("fpsi_set_lines: cell %d out of range", c);
+        return FPSI_E_INVALID;
+      }
+      lines[l].push_back(x->H.iperm[c]);
+    }
+  }
+  int rc = fpsi::build_lines(x, &lines);
+  if (rc) return rc;
+  x->lsgs_prec = -1;
+  x->have_asm = x->have_dq = false;
+  return alloc_lsgs(x);
+}
+
+int fpsi_get_lines(fpsi_ctx* x, int32_t* line_of_cell, int32_t* position, int32_t* line_colour,
+                   int64_t* nlines) {
+  if (!x) return FPSI_E_INVALID;
+  if (!x->LY.built) {
+    int rc = fpsi::build_lines(x, nullptr);
+    if (rc) return rc;
+  }
+  const fpsi::LineLayout& Y = x->LY;
+  if (nlines) *nlines = Y.nlines;
+  for (int64_t i = 0; i < x->H.nc; ++i) {
+    const int64_t c = x->H.perm[i];
+    if (line_of_cell) line_of_cell[c] = Y.line_of[i];
+    if (position) {
+      // position along the line from the padded row of the cell
+      const int64_t t = Y.t_of[i], r = t / 32, g_lane = t % 32;
+      int64_t g = std::upper_bound(Y.grp_row0.begin(), Y.grp_row0.end(), r) - Y.grp_row0.begin() - 1;
+      (void)g_lane;
+      position[c] = int32_t(r - Y.grp_row0[g]);
+    }
+  }
+  if (line_colour)
+    for (int64_t l = 0; l < Y.nlines; ++l) line_colour[l] = Y.line_colour[l];
   return FPSI_OK;
 }
 
@@ -385,6 +499,7 @@ int fpsi_get_state(fpsi_ctx* x, double* T, double* pg, double* u) {
 
 int fpsi_keep_blocks(fpsi_ctx* x, int32_t keep) {
   if (!x) return FPSI_E_INVALID;
+  if (is_lsgs(x)) return keep ? FPSI_OK : FPSI_E_UNSUPPORTED;  // lines need fluid_D
   if (bool(keep) == x->keep_D) return FPSI_OK;
   x->keep_D = keep != 0;
   x->alloc_prec = -1;  // reallocate the system arrays
@@ -456,6 +571,7 @@ int fpsi_assemble(fpsi_ctx* x) {
   if (!x->have_resid) return FPSI_E_STATE;
   int rc = fpsi::launch_assemble(x);
   if (rc) return rc;
+  if (is_lsgs(x) && (rc = fpsi::lsgs_assemble(x))) return rc;
   if ((rc = finish_assemble(x))) return rc;
   x->have_asm = true;
   x->have_dq = false;
@@ -489,7 +605,7 @@ int fpsi_get_blocks(fpsi_ctx* x, void* D, void* fjp, void* fjm, void* B) {
     }
   }
   if (B) {
-    h.resize(size_t(nc) * 5 * tb);
+    h.resize(size_t(x->H.ncp) * 5 * tb);
     FPSI_CUDA_TRY(cudaMemcpy(h.data(), x->d_bc, h.size(), cudaMemcpyDeviceToHost));
     const HostMesh& H = x->H;
     for (int k = 0; k < H.ncolours; ++k)
@@ -497,7 +613,8 @@ int fpsi_get_blocks(fpsi_ctx* x, void* D, void* fjp, void* fjm, void* B) {
         const int64_t c = H.colour_cells[H.col_cb[k] + i];
         char* o = (char*)B + size_t(H.perm[c]) * 5 * tb;
         for (int j = 0; j < 5; ++j)
-          std::memcpy(o + j * tb, h.data() + (size_t(5 * H.col_cb[k]) + j * H.col_n[k] + i) * tb, tb);
+          std::memcpy(o + j * tb, h.data() + (size_t(5 * H.col_cbp[k]) + j * H.col_ld[k] + i) * tb,
+                      tb);
       }
   }
   return FPSI_OK;
@@ -505,6 +622,20 @@ int fpsi_get_blocks(fpsi_ctx* x, void* D, void* fjp, void* fjm, void* B) {
 
 static int upload_x(fpsi_ctx* x, const double* x0) {
   const int64_t nc = x->H.nc;
+  if (is_lsgs(x)) {
+    const size_t nt = size_t(x->LY.nrows) * 32;
+    std::vector<double> v(5 * nt, 0.0);
+    for (int64_t i = 0; i < nc; ++i)
+      for (int k = 0; k < 5; ++k)
+        v[5 * int64_t(x->LY.t_of[i]) + k] = x0[5 * int64_t(x->H.perm[i]) + k];
+    if (x->x_bytes == 8 && x->P.precision != FPSI_PREC_MIXED) {
+      FPSI_CUDA_TRY(cudaMemcpy(x->d_lx, v.data(), v.size() * 8, cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> f(v.begin(), v.end());
+      FPSI_CUDA_TRY(cudaMemcpy(x->d_lx, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+    }
+    return FPSI_OK;
+  }
   if (x->x_bytes == 8) {
     std::vector<double> v(5 * nc);
     for (int64_t i = 0; i < nc; ++i)
@@ -523,6 +654,21 @@ static int upload_x(fpsi_ctx* x, const double* x0) {
 
 static int download_x(fpsi_ctx* x, double* dq) {
   const int64_t nc = x->H.nc;
+  if (is_lsgs(x)) {
+    const size_t nt = size_t(x->LY.nrows) * 32;
+    std::vector<double> v(5 * nt);
+    if (x->P.precision != FPSI_PREC_MIXED) {
+      FPSI_CUDA_TRY(cudaMemcpy(v.data(), x->d_lx, v.size() * 8, cudaMemcpyDeviceToHost));
+    } else {
+      std::vector<float> f(5 * nt);
+      FPSI_CUDA_TRY(cudaMemcpy(f.data(), x->d_lx, f.size() * 4, cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < f.size(); ++i) v[i] = f[i];
+    }
+    for (int64_t i = 0; i < nc; ++i)
+      for (int k = 0; k < 5; ++k)
+        dq[5 * int64_t(x->H.perm[i]) + k] = v[5 * int64_t(x->LY.t_of[i]) + k];
+    return FPSI_OK;
+  }
   std::vector<double> v(5 * nc);
   if (x->x_bytes == 8) {
     FPSI_CUDA_TRY(cudaMemcpy(v.data(), x->d_x, v.size() * 8, cudaMemcpyDeviceToHost));
@@ -541,6 +687,25 @@ int fpsi_linear_solve(fpsi_ctx* x, const double* x0, double* dq, fpsi_lsinfo* in
   if (!x) return FPSI_E_INVALID;
   if (!x->have_asm) return FPSI_E_STATE;
   int rc;
+  if (is_lsgs(x)) {
+    if (x0 && (rc = upload_x(x, x0))) return rc;
+    if ((rc = fpsi::lsgs_solve(x, x0 == nullptr))) return rc;
+    struct {
+      double w, zero, resid;
+      int32_t iter, done;
+    } ctl;
+    FPSI_CUDA_TRY(cudaMemcpyAsync(&ctl, x->d_lctl, sizeof(ctl), cudaMemcpyDeviceToHost, x->stream));
+    if ((rc = finish_assemble(x))) return rc;
+    x->have_dq = true;
+    if (dq && (rc = download_x(x, dq))) return rc;
+    if (info) {
+      info->iterations = ctl.iter;
+      info->status = FPSI_OK;
+      info->resid0 = ctl.zero;
+      info->resid = ctl.resid;
+    }
+    return FPSI_OK;
+  }
   if (x0) {
     if ((rc = upload_x(x, x0))) return rc;
   } else if (x->have_dq) {
@@ -591,7 +756,12 @@ int fpsi_newton_step(fpsi_ctx* x, fpsi_stepinfo* info) {
   int rc;
   if ((rc = fpsi::launch_residual(x, x->d_resid))) return rc;
   if ((rc = fpsi::launch_assemble(x))) return rc;
-  if ((rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter))) return rc;
+  if (is_lsgs(x)) {
+    if ((rc = fpsi::lsgs_assemble(x))) return rc;
+    if ((rc = fpsi::lsgs_solve(x, true))) return rc;
+  } else if ((rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter))) {
+    return rc;
+  }
   if ((rc = fpsi::launch_update(x))) return rc;
   FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid, x->d_resid, 8 * sizeof(double),
                                 cudaMemcpyDeviceToHost, x->stream));
@@ -621,7 +791,12 @@ int fpsi_run(fpsi_ctx* x, int32_t nsteps, fpsi_resid* norms) {
   for (int32_t s = 0; s < nsteps && !rc; ++s) {
     rc = fpsi::launch_residual(x, hist + 8 * s);
     if (!rc) rc = fpsi::launch_assemble(x);
-    if (!rc) rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter);
+    if (!rc && is_lsgs(x)) {
+      rc = fpsi::lsgs_assemble(x);
+      if (!rc) rc = fpsi::lsgs_solve(x, true);
+    } else if (!rc) {
+      rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter);
+    }
     if (!rc) rc = fpsi::launch_update(x);
   }
   std::vector<double> h(size_t(nsteps) * 8);
@@ -645,7 +820,12 @@ static int run_steps(fpsi_ctx* x, int32_t nsteps, double* hist) {
   for (int32_t s = 0; s < nsteps && !rc; ++s) {
     rc = fpsi::launch_residual(x, hist + 8 * s);
     if (!rc) rc = fpsi::launch_assemble(x);
-    if (!rc) rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter);
+    if (!rc && is_lsgs(x)) {
+      rc = fpsi::lsgs_assemble(x);
+      if (!rc) rc = fpsi::lsgs_solve(x, true);
+    } else if (!rc) {
+      rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter);
+    }
     if (!rc) rc = fpsi::launch_update(x);
   }
   return rc;

@@ -45,19 +45,46 @@ struct HostMesh {
   // colour) and the off-diagonal blocks in slots: slot s of colour k holds,
   // for each of its n_k cells, the block coupling to the s-th interior
   // neighbour (upper faces first, then lower faces, as the cell's face list).
+  // Every structure-of-arrays row of a colour has a leading dimension ld_k
+  // = n_k rounded up to 32, so a warp's 32 consecutive cells read whole
+  // aligned 128 B lines (FP32) and no DRAM burst straddles two rows.
   std::vector<int32_t> ci_of;        // RCM cell -> colour-order index
-  std::vector<int64_t> col_n, col_cb, col_eb, col_m;  // per colour: cells, first ci, first slot, slots
-  std::vector<int32_t> nbr;          // [sum m_k n_k]: ci of the slot's neighbour, -1 = empty
-  int64_t nslots = 0;                // sum m_k n_k
+  std::vector<int64_t> col_n, col_cb, col_m, col_ld, col_cbp, col_ebp;
+  std::vector<int32_t> nbr;          // padded slots: ci of the slot's neighbour, -1 = empty
+  int64_t ncp = 0;                   // sum ld_k  (padded cells)
+  int64_t nslots = 0;                // sum m_k ld_k  (padded slots)
   double vol_tot = 0;
 };
 
-// per-colour description passed to the kernels
+// per-colour description passed to the kernels: cb = first ci of the colour
+// (iterate, pivots), n cells, m slots per cell, ld row stride, cbp and ebp
+// padded bases of the per-cell rows and of the slots
 struct ColInfo {
-  int64_t cb, n, eb, m;
+  int64_t cb, n, m, ld, cbp, ebp;
 };
 
 int build_host_mesh(const fpsi_mesh* m, HostMesh& h);
+
+// Line structure of the line-SGS solver.  Lines are coloured (no two lines
+// of one colour couple) and packed 32 to a group; a group's cells are stored
+// position-major: cell p of lane l of group g sits at t = (row0_g + p)*32 + l,
+// so the 32 threads walking the group's lines read coalesced rows.
+struct LineLayout {
+  bool built = false;
+  int64_t nlines = 0, ngroups = 0, nrows = 0;   // nrows = sum of group lengths
+  int ncolours = 0;
+  std::vector<int64_t> col_goff;   // ncolours+1: groups of colour k
+  std::vector<int64_t> grp_row0;   // per group: first row
+  std::vector<int32_t> grp_len;    // per group: longest line
+  std::vector<int32_t> lane_len;   // per group*32+lane: line length (0 = empty lane)
+  std::vector<int32_t> t_of;       // RCM cell -> t
+  std::vector<int32_t> c_of_t;     // t -> RCM cell, -1 for padding
+  std::vector<int8_t> role;        // per cf entry: 0 boundary, 1 prev, 2 next, 3+s outer slot s
+  int mout = 0;                    // outer slots per cell
+  std::vector<int32_t> onbr;       // [(row*mout + s)*32 + lane]: t of the outer neighbour or -1
+  std::vector<int32_t> line_of;    // RCM cell -> line id (caller-visible order)
+  std::vector<int32_t> line_colour;  // per line id
+};
 
 template <class T>
 struct DevBuf {
@@ -126,6 +153,16 @@ struct fpsi_ctx {
   // caller-order staging for state transfers (T, pg, u) and the permutation
   int32_t* d_perm = nullptr;   // new cell id -> caller cell id
   double* d_stage = nullptr;   // [nc] T, [nc] pg, [3 nc] u (caller order)
+  // line SGS (solver == LSGS)
+  fpsi::LineLayout LY;
+  int32_t *d_lt = nullptr, *d_lonbr = nullptr, *d_llen = nullptr;
+  int8_t* d_lrole = nullptr;
+  int64_t* d_lrow0 = nullptr;
+  void *d_lD = nullptr, *d_lL = nullptr, *d_lU = nullptr, *d_lF = nullptr, *d_lB = nullptr;
+  void *d_lrhs = nullptr, *d_lx = nullptr, *d_lxt = nullptr;
+  void* d_lctl = nullptr;
+  double* d_lpart = nullptr;
+  int lsgs_prec = -1;
   // per-kernel timing (fpsi_kernel_times)
   bool profiling = false;
   std::vector<fpsi_prof_rec> prof;
@@ -136,4 +173,8 @@ struct fpsi_ctx {
 namespace fpsi {
 void prof_begin(fpsi_ctx* x, const char* name);
 void prof_end(fpsi_ctx* x);
+// line SGS: layout from caller lines (RCM ids) or the default rule
+int build_lines(fpsi_ctx* x, const std::vector<std::vector<int32_t>>* lines);
+int lsgs_assemble(fpsi_ctx* x);
+int lsgs_solve(fpsi_ctx* x, bool jacobi_start);
 }  // namespace fpsi

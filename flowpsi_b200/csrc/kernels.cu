@@ -583,7 +583,7 @@ __global__ void k_assemble(MeshView M, SweepView S, const double* __restrict__ q
   if (c >= M.nc) return;
   const int64_t ci = S.ci[c];
   const ColInfo ck = S.col[S.ccol[c]];
-  const int64_t i = ci - ck.cb, n = ck.n;
+  const int64_t i = ci - ck.cb, ld = ck.ld;
   TB sJ[25];
 #pragma unroll
   for (int k = 0; k < 25; ++k) sJ[k] = TB(0);
@@ -592,14 +592,15 @@ __global__ void k_assemble(MeshView M, SweepView S, const double* __restrict__ q
     const int32_t ent = M.cf[e];
     const int64_t f = ent >> 1;
     const bool interior = f < M.nfi;
-    TB* ao = aoff + 25 * ck.eb + slot * 25 * n + i;
+    TB* ao = aoff ? aoff + 25 * ck.ebp + slot * 25 * ld + i : nullptr;
     if (ent & 1) {
       const TB* p = fjm + 25 * f;
-      const TB* l = fjp + 25 * f;
 #pragma unroll
-      for (int k = 0; k < 25; ++k) {
-        sJ[k] += p[k];
-        ao[k * n] = -l[k];
+      for (int k = 0; k < 25; ++k) sJ[k] += p[k];
+      if (ao) {
+        const TB* l = fjp + 25 * f;
+#pragma unroll
+        for (int k = 0; k < 25; ++k) ao[k * ld] = -l[k];
       }
       ++slot;
     } else {
@@ -607,9 +608,11 @@ __global__ void k_assemble(MeshView M, SweepView S, const double* __restrict__ q
 #pragma unroll
       for (int k = 0; k < 25; ++k) sJ[k] -= p[k];
       if (interior) {
-        const TB* u = fjm + 25 * f;
+        if (ao) {
+          const TB* u = fjm + 25 * f;
 #pragma unroll
-        for (int k = 0; k < 25; ++k) ao[k * n] = u[k];
+          for (int k = 0; k < 25; ++k) ao[k * ld] = u[k];
+        }
         ++slot;
       }
     }
@@ -653,12 +656,12 @@ __global__ void k_assemble(MeshView M, SweepView S, const double* __restrict__ q
   TB Bv[5];
 #pragma unroll
   for (int k = 0; k < 5; ++k) Bv[k] = TB(src[5 * c + k]);
-  TB* lo = luc + 25 * ck.cb + i;
+  TB* lo = luc + 25 * ck.cbp + i;
 #pragma unroll
-  for (int k = 0; k < 25; ++k) lo[k * n] = D[k];
-  TB* bo = bcv + 5 * ck.cb + i;
+  for (int k = 0; k < 25; ++k) lo[k * ld] = D[k];
+  TB* bo = bcv + 5 * ck.cbp + i;
 #pragma unroll
-  for (int k = 0; k < 5; ++k) bo[k * n] = Bv[k];
+  for (int k = 0; k < 5; ++k) bo[k * ld] = Bv[k];
   pvv[ci] = pv;
   // block Jacobi start D x = B (linearSolverSGS.loci:57-69)
   TX y[5];
@@ -672,20 +675,20 @@ __global__ void k_assemble(MeshView M, SweepView S, const double* __restrict__ q
 
 // block Jacobi start alone (a second solve on an assembled system)
 template <class TB, class TX>
-__global__ void k_jacobi_start(int64_t cb, int64_t n, const TB* __restrict__ luc,
+__global__ void k_jacobi_start(ColInfo ck, const TB* __restrict__ luc,
                                const TB* __restrict__ bcv, const int32_t* __restrict__ pvv,
                                TX* __restrict__ x) {
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  if (i >= ck.n) return;
   TB LU[25];
 #pragma unroll
-  for (int k = 0; k < 25; ++k) LU[k] = luc[25 * cb + k * n + i];
+  for (int k = 0; k < 25; ++k) LU[k] = luc[25 * ck.cbp + k * ck.ld + i];
   TX y[5];
 #pragma unroll
-  for (int k = 0; k < 5; ++k) y[k] = TX(bcv[5 * cb + k * n + i]);
-  lu5_solve<TB, TX>(LU, pvv[cb + i], y);
+  for (int k = 0; k < 5; ++k) y[k] = TX(bcv[5 * ck.cbp + k * ck.ld + i]);
+  lu5_solve<TB, TX>(LU, pvv[ck.cb + i], y);
 #pragma unroll
-  for (int k = 0; k < 5; ++k) x[5 * (cb + i) + k] = y[k];
+  for (int k = 0; k < 5; ++k) x[5 * (ck.cb + i) + k] = y[k];
 }
 
 // ---------------------------------------------------------------------------
@@ -695,37 +698,39 @@ __global__ void k_jacobi_start(int64_t cb, int64_t n, const TB* __restrict__ luc
 // ---------------------------------------------------------------------------
 // One thread per cell of colour k; every per-cell stream (slots, LU, B,
 // pivots, own iterate) is read with consecutive threads on consecutive
-// addresses; only the neighbours' iterates are gathered.
+// addresses; only the neighbours' iterates are gathered.  The one-pass
+// streams are loaded with the streaming hint (evict first) so that the
+// iterate, which every colour re-reads, stays resident in L2.
 template <class TB, class TX>
 __global__ void k_sgs_colour(ColInfo ck, const int32_t* __restrict__ nbr,
                              const TB* __restrict__ aoff, const TB* __restrict__ luc,
                              const TB* __restrict__ bcv, const int32_t* __restrict__ pvv,
                              TX* __restrict__ x) {
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  const int64_t n = ck.n;
+  const int64_t n = ck.n, ld = ck.ld;
   if (i >= n) return;
   TX t[5];
 #pragma unroll
-  for (int k = 0; k < 5; ++k) t[k] = -TX(__ldg(bcv + 5 * ck.cb + k * n + i));
+  for (int k = 0; k < 5; ++k) t[k] = -TX(__ldcs(bcv + 5 * ck.cbp + k * ld + i));
   for (int64_t s = 0; s < ck.m; ++s) {
-    const int32_t o = __ldg(nbr + ck.eb + s * n + i);
+    const int32_t o = __ldcs(nbr + ck.ebp + s * ld + i);
     if (o < 0) break;
     TX xv[5];
 #pragma unroll
     for (int k = 0; k < 5; ++k) xv[k] = x[5 * int64_t(o) + k];
-    const TB* A = aoff + 25 * ck.eb + s * 25 * n + i;
+    const TB* A = aoff + 25 * ck.ebp + s * 25 * ld + i;
 #pragma unroll
     for (int r = 0; r < 5; ++r)
 #pragma unroll
-      for (int j = 0; j < 5; ++j) t[r] += TX(__ldg(A + (5 * r + j) * n)) * xv[j];
+      for (int j = 0; j < 5; ++j) t[r] += TX(__ldcs(A + (5 * r + j) * ld)) * xv[j];
   }
   TB LU[25];
 #pragma unroll
-  for (int k = 0; k < 25; ++k) LU[k] = __ldg(luc + 25 * ck.cb + k * n + i);
+  for (int k = 0; k < 25; ++k) LU[k] = __ldcs(luc + 25 * ck.cbp + k * ld + i);
   TX y[5];
 #pragma unroll
   for (int k = 0; k < 5; ++k) y[k] = -t[k];
-  lu5_solve<TB, TX>(LU, __ldg(pvv + ck.cb + i), y);
+  lu5_solve<TB, TX>(LU, __ldcs(pvv + ck.cb + i), y);
   TX* xo = x + 5 * (ck.cb + i);
 #pragma unroll
   for (int k = 0; k < 5; ++k) xo[k] = y[k];
@@ -735,17 +740,16 @@ __global__ void k_sgs_colour(ColInfo ck, const int32_t* __restrict__ nbr,
 // k_assemble and the face blocks)
 template <class TB, class TX>
 __global__ void __launch_bounds__(NORM_THREADS)
-k_linres(MeshView M, SweepView S, const TB* __restrict__ D, const TB* __restrict__ bcv,
-         const TB* __restrict__ fjp, const TB* __restrict__ fjm, const TX* __restrict__ x,
-         double* __restrict__ part) {
+k_linres(MeshView M, const int32_t* __restrict__ xmap, const TB* __restrict__ D,
+         const double* __restrict__ src, const TB* __restrict__ fjp, const TB* __restrict__ fjm,
+         const TX* __restrict__ x, double* __restrict__ part) {
   const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   double sb = 0, sr = 0;
   if (c < M.nc) {
-    const int64_t ci = S.ci[c];
-    const ColInfo ck = S.col[S.ccol[c]];
+    const int64_t ci = xmap[c];
     double r[5];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) r[k] = double(bcv[5 * ck.cb + k * ck.n + (ci - ck.cb)]);
+    for (int k = 0; k < 5; ++k) r[k] = double(TB(src[5 * c + k]));
 #pragma unroll
     for (int k = 0; k < 5; ++k) sb += r[k] * r[k];
 #pragma unroll
@@ -757,13 +761,13 @@ k_linres(MeshView M, SweepView S, const TB* __restrict__ D, const TB* __restrict
       const int64_t f = ent >> 1;
       if (f >= M.nfi) continue;
       if (ent & 1) {
-        const TX* xn = x + 5 * int64_t(S.ci[M.cl[f]]);
+        const TX* xn = x + 5 * int64_t(xmap[M.cl[f]]);
 #pragma unroll
         for (int i = 0; i < 5; ++i)
 #pragma unroll
           for (int j = 0; j < 5; ++j) r[i] += double(fjp[25 * f + 5 * i + j]) * double(xn[j]);
       } else {
-        const TX* xn = x + 5 * int64_t(S.ci[M.cr[f]]);
+        const TX* xn = x + 5 * int64_t(xmap[M.cr[f]]);
 #pragma unroll
         for (int i = 0; i < 5; ++i)
 #pragma unroll
@@ -953,6 +957,11 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
   return FPSI_OK;
 }
 
+static ColInfo col_info(const fpsi_ctx* x, int k) {
+  const HostMesh& H = x->H;
+  return ColInfo{H.col_cb[k], H.col_n[k], H.col_m[k], H.col_ld[k], H.col_cbp[k], H.col_ebp[k]};
+}
+
 static dev::SweepView sweep_view(const fpsi_ctx* x) {
   dev::SweepView S;
   S.ci = x->d_ci;
@@ -975,7 +984,8 @@ static int launch_assemble_t(fpsi_ctx* x) {
   prof_begin(x, "assemble_lu");
   dev::k_assemble<TB, TX><<<blocks_for(M.nc, 128), 128, 0, s>>>(
       M, sweep_view(x), x->d_q, x->d_src, x->d_dtau, fjp, fjm, g, (TB*)x->d_luc, (TB*)x->d_bc,
-      x->d_pv, (TB*)x->d_aoff, x->keep_D ? (TB*)x->d_D : nullptr, (TX*)x->d_x, x->d_err);
+      x->d_pv, x->P.solver == FPSI_SOLVER_LSGS ? nullptr : (TB*)x->d_aoff,
+      x->keep_D ? (TB*)x->d_D : nullptr, (TX*)x->d_x, x->d_err);
   prof_end(x);
   FPSI_CUDA_TRY(cudaGetLastError());
   return FPSI_OK;
@@ -995,10 +1005,10 @@ int launch_assemble(fpsi_ctx* x) {
 template <class TB, class TX>
 static int launch_jacobi_t(fpsi_ctx* x) {
   for (int k = 0; k < x->H.ncolours; ++k) {
-    const int64_t n = x->H.col_n[k];
-    if (n == 0) continue;
-    dev::k_jacobi_start<TB, TX><<<blocks_for(n, 128), 128, 0, x->stream>>>(
-        x->H.col_cb[k], n, (const TB*)x->d_luc, (const TB*)x->d_bc, x->d_pv, (TX*)x->d_x);
+    const ColInfo ck = col_info(x, k);
+    if (ck.n == 0) continue;
+    dev::k_jacobi_start<TB, TX><<<blocks_for(ck.n, 128), 128, 0, x->stream>>>(
+        ck, (const TB*)x->d_luc, (const TB*)x->d_bc, x->d_pv, (TX*)x->d_x);
   }
   FPSI_CUDA_TRY(cudaGetLastError());
   return FPSI_OK;
@@ -1024,11 +1034,7 @@ static int launch_sgs_t(fpsi_ctx* x, int sweeps) {
     for (int pass = 0; pass < 2; ++pass)
       for (int kk = 0; kk < K; ++kk) {
         const int k = pass == 0 ? kk : K - 1 - kk;
-        ColInfo ck;
-        ck.cb = x->H.col_cb[k];
-        ck.n = x->H.col_n[k];
-        ck.eb = x->H.col_eb[k];
-        ck.m = x->H.col_m[k];
+        const ColInfo ck = col_info(x, k);
         if (ck.n == 0) continue;
         prof_begin(x, "sgs_colour");
         dev::k_sgs_colour<TB, TX><<<blocks_for(ck.n, T), T, 0, s>>>(
@@ -1055,9 +1061,10 @@ int launch_sgs(fpsi_ctx* x, int sweeps) {
 template <class TB, class TX>
 static int launch_linres_t(fpsi_ctx* x, double* out2) {
   const dev::MeshView M = view(x);
+  const bool lsgs = x->P.solver == FPSI_SOLVER_LSGS;
   dev::k_linres<TB, TX><<<x->nblk_norm, dev::NORM_THREADS, 0, x->stream>>>(
-      M, sweep_view(x), (const TB*)x->d_D, (const TB*)x->d_bc, (const TB*)x->d_fjp,
-      (const TB*)x->d_fjm, (const TX*)x->d_x, x->d_part);
+      M, lsgs ? x->d_lt : x->d_ci, (const TB*)x->d_D, x->d_src, (const TB*)x->d_fjp,
+      (const TB*)x->d_fjm, (const TX*)(lsgs ? x->d_lx : x->d_x), x->d_part);
   dev::k_sum2<<<1, dev::NORM_THREADS, 0, x->stream>>>(x->d_part, x->nblk_norm, out2);
   FPSI_CUDA_TRY(cudaGetLastError());
   return FPSI_OK;
@@ -1076,13 +1083,16 @@ int launch_linres(fpsi_ctx* x, double* out2) {
 
 int launch_update(fpsi_ctx* x) {
   const int64_t nc = x->H.nc;
+  const bool lsgs = x->P.solver == FPSI_SOLVER_LSGS;
+  const int32_t* map = lsgs ? x->d_lt : x->d_ci;
+  const void* xv = lsgs ? x->d_lx : x->d_x;
   prof_begin(x, "update");
   if (x->P.precision == FPSI_PREC_MIXED)
     dev::k_update<float><<<x->nblk_norm, dev::NORM_THREADS, 0, x->stream>>>(
-        nc, x->P.Pambient, x->d_ci, (const float*)x->d_x, x->d_q, x->d_amin);
+        nc, x->P.Pambient, map, (const float*)xv, x->d_q, x->d_amin);
   else
     dev::k_update<double><<<x->nblk_norm, dev::NORM_THREADS, 0, x->stream>>>(
-        nc, x->P.Pambient, x->d_ci, (const double*)x->d_x, x->d_q, x->d_amin);
+        nc, x->P.Pambient, map, (const double*)xv, x->d_q, x->d_amin);
   prof_end(x);
   FPSI_CUDA_TRY(cudaGetLastError());
   return FPSI_OK;

@@ -378,25 +378,31 @@ int build_host_mesh(const fpsi_mesh* m, HostMesh& h) {
   for (int64_t j = 0; j < nc; ++j) h.ci_of[h.colour_cells[j]] = int32_t(j);
   h.col_n.assign(ncol, 0);
   h.col_cb.assign(ncol, 0);
-  h.col_eb.assign(ncol, 0);
   h.col_m.assign(ncol, 0);
+  h.col_ld.assign(ncol, 0);
+  h.col_cbp.assign(ncol, 0);
+  h.col_ebp.assign(ncol, 0);
   auto ninterior = [&](int64_t c) {
     int32_t k = 0;
     for (int32_t e = h.cf_off[c]; e < h.cf_off[c + 1]; ++e)
       if (h.cr[h.cf[e] >> 1] >= 0) ++k;
     return k;
   };
-  int64_t eb = 0;
+  int64_t eb = 0, cbp = 0;
   for (int k = 0; k < ncol; ++k) {
     h.col_cb[k] = h.colour_off[k];
     h.col_n[k] = h.colour_off[k + 1] - h.colour_off[k];
+    h.col_ld[k] = (h.col_n[k] + 31) / 32 * 32;
     int64_t m = 0;
     for (int32_t j = h.colour_off[k]; j < h.colour_off[k + 1]; ++j)
       m = std::max<int64_t>(m, ninterior(h.colour_cells[j]));
     h.col_m[k] = m;
-    h.col_eb[k] = eb;
-    eb += m * h.col_n[k];
+    h.col_cbp[k] = cbp;
+    h.col_ebp[k] = eb;
+    cbp += h.col_ld[k];
+    eb += m * h.col_ld[k];
   }
+  h.ncp = cbp;
   h.nslots = eb;
   h.nbr.assign(size_t(eb), -1);
   for (int k = 0; k < ncol; ++k)
@@ -407,7 +413,7 @@ int build_host_mesh(const fpsi_mesh* m, HostMesh& h) {
         const int64_t f = h.cf[e] >> 1;
         if (h.cr[f] < 0) continue;
         const int32_t o = (h.cf[e] & 1) ? h.cl[f] : h.cr[f];
-        h.nbr[h.col_eb[k] + s * h.col_n[k] + i] = h.ci_of[o];
+        h.nbr[h.col_ebp[k] + s * h.col_ld[k] + i] = h.ci_of[o];
         ++s;
       }
     }

@@ -108,6 +108,18 @@ class GeneratedMesh:
             bcs=[m.bcs[i] for i in range(m.nbc)],
         )
 
+    def lines_along(self, axis: int = 1) -> list[np.ndarray]:
+        """Cell lines of a structured hex grid (kinds hex and bl) along one
+        axis; axis 1 gives the wall-normal lines of the boundary-layer block."""
+        s = self.spec
+        if s.kind == 1:
+            raise ValueError("split-tet grids have no structured lines")
+        n = (s.nx, s.ny, s.nz)
+        idx = np.arange(n[0] * n[1] * n[2], dtype=np.int32).reshape(n[2], n[1], n[0])
+        a = {0: 2, 1: 1, 2: 0}[axis]  # array axis of the grid direction
+        cols = np.moveaxis(idx, a, -1).reshape(-1, n[axis])
+        return [c.copy() for c in cols]
+
     def __del__(self):
         if getattr(self, "_p", None):
             N.lib().fpsi_mesh_free(self._p)
@@ -160,6 +172,33 @@ class FlowPsi:
                                           N.dptr(ar), N.dptr(fc)), "fpsi_get_geometry")
         return {"vol": vol, "cellcenter": cc.reshape(nc, 3), "area_vec": an.reshape(nf, 3),
                 "area": ar, "facecenter": fc.reshape(nf, 3)}
+
+    def set_lines(self, lines) -> None:
+        """lines of the line solver (list of caller cell-index arrays)"""
+        off = np.zeros(len(lines) + 1, np.int64)
+        off[1:] = np.cumsum([len(l) for l in lines])
+        cells = np.ascontiguousarray(np.concatenate(lines).astype(np.int32)) if lines else \
+            np.zeros(0, np.int32)
+        N.check(N.lib().fpsi_set_lines(self._ctx, len(lines),
+                                       off.ctypes.data_as(C.POINTER(C.c_int64)), N.iptr(cells)),
+                "fpsi_set_lines")
+
+    def lines(self):
+        """(line of each cell, position on the line, colour of each line)"""
+        nl = C.c_int64()
+        N.check(N.lib().fpsi_get_lines(self._ctx, None, None, None, C.byref(nl)), "fpsi_get_lines")
+        lo, po = np.empty(self.ncells, np.int32), np.empty(self.ncells, np.int32)
+        lc = np.empty(max(nl.value, 1), np.int32)
+        N.check(N.lib().fpsi_get_lines(self._ctx, N.iptr(lo), N.iptr(po), N.iptr(lc), C.byref(nl)),
+                "fpsi_get_lines")
+        return lo, po, lc[:nl.value]
+
+    def line_list(self):
+        """the lines as lists of caller cells in line order, and their colours"""
+        lo, po, lc = self.lines()
+        order = np.lexsort((po, lo))
+        bounds = np.searchsorted(lo[order], np.arange(len(lc) + 1))
+        return [order[bounds[i]:bounds[i + 1]].astype(np.int32) for i in range(len(lc))], lc
 
     def colours(self) -> np.ndarray:
         c = np.empty(self.ncells, np.int32)
@@ -218,14 +257,18 @@ class FlowPsi:
                                         N.vptr(B)), "fpsi_get_blocks")
         return {"fluid_D": D, "fjp": fjp, "fjm": fjm, "fluid_B": B}
 
-    def linear_solve(self, x0: np.ndarray | None = None) -> np.ndarray:
-        """SGSBlockedSSolve(fluid) -> dfluid (linearSolverSGS.loci:57-329,
-        solverNewton.loci:252-259); x0 None = block Jacobi start."""
+    def linear_solve(self, x0: np.ndarray | None = None, info: bool = False):
+        """SGSBlockedSSolve(fluid) or LSGSBlockedSSolve(fluid,fluid_B) ->
+        dfluid (linearSolverSGS.loci:57-329, linearSolverLSGS.loci:1692-1954,
+        solverNewton.loci:252-269); x0 None = the reference's start."""
         dq = np.empty(self.ncells * 5)
         x0p = None if x0 is None else np.ascontiguousarray(x0, np.float64).reshape(-1)
-        info = N.LsInfo()
-        N.check(N.lib().fpsi_linear_solve(self._ctx, N.dptr(x0p), N.dptr(dq), C.byref(info)),
+        li = N.LsInfo()
+        N.check(N.lib().fpsi_linear_solve(self._ctx, N.dptr(x0p), N.dptr(dq), C.byref(li)),
                 "fpsi_linear_solve")
+        if info:
+            return dq.reshape(-1, 5), {"iterations": li.iterations, "resid0": li.resid0,
+                                       "resid": li.resid}
         return dq.reshape(-1, 5)
 
     def linear_residual(self):

@@ -192,6 +192,19 @@ int fpsi_get_geometry(fpsi_ctx* ctx, double* vol, double* cellcenter,
 /* keep (1, default) or drop (0) the unfactored diagonal blocks after the LU;
  * fpsi_linear_residual and the D export of fpsi_get_blocks need them */
 int fpsi_keep_blocks(fpsi_ctx* ctx, int32_t keep);
+/* Lines of the line-SGS solver (fluidLinearSolver 'lsgs',
+ * linearSolverLSGS.loci:361-1110), caller order: line l is
+ * line_cells[line_off[l] .. line_off[l+1]); consecutive cells must share a
+ * face; cells left out become single-cell lines.  Without this call the
+ * library links cells that are mutually among each other's two strongest
+ * couplings (face area over centre distance; a second link only within a
+ * factor 25 of the first, as linearSolverLSGS.loci:620).  Lines are coloured
+ * so the lines of one colour are solved together. */
+int fpsi_set_lines(fpsi_ctx* ctx, int64_t nlines, const int64_t* line_off,
+                   const int32_t* line_cells);
+/* per caller cell its line and position on the line; per line its colour */
+int fpsi_get_lines(fpsi_ctx* ctx, int32_t* line_of_cell, int32_t* position,
+                   int32_t* line_colour, int64_t* nlines);
 /* cell colour used by the multi-colour sweeps (caller order) */
 int fpsi_get_colours(fpsi_ctx* ctx, int32_t* colour);
 

@@ -1234,6 +1234,219 @@ extern "C" int orc_linear_solve(orc_ctx* o, const int32_t* colour, const double*
   return rc;
 }
 
+// ---------------------------------------------------------------------------
+// Line SGS, linearSolverLSGS.loci:1465-1572 (line kernels) and :1692-1954
+// (solve loop), over given lines.  Lines are processed in the given order,
+// or, with line colours, colour by colour (forward 0..K-1, backward K-1..0).
+// ---------------------------------------------------------------------------
+template <class T>
+static void lu_nopiv(T* A) {  // decompose_lu
+  for (int k = 0; k < 5; ++k)
+    for (int i = k + 1; i < 5; ++i) {
+      A[5 * i + k] /= A[5 * k + k];
+      for (int j = k + 1; j < 5; ++j) A[5 * i + j] -= A[5 * i + k] * A[5 * k + j];
+    }
+}
+template <class T, class V>
+static void lu_nopiv_solve(const T* A, V* y) {  // solve_lu
+  for (int i = 1; i < 5; ++i)
+    for (int j = 0; j < i; ++j) y[i] -= V(A[5 * i + j]) * y[j];
+  for (int i = 4; i >= 0; --i) {
+    for (int j = i + 1; j < 5; ++j) y[i] -= V(A[5 * i + j]) * y[j];
+    y[i] /= V(A[5 * i + i]);
+  }
+}
+
+template <class TB, class TD, class TX>
+static int lsgs_t(orc_ctx* o, int64_t nlines, const int64_t* loff, const int32_t* lcells,
+                  const int32_t* lcolour, const std::vector<TB>& fjp, const std::vector<TB>& fjm,
+                  const std::vector<TB>& D, const std::vector<TB>& B, const double* x0,
+                  fpsi_lsinfo* info) {
+  const int64_t nc = o->nc;
+  std::vector<int32_t> line_of(nc, -1), pos(nc, -1);
+  for (int64_t l = 0; l < nlines; ++l)
+    for (int64_t k = loff[l]; k < loff[l + 1]; ++k) {
+      line_of[lcells[k]] = int32_t(l);
+      pos[lcells[k]] = int32_t(k - loff[l]);
+    }
+  for (int64_t c = 0; c < nc; ++c)
+    if (line_of[c] < 0) return FPSI_E_INVALID;
+  // coupling block of row c to neighbour n through face f
+  auto coupling = [&](int64_t c, int64_t f, TB* out) {
+    if (o->cl[f] == c)
+      for (int k = 0; k < 25; ++k) out[k] = fjm[25 * f + k];
+    else
+      for (int k = 0; k < 25; ++k) out[k] = -fjp[25 * f + k];
+  };
+  // line matrices: D' (TD), L (row p to p-1), U (row p to p+1), outer list
+  std::vector<TD> Dp(nc * 25);
+  std::vector<TB> Lb(nc * 25, TB(0)), Ub(nc * 25, TB(0));
+  struct Outer {
+    int64_t row, col;
+    TB F[25];
+  };
+  std::vector<std::vector<Outer>> outer(nlines);
+  auto nbr_of = [&](int64_t c, int64_t f) { return o->cl[f] == c ? o->cr[f] : o->cl[f]; };
+  for (int64_t c = 0; c < nc; ++c) {
+    for (int k = 0; k < 25; ++k) Dp[25 * c + k] = TD(D[25 * c + k]);
+    const int64_t l = line_of[c];
+    const int64_t p = pos[c];
+    const int64_t len = loff[l + 1] - loff[l];
+    const int64_t prv = p > 0 ? lcells[loff[l] + p - 1] : -1;
+    const int64_t nxt = p + 1 < len ? lcells[loff[l] + p + 1] : -1;
+    bool hp = false, hn = false;
+    auto face = [&](int64_t f) {
+      const int64_t n = nbr_of(c, f);
+      TB blk[25];
+      coupling(c, f, blk);
+      if (n == prv && !hp) {
+        hp = true;
+        for (int k = 0; k < 25; ++k) Lb[25 * c + k] = blk[k];
+      } else if (n == nxt && !hn) {
+        hn = true;
+        for (int k = 0; k < 25; ++k) Ub[25 * c + k] = blk[k];
+      } else {
+        Outer ou;
+        ou.row = c, ou.col = n;
+        for (int k = 0; k < 25; ++k) ou.F[k] = blk[k];
+        outer[l].push_back(ou);
+      }
+    };
+    for (int64_t k = o->up_off[c]; k < o->up_off[c + 1]; ++k) face(o->up[k]);
+    for (int64_t k = o->lo_off[c]; k < o->lo_off[c + 1]; ++k) face(o->lo[k]);
+  }
+  // preprocessLine (:1465-1495): Schur products with real_fj intermediates
+  for (int64_t l = 0; l < nlines; ++l) {
+    const int64_t len = loff[l + 1] - loff[l];
+    lu_nopiv<TD>(&Dp[25 * lcells[loff[l]]]);
+    for (int64_t i = 1; i < len; ++i) {
+      const int64_t cm = lcells[loff[l] + i - 1], cn = lcells[loff[l] + i];
+      const TD* Dm = &Dp[25 * cm];
+      TD* Dn = &Dp[25 * cn];
+      const TB* Lm = &Lb[25 * cn];
+      const TB* Um = &Ub[25 * cm];
+      for (int j = 0; j < 5; ++j) {
+        TD v[5];
+        for (int k = 0; k < 5; ++k) v[k] = TD(Um[5 * k + j]);
+        lu_nopiv_solve<TD, TD>(Dm, v);
+        TB t[5], w[5];
+        for (int k = 0; k < 5; ++k) t[k] = TB(v[k]), w[k] = TB(0);
+        for (int k = 0; k < 5; ++k)
+          for (int m = 0; m < 5; ++m) w[k] += Lm[5 * k + m] * t[m];
+        for (int k = 0; k < 5; ++k) Dn[5 * k + j] -= TD(w[k]);
+      }
+      lu_nopiv<TD>(Dn);
+    }
+  }
+  std::vector<TX> X(nc * 5, TX(0)), xt(nc * 5, TX(0));
+  // lineSolve (:1523-1572) with right-hand side r (r = B - sum_outer F X)
+  auto line_solve = [&](int64_t l, bool with_outer, bool save) {
+    const int64_t len = loff[l + 1] - loff[l];
+    std::vector<TX> r(len * 5);
+    for (int64_t i = 0; i < len; ++i)
+      for (int k = 0; k < 5; ++k) r[5 * i + k] = TX(B[5 * lcells[loff[l] + i] + k]);
+    if (with_outer)
+      for (const Outer& ou : outer[l]) {
+        const int64_t i = pos[ou.row];
+        for (int k = 0; k < 5; ++k)
+          for (int j = 0; j < 5; ++j) r[5 * i + k] -= TX(ou.F[5 * k + j]) * X[5 * ou.col + j];
+      }
+    if (save)
+      for (int64_t i = 0; i < len; ++i)
+        for (int k = 0; k < 5; ++k) xt[5 * lcells[loff[l] + i] + k] = X[5 * lcells[loff[l] + i] + k];
+    std::vector<TX> y(len * 5);
+    for (int k = 0; k < 5; ++k) y[k] = r[k];
+    for (int64_t i = 1; i < len; ++i) {
+      TX v[5];
+      for (int k = 0; k < 5; ++k) v[k] = y[5 * (i - 1) + k];
+      lu_nopiv_solve<TD, TX>(&Dp[25 * lcells[loff[l] + i - 1]], v);
+      const TB* Lm = &Lb[25 * lcells[loff[l] + i]];
+      for (int k = 0; k < 5; ++k) {
+        TX a = r[5 * i + k];
+        for (int j = 0; j < 5; ++j) a -= TX(Lm[5 * k + j]) * v[j];
+        y[5 * i + k] = a;
+      }
+    }
+    for (int64_t i = len - 1; i >= 0; --i) {
+      TX v[5];
+      for (int k = 0; k < 5; ++k) v[k] = y[5 * i + k];
+      if (i < len - 1) {
+        const TB* Um = &Ub[25 * lcells[loff[l] + i]];
+        const int64_t cn = lcells[loff[l] + i + 1];
+        for (int k = 0; k < 5; ++k)
+          for (int j = 0; j < 5; ++j) v[k] -= TX(Um[5 * k + j]) * X[5 * cn + j];
+      }
+      lu_nopiv_solve<TD, TX>(&Dp[25 * lcells[loff[l] + i]], v);
+      for (int k = 0; k < 5; ++k) X[5 * lcells[loff[l] + i] + k] = v[k];
+    }
+  };
+  if (x0) {
+    for (int64_t i = 0; i < nc * 5; ++i) X[i] = TX(x0[i]);
+  } else {
+    for (int64_t l = 0; l < nlines; ++l) line_solve(l, false, false);  // (:1708-1728)
+  }
+  std::vector<int64_t> order;
+  if (lcolour) {
+    int ncol = 0;
+    for (int64_t l = 0; l < nlines; ++l) ncol = std::max(ncol, lcolour[l] + 1);
+    for (int k = 0; k < ncol; ++k)
+      for (int64_t l = 0; l < nlines; ++l)
+        if (lcolour[l] == k) order.push_back(l);
+  } else {
+    for (int64_t l = 0; l < nlines; ++l) order.push_back(l);
+  }
+  double w = o->P.lsgs_relaxation, zero = 1.0, resid = 0.0;
+  int iter = 0;
+  for (; iter < o->P.lsgs_max_iter;) {
+    for (int64_t l : order) line_solve(l, true, false);
+    for (auto it = order.rbegin(); it != order.rend(); ++it) line_solve(*it, true, true);
+    double s = 0;
+    for (int64_t i = 0; i < nc * 5; ++i) {
+      X[i] = TX(w * double(X[i]) + (1. - w) * double(xt[i]));
+      const double r = double(X[i]) - double(xt[i]);
+      s += r * r;
+    }
+    resid = std::sqrt(s);
+    if (iter == 0) zero = std::max(resid, 1e-16);
+    const double rel = resid / zero;
+    if (rel > 1.0) w *= 1. / rel;
+    ++iter;
+    if (resid < o->P.lsgs_abs_tol || rel < o->P.lsgs_rel_tol) break;
+  }
+  o->dq.resize(nc * 5);
+  for (int64_t i = 0; i < nc * 5; ++i) o->dq[i] = double(X[i]);
+  o->have_dq = true;
+  if (info) {
+    info->iterations = iter;
+    info->status = FPSI_OK;
+    info->resid0 = zero;
+    info->resid = resid;
+  }
+  return FPSI_OK;
+}
+
+extern "C" int orc_lsgs_solve(orc_ctx* o, int64_t nlines, const int64_t* line_off,
+                              const int32_t* line_cells, const int32_t* line_colour,
+                              const double* x0, double* dq, fpsi_lsinfo* info) {
+  if (!o->have_asm) return FPSI_E_STATE;
+  int rc;
+  switch (o->P.precision) {
+    case FPSI_PREC_FP64:
+      rc = lsgs_t<double, double, double>(o, nlines, line_off, line_cells, line_colour, o->fjp64,
+                                          o->fjm64, o->D64, o->B64, x0, info);
+      break;
+    case FPSI_PREC_MIXED:
+      rc = lsgs_t<float, float, float>(o, nlines, line_off, line_cells, line_colour, o->fjp32,
+                                       o->fjm32, o->D32, o->B32, x0, info);
+      break;
+    default:
+      rc = lsgs_t<float, double, double>(o, nlines, line_off, line_cells, line_colour, o->fjp32,
+                                         o->fjm32, o->D32, o->B32, x0, info);
+  }
+  if (!rc && dq) std::memcpy(dq, o->dq.data(), sizeof(double) * o->nc * 5);
+  return rc;
+}
+
 // ||B - A dq|| with A from the unfactored blocks
 template <class TB>
 static void linres_t(orc_ctx* o, const std::vector<TB>& fjp, const std::vector<TB>& fjm,

@@ -36,6 +36,11 @@ int  orc_get_blocks(orc_ctx* o, void* D, void* fjp, void* fjm, void* B);
 int  orc_linear_solve(orc_ctx* o, const int32_t* colour, const double* x0, double* dq,
                       fpsi_lsinfo* info);
 int  orc_linear_residual(orc_ctx* o, double* norm_b, double* norm_r);
+/* line SGS (linearSolverLSGS.loci:1465-1954) over caller lines; with
+ * line_colour the lines are swept colour by colour, else in line order */
+int  orc_lsgs_solve(orc_ctx* o, int64_t nlines, const int64_t* line_off,
+                    const int32_t* line_cells, const int32_t* line_colour, const double* x0,
+                    double* dq, fpsi_lsinfo* info);
 int  orc_update(orc_ctx* o, double* min_alpha);
 int  orc_newton_step(orc_ctx* o, const int32_t* colour, fpsi_stepinfo* info);
 /* number of OpenMP threads the oracle loops use (1 = scalar) */

@@ -35,6 +35,8 @@ _SIGS = {
     "orc_get_blocks": (C.c_int, [C.c_void_p, _vp, _vp, _vp, _vp]),
     "orc_linear_solve": (C.c_int, [C.c_void_p, _ip, _dp, _dp, C.POINTER(N.LsInfo)]),
     "orc_linear_residual": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "orc_lsgs_solve": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_int64), _ip, _ip, _dp, _dp,
+                                 C.POINTER(N.LsInfo)]),
     "orc_update": (C.c_int, [C.c_void_p, _dp]),
     "orc_newton_step": (C.c_int, [C.c_void_p, _ip, C.POINTER(N.StepInfo)]),
     "orc_set_threads": (C.c_int, [C.c_int]),
@@ -243,6 +245,23 @@ class Oracle:
                                      _d(None if x0 is None else np.asarray(x0).reshape(-1)),
                                      dq.ctypes.data_as(_dp), C.byref(info)), "orc_linear_solve")
         return dq.reshape(-1, 5)
+
+    def lsgs_solve(self, lines, colours=None, x0=None):
+        """line SGS over the given lines (list of caller cell arrays); with
+        colours (one per line) the lines are swept colour by colour"""
+        off = np.zeros(len(lines) + 1, np.int64)
+        off[1:] = np.cumsum([len(l) for l in lines])
+        cells = np.ascontiguousarray(np.concatenate(lines).astype(np.int32))
+        col = None if colours is None else np.ascontiguousarray(colours, np.int32)
+        dq = np.empty(self.ncells * 5)
+        info = N.LsInfo()
+        _chk(olib().orc_lsgs_solve(self._h, len(lines), off.ctypes.data_as(C.POINTER(C.c_int64)),
+                                   cells.ctypes.data_as(_ip),
+                                   None if col is None else col.ctypes.data_as(_ip),
+                                   _d(None if x0 is None else np.asarray(x0).reshape(-1)),
+                                   dq.ctypes.data_as(_dp), C.byref(info)), "orc_lsgs_solve")
+        return dq.reshape(-1, 5), {"iterations": info.iterations, "resid0": info.resid0,
+                                   "resid": info.resid}
 
     def linear_residual(self):
         nb, nr = C.c_double(), C.c_double()

@@ -121,3 +121,40 @@ def test_newton_decreases_residual():
     o.set_state(T, p, u)
     r = [o.newton_step()["rtrms"] for _ in range(8)]
     assert r[-1] < 0.1 * r[0]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "ref"])
+def test_lsgs_converges_to_the_linear_solution(prec):
+    """line SGS with tight tolerances reaches the solution that many SGS
+    sweeps reach (same blocks)"""
+    case = cases.boundary_layer_block(6, 10, 4, dy0=1e-4, growth=1.3, precision=prec)
+    p = case.params
+    p.lsgs_max_iter, p.lsgs_rel_tol, p.lsgs_abs_tol, p.gauss_seidel_iter = 400, 1e-14, 0.0, 400
+    o = Oracle(case.mesh, p)
+    T, pr, u = case.initial_state(o.geometry()["cellcenter"])
+    o.set_state(T, pr, u)
+    o.residual()
+    o.assemble()
+    dl, info = o.lsgs_solve(case.lines)
+    nb, nr = o.linear_residual()
+    assert nr < (1e-9 if prec == "fp64" else 1e-4) * nb
+    ds = o.linear_solve()
+    assert np.abs(dl - ds).max() < (1e-8 if prec == "fp64" else 1e-3) * np.abs(ds).max()
+
+
+def test_lsgs_relaxation_and_stopping_rules():
+    """the default controls (w=0.25, rel 0.1, max 10) stop early and never
+    exceed the iteration cap; a longer line sweep lowers the residual"""
+    case = cases.boundary_layer_block(6, 10, 4, dy0=1e-4, growth=1.3, precision="fp64")
+    o = Oracle(case.mesh, case.params)
+    T, pr, u = case.initial_state(o.geometry()["cellcenter"])
+    o.set_state(T, pr, u)
+    o.residual()
+    o.assemble()
+    _, info = o.lsgs_solve(case.lines)
+    assert 1 <= info["iterations"] <= 10
+    assert info["resid"] < 0.1 * info["resid0"] or info["iterations"] == 10
+    r_default = o.linear_residual()[1]
+    single = [np.array([c], np.int32) for c in range(o.ncells)]
+    o.lsgs_solve(single)
+    assert r_default <= o.linear_residual()[1] * 1.0001
