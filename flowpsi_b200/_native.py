@@ -35,8 +35,9 @@ class Params(C.Structure):
         ("lsgs_relaxation", C.c_double), ("lsgs_abs_tol", C.c_double),
         ("lsgs_rel_tol", C.c_double), ("lsgs_max_iter", C.c_int32),
         ("precision", C.c_int32), ("viscous", C.c_int32), ("reserved0", C.c_int32),
-        ("Pr", C.c_double), ("Prt", C.c_double), ("sutherland_mu0", C.c_double),
-        ("sutherland_T0", C.c_double), ("sutherland_S", C.c_double),
+        ("Prt", C.c_double), ("mu_a1", C.c_double), ("mu_a2", C.c_double),
+        ("mu_a3", C.c_double), ("k_a1", C.c_double), ("k_a2", C.c_double),
+        ("k_a3", C.c_double),
     ]
 
 
@@ -109,6 +110,7 @@ _SIGS = {
     "fpsi_set_lines": (C.c_int, [_ctx, C.c_int64, C.POINTER(C.c_int64), _ip]),
     "fpsi_get_lines": (C.c_int, [_ctx, _ip, _ip, _ip, C.POINTER(C.c_int64)]),
     "fpsi_set_state": (C.c_int, [_ctx, _dp, _dp, _dp]),
+    "fpsi_set_eddy_viscosity": (C.c_int, [_ctx, _dp]),
     "fpsi_get_state": (C.c_int, [_ctx, _dp, _dp, _dp]),
     "fpsi_residual": (C.c_int, [_ctx, _dp, C.POINTER(Resid)]),
     "fpsi_get_reconstruction": (C.c_int, [_ctx, _dp, _dp]),

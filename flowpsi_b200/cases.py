@@ -117,22 +117,49 @@ def taylor_green_tets(n: int = 128, seed: int = 0, sweeps: int = 8, jitter: floa
     return Case(f"taylor_green_tets_{n}", mesh, params, 200, init)
 
 
+MU_A = (1.458e-6, 1.5, 110.4)  # Sutherland, fluxViscous.loci:58-80
+SA_CV1 = 7.1                    # SA_param.h:34
+
+
+def sutherland_mu(T):
+    return MU_A[0] * np.power(T, MU_A[1]) / (T + MU_A[2])
+
+
+def sa_eddy_viscosity(nu_tilde, rho, mu):
+    """Spalart-Allmaras eddy viscosity tmu = rho nu~ fv1, chi = rho nu~ / mu,
+    fv1 = chi^3 / (chi^3 + cv1^3) (SA_turb.loci:91-107)"""
+    chi3 = (rho * nu_tilde / mu) ** 3
+    return nu_tilde * chi3 / (chi3 + SA_CV1 ** 3) * rho
+
+
 def boundary_layer_block(nx: int = 256, ny: int = 128, nz: int = 64, dy0: float = 1e-6,
                          growth: float = 1.15, seed: int = 0,
-                         precision: str = "mixed", solver: str = "lsgs",
-                         wall: str = "reflecting", Lx: float = 1.0, Lz: float = 0.25) -> Case:
+                         precision: str = "mixed", solver: str = "lsgs", viscous: int = 0,
+                         Re: float = 1e6, Lx: float = 1.0, Lz: float = 0.25) -> Case:
     """Flat-plate block: x streamwise, y wall-normal (first spacing dy0,
-    geometric growth), z spanwise periodic; wall at y = 0, farfield at the
-    top, inflow and outflow sides.  M=0.3, T=300 K, p=1e5 Pa.  The
-    wall-normal columns are the LSGS lines (case.lines)."""
-    T0, p0, M = 300.0, 1e5, 0.3
+    geometric growth), z spanwise periodic; wall at y = 0 (slip wall when
+    inviscid, adiabatic no-slip wall otherwise), farfield at the top, inflow
+    and outflow sides.  M=0.3, T=300 K; viscous cases set the freestream
+    density so that Re = rho U / mu(T) per unit length, inviscid ones use
+    p = 1e5 Pa.  viscous: 0 inviscid, 1 laminar, 2 turbulent with the
+    Spalart-Allmaras eddy viscosity of a frozen nu~ = 3 nu_inf field
+    (case.tmu).  The wall-normal columns are the LSGS lines (case.lines)."""
+    T0, M = 300.0, 0.3
     U0 = M * math.sqrt(GAMMA * RTILDE * T0)
+    mu0 = float(sutherland_mu(T0))
+    if viscous:
+        rho0 = Re * mu0 / U0
+        p0 = rho0 * RTILDE * T0
+    else:
+        p0 = 1e5
+        rho0 = p0 / (RTILDE * T0)
     ff = bc("farfield", T=T0, pg=p0, u=(U0, 0.0, 0.0))
-    wl = bc(wall, T=T0, pg=p0)
+    wl = bc("viscousWall" if viscous else "reflecting", T=T0, pg=p0)
     mesh = GeneratedMesh("bl", n=(nx, ny, nz), L=(Lx, 1.0, Lz), dy0=dy0, growth=growth,
                          bc_side=(0, 0, 1, 0, -1, -1), bcs=[ff, wl])
     params = default_params(flux="roe", limiter="venkatakrishnan", solver=solver,
-                            gauss_seidel_iter=8, cflmax=50.0, precision=precision)
+                            gauss_seidel_iter=8, cflmax=50.0, precision=precision,
+                            viscous=viscous)
 
     def init(cc):
         nc = cc.shape[0]
@@ -146,6 +173,10 @@ def boundary_layer_block(nx: int = 256, ny: int = 128, nz: int = 64, dy0: float 
 
     c = Case(f"boundary_layer_{nx}x{ny}x{nz}", mesh, params, 100, init)
     c.lines = mesh.lines_along(1)
+    c.tmu = None
+    if viscous == 2:
+        nc = nx * ny * nz
+        c.tmu = np.full(nc, float(sa_eddy_viscosity(3.0 * mu0 / rho0, rho0, mu0)))
     return c
 
 

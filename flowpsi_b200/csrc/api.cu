@@ -171,9 +171,10 @@ int check_params(const fpsi_params* p) {
     fpsi::set_error("LSGS controls out of range");
     return FPSI_E_INVALID;
   }
-  if (p->viscous != 0) {
-    fpsi::set_error("viscous fluxes are not available on this build");
-    return FPSI_E_UNSUPPORTED;
+  if (p->viscous < 0 || p->viscous > 2 ||
+      (p->viscous && (!(p->mu_a1 > 0) || !(p->k_a1 > 0) || !(p->Prt > 0)))) {
+    fpsi::set_error("flowRegime / Sutherland parameters out of range");
+    return FPSI_E_INVALID;
   }
   return FPSI_OK;
 }
@@ -234,11 +235,13 @@ void fpsi_default_params(fpsi_params* p) {
   p->lsgs_max_iter = 10;
   p->precision = FPSI_PREC_REF;
   p->viscous = 0;
-  p->Pr = 0.72;
   p->Prt = 0.9;
-  p->sutherland_mu0 = 1.716e-5;
-  p->sutherland_T0 = 273.15;
-  p->sutherland_S = 110.4;
+  p->mu_a1 = 1.458e-6;
+  p->mu_a2 = 1.5;
+  p->mu_a3 = 110.4;
+  p->k_a1 = 2.495e-3;
+  p->k_a2 = 1.5;
+  p->k_a3 = 194.0;
 }
 
 const char* fpsi_strerror(int code) {
@@ -270,7 +273,7 @@ int fpsi_destroy(fpsi_ctx* x) {
   free_lsgs(x);
   void* ps[] = {x->d_cl, x->d_cr, x->d_n, x->d_area, x->d_rL, x->d_rR, x->d_vol, x->d_cc,
                 x->d_Minv, x->d_cf_off, x->d_cf, x->d_colour_cells, x->d_bcs, x->d_q,
-                x->d_qb, x->d_grad, x->d_phi, x->d_F, x->d_mev, x->d_src, x->d_dtau,
+                x->d_qb, x->d_grad, x->d_phi, x->d_F, x->d_mev, x->d_src, x->d_dtau, x->d_tmu,
                 x->d_part, x->d_resid, x->d_amin, x->d_err, x->d_perm, x->d_stage, x->d_ci, x->d_ccol,
                 x->d_nbr, x->d_colinfo};
   for (void* p : ps)
@@ -305,7 +308,7 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
   }
   x->bcs.assign(mesh->bcs, mesh->bcs + mesh->nbc);
   for (const fpsi_bc& b : x->bcs)
-    if (b.kind < FPSI_BC_FARFIELD || b.kind > FPSI_BC_REFLECTING) {
+    if (b.kind < FPSI_BC_FARFIELD || b.kind > FPSI_BC_VISCOUS_WALL) {
       fpsi::set_error("boundary condition kind %d is not on the device path", b.kind);
       delete x;
       return FPSI_E_UNSUPPORTED;
@@ -363,6 +366,11 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
   TRY(dalloc(x, &x->d_mev, nf));
   TRY(dalloc(x, &x->d_src, nc * 5));
   TRY(dalloc(x, &x->d_dtau, nc));
+  TRY(dalloc(x, &x->d_tmu, nc));
+  if (cudaMemset(x->d_tmu, 0, nc * sizeof(double)) != cudaSuccess) {
+    fpsi_destroy(x);
+    return FPSI_E_CUDA;
+  }
   x->nblk_norm = int((nc + 255) / 256);
   TRY(dalloc(x, &x->d_part, size_t(x->nblk_norm) * 8));
   TRY(dalloc(x, &x->d_resid, 16));
@@ -469,6 +477,15 @@ int fpsi_get_lines(fpsi_ctx* x, int32_t* line_of_cell, int32_t* position, int32_
   }
   if (line_colour)
     for (int64_t l = 0; l < Y.nlines; ++l) line_colour[l] = Y.line_colour[l];
+  return FPSI_OK;
+}
+
+int fpsi_set_eddy_viscosity(fpsi_ctx* x, const double* tmu) {
+  if (!x || !tmu) return FPSI_E_INVALID;
+  std::vector<double> t(x->H.nc);
+  for (int64_t i = 0; i < x->H.nc; ++i) t[i] = tmu[x->H.perm[i]];
+  FPSI_CUDA_TRY(cudaMemcpy(x->d_tmu, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice));
+  x->have_resid = x->have_asm = x->have_dq = false;
   return FPSI_OK;
 }
 

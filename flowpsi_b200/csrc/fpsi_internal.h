@@ -124,6 +124,7 @@ struct fpsi_ctx {
   double* d_mev = nullptr;     // [nf] maxev_f * area
   double* d_src = nullptr;     // [nc][5]
   double* d_dtau = nullptr;    // [nc]
+  double* d_tmu = nullptr;     // [nc] eddy viscosity (flowRegime turbulent)
   double* d_part = nullptr;    // per-block partial norms
   double* d_resid = nullptr;   // 16 doubles: final norms
   double* h_resid = nullptr;   // pinned mirror

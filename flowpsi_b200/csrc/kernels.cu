@@ -39,6 +39,7 @@ struct MeshView {
   const double* Minv;  // [6][nc]
   const int32_t* cf_off;
   const int32_t* cf;
+  const fpsi_bc* bcs;
 };
 
 __device__ __forceinline__ Q5 load_q(const double* q, int64_t c) {
@@ -96,6 +97,9 @@ __global__ void k_bc_state(MeshView M, const double* __restrict__ q, const fpsi_
       if (ut < ai) r.p -= (qi.p + g.pamb) * 0.1;
       break;
     }
+    case FPSI_BC_VISCOUS_WALL:  // adiabatic no-slip wall, bcViscousWall.loci:148-218
+      r.u = r.v = r.w = 0.0;
+      break;
     case FPSI_BC_REFLECTING: {
       const double un = qi.u * nx + qi.v * ny + qi.w * nz;
       r.u = qi.u - 2.0 * un * nx;
@@ -262,11 +266,140 @@ __device__ __forceinline__ void reconstruct(const MeshView& M, const double* __r
 }
 
 // ---------------------------------------------------------------------------
+// viscous face flux (fluxViscous.loci:112-310) and its thin-layer Jacobian
+// (:315-448).  Face gradients (Loci FVM gradv3d_f / grads_f) are the mean of
+// the two cell gradients with the component along d = x_R - x_L replaced
+// by the difference quotient; at boundary faces the cell gradient corrected
+// the same way towards the face state.
+// ---------------------------------------------------------------------------
+struct Visc {
+  int on;  // 0 inviscid, 1 laminar, 2 turbulent
+  double a1, a2, a3, k1, k2, k3, cp_prt;
+  const double* tmu;
+};
+
+struct VFace {
+  double vf[4];   // momentum x,y,z and energy (added to src[cl], taken from src[cr])
+  double uf[3];
+  double muT, kT, dist;
+};
+
+__device__ __forceinline__ double suth(double T, double a1, double a2, double a3) {
+  return a1 * pow(T, a2) / (T + a3);
+}
+
+__device__ __forceinline__ int bc_kind(const MeshView& M, int64_t f) {
+  return f >= M.nfi ? M.bcs[-M.cr[f] - 1].kind : 0;
+}
+
+__device__ VFace viscous_face(const MeshView& M, const double* __restrict__ q,
+                              const double* __restrict__ qb, const double* __restrict__ grad,
+                              const Visc& V, int64_t f) {
+  VFace o;
+  const int64_t nf = M.nf;
+  const double n[3] = {M.n[f], M.n[nf + f], M.n[2 * nf + f]};
+  const double A = M.area[f];
+  const int64_t a = M.cl[f];
+  double qa[5];
+  q_arr(load_q(q, a), qa);
+  const double* ga = grad + 15 * a;
+  // face gradients of T, u, v, w (rows 0..3 of the cell gradient)
+  double gf[4][3];
+  double muf, kf, tmuf = 0.0;
+  const int kind = bc_kind(M, f);
+  if (kind == 0) {
+    const int64_t b = M.cr[f];
+    double qc[5];
+    q_arr(load_q(q, b), qc);
+    const double* gb = grad + 15 * b;
+    const double vl = M.vol[a], vr = M.vol[b];
+    const double iv = 1.0 / (vl + vr);
+    muf = (vl * suth(qc[0], V.a1, V.a2, V.a3) + vr * suth(qa[0], V.a1, V.a2, V.a3)) / (vl + vr);
+    kf = (vl * suth(qc[0], V.k1, V.k2, V.k3) + vr * suth(qa[0], V.k1, V.k2, V.k3)) / (vl + vr);
+    if (V.on == 2) tmuf = (V.tmu[b] * vl + V.tmu[a] * vr) / (vr + vl);
+    for (int k = 0; k < 3; ++k) o.uf[k] = iv * (vl * qc[1 + k] + vr * qa[1 + k]);
+    double d[3], d2 = 0;
+    for (int k = 0; k < 3; ++k) {
+      d[k] = M.rL[k * nf + f] - M.rR[k * nf + f];
+      d2 += d[k] * d[k];
+    }
+    o.dist = n[0] * d[0] + n[1] * d[1] + n[2] * d[2];
+    for (int v = 0; v < 4; ++v) {
+      double gm[3];
+      for (int k = 0; k < 3; ++k) gm[k] = 0.5 * (ga[3 * v + k] + gb[3 * v + k]);
+      const double c = ((qc[v] - qa[v]) - (gm[0] * d[0] + gm[1] * d[1] + gm[2] * d[2])) / d2;
+      for (int k = 0; k < 3; ++k) gf[v][k] = gm[k] + c * d[k];
+    }
+  } else {
+    const double* pb = qb + 5 * (f - M.nfi);
+    double qf[5];
+    for (int k = 0; k < 5; ++k) qf[k] = pb[k];
+    muf = suth(qf[0], V.a1, V.a2, V.a3);
+    kf = suth(qf[0], V.k1, V.k2, V.k3);
+    if (V.on == 2 && kind != FPSI_BC_VISCOUS_WALL) tmuf = V.tmu[a];
+    for (int k = 0; k < 3; ++k) o.uf[k] = qf[1 + k];
+    double r[3], r2 = 0;
+    for (int k = 0; k < 3; ++k) {
+      r[k] = M.rL[k * nf + f];
+      r2 += r[k] * r[k];
+    }
+    o.dist = n[0] * r[0] + n[1] * r[1] + n[2] * r[2];
+    for (int v = 0; v < 4; ++v) {
+      const double* gv = ga + 3 * v;
+      const double c = ((qf[v] - qa[v]) - (gv[0] * r[0] + gv[1] * r[1] + gv[2] * r[2])) / r2;
+      for (int k = 0; k < 3; ++k) gf[v][k] = gv[k] + c * r[k];
+    }
+  }
+  o.muT = muf + tmuf;
+  o.kT = kf + (V.on == 2 ? tmuf * V.cp_prt : 0.0);
+  if (kind == FPSI_BC_REFLECTING) {  // symmetry: no viscous flux (fluxViscous.loci:294-297)
+    for (int k = 0; k < 4; ++k) o.vf[k] = 0.0;
+    return o;
+  }
+  const double mt = o.muT;
+  const double dudx = gf[1][0], dvdy = gf[2][1], dwdz = gf[3][2];
+  const double dvdx = gf[2][0], dwdx = gf[3][0], dwdy = gf[3][1];
+  const double dudy = gf[1][1], dudz = gf[1][2], dvdz = gf[2][2];
+  const double divm = (dudx + dvdy + dwdz) * (1. / 3.);
+  const double txx = 2.0 * mt * (dudx - divm), tyy = 2.0 * mt * (dvdy - divm),
+               tzz = 2.0 * mt * (dwdz - divm);
+  const double txy = mt * (dudy + dvdx), txz = mt * (dudz + dwdx), tyz = mt * (dvdz + dwdy);
+  o.vf[0] = (txx * n[0] + txy * n[1] + txz * n[2]) * A;
+  o.vf[1] = (txy * n[0] + tyy * n[1] + tyz * n[2]) * A;
+  o.vf[2] = (txz * n[0] + tyz * n[1] + tzz * n[2]) * A;
+  o.vf[3] = (o.uf[0] * o.vf[0] + o.uf[1] * o.vf[1] + o.uf[2] * o.vf[2]);
+  // conduction; an adiabatic wall carries -qwall*A = 0 instead (bcViscousWall.loci:172-184)
+  if (kind != FPSI_BC_VISCOUS_WALL)
+    o.vf[3] += (gf[0][0] * n[0] + gf[0][1] * n[1] + gf[0][2] * n[2]) * o.kT * A;
+  return o;
+}
+
+// Adds sgn * (thin-layer viscous Jacobian) to a block stored in TB, one
+// rounding per term as the reference's += on real_fj blocks.
+template <class TB>
+__device__ __forceinline__ void add_visc_jac(TB* M, const VFace& v, const double n[3], double A,
+                                             double sgn) {
+  const double coef = v.muT * A / v.dist, third = 1.0 / 3.0;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      const double t = coef * ((r == c ? 1.0 : 0.0) + n[r] * n[c] * third);
+      M[5 * (1 + r) + 1 + c] = TB(double(M[5 * (1 + r) + 1 + c]) + sgn * t);
+    }
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) {
+      const double t = v.uf[r] * coef * ((r == c ? 1.0 : 0.0) + n[r] * n[c] * third);
+      M[21 + c] = TB(double(M[21 + c]) + sgn * t);
+    }
+  for (int c = 0; c < 3; ++c) M[21 + c] = TB(double(M[21 + c]) + sgn * 0.5 * v.vf[c]);
+  M[20] = TB(double(M[20]) + sgn * (v.kT * A / v.dist));
+}
+
+// ---------------------------------------------------------------------------
 // face flux + spectral radius, one thread per face
 // ---------------------------------------------------------------------------
 __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
                             const double* __restrict__ qb, const double* __restrict__ grad,
-                            const double* __restrict__ phi, Gas g, int kind,
+                            const double* __restrict__ phi, Gas g, int kind, Visc V,
                             double* __restrict__ F, double* __restrict__ mev) {
   const int64_t f = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (f >= M.nf) return;
@@ -275,7 +408,18 @@ __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
   const double nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
   const double A = M.area[f];
   double fl[5];
-  riemann(kind, s.L, s.R, nx, ny, nz, A, g, 0.0, 1.0, fl);
+  if (bc_kind(M, f) == FPSI_BC_VISCOUS_WALL) {
+    // pressure only, from the cell-centre pressure (bcViscousWall.loci:220-230)
+    const double p = s.qr[4];
+    fl[0] = 0.0, fl[1] = p * nx * A, fl[2] = p * ny * A, fl[3] = p * nz * A, fl[4] = 0.0;
+  } else {
+    riemann(kind, s.L, s.R, nx, ny, nz, A, g, 0.0, 1.0, fl);
+  }
+  if (V.on) {
+    const VFace v = viscous_face(M, q, qb, grad, V, f);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) fl[1 + k] -= v.vf[k];
+  }
   double* o = F + 5 * f;
 #pragma unroll
   for (int k = 0; k < 5; ++k) o[k] = fl[k];
@@ -453,7 +597,7 @@ constexpr int JAC_THREADS = 128;
 template <class TB>
 __global__ void __launch_bounds__(JAC_THREADS)
 k_face_jacobian(MeshView M, const double* __restrict__ q, const double* __restrict__ qb,
-                const double* __restrict__ grad, const double* __restrict__ phi, Gas g,
+                const double* __restrict__ grad, const double* __restrict__ phi, Gas g, Visc V,
                 TB* __restrict__ fjp, TB* __restrict__ fjm) {
   __shared__ TB stage[JAC_THREADS * 25];
   const int64_t f0 = int64_t(blockIdx.x) * JAC_THREADS;
@@ -468,12 +612,30 @@ k_face_jacobian(MeshView M, const double* __restrict__ q, const double* __restri
     nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
     A = M.area[f];
     ra = roe_average(s.L, s.R, nx, ny, nz, g, 0.0, 1.0);
-    jac_roe<TB>(ra, nx, ny, nz, A, g, +1, stage + 25 * threadIdx.x);
+    TB* st = stage + 25 * threadIdx.x;
+    if (bc_kind(M, f) == FPSI_BC_VISCOUS_WALL) {
+      // d(pressure flux)/dq of the wall (bcViscousWall.loci:232-240); u_f.n = 0
+#pragma unroll
+      for (int k = 0; k < 25; ++k) st[k] = TB(0);
+      st[9] = TB(nx * A), st[14] = TB(ny * A), st[19] = TB(nz * A);
+    } else {
+      jac_roe<TB>(ra, nx, ny, nz, A, g, +1, st);
+    }
+    if (V.on) {
+      const double nn[3] = {nx, ny, nz};
+      add_visc_jac<TB>(st, viscous_face(M, q, qb, grad, V, f), nn, A, +1.0);
+    }
   }
   __syncthreads();
   for (int64_t k = threadIdx.x; k < cnt; k += JAC_THREADS) fjp[25 * f0 + k] = stage[k];
   __syncthreads();
-  if (live && f < M.nfi) jac_roe<TB>(ra, nx, ny, nz, A, g, -1, stage + 25 * threadIdx.x);
+  if (live && f < M.nfi) {
+    jac_roe<TB>(ra, nx, ny, nz, A, g, -1, stage + 25 * threadIdx.x);
+    if (V.on) {
+      const double nn[3] = {nx, ny, nz};
+      add_visc_jac<TB>(stage + 25 * threadIdx.x, viscous_face(M, q, qb, grad, V, f), nn, A, -1.0);
+    }
+  }
   __syncthreads();
   // boundary faces have no fjm; their slots are written with whatever the
   // stage holds and never read
@@ -917,7 +1079,17 @@ dev::MeshView view(const fpsi_ctx* x) {
   M.Minv = x->d_Minv;
   M.cf_off = x->d_cf_off;
   M.cf = x->d_cf;
+  M.bcs = x->d_bcs;
   return M;
+}
+dev::Visc visc(const fpsi_ctx* x) {
+  dev::Visc V;
+  V.on = x->P.viscous;
+  V.a1 = x->P.mu_a1, V.a2 = x->P.mu_a2, V.a3 = x->P.mu_a3;
+  V.k1 = x->P.k_a1, V.k2 = x->P.k_a2, V.k3 = x->P.k_a3;
+  V.cp_prt = x->P.gamma * x->P.Rtilde / (x->P.gamma - 1.0) / x->P.Prt;
+  V.tmu = x->d_tmu;
+  return V;
 }
 dev::Gas gas(const fpsi_ctx* x) {
   dev::Gas g;
@@ -944,8 +1116,8 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
   prof_end(x);
   prof_begin(x, "face_flux");
   dev::k_face_flux<<<blocks_for(M.nf, 128), 128, 0, s>>>(M, x->d_q, x->d_qb, x->d_grad,
-                                                          x->d_phi, g, x->P.flux, x->d_F,
-                                                          x->d_mev);
+                                                          x->d_phi, g, x->P.flux, visc(x),
+                                                          x->d_F, x->d_mev);
   prof_end(x);
   prof_begin(x, "cell_residual");
   dev::k_cell_residual<<<x->nblk_norm, dev::NORM_THREADS, 0, s>>>(
@@ -979,7 +1151,7 @@ static int launch_assemble_t(fpsi_ctx* x) {
   TB* fjm = (TB*)x->d_fjm;
   prof_begin(x, "face_jacobian");
   dev::k_face_jacobian<TB><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
-      M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, fjp, fjm);
+      M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, visc(x), fjp, fjm);
   prof_end(x);
   prof_begin(x, "assemble_lu");
   dev::k_assemble<TB, TX><<<blocks_for(M.nc, 128), 128, 0, s>>>(

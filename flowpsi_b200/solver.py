@@ -214,6 +214,12 @@ class FlowPsi:
         N.check(N.lib().fpsi_set_state(self._ctx, N.dptr(T), N.dptr(pg), N.dptr(u)),
                 "fpsi_set_state")
 
+    def set_eddy_viscosity(self, tmu) -> None:
+        """eddy viscosity per cell for flowRegime turbulent (caller order)"""
+        t = np.ascontiguousarray(tmu, np.float64)
+        assert t.size == self.ncells
+        N.check(N.lib().fpsi_set_eddy_viscosity(self._ctx, N.dptr(t)), "fpsi_set_eddy_viscosity")
+
     def get_state(self):
         nc = self.ncells
         T, pg, u = np.empty(nc), np.empty(nc), np.empty(nc * 3)

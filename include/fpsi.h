@@ -96,11 +96,13 @@ typedef struct fpsi_params {
   double lsgs_rel_tol;     /* 0.1 */
   int32_t lsgs_max_iter;   /* 10 */
   int32_t precision;       /* fpsi_precision, default FPSI_PREC_REF */
-  int32_t viscous;         /* 0 inviscid, 1 laminar (Sutherland), 2 turbulent (needs tmu) */
+  int32_t viscous;         /* flowRegime: 0 inviscid, 1 laminar, 2 turbulent (eddy viscosity
+                              from fpsi_set_eddy_viscosity)      fluxViscous.loci:28-52 */
   int32_t reserved0;
-  double Pr;               /* 0.72 laminar Prandtl */
-  double Prt;              /* 0.9 turbulent Prandtl */
-  double sutherland_mu0, sutherland_T0, sutherland_S; /* air: 1.716e-5, 273.15, 110.4 */
+  double Prt;              /* turbulentPrandtlNumber 0.9           fluxViscous.loci:268-270 */
+  double mu_a1, mu_a2, mu_a3; /* Sutherland mu = a1 T^a2/(T+a3): 1.458e-6, 1.5, 110.4 */
+  double k_a1, k_a2, k_a3;    /* conductivity k = k1 T^k2/(T+k3): 2.495e-3, 1.5, 194
+                                 (sutherlandParameters, fluxViscous.loci:58-80) */
 } fpsi_params;
 
 typedef struct fpsi_bc {
@@ -207,6 +209,11 @@ int fpsi_get_lines(fpsi_ctx* ctx, int32_t* line_of_cell, int32_t* position,
                    int32_t* line_colour, int64_t* nlines);
 /* cell colour used by the multi-colour sweeps (caller order) */
 int fpsi_get_colours(fpsi_ctx* ctx, int32_t* colour);
+
+/* turbulent eddy viscosity tmu[nc] (caller order) used by flowRegime
+ * turbulent (muTotal = mu + tmu, kTotal = k + tmu Cp/Prt,
+ * fluxViscous.loci:179-201,268-277); zero until set */
+int fpsi_set_eddy_viscosity(fpsi_ctx* ctx, const double* tmu);
 
 /* state in Loci layout: T[nc], pg[nc], u[nc*3] (AoS) */
 int fpsi_set_state(fpsi_ctx* ctx, const double* T, const double* pg, const double* u);

@@ -475,6 +475,7 @@ struct orc_ctx {
   std::vector<int64_t> up, lo, bd;
   // state & results
   std::vector<double> T, pg, u;         // nc, nc, nc*3
+  std::vector<double> tmu;              // nc eddy viscosity (turbulent regime)
   std::vector<double> qb;               // nbf... stored per face (nf*5): boundary face state
   std::vector<double> grad, phi;        // nc*15, nc*5
   std::vector<double> F, maxev;         // nf*5, nf
@@ -671,6 +672,7 @@ extern "C" int orc_create(orc_ctx** out, const fpsi_mesh* m, const fpsi_params* 
   o->T.assign(nc, 0);
   o->pg.assign(nc, 0);
   o->u.assign(nc * 3, 0);
+  o->tmu.assign(nc, 0);
   *out = o;
   return FPSI_OK;
 }
@@ -762,6 +764,9 @@ static void bc_face_state(const orc_ctx* o, int64_t f, double q[5]) {
       ub = ui - 2.0 * un * n;
       break;
     }
+    case FPSI_BC_VISCOUS_WALL:  // stationary adiabatic wall (bcViscousWall.loci:148-218)
+      ub = mk(0, 0, 0);
+      break;
     default:  // extrapolate
       break;
   }
@@ -893,6 +898,124 @@ static void face_states(const orc_ctx* o, int64_t f, double qL[5], double qR[5])
   qR[4] = std::max(qR[4], plim);
 }
 
+static int bc_kind_of(const orc_ctx* o, int64_t f) {
+  return o->cr[f] >= 0 ? 0 : o->bcs[-o->cr[f] - 1].kind;
+}
+
+// viscous face flux, fluxViscous.loci:112-292 (+ bcViscousWall.loci:172-184
+// on adiabatic walls, no viscous flux on symmetry planes :294-297).  Face
+// gradients (Loci FVM gradv3d_f / grads_f, not vendored): mean of the two
+// cell gradients with the component along d = x_R - x_L replaced by the
+// difference quotient; at boundary faces the cell gradient corrected the
+// same way towards the face state.
+struct VFace {
+  double vf[4], uf[3], muT, kT, dist;
+};
+static double suth(double T, double a1, double a2, double a3) {
+  return a1 * std::pow(T, a2) / (T + a3);
+}
+static VFace viscous_face(const orc_ctx* o, int64_t f) {
+  const fpsi_params& P = o->P;
+  VFace v;
+  V3 n = v3(&o->an[3 * f]);
+  const double A = o->area[f];
+  const int64_t a = o->cl[f];
+  double qa[5];
+  cell_q(o, a, qa);
+  const double* ga = &o->grad[15 * a];
+  double gf[4][3];
+  double muf, kf, tmuf = 0;
+  const int kind = bc_kind_of(o, f);
+  if (kind == 0) {
+    const int64_t b = o->cr[f];
+    double qc[5];
+    cell_q(o, b, qc);
+    const double* gb = &o->grad[15 * b];
+    const double vl = o->vol[a], vr = o->vol[b];
+    muf = (vl * suth(qc[0], P.mu_a1, P.mu_a2, P.mu_a3) + vr * suth(qa[0], P.mu_a1, P.mu_a2, P.mu_a3)) /
+          (vl + vr);
+    kf = (vl * suth(qc[0], P.k_a1, P.k_a2, P.k_a3) + vr * suth(qa[0], P.k_a1, P.k_a2, P.k_a3)) /
+         (vl + vr);
+    if (P.viscous == 2) tmuf = (o->tmu[b] * vl + o->tmu[a] * vr) / (vr + vl);
+    const double factor = 1. / (vl + vr);
+    for (int k = 0; k < 3; ++k) v.uf[k] = factor * (vl * qc[1 + k] + vr * qa[1 + k]);
+    V3 d = v3(&o->rL[3 * f]) - v3(&o->rR[3 * f]);
+    v.dist = dot(n, d);
+    const double dd[3] = {d.x, d.y, d.z};
+    const double d2 = dot(d, d);
+    for (int w = 0; w < 4; ++w) {
+      double gm[3];
+      for (int k = 0; k < 3; ++k) gm[k] = 0.5 * (ga[3 * w + k] + gb[3 * w + k]);
+      const double c = ((qc[w] - qa[w]) - (gm[0] * dd[0] + gm[1] * dd[1] + gm[2] * dd[2])) / d2;
+      for (int k = 0; k < 3; ++k) gf[w][k] = gm[k] + c * dd[k];
+    }
+  } else {
+    const double* qf = &o->qb[5 * f];
+    muf = suth(qf[0], P.mu_a1, P.mu_a2, P.mu_a3);
+    kf = suth(qf[0], P.k_a1, P.k_a2, P.k_a3);
+    if (P.viscous == 2 && kind != FPSI_BC_VISCOUS_WALL) tmuf = o->tmu[a];
+    for (int k = 0; k < 3; ++k) v.uf[k] = qf[1 + k];
+    V3 r = v3(&o->rL[3 * f]);
+    v.dist = dot(n, r);
+    const double rr[3] = {r.x, r.y, r.z};
+    const double r2 = dot(r, r);
+    for (int w = 0; w < 4; ++w) {
+      const double* gv = ga + 3 * w;
+      const double c = ((qf[w] - qa[w]) - (gv[0] * rr[0] + gv[1] * rr[1] + gv[2] * rr[2])) / r2;
+      for (int k = 0; k < 3; ++k) gf[w][k] = gv[k] + c * rr[k];
+    }
+  }
+  v.muT = muf + tmuf;
+  v.kT = kf + (P.viscous == 2 ? tmuf * (P.gamma * P.Rtilde / (P.gamma - 1.0)) / P.Prt : 0.0);
+  if (kind == FPSI_BC_REFLECTING) {
+    for (int k = 0; k < 4; ++k) v.vf[k] = 0;
+    return v;
+  }
+  // tau, fluxViscous.loci:217-238
+  const double mt = v.muT;
+  const double dudx = gf[1][0], dvdy = gf[2][1], dwdz = gf[3][2];
+  const double dvdx = gf[2][0], dwdx = gf[3][0], dwdy = gf[3][1];
+  const double dudy = gf[1][1], dudz = gf[1][2], dvdz = gf[2][2];
+  const double divm = (dudx + dvdy + dwdz) * (1. / 3.);
+  const double txx = 2.0 * mt * (dudx - divm), tyy = 2.0 * mt * (dvdy - divm),
+               tzz = 2.0 * mt * (dwdz - divm);
+  const double txy = mt * (dudy + dvdx), txz = mt * (dudz + dwdx), tyz = mt * (dvdz + dwdy);
+  // vflux, fluxViscous.loci:279-292
+  v.vf[0] = (txx * n.x + txy * n.y + txz * n.z) * A;
+  v.vf[1] = (txy * n.x + tyy * n.y + tyz * n.z) * A;
+  v.vf[2] = (txz * n.x + tyz * n.y + tzz * n.z) * A;
+  v.vf[3] = (v.uf[0] * v.vf[0] + v.uf[1] * v.vf[1] + v.uf[2] * v.vf[2]);
+  if (kind != FPSI_BC_VISCOUS_WALL)
+    v.vf[3] += (gf[0][0] * n.x + gf[0][1] * n.y + gf[0][2] * n.z) * v.kT * A;
+  return v;
+}
+
+// thin-layer viscous Jacobian, fluxViscous.loci:315-448: Fj += sgn * J,
+// each term added separately as the reference's += on real_fj blocks
+template <class TB>
+static void add_visc_jac(TB* M, const VFace& v, V3 n3, double A, double sgn) {
+  const double n[3] = {n3.x, n3.y, n3.z};
+  const double coef = v.muT * A / v.dist, third = 1.0 / 3.0;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      const double t = coef * ((r == c ? 1.0 : 0.0) + n[r] * n[c] * third);
+      M[5 * (1 + r) + 1 + c] = TB(double(M[5 * (1 + r) + 1 + c]) + sgn * t);
+    }
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) {
+      const double t = v.uf[r] * coef * ((r == c ? 1.0 : 0.0) + n[r] * n[c] * third);
+      M[21 + c] = TB(double(M[21 + c]) + sgn * t);
+    }
+  for (int c = 0; c < 3; ++c) M[21 + c] = TB(double(M[21 + c]) + sgn * 0.5 * v.vf[c]);
+  M[20] = TB(double(M[20]) + sgn * (v.kT * A / v.dist));
+}
+
+extern "C" int orc_set_eddy_viscosity(orc_ctx* o, const double* tmu) {
+  std::memcpy(o->tmu.data(), tmu, sizeof(double) * o->nc);
+  o->have_resid = o->have_asm = o->have_dq = false;
+  return FPSI_OK;
+}
+
 extern "C" int orc_residual(orc_ctx* o, double* src_out, fpsi_resid* norms) {
   const int64_t nc = o->nc, nf = o->nf;
   const fpsi_params& P = o->P;
@@ -908,9 +1031,22 @@ extern "C" int orc_residual(orc_ctx* o, double* src_out, fpsi_resid* norms) {
     double qL[5], qR[5];
     face_states(o, f, qL, qR);
     V3 n = v3(&o->an[3 * f]);
-    riemann_flux(P.flux, &o->F[5 * f], qL[4], qL[0], mk(qL[1], qL[2], qL[3]), qR[4], qR[0],
-                 mk(qR[1], qR[2], qR[3]), n, o->area[f], P.Pambient, P.Rtilde, P.gamma, 0.0,
-                 1.0);
+    if (bc_kind_of(o, f) == FPSI_BC_VISCOUS_WALL) {
+      // wall iflux: pressure only, cell-centre pressure (bcViscousWall.loci:220-230)
+      const double p = o->qb[5 * f + 4];
+      const V3 a = n * o->area[f];
+      double* F = &o->F[5 * f];
+      F[0] = 0, F[1] = p * a.x, F[2] = p * a.y, F[3] = p * a.z, F[4] = 0;
+    } else {
+      riemann_flux(P.flux, &o->F[5 * f], qL[4], qL[0], mk(qL[1], qL[2], qL[3]), qR[4], qR[0],
+                   mk(qR[1], qR[2], qR[3]), n, o->area[f], P.Pambient, P.Rtilde, P.gamma, 0.0,
+                   1.0);
+    }
+    if (P.viscous) {
+      // src[cl] += vflux, src[cr] -= vflux (fluxViscous.loci:299-310)
+      const VFace v = viscous_face(o, f);
+      for (int k = 0; k < 4; ++k) o->F[5 * f + 1 + k] -= v.vf[k];
+    }
     // maxev_f, solverSetup.loci:81-105 (eta == 1)
     double ql[5], qr[5];
     cell_q(o, o->cl[f], ql);
@@ -1056,13 +1192,24 @@ static int assemble_t(orc_ctx* o, std::vector<TB>& fjp, std::vector<TB>& fjm,
     double qL[5], qR[5];
     face_states(o, f, qL, qR);
     V3 n = v3(&o->an[3 * f]);
-    roe_jacobian<TB>(&fjp[25 * f], qL[4], qL[0], mk(qL[1], qL[2], qL[3]), qR[4], qR[0],
-                     mk(qR[1], qR[2], qR[3]), n, o->area[f], P.Pambient, P.Rtilde, P.gamma,
-                     0.0, 1.0, 1);
+    if (bc_kind_of(o, f) == FPSI_BC_VISCOUS_WALL) {
+      // srcJ -= d(wall pressure flux)/dq (bcViscousWall.loci:232-240), u_f.n = 0
+      TB* J = &fjp[25 * f];
+      J[9] = TB(n.x * o->area[f]), J[14] = TB(n.y * o->area[f]), J[19] = TB(n.z * o->area[f]);
+    } else {
+      roe_jacobian<TB>(&fjp[25 * f], qL[4], qL[0], mk(qL[1], qL[2], qL[3]), qR[4], qR[0],
+                       mk(qR[1], qR[2], qR[3]), n, o->area[f], P.Pambient, P.Rtilde, P.gamma,
+                       0.0, 1.0, 1);
+    }
     if (o->cr[f] >= 0)
       roe_jacobian<TB>(&fjm[25 * f], qL[4], qL[0], mk(qL[1], qL[2], qL[3]), qR[4], qR[0],
                        mk(qR[1], qR[2], qR[3]), n, o->area[f], P.Pambient, P.Rtilde, P.gamma,
                        0.0, 1.0, -1);
+    if (P.viscous) {
+      const VFace v = viscous_face(o, f);
+      add_visc_jac<TB>(&fjp[25 * f], v, n, o->area[f], +1.0);
+      if (o->cr[f] >= 0) add_visc_jac<TB>(&fjm[25 * f], v, n, o->area[f], -1.0);
+    }
   }
   D.assign(nc * 25, TB(0));
   LU.assign(nc * 25, TB(0));

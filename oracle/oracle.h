@@ -25,6 +25,7 @@ int  orc_set_params(orc_ctx* o, const fpsi_params* params);
 int  orc_get_geometry(orc_ctx* o, double* vol, double* cellcenter, double* face_an,
                       double* face_area, double* facecenter);
 int  orc_set_state(orc_ctx* o, const double* T, const double* pg, const double* u);
+int  orc_set_eddy_viscosity(orc_ctx* o, const double* tmu);
 int  orc_get_state(orc_ctx* o, double* T, double* pg, double* u);
 int  orc_residual(orc_ctx* o, double* src, fpsi_resid* norms);
 int  orc_get_reconstruction(orc_ctx* o, double* grad, double* limiter);

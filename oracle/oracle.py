@@ -27,6 +27,7 @@ _SIGS = {
     "orc_set_params": (C.c_int, [C.c_void_p, C.POINTER(N.Params)]),
     "orc_get_geometry": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp]),
     "orc_set_state": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+    "orc_set_eddy_viscosity": (C.c_int, [C.c_void_p, _dp]),
     "orc_get_state": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
     "orc_residual": (C.c_int, [C.c_void_p, _dp, C.POINTER(N.Resid)]),
     "orc_get_reconstruction": (C.c_int, [C.c_void_p, _dp, _dp]),
@@ -199,6 +200,10 @@ class Oracle:
     def set_state(self, T, pg, u):
         T, pg, u = (np.ascontiguousarray(v, np.float64).reshape(-1) for v in (T, pg, u))
         _chk(olib().orc_set_state(self._h, _d(T), _d(pg), _d(u)), "orc_set_state")
+
+    def set_eddy_viscosity(self, tmu):
+        t = np.ascontiguousarray(tmu, np.float64)
+        _chk(olib().orc_set_eddy_viscosity(self._h, _d(t)), "orc_set_eddy_viscosity")
 
     def get_state(self):
         nc = self.ncells

@@ -158,3 +158,31 @@ def test_lsgs_relaxation_and_stopping_rules():
     single = [np.array([c], np.int32) for c in range(o.ncells)]
     o.lsgs_solve(single)
     assert r_default <= o.linear_residual()[1] * 1.0001
+
+
+def test_viscous_linear_shear_has_no_net_force_inside():
+    """a linear velocity field at constant T has constant stress: the viscous
+    fluxes of a closed interior cell cancel (face gradients are exact for
+    linear fields), so laminar and inviscid residuals agree there"""
+    res = {}
+    for visc in (0, 1):
+        case = cases.boundary_layer_block(6, 8, 4, dy0=1e-3, growth=1.2, viscous=visc,
+                                          solver="sgs", precision="fp64")
+        p = case.params
+        p.limiter = 2  # none: unlimited gradients keep the linear field exact
+        o = Oracle(case.mesh, p)
+        cc = o.geometry()["cellcenter"]
+        nc = o.ncells
+        u = np.zeros((nc, 3))
+        u[:, 0] = 50.0 + 2.0e3 * cc[:, 1]  # z is periodic: no z dependence
+        o.set_state(np.full(nc, 300.0), np.full(nc, 2e4), u)
+        res[visc] = o.residual()[0]
+    # two cells away from the walls: the boundary states (which differ
+    # between the two regimes) reach one cell further through the gradients
+    idx = np.arange(nc)
+    i, j = idx % 6, (idx // 6) % 8
+    inner = (i >= 2) & (i <= 3) & (j >= 2) & (j <= 5)
+    mu = float(cases.sutherland_mu(300.0))
+    scale = mu * 2.0e3 * o.geometry()["area"].max()
+    d = np.abs(res[1][inner, 1:4] - res[0][inner, 1:4]).max()
+    assert d < 1e-10 * scale, (d, scale)
