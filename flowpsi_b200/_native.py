@@ -119,6 +119,25 @@ _SIGS = {
     "fpsi_get_blocks": (C.c_int, [_ctx, _vp, _vp, _vp, _vp]),
     "fpsi_linear_solve": (C.c_int, [_ctx, _dp, _dp, C.POINTER(LsInfo)]),
     "fpsi_linear_residual": (C.c_int, [_ctx, _dp, _dp]),
+    "fpsi_set_iterate": (C.c_int, [_ctx, _dp]),
+    "fpsi_get_iterate": (C.c_int, [_ctx, _dp]),
+    "fpsi_linear_sweeps": (C.c_int, [_ctx, C.c_int32]),
+    "fpsi_gnn_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_uint64]),
+    "fpsi_gnn_destroy": (C.c_int, [C.c_void_p]),
+    "fpsi_gnn_num_params": (C.c_int64, [C.c_void_p]),
+    "fpsi_gnn_get_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "fpsi_gnn_set_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "fpsi_gnn_add_snapshot": (C.c_int, [C.c_void_p, _ctx, _dp]),
+    "fpsi_gnn_clear_snapshots": (C.c_int, [C.c_void_p]),
+    "fpsi_gnn_num_snapshots": (C.c_int, [C.c_void_p]),
+    "fpsi_gnn_snapshot_cells": (C.c_int64, [C.c_void_p, C.c_int32]),
+    "fpsi_gnn_get_snapshot": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_float),
+                                        C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                        C.POINTER(C.c_float)]),
+    "fpsi_gnn_loss_grad": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_uint64, _dp,
+                                     C.POINTER(C.c_float)]),
+    "fpsi_gnn_train": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_uint64, C.c_double, _dp]),
+    "fpsi_gnn_predict": (C.c_int, [C.c_void_p, _ctx, _dp]),
     "fpsi_update": (C.c_int, [_ctx, _dp]),
     "fpsi_newton_step": (C.c_int, [_ctx, C.POINTER(StepInfo)]),
     "fpsi_run": (C.c_int, [_ctx, C.c_int32, C.POINTER(Resid)]),

@@ -275,7 +275,7 @@ int fpsi_destroy(fpsi_ctx* x) {
                 x->d_Minv, x->d_cf_off, x->d_cf, x->d_colour_cells, x->d_bcs, x->d_q,
                 x->d_qb, x->d_grad, x->d_phi, x->d_F, x->d_mev, x->d_src, x->d_dtau, x->d_tmu,
                 x->d_part, x->d_resid, x->d_amin, x->d_err, x->d_perm, x->d_stage, x->d_ci, x->d_ccol,
-                x->d_nbr, x->d_colinfo};
+                x->d_nbr, x->d_colinfo, x->d_cnb_off, x->d_cnb, x->d_xprev};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (x->h_resid) cudaFreeHost(x->h_resid);
@@ -397,7 +397,7 @@ int fpsi_set_params(fpsi_ctx* x, const fpsi_params* p) {
   int rc = check_params(p);
   if (rc) return rc;
   x->P = *p;
-  x->have_asm = x->have_dq = false;
+  x->have_asm = x->have_dq = x->have_xprev = false;
   if (is_lsgs(x) && !x->keep_D) {
     x->keep_D = true;
     x->alloc_prec = -1;
@@ -498,7 +498,7 @@ int fpsi_set_state(fpsi_ctx* x, const double* T, const double* pg, const double*
   FPSI_CUDA_TRY(cudaMemcpyAsync(x->d_stage + 2 * nc, u, 3 * b, cudaMemcpyHostToDevice, x->stream));
   int rc = fpsi::launch_state(x, true);
   if (rc) return rc;
-  x->have_resid = x->have_asm = x->have_dq = false;
+  x->have_resid = x->have_asm = x->have_dq = x->have_xprev = false;
   return sync(x);
 }
 
@@ -539,7 +539,7 @@ int fpsi_residual(fpsi_ctx* x, double* src, fpsi_resid* norms) {
   if (src) unpermute_cells(x, s.data(), 5, src);
   if (norms) fill_norms(x, x->h_resid, norms);
   x->have_resid = true;
-  x->have_asm = x->have_dq = false;
+  x->have_asm = x->have_dq = x->x_preset = false;
   return has_nan(x->h_resid) ? FPSI_E_NAN : FPSI_OK;
 }
 
@@ -725,10 +725,11 @@ int fpsi_linear_solve(fpsi_ctx* x, const double* x0, double* dq, fpsi_lsinfo* in
   }
   if (x0) {
     if ((rc = upload_x(x, x0))) return rc;
-  } else if (x->have_dq) {
+  } else if (x->have_dq && !x->x_preset) {
     // iterate was consumed by an earlier solve: rebuild the block Jacobi start
     if ((rc = fpsi::launch_jacobi_start(x))) return rc;
   }
+  x->x_preset = false;
   if ((rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter))) return rc;
   if ((rc = sync(x))) return rc;
   x->have_dq = true;
@@ -738,6 +739,33 @@ int fpsi_linear_solve(fpsi_ctx* x, const double* x0, double* dq, fpsi_lsinfo* in
     info->status = FPSI_OK;
     info->resid0 = info->resid = 0;
   }
+  return FPSI_OK;
+}
+
+int fpsi_set_iterate(fpsi_ctx* x, const double* x0) {
+  if (!x || !x0) return FPSI_E_INVALID;
+  if (!x->have_asm) return FPSI_E_STATE;
+  int rc = upload_x(x, x0);
+  if (rc) return rc;
+  x->x_preset = true;
+  return FPSI_OK;
+}
+
+int fpsi_get_iterate(fpsi_ctx* x, double* dq) {
+  if (!x || !dq) return FPSI_E_INVALID;
+  if (!x->have_asm) return FPSI_E_STATE;
+  return download_x(x, dq);
+}
+
+int fpsi_linear_sweeps(fpsi_ctx* x, int32_t nsweeps) {
+  if (!x || nsweeps < 0) return FPSI_E_INVALID;
+  if (!x->have_asm) return FPSI_E_STATE;
+  if (is_lsgs(x)) return FPSI_E_UNSUPPORTED;
+  int rc = fpsi::launch_sgs(x, nsweeps);
+  if (rc) return rc;
+  if ((rc = sync(x))) return rc;
+  x->have_dq = true;
+  x->x_preset = false;
   return FPSI_OK;
 }
 

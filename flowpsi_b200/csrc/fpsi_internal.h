@@ -150,6 +150,15 @@ struct fpsi_ctx {
   int alloc_prec = -1;
   bool keep_D = true;
   bool have_resid = false, have_asm = false, have_dq = false;
+  bool x_preset = false;       // the iterate holds a caller-provided start
+  // interior-face cell graph (RCM order, CSR), built on first use by the
+  // learned start
+  int32_t *d_cnb_off = nullptr, *d_cnb = nullptr;
+  int64_t cnb_n = 0;
+  // copy of the last applied update (colour order, TX), kept once a learned
+  // start has used this context: the next system's start uses it as input
+  void* d_xprev = nullptr;     // nc * 5 * 8 bytes
+  bool keep_prev = false, have_xprev = false;
   int64_t device_bytes = 0;
   // caller-order staging for state transfers (T, pg, u) and the permutation
   int32_t* d_perm = nullptr;   // new cell id -> caller cell id

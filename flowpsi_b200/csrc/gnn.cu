@@ -1,0 +1,905 @@
+// gnn.cu -- learned starting iterate for the block relaxation.
+//
+// No counterpart in the reference: the hook is the starting iterate of the
+// SGS/LSGS solve (linearSolverSGS.loci:57-69, linearSolverLSGS.loci:1708-1728),
+// which the reference sets to the block Jacobi solution x_J = D^-1 B.
+//
+// Model.  Per cell c the 40 inputs are the right-hand side B_c (5), the
+// diagonal block D_c (25), the block Jacobi solution x_J,c = D_c^-1 B_c (5)
+// and the context's previous update dq_prev,c (5; zero before the first
+// update), made scale free per system: B by its RMS per component (rs),
+// x_J and dq_prev by the RMS of x_J per component (xs), D_ij by xs_j/rs_i (so
+// that the scaled blocks map the scaled x_J onto the scaled B).  Neighbour
+// information enters through the mean aggregation of every layer.  Three
+// message-passing layers
+//     h' = GELU(W_s h + W_n mean_{n in N(c)} h + b)        (40 -> 64 -> 64 -> 64)
+// and a linear head (64 -> 5) give d, and the starting iterate is
+//     x0 = x_J + xs * d,
+// so a network that outputs zero reproduces the reference's start.  Weights
+// are used in BF16 with FP32 accumulation; FP32 master weights and Adam
+// moments are kept for training.  Training targets are (dq - x_J)/xs for
+// solver-generated converged dq.  All reductions (weight gradients, loss)
+// are per-block partials summed in a fixed order: training is reproducible.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "fpsi_internal.h"
+#include "kernels.cuh"
+
+namespace {
+
+constexpr int NIN = 40;
+constexpr int W = 64;  // hidden width
+constexpr int NOUT = 5;
+constexpr int NLAYER = 3;
+constexpr int GT = 128;  // threads per block for the per-cell kernels
+
+// flat parameter layout (FP32 masters)
+struct Layout {
+  int64_t ws[NLAYER], wn[NLAYER], b[NLAYER], wo, bo, total;
+  int fan_in[NLAYER];
+};
+Layout layout() {
+  Layout L;
+  int64_t o = 0;
+  for (int l = 0; l < NLAYER; ++l) {
+    const int fin = l == 0 ? NIN : W;
+    L.fan_in[l] = fin;
+    L.ws[l] = o, o += int64_t(W) * fin;
+    L.wn[l] = o, o += int64_t(W) * fin;
+    L.b[l] = o, o += W;
+  }
+  L.wo = o, o += int64_t(NOUT) * W;
+  L.bo = o, o += NOUT;
+  L.total = o;
+  return L;
+}
+
+// cell graph of one mesh: interior-face neighbours in RCM order (CSR) and
+// the RCM -> caller cell map
+struct Graph {
+  int64_t nc = 0;
+  const int32_t* off = nullptr;
+  const int32_t* nb = nullptr;
+};
+
+struct Snapshot {
+  int64_t nc = 0;
+  int32_t *d_off = nullptr, *d_nb = nullptr;  // own copy of the system's graph
+  std::vector<int32_t> perm;
+  float* feat = nullptr;    // [nc][40]
+  float* target = nullptr;  // [nc][5]  (dq - xJ)/xs
+  float* xj = nullptr;      // [nc][5]
+  float xs[5], rs[5];
+  Graph graph() const { return Graph{nc, d_off, d_nb}; }
+};
+
+}  // namespace
+
+struct fpsi_gnn {
+  Layout L;
+  float *d_w = nullptr, *d_m = nullptr, *d_v = nullptr, *d_g = nullptr;
+  __nv_bfloat16* d_wb = nullptr;
+  int64_t adam_t = 0;
+  // activations for one full-graph pass, sized for `cap` cells
+  int64_t cap = 0;
+  float *d_h[NLAYER + 1] = {nullptr}, *d_agg[NLAYER] = {nullptr}, *d_z[NLAYER] = {nullptr};
+  float *d_y = nullptr, *d_dh = nullptr, *d_dh2 = nullptr, *d_dz = nullptr, *d_dagg = nullptr;
+  float* d_part = nullptr;  // weight-gradient partials
+  double* d_lpart = nullptr;
+  std::vector<Snapshot> snaps;
+  cudaStream_t stream = nullptr;
+};
+
+namespace {
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float x) {
+  const float cdf = 0.5f * (1.0f + erff(x * 0.70710678118654752f));
+  const float pdf = expf(-0.5f * x * x) * 0.39894228040143268f;
+  return cdf + x * pdf;
+}
+
+// agg[c] = mean over neighbours of h[n]  (width fin)
+__global__ void k_aggregate(int64_t nc, int fin, const int32_t* __restrict__ off,
+                            const int32_t* __restrict__ nb, const float* __restrict__ h,
+                            float* __restrict__ agg) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= nc * fin) return;
+  const int64_t c = i / fin;
+  const int k = int(i % fin);
+  const int32_t a = off[c], b = off[c + 1];
+  float s = 0.f;
+  for (int32_t e = a; e < b; ++e) s += h[int64_t(nb[e]) * fin + k];
+  agg[i] = b > a ? s / float(b - a) : 0.f;
+}
+
+// out[c][j] = act(b_j + sum_i Ws[j][i] h[c][i] + Wn[j][i] agg[c][i]); z = pre-activation
+__global__ void __launch_bounds__(GT) k_mp_forward(int64_t nc, int fin, const __nv_bfloat16* __restrict__ ws,
+                                                   const __nv_bfloat16* __restrict__ wn,
+                                                   const __nv_bfloat16* __restrict__ bb,
+                                                   const float* __restrict__ h,
+                                                   const float* __restrict__ agg,
+                                                   float* __restrict__ z, float* __restrict__ out) {
+  __shared__ float sws[W * W], swn[W * W], sb[W];
+  for (int i = threadIdx.x; i < W * fin; i += GT) {
+    sws[i] = __bfloat162float(ws[i]);
+    swn[i] = __bfloat162float(wn[i]);
+  }
+  for (int i = threadIdx.x; i < W; i += GT) sb[i] = __bfloat162float(bb[i]);
+  __syncthreads();
+  const int64_t c = int64_t(blockIdx.x) * GT + threadIdx.x;
+  if (c >= nc) return;
+  const float* hc = h + c * fin;
+  const float* ac = agg + c * fin;
+  for (int j0 = 0; j0 < W; j0 += 16) {
+    float acc[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) acc[j] = sb[j0 + j];
+    for (int i = 0; i < fin; ++i) {
+      const float hv = hc[i], av = ac[i];
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        acc[j] += sws[(j0 + j) * fin + i] * hv + swn[(j0 + j) * fin + i] * av;
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      z[c * W + j0 + j] = acc[j];
+      out[c * W + j0 + j] = gelu(acc[j]);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(GT) k_head_forward(int64_t nc, const __nv_bfloat16* __restrict__ wo,
+                                                     const __nv_bfloat16* __restrict__ bo,
+                                                     const float* __restrict__ h, float* __restrict__ y) {
+  __shared__ float sw[NOUT * W], sb[NOUT];
+  for (int i = threadIdx.x; i < NOUT * W; i += GT) sw[i] = __bfloat162float(wo[i]);
+  if (threadIdx.x < NOUT) sb[threadIdx.x] = __bfloat162float(bo[threadIdx.x]);
+  __syncthreads();
+  const int64_t c = int64_t(blockIdx.x) * GT + threadIdx.x;
+  if (c >= nc) return;
+  float acc[NOUT];
+#pragma unroll
+  for (int k = 0; k < NOUT; ++k) acc[k] = sb[k];
+  for (int i = 0; i < W; ++i) {
+    const float hv = h[c * W + i];
+#pragma unroll
+    for (int k = 0; k < NOUT; ++k) acc[k] += sw[k * W + i] * hv;
+  }
+#pragma unroll
+  for (int k = 0; k < NOUT; ++k) y[c * NOUT + k] = acc[k];
+}
+
+// batch membership: a counter-based hash of (seed, cell) below the threshold
+__device__ __forceinline__ bool in_batch(uint64_t seed, int64_t c, uint64_t thr) {
+  uint64_t x = seed * 0x9E3779B97F4A7C15ull + uint64_t(c) + 0x632BE59BD9B4E019ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  x ^= x >> 31;
+  return x <= thr;
+}
+
+// dy = 2 (y - t) / (5 n_batch) on the batch, 0 elsewhere; block partials of
+// the squared error and of the batch count
+__global__ void __launch_bounds__(GT) k_loss(int64_t nc, const float* __restrict__ y,
+                                             const float* __restrict__ t, uint64_t seed, uint64_t thr,
+                                             float* __restrict__ dy, double* __restrict__ part) {
+  const int64_t c = int64_t(blockIdx.x) * GT + threadIdx.x;
+  double se = 0, cnt = 0;
+  if (c < nc) {
+    const bool m = in_batch(seed, c, thr);
+#pragma unroll
+    for (int k = 0; k < NOUT; ++k) {
+      const float d = y[c * NOUT + k] - t[c * NOUT + k];
+      dy[c * NOUT + k] = m ? d : 0.f;  // scaled later by 2/(5 n)
+      if (m) se += double(d) * double(d);
+    }
+    cnt = m ? 1.0 : 0.0;
+  }
+  __shared__ double s1[GT], s2[GT];
+  s1[threadIdx.x] = se, s2[threadIdx.x] = cnt;
+  __syncthreads();
+  for (int st = GT / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) s1[threadIdx.x] += s1[threadIdx.x + st], s2[threadIdx.x] += s2[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[2 * blockIdx.x] = s1[0], part[2 * blockIdx.x + 1] = s2[0];
+}
+
+__global__ void k_scale(int64_t n, float* __restrict__ a, const double* __restrict__ loss_cnt) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double cnt = loss_cnt[1];
+  a[i] = float(double(a[i]) * (cnt > 0 ? 2.0 / (5.0 * cnt) : 0.0));
+}
+
+// sum of the loss partials: out[0] = mean squared error, out[1] = batch size
+__global__ void k_loss_final(const double* __restrict__ part, int nblk, double* __restrict__ out) {
+  __shared__ double s1[256], s2[256];
+  double a = 0, b = 0;
+  for (int i = threadIdx.x; i < nblk; i += 256) a += part[2 * i], b += part[2 * i + 1];
+  s1[threadIdx.x] = a, s2[threadIdx.x] = b;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st) s1[threadIdx.x] += s1[threadIdx.x + st], s2[threadIdx.x] += s2[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = s2[0] > 0 ? s1[0] / (5.0 * s2[0]) : 0.0;
+    out[1] = s2[0];
+  }
+}
+
+// weight-gradient partials over blocks of RB cells:
+// part[blk][j][i] = sum_c dz[c][j] * a[c][i]   (a = h or agg), and bias sums
+constexpr int RB = 256;
+__global__ void k_wgrad_partial(int64_t nc, int nout, int fin, const float* __restrict__ dz,
+                                const float* __restrict__ a, float* __restrict__ part) {
+  const int64_t c0 = int64_t(blockIdx.x) * RB;
+  const int64_t c1 = min(nc, c0 + RB);
+  float* o = part + int64_t(blockIdx.x) * nout * (fin + 1);
+  for (int w = threadIdx.x; w < nout * (fin + 1); w += blockDim.x) {
+    const int j = w / (fin + 1), i = w % (fin + 1);
+    float s = 0.f;
+    if (i < fin) {
+      for (int64_t c = c0; c < c1; ++c) s += dz[c * nout + j] * a[c * fin + i];
+    } else {
+      for (int64_t c = c0; c < c1; ++c) s += dz[c * nout + j];
+    }
+    o[w] = s;
+  }
+}
+// g[wofs + j*fin + i] (and g[bofs + j] when bofs >= 0) = sum over blocks
+__global__ void k_wgrad_reduce(int nblk, int nout, int fin, const float* __restrict__ part,
+                               float* __restrict__ g, int64_t wofs, int64_t bofs) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= nout * (fin + 1)) return;
+  const int j = w / (fin + 1), i = w % (fin + 1);
+  double s = 0;
+  for (int b = 0; b < nblk; ++b) s += part[int64_t(b) * nout * (fin + 1) + w];
+  if (i < fin)
+    g[wofs + j * fin + i] = float(s);
+  else if (bofs >= 0)
+    g[bofs + j] = float(s);
+}
+
+// dh[c][i] = sum_j W[j][i] dz[c][j]   (W: nout x fin, bf16)
+__global__ void __launch_bounds__(GT) k_back_dense(int64_t nc, int nout, int fin,
+                                                   const __nv_bfloat16* __restrict__ w,
+                                                   const float* __restrict__ dz,
+                                                   float* __restrict__ dh) {
+  __shared__ float sw[W * W];
+  for (int i = threadIdx.x; i < nout * fin; i += GT) sw[i] = __bfloat162float(w[i]);
+  __syncthreads();
+  const int64_t c = int64_t(blockIdx.x) * GT + threadIdx.x;
+  if (c >= nc) return;
+  for (int i0 = 0; i0 < fin; i0 += 16) {
+    float acc[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) acc[i] = 0.f;
+    for (int j = 0; j < nout; ++j) {
+      const float d = dz[c * nout + j];
+#pragma unroll
+      for (int i = 0; i < 16; ++i)
+        if (i0 + i < fin) acc[i] += sw[j * fin + i0 + i] * d;
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+      if (i0 + i < fin) dh[c * fin + i0 + i] = acc[i];
+  }
+}
+
+// dh[n] += sum_{c in N(n)} dagg[c] / deg(c)  (the graph is symmetric)
+__global__ void k_back_aggregate(int64_t nc, int fin, const int32_t* __restrict__ off,
+                                 const int32_t* __restrict__ nb, const float* __restrict__ dagg,
+                                 float* __restrict__ dh) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= nc * fin) return;
+  const int64_t n = i / fin;
+  const int k = int(i % fin);
+  float s = 0.f;
+  for (int32_t e = off[n]; e < off[n + 1]; ++e) {
+    const int32_t c = nb[e];
+    const int32_t deg = off[c + 1] - off[c];
+    s += dagg[int64_t(c) * fin + k] / float(deg);
+  }
+  dh[i] += s;
+}
+
+// dz = dh * GELU'(z)
+__global__ void k_back_gelu(int64_t n, const float* __restrict__ dh, const float* __restrict__ z,
+                            float* __restrict__ dz) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) dz[i] = dh[i] * gelu_grad(z[i]);
+}
+
+__global__ void k_adam(int64_t n, float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
+                       const float* __restrict__ g, __nv_bfloat16* __restrict__ wb, float lr,
+                       float b1, float b2, float eps, float c1, float c2) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi, v[i] = vi;
+  const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  w[i] = wi;
+  wb[i] = __float2bfloat16_rn(wi);
+}
+
+__global__ void k_to_bf16(int64_t n, const float* __restrict__ w, __nv_bfloat16* __restrict__ wb) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) wb[i] = __float2bfloat16_rn(w[i]);
+}
+
+// features of one assembled system (RCM order): B = float(src), D, x_J
+// gathered from the colour-order iterate right after assembly, dq_prev from
+// the colour-order copy of the last update (null: zero)
+template <class TB, class TX>
+__global__ void k_features_raw(int64_t nc, const double* __restrict__ src, const TB* __restrict__ D,
+                               const TX* __restrict__ xj_ci, const TX* __restrict__ xprev_ci,
+                               const int32_t* __restrict__ ci,
+                               float* __restrict__ raw /* [nc][40]: B, D, unused, dq_prev */,
+                               float* __restrict__ xj) {
+  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  for (int k = 0; k < 5; ++k) raw[c * NIN + k] = float(src[5 * c + k]);
+  for (int k = 0; k < 25; ++k) raw[c * NIN + 5 + k] = float(D[25 * c + k]);
+  const int64_t x = ci[c];
+  for (int k = 0; k < 5; ++k) xj[c * 5 + k] = float(xj_ci[5 * x + k]);
+  for (int k = 0; k < 5; ++k) raw[c * NIN + 35 + k] = xprev_ci ? float(xprev_ci[5 * x + k]) : 0.f;
+}
+
+// per-component sums of squares of B (raw[:,0:5]) and x_J, block partials
+__global__ void k_rms_partial(int64_t nc, const float* __restrict__ raw, const float* __restrict__ xj,
+                              double* __restrict__ part) {
+  const int64_t c = int64_t(blockIdx.x) * GT + threadIdx.x;
+  __shared__ double sh[10][GT];
+  for (int k = 0; k < 5; ++k) {
+    const double b = c < nc ? double(raw[c * NIN + k]) : 0.0;
+    const double x = c < nc ? double(xj[c * 5 + k]) : 0.0;
+    sh[k][threadIdx.x] = b * b;
+    sh[5 + k][threadIdx.x] = x * x;
+  }
+  __syncthreads();
+  for (int st = GT / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int k = 0; k < 10; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 10; ++k) part[10 * blockIdx.x + k] = sh[k][0];
+}
+
+// normalise: B/rs, D_ij xs_j / rs_i, x_J/xs, dq_prev/xs
+__global__ void k_features_norm(int64_t nc, const float* __restrict__ raw, const float* __restrict__ xj,
+                                const float* __restrict__ scl /*rs[5],xs[5]*/, float* __restrict__ feat) {
+  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const float* rs = scl;
+  const float* xs = scl + 5;
+  for (int k = 0; k < 5; ++k) feat[c * NIN + k] = raw[c * NIN + k] / rs[k];
+  for (int i = 0; i < 5; ++i)
+    for (int j = 0; j < 5; ++j)
+      feat[c * NIN + 5 + 5 * i + j] = raw[c * NIN + 5 + 5 * i + j] * xs[j] / rs[i];
+  for (int k = 0; k < 5; ++k) feat[c * NIN + 30 + k] = xj[c * 5 + k] / xs[k];
+  for (int k = 0; k < 5; ++k) feat[c * NIN + 35 + k] = raw[c * NIN + 35 + k] / xs[k];
+}
+
+inline unsigned nb_(int64_t n, int t) { return unsigned((n + t - 1) / t); }
+
+// forward over the whole graph from features; returns head output in m->d_y
+int forward(fpsi_gnn* m, const Graph& G, const float* feat) {
+  cudaStream_t s = m->stream;
+  const int64_t nc = G.nc;
+  const float* h = feat;
+  for (int l = 0; l < NLAYER; ++l) {
+    const int fin = m->L.fan_in[l];
+    k_aggregate<<<nb_(nc * fin, 256), 256, 0, s>>>(nc, fin, G.off, G.nb, h, m->d_agg[l]);
+    k_mp_forward<<<nb_(nc, GT), GT, 0, s>>>(nc, fin, m->d_wb + m->L.ws[l], m->d_wb + m->L.wn[l],
+                                            m->d_wb + m->L.b[l], h, m->d_agg[l], m->d_z[l],
+                                            m->d_h[l + 1]);
+    h = m->d_h[l + 1];
+  }
+  k_head_forward<<<nb_(nc, GT), GT, 0, s>>>(nc, m->d_wb + m->L.wo, m->d_wb + m->L.bo, h, m->d_y);
+  FPSI_CUDA_TRY(cudaGetLastError());
+  return FPSI_OK;
+}
+
+// loss over the batch and full gradient into m->d_g; loss_out (device) [2]
+int backward(fpsi_gnn* m, const Graph& G, const float* feat, const float* target, uint64_t seed,
+             uint64_t thr, double* loss_out) {
+  cudaStream_t s = m->stream;
+  const int64_t nc = G.nc;
+  const int nblk = int(nb_(nc, GT));
+  float* dy = m->d_dz;  // [nc][5] fits in the [nc][64] buffer
+  k_loss<<<nblk, GT, 0, s>>>(nc, m->d_y, target, seed, thr, dy, m->d_lpart);
+  k_loss_final<<<1, 256, 0, s>>>(m->d_lpart, nblk, loss_out);
+  k_scale<<<nb_(nc * NOUT, 256), 256, 0, s>>>(nc * NOUT, dy, loss_out);
+  const int rb = int(nb_(nc, RB));
+  // head
+  k_wgrad_partial<<<rb, 256, 0, s>>>(nc, NOUT, W, dy, m->d_h[NLAYER], m->d_part);
+  k_wgrad_reduce<<<nb_(NOUT * (W + 1), 256), 256, 0, s>>>(rb, NOUT, W, m->d_part, m->d_g, m->L.wo, m->L.bo);
+  k_back_dense<<<nb_(nc, GT), GT, 0, s>>>(nc, NOUT, W, m->d_wb + m->L.wo, dy, m->d_dh);
+  for (int l = NLAYER - 1; l >= 0; --l) {
+    const int fin = m->L.fan_in[l];
+    const float* hin = l == 0 ? feat : m->d_h[l];
+    k_back_gelu<<<nb_(nc * W, 256), 256, 0, s>>>(nc * W, m->d_dh, m->d_z[l], m->d_dz);
+    k_wgrad_partial<<<rb, 256, 0, s>>>(nc, W, fin, m->d_dz, hin, m->d_part);
+    k_wgrad_reduce<<<nb_(W * (fin + 1), 256), 256, 0, s>>>(rb, W, fin, m->d_part, m->d_g, m->L.ws[l],
+                                                          m->L.b[l]);
+    k_wgrad_partial<<<rb, 256, 0, s>>>(nc, W, fin, m->d_dz, m->d_agg[l], m->d_part);
+    k_wgrad_reduce<<<nb_(W * (fin + 1), 256), 256, 0, s>>>(rb, W, fin, m->d_part, m->d_g, m->L.wn[l], -1);
+    if (l > 0) {
+      // dh_in = Ws^T dz + scatter(Wn^T dz)
+      k_back_dense<<<nb_(nc, GT), GT, 0, s>>>(nc, W, fin, m->d_wb + m->L.wn[l], m->d_dz, m->d_dagg);
+      k_back_dense<<<nb_(nc, GT), GT, 0, s>>>(nc, W, fin, m->d_wb + m->L.ws[l], m->d_dz, m->d_dh2);
+      k_back_aggregate<<<nb_(nc * fin, 256), 256, 0, s>>>(nc, fin, G.off, G.nb, m->d_dagg, m->d_dh2);
+      std::swap(m->d_dh, m->d_dh2);
+    }
+  }
+  FPSI_CUDA_TRY(cudaGetLastError());
+  return FPSI_OK;
+}
+
+template <class T>
+int galloc(T** p, size_t n) {
+  if (cudaMalloc((void**)p, (n ? n : 1) * sizeof(T)) != cudaSuccess) {
+    fpsi::set_error("cudaMalloc failed in the learned-start model");
+    *p = nullptr;
+    return FPSI_E_NOMEM;
+  }
+  return FPSI_OK;
+}
+
+void free_activations(fpsi_gnn* m) {
+  void* ps[] = {m->d_y, m->d_dh, m->d_dh2, m->d_dz, m->d_dagg, m->d_part, m->d_lpart};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  m->d_y = m->d_dh = m->d_dh2 = m->d_dz = m->d_dagg = m->d_part = nullptr;
+  m->d_lpart = nullptr;
+  for (int l = 0; l <= NLAYER; ++l) {
+    if (m->d_h[l]) cudaFree(m->d_h[l]);
+    m->d_h[l] = nullptr;
+  }
+  for (int l = 0; l < NLAYER; ++l) {
+    if (m->d_agg[l]) cudaFree(m->d_agg[l]);
+    if (m->d_z[l]) cudaFree(m->d_z[l]);
+    m->d_agg[l] = m->d_z[l] = nullptr;
+  }
+  m->cap = 0;
+}
+
+// activation buffers for graphs of up to nc cells
+int ensure_capacity(fpsi_gnn* m, int64_t nc) {
+  if (nc <= m->cap) return FPSI_OK;
+  if (cudaStreamSynchronize(m->stream) != cudaSuccess) return FPSI_E_CUDA;
+  free_activations(m);
+  int rc = FPSI_OK;
+#define G(e) \
+  if (!rc) rc = (e)
+  for (int l = 1; l <= NLAYER; ++l) G(galloc(&m->d_h[l], nc * W));
+  for (int l = 0; l < NLAYER; ++l) {
+    G(galloc(&m->d_agg[l], nc * W));
+    G(galloc(&m->d_z[l], nc * W));
+  }
+  G(galloc(&m->d_y, nc * NOUT));
+  G(galloc(&m->d_dh, nc * W));
+  G(galloc(&m->d_dh2, nc * W));
+  G(galloc(&m->d_dz, nc * W));
+  G(galloc(&m->d_dagg, nc * W));
+  G(galloc(&m->d_part, ((nc + RB - 1) / RB) * W * (W + 1)));
+  G(galloc(&m->d_lpart, ((nc + GT - 1) / GT) * 10 + 16));
+#undef G
+  if (rc) {
+    free_activations(m);
+    return rc;
+  }
+  m->cap = nc;
+  return FPSI_OK;
+}
+
+// the context's interior-face cell graph (RCM order), built on first use
+int ctx_graph(fpsi_ctx* x, Graph* G) {
+  const int64_t nc = x->H.nc;
+  if (!x->d_cnb_off) {
+    std::vector<int32_t> off(nc + 1, 0), nb;
+    for (int64_t c = 0; c < nc; ++c) {
+      for (int32_t e = x->H.cf_off[c]; e < x->H.cf_off[c + 1]; ++e) {
+        const int64_t f = x->H.cf[e] >> 1;
+        if (x->H.cr[f] < 0) continue;
+        nb.push_back((x->H.cf[e] & 1) ? x->H.cl[f] : x->H.cr[f]);
+      }
+      off[c + 1] = int32_t(nb.size());
+    }
+    int rc = galloc(&x->d_cnb_off, off.size());
+    if (!rc) rc = galloc(&x->d_cnb, nb.size());
+    if (rc) {
+      cudaFree(x->d_cnb_off), cudaFree(x->d_cnb);
+      x->d_cnb_off = x->d_cnb = nullptr;
+      return rc;
+    }
+    FPSI_CUDA_TRY(cudaMemcpy(x->d_cnb_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice));
+    if (!nb.empty())
+      FPSI_CUDA_TRY(cudaMemcpy(x->d_cnb, nb.data(), nb.size() * 4, cudaMemcpyHostToDevice));
+    x->cnb_n = int64_t(nb.size());
+  }
+  *G = Graph{nc, x->d_cnb_off, x->d_cnb};
+  return FPSI_OK;
+}
+
+void free_snapshot(Snapshot& s) {
+  void* ps[] = {s.d_off, s.d_nb, s.feat, s.target, s.xj};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  s.d_off = s.d_nb = nullptr;
+  s.feat = s.target = s.xj = nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fpsi_gnn_create(fpsi_gnn** out, uint64_t seed) {
+  if (!out) return FPSI_E_INVALID;
+  *out = nullptr;
+  fpsi_gnn* m = new (std::nothrow) fpsi_gnn();
+  if (!m) return FPSI_E_NOMEM;
+  m->L = layout();
+  if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete m;
+    fpsi::set_error("learned start: cudaStreamCreate failed");
+    return FPSI_E_CUDA;
+  }
+  const int64_t np = m->L.total;
+  int rc = FPSI_OK;
+#define G(e) \
+  if (!rc) rc = (e)
+  G(galloc(&m->d_w, np));
+  G(galloc(&m->d_m, np));
+  G(galloc(&m->d_v, np));
+  G(galloc(&m->d_g, np));
+  G(galloc(&m->d_wb, np));
+#undef G
+  if (rc) {
+    fpsi_gnn_destroy(m);
+    return rc;
+  }
+  // He-style uniform initialisation from a counter-based generator; the
+  // head starts at zero so the untrained model gives the Jacobi start
+  std::vector<float> w(np, 0.f);
+  auto u01 = [&](uint64_t i) {
+    uint64_t z = seed * 0x100000001B3ull + i + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return double(z >> 11) * (1.0 / 9007199254740992.0);
+  };
+  for (int l = 0; l < NLAYER; ++l) {
+    const int fin = m->L.fan_in[l];
+    const double a = std::sqrt(3.0 / (2.0 * fin));
+    for (int64_t i = 0; i < int64_t(W) * fin; ++i) {
+      w[m->L.ws[l] + i] = float(a * (2 * u01(m->L.ws[l] + i) - 1));
+      w[m->L.wn[l] + i] = float(a * (2 * u01(m->L.wn[l] + i) - 1));
+    }
+  }
+  rc = fpsi_gnn_set_params(m, w.data());
+  if (rc) {
+    fpsi_gnn_destroy(m);
+    return rc;
+  }
+  *out = m;
+  return FPSI_OK;
+}
+
+int fpsi_gnn_clear_snapshots(fpsi_gnn* m) {
+  if (!m) return FPSI_E_INVALID;
+  if (m->stream) cudaStreamSynchronize(m->stream);
+  for (Snapshot& s : m->snaps) free_snapshot(s);
+  m->snaps.clear();
+  return FPSI_OK;
+}
+
+int fpsi_gnn_destroy(fpsi_gnn* m) {
+  if (!m) return FPSI_OK;
+  fpsi_gnn_clear_snapshots(m);
+  free_activations(m);
+  void* ps[] = {m->d_w, m->d_m, m->d_v, m->d_g, m->d_wb};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  if (m->stream) cudaStreamDestroy(m->stream);
+  delete m;
+  return FPSI_OK;
+}
+
+int64_t fpsi_gnn_num_params(const fpsi_gnn* m) { return m ? m->L.total : 0; }
+
+int fpsi_gnn_get_params(fpsi_gnn* m, float* w) {
+  if (!m || !w) return FPSI_E_INVALID;
+  FPSI_CUDA_TRY(cudaMemcpy(w, m->d_w, m->L.total * 4, cudaMemcpyDeviceToHost));
+  return FPSI_OK;
+}
+
+int fpsi_gnn_set_params(fpsi_gnn* m, const float* w) {
+  if (!m || !w) return FPSI_E_INVALID;
+  FPSI_CUDA_TRY(cudaMemcpy(m->d_w, w, m->L.total * 4, cudaMemcpyHostToDevice));
+  FPSI_CUDA_TRY(cudaMemset(m->d_m, 0, m->L.total * 4));
+  FPSI_CUDA_TRY(cudaMemset(m->d_v, 0, m->L.total * 4));
+  m->adam_t = 0;
+  k_to_bf16<<<nb_(m->L.total, 256), 256, 0, m->stream>>>(m->L.total, m->d_w, m->d_wb);
+  FPSI_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  return FPSI_OK;
+}
+
+// features of ctx's assembled system into (feat, xj, scales)
+// (activation buffers must hold x's cells)
+static int make_features(fpsi_gnn* m, fpsi_ctx* x, float* feat, float* xj, float* rs, float* xs) {
+  if (!x->have_asm || !x->d_D || x->P.solver != FPSI_SOLVER_SGS) {
+    fpsi::set_error("learned start: needs an assembled SGS system with the diagonal blocks kept");
+    return FPSI_E_STATE;
+  }
+  const int64_t nc = x->H.nc;
+  if (nc > m->cap) return FPSI_E_INVALID;
+  // from now on the context keeps a copy of each applied update
+  if (!x->d_xprev) {
+    if (cudaMalloc(&x->d_xprev, size_t(nc) * 5 * 8) != cudaSuccess) {
+      x->d_xprev = nullptr;
+      fpsi::set_error("cudaMalloc failed for the previous-update copy");
+      return FPSI_E_NOMEM;
+    }
+    x->have_xprev = false;
+  }
+  x->keep_prev = true;
+  const void* xprev = x->have_xprev ? x->d_xprev : nullptr;
+  // x_J = D^-1 B from the factored blocks (the iterate may hold a solve)
+  FPSI_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  int rc0 = fpsi::launch_jacobi_start(x);
+  if (rc0) return rc0;
+  FPSI_CUDA_TRY(cudaStreamSynchronize(x->stream));
+  float* raw = m->d_dagg;  // [nc][40] scratch inside an [nc][64] buffer
+  if (x->P.precision == FPSI_PREC_FP64)
+    k_features_raw<double, double><<<nb_(nc, 256), 256, 0, m->stream>>>(
+        nc, x->d_src, (const double*)x->d_D, (const double*)x->d_x, (const double*)xprev, x->d_ci, raw,
+        xj);
+  else if (x->P.precision == FPSI_PREC_MIXED)
+    k_features_raw<float, float><<<nb_(nc, 256), 256, 0, m->stream>>>(
+        nc, x->d_src, (const float*)x->d_D, (const float*)x->d_x, (const float*)xprev, x->d_ci, raw, xj);
+  else
+    k_features_raw<float, double><<<nb_(nc, 256), 256, 0, m->stream>>>(
+        nc, x->d_src, (const float*)x->d_D, (const double*)x->d_x, (const double*)xprev, x->d_ci, raw,
+        xj);
+  const int nblk = int(nb_(nc, GT));
+  k_rms_partial<<<nblk, GT, 0, m->stream>>>(nc, raw, xj, m->d_lpart);
+  std::vector<double> part(size_t(nblk) * 10);
+  FPSI_CUDA_TRY(cudaMemcpyAsync(part.data(), m->d_lpart, part.size() * 8, cudaMemcpyDeviceToHost, m->stream));
+  FPSI_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  float scl[10];
+  for (int k = 0; k < 10; ++k) {
+    double s = 0;
+    for (int b = 0; b < nblk; ++b) s += part[10 * b + k];
+    scl[k] = float(std::sqrt(s / double(nc)) + 1e-30);
+  }
+  for (int k = 0; k < 5; ++k) rs[k] = scl[k], xs[k] = scl[5 + k];
+  float* dscl = reinterpret_cast<float*>(m->d_lpart);
+  FPSI_CUDA_TRY(cudaMemcpyAsync(dscl, scl, sizeof(scl), cudaMemcpyHostToDevice, m->stream));
+  k_features_norm<<<nb_(nc, 256), 256, 0, m->stream>>>(nc, raw, xj, dscl, feat);
+  FPSI_CUDA_TRY(cudaGetLastError());
+  return FPSI_OK;
+}
+
+__global__ void k_target(int64_t nc, const double* __restrict__ dq_rcm, const float* __restrict__ xj,
+                         const float* __restrict__ scl, float* __restrict__ t) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= nc * 5) return;
+  const int k = int(i % 5);
+  t[i] = float((dq_rcm[i] - double(xj[i])) / double(scl[k]));
+}
+
+int fpsi_gnn_add_snapshot(fpsi_gnn* m, fpsi_ctx* x, const double* dq) {
+  if (!m || !x || !dq) return FPSI_E_INVALID;
+  Snapshot s;
+  const int64_t nc = x->H.nc;
+  Graph G;
+  int rc = ensure_capacity(m, nc);
+  if (!rc) rc = ctx_graph(x, &G);
+  if (!rc) rc = galloc(&s.d_off, nc + 1);
+  if (!rc) rc = galloc(&s.d_nb, x->cnb_n);
+  if (!rc) rc = galloc(&s.feat, nc * NIN);
+  if (!rc) rc = galloc(&s.target, nc * 5);
+  if (!rc) rc = galloc(&s.xj, nc * 5);
+  if (!rc) rc = make_features(m, x, s.feat, s.xj, s.rs, s.xs);
+  double* dd = nullptr;
+  if (!rc) rc = galloc(&dd, nc * 5);
+  if (rc) {
+    free_snapshot(s);
+    return rc;
+  }
+  s.nc = nc;
+  s.perm = x->H.perm;
+  // target in RCM order
+  std::vector<double> d(nc * 5);
+  for (int64_t i = 0; i < nc; ++i)
+    for (int k = 0; k < 5; ++k) d[5 * i + k] = dq[5 * int64_t(s.perm[i]) + k];
+  float* dscl = reinterpret_cast<float*>(m->d_lpart);
+  bool ok = cudaMemcpyAsync(s.d_off, G.off, (nc + 1) * 4, cudaMemcpyDeviceToDevice, m->stream) == cudaSuccess &&
+            (x->cnb_n == 0 || cudaMemcpyAsync(s.d_nb, G.nb, x->cnb_n * 4, cudaMemcpyDeviceToDevice,
+                                              m->stream) == cudaSuccess) &&
+            cudaMemcpyAsync(dd, d.data(), d.size() * 8, cudaMemcpyHostToDevice, m->stream) == cudaSuccess &&
+            cudaMemcpyAsync(dscl, s.xs, 5 * sizeof(float), cudaMemcpyHostToDevice, m->stream) == cudaSuccess;
+  if (ok) {
+    k_target<<<nb_(nc * 5, 256), 256, 0, m->stream>>>(nc, dd, s.xj, dscl, s.target);
+    ok = cudaStreamSynchronize(m->stream) == cudaSuccess;
+  }
+  cudaFree(dd);
+  if (!ok) {
+    free_snapshot(s);
+    fpsi::set_error("learned start: snapshot upload failed");
+    return FPSI_E_CUDA;
+  }
+  m->snaps.push_back(std::move(s));
+  return FPSI_OK;
+}
+
+int fpsi_gnn_num_snapshots(const fpsi_gnn* m) { return m ? int(m->snaps.size()) : 0; }
+
+int64_t fpsi_gnn_snapshot_cells(const fpsi_gnn* m, int32_t si) {
+  if (!m || si < 0 || si >= int32_t(m->snaps.size())) return -1;
+  return m->snaps[si].nc;
+}
+
+int fpsi_gnn_get_snapshot(fpsi_gnn* m, int32_t si, float* feat, float* target, float* xj,
+                          float* scales) {
+  if (!m || si < 0 || si >= int32_t(m->snaps.size())) return FPSI_E_INVALID;
+  const Snapshot& s = m->snaps[si];
+  const int64_t nc = s.nc;
+  auto fetch = [&](const float* dsrc, int w, float* dst) -> int {
+    if (!dst) return FPSI_OK;
+    std::vector<float> h(nc * w);
+    FPSI_CUDA_TRY(cudaMemcpy(h.data(), dsrc, h.size() * 4, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < nc; ++i)
+      for (int k = 0; k < w; ++k) dst[int64_t(s.perm[i]) * w + k] = h[i * w + k];
+    return FPSI_OK;
+  };
+  int rc = fetch(s.feat, NIN, feat);
+  if (!rc) rc = fetch(s.target, 5, target);
+  if (!rc) rc = fetch(s.xj, 5, xj);
+  if (scales)
+    for (int k = 0; k < 5; ++k) scales[k] = s.rs[k], scales[5 + k] = s.xs[k];
+  return rc;
+}
+
+// loss (batch = cells whose hash is below the threshold; batch >= nc: all)
+static uint64_t threshold(int64_t nc, int64_t batch) {
+  if (batch >= nc) return ~uint64_t(0);
+  return uint64_t((long double)batch / (long double)nc * 18446744073709551615.0L);
+}
+
+int fpsi_gnn_loss_grad(fpsi_gnn* m, int32_t si, int64_t batch, uint64_t seed, double* loss,
+                       float* grad) {
+  if (!m || si < 0 || si >= int32_t(m->snaps.size())) return FPSI_E_INVALID;
+  const Snapshot& s = m->snaps[si];
+  int rc = ensure_capacity(m, s.nc);
+  if (!rc) rc = forward(m, s.graph(), s.feat);
+  if (rc) return rc;
+  double* dl = m->d_lpart + ((s.nc + GT - 1) / GT) * 2 + 2;
+  if ((rc = backward(m, s.graph(), s.feat, s.target, seed, threshold(s.nc, batch), dl))) return rc;
+  double h[2];
+  FPSI_CUDA_TRY(cudaMemcpyAsync(h, dl, sizeof(h), cudaMemcpyDeviceToHost, m->stream));
+  FPSI_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  if (loss) *loss = h[0];
+  if (grad) FPSI_CUDA_TRY(cudaMemcpy(grad, m->d_g, m->L.total * 4, cudaMemcpyDeviceToHost));
+  return FPSI_OK;
+}
+
+int fpsi_gnn_train(fpsi_gnn* m, int32_t nsteps, int64_t batch, uint64_t seed, double lr,
+                   double* losses) {
+  if (!m || nsteps < 0 || m->snaps.empty()) return FPSI_E_INVALID;
+  const int64_t np = m->L.total;
+  const int ns = int(m->snaps.size());
+  int64_t ncmax = 0;
+  for (const Snapshot& s : m->snaps) ncmax = std::max(ncmax, s.nc);
+  int rc0 = ensure_capacity(m, ncmax);
+  if (rc0) return rc0;
+  double* dhist = nullptr;
+  if (losses && galloc(&dhist, size_t(nsteps) + 1)) return FPSI_E_NOMEM;
+  for (int32_t it = 0; it < nsteps; ++it) {
+    const uint64_t sd = seed * 1000003ull + uint64_t(it);
+    const Snapshot& s = m->snaps[size_t(sd % uint64_t(ns))];
+    double* dl = m->d_lpart + ((s.nc + GT - 1) / GT) * 2 + 2;
+    int rc = forward(m, s.graph(), s.feat);
+    if (!rc) rc = backward(m, s.graph(), s.feat, s.target, sd, threshold(s.nc, batch), dl);
+    if (rc) {
+      cudaFree(dhist);
+      return rc;
+    }
+    m->adam_t += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = float(1.0 - std::pow(double(b1), double(m->adam_t)));
+    const float c2 = float(1.0 - std::pow(double(b2), double(m->adam_t)));
+    k_adam<<<nb_(np, 256), 256, 0, m->stream>>>(np, m->d_w, m->d_m, m->d_v, m->d_g, m->d_wb,
+                                                float(lr), b1, b2, 1e-8f, c1, c2);
+    if (dhist) cudaMemcpyAsync(dhist + it, dl, 8, cudaMemcpyDeviceToDevice, m->stream);
+  }
+  FPSI_CUDA_TRY(cudaGetLastError());
+  if (dhist) {
+    FPSI_CUDA_TRY(cudaMemcpyAsync(losses, dhist, size_t(nsteps) * 8, cudaMemcpyDeviceToHost, m->stream));
+  }
+  FPSI_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  cudaFree(dhist);
+  return FPSI_OK;
+}
+
+}  // extern "C"
+
+namespace {
+// x0 = x_J + xs * d into ctx's colour-order iterate (the next linear solve
+// starts from it); x0_out (caller order) optional
+template <class TX>
+__global__ void k_apply_start(int64_t nc, const float* __restrict__ xj, const float* __restrict__ y,
+                              const float* __restrict__ scl, const int32_t* __restrict__ ci,
+                              TX* __restrict__ x, double* __restrict__ x0) {
+  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const int64_t i = ci[c];
+  for (int k = 0; k < 5; ++k) {
+    const double v = double(xj[c * 5 + k]) + double(scl[k]) * double(y[c * 5 + k]);
+    x[5 * i + k] = TX(v);
+    if (x0) x0[5 * c + k] = v;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int fpsi_gnn_predict(fpsi_gnn* m, fpsi_ctx* x, double* x0) {
+  if (!m || !x) return FPSI_E_INVALID;
+  const int64_t nc = x->H.nc;
+  float rs[5], xs[5];
+  Graph G;
+  int rc = ensure_capacity(m, nc);
+  if (!rc) rc = ctx_graph(x, &G);
+  if (rc) return rc;
+  float* fbuf = nullptr;
+  if ((rc = galloc(&fbuf, nc * NIN))) return rc;
+  float* xjb = nullptr;
+  if ((rc = galloc(&xjb, nc * 5))) {
+    cudaFree(fbuf);
+    return rc;
+  }
+  rc = make_features(m, x, fbuf, xjb, rs, xs);
+  if (!rc) rc = forward(m, G, fbuf);
+  double* dx0 = nullptr;
+  if (!rc && x0) rc = galloc(&dx0, nc * 5);
+  if (!rc) {
+    float* dscl = reinterpret_cast<float*>(m->d_lpart);
+    cudaMemcpyAsync(dscl, xs, sizeof(xs), cudaMemcpyHostToDevice, m->stream);
+    if (x->P.precision == FPSI_PREC_MIXED)
+      k_apply_start<float><<<nb_(nc, 256), 256, 0, m->stream>>>(nc, xjb, m->d_y, dscl, x->d_ci,
+                                                               (float*)x->d_x, dx0);
+    else
+      k_apply_start<double><<<nb_(nc, 256), 256, 0, m->stream>>>(nc, xjb, m->d_y, dscl, x->d_ci,
+                                                                (double*)x->d_x, dx0);
+    if (cudaStreamSynchronize(m->stream) != cudaSuccess) rc = FPSI_E_CUDA;
+  }
+  if (!rc && x0) {
+    std::vector<double> h(nc * 5);
+    if (cudaMemcpy(h.data(), dx0, h.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess) rc = FPSI_E_CUDA;
+    for (int64_t i = 0; !rc && i < nc; ++i)
+      for (int k = 0; k < 5; ++k) x0[5 * int64_t(x->H.perm[i]) + k] = h[5 * i + k];
+  }
+  cudaFree(fbuf);
+  cudaFree(xjb);
+  cudaFree(dx0);
+  if (!rc) x->x_preset = true;
+  return rc;
+}
+
+}  // extern "C"

@@ -1267,6 +1267,11 @@ int launch_update(fpsi_ctx* x) {
         nc, x->P.Pambient, map, (const double*)xv, x->d_q, x->d_amin);
   prof_end(x);
   FPSI_CUDA_TRY(cudaGetLastError());
+  if (x->keep_prev && x->d_xprev && !lsgs) {
+    FPSI_CUDA_TRY(cudaMemcpyAsync(x->d_xprev, x->d_x, size_t(nc) * 5 * x->x_bytes,
+                                  cudaMemcpyDeviceToDevice, x->stream));
+    x->have_xprev = true;
+  }
   return FPSI_OK;
 }
 

@@ -1,0 +1,139 @@
+"""Learned starting iterate of the block relaxation (host side).
+
+No counterpart in the reference; the hook is the relaxation's starting
+iterate (linearSolverSGS.loci:57-69).  The network, its training and its
+inference run in the library's CUDA kernels (flowpsi_b200/csrc/gnn.cu); this
+module drives them: snapshot generation from the solver itself, training,
+and the start used inside a Newton step with the reference's Jacobi start
+as the fallback and a rejection of steps whose FP64 residual does not drop.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from .solver import FlowPsi
+
+_fp = C.POINTER(C.c_float)
+
+
+class LearnedStart:
+    """The network's weights (independent of the mesh) and its training set;
+    one model serves any FlowPsi context."""
+
+    def __init__(self, seed: int = 0):
+        h = C.c_void_p()
+        N.check(N.lib().fpsi_gnn_create(C.byref(h), seed), "fpsi_gnn_create")
+        self._h = h
+        self.n_params = int(N.lib().fpsi_gnn_num_params(h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib().fpsi_gnn_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def get_params(self) -> np.ndarray:
+        w = np.empty(self.n_params, np.float32)
+        N.check(N.lib().fpsi_gnn_get_params(self._h, w.ctypes.data_as(_fp)), "fpsi_gnn_get_params")
+        return w
+
+    def set_params(self, w) -> None:
+        w = np.ascontiguousarray(w, np.float32)
+        assert w.size == self.n_params
+        N.check(N.lib().fpsi_gnn_set_params(self._h, w.ctypes.data_as(_fp)), "fpsi_gnn_set_params")
+
+    def add_snapshot(self, solver: FlowPsi, dq) -> None:
+        """features of solver's assembled system and its converged update"""
+        d = np.ascontiguousarray(dq, np.float64).reshape(-1)
+        N.check(N.lib().fpsi_gnn_add_snapshot(self._h, solver._ctx, N.dptr(d)),
+                "fpsi_gnn_add_snapshot")
+
+    @property
+    def n_snapshots(self) -> int:
+        return int(N.lib().fpsi_gnn_num_snapshots(self._h))
+
+    def snapshot(self, i: int):
+        """(features [nc,40], target [nc,5], x_J [nc,5], scales rs|xs [10]) of
+        snapshot i, caller cell order"""
+        nc = int(N.lib().fpsi_gnn_snapshot_cells(self._h, i))
+        if nc < 0:
+            raise IndexError(i)
+        f, t, xj = (np.empty((nc, 40), np.float32), np.empty((nc, 5), np.float32),
+                    np.empty((nc, 5), np.float32))
+        sc = np.empty(10, np.float32)
+        N.check(N.lib().fpsi_gnn_get_snapshot(self._h, i, f.ctypes.data_as(_fp),
+                                              t.ctypes.data_as(_fp), xj.ctypes.data_as(_fp),
+                                              sc.ctypes.data_as(_fp)), "fpsi_gnn_get_snapshot")
+        return f, t, xj, sc
+
+    def loss_grad(self, i: int, batch: int | None = None, seed: int = 0):
+        """mean squared error on snapshot i over about `batch` cells (all by
+        default) and its gradient"""
+        g = np.empty(self.n_params, np.float32)
+        loss = C.c_double()
+        nb = batch if batch is not None else (1 << 62)
+        N.check(N.lib().fpsi_gnn_loss_grad(self._h, i, nb, seed, C.byref(loss),
+                                           g.ctypes.data_as(_fp)), "fpsi_gnn_loss_grad")
+        return loss.value, g
+
+    def train(self, nsteps: int, batch: int = 65536, seed: int = 0, lr: float = 1e-3):
+        out = np.empty(max(nsteps, 1))
+        N.check(N.lib().fpsi_gnn_train(self._h, nsteps, batch, seed, lr, N.dptr(out)),
+                "fpsi_gnn_train")
+        return out[:nsteps]
+
+    def predict(self, solver: FlowPsi, want: bool = False):
+        """set solver's next starting iterate to the learned one"""
+        x0 = np.empty(solver.ncells * 5) if want else None
+        N.check(N.lib().fpsi_gnn_predict(self._h, solver._ctx, N.dptr(x0)), "fpsi_gnn_predict")
+        return None if x0 is None else x0.reshape(-1, 5)
+
+
+def converged_update(solver: FlowPsi, rtol: float = 1e-10, max_sweeps: int = 400) -> np.ndarray:
+    """dq of solver's assembled system, swept from the current iterate until
+    ||B - A dq|| <= rtol ||B||"""
+    solver.sweeps_to_tolerance(rtol, max_sweeps)
+    return solver.get_iterate()
+
+
+def make_snapshots(model: LearnedStart, case, steps: int, rtol: float = 1e-10,
+                   every: int = 1) -> list[float]:
+    """run `steps` implicit steps of `case` (a FlowPsi case with the SGS
+    solver and the diagonal blocks kept) and add (system, converged dq)
+    pairs; returns the residual history"""
+    s = FlowPsi(case.mesh, case.params)
+    s.keep_blocks(True)
+    T, p, u = case.initial_state(s.geometry()["cellcenter"])
+    s.set_state(T, p, u)
+    hist = []
+    for k in range(steps):
+        _, r = s.residual(want_src=False)
+        hist.append(r["rtrms"])
+        s.assemble()
+        if k % every == 0:
+            model.add_snapshot(s, converged_update(s, rtol))
+            s.assemble()  # back to the reference's start for the solver's own step
+        s.sweeps(case.params.gauss_seidel_iter)
+        s.update()
+    s.close()
+    return hist
+
+
+def sweeps_to_tolerance(solver: FlowPsi, start: str, rtol: float = 1e-3,
+                        model: LearnedStart | None = None, max_sweeps: int = 200) -> int:
+    """symmetric sweeps the assembled system needs from a given start
+    ('zero', 'jacobi' -- the reference's D^-1 B -- or 'learned')"""
+    if start == "zero":
+        solver.set_iterate(np.zeros((solver.ncells, 5)))
+    elif start == "jacobi":
+        solver.assemble()  # the assembly leaves D^-1 B as the iterate
+    elif start == "learned":
+        model.predict(solver)
+    else:
+        raise ValueError(start)
+    return solver.sweeps_to_tolerance(rtol, max_sweeps)

@@ -277,6 +277,31 @@ class FlowPsi:
                                        "resid": li.resid}
         return dq.reshape(-1, 5)
 
+    def set_iterate(self, x0) -> None:
+        """start the next sweeps from x0 (caller order, nc x 5)"""
+        x = np.ascontiguousarray(x0, np.float64).reshape(-1)
+        N.check(N.lib().fpsi_set_iterate(self._ctx, N.dptr(x)), "fpsi_set_iterate")
+
+    def get_iterate(self) -> np.ndarray:
+        x = np.empty(self.ncells * 5)
+        N.check(N.lib().fpsi_get_iterate(self._ctx, N.dptr(x)), "fpsi_get_iterate")
+        return x.reshape(-1, 5)
+
+    def sweeps(self, n: int) -> None:
+        """n more symmetric sweeps from the current device iterate"""
+        N.check(N.lib().fpsi_linear_sweeps(self._ctx, n), "fpsi_linear_sweeps")
+
+    def sweeps_to_tolerance(self, rtol: float, max_sweeps: int = 200) -> int:
+        """symmetric sweeps from the current iterate until ||B - A x|| <=
+        rtol ||B|| (the relative linear tolerance); returns the count"""
+        for k in range(max_sweeps + 1):
+            nb, nr = self.linear_residual()
+            if nr <= rtol * nb:
+                return k
+            if k < max_sweeps:
+                self.sweeps(1)
+        return max_sweeps + 1
+
     def linear_residual(self):
         nb, nr = C.c_double(), C.c_double()
         N.check(N.lib().fpsi_linear_residual(self._ctx, C.byref(nb), C.byref(nr)),

@@ -241,6 +241,14 @@ int fpsi_get_blocks(fpsi_ctx* ctx, void* D, void* fjp, void* fjm, void* B);
  * (block Jacobi D^-1 B).  dq (nc*5 AoS) may be NULL (result stays on the
  * device for fpsi_update). */
 int fpsi_linear_solve(fpsi_ctx* ctx, const double* x0, double* dq, fpsi_lsinfo* info);
+/* set the device iterate (caller order nc*5) of the assembled system: the
+ * next fpsi_linear_solve(ctx, NULL, ...) or fpsi_linear_sweeps starts there */
+int fpsi_set_iterate(fpsi_ctx* ctx, const double* x0);
+/* the current device iterate (caller order nc*5) */
+int fpsi_get_iterate(fpsi_ctx* ctx, double* x);
+/* nsweeps more symmetric multi-colour sweeps from the current device iterate
+ * (no restart), e.g. to run a solve to a tolerance with fpsi_linear_residual */
+int fpsi_linear_sweeps(fpsi_ctx* ctx, int32_t nsweeps);
 /* || B - A x || (2-norm over all cells) of the device iterate */
 int fpsi_linear_residual(fpsi_ctx* ctx, double* norm_b, double* norm_r);
 /* clipped Newton update with the device dq (solverNewton.loci:62-78) */
@@ -259,6 +267,45 @@ int fpsi_run_timed(fpsi_ctx* ctx, int32_t nsteps, fpsi_resid* norms, double* dev
  * kernel kinds. */
 int fpsi_kernel_times(fpsi_ctx* ctx, int32_t nsteps, int32_t cap, char* names, double* ms,
                       int64_t* launches, int32_t* count);
+
+/* ---- learned starting iterate ---------------------------------------------
+ * No counterpart in the reference; the hook is the starting iterate of the
+ * relaxation (linearSolverSGS.loci:57-69).  A message-passing network over
+ * the cell graph (3 layers of width 64, GELU, linear head; BF16 weights,
+ * FP32 accumulation) maps each cell's fluid_B, fluid_D, block Jacobi
+ * solution D^-1 B and the context's previous update (kept on the device
+ * from the first use of a model with the context on; zero before), made
+ * scale free per system, to a correction d of the block Jacobi start:
+ * x0 = D^-1 B + xs * d (xs = RMS of D^-1 B per component).  The weights do not depend on the mesh: one model serves any
+ * context.  Training pairs come from the solver: fpsi_gnn_add_snapshot takes
+ * the features of an assembled system, its cell graph and its converged dq
+ * (caller order).  The model runs on its own stream. */
+typedef struct fpsi_gnn fpsi_gnn;
+int fpsi_gnn_create(fpsi_gnn** out, uint64_t seed);
+int fpsi_gnn_destroy(fpsi_gnn* m);
+int64_t fpsi_gnn_num_params(const fpsi_gnn* m);
+/* FP32 master weights, flat: per layer l: Ws[64][fin], Wn[64][fin], b[64]
+ * (fin = 40, 64, 64), then head Wo[5][64], bo[5] */
+int fpsi_gnn_get_params(fpsi_gnn* m, float* w);
+int fpsi_gnn_set_params(fpsi_gnn* m, const float* w);
+int fpsi_gnn_add_snapshot(fpsi_gnn* m, fpsi_ctx* ctx, const double* dq);
+int fpsi_gnn_clear_snapshots(fpsi_gnn* m);
+int fpsi_gnn_num_snapshots(const fpsi_gnn* m);
+/* cells of snapshot s (-1 when s is out of range) */
+int64_t fpsi_gnn_snapshot_cells(const fpsi_gnn* m, int32_t s);
+/* features (nc*40), targets (nc*5), Jacobi start (nc*5), scales rs[5] xs[5] */
+int fpsi_gnn_get_snapshot(fpsi_gnn* m, int32_t s, float* feat, float* target, float* xjac,
+                          float* scales);
+/* mean squared error and its gradient (flat, as the parameters) on snapshot
+ * s over a batch of about `batch` cells chosen by seed (all when batch >= nc) */
+int fpsi_gnn_loss_grad(fpsi_gnn* m, int32_t s, int64_t batch, uint64_t seed, double* loss,
+                       float* grad);
+/* nsteps Adam steps (lr; beta 0.9/0.999) on random snapshots and batches */
+int fpsi_gnn_train(fpsi_gnn* m, int32_t nsteps, int64_t batch, uint64_t seed, double lr,
+                   double* losses);
+/* learned start for ctx's assembled system: the next fpsi_linear_solve(ctx,
+ * NULL, ...) or fpsi_linear_sweeps starts from it; x0 (caller order) optional */
+int fpsi_gnn_predict(fpsi_gnn* m, fpsi_ctx* ctx, double* x0);
 
 /* ---- residual norms without allocation -----------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc

@@ -1,0 +1,72 @@
+"""CPU oracle of the learned-start network (torch CPU autograd).
+
+TEST INFRASTRUCTURE: restates the network of flowpsi_b200/csrc/gnn.cu in
+torch on the CPU, with the same BF16-rounded weights and FP32 arithmetic,
+to check the device's loss and gradients.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+NIN, W, NOUT, NLAYER = 40, 64, 5, 3
+
+
+def unpack(w: np.ndarray):
+    """flat FP32 masters -> list of tensors (rounded to BF16 as the device
+    uses them)"""
+    t = torch.from_numpy(np.ascontiguousarray(w, np.float32)).to(torch.bfloat16).to(torch.float32)
+    t = t.clone().requires_grad_(True)
+    parts, o = [], 0
+    for l in range(NLAYER):
+        fin = NIN if l == 0 else W
+        parts.append((o, o + W * fin, (W, fin)))
+        o += W * fin
+        parts.append((o, o + W * fin, (W, fin)))
+        o += W * fin
+        parts.append((o, o + W, (W,)))
+        o += W
+    parts.append((o, o + NOUT * W, (NOUT, W)))
+    o += NOUT * W
+    parts.append((o, o + NOUT, (NOUT,)))
+    o += NOUT
+    assert o == t.numel()
+    return t, [t[a:b].view(*shape) for a, b, shape in parts]
+
+
+def neighbour_mean_matrix(nc: int, cl: np.ndarray, cr: np.ndarray) -> torch.Tensor:
+    inner = cr >= 0
+    a, b = cl[inner].astype(np.int64), cr[inner].astype(np.int64)
+    rows = np.concatenate([a, b])
+    cols = np.concatenate([b, a])
+    deg = np.bincount(rows, minlength=nc).astype(np.float32)
+    vals = 1.0 / deg[rows]
+    return torch.sparse_coo_tensor(np.vstack([rows, cols]), vals, (nc, nc)).coalesce()
+
+
+def loss_and_grad(w: np.ndarray, feat: np.ndarray, target: np.ndarray, A: torch.Tensor):
+    flat, p = unpack(w)
+    h = torch.from_numpy(np.ascontiguousarray(feat, np.float32))
+    for l in range(NLAYER):
+        ws, wn, b = p[3 * l], p[3 * l + 1], p[3 * l + 2]
+        agg = torch.sparse.mm(A, h)
+        h = torch.nn.functional.gelu(h @ ws.T + agg @ wn.T + b)
+    y = h @ p[-2].T + p[-1]
+    t = torch.from_numpy(np.ascontiguousarray(target, np.float32))
+    loss = ((y - t) ** 2).mean()
+    loss.backward()
+    return float(loss), flat.grad.numpy().copy(), y.detach().numpy()
+
+
+def groups():
+    """(name, start, end) of each parameter block in the flat layout"""
+    out, o = [], 0
+    for l in range(NLAYER):
+        fin = NIN if l == 0 else W
+        for nm, n in (("ws", W * fin), ("wn", W * fin), ("b", W)):
+            out.append((f"{nm}{l}", o, o + n))
+            o += n
+    out.append(("wo", o, o + NOUT * W))
+    o += NOUT * W
+    out.append(("bo", o, o + NOUT))
+    return out

@@ -1,0 +1,201 @@
+"""Learned starting iterate: the CUDA network against a torch CPU autograd
+replica (oracle/gnn_oracle.py), and what the trained network gains over the
+reference's block Jacobi start (linearSolverSGS.loci:57-69).  GPU only.
+
+Tolerances: features exact to FP32 rounding (1e-5 relative); loss 1e-5
+relative; gradients per parameter group 1e-4 of the group's largest entry
+(FP32 sums in a different order, BF16 weights on both sides).
+"""
+import numpy as np
+import pytest
+
+from flowpsi_b200 import FlowPsi, cases
+from flowpsi_b200.learned import LearnedStart, converged_update, make_snapshots, sweeps_to_tolerance
+from oracle import gnn_oracle as G
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(seed=0, n=6, prec="fp64", steps=2):
+    case = cases.taylor_green_tets(n, seed=seed, precision=prec)
+    g = FlowPsi(case.mesh, case.params)
+    g.keep_blocks(True)
+    T, p, u = case.initial_state(g.geometry()["cellcenter"])
+    g.set_state(T, p, u)
+    for _ in range(steps):
+        g.newton_step()
+    src, _ = g.residual()
+    g.assemble()
+    return case, g, src
+
+
+def _random_head(model, seed=3, scale=0.2):
+    w = model.get_params()
+    rng = np.random.default_rng(seed)
+    nh = G.NOUT * G.W + G.NOUT
+    w[-nh:] = scale * rng.standard_normal(nh).astype(np.float32)
+    model.set_params(w)
+    return w
+
+
+def test_features_and_target(need_gpu):
+    case, g, src = _system()
+    blk = g.blocks()
+    D, B = blk["fluid_D"].astype(np.float64), blk["fluid_B"].astype(np.float64)
+    dq = converged_update(g, 1e-12, 600)
+    model = LearnedStart()
+    model.add_snapshot(g, dq)
+    f, t, xj, sc = model.snapshot(0)
+    rs, xs = sc[:5].astype(np.float64), sc[5:].astype(np.float64)
+    assert np.allclose(rs, np.sqrt((B ** 2).mean(0)), rtol=1e-5)
+    xj_ref = np.linalg.solve(D, B[:, :, None])[:, :, 0]
+    assert np.allclose(xs, np.sqrt((xj_ref ** 2).mean(0)), rtol=1e-5)
+    for k in range(5):
+        assert np.abs(xj[:, k] - xj_ref[:, k]).max() <= 1e-5 * np.abs(xj_ref[:, k]).max()
+    assert np.allclose(f[:, :5], B / rs, rtol=1e-5, atol=1e-6)
+    Ds = D * xs[None, None, :] / rs[None, :, None]
+    assert np.allclose(f[:, 5:30], Ds.reshape(-1, 25), rtol=1e-5, atol=1e-6 * np.abs(Ds).max())
+    assert np.allclose(f[:, 30:35], xj_ref / xs, rtol=1e-4, atol=1e-5)
+    assert np.all(f[:, 35:] == 0)  # no update applied since the model first saw g
+    assert np.allclose(t, (dq - xj_ref) / xs, rtol=1e-4, atol=1e-4)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_previous_update_feature(need_gpu, prec):
+    """once a model has seen a context, the context keeps its last applied
+    update; the next system's features carry it (scaled by xs)"""
+    case, g, _ = _system(prec=prec)
+    model = LearnedStart()
+    model.predict(g)
+    dq = g.linear_solve()
+    g.update()
+    g.residual()
+    g.assemble()
+    model.add_snapshot(g, g.get_iterate())
+    f, _, _, sc = model.snapshot(0)
+    xs = sc[5:].astype(np.float64)
+    assert np.allclose(f[:, 35:] * xs, dq, rtol=1e-5, atol=1e-6 * np.abs(dq).max())
+    g.set_state(*g.get_state())  # a new state forgets the previous update
+    g.residual()
+    g.assemble()
+    model.add_snapshot(g, g.get_iterate())
+    assert np.all(model.snapshot(1)[0][:, 35:] == 0)
+
+
+@pytest.mark.parametrize("mesh", ["tets", "hex"])
+def test_loss_and_gradient_match_autograd(need_gpu, mesh):
+    if mesh == "tets":
+        case, g, _ = _system()
+    else:
+        case = cases.farfield_cube(6, precision="fp64")
+        g = FlowPsi(case.mesh, case.params)
+        g.keep_blocks(True)
+        g.set_state(*case.initial_state(g.geometry()["cellcenter"]))
+        g.residual()
+        g.assemble()
+    dq = converged_update(g, 1e-10, 400)
+    model = LearnedStart(seed=5)
+    model.add_snapshot(g, dq)
+    w = _random_head(model)
+    loss, grad = model.loss_grad(0)
+    f, t, _, _ = model.snapshot(0)
+    a = case.mesh.arrays()
+    A = G.neighbour_mean_matrix(a.ncells, np.asarray(a.cl), np.asarray(a.cr))
+    loss_o, grad_o, _ = G.loss_and_grad(w, f, t, A)
+    assert abs(loss - loss_o) <= 1e-5 * loss_o
+    for name, lo, hi in G.groups():
+        go, gg = grad_o[lo:hi], grad[lo:hi]
+        assert np.abs(gg - go).max() <= 1e-4 * np.abs(go).max() + 1e-12, name
+
+
+def test_minibatch_gradient_is_the_batch_mean(need_gpu):
+    """the batch is a hashed subset of cells: its loss and gradient are those
+    of the masked mean squared error"""
+    case, g, _ = _system()
+    dq = converged_update(g, 1e-10, 400)
+    model = LearnedStart(seed=2)
+    model.add_snapshot(g, dq)
+    w = _random_head(model, seed=4)
+    l_all, g_all = model.loss_grad(0)
+    l1, g1 = model.loss_grad(0, batch=g.ncells // 2, seed=11)
+    l2, g2 = model.loss_grad(0, batch=g.ncells // 2, seed=11)
+    assert l1 == l2 and np.array_equal(g1, g2)  # deterministic
+    assert l1 != l_all
+
+
+def test_training_is_reproducible(need_gpu):
+    case, g, _ = _system(n=5)
+    dq = converged_update(g, 1e-10, 400)
+    hs = []
+    for _ in range(2):
+        m = LearnedStart(seed=1)
+        m.add_snapshot(g, dq)
+        h = m.train(50, batch=g.ncells, lr=3e-3)
+        hs.append((h, m.get_params()))
+    assert np.array_equal(hs[0][0], hs[1][0])
+    assert np.array_equal(hs[0][1], hs[1][1])
+    assert hs[0][0][-1] < hs[0][0][0]
+
+
+def test_untrained_model_gives_the_jacobi_start(need_gpu):
+    """the head starts at zero: x0 = x_J exactly"""
+    case, g, _ = _system(prec="ref")
+    xj = g.get_iterate().copy()
+    model = LearnedStart()
+    x0 = model.predict(g, want=True)
+    assert np.abs(x0 - xj).max() <= 1e-6 * np.abs(xj).max()
+    assert np.array_equal(g.get_iterate(), x0)
+
+
+def _train(prec, n, seeds, steps, nsteps):
+    model = LearnedStart(seed=0)
+    for sd in seeds:
+        make_snapshots(model, cases.taylor_green_tets(n, seed=sd, precision=prec), steps,
+                       rtol=1e-8)
+    hist = model.train(nsteps, batch=3 * n ** 3, lr=2e-3)
+    return model, hist
+
+
+def test_learned_start_needs_fewer_sweeps(need_gpu):
+    """Trained on Newton systems of Taylor-Green runs with jittered tet grids
+    (seeds 0-3), evaluated on held-out grids and states (seeds 7, 8): once
+    the run has left its first steps (k >= 3, a previous update exists), the
+    learned start has a lower initial linear residual than the block Jacobi
+    start and reaches ||B - A x|| <= 1e-3 ||B|| in fewer symmetric sweeps.
+    Every start is evaluated on the same systems: the run itself takes the
+    reference's steps (Jacobi start, 8 sweeps).  In the first steps the
+    learned start is not better; the test records that without asserting."""
+    n, prec, k0 = 8, "ref", 3
+    model, hist = _train(prec, n, seeds=[0, 1, 2, 3], steps=12, nsteps=3000)
+    assert hist[-50:].mean() < 0.5 * hist[:10].mean()
+    tot = {"zero": 0, "jacobi": 0, "learned": 0}
+    early = {"zero": 0, "jacobi": 0, "learned": 0}
+    r0 = {"jacobi": [], "learned": []}
+    for sd in (7, 8):
+        case = cases.taylor_green_tets(n, seed=sd, precision=prec)
+        g = FlowPsi(case.mesh, case.params)
+        g.keep_blocks(True)
+        g.set_state(*case.initial_state(g.geometry()["cellcenter"]))
+        for k in range(10):
+            g.residual(want_src=False)
+            g.assemble()
+            for start in ("zero", "jacobi", "learned"):
+                (tot if k >= k0 else early)[start] += sweeps_to_tolerance(g, start, 1e-3, model)
+            for start in ("jacobi", "learned"):
+                if start == "jacobi":
+                    g.assemble()
+                else:
+                    model.predict(g)
+                nb, nr = g.linear_residual()
+                if k >= k0:
+                    r0[start].append(nr / nb)
+            g.assemble()
+            g.sweeps(case.params.gauss_seidel_iter)
+            g.update()
+        g.close()
+    rj, rl = np.mean(r0["jacobi"]), np.mean(r0["learned"])
+    print(f"\nloss {hist[:10].mean():.4g} -> {hist[-50:].mean():.4g}; sweeps to 1e-3, steps "
+          f"< {k0}: {early}, steps >= {k0}: {tot}; initial residual (steps >= {k0}) "
+          f"jacobi {rj:.4g} learned {rl:.4g}")
+    assert rl < 0.8 * rj
+    assert tot["learned"] < tot["jacobi"] <= tot["zero"]
