@@ -152,7 +152,11 @@ def kernel_bytes(name, nc, nfi, nbf, sweeps, tb, tx):
         "face_flux": nc * (40 + 120 + 40) + nf * (geo_face + 48),
         "cell_residual": nc * (40 + 8 + 40 + 8) + nf * 48,
         "face_jacobian": nc * (40 + 120 + 40) + nf * geo_face + (nfi * 2 + nbf) * 25 * tb,
-        "assemble_lu": nc * (40 + 40 + 8 + 8 + 32 * tb + 5 * tx) + (2 * nfi + nbf) * 25 * tb,
+        # q, src, dtau, vol; LU + B slots, pivots, Jacobi start; each face
+        # block read once for the diagonal sum, interior ones written once
+        # more into the off-diagonal slots
+        "assemble_lu": (nc * (40 + 40 + 8 + 8 + 30 * tb + 4 + 5 * tx) + (2 * nfi + nbf) * 25 * tb
+                        + 2 * nfi * 25 * tb),
         "sgs_colour": sgs_bytes_per_step(nc, nfi, nbf, sweeps, tb, tx),
         "update": nc * (80 + 5 * tx),
     }.get(name)
@@ -306,13 +310,17 @@ def run_fpsi(args, ws, rank, local):
 
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
     Th, ph, uh = pin(T0), pin(p0), pin(u0)
+    outs = (pin(np.empty(nc)), pin(np.empty(nc)), pin(np.empty(3 * nc)))
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    solver.set_state(Th, ph, uh)
+    solver.newton_step()  # first touch of the pinned pages
+    solver.get_state(out=outs)
     dist_barrier(ws)
     t1 = time.perf_counter()
     for _ in range(e2e_steps):
         solver.set_state(Th, ph, uh)
         solver.newton_step()
-        Tn, pn, un = solver.get_state()
+        solver.get_state(out=outs)
     e2e_s = dist_max(time.perf_counter() - t1, ws)
     e2e = {"value": nc * e2e_steps * ws / e2e_s, "unit": "cell-iters/s",
            "h2d_bytes_per_step": 5 * 8 * nc, "d2h_bytes_per_step": 5 * 8 * nc + 64,
@@ -364,8 +372,8 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--profile-steps", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--cpu-n", type=int, default=40)
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-n", type=int, default=48)
+    ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -220,9 +220,16 @@ class FlowPsi:
         assert t.size == self.ncells
         N.check(N.lib().fpsi_set_eddy_viscosity(self._ctx, N.dptr(t)), "fpsi_set_eddy_viscosity")
 
-    def get_state(self):
+    def get_state(self, out=None):
+        """(T, pg, u) in caller order; `out` = caller arrays (float64,
+        contiguous; e.g. pinned host memory) to fill instead of new ones"""
         nc = self.ncells
-        T, pg, u = np.empty(nc), np.empty(nc), np.empty(nc * 3)
+        if out is None:
+            T, pg, u = np.empty(nc), np.empty(nc), np.empty(nc * 3)
+        else:
+            T, pg, u = out
+            for a, n in ((T, nc), (pg, nc), (u, 3 * nc)):
+                assert a.dtype == np.float64 and a.flags.c_contiguous and a.size == n
         N.check(N.lib().fpsi_get_state(self._ctx, N.dptr(T), N.dptr(pg), N.dptr(u)),
                 "fpsi_get_state")
         return T, pg, u.reshape(nc, 3)
