@@ -250,6 +250,36 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def time_to_drop(n: int, precision: str, drop: float = 1e-8, max_steps: int = 2000,
+                 chunk: int = 25, seed: int = 0):
+    """device time and implicit steps until the density residual (rtrms)
+    falls below drop x its step-0 value, on the steady farfield cube
+    (freestream M=0.5 with 1% noise, Roe + MUSCL + Venkatakrishnan, 5 SGS
+    sweeps, CFL 50)"""
+    from flowpsi_b200 import FlowPsi, cases
+
+    case = cases.farfield_cube(n, seed=seed, precision=precision)
+    s = FlowPsi(case.mesh, case.params)
+    s.keep_blocks(False)
+    s.set_state(*case.initial_state(s.geometry()["cellcenter"]))
+    r0, done, ms_tot, reached = None, 0, 0.0, None
+    while done < max_steps and reached is None:
+        hist, ms = s.run_timed(chunk)
+        if r0 is None:
+            r0 = hist[0]["rtrms"]
+        for k, h in enumerate(hist):
+            if h["rtrms"] < drop * r0:
+                reached = done + k
+                ms_tot += ms * k / chunk
+                break
+        else:
+            ms_tot += ms
+        done += chunk
+    s.close()
+    return {"steps": reached, "ms": ms_tot if reached is not None else None,
+            "cells": n ** 3}
+
+
 def run_fpsi(args, ws, rank, local):
     from flowpsi_b200 import FlowPsi
     from flowpsi_b200 import _native as N
@@ -334,6 +364,16 @@ def run_fpsi(args, ws, rank, local):
                "sample": f"taylor_green_tets {args.cpu_n}^3 x 6 = {ncs} cells, "
                          f"{args.cpu_steps} implicit steps ({dt:.1f} s), multi-colour SGS"}
 
+    converge = None
+    if args.converge_n > 0:
+        # second half of the metric: time to a 1e-8 residual drop on a steady
+        # case, FP64 against FP32 relaxation (MIXED)
+        c64 = time_to_drop(args.converge_n, "fp64")
+        c32 = time_to_drop(args.converge_n, "mixed")
+        converge = {"case": f"farfield_cube_{args.converge_n}", "drop": 1e-8, "fp64": c64,
+                    "mixed": c32,
+                    "speedup": (c64["ms"] / c32["ms"]) if c64["ms"] and c32["ms"] else None}
+
     launches = sum(v[1] for v in kt.values()) / args.profile_steps * args.steps
     line = {
         "metric": METRIC, "value": value, "unit": "cell-iters/s", "n_gpus": ws,
@@ -352,6 +392,7 @@ def run_fpsi(args, ws, rank, local):
         "gpu_launches": int(round(launches)),
         "clocks": clocks,
         "kernels": kernels,
+        "time_to_1e-8": converge,
         "resid_first": hist[0]["rtrms"] if hist else None,
         "resid_last": hist[-1]["rtrms"] if hist else None,
     }
@@ -375,6 +416,8 @@ def main():
     ap.add_argument("--cpu-n", type=int, default=48)
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--converge-n", type=int, default=128,
+                    help="farfield cube size for the time-to-1e-8 runs (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warning: fewer than 3 warm-up steps")

@@ -397,6 +397,7 @@ __device__ __forceinline__ void add_visc_jac(TB* M, const VFace& v, const double
 // ---------------------------------------------------------------------------
 // face flux + spectral radius, one thread per face
 // ---------------------------------------------------------------------------
+template <bool VIS>
 __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
                             const double* __restrict__ qb, const double* __restrict__ grad,
                             const double* __restrict__ phi, Gas g, int kind, Visc V,
@@ -415,7 +416,7 @@ __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
   } else {
     riemann(kind, s.L, s.R, nx, ny, nz, A, g, 0.0, 1.0, fl);
   }
-  if (V.on) {
+  if constexpr (VIS) {
     const VFace v = viscous_face(M, q, qb, grad, V, f);
 #pragma unroll
     for (int k = 0; k < 4; ++k) fl[1 + k] -= v.vf[k];
@@ -594,7 +595,7 @@ __global__ void k_norm_final(const double* __restrict__ part, int nblk,
 // touch 25 cache lines per instruction across the warp).
 constexpr int JAC_THREADS = 128;
 
-template <class TB>
+template <class TB, bool VIS>
 __global__ void __launch_bounds__(JAC_THREADS)
 k_face_jacobian(MeshView M, const double* __restrict__ q, const double* __restrict__ qb,
                 const double* __restrict__ grad, const double* __restrict__ phi, Gas g, Visc V,
@@ -621,7 +622,7 @@ k_face_jacobian(MeshView M, const double* __restrict__ q, const double* __restri
     } else {
       jac_roe<TB>(ra, nx, ny, nz, A, g, +1, st);
     }
-    if (V.on) {
+    if constexpr (VIS) {
       const double nn[3] = {nx, ny, nz};
       add_visc_jac<TB>(st, viscous_face(M, q, qb, grad, V, f), nn, A, +1.0);
     }
@@ -631,7 +632,7 @@ k_face_jacobian(MeshView M, const double* __restrict__ q, const double* __restri
   __syncthreads();
   if (live && f < M.nfi) {
     jac_roe<TB>(ra, nx, ny, nz, A, g, -1, stage + 25 * threadIdx.x);
-    if (V.on) {
+    if constexpr (VIS) {
       const double nn[3] = {nx, ny, nz};
       add_visc_jac<TB>(stage + 25 * threadIdx.x, viscous_face(M, q, qb, grad, V, f), nn, A, -1.0);
     }
@@ -734,51 +735,98 @@ struct SweepView {
 // with L = -fjp (solverLinearSystem.loci:57-77).  Threads run in RCM order;
 // the cells of one colour inside a warp have consecutive colour positions,
 // so every slot store fills whole 32 B sectors.
+//
+// Face blocks reach the threads through shared memory: for face entry e of
+// its 32 cells, a warp copies the (fjp, fjm) pairs with consecutive lanes on
+// consecutive words of each 25-entry block, then every thread adds its own
+// pair.  Each cell still sums its faces in list order.
+constexpr int ASM_THREADS = 128;
+constexpr int ASM_STRIDE = 33;  // shared row stride: 32 cells + 1 (no bank conflicts)
+constexpr int ASM_BATCH = 10;   // loads in flight per lane while staging
+template <class TB>
+constexpr size_t asm_smem_bytes() {
+  return size_t(ASM_THREADS / 32) * 50 * ASM_STRIDE * sizeof(TB);
+}
+
 template <class TB, class TX>
-__global__ void k_assemble(MeshView M, SweepView S, const double* __restrict__ q,
-                           const double* __restrict__ src, const double* __restrict__ dtau,
-                           const TB* __restrict__ fjp, const TB* __restrict__ fjm, Gas g,
-                           TB* __restrict__ luc, TB* __restrict__ bcv, int32_t* __restrict__ pvv,
-                           TB* __restrict__ aoff, TB* __restrict__ Dout, TX* __restrict__ x,
-                           int32_t* __restrict__ err) {
+__global__ void __launch_bounds__(ASM_THREADS, sizeof(TB) == 4 ? 6 : 4)
+k_assemble(MeshView M, SweepView S, const double* __restrict__ q, const double* __restrict__ src,
+           const double* __restrict__ dtau, const TB* __restrict__ fjp, const TB* __restrict__ fjm,
+           Gas g, TB* __restrict__ luc, TB* __restrict__ bcv, int32_t* __restrict__ pvv,
+           TB* __restrict__ aoff, TB* __restrict__ Dout, TX* __restrict__ x, int32_t* __restrict__ err) {
+  extern __shared__ __align__(16) unsigned char asm_smem[];
+  TB* st = reinterpret_cast<TB*>(asm_smem) + (threadIdx.x >> 5) * (50 * ASM_STRIDE);
+  const int lane = threadIdx.x & 31;
   const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (c >= M.nc) return;
-  const int64_t ci = S.ci[c];
-  const ColInfo ck = S.col[S.ccol[c]];
-  const int64_t i = ci - ck.cb, ld = ck.ld;
+  const bool active = c < M.nc;
+  int32_t e0 = 0, deg = 0;
+  int64_t ci = 0, i = 0, ld = 0;
+  ColInfo ck{};
+  if (active) {
+    e0 = M.cf_off[c];
+    deg = M.cf_off[c + 1] - e0;
+    ci = S.ci[c];
+    ck = S.col[S.ccol[c]];
+    i = ci - ck.cb;
+    ld = ck.ld;
+  }
+  const int maxdeg = __reduce_max_sync(0xffffffffu, deg);
   TB sJ[25];
 #pragma unroll
   for (int k = 0; k < 25; ++k) sJ[k] = TB(0);
   int64_t slot = 0;
-  for (int32_t e = M.cf_off[c]; e < M.cf_off[c + 1]; ++e) {
-    const int32_t ent = M.cf[e];
-    const int64_t f = ent >> 1;
-    const bool interior = f < M.nfi;
-    TB* ao = aoff ? aoff + 25 * ck.ebp + slot * 25 * ld + i : nullptr;
-    if (ent & 1) {
-      const TB* p = fjm + 25 * f;
+  for (int e = 0; e < maxdeg; ++e) {
+    const int32_t my_ent = e < deg ? M.cf[e0 + e] : -1;
+    // 1600 words per round, 50 per lane, in batches of ASM_BATCH independent
+    // loads (fjm is allocated for every face, so every address is valid;
+    // lanes without an entry read face 0 and their words are never used)
+#pragma unroll 1
+    for (int b = 0; b < 50 / ASM_BATCH; ++b) {
+      TB v[ASM_BATCH];
 #pragma unroll
-      for (int k = 0; k < 25; ++k) sJ[k] += p[k];
-      if (ao) {
-        const TB* l = fjp + 25 * f;
-#pragma unroll
-        for (int k = 0; k < 25; ++k) ao[k * ld] = -l[k];
+      for (int u = 0; u < ASM_BATCH; ++u) {
+        const int idx = lane + 32 * (ASM_BATCH * b + u);
+        const int L = idx / 50, k = idx - 50 * L;
+        const int32_t ent = __shfl_sync(0xffffffffu, my_ent, L);
+        const int64_t f = ent >= 0 ? int64_t(ent >> 1) : 0;
+        v[u] = k < 25 ? __ldg(fjp + 25 * f + k) : __ldg(fjm + 25 * f + (k - 25));
       }
-      ++slot;
-    } else {
-      const TB* p = fjp + 25 * f;
 #pragma unroll
-      for (int k = 0; k < 25; ++k) sJ[k] -= p[k];
-      if (interior) {
-        if (ao) {
-          const TB* u = fjm + 25 * f;
-#pragma unroll
-          for (int k = 0; k < 25; ++k) ao[k * ld] = u[k];
-        }
-        ++slot;
+      for (int u = 0; u < ASM_BATCH; ++u) {
+        const int idx = lane + 32 * (ASM_BATCH * b + u);
+        const int L = idx / 50, k = idx - 50 * L;
+        st[k * ASM_STRIDE + L] = v[u];
       }
     }
+    __syncwarp();
+    if (my_ent >= 0) {
+      const int64_t f = my_ent >> 1;
+      const TB* sp = st + lane;                    // fjp of the face
+      const TB* sm = st + 25 * ASM_STRIDE + lane;  // fjm of the face
+      TB* ao = aoff ? aoff + 25 * ck.ebp + slot * 25 * ld + i : nullptr;
+      if (my_ent & 1) {
+#pragma unroll
+        for (int k = 0; k < 25; ++k) sJ[k] += sm[k * ASM_STRIDE];
+        if (ao) {
+#pragma unroll
+          for (int k = 0; k < 25; ++k) ao[k * ld] = -sp[k * ASM_STRIDE];
+        }
+        ++slot;
+      } else {
+#pragma unroll
+        for (int k = 0; k < 25; ++k) sJ[k] -= sp[k * ASM_STRIDE];
+        if (f < M.nfi) {
+          if (ao) {
+#pragma unroll
+            for (int k = 0; k < 25; ++k) ao[k * ld] = sm[k * ASM_STRIDE];
+          }
+          ++slot;
+        }
+      }
+    }
+    __syncwarp();
   }
+  if (!active) return;
   TB D[25];
 #pragma unroll
   for (int i = 0; i < 25; ++i) D[i] = -sJ[i];
@@ -1115,9 +1163,14 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
                                                              x->P.Kl, x->d_grad, x->d_phi);
   prof_end(x);
   prof_begin(x, "face_flux");
-  dev::k_face_flux<<<blocks_for(M.nf, 128), 128, 0, s>>>(M, x->d_q, x->d_qb, x->d_grad,
-                                                          x->d_phi, g, x->P.flux, visc(x),
-                                                          x->d_F, x->d_mev);
+  // the viscous terms are a separate instantiation: the inviscid kernel
+  // does not carry their registers
+  if (x->P.viscous)
+    dev::k_face_flux<true><<<blocks_for(M.nf, 128), 128, 0, s>>>(
+        M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, x->P.flux, visc(x), x->d_F, x->d_mev);
+  else
+    dev::k_face_flux<false><<<blocks_for(M.nf, 128), 128, 0, s>>>(
+        M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, x->P.flux, visc(x), x->d_F, x->d_mev);
   prof_end(x);
   prof_begin(x, "cell_residual");
   dev::k_cell_residual<<<x->nblk_norm, dev::NORM_THREADS, 0, s>>>(
@@ -1150,11 +1203,19 @@ static int launch_assemble_t(fpsi_ctx* x) {
   TB* fjp = (TB*)x->d_fjp;
   TB* fjm = (TB*)x->d_fjm;
   prof_begin(x, "face_jacobian");
-  dev::k_face_jacobian<TB><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
-      M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, visc(x), fjp, fjm);
+  if (x->P.viscous)
+    dev::k_face_jacobian<TB, true><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
+        M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, visc(x), fjp, fjm);
+  else
+    dev::k_face_jacobian<TB, false><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
+        M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, visc(x), fjp, fjm);
   prof_end(x);
   prof_begin(x, "assemble_lu");
-  dev::k_assemble<TB, TX><<<blocks_for(M.nc, 128), 128, 0, s>>>(
+  constexpr size_t smem = dev::asm_smem_bytes<TB>();
+  if (smem > 48 * 1024)
+    FPSI_CUDA_TRY(cudaFuncSetAttribute(dev::k_assemble<TB, TX>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  dev::k_assemble<TB, TX><<<blocks_for(M.nc, dev::ASM_THREADS), dev::ASM_THREADS, smem, s>>>(
       M, sweep_view(x), x->d_q, x->d_src, x->d_dtau, fjp, fjm, g, (TB*)x->d_luc, (TB*)x->d_bc,
       x->d_pv, x->P.solver == FPSI_SOLVER_LSGS ? nullptr : (TB*)x->d_aoff,
       x->keep_D ? (TB*)x->d_D : nullptr, (TX*)x->d_x, x->d_err);
