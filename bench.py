@@ -163,10 +163,28 @@ def kernel_bytes(name, nc, nfi, nbf, sweeps, tb, tx):
 
 
 def build_case(args):
+    """the bench workload: the Taylor-Green split-tet grid (default), the
+    turbulent boundary-layer block with line SGS and the viscous terms, or
+    the oblique-shock hex cube"""
     from flowpsi_b200 import cases
 
+    if args.workload == "bl":
+        return cases.boundary_layer_block(args.bl_nx, args.bl_ny, args.bl_nz,
+                                          precision=args.precision, viscous=args.viscous,
+                                          solver="lsgs")
+    if args.workload == "shock":
+        return cases.oblique_shock_cube(args.n, seed=args.seed, sweeps=args.sweeps,
+                                        precision=args.precision)
     return cases.taylor_green_tets(args.n, seed=args.seed, sweeps=args.sweeps,
                                    precision=args.precision)
+
+
+def workload_name(args) -> str:
+    if args.workload == "bl":
+        return f"boundary_layer_{args.bl_nx}x{args.bl_ny}x{args.bl_nz}_visc{args.viscous}"
+    if args.workload == "shock":
+        return f"oblique_shock_cube_{args.n}"
+    return f"taylor_green_tets_{args.n}"
 
 
 class OracleSample:
@@ -289,7 +307,12 @@ def run_fpsi(args, ws, rank, local):
     t0 = time.perf_counter()
     case = build_case(args)
     solver = FlowPsi(case.mesh, case.params)
-    solver.keep_blocks(False)
+    if case.params.solver == 1:  # line SGS over the case's wall-normal lines
+        solver.set_lines(case.lines)
+    else:
+        solver.keep_blocks(False)
+    if getattr(case, "tmu", None) is not None:
+        solver.set_eddy_viscosity(case.tmu)
     log(f"[rank {rank}] setup {time.perf_counter() - t0:.1f}s: {solver.ncells} cells, "
         f"{solver.nfaces} faces, {solver.ncolours} colours, "
         f"{solver.device_bytes / 1e9:.2f} GB device")
@@ -297,7 +320,8 @@ def run_fpsi(args, ws, rank, local):
     T0, p0, u0 = case.initial_state(geo["cellcenter"])
     solver.set_state(T0, p0, u0)
     nc, nf = solver.ncells, solver.nfaces
-    nfi = nf  # periodic grid: every face is interior
+    nfi = int((np.asarray(case.mesh.arrays().cr) >= 0).sum())
+    nbf = nf - nfi
     hist_w = solver.run(args.warmup) if args.warmup > 0 else []
     dist_barrier(ws)
     with Clocks(local) as clk:
@@ -314,21 +338,21 @@ def run_fpsi(args, ws, rank, local):
     peak = float(peaks["hbm_gbs"])
     kernels = {}
     for name, (kms, launches) in kt.items():
-        b = kernel_bytes(name, nc, nfi, 0, args.sweeps, tb, tx)
-        if b is None:
-            continue
+        b = kernel_bytes(name, nc, nfi, nbf, args.sweeps, tb, tx)
         per_step_ms = kms / args.profile_steps
         kernels[name] = {"ms_per_step": per_step_ms, "launches_per_step": launches / args.profile_steps,
-                         "gbs": b / (per_step_ms / 1e3) / 1e9}
-    dom = max(kernels, key=lambda k: kernels[k]["ms_per_step"])
+                         "gbs": None if b is None else b / (per_step_ms / 1e3) / 1e9}
+    dom = max((k for k in kernels if kernels[k]["gbs"] is not None),
+              key=lambda k: kernels[k]["ms_per_step"])
     dk = kernels[dom]
-    b_launch = kernel_bytes(dom, nc, nfi, 0, args.sweeps, tb, tx) / dk["launches_per_step"]
+    b_launch = kernel_bytes(dom, nc, nfi, nbf, args.sweeps, tb, tx) / dk["launches_per_step"]
     avg_launch_s = dk["ms_per_step"] / dk["launches_per_step"] / 1e3
     achieved = b_launch / avg_launch_s / 1e9
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
-        traffic = json.loads(tf.read_text()).get(f"{dom}:{args.precision}:{args.n}")
+        key = f"{dom}:{args.precision}:{args.n}" if args.workload == "tgv" else None
+        traffic = json.loads(tf.read_text()).get(key) if key else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "kernel": dom,
                 "peak_source": src, "bytes_per_launch": b_launch}
@@ -380,10 +404,15 @@ def run_fpsi(args, ws, rank, local):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 residual + f32 blocks/sweeps" if args.precision == "mixed" else args.precision,
-        "data": "synthetic (seeded Taylor-Green on a jittered split-tet grid)",
-        "config": {"workload": f"taylor_green_tets_{args.n}", "cells": nc, "faces": nf,
+        "data": {"tgv": "synthetic (seeded Taylor-Green on a jittered split-tet grid)",
+                 "bl": "synthetic (seeded noise on a flat-plate block, frozen SA eddy viscosity)",
+                 "shock": "synthetic (seeded oblique Mach-2 shock on a hex cube)"}[args.workload],
+        "config": {"workload": workload_name(args), "cells": nc, "faces": nf,
                    "colours": solver.ncolours, "precision": args.precision,
-                   "flux": "roe", "limiter": "venkatakrishnan", "sgs_sweeps": args.sweeps,
+                   "flux": {v: k for k, v in N.FLUX.items()}[case.params.flux],
+                   "limiter": {v: k for k, v in N.LIMITER.items()}[case.params.limiter],
+                   "solver": "lsgs" if case.params.solver == 1 else "sgs",
+                   "sgs_sweeps": case.params.gauss_seidel_iter,
                    "parallelism": f"replicas{ws}",
                    "l2": "inputs larger than L2 (%.1f GB resident)" % (solver.device_bytes / 1e9)},
         "roofline": roofline,
@@ -416,6 +445,11 @@ def main():
     ap.add_argument("--cpu-n", type=int, default=48)
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "bl", "shock"])
+    ap.add_argument("--bl-nx", type=int, default=256)
+    ap.add_argument("--bl-ny", type=int, default=128)
+    ap.add_argument("--bl-nz", type=int, default=64)
+    ap.add_argument("--viscous", type=int, default=2, help="bl: 0 inviscid, 1 laminar, 2 SA tmu")
     ap.add_argument("--converge-n", type=int, default=128,
                     help="farfield cube size for the time-to-1e-8 runs (0: skip)")
     args = ap.parse_args()

@@ -101,11 +101,11 @@ int alloc_system(fpsi_ctx* x) {
 }
 
 void free_lsgs(fpsi_ctx* x) {
-  void* ps[] = {x->d_lt, x->d_lonbr, x->d_llen, x->d_lrole, x->d_lrow0, x->d_lD, x->d_lL,
+  void* ps[] = {x->d_lt, x->d_lct, x->d_lonbr, x->d_llen, x->d_lrole, x->d_lrow0, x->d_lD, x->d_lL,
                 x->d_lU, x->d_lF, x->d_lB, x->d_lrhs, x->d_lx, x->d_lxt, x->d_lctl, x->d_lpart};
   for (void* p : ps)
     if (p) cudaFree(p);
-  x->d_lt = x->d_lonbr = x->d_llen = nullptr;
+  x->d_lt = x->d_lct = x->d_lonbr = x->d_llen = nullptr;
   x->d_lrole = nullptr;
   x->d_lrow0 = nullptr;
   x->d_lD = x->d_lL = x->d_lU = x->d_lF = x->d_lB = x->d_lrhs = x->d_lx = x->d_lxt = nullptr;
@@ -127,6 +127,7 @@ int alloc_lsgs(fpsi_ctx* x) {
   const int tx = td;
   const size_t nt = size_t(Y.nrows) * 32;
   if ((rc = upload(x, &x->d_lt, Y.t_of))) return rc;
+  if ((rc = upload(x, &x->d_lct, Y.c_of_t))) return rc;
   if ((rc = upload(x, &x->d_lrole, Y.role))) return rc;
   if ((rc = upload(x, &x->d_lonbr, Y.onbr))) return rc;
   if ((rc = upload(x, &x->d_llen, Y.lane_len))) return rc;
@@ -577,6 +578,10 @@ static int finish_assemble(fpsi_ctx* x) {
   if (rc) return rc;
   if (err) {
     FPSI_CUDA_TRY(cudaMemset(x->d_err, 0, sizeof(int32_t)));
+    if (err & 4) {
+      fpsi::set_error("a line solve gave up waiting for its staged rows");
+      return FPSI_E_TIMEOUT;
+    }
     fpsi::set_error("zero pivot in a diagonal block LU");
     return FPSI_E_SINGULAR;
   }

@@ -166,6 +166,7 @@ struct fpsi_ctx {
   // line SGS (solver == LSGS)
   fpsi::LineLayout LY;
   int32_t *d_lt = nullptr, *d_lonbr = nullptr, *d_llen = nullptr;
+  int32_t* d_lct = nullptr;    // line slot t -> RCM cell (-1: padding)
   int8_t* d_lrole = nullptr;
   int64_t* d_lrow0 = nullptr;
   void *d_lD = nullptr, *d_lL = nullptr, *d_lU = nullptr, *d_lF = nullptr, *d_lB = nullptr;

@@ -261,21 +261,25 @@ struct LsgsCtl {
 // Gather the line-ordered system: raw diagonal block, in-line couplings
 // (row p to p-1 in L, to p+1 in U), outer couplings and B.  The coupling of
 // row c to neighbour n through face f is fjm_f when c = cl(f), -fjp_f when
-// c = cr(f) (solverLinearSystem.loci:57-77).
+// c = cr(f) (solverLinearSystem.loci:57-77).  One thread per line slot t,
+// so that the 32 lanes of a row store 32 consecutive words of every stream;
+// padding slots are left as they are (never read as data).
 template <class TB, class TD>
-__global__ void k_lsgs_scatter(int64_t nc, const int32_t* __restrict__ cf_off,
-                               const int32_t* __restrict__ cf, LineView V,
-                               const TB* __restrict__ D, const TB* __restrict__ fjp,
+__global__ void k_lsgs_scatter(int64_t nt, const int32_t* __restrict__ c_of_t,
+                               const int32_t* __restrict__ cf_off, const int32_t* __restrict__ cf,
+                               LineView V, const TB* __restrict__ D, const TB* __restrict__ fjp,
                                const TB* __restrict__ fjm, const double* __restrict__ src,
                                TD* __restrict__ lD, TB* __restrict__ lL, TB* __restrict__ lU,
                                TB* __restrict__ lF, TB* __restrict__ lB) {
-  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (c >= nc) return;
-  const int64_t t = V.t_of[c], r = t >> 5, lane = t & 31;
+  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  const int64_t c = c_of_t[t];
+  if (c < 0) return;
+  const int64_t r = t >> 5, lane = t & 31;
 #pragma unroll
-  for (int e = 0; e < 25; ++e) lD[(r * 25 + e) * 32 + lane] = TD(D[25 * c + e]);
+  for (int e = 0; e < 25; ++e) lD[(r * 25 + e) * 32 + lane] = TD(__ldg(D + 25 * c + e));
 #pragma unroll
-  for (int k = 0; k < 5; ++k) lB[(r * 5 + k) * 32 + lane] = TB(src[5 * c + k]);
+  for (int k = 0; k < 5; ++k) lB[(r * 5 + k) * 32 + lane] = TB(__ldg(src + 5 * c + k));
   for (int32_t e = cf_off[c]; e < cf_off[c + 1]; ++e) {
     const int ro = V.role[e];
     if (ro == 0) continue;
@@ -291,7 +295,7 @@ __global__ void k_lsgs_scatter(int64_t nc, const int32_t* __restrict__ cf_off,
     else
       o = lF + (r * V.mout + (ro - 3)) * 25 * 32 + lane;
 #pragma unroll
-    for (int k = 0; k < 25; ++k) o[k * 32] = neg ? TB(-A[k]) : A[k];
+    for (int k = 0; k < 25; ++k) o[k * 32] = neg ? TB(-__ldg(A + k)) : __ldg(A + k);
   }
 }
 
@@ -408,73 +412,236 @@ __global__ void k_lsgs_rhs(int64_t row_begin, int64_t nrows, LineView V,
   for (int k = 0; k < 5; ++k) rhs[(r * 5 + k) * 32 + lane] = b[k];
 }
 
-// block Thomas solve of the lines of groups [g0, g0+ng) (lineSolve,
-// linearSolverLSGS.loci:1523-1572).  use_B: right-hand side B (start);
-// save_xt: keep the iterate before the solve for the relaxation.
+// ---- bulk-copy pipeline (TMA engine, no multicast) -------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait: false after ~2^24 polls (each poll may suspend the warp)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (uint32_t it = 0; it < (1u << 24); ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+constexpr int LSGS_NST = 4;  // pipeline depth (rows in flight per group)
+
 template <class TB, class TD, class TX>
-__global__ void k_lsgs_thomas(int64_t g0, int64_t ng, LineView V, const TD* __restrict__ lD,
-                              const TB* __restrict__ lL, const TB* __restrict__ lU,
-                              const TX* __restrict__ rhs, const TB* __restrict__ lB, int use_B,
-                              int save_xt, TX* __restrict__ x, TX* __restrict__ xt,
-                              const LsgsCtl* __restrict__ ctl) {
+struct ThomasStage {
+  static constexpr uint32_t d_bytes = 25 * 32 * sizeof(TD);
+  static constexpr uint32_t m_bytes = 25 * 32 * sizeof(TB);  // L (forward) or U (backward)
+  static constexpr uint32_t b_bytes = 5 * 32 * (sizeof(TX) > sizeof(TB) ? sizeof(TX) : sizeof(TB));
+  static constexpr uint32_t x_bytes = 5 * 32 * sizeof(TX);  // one row of the iterate
+  static constexpr uint32_t bytes = d_bytes + m_bytes + b_bytes + x_bytes;  // multiple of 16
+};
+template <class TB, class TD, class TX>
+constexpr size_t thomas_smem_bytes() {
+  return size_t(LSGS_NST) * ThomasStage<TB, TD, TX>::bytes + 16 * LSGS_NST;
+}
+
+// block Thomas solve of the lines of groups [g0, g0+ng) (lineSolve,
+// linearSolverLSGS.loci:1523-1572), one warp per group of 32 lines, one
+// line per lane.  use_B: right-hand side B (start); save_xt: keep the
+// iterate before the solve for the relaxation.
+//
+// A group's rows are contiguous ([row][entry][32 lanes]), so each row's
+// factored diagonal block, coupling block and right-hand side arrive as
+// bulk copies into shared memory, LSGS_NST rows ahead of the recurrence.
+// The iterate's row comes the same way: before the forward solve
+// overwrites it (kept for the relaxation) and, in the back substitution,
+// the forward result (written by this warp, then made visible to the copy
+// engine by a proxy fence).  Lane 0 issues the copies; every wait is
+// bounded and a wait that gives up sets bit 4 of err and ends the kernel
+// once the copies in flight landed.
+template <class TB, class TD, class TX>
+__global__ void __launch_bounds__(32)
+k_lsgs_thomas(int64_t g0, LineView V, const TD* __restrict__ lD, const TB* __restrict__ lL,
+              const TB* __restrict__ lU, const TX* __restrict__ rhs, const TB* __restrict__ lB,
+              int use_B, int save_xt, TX* __restrict__ x, TX* __restrict__ xt,
+              const LsgsCtl* __restrict__ ctl, int32_t* __restrict__ err) {
+  using S = ThomasStage<TB, TD, TX>;
   if (ctl && ctl->done) return;
-  const int64_t gl = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (gl >= ng * 32) return;
-  const int64_t g = g0 + (gl >> 5), lane = gl & 31;
+  extern __shared__ __align__(128) unsigned char th_smem[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(th_smem + size_t(LSGS_NST) * S::bytes);
+  auto stage = [&](int s) { return th_smem + size_t(s) * S::bytes; };
+  const int lane = threadIdx.x;
+  const int64_t g = g0 + blockIdx.x;
   const int len = V.lane_len[g * 32 + lane];
+  const int glen = __reduce_max_sync(0xffffffffu, len);
   const int64_t r0 = V.grp_row0[g];
-  // forward elimination: y_p = rhs_p - L_p D'_{p-1}^{-1} y_{p-1}
-  TX y[5];
-  for (int p = 0; p < len; ++p) {
+  if (lane == 0)
+    for (int s = 0; s < LSGS_NST; ++s) mbar_init(bar + s);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  __syncwarp();
+  uint32_t phase = 0;  // bit s: parity of the next completion of stage s
+  int inflight = 0;    // bit s: stage s has copies outstanding
+  bool ok = true;
+
+  // forward stage for row p: D'_{p-1}, L_p (p > 0) and the right-hand side
+  auto issue_fwd = [&](int p) {
+    const int s = p % LSGS_NST;
     const int64_t r = r0 + p;
-    const int64_t t = r * 32 + lane;
-    TX yn[5];
-#pragma unroll
-    for (int k = 0; k < 5; ++k)
-      yn[k] = use_B ? TX(lB[(r * 5 + k) * 32 + lane]) : rhs[(r * 5 + k) * 32 + lane];
+    unsigned char* st = stage(s);
+    const uint32_t bb = 5 * 32 * uint32_t(use_B ? sizeof(TB) : sizeof(TX));
+    mbar_expect_tx(bar + s, (p > 0 ? S::d_bytes + S::m_bytes : 0) + bb + (save_xt ? S::x_bytes : 0));
+    if (save_xt) bulk_g2s(st + S::d_bytes + S::m_bytes + S::b_bytes, x + r * 32 * 5, S::x_bytes, bar + s);
     if (p > 0) {
+      bulk_g2s(st, lD + (r - 1) * 25 * 32, S::d_bytes, bar + s);
+      bulk_g2s(st + S::d_bytes, lL + r * 25 * 32, S::m_bytes, bar + s);
+    }
+    if (use_B)
+      bulk_g2s(st + S::d_bytes + S::m_bytes, lB + r * 5 * 32, bb, bar + s);
+    else
+      bulk_g2s(st + S::d_bytes + S::m_bytes, rhs + r * 5 * 32, bb, bar + s);
+  };
+  // backward stage for row p: D'_p, U_p and the forward result y_p
+  auto issue_bwd = [&](int p) {
+    const int s = (glen - 1 - p) % LSGS_NST;
+    const int64_t r = r0 + p;
+    unsigned char* st = stage(s);
+    mbar_expect_tx(bar + s, S::d_bytes + S::m_bytes + S::x_bytes);
+    bulk_g2s(st, lD + r * 25 * 32, S::d_bytes, bar + s);
+    bulk_g2s(st + S::d_bytes, lU + r * 25 * 32, S::m_bytes, bar + s);
+    bulk_g2s(st + S::d_bytes + S::m_bytes + S::b_bytes, x + r * 32 * 5, S::x_bytes, bar + s);
+  };
+  auto wait_stage = [&](int s) {
+    const bool got = mbar_wait(bar + s, (phase >> s) & 1u);
+    if (got) {
+      phase ^= 1u << s;
+      inflight &= ~(1 << s);
+    }
+    return got;
+  };
+
+  // forward elimination: y_p = rhs_p - L_p D'_{p-1}^{-1} y_{p-1}
+  for (int p = 0; p < min(glen, LSGS_NST); ++p) {
+    if (lane == 0) issue_fwd(p);
+    inflight |= 1 << (p % LSGS_NST);
+  }
+  TX y[5];
+  for (int p = 0; p < glen && ok; ++p) {
+    const int s = p % LSGS_NST;
+    ok = __all_sync(0xffffffffu, wait_stage(s));
+    if (!ok) break;
+    const unsigned char* st = stage(s);
+    const TD* sD = reinterpret_cast<const TD*>(st) + lane;
+    const TB* sL = reinterpret_cast<const TB*>(st + S::d_bytes) + lane;
+    const int64_t t = (r0 + p) * 32 + lane;
+    TX yn[5];
+    if (use_B) {
+      const TB* sb = reinterpret_cast<const TB*>(st + S::d_bytes + S::m_bytes) + lane;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) yn[k] = TX(sb[k * 32]);
+    } else {
+      const TX* sb = reinterpret_cast<const TX*>(st + S::d_bytes + S::m_bytes) + lane;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) yn[k] = sb[k * 32];
+    }
+    if (p > 0 && p < len) {
       TD Dm[25];
 #pragma unroll
-      for (int e = 0; e < 25; ++e) Dm[e] = lD[((r - 1) * 25 + e) * 32 + lane];
+      for (int e = 0; e < 25; ++e) Dm[e] = sD[e * 32];
       lu5_nopiv_solve<TD, TX>(Dm, y);
 #pragma unroll
       for (int k = 0; k < 5; ++k)
 #pragma unroll
-        for (int j = 0; j < 5; ++j) yn[k] -= TX(lL[(r * 25 + 5 * k + j) * 32 + lane]) * y[j];
+        for (int j = 0; j < 5; ++j) yn[k] -= TX(sL[(5 * k + j) * 32]) * y[j];
     }
+    TX xo[5];
     if (save_xt) {
+      const TX* sx = reinterpret_cast<const TX*>(st + S::d_bytes + S::m_bytes + S::b_bytes) + 5 * lane;
 #pragma unroll
-      for (int k = 0; k < 5; ++k) xt[5 * t + k] = x[5 * t + k];
+      for (int k = 0; k < 5; ++k) xo[k] = sx[k];
     }
+    __syncwarp();
+    if (lane == 0 && p + LSGS_NST < glen) issue_fwd(p + LSGS_NST);
+    if (p + LSGS_NST < glen) inflight |= 1 << s;
+    if (p < len) {
+      if (save_xt) {
 #pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      y[k] = yn[k];
-      x[5 * t + k] = yn[k];
+        for (int k = 0; k < 5; ++k) xt[5 * t + k] = xo[k];
+      }
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        y[k] = yn[k];
+        x[5 * t + k] = yn[k];
+      }
     }
   }
-  // back substitution: x_p = D'_p^{-1} (y_p - U_p x_{p+1})
-  TX xn[5];
-  for (int p = len - 1; p >= 0; --p) {
-    const int64_t r = r0 + p;
-    const int64_t t = r * 32 + lane;
-    TX v[5];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) v[k] = x[5 * t + k];
-    if (p < len - 1) {
-#pragma unroll
-      for (int k = 0; k < 5; ++k)
-#pragma unroll
-        for (int j = 0; j < 5; ++j) v[k] -= TX(lU[(r * 25 + 5 * k + j) * 32 + lane]) * xn[j];
+  // back substitution: x_p = D'_p^{-1} (y_p - U_p x_{p+1}); the forward
+  // results are read back through the copy engine
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+  __syncwarp();
+  if (ok) {
+    for (int q = 0; q < min(glen, LSGS_NST); ++q) {
+      if (lane == 0) issue_bwd(glen - 1 - q);
+      inflight |= 1 << (q % LSGS_NST);
     }
-    TD Dp[25];
+    TX xn[5];
+    for (int q = 0; q < glen && ok; ++q) {
+      const int p = glen - 1 - q;
+      const int s = q % LSGS_NST;
+      ok = __all_sync(0xffffffffu, wait_stage(s));
+      if (!ok) break;
+      const unsigned char* st = stage(s);
+      const TD* sD = reinterpret_cast<const TD*>(st) + lane;
+      const TB* sU = reinterpret_cast<const TB*>(st + S::d_bytes) + lane;
+      const int64_t t = (r0 + p) * 32 + lane;
+      TX v[5];
+      TD Dp[25];
+      if (p < len) {
+        const TX* sx = reinterpret_cast<const TX*>(st + S::d_bytes + S::m_bytes + S::b_bytes) + 5 * lane;
 #pragma unroll
-    for (int e = 0; e < 25; ++e) Dp[e] = lD[(r * 25 + e) * 32 + lane];
-    lu5_nopiv_solve<TD, TX>(Dp, v);
+        for (int k = 0; k < 5; ++k) v[k] = sx[k];
+        if (p < len - 1) {
 #pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      x[5 * t + k] = v[k];
-      xn[k] = v[k];
+          for (int k = 0; k < 5; ++k)
+#pragma unroll
+            for (int j = 0; j < 5; ++j) v[k] -= TX(sU[(5 * k + j) * 32]) * xn[j];
+        }
+#pragma unroll
+        for (int e = 0; e < 25; ++e) Dp[e] = sD[e * 32];
+      }
+      __syncwarp();
+      if (lane == 0 && q + LSGS_NST < glen) issue_bwd(p - LSGS_NST);
+      if (q + LSGS_NST < glen) inflight |= 1 << s;
+      if (p < len) {
+        lu5_nopiv_solve<TD, TX>(Dp, v);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+          x[5 * t + k] = v[k];
+          xn[k] = v[k];
+        }
+      }
     }
+  }
+  if (!ok) {
+    if (lane == 0) atomicOr(err, 4);
+    // let the copies in flight land before the block's shared memory goes
+    for (int s = 0; s < LSGS_NST; ++s)
+      if (inflight & (1 << s)) mbar_wait(bar + s, (phase >> s) & 1u);
   }
 }
 
@@ -567,8 +734,8 @@ static int lsgs_assemble_t(fpsi_ctx* x) {
   cudaStream_t s = x->stream;
   const dev::LineView V = line_view(x);
   prof_begin(x, "lsgs_scatter");
-  dev::k_lsgs_scatter<TB, TD><<<nblocks(x->H.nc, 128), 128, 0, s>>>(
-      x->H.nc, x->d_cf_off, x->d_cf, V, (const TB*)x->d_D, (const TB*)x->d_fjp,
+  dev::k_lsgs_scatter<TB, TD><<<nblocks(Y.nrows * 32, 128), 128, 0, s>>>(
+      Y.nrows * 32, x->d_lct, x->d_cf_off, x->d_cf, V, (const TB*)x->d_D, (const TB*)x->d_fjp,
       (const TB*)x->d_fjm, x->d_src, (TD*)x->d_lD, (TB*)x->d_lL, (TB*)x->d_lU, (TB*)x->d_lF,
       (TB*)x->d_lB);
   prof_end(x);
@@ -601,11 +768,15 @@ static int lsgs_solve_t(fpsi_ctx* x, bool jacobi_start) {
   TX* X = (TX*)x->d_lx;
   TX* XT = (TX*)x->d_lxt;
   dev::k_lsgs_init<<<1, 1, 0, s>>>(ctl, x->P.lsgs_relaxation);
+  constexpr size_t th_smem = dev::thomas_smem_bytes<TB, TD, TX>();
+  if (th_smem > 48 * 1024)
+    FPSI_CUDA_TRY(cudaFuncSetAttribute(dev::k_lsgs_thomas<TB, TD, TX>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(th_smem)));
   if (jacobi_start) {
     prof_begin(x, "lsgs_thomas");
-    dev::k_lsgs_thomas<TB, TD, TX><<<nblocks(Y.ngroups * 32, 64), 64, 0, s>>>(
-        0, Y.ngroups, V, (const TD*)x->d_lD, (const TB*)x->d_lL, (const TB*)x->d_lU, nullptr,
-        (const TB*)x->d_lB, 1, 0, X, XT, nullptr);
+    dev::k_lsgs_thomas<TB, TD, TX><<<unsigned(Y.ngroups), 32, th_smem, s>>>(
+        0, V, (const TD*)x->d_lD, (const TB*)x->d_lL, (const TB*)x->d_lU, nullptr,
+        (const TB*)x->d_lB, 1, 0, X, XT, nullptr, x->d_err);
     prof_end(x);
   }
   const int K = Y.ncolours;
@@ -623,9 +794,9 @@ static int lsgs_solve_t(fpsi_ctx* x, bool jacobi_start) {
             rb, re - rb, V, (const TB*)x->d_lF, (const TB*)x->d_lB, X, (TX*)x->d_lrhs, ctl);
         prof_end(x);
         prof_begin(x, "lsgs_thomas");
-        dev::k_lsgs_thomas<TB, TD, TX><<<nblocks(ng * 32, 64), 64, 0, s>>>(
-            g0, ng, V, (const TD*)x->d_lD, (const TB*)x->d_lL, (const TB*)x->d_lU,
-            (const TX*)x->d_lrhs, (const TB*)x->d_lB, 0, pass == 1 ? 1 : 0, X, XT, ctl);
+        dev::k_lsgs_thomas<TB, TD, TX><<<unsigned(ng), 32, th_smem, s>>>(
+            g0, V, (const TD*)x->d_lD, (const TB*)x->d_lL, (const TB*)x->d_lU,
+            (const TX*)x->d_lrhs, (const TB*)x->d_lB, 0, pass == 1 ? 1 : 0, X, XT, ctl, x->d_err);
         prof_end(x);
       }
     prof_begin(x, "lsgs_relax");
