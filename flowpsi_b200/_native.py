@@ -34,7 +34,7 @@ class Params(C.Structure):
         ("cflmax", C.c_double), ("solver", C.c_int32), ("gauss_seidel_iter", C.c_int32),
         ("lsgs_relaxation", C.c_double), ("lsgs_abs_tol", C.c_double),
         ("lsgs_rel_tol", C.c_double), ("lsgs_max_iter", C.c_int32),
-        ("precision", C.c_int32), ("viscous", C.c_int32), ("reserved0", C.c_int32),
+        ("precision", C.c_int32), ("viscous", C.c_int32), ("turbulence", C.c_int32),
         ("Prt", C.c_double), ("mu_a1", C.c_double), ("mu_a2", C.c_double),
         ("mu_a3", C.c_double), ("k_a1", C.c_double), ("k_a2", C.c_double),
         ("k_a3", C.c_double),
@@ -43,7 +43,7 @@ class Params(C.Structure):
 
 class BCSpec(C.Structure):
     _fields_ = [("kind", C.c_int32), ("reserved", C.c_int32), ("T", C.c_double),
-                ("pg", C.c_double), ("u", C.c_double * 3)]
+                ("pg", C.c_double), ("u", C.c_double * 3), ("nu_t", C.c_double)]
 
 
 class Mesh(C.Structure):
@@ -111,6 +111,14 @@ _SIGS = {
     "fpsi_get_lines": (C.c_int, [_ctx, _ip, _ip, _ip, C.POINTER(C.c_int64)]),
     "fpsi_set_state": (C.c_int, [_ctx, _dp, _dp, _dp]),
     "fpsi_set_eddy_viscosity": (C.c_int, [_ctx, _dp]),
+    "fpsi_set_nutilde": (C.c_int, [_ctx, _dp]),
+    "fpsi_get_nutilde": (C.c_int, [_ctx, _dp]),
+    "fpsi_get_eddy_viscosity": (C.c_int, [_ctx, _dp]),
+    "fpsi_get_wall_distance": (C.c_int, [_ctx, _dp]),
+    "fpsi_sa_residual": (C.c_int, [_ctx, _dp]),
+    "fpsi_sa_get_system": (C.c_int, [_ctx, _dp, _dp, _dp]),
+    "fpsi_sa_solve": (C.c_int, [_ctx, _dp]),
+    "fpsi_sa_update": (C.c_int, [_ctx]),
     "fpsi_get_state": (C.c_int, [_ctx, _dp, _dp, _dp]),
     "fpsi_residual": (C.c_int, [_ctx, _dp, C.POINTER(Resid)]),
     "fpsi_get_reconstruction": (C.c_int, [_ctx, _dp, _dp]),

@@ -135,7 +135,8 @@ def sa_eddy_viscosity(nu_tilde, rho, mu):
 def boundary_layer_block(nx: int = 256, ny: int = 128, nz: int = 64, dy0: float = 1e-6,
                          growth: float = 1.15, seed: int = 0,
                          precision: str = "mixed", solver: str = "lsgs", viscous: int = 0,
-                         Re: float = 1e6, Lx: float = 1.0, Lz: float = 0.25) -> Case:
+                         Re: float = 1e6, Lx: float = 1.0, Lz: float = 0.25,
+                         sa: bool = False) -> Case:
     """Flat-plate block: x streamwise, y wall-normal (first spacing dy0,
     geometric growth), z spanwise periodic; wall at y = 0 (slip wall when
     inviscid, adiabatic no-slip wall otherwise), farfield at the top, inflow
@@ -143,7 +144,9 @@ def boundary_layer_block(nx: int = 256, ny: int = 128, nz: int = 64, dy0: float 
     density so that Re = rho U / mu(T) per unit length, inviscid ones use
     p = 1e5 Pa.  viscous: 0 inviscid, 1 laminar, 2 turbulent with the
     Spalart-Allmaras eddy viscosity of a frozen nu~ = 3 nu_inf field
-    (case.tmu).  The wall-normal columns are the LSGS lines (case.lines)."""
+    (case.tmu), or with sa=True the Spalart-Allmaras transport of nu~ from
+    nu~ = 3 nu_inf (case.nut0; inflow boundaries carry the same value).  The
+    wall-normal columns are the LSGS lines (case.lines)."""
     T0, M = 300.0, 0.3
     U0 = M * math.sqrt(GAMMA * RTILDE * T0)
     mu0 = float(sutherland_mu(T0))
@@ -153,13 +156,16 @@ def boundary_layer_block(nx: int = 256, ny: int = 128, nz: int = 64, dy0: float 
     else:
         p0 = 1e5
         rho0 = p0 / (RTILDE * T0)
-    ff = bc("farfield", T=T0, pg=p0, u=(U0, 0.0, 0.0))
+    nut_inf = 3.0 * mu0 / rho0
+    ff = bc("farfield", T=T0, pg=p0, u=(U0, 0.0, 0.0), nu_t=nut_inf if sa else 0.0)
     wl = bc("viscousWall" if viscous else "reflecting", T=T0, pg=p0)
     mesh = GeneratedMesh("bl", n=(nx, ny, nz), L=(Lx, 1.0, Lz), dy0=dy0, growth=growth,
                          bc_side=(0, 0, 1, 0, -1, -1), bcs=[ff, wl])
+    if sa and viscous != 2:
+        raise ValueError("the SA model needs viscous=2")
     params = default_params(flux="roe", limiter="venkatakrishnan", solver=solver,
                             gauss_seidel_iter=8, cflmax=50.0, precision=precision,
-                            viscous=viscous)
+                            viscous=viscous, turbulence=1 if sa else 0)
 
     def init(cc):
         nc = cc.shape[0]
@@ -173,10 +179,12 @@ def boundary_layer_block(nx: int = 256, ny: int = 128, nz: int = 64, dy0: float 
 
     c = Case(f"boundary_layer_{nx}x{ny}x{nz}", mesh, params, 100, init)
     c.lines = mesh.lines_along(1)
-    c.tmu = None
-    if viscous == 2:
-        nc = nx * ny * nz
-        c.tmu = np.full(nc, float(sa_eddy_viscosity(3.0 * mu0 / rho0, rho0, mu0)))
+    c.tmu = c.nut0 = None
+    nc = nx * ny * nz
+    if sa:
+        c.nut0 = np.full(nc, nut_inf)
+    elif viscous == 2:
+        c.tmu = np.full(nc, float(sa_eddy_viscosity(nut_inf, rho0, mu0)))
     return c
 
 

@@ -115,6 +115,38 @@ void free_lsgs(fpsi_ctx* x) {
 }
 
 // device arrays of the line solver for the current line layout and precision
+void free_sa(fpsi_ctx* x) {
+  double* ps[] = {x->d_nut, x->d_wdist, x->d_sa_grad, x->d_sa_phi, x->d_sa_nub,
+                  x->d_sa_face, x->d_sa_B, x->d_sa_D, x->d_sa_Dinv, x->d_sa_x};
+  for (double* p : ps)
+    if (p) cudaFree(p);
+  x->d_nut = x->d_wdist = x->d_sa_grad = x->d_sa_phi = x->d_sa_nub = nullptr;
+  x->d_sa_face = x->d_sa_B = x->d_sa_D = x->d_sa_Dinv = x->d_sa_x = nullptr;
+  x->have_sa = x->have_sa_dq = false;
+}
+
+// Spalart-Allmaras arrays, on first use of the model; nu~ starts at the
+// reference's nuTilde_ic default 1e-6 (SA_ic.loci:39-50)
+int alloc_sa(fpsi_ctx* x) {
+  if (!fpsi::sa_active(x) || x->d_nut) return FPSI_OK;
+  const int64_t nc = x->H.nc, nf = x->H.nf;
+  int rc;
+  if ((rc = dalloc(x, &x->d_nut, nc))) return rc;
+  if ((rc = dalloc(x, &x->d_wdist, nc))) return rc;
+  if ((rc = dalloc(x, &x->d_sa_grad, nc * 3))) return rc;
+  if ((rc = dalloc(x, &x->d_sa_phi, nc))) return rc;
+  if ((rc = dalloc(x, &x->d_sa_nub, std::max<int64_t>(x->H.nbf, 1)))) return rc;
+  if ((rc = dalloc(x, &x->d_sa_face, nf * 7))) return rc;
+  if ((rc = dalloc(x, &x->d_sa_B, nc))) return rc;
+  if ((rc = dalloc(x, &x->d_sa_D, nc))) return rc;
+  if ((rc = dalloc(x, &x->d_sa_Dinv, nc))) return rc;
+  if ((rc = dalloc(x, &x->d_sa_x, nc))) return rc;
+  std::vector<double> v(nc, 1e-6);
+  FPSI_CUDA_TRY(cudaMemcpy(x->d_nut, v.data(), nc * sizeof(double), cudaMemcpyHostToDevice));
+  FPSI_CUDA_TRY(cudaMemcpy(x->d_wdist, x->h_wdist.data(), nc * sizeof(double), cudaMemcpyHostToDevice));
+  return FPSI_OK;
+}
+
 int alloc_lsgs(fpsi_ctx* x) {
   if (x->P.solver != FPSI_SOLVER_LSGS) return FPSI_OK;
   int rc;
@@ -272,6 +304,7 @@ int fpsi_destroy(fpsi_ctx* x) {
   if (!x) return FPSI_OK;
   free_system(x);
   free_lsgs(x);
+  free_sa(x);
   void* ps[] = {x->d_cl, x->d_cr, x->d_n, x->d_area, x->d_rL, x->d_rR, x->d_vol, x->d_cc,
                 x->d_Minv, x->d_cf_off, x->d_cf, x->d_colour_cells, x->d_bcs, x->d_q,
                 x->d_qb, x->d_grad, x->d_phi, x->d_F, x->d_mev, x->d_src, x->d_dtau, x->d_tmu,
@@ -388,6 +421,8 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
   if (params->solver == FPSI_SOLVER_LSGS) x->keep_D = true;
   TRY(alloc_system(x));
   TRY(alloc_lsgs(x));
+  fpsi::wall_distance(mesh, x->H, x->h_wdist);
+  TRY(alloc_sa(x));
 #undef TRY
   *out = x;
   return FPSI_OK;
@@ -405,6 +440,8 @@ int fpsi_set_params(fpsi_ctx* x, const fpsi_params* p) {
   }
   rc = alloc_system(x);
   if (rc) return rc;
+  if ((rc = alloc_sa(x))) return rc;
+  x->have_sa = x->have_sa_dq = false;
   return alloc_lsgs(x);
 }
 
@@ -490,6 +527,101 @@ int fpsi_set_eddy_viscosity(fpsi_ctx* x, const double* tmu) {
   return FPSI_OK;
 }
 
+// ---- Spalart-Allmaras nu~ -------------------------------------------------
+static int sa_down(fpsi_ctx* x, const double* d, double* out) {
+  std::vector<double> h(x->H.nc);
+  FPSI_CUDA_TRY(cudaMemcpyAsync(h.data(), d, h.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                x->stream));
+  int rc = sync(x);
+  if (rc) return rc;
+  for (int64_t i = 0; i < x->H.nc; ++i) out[x->H.perm[i]] = h[i];
+  return FPSI_OK;
+}
+
+int fpsi_set_nutilde(fpsi_ctx* x, const double* nut) {
+  if (!x || !nut) return FPSI_E_INVALID;
+  if (!x->d_nut) return FPSI_E_STATE;
+  std::vector<double> t(x->H.nc);
+  for (int64_t i = 0; i < x->H.nc; ++i) t[i] = nut[x->H.perm[i]];
+  FPSI_CUDA_TRY(cudaMemcpy(x->d_nut, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice));
+  x->have_resid = x->have_asm = x->have_dq = x->have_sa = x->have_sa_dq = false;
+  return FPSI_OK;
+}
+
+int fpsi_get_nutilde(fpsi_ctx* x, double* nut) {
+  if (!x || !nut) return FPSI_E_INVALID;
+  if (!x->d_nut) return FPSI_E_STATE;
+  return sa_down(x, x->d_nut, nut);
+}
+
+int fpsi_get_eddy_viscosity(fpsi_ctx* x, double* tmu) {
+  if (!x || !tmu) return FPSI_E_INVALID;
+  return sa_down(x, x->d_tmu, tmu);
+}
+
+int fpsi_get_wall_distance(fpsi_ctx* x, double* d) {
+  if (!x || !d) return FPSI_E_INVALID;
+  for (int64_t i = 0; i < x->H.nc; ++i) d[x->H.perm[i]] = x->h_wdist[i];
+  return FPSI_OK;
+}
+
+int fpsi_sa_residual(fpsi_ctx* x, double* src) {
+  if (!x) return FPSI_E_INVALID;
+  if (!fpsi::sa_active(x)) return FPSI_E_STATE;
+  if (!x->have_resid) return FPSI_E_STATE;
+  int rc = fpsi::sa_launch_residual(x);
+  if (rc) return rc;
+  if (src) {
+    if ((rc = sa_down(x, x->d_sa_B, src))) return rc;
+  } else if ((rc = sync(x))) {
+    return rc;
+  }
+  x->have_sa = true;
+  x->have_sa_dq = false;
+  return FPSI_OK;
+}
+
+int fpsi_sa_get_system(fpsi_ctx* x, double* D, double* fjp, double* fjm) {
+  if (!x) return FPSI_E_INVALID;
+  if (!x->have_sa) return FPSI_E_STATE;
+  int rc;
+  if (D && (rc = sa_down(x, x->d_sa_D, D))) return rc;
+  const int64_t nf = x->H.nf;
+  for (int w = 0; w < 2; ++w) {
+    double* dst = w ? fjm : fjp;
+    if (!dst) continue;
+    std::vector<double> h(nf);
+    FPSI_CUDA_TRY(cudaMemcpy(h.data(), x->d_sa_face + (3 + w) * nf, nf * sizeof(double),
+                             cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < nf; ++i) dst[x->H.fperm[i]] = h[i];
+  }
+  return FPSI_OK;
+}
+
+int fpsi_sa_solve(fpsi_ctx* x, double* dq) {
+  if (!x) return FPSI_E_INVALID;
+  if (!x->have_sa) return FPSI_E_STATE;
+  int rc = fpsi::sa_launch_solve(x);
+  if (rc) return rc;
+  if (dq) {
+    if ((rc = sa_down(x, x->d_sa_x, dq))) return rc;
+  } else if ((rc = sync(x))) {
+    return rc;
+  }
+  x->have_sa_dq = true;
+  return FPSI_OK;
+}
+
+int fpsi_sa_update(fpsi_ctx* x) {
+  if (!x) return FPSI_E_INVALID;
+  if (!x->have_sa_dq) return FPSI_E_STATE;
+  int rc = fpsi::sa_launch_update(x);
+  if (rc) return rc;
+  if ((rc = sync(x))) return rc;
+  x->have_sa = x->have_sa_dq = false;
+  return FPSI_OK;
+}
+
 int fpsi_set_state(fpsi_ctx* x, const double* T, const double* pg, const double* u) {
   if (!x || !T || !pg || !u) return FPSI_E_INVALID;
   const int64_t nc = x->H.nc;
@@ -526,7 +658,10 @@ int fpsi_keep_blocks(fpsi_ctx* x, int32_t keep) {
 
 int fpsi_residual(fpsi_ctx* x, double* src, fpsi_resid* norms) {
   if (!x) return FPSI_E_INVALID;
-  int rc = fpsi::launch_residual(x, x->d_resid);
+  int rc;
+  x->have_sa = x->have_sa_dq = false;
+  if (fpsi::sa_active(x) && (rc = fpsi::sa_launch_tmu(x))) return rc;
+  rc = fpsi::launch_residual(x, x->d_resid);
   if (rc) return rc;
   FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid, x->d_resid, 8 * sizeof(double),
                                 cudaMemcpyDeviceToHost, x->stream));
@@ -804,7 +939,10 @@ int fpsi_update(fpsi_ctx* x, double* min_alpha) {
 int fpsi_newton_step(fpsi_ctx* x, fpsi_stepinfo* info) {
   if (!x) return FPSI_E_INVALID;
   int rc;
+  const bool sa = fpsi::sa_active(x);
+  if (sa && (rc = fpsi::sa_launch_tmu(x))) return rc;
   if ((rc = fpsi::launch_residual(x, x->d_resid))) return rc;
+  if (sa && ((rc = fpsi::sa_launch_residual(x)) || (rc = fpsi::sa_launch_solve(x)))) return rc;
   if ((rc = fpsi::launch_assemble(x))) return rc;
   if (is_lsgs(x)) {
     if ((rc = fpsi::lsgs_assemble(x))) return rc;
@@ -813,6 +951,7 @@ int fpsi_newton_step(fpsi_ctx* x, fpsi_stepinfo* info) {
     return rc;
   }
   if ((rc = fpsi::launch_update(x))) return rc;
+  if (sa && (rc = fpsi::sa_launch_update(x))) return rc;
   FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid, x->d_resid, 8 * sizeof(double),
                                 cudaMemcpyDeviceToHost, x->stream));
   std::vector<double> a(x->nblk_norm);
@@ -829,17 +968,16 @@ int fpsi_newton_step(fpsi_ctx* x, fpsi_stepinfo* info) {
   return has_nan(x->h_resid) ? FPSI_E_NAN : FPSI_OK;
 }
 
-int fpsi_run(fpsi_ctx* x, int32_t nsteps, fpsi_resid* norms) {
-  if (!x || nsteps < 0) return FPSI_E_INVALID;
-  if (nsteps == 0) return FPSI_OK;
-  double* hist = nullptr;
-  if (cudaMalloc((void**)&hist, size_t(nsteps) * 8 * sizeof(double)) != cudaSuccess) {
-    fpsi::set_error("cudaMalloc of the residual history failed");
-    return FPSI_E_NOMEM;
-  }
+// nsteps implicit steps on the stream; with the SA model nu~ is advanced in
+// each step from the same residual state, after the mean flow's solve
+static int run_steps(fpsi_ctx* x, int32_t nsteps, double* hist) {
   int rc = FPSI_OK;
+  const bool sa = fpsi::sa_active(x);
   for (int32_t s = 0; s < nsteps && !rc; ++s) {
-    rc = fpsi::launch_residual(x, hist + 8 * s);
+    if (sa) rc = fpsi::sa_launch_tmu(x);
+    if (!rc) rc = fpsi::launch_residual(x, hist + 8 * s);
+    if (!rc && sa) rc = fpsi::sa_launch_residual(x);
+    if (!rc && sa) rc = fpsi::sa_launch_solve(x);
     if (!rc) rc = fpsi::launch_assemble(x);
     if (!rc && is_lsgs(x)) {
       rc = fpsi::lsgs_assemble(x);
@@ -848,7 +986,21 @@ int fpsi_run(fpsi_ctx* x, int32_t nsteps, fpsi_resid* norms) {
       rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter);
     }
     if (!rc) rc = fpsi::launch_update(x);
+    if (!rc && sa) rc = fpsi::sa_launch_update(x);
   }
+  x->have_sa = x->have_sa_dq = false;
+  return rc;
+}
+
+int fpsi_run(fpsi_ctx* x, int32_t nsteps, fpsi_resid* norms) {
+  if (!x || nsteps < 0) return FPSI_E_INVALID;
+  if (nsteps == 0) return FPSI_OK;
+  double* hist = nullptr;
+  if (cudaMalloc((void**)&hist, size_t(nsteps) * 8 * sizeof(double)) != cudaSuccess) {
+    fpsi::set_error("cudaMalloc of the residual history failed");
+    return FPSI_E_NOMEM;
+  }
+  int rc = run_steps(x, nsteps, hist);
   std::vector<double> h(size_t(nsteps) * 8);
   if (!rc && cudaMemcpyAsync(h.data(), hist, h.size() * sizeof(double), cudaMemcpyDeviceToHost,
                              x->stream) != cudaSuccess)
@@ -863,22 +1015,6 @@ int fpsi_run(fpsi_ctx* x, int32_t nsteps, fpsi_resid* norms) {
     nan = nan || has_nan(&h[8 * s]);
   }
   return nan ? FPSI_E_NAN : FPSI_OK;
-}
-
-static int run_steps(fpsi_ctx* x, int32_t nsteps, double* hist) {
-  int rc = FPSI_OK;
-  for (int32_t s = 0; s < nsteps && !rc; ++s) {
-    rc = fpsi::launch_residual(x, hist + 8 * s);
-    if (!rc) rc = fpsi::launch_assemble(x);
-    if (!rc && is_lsgs(x)) {
-      rc = fpsi::lsgs_assemble(x);
-      if (!rc) rc = fpsi::lsgs_solve(x, true);
-    } else if (!rc) {
-      rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter);
-    }
-    if (!rc) rc = fpsi::launch_update(x);
-  }
-  return rc;
 }
 
 int fpsi_run_timed(fpsi_ctx* x, int32_t nsteps, fpsi_resid* norms, double* device_ms) {

@@ -159,6 +159,12 @@ struct fpsi_ctx {
   // start has used this context: the next system's start uses it as input
   void* d_xprev = nullptr;     // nc * 5 * 8 bytes
   bool keep_prev = false, have_xprev = false;
+  // Spalart-Allmaras working variable (RCM order) and its scalar system
+  std::vector<double> h_wdist;   // wall distance, RCM order
+  double *d_nut = nullptr, *d_wdist = nullptr, *d_sa_grad = nullptr, *d_sa_phi = nullptr;
+  double *d_sa_nub = nullptr, *d_sa_face = nullptr;  // [nbf], [7][nf]
+  double *d_sa_B = nullptr, *d_sa_D = nullptr, *d_sa_Dinv = nullptr, *d_sa_x = nullptr;
+  bool have_sa = false, have_sa_dq = false;
   int64_t device_bytes = 0;
   // caller-order staging for state transfers (T, pg, u) and the permutation
   int32_t* d_perm = nullptr;   // new cell id -> caller cell id
@@ -188,4 +194,12 @@ void prof_end(fpsi_ctx* x);
 int build_lines(fpsi_ctx* x, const std::vector<std::vector<int32_t>>* lines);
 int lsgs_assemble(fpsi_ctx* x);
 int lsgs_solve(fpsi_ctx* x, bool jacobi_start);
+// distance to the nearest no-slip wall per cell (RCM order)
+void wall_distance(const fpsi_mesh* m, const HostMesh& H, std::vector<double>& out);
+// Spalart-Allmaras nu~ (sa.cu)
+bool sa_active(const fpsi_ctx* x);
+int sa_launch_tmu(fpsi_ctx* x);
+int sa_launch_residual(fpsi_ctx* x);
+int sa_launch_solve(fpsi_ctx* x);
+int sa_launch_update(fpsi_ctx* x);
 }  // namespace fpsi

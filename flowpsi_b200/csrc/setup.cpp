@@ -420,4 +420,137 @@ int build_host_mesh(const fpsi_mesh* m, HostMesh& h) {
   return FPSI_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// distance to the nearest no-slip wall (find_mind, gridSetup.loci:418-640;
+// dist_noslip, solverTurbulence.loci:133-137): the wall face is chosen by the
+// distance between its edge-length weighted centre and the cell's area
+// weighted face-centre average (ties: lowest face), the distance is
+// |(x_f - x_c).n| with the finite-volume centres.  k-d tree over the wall
+// faces.  Result in the context's (RCM) cell order; 1e30 without walls.
+// ---------------------------------------------------------------------------
+namespace {
+struct WallTree {
+  std::vector<double> p;     // 3 per wall face (search centres)
+  std::vector<int64_t> id;   // caller face id
+  std::vector<int32_t> ord;  // tree order: node k = ord[k]
+  std::vector<int8_t> axis;  // per tree position
+  void build(int64_t lo, int64_t hi) {
+    if (hi - lo <= 0) return;
+    double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+    for (int64_t k = lo; k < hi; ++k)
+      for (int d = 0; d < 3; ++d) {
+        mn[d] = std::min(mn[d], p[3 * ord[k] + d]);
+        mx[d] = std::max(mx[d], p[3 * ord[k] + d]);
+      }
+    int ax = 0;
+    for (int d = 1; d < 3; ++d)
+      if (mx[d] - mn[d] > mx[ax] - mn[ax]) ax = d;
+    const int64_t mid = lo + (hi - lo) / 2;
+    std::nth_element(ord.begin() + lo, ord.begin() + mid, ord.begin() + hi, [&](int32_t a, int32_t b) {
+      const double va = p[3 * a + ax], vb = p[3 * b + ax];
+      return va < vb || (va == vb && id[a] < id[b]);
+    });
+    axis[mid] = int8_t(ax);
+    build(lo, mid);
+    build(mid + 1, hi);
+  }
+  void query(int64_t lo, int64_t hi, const double q[3], double& bd, int64_t& bid, int32_t& bk) const {
+    if (hi - lo <= 0) return;
+    const int64_t mid = lo + (hi - lo) / 2;
+    const int32_t k = ord[mid];
+    double d2 = 0;
+    for (int d = 0; d < 3; ++d) {
+      const double t = p[3 * k + d] - q[d];
+      d2 += t * t;
+    }
+    if (d2 < bd || (d2 == bd && id[k] < bid)) bd = d2, bid = id[k], bk = k;
+    const int ax = axis[mid];
+    const double diff = q[ax] - p[3 * k + ax];
+    const bool left_first = diff <= 0;
+    if (left_first) {
+      query(lo, mid, q, bd, bid, bk);
+      if (diff * diff <= bd) query(mid + 1, hi, q, bd, bid, bk);
+    } else {
+      query(mid + 1, hi, q, bd, bid, bk);
+      if (diff * diff <= bd) query(lo, mid, q, bd, bid, bk);
+    }
+  }
+};
+}  // namespace
+
+void wall_distance(const fpsi_mesh* m, const HostMesh& H, std::vector<double>& out) {
+  const int64_t nc = m->ncells, nf = m->nfaces;
+  out.assign(nc, 1e30);
+  std::vector<int64_t> walls;
+  for (int64_t f = 0; f < nf; ++f)
+    if (m->cr[f] < 0 && m->bcs[-m->cr[f] - 1].kind == FPSI_BC_VISCOUS_WALL) walls.push_back(f);
+  if (walls.empty()) return;
+  // search centres (caller numbering)
+  std::vector<double> fce(nf * 3), fa(nf);
+  for (int64_t f = 0; f < nf; ++f) {
+    const int64_t a = m->face_off[f], b = m->face_off[f + 1];
+    const int n = int(b - a);
+    double ns[3] = {0, 0, 0}, ls = 0;
+    for (int i = 0; i < n; ++i) {
+      const double* p1 = m->xyz + 3 * int64_t(m->face_nodes[a + i]);
+      const double* p2 = m->xyz + 3 * int64_t(m->face_nodes[a + (i + 1) % n]);
+      const double len = std::sqrt((p1[0] - p2[0]) * (p1[0] - p2[0]) + (p1[1] - p2[1]) * (p1[1] - p2[1]) +
+                                   (p1[2] - p2[2]) * (p1[2] - p2[2]));
+      for (int d = 0; d < 3; ++d) ns[d] += len * (0.5 * (p1[d] + p2[d]));
+      ls += len;
+    }
+    double c[3];
+    for (int d = 0; d < 3; ++d) c[d] = (1.0 / ls) * ns[d];
+    double sx = 0, sy = 0, sz = 0;
+    for (int i = 0; i < n; ++i) {
+      const double* p1 = m->xyz + 3 * int64_t(m->face_nodes[a + i]);
+      const double* p2 = m->xyz + 3 * int64_t(m->face_nodes[a + (i + 1) % n]);
+      const double u0 = p1[0] - c[0], u1 = p1[1] - c[1], u2 = p1[2] - c[2];
+      const double v0 = p2[0] - c[0], v1 = p2[1] - c[1], v2 = p2[2] - c[2];
+      sx += u1 * v2 - u2 * v1, sy += u2 * v0 - u0 * v2, sz += u0 * v1 - u1 * v0;
+    }
+    for (int d = 0; d < 3; ++d) fce[3 * f + d] = c[d];
+    fa[f] = 0.5 * std::sqrt(sx * sx + sy * sy + sz * sz);
+  }
+  std::vector<double> csum(nc * 3, 0.0), asum(nc, 0.0);
+  for (int64_t f = 0; f < nf; ++f)
+    for (int side = 0; side < 2; ++side) {
+      const int64_t c = side ? m->cr[f] : m->cl[f];
+      if (c < 0) continue;
+      for (int d = 0; d < 3; ++d) csum[3 * c + d] += fce[3 * f + d] * fa[f];
+      asum[c] += fa[f];
+    }
+  WallTree T;
+  const int64_t nw = int64_t(walls.size());
+  T.p.resize(3 * nw);
+  T.id.resize(nw);
+  T.ord.resize(nw);
+  T.axis.assign(nw, 0);
+  for (int64_t k = 0; k < nw; ++k) {
+    for (int d = 0; d < 3; ++d) T.p[3 * k + d] = fce[3 * walls[k] + d];
+    T.id[k] = walls[k];
+    T.ord[k] = int32_t(k);
+  }
+  T.build(0, nw);
+  std::vector<double> cc_caller(nc * 3);
+  for (int64_t i = 0; i < nc; ++i)
+    for (int d = 0; d < 3; ++d) cc_caller[3 * H.perm[i] + d] = H.cc[3 * i + d];
+  std::vector<double> dc(nc);
+  for (int64_t c = 0; c < nc; ++c) {
+    double q[3];
+    for (int d = 0; d < 3; ++d) q[d] = (1.0 / asum[c]) * csum[3 * c + d];
+    double bd = 1e300;
+    int64_t bid = -1;
+    int32_t bk = -1;
+    T.query(0, nw, q, bd, bid, bk);
+    const int64_t w = bid;
+    double dot = 0;
+    for (int d = 0; d < 3; ++d)
+      dot += (H.fc_caller[3 * w + d] - cc_caller[3 * c + d]) * (H.an_caller[3 * w + d] / H.area_caller[w]);
+    dc[c] = std::fabs(dot);
+  }
+  for (int64_t i = 0; i < nc; ++i) out[i] = dc[H.perm[i]];
+}
+
 }  // namespace fpsi

@@ -39,10 +39,12 @@ def default_params(**kw) -> N.Params:
     return p
 
 
-def bc(kind: str, T: float = 300.0, pg: float = 1e5, u=(0.0, 0.0, 0.0)) -> N.BCSpec:
+def bc(kind: str, T: float = 300.0, pg: float = 1e5, u=(0.0, 0.0, 0.0),
+       nu_t: float = 0.0) -> N.BCSpec:
+    """boundary condition; nu_t: SA nu~ entering through it (<= 0: 5e-9)"""
     b = N.BCSpec()
     b.kind = N.BC[kind]
-    b.T, b.pg = T, pg
+    b.T, b.pg, b.nu_t = T, pg, nu_t
     for i in range(3):
         b.u[i] = u[i]
     return b
@@ -219,6 +221,44 @@ class FlowPsi:
         t = np.ascontiguousarray(tmu, np.float64)
         assert t.size == self.ncells
         N.check(N.lib().fpsi_set_eddy_viscosity(self._ctx, N.dptr(t)), "fpsi_set_eddy_viscosity")
+
+    # -- Spalart-Allmaras nu~ (turbulence/SA/SA_turb.loci) -------------------
+    def set_nutilde(self, nut) -> None:
+        """the SA working variable nu~ per cell (caller order)"""
+        v = np.ascontiguousarray(nut, np.float64)
+        assert v.size == self.ncells
+        N.check(N.lib().fpsi_set_nutilde(self._ctx, N.dptr(v)), "fpsi_set_nutilde")
+
+    def _cells(self, fn, name):
+        v = np.empty(self.ncells)
+        N.check(fn(self._ctx, N.dptr(v)), name)
+        return v
+
+    def nutilde(self) -> np.ndarray:
+        return self._cells(N.lib().fpsi_get_nutilde, "fpsi_get_nutilde")
+
+    def eddy_viscosity(self) -> np.ndarray:
+        return self._cells(N.lib().fpsi_get_eddy_viscosity, "fpsi_get_eddy_viscosity")
+
+    def wall_distance(self) -> np.ndarray:
+        """dist_noslip (solverTurbulence.loci:133-137)"""
+        return self._cells(N.lib().fpsi_get_wall_distance, "fpsi_get_wall_distance")
+
+    def sa_residual(self) -> np.ndarray:
+        """nuTilde_src, the scalar right-hand side (after residual())"""
+        return self._cells(N.lib().fpsi_sa_residual, "fpsi_sa_residual")
+
+    def sa_system(self) -> dict:
+        D, fjp, fjm = np.empty(self.ncells), np.empty(self.nfaces), np.empty(self.nfaces)
+        N.check(N.lib().fpsi_sa_get_system(self._ctx, N.dptr(D), N.dptr(fjp), N.dptr(fjm)),
+                "fpsi_sa_get_system")
+        return {"D": D, "fjp": fjp, "fjm": fjm}
+
+    def sa_solve(self) -> np.ndarray:
+        return self._cells(N.lib().fpsi_sa_solve, "fpsi_sa_solve")
+
+    def sa_update(self) -> None:
+        N.check(N.lib().fpsi_sa_update(self._ctx), "fpsi_sa_update")
 
     def get_state(self, out=None):
         """(T, pg, u) in caller order; `out` = caller arrays (float64,

@@ -69,6 +69,10 @@ enum fpsi_precision {
   FPSI_PREC_REF = 1,           /* reference precision: FP32 blocks and B, FP64 iterate */
   FPSI_PREC_MIXED = 2          /* FP32 blocks, LU and sweeps (defect correction) */
 };
+enum fpsi_turbulence_kind {
+  FPSI_TURB_EDDY_VISCOSITY = 0,    /* tmu given by fpsi_set_eddy_viscosity */
+  FPSI_TURB_SA = 1                 /* Spalart-Allmaras nu~ transport, turbulence/SA/SA_turb.loci */
+};
 enum fpsi_bc_kind {
   FPSI_BC_FARFIELD = 1,            /* bcInflow.loci:311-375 */
   FPSI_BC_SUPERSONIC_INFLOW = 2,   /* bcInflow.loci:270-309 */
@@ -96,9 +100,9 @@ typedef struct fpsi_params {
   double lsgs_rel_tol;     /* 0.1 */
   int32_t lsgs_max_iter;   /* 10 */
   int32_t precision;       /* fpsi_precision, default FPSI_PREC_REF */
-  int32_t viscous;         /* flowRegime: 0 inviscid, 1 laminar, 2 turbulent (eddy viscosity
-                              from fpsi_set_eddy_viscosity)      fluxViscous.loci:28-52 */
-  int32_t reserved0;
+  int32_t viscous;         /* flowRegime: 0 inviscid, 1 laminar, 2 turbulent
+                                                                   fluxViscous.loci:28-52 */
+  int32_t turbulence;      /* fpsi_turbulence_kind (viscous == 2): where tmu comes from */
   double Prt;              /* turbulentPrandtlNumber 0.9           fluxViscous.loci:268-270 */
   double mu_a1, mu_a2, mu_a3; /* Sutherland mu = a1 T^a2/(T+a3): 1.458e-6, 1.5, 110.4 */
   double k_a1, k_a2, k_a3;    /* conductivity k = k1 T^k2/(T+k3): 2.495e-3, 1.5, 194
@@ -109,6 +113,8 @@ typedef struct fpsi_bc {
   int32_t kind;            /* fpsi_bc_kind */
   int32_t reserved;
   double T, pg, u[3];      /* reference state (temperatureRef, gagePressureRef, uRef) */
+  double nu_t;             /* SA nu~ entering through the boundary (BC option nu_t,
+                              SA_turb.loci:167-179); <= 0 selects the default 5e-9 */
 } fpsi_bc;
 
 /* Unstructured mesh in the caller's numbering.  Face nodes are ordered so
@@ -306,6 +312,32 @@ int fpsi_gnn_train(fpsi_gnn* m, int32_t nsteps, int64_t batch, uint64_t seed, do
 /* learned start for ctx's assembled system: the next fpsi_linear_solve(ctx,
  * NULL, ...) or fpsi_linear_sweeps starts from it; x0 (caller order) optional */
 int fpsi_gnn_predict(fpsi_gnn* m, fpsi_ctx* ctx, double* x0);
+
+/* ---- Spalart-Allmaras turbulence model ----------------------------------
+ * With params.viscous = 2 and params.turbulence = FPSI_TURB_SA the context
+ * owns the working variable nu~ (nuTilde; baseline model, standard
+ * production, SA_turb.loci:85-476).  fpsi_residual first sets the eddy
+ * viscosity tmu = rho nu~ f_v1 (:105-107) from it.  fpsi_newton_step and
+ * fpsi_run advance nu~ once per step, segregated from the mean flow as the
+ * reference's scalar transport (solverScalarTransport.loci:36-700): upwind
+ * convection by the mean flow's mass flux, production, destruction and
+ * diffusion, the steady pseudo-time term with the mean flow's dtau, scalar
+ * multi-colour SGS (linearSolverSGS.loci:333-470) and the relaxed positive
+ * update (:397-405).  The wall distance is the distance from the cell centre
+ * to the plane of the nearest no-slip wall face (gridSetup.loci:418-640,
+ * solverTurbulence.loci:133-137); without walls it is 1e30. */
+int fpsi_set_nutilde(fpsi_ctx* ctx, const double* nut);      /* caller order, nc */
+int fpsi_get_nutilde(fpsi_ctx* ctx, double* nut);
+int fpsi_get_eddy_viscosity(fpsi_ctx* ctx, double* tmu);     /* as last used */
+int fpsi_get_wall_distance(fpsi_ctx* ctx, double* dist);
+/* after fpsi_residual: nuTilde_src (the scalar right-hand side), optional */
+int fpsi_sa_residual(fpsi_ctx* ctx, double* src);
+/* scalar system of the last fpsi_sa_residual: X_D (nc), X_fjp and X_fjm
+ * (nf; L = -fjp, U = fjm), any may be NULL; caller order */
+int fpsi_sa_get_system(fpsi_ctx* ctx, double* D, double* fjp, double* fjm);
+/* Jacobi start and gauss_seidel_iter symmetric sweeps; dq optional */
+int fpsi_sa_solve(fpsi_ctx* ctx, double* dq);
+int fpsi_sa_update(fpsi_ctx* ctx);
 
 /* ---- residual norms without allocation -----------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc

@@ -486,6 +486,13 @@ struct orc_ctx {
   std::vector<double> fjp64, fjm64, D64, LU64, B64;
   std::vector<int> piv;                 // nc*5
   std::vector<double> dq;               // nc*5 (FP64 copy of the result)
+  // Spalart-Allmaras working variable and its scalar system
+  std::vector<double> nut, wdist;       // nc
+  std::vector<double> sa_grad, sa_phi;  // nc*3, nc
+  std::vector<double> sa_src, sa_D;     // nc
+  std::vector<double> sa_fjp, sa_fjm;   // nf
+  std::vector<double> sa_dq;            // nc
+  bool have_sa = false, have_sa_dq = false;
 };
 
 static int g_threads = 1;
@@ -600,6 +607,9 @@ static void compute_geometry(orc_ctx* o, const fpsi_mesh* m) {
   }
 }
 
+static void wall_distance(orc_ctx* o, const fpsi_mesh* m);
+static void sa_tmu(orc_ctx* o);
+
 extern "C" int orc_create(orc_ctx** out, const fpsi_mesh* m, const fpsi_params* p) {
   if (!out || !m || !p) return FPSI_E_INVALID;
   orc_ctx* o = new orc_ctx();
@@ -673,6 +683,8 @@ extern "C" int orc_create(orc_ctx** out, const fpsi_mesh* m, const fpsi_params* 
   o->pg.assign(nc, 0);
   o->u.assign(nc * 3, 0);
   o->tmu.assign(nc, 0);
+  o->nut.assign(nc, 1e-6);  // nuTilde_ic default (SA_ic.loci:39-50)
+  wall_distance(o, m);
   *out = o;
   return FPSI_OK;
 }
@@ -1020,6 +1032,8 @@ extern "C" int orc_residual(orc_ctx* o, double* src_out, fpsi_resid* norms) {
   const int64_t nc = o->nc, nf = o->nf;
   const fpsi_params& P = o->P;
   if (P.Minf < 0.5) return FPSI_E_UNSUPPORTED;
+  if (P.viscous == 2 && P.turbulence == FPSI_TURB_SA) sa_tmu(o);
+  o->have_sa = o->have_sa_dq = false;
   o->qb.assign(nf * 5, 0);
   for (int64_t f = 0; f < nf; ++f)
     if (o->cr[f] < 0) bc_face_state(o, f, &o->qb[5 * f]);
@@ -1657,6 +1671,12 @@ extern "C" int orc_update(orc_ctx* o, double* min_alpha) {
   return FPSI_OK;
 }
 
+extern "C" int orc_sa_residual(orc_ctx* o, double* src_out);
+extern "C" int orc_sa_solve(orc_ctx* o, const int32_t* colour, double* dq);
+extern "C" int orc_sa_update(orc_ctx* o);
+
+// one implicit step; with the SA model the nu~ system is built from the same
+// residual state and its update applied after the mean flow's
 extern "C" int orc_newton_step(orc_ctx* o, const int32_t* colour, fpsi_stepinfo* info) {
   fpsi_stepinfo si;
   std::memset(&si, 0, sizeof(si));
@@ -1664,11 +1684,17 @@ extern "C" int orc_newton_step(orc_ctx* o, const int32_t* colour, fpsi_stepinfo*
   if (rc) return rc;
   si.dtau_min = *std::min_element(o->dtau.begin(), o->dtau.end());
   si.dtau_max = *std::max_element(o->dtau.begin(), o->dtau.end());
+  const bool sa = o->P.viscous == 2 && o->P.turbulence == FPSI_TURB_SA;
+  if (sa) {
+    if ((rc = orc_sa_residual(o, nullptr))) return rc;
+    if ((rc = orc_sa_solve(o, colour, nullptr))) return rc;
+  }
   rc = orc_assemble(o);
   if (rc) return rc;
   rc = orc_linear_solve(o, colour, nullptr, nullptr, &si.ls);
   if (rc) return rc;
   rc = orc_update(o, &si.min_alpha);
+  if (!rc && sa) rc = orc_sa_update(o);
   if (info) *info = si;
   return rc;
 }
@@ -1729,5 +1755,411 @@ extern "C" int orc_cv_state(int32_t outflow, int64_t n, const double* qi, const 
     double* o = out + 5 * i;
     o[0] = pgb, o[1] = Tb, o[2] = ub.x, o[3] = ub.y, o[4] = ub.z;
   }
+  return FPSI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Spalart-Allmaras nu~ transport (turbulence/SA/SA_turb.loci, baseline model,
+// standard production) in the reference's scalar transport
+// (solverScalarTransport.loci), steady pseudo time, one Newton iteration per
+// step.
+// ---------------------------------------------------------------------------
+namespace {
+struct SAConst {  // Spa_All_param, SA_param.h:28-40
+  double cb1 = 0.1355, k = 0.41, cv1 = 7.1, cb2 = 0.622, cw2 = 0.3, cw3 = 2.0, sigma = 2. / 3.;
+};
+constexpr double SA_FACTORX = 2, SA_FACTORY = .5;  // SA_turb.loci:426-427
+}  // namespace
+
+// Nearest no-slip wall face by its edge-weighted centre from each cell's
+// area-weighted face-centre average (find_mind, gridSetup.loci:418-640; ties:
+// lowest face), then |(x_f - x_c).n| with the finite-volume centres
+// (dist_noslip, solverTurbulence.loci:133-137).  No walls: 1e30.
+static void wall_distance(orc_ctx* o, const fpsi_mesh* m) {
+  const int64_t nc = o->nc, nf = o->nf;
+  o->wdist.assign(nc, 1e30);
+  std::vector<int64_t> walls;
+  for (int64_t f = 0; f < nf; ++f)
+    if (o->cr[f] < 0 && o->bcs[-o->cr[f] - 1].kind == FPSI_BC_VISCOUS_WALL) walls.push_back(f);
+  if (walls.empty()) return;
+  std::vector<double> fce(nf * 3), fa(nf);
+  for (int64_t f = 0; f < nf; ++f) {
+    const int64_t a = m->face_off[f], b = m->face_off[f + 1];
+    const int n = int(b - a);
+    V3 ns = mk(0, 0, 0);
+    double ls = 0;
+    for (int i = 0; i < n; ++i) {
+      V3 p1 = v3(&m->xyz[3 * int64_t(m->face_nodes[a + i])]);
+      V3 p2 = v3(&m->xyz[3 * int64_t(m->face_nodes[a + (i + 1) % n])]);
+      const double len = norm(p1 - p2);
+      ns = ns + len * (0.5 * (p1 + p2));
+      ls += len;
+    }
+    V3 c = (1.0 / ls) * ns;
+    V3 s = mk(0, 0, 0);
+    for (int i = 0; i < n; ++i) {
+      V3 p1 = v3(&m->xyz[3 * int64_t(m->face_nodes[a + i])]);
+      V3 p2 = v3(&m->xyz[3 * int64_t(m->face_nodes[a + (i + 1) % n])]);
+      s = s + cross(p1 - c, p2 - c);
+    }
+    fce[3 * f] = c.x, fce[3 * f + 1] = c.y, fce[3 * f + 2] = c.z;
+    fa[f] = 0.5 * norm(s);
+  }
+  std::vector<double> csum(nc * 3, 0), asum(nc, 0);
+  for (int64_t f = 0; f < nf; ++f) {
+    for (int side = 0; side < 2; ++side) {
+      const int64_t c = side ? o->cr[f] : o->cl[f];
+      if (c < 0) continue;
+      for (int k = 0; k < 3; ++k) csum[3 * c + k] += fce[3 * f + k] * fa[f];
+      asum[c] += fa[f];
+    }
+  }
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < nc; ++c) {
+    const V3 p = (1.0 / asum[c]) * v3(&csum[3 * c]);
+    double best = 1e300;
+    int64_t bf = -1;
+    for (int64_t w : walls) {
+      const V3 d = v3(&fce[3 * w]) - p;
+      const double d2 = dot(d, d);
+      if (d2 < best) best = d2, bf = w;
+    }
+    const V3 dist = v3(&o->fc[3 * bf]) - v3(&o->cc[3 * c]);
+    o->wdist[c] = std::fabs(dot(dist, v3(&o->an[3 * bf])));
+  }
+}
+
+static inline double sa_rho(const orc_ctx* o, int64_t c) {
+  return (o->pg[c] + o->P.Pambient) / (o->P.Rtilde * o->T[c]);
+}
+static inline double sa_mu(const orc_ctx* o, int64_t c) {
+  return suth(o->T[c], o->P.mu_a1, o->P.mu_a2, o->P.mu_a3);
+}
+
+// tmu = nu~ f_v1 rho (SA_turb.loci:91-107)
+static void sa_tmu(orc_ctx* o) {
+  const SAConst S;
+  for (int64_t c = 0; c < o->nc; ++c) {
+    const double rho = sa_rho(o, c), mu = sa_mu(o, c);
+    const double x = rho * o->nut[c] / mu;
+    const double fv1 = std::pow(x, 3) / (std::pow(x, 3) + std::pow(S.cv1, 3));
+    o->tmu[c] = o->nut[c] * fv1 * rho;
+  }
+}
+
+// nu~ on a boundary face: 0 on no-slip walls (:181-183), the inside value
+// where the face velocity leaves or on symmetry planes, else the boundary's
+// nu_t (solverScalarTransport.loci:423-466, SA_turb.loci:167-179)
+static double sa_face_bc(const orc_ctx* o, int64_t f) {
+  const fpsi_bc& bc = o->bcs[-o->cr[f] - 1];
+  const int64_t a = o->cl[f];
+  if (bc.kind == FPSI_BC_VISCOUS_WALL) return 0.0;
+  if (bc.kind == FPSI_BC_REFLECTING) return o->nut[a];
+  const double* qf = &o->qb[5 * f];
+  const double uit = o->an[3 * f] * qf[1] + o->an[3 * f + 1] * qf[2] + o->an[3 * f + 2] * qf[3];
+  if (uit >= -0.0) return o->nut[a];
+  return bc.nu_t > 0 ? bc.nu_t : 5e-9;
+}
+
+extern "C" int orc_set_nutilde(orc_ctx* o, const double* nut) {
+  std::memcpy(o->nut.data(), nut, sizeof(double) * o->nc);
+  o->have_resid = o->have_asm = o->have_dq = o->have_sa = o->have_sa_dq = false;
+  return FPSI_OK;
+}
+extern "C" int orc_get_nutilde(orc_ctx* o, double* nut) {
+  std::memcpy(nut, o->nut.data(), sizeof(double) * o->nc);
+  return FPSI_OK;
+}
+extern "C" int orc_get_eddy_viscosity(orc_ctx* o, double* tmu) {
+  std::memcpy(tmu, o->tmu.data(), sizeof(double) * o->nc);
+  return FPSI_OK;
+}
+extern "C" int orc_get_wall_distance(orc_ctx* o, double* d) {
+  std::memcpy(d, o->wdist.data(), sizeof(double) * o->nc);
+  return FPSI_OK;
+}
+
+// SA sources, convection, diffusion and their Jacobians into X_src, X_D,
+// X_fjp, X_fjm (SA_turb.loci:85-476, solverScalarTransport.loci:457-700)
+extern "C" int orc_sa_residual(orc_ctx* o, double* src_out) {
+  if (!o->have_resid) return FPSI_E_STATE;
+  const fpsi_params& P = o->P;
+  if (!(P.viscous == 2 && P.turbulence == FPSI_TURB_SA)) return FPSI_E_STATE;
+  const SAConst S;
+  const int64_t nc = o->nc, nf = o->nf;
+  // gradient and limiter of nu~, boundary values at the boundary faces
+  std::vector<double> nub(nf, 0.0);
+  for (int64_t f = 0; f < nf; ++f)
+    if (o->cr[f] < 0) nub[f] = sa_face_bc(o, f);
+  o->sa_grad.assign(nc * 3, 0);
+  o->sa_phi.assign(nc, 1.0);
+  const int lim = P.limiter;
+  for (int64_t c = 0; c < nc; ++c) {
+    const double xc = o->nut[c];
+    double b[3] = {0, 0, 0}, xmax = xc, xmin = xc;
+    auto nb = [&](V3 d, double xn) {
+      const double dx = xn - xc;
+      b[0] += d.x * dx, b[1] += d.y * dx, b[2] += d.z * dx;
+      xmax = std::max(xmax, xn), xmin = std::min(xmin, xn);
+    };
+    for (int64_t k = o->up_off[c]; k < o->up_off[c + 1]; ++k) {
+      const int64_t f = o->up[k];
+      nb(v3(&o->rL[3 * f]) - v3(&o->rR[3 * f]), o->nut[o->cr[f]]);
+    }
+    for (int64_t k = o->lo_off[c]; k < o->lo_off[c + 1]; ++k) {
+      const int64_t f = o->lo[k];
+      nb(v3(&o->rR[3 * f]) - v3(&o->rL[3 * f]), o->nut[o->cl[f]]);
+    }
+    for (int64_t k = o->bd_off[c]; k < o->bd_off[c + 1]; ++k) {
+      const int64_t f = o->bd[k];
+      nb(v3(&o->rL[3 * f]), nub[f]);
+    }
+    const double* mi = &o->Minv[6 * c];
+    double* g = &o->sa_grad[3 * c];
+    g[0] = mi[0] * b[0] + mi[1] * b[1] + mi[2] * b[2];
+    g[1] = mi[1] * b[0] + mi[3] * b[1] + mi[4] * b[2];
+    g[2] = mi[2] * b[0] + mi[4] * b[1] + mi[5] * b[2];
+    double ph = lim == FPSI_LIMITER_ZERO ? 0.0 : 1.0;
+    if (lim == FPSI_LIMITER_VENKATAKRISHNAN || lim == FPSI_LIMITER_BARTH) {
+      const double h = std::cbrt(o->vol[c]);
+      const double kh = P.Kl * h, eps2 = kh * kh * kh;
+      auto side = [&](V3 r) {
+        const double d2 = g[0] * r.x + g[1] * r.y + g[2] * r.z;
+        double p = 1.0;
+        if (d2 != 0.0) {
+          const double d1 = d2 > 0 ? xmax - xc : xmin - xc;
+          if (lim == FPSI_LIMITER_BARTH) {
+            p = std::min(1.0, d1 / d2);
+          } else {
+            const double num = (d1 * d1 + eps2) + 2.0 * d2 * d1;
+            const double den = d1 * d1 + 2.0 * d2 * d2 + d1 * d2 + eps2;
+            p = std::min(1.0, num / den);
+          }
+        }
+        ph = std::min(ph, p);
+      };
+      for (int64_t k = o->up_off[c]; k < o->up_off[c + 1]; ++k) side(v3(&o->rL[3 * o->up[k]]));
+      for (int64_t k = o->lo_off[c]; k < o->lo_off[c + 1]; ++k) side(v3(&o->rR[3 * o->lo[k]]));
+      for (int64_t k = o->bd_off[c]; k < o->bd_off[c + 1]; ++k) side(v3(&o->rL[3 * o->bd[k]]));
+    }
+    o->sa_phi[c] = ph;
+  }
+  std::vector<double> rho(nc), mu(nc);
+  for (int64_t c = 0; c < nc; ++c) rho[c] = sa_rho(o, c), mu[c] = sa_mu(o, c);
+  // per-cell accumulators
+  std::vector<double> src(nc, 0.0), srcJ(nc, 0.0), rhodot(nc, 0.0), divn(nc, 0.0);
+  o->sa_fjp.assign(nf, 0.0);
+  o->sa_fjm.assign(nf, 0.0);
+  for (int64_t f = 0; f < nf; ++f) {
+    const int64_t a = o->cl[f];
+    const V3 n = v3(&o->an[3 * f]);
+    const double A = o->area[f];
+    const double mdot = o->F[5 * f];  // scalar_mdot_f = iflux[0]
+    const double* ga = &o->sa_grad[3 * a];
+    const V3 rl = v3(&o->rL[3 * f]);
+    const double xl = o->nut[a] + o->sa_phi[a] * (ga[0] * rl.x + ga[1] * rl.y + ga[2] * rl.z);
+    if (o->cr[f] >= 0) {
+      const int64_t b = o->cr[f];
+      const double* gb = &o->sa_grad[3 * b];
+      const V3 rr = v3(&o->rR[3 * f]);
+      const double xr = o->nut[b] + o->sa_phi[b] * (gb[0] * rr.x + gb[1] * rr.y + gb[2] * rr.z);
+      const double vl = o->vol[a], vr = o->vol[b];
+      const double nuf = (vr * o->nut[a] + vl * o->nut[b]) * (1.0 / (vr + vl));
+      const double muf = (vl * mu[b] + vr * mu[a]) / (vl + vr);
+      const double rhof = (1. / (vl + vr)) * (vl * rho[b] + vr * rho[a]);
+      // face gradient: mean + correction along d = x_b - x_a
+      const V3 d = rl - rr;
+      const double d2 = dot(d, d);
+      double gm[3];
+      for (int k = 0; k < 3; ++k) gm[k] = 0.5 * (ga[k] + gb[k]);
+      const double cc = ((o->nut[b] - o->nut[a]) - (gm[0] * d.x + gm[1] * d.y + gm[2] * d.z)) / d2;
+      const V3 gf = mk(gm[0] + cc * d.x, gm[1] + cc * d.y, gm[2] + cc * d.z);
+      const double divf = dot(gf, n) * A;
+      double diff1 = dot(gf, n) * A;
+      diff1 = (diff1 * (muf / rhof + (1. + S.cb2) * nuf)) / S.sigma;
+      // convection (inviscid_fluxP(X,Zero))
+      const double xv = mdot < 0.0 ? xr : xl;
+      const double conv = mdot * std::max(xv, 0.0);
+      src[a] -= conv, src[b] += conv;
+      rhodot[a] -= mdot, rhodot[b] += mdot;
+      src[a] += rho[a] * diff1, src[b] -= rho[b] * diff1;
+      divn[a] += divf, divn[b] -= divf;
+      // Jacobians
+      double fjp = 0.0, fjm = 0.0;
+      fjp += std::max(mdot, 0.0);
+      fjm += std::min(mdot, 0.0);
+      const double rbar = .5 * (rho[a] + rho[b]);
+      const double C = (muf + (1. + S.cb2) * rbar * nuf) * A;
+      const double dd = dot(d, n);  // (x_b - x_a).n
+      fjp -= -C / (dd * S.sigma);
+      fjm += -C / (dd * S.sigma);
+      const double C2 = S.cb2 * A, d2s = S.sigma * dd;
+      const double sU = -SA_FACTORX * (C2 / d2s) * rho[a] * o->nut[a];
+      const double sL = -SA_FACTORX * (C2 / d2s) * rho[b] * o->nut[b];
+      fjp += sL;
+      fjm -= sU;
+      srcJ[a] += SA_FACTORX * SA_FACTORY * (C2 / d2s) * rho[a] * o->nut[a];
+      srcJ[b] += SA_FACTORX * SA_FACTORY * (C2 / d2s) * rho[b] * o->nut[b];
+      // X_srcJ += -sum_upper fjp + sum_lower fjm, minus the L/U
+      // non-conservative parts (SA_turb.loci:745-752)
+      srcJ[a] -= fjp, srcJ[b] += fjm;
+      srcJ[a] += sL, srcJ[b] += sU;
+      o->sa_fjp[f] = fjp, o->sa_fjm[f] = fjm;
+    } else {
+      const int kind = o->bcs[-o->cr[f] - 1].kind;
+      const double* qf = &o->qb[5 * f];
+      const double nuf = nub[f];
+      const double muf = suth(qf[0], P.mu_a1, P.mu_a2, P.mu_a3);
+      const double rhof = (qf[4] + P.Pambient) / (P.Rtilde * qf[0]);  // solverEoS.loci:53-56
+      const V3 r = rl;
+      const double r2 = dot(r, r);
+      const double cc = ((nuf - o->nut[a]) - (ga[0] * r.x + ga[1] * r.y + ga[2] * r.z)) / r2;
+      const V3 gf = mk(ga[0] + cc * r.x, ga[1] + cc * r.y, ga[2] + cc * r.z);
+      const double divf = dot(gf, n) * A;
+      double diff1 = dot(gf, n) * A;
+      diff1 = (diff1 * (muf / rhof + (1. + S.cb2) * nuf)) / S.sigma;
+      const double xv = mdot < 0.0 ? nuf : xl;
+      const double conv = mdot * std::max(xv, 0.0);
+      src[a] -= conv;
+      rhodot[a] -= mdot;
+      src[a] += rho[a] * diff1;
+      divn[a] += divf;
+      srcJ[a] -= std::max(mdot, 0.0);
+      if (kind != FPSI_BC_REFLECTING) {  // no_symmetry_BC
+        const double C = (muf + (1. + S.cb2) * rhof * nuf) * A;
+        const double db = dot(r, n);
+        srcJ[a] += -C / (db * S.sigma);
+        const double C2 = S.cb2 * A, d2s = S.sigma * db;
+        srcJ[a] += SA_FACTORX * SA_FACTORY * (C2 / d2s) * rho[a] * o->nut[a];
+      }
+    }
+  }
+  // cell terms
+  const double k2 = S.k * S.k;
+  const double cw1 = (S.cb1) / (k2) + (1.0 + (S.cb2)) / (S.sigma);
+  const double cw36 = std::pow(S.cw3, 6);
+  const double cv13 = S.cv1 * S.cv1 * S.cv1;
+  o->sa_src.assign(nc, 0.0);
+  o->sa_D.assign(nc, 0.0);
+  for (int64_t c = 0; c < nc; ++c) {
+    const double nu = o->nut[c], r0 = rho[c], V = o->vol[c], y = o->wdist[c];
+    const double* gu = &o->grad[15 * c + 3];  // rows u, v, w: d u_i / d x_j
+    const double wx = gu[3 * 2 + 1] - gu[3 * 1 + 2];
+    const double wy = gu[3 * 0 + 2] - gu[3 * 2 + 0];
+    const double wz = gu[3 * 1 + 0] - gu[3 * 0 + 1];
+    const double vort = std::sqrt(wx * wx + wy * wy + wz * wz);
+    const double x = r0 * nu / mu[c];
+    const double fv1 = std::pow(x, 3) / (std::pow(x, 3) + std::pow(S.cv1, 3));
+    const double fv2 = 1.0 - (x / (1.0 + x * fv1));
+    const double denom = k2 * y * y;
+    double St = 0.0;
+    St += vort;
+    St += nu * fv2 / denom;
+    const double Sl = std::max(St, 0.3 * vort);
+    double rc;
+    if (Sl < nu / (10 * denom))
+      rc = 10;
+    else
+      rc = nu / (Sl * denom);
+    const double r2 = rc * rc, r6 = r2 * r2 * r2;
+    const double gc = rc + S.cw2 * (r6 - rc);
+    const double g2 = gc * gc, g6 = g2 * g2 * g2;
+    const double fw = gc * std::pow((1.0 + cw36) / (g6 + cw36), 1.0 / 6.0);
+    double s = src[c];
+    s += r0 * nu * Sl * S.cb1 * V;
+    const double t = nu / y;
+    s -= r0 * fw * cw1 * t * t * V;
+    s += -r0 * nu * divn[c] * S.cb2 / S.sigma;
+    s -= nu * rhodot[c];
+    // destruction Jacobian (:275-357)
+    double rp;
+    if (Sl < nu / (9e6 * denom)) {
+      rp = 0;
+    } else {
+      const double chi = x, chiP = 1. / mu[c];
+      const double chi3 = chi * chi * chi, chi4 = chi3 * chi, chi6 = chi3 * chi3;
+      const double fv2p = chi * (4 * (chi3 * chiP) / (chi3 + cv13) -
+                                 3 * (chi6 * chiP) / std::pow(chi3 + cv13, 2)) /
+                              std::pow(chi4 / (chi3 + cv13) + 1, 2) -
+                          chiP / (chi4 / (chi3 + cv13) + 1);
+      const double Stp = (fv2 / r0 + nu * fv2p) / (denom);
+      rp = 1. / (r0 * denom * Sl) - nu * Stp / (denom * Sl * Sl);
+    }
+    const double gp = rp + S.cw2 * (6. * std::pow(rc, 5) * rp - rp);
+    const double term = std::pow((cw36 + 1.) / (cw36 + g6), 1. / 6.);
+    const double term2 = term * term, term5 = term2 * term2 * term;
+    const double rterm5 = 1. / term5, rsum = 1. / (g6 + cw36);
+    const double fwp = gp * term - gp * ((cw36 + 1) * g6) * rsum * rsum * rterm5;
+    double sJ = srcJ[c];
+    sJ -= V * cw1 * r0 * nu * (r0 * nu * fwp + 2. * fw) / (y * y);
+    sJ += -rhodot[c];
+    o->sa_src[c] = s;
+    o->sa_D[c] = -sJ + r0 * (V / o->dtau[c]);
+  }
+  if (src_out) std::memcpy(src_out, o->sa_src.data(), sizeof(double) * nc);
+  o->have_sa = true;
+  o->have_sa_dq = false;
+  return FPSI_OK;
+}
+
+extern "C" int orc_sa_get_system(orc_ctx* o, double* D, double* fjp, double* fjm) {
+  if (!o->have_sa) return FPSI_E_STATE;
+  if (D) std::memcpy(D, o->sa_D.data(), sizeof(double) * o->nc);
+  if (fjp) std::memcpy(fjp, o->sa_fjp.data(), sizeof(double) * o->nf);
+  if (fjm) std::memcpy(fjm, o->sa_fjm.data(), sizeof(double) * o->nf);
+  return FPSI_OK;
+}
+
+// scalar SGS (linearSolverSGS.loci:333-470): x = B/D, then per sweep the
+// forward and backward passes x_c = Dinv (B - sum_upper U x_cr - sum_lower L x_cl)
+// with L = -fjp, U = fjm; colour == NULL: sequential order, else multi-colour
+extern "C" int orc_sa_solve(orc_ctx* o, const int32_t* colour, double* dq) {
+  if (!o->have_sa) return FPSI_E_STATE;
+  const int64_t nc = o->nc;
+  std::vector<double> Dinv(nc), x(nc);
+  for (int64_t c = 0; c < nc; ++c) {
+    Dinv[c] = 1. / o->sa_D[c];
+    x[c] = Dinv[c] * o->sa_src[c];
+  }
+  auto gs = [&](int64_t c) {
+    double t = -o->sa_src[c];
+    for (int64_t k = o->up_off[c]; k < o->up_off[c + 1]; ++k) {
+      const int64_t f = o->up[k];
+      t += x[o->cr[f]] * o->sa_fjm[f];
+    }
+    for (int64_t k = o->lo_off[c]; k < o->lo_off[c + 1]; ++k) {
+      const int64_t f = o->lo[k];
+      t += x[o->cl[f]] * (-o->sa_fjp[f]);
+    }
+    x[c] = Dinv[c] * (-t);
+  };
+  std::vector<int64_t> order(nc);
+  for (int64_t c = 0; c < nc; ++c) order[c] = c;
+  if (colour) {
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int64_t a, int64_t b) { return colour[a] < colour[b]; });
+  }
+  for (int it = 0; it < o->P.gauss_seidel_iter; ++it) {
+    for (int64_t i = 0; i < nc; ++i) gs(order[i]);
+    for (int64_t i = nc - 1; i >= 0; --i) gs(order[i]);
+  }
+  o->sa_dq = x;
+  if (dq) std::memcpy(dq, x.data(), sizeof(double) * nc);
+  o->have_sa_dq = true;
+  return FPSI_OK;
+}
+
+// X_next = max(X + min(1, urelax X / (|dq| + 1e-15)) dq, 1e-15)
+// (solverScalarTransport.loci:397-405)
+extern "C" int orc_sa_update(orc_ctx* o) {
+  if (!o->have_sa_dq) return FPSI_E_STATE;
+  const double relax = o->P.urelax;
+  for (int64_t c = 0; c < o->nc; ++c) {
+    double tscale = 1.0;
+    tscale = std::min(tscale, relax * o->nut[c] / (std::fabs(o->sa_dq[c]) + 1e-15));
+    double xn = o->nut[c] + tscale * o->sa_dq[c];
+    o->nut[c] = std::max(xn, 1e-15);
+  }
+  o->have_sa = o->have_sa_dq = false;
   return FPSI_OK;
 }

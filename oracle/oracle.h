@@ -44,6 +44,17 @@ int  orc_lsgs_solve(orc_ctx* o, int64_t nlines, const int64_t* line_off,
                     double* dq, fpsi_lsinfo* info);
 int  orc_update(orc_ctx* o, double* min_alpha);
 int  orc_newton_step(orc_ctx* o, const int32_t* colour, fpsi_stepinfo* info);
+/* Spalart-Allmaras nu~ transport (turbulence/SA/SA_turb.loci), as
+ * fpsi_set_nutilde ... fpsi_sa_update; orc_sa_solve takes the sweep order
+ * like orc_linear_solve */
+int  orc_set_nutilde(orc_ctx* o, const double* nut);
+int  orc_get_nutilde(orc_ctx* o, double* nut);
+int  orc_get_eddy_viscosity(orc_ctx* o, double* tmu);
+int  orc_get_wall_distance(orc_ctx* o, double* dist);
+int  orc_sa_residual(orc_ctx* o, double* src);
+int  orc_sa_get_system(orc_ctx* o, double* D, double* fjp, double* fjm);
+int  orc_sa_solve(orc_ctx* o, const int32_t* colour, double* dq);
+int  orc_sa_update(orc_ctx* o);
 /* number of OpenMP threads the oracle loops use (1 = scalar) */
 int  orc_set_threads(int n);
 

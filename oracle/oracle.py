@@ -41,6 +41,14 @@ _SIGS = {
     "orc_update": (C.c_int, [C.c_void_p, _dp]),
     "orc_newton_step": (C.c_int, [C.c_void_p, _ip, C.POINTER(N.StepInfo)]),
     "orc_set_threads": (C.c_int, [C.c_int]),
+    "orc_set_nutilde": (C.c_int, [C.c_void_p, _dp]),
+    "orc_get_nutilde": (C.c_int, [C.c_void_p, _dp]),
+    "orc_get_eddy_viscosity": (C.c_int, [C.c_void_p, _dp]),
+    "orc_get_wall_distance": (C.c_int, [C.c_void_p, _dp]),
+    "orc_sa_residual": (C.c_int, [C.c_void_p, _dp]),
+    "orc_sa_get_system": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+    "orc_sa_solve": (C.c_int, [C.c_void_p, _ip, _dp]),
+    "orc_sa_update": (C.c_int, [C.c_void_p]),
     "orc_face_flux": (C.c_int, [C.c_int32, C.c_int64, _dp, _dp, _dp, _dp, C.c_double,
                                 C.c_double, C.c_double, C.c_double, C.c_double, _dp]),
     "orc_face_jacobian": (C.c_int, [C.c_int64, _dp, _dp, _dp, _dp, C.c_double, C.c_double,
@@ -286,3 +294,41 @@ class Oracle:
         d = si.resid.as_dict()
         d["min_alpha"] = si.min_alpha
         return d
+
+    # -- Spalart-Allmaras nu~ (turbulence/SA/SA_turb.loci) -------------------
+    def set_nutilde(self, nut):
+        _chk(olib().orc_set_nutilde(self._h, _d(np.ascontiguousarray(nut, np.float64))),
+             "orc_set_nutilde")
+
+    def _cellvec(self, fn, name):
+        v = np.empty(self.ncells)
+        _chk(fn(self._h, v.ctypes.data_as(_dp)), name)
+        return v
+
+    def nutilde(self):
+        return self._cellvec(olib().orc_get_nutilde, "orc_get_nutilde")
+
+    def eddy_viscosity(self):
+        return self._cellvec(olib().orc_get_eddy_viscosity, "orc_get_eddy_viscosity")
+
+    def wall_distance(self):
+        return self._cellvec(olib().orc_get_wall_distance, "orc_get_wall_distance")
+
+    def sa_residual(self):
+        return self._cellvec(olib().orc_sa_residual, "orc_sa_residual")
+
+    def sa_system(self):
+        D, fjp, fjm = np.empty(self.ncells), np.empty(self.nfaces), np.empty(self.nfaces)
+        _chk(olib().orc_sa_get_system(self._h, D.ctypes.data_as(_dp), fjp.ctypes.data_as(_dp),
+                                      fjm.ctypes.data_as(_dp)), "orc_sa_get_system")
+        return {"D": D, "fjp": fjp, "fjm": fjm}
+
+    def sa_solve(self, colour=None):
+        col = None if colour is None else np.ascontiguousarray(colour, np.int32)
+        dq = np.empty(self.ncells)
+        _chk(olib().orc_sa_solve(self._h, None if col is None else col.ctypes.data_as(_ip),
+                                 dq.ctypes.data_as(_dp)), "orc_sa_solve")
+        return dq
+
+    def sa_update(self):
+        _chk(olib().orc_sa_update(self._h), "orc_sa_update")
