@@ -171,7 +171,8 @@ def build_case(args):
     if args.workload == "bl":
         return cases.boundary_layer_block(args.bl_nx, args.bl_ny, args.bl_nz,
                                           precision=args.precision, viscous=args.viscous,
-                                          solver="lsgs")
+                                          solver="lsgs",
+                                          sa=args.viscous == 2 and args.turb == "sa")
     if args.workload == "shock":
         return cases.oblique_shock_cube(args.n, seed=args.seed, sweeps=args.sweeps,
                                         precision=args.precision)
@@ -181,7 +182,8 @@ def build_case(args):
 
 def workload_name(args) -> str:
     if args.workload == "bl":
-        return f"boundary_layer_{args.bl_nx}x{args.bl_ny}x{args.bl_nz}_visc{args.viscous}"
+        turb = f"_{args.turb}" if args.viscous == 2 else ""
+        return f"boundary_layer_{args.bl_nx}x{args.bl_ny}x{args.bl_nz}_visc{args.viscous}{turb}"
     if args.workload == "shock":
         return f"oblique_shock_cube_{args.n}"
     return f"taylor_green_tets_{args.n}"
@@ -313,6 +315,8 @@ def run_fpsi(args, ws, rank, local):
         solver.keep_blocks(False)
     if getattr(case, "tmu", None) is not None:
         solver.set_eddy_viscosity(case.tmu)
+    if getattr(case, "nut0", None) is not None:
+        solver.set_nutilde(case.nut0)
     log(f"[rank {rank}] setup {time.perf_counter() - t0:.1f}s: {solver.ncells} cells, "
         f"{solver.nfaces} faces, {solver.ncolours} colours, "
         f"{solver.device_bytes / 1e9:.2f} GB device")
@@ -405,7 +409,7 @@ def run_fpsi(args, ws, rank, local):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 residual + f32 blocks/sweeps" if args.precision == "mixed" else args.precision,
         "data": {"tgv": "synthetic (seeded Taylor-Green on a jittered split-tet grid)",
-                 "bl": "synthetic (seeded noise on a flat-plate block, frozen SA eddy viscosity)",
+                 "bl": "synthetic (seeded noise on a flat-plate block; SA nu~ from 3 nu_inf)",
                  "shock": "synthetic (seeded oblique Mach-2 shock on a hex cube)"}[args.workload],
         "config": {"workload": workload_name(args), "cells": nc, "faces": nf,
                    "colours": solver.ncolours, "precision": args.precision,
@@ -449,7 +453,9 @@ def main():
     ap.add_argument("--bl-nx", type=int, default=256)
     ap.add_argument("--bl-ny", type=int, default=128)
     ap.add_argument("--bl-nz", type=int, default=64)
-    ap.add_argument("--viscous", type=int, default=2, help="bl: 0 inviscid, 1 laminar, 2 SA tmu")
+    ap.add_argument("--viscous", type=int, default=2, help="bl: 0 inviscid, 1 laminar, 2 turbulent")
+    ap.add_argument("--turb", default="sa", choices=["sa", "frozen"],
+                    help="bl turbulent: SA nu~ transport or a frozen eddy viscosity")
     ap.add_argument("--converge-n", type=int, default=128,
                     help="farfield cube size for the time-to-1e-8 runs (0: skip)")
     args = ap.parse_args()
