@@ -131,15 +131,32 @@ def dist_barrier(ws: int):
         dist.barrier()
 
 
-def sgs_bytes_per_step(nc, nfi, nbf, sweeps, tb, tx):
-    """algorithmic bytes of all SGS colour launches of one step: per cell
-    LU 25*tb + B 5*tb + x write 5*tx; per interior face side block 25*tb +
-    face index 4 + neighbour x 5*tx; two directions per sweep"""
-    per_dir = nc * (30 * tb + 5 * tx) + 2 * nfi * (25 * tb + 4 + 5 * tx)
-    return 2 * sweeps * per_dir
+def sgs_launch_sequence(ncolours, sweeps):
+    """colours launched by one step's sweeps: forward then backward, a
+    colour that directly follows itself is not relaunched"""
+    seq, last = [], -1
+    for _ in range(sweeps):
+        for k in list(range(ncolours)) + list(range(ncolours - 1, -1, -1)):
+            if k != last:
+                seq.append(k)
+                last = k
+    return seq
 
 
-def kernel_bytes(name, nc, nfi, nbf, sweeps, tb, tx):
+def sgs_colour_bytes(colour, nint, tb, tx):
+    """algorithmic bytes of one launch of each colour: per cell LU 25*tb +
+    B 5*tb + x write 5*tx; per interior face side block 25*tb + index 4 +
+    neighbour x 5*tx"""
+    per_cell = (30 * tb + 5 * tx) + nint * (25 * tb + 4 + 5 * tx)
+    return np.bincount(colour, weights=per_cell.astype(np.float64))
+
+
+def sgs_bytes_per_step(colour_bytes, sweeps):
+    seq = sgs_launch_sequence(len(colour_bytes), sweeps)
+    return float(sum(colour_bytes[k] for k in seq)), len(seq)
+
+
+def kernel_bytes(name, nc, nfi, nbf, sweeps, tb, tx, sgs_step_bytes=None):
     """algorithmic bytes of one step of each kernel (every array the kernel
     must touch counted once: FP64 8 B, FP32 4 B, index 4 B)"""
     nf = nfi + nbf
@@ -157,7 +174,7 @@ def kernel_bytes(name, nc, nfi, nbf, sweeps, tb, tx):
         # more into the off-diagonal slots
         "assemble_lu": (nc * (40 + 40 + 8 + 8 + 30 * tb + 4 + 5 * tx) + (2 * nfi + nbf) * 25 * tb
                         + 2 * nfi * 25 * tb),
-        "sgs_colour": sgs_bytes_per_step(nc, nfi, nbf, sweeps, tb, tx),
+        "sgs_colour": sgs_step_bytes,
         "update": nc * (80 + 5 * tx),
     }.get(name)
 
@@ -324,8 +341,12 @@ def run_fpsi(args, ws, rank, local):
     T0, p0, u0 = case.initial_state(geo["cellcenter"])
     solver.set_state(T0, p0, u0)
     nc, nf = solver.ncells, solver.nfaces
-    nfi = int((np.asarray(case.mesh.arrays().cr) >= 0).sum())
+    arr = case.mesh.arrays()
+    inner = np.asarray(arr.cr) >= 0
+    nfi = int(inner.sum())
     nbf = nf - nfi
+    nint = (np.bincount(np.asarray(arr.cl)[inner], minlength=nc)
+            + np.bincount(np.asarray(arr.cr)[inner], minlength=nc))
     hist_w = solver.run(args.warmup) if args.warmup > 0 else []
     dist_barrier(ws)
     with Clocks(local) as clk:
@@ -341,15 +362,19 @@ def run_fpsi(args, ws, rank, local):
     peaks, src = load_peaks()
     peak = float(peaks["hbm_gbs"])
     kernels = {}
+    sgs_step = None
+    if case.params.solver == 0:
+        cb = sgs_colour_bytes(solver.colours(), nint, tb, tx)
+        sgs_step, _ = sgs_bytes_per_step(cb, case.params.gauss_seidel_iter)
     for name, (kms, launches) in kt.items():
-        b = kernel_bytes(name, nc, nfi, nbf, args.sweeps, tb, tx)
+        b = kernel_bytes(name, nc, nfi, nbf, args.sweeps, tb, tx, sgs_step)
         per_step_ms = kms / args.profile_steps
         kernels[name] = {"ms_per_step": per_step_ms, "launches_per_step": launches / args.profile_steps,
                          "gbs": None if b is None else b / (per_step_ms / 1e3) / 1e9}
     dom = max((k for k in kernels if kernels[k]["gbs"] is not None),
               key=lambda k: kernels[k]["ms_per_step"])
     dk = kernels[dom]
-    b_launch = kernel_bytes(dom, nc, nfi, nbf, args.sweeps, tb, tx) / dk["launches_per_step"]
+    b_launch = kernel_bytes(dom, nc, nfi, nbf, args.sweeps, tb, tx, sgs_step) / dk["launches_per_step"]
     avg_launch_s = dk["ms_per_step"] / dk["launches_per_step"] / 1e3
     achieved = b_launch / avg_launch_s / 1e9
     traffic = None

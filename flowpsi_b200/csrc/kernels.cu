@@ -1259,16 +1259,23 @@ int launch_jacobi_start(fpsi_ctx* x) {
 }
 
 template <class TB, class TX>
+// Forward then backward over the colours, `sweeps` times.  A colour's cells
+// read only other colours' iterates, so a colour that directly follows
+// itself (the turn of each sweep, and the step from one sweep to the next)
+// would reproduce the values it just wrote: those launches are skipped and
+// the iterate is bitwise the same as with every launch made.
 static int launch_sgs_t(fpsi_ctx* x, int sweeps) {
   cudaStream_t s = x->stream;
   const int T = 128;
   const int K = x->H.ncolours;
+  int last = -1;
   for (int it = 0; it < sweeps; ++it) {
     for (int pass = 0; pass < 2; ++pass)
       for (int kk = 0; kk < K; ++kk) {
         const int k = pass == 0 ? kk : K - 1 - kk;
         const ColInfo ck = col_info(x, k);
-        if (ck.n == 0) continue;
+        if (ck.n == 0 || k == last) continue;
+        last = k;
         prof_begin(x, "sgs_colour");
         dev::k_sgs_colour<TB, TX><<<blocks_for(ck.n, T), T, 0, s>>>(
             ck, x->d_nbr, (const TB*)x->d_aoff, (const TB*)x->d_luc, (const TB*)x->d_bc, x->d_pv,

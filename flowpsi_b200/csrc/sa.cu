@@ -428,12 +428,16 @@ int sa_launch_solve(fpsi_ctx* x) {
   const HostMesh& H = x->H;
   prof_begin(x, "sa_sgs");
   sa::k_sa_jacobi<<<nblk(G.nc, 256), 256, 0, s>>>(G.nc, x->d_sa_B, x->d_sa_Dinv, x->d_sa_x);
+  // a colour directly following itself would rewrite the same values
+  // (its cells read only other colours): skipped, the result is unchanged
+  int last = -1;
   for (int it = 0; it < x->P.gauss_seidel_iter; ++it)
     for (int pass = 0; pass < 2; ++pass)
       for (int kk = 0; kk < H.ncolours; ++kk) {
         const int k = pass == 0 ? kk : H.ncolours - 1 - kk;
         const int64_t b = H.colour_off[k], n = H.colour_off[k + 1] - b;
-        if (n == 0) continue;
+        if (n == 0 || k == last) continue;
+        last = k;
         sa::k_sa_gs<<<nblk(n, 128), 128, 0, s>>>(G, x->d_colour_cells + b, n, x->d_sa_B,
                                                  x->d_sa_Dinv, x->d_sa_face, x->d_sa_x);
       }
