@@ -4,12 +4,16 @@
 // kind 1: periodic hex box, each hex split into 6 Kuhn tetrahedra along its
 //         main diagonal, nodes jittered (128^3 Taylor-Green case)
 // kind 2: boundary-layer hex block with geometric wall-normal stretching
+// kind 3: hex box (as kind 0, periodic sides allowed) with each hex split
+//         into two triangular prisms across the diagonal v000-v110 of its
+//         z-faces: 5 faces per cell, triangles and quads mixed
 //
 // Faces are produced directly from the structured topology (no hashing), with
 // interior faces oriented cl < cr and node order giving a cl->cr normal.
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <initializer_list>
 #include <new>
 #include <vector>
 
@@ -54,7 +58,12 @@ void finish(OwnedMesh* o) {
 // Hex box.  Node (i,j,k) = i + (nx+1)*(j + (ny+1)*k); cell (i,j,k) =
 // i + nx*(j + ny*k).  Periodic directions reuse node index i mod n for the
 // face of the last layer and record the translation in pshift.
-int gen_hex(const fpsi_mesh_spec* s, OwnedMesh* o, bool stretched) {
+// With `prism` each hex c becomes prisms 2c (P0: corners v000 v100 v110 and
+// the three above) and 2c+1 (P1: v000 v110 v010 and above).  P0 owns the
+// hex's x-max and y-min faces, P1 its x-min and y-max faces; z-faces split
+// into two triangles (P0's and P1's), and the diagonal quad separates P0
+// from P1 with its normal towards P1.
+int gen_hex(const fpsi_mesh_spec* s, OwnedMesh* o, bool stretched, bool prism = false) {
   const int nx = s->nx, ny = s->ny, nz = s->nz;
   if (nx < 2 || ny < 2 || nz < 2) return FPSI_E_INVALID;
   const bool per[3] = {s->bc_side[0] < 0, s->bc_side[2] < 0, s->bc_side[4] < 0};
@@ -89,8 +98,42 @@ int gen_hex(const fpsi_mesh_spec* s, OwnedMesh* o, bool stretched) {
   const int64_t nc = int64_t(nx) * ny * nz;
   o->face_off.push_back(0);
   bool anyper = per[0] || per[1] || per[2];
+  auto add_poly = [&](std::initializer_list<int32_t> nodes, int32_t L, int32_t R, double sx,
+                      double sy, double sz) {
+    for (int32_t v : nodes) o->face_nodes.push_back(v);
+    o->face_off.push_back(int64_t(o->face_nodes.size()));
+    o->cl.push_back(L);
+    o->cr.push_back(R);
+    if (anyper) {
+      o->pshift.push_back(sx);
+      o->pshift.push_back(sy);
+      o->pshift.push_back(sz);
+    }
+  };
+  // where = 0 interior (+d node order), 1 emitted at p = 0 (reversed
+  // order; R is the last layer's hex on a periodic seam, else a boundary
+  // code), 2 the boundary at p = n_d
+  int cur_d = 0, where = 0;
   auto add_face = [&](int32_t a, int32_t b, int32_t c, int32_t d, int32_t L, int32_t R,
                       double sx, double sy, double sz) {
+    if (prism) {
+      const bool rb = R < 0;  // boundary code
+      auto P = [](int32_t h, int side) { return 2 * h + side; };
+      if (cur_d == 2) {
+        // triangles (a,b,c) and (a,c,d); in +z order the first is P0's
+        const int sa = where == 1 ? 1 : 0, sb = 1 - sa;
+        add_poly({a, b, c}, P(L, sa), rb ? R : P(R, sa), sx, sy, sz);
+        add_poly({a, c, d}, P(L, sb), rb ? R : P(R, sb), sx, sy, sz);
+      } else {
+        // the face's side of the hex on each side: x-max and y-min in P0
+        const int lo_side = cur_d == 0 ? 1 : 0;  // the hex's min-plane face
+        const int hi_side = 1 - lo_side;         // the hex's max-plane face
+        const int sl = where == 1 ? lo_side : hi_side;  // cl's face: min plane at p = 0
+        const int sr = where == 1 ? hi_side : lo_side;
+        add_poly({a, b, c, d}, P(L, sl), rb ? R : P(R, sr), sx, sy, sz);
+      }
+      return;
+    }
     o->face_nodes.push_back(a);
     o->face_nodes.push_back(b);
     o->face_nodes.push_back(c);
@@ -130,6 +173,8 @@ int gen_hex(const fpsi_mesh_spec* s, OwnedMesh* o, bool stretched) {
           int32_t n0 = nid(p, a, b), n1 = nid(p, a + 1, b), n2 = nid(p, a + 1, b + 1),
                   n3 = nid(p, a, b + 1);
           double sh[3] = {0, 0, 0};
+          cur_d = d;
+          where = (p > 0 && p < Nn[d]) ? 0 : (p == 0 ? 1 : 2);
           if (p > 0 && p < Nn[d]) {
             add_face(n0, n1, n2, n3, cid(p - 1), cid(p), 0, 0, 0);
           } else if (per[d]) {
@@ -144,10 +189,21 @@ int gen_hex(const fpsi_mesh_spec* s, OwnedMesh* o, bool stretched) {
           }
         }
   }
-  o->m.ncells = nc;
+  if (prism) {
+    // the diagonal quad of every hex, P0 -> P1
+    for (int64_t k = 0; k < nz; ++k)
+      for (int64_t j = 0; j < ny; ++j)
+        for (int64_t i = 0; i < nx; ++i) {
+          const int32_t c = cell(i, j, k);
+          add_poly({node(i, j, k), node(i, j, k + 1), node(i + 1, j + 1, k + 1), node(i + 1, j + 1, k)},
+                   2 * c, 2 * c + 1, 0, 0, 0);
+        }
+  }
+  const int64_t ncells = prism ? 2 * nc : nc;
+  o->m.ncells = ncells;
   o->bcs.assign(s->bcs, s->bcs + s->nbc);
   finish(o);
-  o->m.ncells = nc;
+  o->m.ncells = ncells;
   return FPSI_OK;
 }
 
@@ -328,6 +384,8 @@ extern "C" int fpsi_mesh_generate(const fpsi_mesh_spec* s, fpsi_mesh** out) {
       rc = gen_kuhn(s, o);
     else if (s->kind == 2)
       rc = gen_hex(s, o, true);
+    else if (s->kind == 3)
+      rc = gen_hex(s, o, false, true);
     else
       rc = FPSI_E_INVALID;
   } catch (const std::bad_alloc&) {

@@ -70,7 +70,7 @@ class GeneratedMesh:
     def __init__(self, kind: str, n=(8, 8, 8), L=(1.0, 1.0, 1.0), jitter=0.0, seed=0,
                  bc_side=(-1, -1, -1, -1, -1, -1), bcs=(), dy0=1e-3, growth=1.1):
         s = N.MeshSpec()
-        s.kind = {"hex": 0, "kuhn": 1, "bl": 2}[kind]
+        s.kind = {"hex": 0, "kuhn": 1, "bl": 2, "prism": 3}[kind]
         s.nx, s.ny, s.nz = n
         s.Lx, s.Ly, s.Lz = L
         s.jitter = jitter

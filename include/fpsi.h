@@ -170,6 +170,9 @@ int         fpsi_device_available(void);
  * kind 1: nx*ny*nz hexes each split into 6 Kuhn tetrahedra on the periodic
  *         box [0,Lx]x[0,Ly]x[0,Lz]; nodes jittered by U(-jitter,+jitter)*h.
  * kind 2: boundary-layer hex block: y spacing dy0*growth^j.
+ * kind 3: the kind-0 box with each hex split into two triangular prisms
+ *         across the diagonal of its z-faces (cells 2c and 2c+1 of hex c):
+ *         five faces per cell, triangular and quadrilateral faces mixed.
  * Returns an fpsi_mesh whose arrays are owned by the library. */
 typedef struct fpsi_mesh_spec {
   int32_t kind;
