@@ -209,6 +209,10 @@ int check_params(const fpsi_params* p) {
     fpsi::set_error("flowRegime / Sutherland parameters out of range");
     return FPSI_E_INVALID;
   }
+  if (p->turbulence < 0 || p->turbulence > 1 || (p->turbulence == FPSI_TURB_SA && p->viscous != 2)) {
+    fpsi::set_error("turbulence: 0 (given eddy viscosity) or 1 (SA, needs viscous = 2)");
+    return FPSI_E_INVALID;
+  }
   return FPSI_OK;
 }
 
