@@ -16,8 +16,11 @@
 // and a linear head (64 -> 5) give d, and the starting iterate is
 //     x0 = x_J + xs * d,
 // so a network that outputs zero reproduces the reference's start.  Weights
-// are used in BF16 with FP32 accumulation; FP32 master weights and Adam
-// moments are kept for training.  Training targets are (dq - x_J)/xs for
+// and activations are BF16, accumulation FP32: each message-passing layer is
+// one tcgen05 tensor-core GEMM per 128-cell tile ([h | agg] times
+// [Ws | Wn]^T, accumulator in tensor memory) with bias and GELU applied as
+// the accumulator is read back.  FP32 master weights and Adam moments are
+// kept for training.  Training targets are (dq - x_J)/xs for
 // solver-generated converged dq.  All reductions (weight gradients, loss)
 // are per-block partials summed in a fixed order: training is reproducible.
 #include <cuda_bf16.h>
@@ -90,12 +93,17 @@ struct fpsi_gnn {
   int64_t adam_t = 0;
   // activations for one full-graph pass, sized for `cap` cells
   int64_t cap = 0;
-  float *d_h[NLAYER + 1] = {nullptr}, *d_agg[NLAYER] = {nullptr}, *d_z[NLAYER] = {nullptr};
+  // BF16 activations (h[0] is the FP32 feature array of the pass), FP32
+  // pre-activations for the backward pass
+  __nv_bfloat16 *d_h[NLAYER + 1] = {nullptr}, *d_agg[NLAYER] = {nullptr};
+  float* d_z[NLAYER] = {nullptr};
   float *d_y = nullptr, *d_dh = nullptr, *d_dh2 = nullptr, *d_dz = nullptr, *d_dagg = nullptr;
   float* d_part = nullptr;  // weight-gradient partials
   double* d_lpart = nullptr;
   std::vector<Snapshot> snaps;
   cudaStream_t stream = nullptr;
+  int nsm = 148;                  // multiprocessors of the device (grid of the layer GEMM)
+  int32_t* d_err = nullptr;       // bit 1: a tensor-core wait gave up
 };
 
 namespace {
@@ -107,59 +115,231 @@ __device__ __forceinline__ float gelu_grad(float x) {
   return cdf + x * pdf;
 }
 
-// agg[c] = mean over neighbours of h[n]  (width fin)
+__device__ __forceinline__ float to_f(float v) { return v; }
+__device__ __forceinline__ float to_f(__nv_bfloat16 v) { return __bfloat162float(v); }
+// a layer input as the tensor cores multiply it (FP32 features rounded to BF16)
+__device__ __forceinline__ float as_operand(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
+__device__ __forceinline__ float as_operand(__nv_bfloat16 v) { return __bfloat162float(v); }
+
+// agg[c] = mean over neighbours of h[n] (width fin), summed in FP32 and
+// rounded to BF16
+template <class TIn>
 __global__ void k_aggregate(int64_t nc, int fin, const int32_t* __restrict__ off,
-                            const int32_t* __restrict__ nb, const float* __restrict__ h,
-                            float* __restrict__ agg) {
+                            const int32_t* __restrict__ nb, const TIn* __restrict__ h,
+                            __nv_bfloat16* __restrict__ agg) {
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= nc * fin) return;
   const int64_t c = i / fin;
   const int k = int(i % fin);
   const int32_t a = off[c], b = off[c + 1];
   float s = 0.f;
-  for (int32_t e = a; e < b; ++e) s += h[int64_t(nb[e]) * fin + k];
-  agg[i] = b > a ? s / float(b - a) : 0.f;
+  for (int32_t e = a; e < b; ++e) s += to_f(h[int64_t(nb[e]) * fin + k]);
+  agg[i] = __float2bfloat16_rn(b > a ? s / float(b - a) : 0.f);
 }
 
-// out[c][j] = act(b_j + sum_i Ws[j][i] h[c][i] + Wn[j][i] agg[c][i]); z = pre-activation
-__global__ void __launch_bounds__(GT) k_mp_forward(int64_t nc, int fin, const __nv_bfloat16* __restrict__ ws,
-                                                   const __nv_bfloat16* __restrict__ wn,
-                                                   const __nv_bfloat16* __restrict__ bb,
-                                                   const float* __restrict__ h,
-                                                   const float* __restrict__ agg,
-                                                   float* __restrict__ z, float* __restrict__ out) {
-  __shared__ float sws[W * W], swn[W * W], sb[W];
-  for (int i = threadIdx.x; i < W * fin; i += GT) {
-    sws[i] = __bfloat162float(ws[i]);
-    swn[i] = __bfloat162float(wn[i]);
+// ---- tcgen05 helpers (single-CTA MMA, no multicast) ----------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+// shared-memory matrix descriptor, K-major without swizzle: 8-row core
+// matrices of 16 B rows; SBO = byte step between 8-row groups, LBO = byte
+// step between the two 8-element K halves of one MMA (version 1, base 0)
+__device__ __forceinline__ uint64_t umma_desc(const void* p, uint32_t lbo, uint32_t sbo) {
+  const uint64_t a = (smem_u32(p) & 0x3FFFFu) >> 4;
+  return a | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) | (uint64_t((sbo >> 4) & 0x3FFFu) << 32) |
+         (uint64_t(1) << 46);
+}
+// instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128, N = 64
+constexpr uint32_t UMMA_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(W >> 3) << 17) |
+                                (uint32_t(128 >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(UMMA_IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void mbar_init1(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+// bounded wait on an mbarrier phase: false after ~2^24 polls
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  for (uint32_t it = 0; it < (1u << 24); ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
   }
-  for (int i = threadIdx.x; i < W; i += GT) sb[i] = __bfloat162float(bb[i]);
+  return false;
+}
+// this warp's 32 lanes x 64 FP32 columns of the accumulator
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float* v) {
+  uint32_t r[64];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+      "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, "
+      "%32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, "
+      "%51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+        "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+        "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+        "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]),
+        "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]),
+        "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]),
+        "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]),
+        "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 64; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+constexpr int TC_ROWS = 128;  // cells per tile (the MMA's M)
+constexpr int TC_COLS = 64;   // tensor-memory columns held per CTA (the MMA's N)
+// dynamic shared memory of k_mp_tc for input width fin
+inline size_t tc_smem_bytes(int fin) {
+  const int nch = 2 * fin / 8;  // 16 B chunks of one operand row
+  return size_t(nch) * TC_ROWS * 16 + size_t(nch) * W * 16 + 16 + W * sizeof(float);
+}
+
+// One message-passing layer on the tensor cores, persistent over 128-cell
+// tiles:  z = [h | agg] [Ws | Wn]^T + b  (BF16 operands, FP32 accumulate in
+// tensor memory), out = GELU(z) in BF16, z kept in FP32 when asked.
+// Operands sit in shared memory chunk-major: chunk c (8 K-elements, 16 B)
+// of row r at (c * rows + r) * 16, so one MMA (K = 16) reads chunks 2s and
+// 2s+1 with SBO = 128 B and LBO = rows * 16 B.  fin is 40 or 64 (K = 80 or
+// 128, whole 16-element steps).  Every wait is bounded; a wait that gives
+// up sets bit 1 of err, waits once more for the MMAs in flight and frees the
+// tensor memory.
+template <class TIn>
+__global__ void __launch_bounds__(TC_ROWS, 1)
+k_mp_tc(int64_t nc, int fin, const TIn* __restrict__ h, const __nv_bfloat16* __restrict__ agg,
+        const __nv_bfloat16* __restrict__ ws, const __nv_bfloat16* __restrict__ wn,
+        const __nv_bfloat16* __restrict__ bias, float* __restrict__ z,
+        __nv_bfloat16* __restrict__ hout, int32_t* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char tsm[];
+  const int nch = 2 * fin / 8, hch = fin / 8;
+  unsigned char* sA = tsm;
+  unsigned char* sB = tsm + size_t(nch) * TC_ROWS * 16;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sB + size_t(nch) * W * 16);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+  float* sbias = reinterpret_cast<float*>(mbar + 2);
+  const int tid = threadIdx.x, warp = tid >> 5;
+
+  // B = [Ws | Wn]: row j (output feature), chunk c of 8 elements
+  for (int idx = tid; idx < W * nch; idx += TC_ROWS) {
+    const int j = idx / nch, c = idx - nch * (idx / nch);
+    const __nv_bfloat16* src = c < hch ? ws + j * fin + 8 * c : wn + j * fin + 8 * (c - hch);
+    *reinterpret_cast<uint4*>(sB + (size_t(c) * W + j) * 16) = *reinterpret_cast<const uint4*>(src);
+  }
+  if (tid < W) sbias[tid] = __bfloat162float(bias[tid]);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(uint32_t(TC_COLS))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init1(mbar);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  tc_fence_before();
   __syncthreads();
-  const int64_t c = int64_t(blockIdx.x) * GT + threadIdx.x;
-  if (c >= nc) return;
-  const float* hc = h + c * fin;
-  const float* ac = agg + c * fin;
-  for (int j0 = 0; j0 < W; j0 += 16) {
-    float acc[16];
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  uint32_t phase = 0;
+  bool ok = true, pending = false;
+  const int64_t ntiles = (nc + TC_ROWS - 1) / TC_ROWS;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int64_t row = t * TC_ROWS + tid;
+    // A row tid = [bf16(h[row]) | agg[row]]
+    if (row < nc) {
+      const TIn* hr = h + row * fin;
+      for (int c = 0; c < hch; ++c) {
+        __align__(16) __nv_bfloat16 v[8];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) acc[j] = sb[j0 + j];
-    for (int i = 0; i < fin; ++i) {
-      const float hv = hc[i], av = ac[i];
-#pragma unroll
-      for (int j = 0; j < 16; ++j)
-        acc[j] += sws[(j0 + j) * fin + i] * hv + swn[(j0 + j) * fin + i] * av;
+        for (int e = 0; e < 8; ++e) v[e] = __float2bfloat16_rn(to_f(hr[8 * c + e]));
+        *reinterpret_cast<uint4*>(sA + (size_t(c) * TC_ROWS + tid) * 16) = *reinterpret_cast<uint4*>(v);
+      }
+      const __nv_bfloat16* ar = agg + row * fin;
+      for (int c = 0; c < hch; ++c)
+        *reinterpret_cast<uint4*>(sA + (size_t(hch + c) * TC_ROWS + tid) * 16) =
+            *reinterpret_cast<const uint4*>(ar + 8 * c);
+    } else {
+      for (int c = 0; c < nch; ++c)
+        *reinterpret_cast<uint4*>(sA + (size_t(c) * TC_ROWS + tid) * 16) = make_uint4(0, 0, 0, 0);
     }
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      z[c * W + j0 + j] = acc[j];
-      out[c * W + j0 + j] = gelu(acc[j]);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (tid == 0) {
+      for (int st = 0; st < nch / 2; ++st) {
+        const uint64_t ad = umma_desc(sA + size_t(2 * st) * TC_ROWS * 16, TC_ROWS * 16, 128);
+        const uint64_t bd = umma_desc(sB + size_t(2 * st) * W * 16, W * 16, 128);
+        umma_bf16(tmem, ad, bd, st > 0 ? 1u : 0u);
+      }
+      umma_commit(mbar);
     }
+    pending = true;
+    __syncwarp();
+    const bool got = mbar_wait_bounded(mbar, phase);
+    ok = __syncthreads_and(got) != 0;
+    if (!ok) break;
+    pending = false;
+    phase ^= 1u;
+    tc_fence_after();
+    float v[64];
+    tmem_ld64(tmem + (uint32_t(warp * 32) << 16), v);
+    if (row < nc) {
+      __align__(16) __nv_bfloat16 o[64];
+#pragma unroll
+      for (int j = 0; j < 64; ++j) {
+        const float zz = v[j] + sbias[j];
+        v[j] = zz;
+        o[j] = __float2bfloat16_rn(gelu(zz));
+      }
+      if (z) {
+        float4* zo = reinterpret_cast<float4*>(z + row * W);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) zo[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+      }
+      uint4* ho = reinterpret_cast<uint4*>(hout + row * W);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) ho[j] = reinterpret_cast<uint4*>(o)[j];
+    }
+    // tensor memory and the A tile are reused by the next tile
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
   }
+  if (!ok) {
+    if (tid == 0) atomicOr(err, 2);
+    if (pending) mbar_wait_bounded(mbar, phase);  // let the MMAs in flight finish
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(uint32_t(TC_COLS))
+                 : "memory");
 }
 
 __global__ void __launch_bounds__(GT) k_head_forward(int64_t nc, const __nv_bfloat16* __restrict__ wo,
                                                      const __nv_bfloat16* __restrict__ bo,
-                                                     const float* __restrict__ h, float* __restrict__ y) {
+                                                     const __nv_bfloat16* __restrict__ h, float* __restrict__ y) {
   __shared__ float sw[NOUT * W], sb[NOUT];
   for (int i = threadIdx.x; i < NOUT * W; i += GT) sw[i] = __bfloat162float(wo[i]);
   if (threadIdx.x < NOUT) sb[threadIdx.x] = __bfloat162float(bo[threadIdx.x]);
@@ -170,7 +350,7 @@ __global__ void __launch_bounds__(GT) k_head_forward(int64_t nc, const __nv_bflo
 #pragma unroll
   for (int k = 0; k < NOUT; ++k) acc[k] = sb[k];
   for (int i = 0; i < W; ++i) {
-    const float hv = h[c * W + i];
+    const float hv = __bfloat162float(h[c * W + i]);
 #pragma unroll
     for (int k = 0; k < NOUT; ++k) acc[k] += sw[k * W + i] * hv;
   }
@@ -239,10 +419,12 @@ __global__ void k_loss_final(const double* __restrict__ part, int nblk, double* 
 }
 
 // weight-gradient partials over blocks of RB cells:
-// part[blk][j][i] = sum_c dz[c][j] * a[c][i]   (a = h or agg), and bias sums
+// part[blk][j][i] = sum_c dz[c][j] * a[c][i]   (a = h or agg, as the forward
+// GEMM used it), and bias sums
 constexpr int RB = 256;
+template <class TA>
 __global__ void k_wgrad_partial(int64_t nc, int nout, int fin, const float* __restrict__ dz,
-                                const float* __restrict__ a, float* __restrict__ part) {
+                                const TA* __restrict__ a, float* __restrict__ part) {
   const int64_t c0 = int64_t(blockIdx.x) * RB;
   const int64_t c1 = min(nc, c0 + RB);
   float* o = part + int64_t(blockIdx.x) * nout * (fin + 1);
@@ -250,7 +432,7 @@ __global__ void k_wgrad_partial(int64_t nc, int nout, int fin, const float* __re
     const int j = w / (fin + 1), i = w % (fin + 1);
     float s = 0.f;
     if (i < fin) {
-      for (int64_t c = c0; c < c1; ++c) s += dz[c * nout + j] * a[c * fin + i];
+      for (int64_t c = c0; c < c1; ++c) s += dz[c * nout + j] * as_operand(a[c * fin + i]);
     } else {
       for (int64_t c = c0; c < c1; ++c) s += dz[c * nout + j];
     }
@@ -396,22 +578,42 @@ __global__ void k_features_norm(int64_t nc, const float* __restrict__ raw, const
 
 inline unsigned nb_(int64_t n, int t) { return unsigned((n + t - 1) / t); }
 
-// forward over the whole graph from features; returns head output in m->d_y
-int forward(fpsi_gnn* m, const Graph& G, const float* feat) {
+// forward over the whole graph from features; returns head output in
+// m->d_y.  keep_z stores the FP32 pre-activations the backward pass needs.
+int forward(fpsi_gnn* m, const Graph& G, const float* feat, bool keep_z) {
   cudaStream_t s = m->stream;
   const int64_t nc = G.nc;
-  const float* h = feat;
+  const int64_t ntiles = (nc + TC_ROWS - 1) / TC_ROWS;
+  const unsigned grid = unsigned(std::max<int64_t>(1, std::min<int64_t>(ntiles, 2 * int64_t(m->nsm))));
   for (int l = 0; l < NLAYER; ++l) {
     const int fin = m->L.fan_in[l];
-    k_aggregate<<<nb_(nc * fin, 256), 256, 0, s>>>(nc, fin, G.off, G.nb, h, m->d_agg[l]);
-    k_mp_forward<<<nb_(nc, GT), GT, 0, s>>>(nc, fin, m->d_wb + m->L.ws[l], m->d_wb + m->L.wn[l],
-                                            m->d_wb + m->L.b[l], h, m->d_agg[l], m->d_z[l],
-                                            m->d_h[l + 1]);
-    h = m->d_h[l + 1];
+    const __nv_bfloat16 *ws = m->d_wb + m->L.ws[l], *wn = m->d_wb + m->L.wn[l], *b = m->d_wb + m->L.b[l];
+    float* z = keep_z ? m->d_z[l] : nullptr;
+    if (l == 0) {
+      k_aggregate<float><<<nb_(nc * fin, 256), 256, 0, s>>>(nc, fin, G.off, G.nb, feat, m->d_agg[l]);
+      k_mp_tc<float><<<grid, TC_ROWS, tc_smem_bytes(fin), s>>>(nc, fin, feat, m->d_agg[l], ws, wn, b, z,
+                                                               m->d_h[l + 1], m->d_err);
+    } else {
+      k_aggregate<__nv_bfloat16><<<nb_(nc * fin, 256), 256, 0, s>>>(nc, fin, G.off, G.nb, m->d_h[l],
+                                                                    m->d_agg[l]);
+      k_mp_tc<__nv_bfloat16><<<grid, TC_ROWS, tc_smem_bytes(fin), s>>>(nc, fin, m->d_h[l], m->d_agg[l], ws,
+                                                                       wn, b, z, m->d_h[l + 1], m->d_err);
+    }
   }
-  k_head_forward<<<nb_(nc, GT), GT, 0, s>>>(nc, m->d_wb + m->L.wo, m->d_wb + m->L.bo, h, m->d_y);
+  k_head_forward<<<nb_(nc, GT), GT, 0, s>>>(nc, m->d_wb + m->L.wo, m->d_wb + m->L.bo, m->d_h[NLAYER], m->d_y);
   FPSI_CUDA_TRY(cudaGetLastError());
   return FPSI_OK;
+}
+
+// after the stream is synchronised: a tensor-core wait that gave up is an
+// error of the pass (flag cleared for the next one)
+int take_error(fpsi_gnn* m) {
+  int32_t e = 0;
+  FPSI_CUDA_TRY(cudaMemcpy(&e, m->d_err, sizeof(e), cudaMemcpyDeviceToHost));
+  if (!e) return FPSI_OK;
+  FPSI_CUDA_TRY(cudaMemset(m->d_err, 0, sizeof(int32_t)));
+  fpsi::set_error("learned start: a tensor-core wait timed out");
+  return FPSI_E_TIMEOUT;
 }
 
 // loss over the batch and full gradient into m->d_g; loss_out (device) [2]
@@ -426,17 +628,19 @@ int backward(fpsi_gnn* m, const Graph& G, const float* feat, const float* target
   k_scale<<<nb_(nc * NOUT, 256), 256, 0, s>>>(nc * NOUT, dy, loss_out);
   const int rb = int(nb_(nc, RB));
   // head
-  k_wgrad_partial<<<rb, 256, 0, s>>>(nc, NOUT, W, dy, m->d_h[NLAYER], m->d_part);
+  k_wgrad_partial<__nv_bfloat16><<<rb, 256, 0, s>>>(nc, NOUT, W, dy, m->d_h[NLAYER], m->d_part);
   k_wgrad_reduce<<<nb_(NOUT * (W + 1), 256), 256, 0, s>>>(rb, NOUT, W, m->d_part, m->d_g, m->L.wo, m->L.bo);
   k_back_dense<<<nb_(nc, GT), GT, 0, s>>>(nc, NOUT, W, m->d_wb + m->L.wo, dy, m->d_dh);
   for (int l = NLAYER - 1; l >= 0; --l) {
     const int fin = m->L.fan_in[l];
-    const float* hin = l == 0 ? feat : m->d_h[l];
     k_back_gelu<<<nb_(nc * W, 256), 256, 0, s>>>(nc * W, m->d_dh, m->d_z[l], m->d_dz);
-    k_wgrad_partial<<<rb, 256, 0, s>>>(nc, W, fin, m->d_dz, hin, m->d_part);
+    if (l == 0)
+      k_wgrad_partial<float><<<rb, 256, 0, s>>>(nc, W, fin, m->d_dz, feat, m->d_part);
+    else
+      k_wgrad_partial<__nv_bfloat16><<<rb, 256, 0, s>>>(nc, W, fin, m->d_dz, m->d_h[l], m->d_part);
     k_wgrad_reduce<<<nb_(W * (fin + 1), 256), 256, 0, s>>>(rb, W, fin, m->d_part, m->d_g, m->L.ws[l],
                                                           m->L.b[l]);
-    k_wgrad_partial<<<rb, 256, 0, s>>>(nc, W, fin, m->d_dz, m->d_agg[l], m->d_part);
+    k_wgrad_partial<__nv_bfloat16><<<rb, 256, 0, s>>>(nc, W, fin, m->d_dz, m->d_agg[l], m->d_part);
     k_wgrad_reduce<<<nb_(W * (fin + 1), 256), 256, 0, s>>>(rb, W, fin, m->d_part, m->d_g, m->L.wn[l], -1);
     if (l > 0) {
       // dh_in = Ws^T dz + scatter(Wn^T dz)
@@ -473,7 +677,8 @@ void free_activations(fpsi_gnn* m) {
   for (int l = 0; l < NLAYER; ++l) {
     if (m->d_agg[l]) cudaFree(m->d_agg[l]);
     if (m->d_z[l]) cudaFree(m->d_z[l]);
-    m->d_agg[l] = m->d_z[l] = nullptr;
+    m->d_agg[l] = nullptr;
+    m->d_z[l] = nullptr;
   }
   m->cap = 0;
 }
@@ -568,7 +773,19 @@ int fpsi_gnn_create(fpsi_gnn** out, uint64_t seed) {
   G(galloc(&m->d_v, np));
   G(galloc(&m->d_g, np));
   G(galloc(&m->d_wb, np));
+  G(galloc(&m->d_err, 1));
 #undef G
+  if (!rc && cudaMemset(m->d_err, 0, sizeof(int32_t)) != cudaSuccess) rc = FPSI_E_CUDA;
+  int dev = 0;
+  if (!rc && (cudaGetDevice(&dev) != cudaSuccess ||
+              cudaDeviceGetAttribute(&m->nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+              cudaFuncSetAttribute(k_mp_tc<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(tc_smem_bytes(W))) != cudaSuccess ||
+              cudaFuncSetAttribute(k_mp_tc<__nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(tc_smem_bytes(W))) != cudaSuccess)) {
+    fpsi::set_error("learned start: device query failed");
+    rc = FPSI_E_CUDA;
+  }
   if (rc) {
     fpsi_gnn_destroy(m);
     return rc;
@@ -612,7 +829,7 @@ int fpsi_gnn_destroy(fpsi_gnn* m) {
   if (!m) return FPSI_OK;
   fpsi_gnn_clear_snapshots(m);
   free_activations(m);
-  void* ps[] = {m->d_w, m->d_m, m->d_v, m->d_g, m->d_wb};
+  void* ps[] = {m->d_w, m->d_m, m->d_v, m->d_g, m->d_wb, m->d_err};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (m->stream) cudaStreamDestroy(m->stream);
@@ -787,13 +1004,14 @@ int fpsi_gnn_loss_grad(fpsi_gnn* m, int32_t si, int64_t batch, uint64_t seed, do
   if (!m || si < 0 || si >= int32_t(m->snaps.size())) return FPSI_E_INVALID;
   const Snapshot& s = m->snaps[si];
   int rc = ensure_capacity(m, s.nc);
-  if (!rc) rc = forward(m, s.graph(), s.feat);
+  if (!rc) rc = forward(m, s.graph(), s.feat, true);
   if (rc) return rc;
   double* dl = m->d_lpart + ((s.nc + GT - 1) / GT) * 2 + 2;
   if ((rc = backward(m, s.graph(), s.feat, s.target, seed, threshold(s.nc, batch), dl))) return rc;
   double h[2];
   FPSI_CUDA_TRY(cudaMemcpyAsync(h, dl, sizeof(h), cudaMemcpyDeviceToHost, m->stream));
   FPSI_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  if ((rc = take_error(m))) return rc;
   if (loss) *loss = h[0];
   if (grad) FPSI_CUDA_TRY(cudaMemcpy(grad, m->d_g, m->L.total * 4, cudaMemcpyDeviceToHost));
   return FPSI_OK;
@@ -814,7 +1032,7 @@ int fpsi_gnn_train(fpsi_gnn* m, int32_t nsteps, int64_t batch, uint64_t seed, do
     const uint64_t sd = seed * 1000003ull + uint64_t(it);
     const Snapshot& s = m->snaps[size_t(sd % uint64_t(ns))];
     double* dl = m->d_lpart + ((s.nc + GT - 1) / GT) * 2 + 2;
-    int rc = forward(m, s.graph(), s.feat);
+    int rc = forward(m, s.graph(), s.feat, true);
     if (!rc) rc = backward(m, s.graph(), s.feat, s.target, sd, threshold(s.nc, batch), dl);
     if (rc) {
       cudaFree(dhist);
@@ -834,7 +1052,7 @@ int fpsi_gnn_train(fpsi_gnn* m, int32_t nsteps, int64_t batch, uint64_t seed, do
   }
   FPSI_CUDA_TRY(cudaStreamSynchronize(m->stream));
   cudaFree(dhist);
-  return FPSI_OK;
+  return take_error(m);
 }
 
 }  // extern "C"
@@ -875,7 +1093,7 @@ int fpsi_gnn_predict(fpsi_gnn* m, fpsi_ctx* x, double* x0) {
     return rc;
   }
   rc = make_features(m, x, fbuf, xjb, rs, xs);
-  if (!rc) rc = forward(m, G, fbuf);
+  if (!rc) rc = forward(m, G, fbuf, false);
   double* dx0 = nullptr;
   if (!rc && x0) rc = galloc(&dx0, nc * 5);
   if (!rc) {
@@ -888,6 +1106,7 @@ int fpsi_gnn_predict(fpsi_gnn* m, fpsi_ctx* x, double* x0) {
       k_apply_start<double><<<nb_(nc, 256), 256, 0, m->stream>>>(nc, xjb, m->d_y, dscl, x->d_ci,
                                                                 (double*)x->d_x, dx0);
     if (cudaStreamSynchronize(m->stream) != cudaSuccess) rc = FPSI_E_CUDA;
+    if (!rc) rc = take_error(m);
   }
   if (!rc && x0) {
     std::vector<double> h(nc * 5);

@@ -123,7 +123,8 @@ class GeneratedMesh:
         return [c.copy() for c in cols]
 
     def __del__(self):
-        if getattr(self, "_p", None):
+        # at interpreter exit the module globals may already be gone
+        if getattr(self, "_p", None) and N is not None and N.lib is not None:
             N.lib().fpsi_mesh_free(self._p)
             self._p = None
 

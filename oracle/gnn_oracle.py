@@ -1,8 +1,10 @@
 """CPU oracle of the learned-start network (torch CPU autograd).
 
 TEST INFRASTRUCTURE: restates the network of flowpsi_b200/csrc/gnn.cu in
-torch on the CPU, with the same BF16-rounded weights and FP32 arithmetic,
-to check the device's loss and gradients.
+torch on the CPU, with the same BF16-rounded weights, the same BF16
+rounding of the layer inputs (features, neighbour means and hidden
+activations; gradients pass straight through the rounding) and FP32
+arithmetic, to check the device's loss and gradients.
 """
 from __future__ import annotations
 
@@ -44,13 +46,18 @@ def neighbour_mean_matrix(nc: int, cl: np.ndarray, cr: np.ndarray) -> torch.Tens
     return torch.sparse_coo_tensor(np.vstack([rows, cols]), vals, (nc, nc)).coalesce()
 
 
+def bf16(x: torch.Tensor) -> torch.Tensor:
+    """round to BF16 in the forward pass, identity in the backward pass"""
+    return x + (x.to(torch.bfloat16).to(torch.float32) - x).detach()
+
+
 def loss_and_grad(w: np.ndarray, feat: np.ndarray, target: np.ndarray, A: torch.Tensor):
     flat, p = unpack(w)
     h = torch.from_numpy(np.ascontiguousarray(feat, np.float32))
     for l in range(NLAYER):
         ws, wn, b = p[3 * l], p[3 * l + 1], p[3 * l + 2]
-        agg = torch.sparse.mm(A, h)
-        h = torch.nn.functional.gelu(h @ ws.T + agg @ wn.T + b)
+        agg = bf16(torch.sparse.mm(A, h))  # mean of the layer input, rounded
+        h = bf16(torch.nn.functional.gelu(bf16(h) @ ws.T + agg @ wn.T + b))
     y = h @ p[-2].T + p[-1]
     t = torch.from_numpy(np.ascontiguousarray(target, np.float32))
     loss = ((y - t) ** 2).mean()

@@ -3,8 +3,15 @@ replica (oracle/gnn_oracle.py), and what the trained network gains over the
 reference's block Jacobi start (linearSolverSGS.loci:57-69).  GPU only.
 
 Tolerances: features exact to FP32 rounding (1e-5 relative); loss 1e-5
-relative; gradients per parameter group 1e-4 of the group's largest entry
-(FP32 sums in a different order, BF16 weights on both sides).
+relative; gradients per parameter group within 1e-3 of the group's norm
+and 3e-3 of its largest entry.  Both sides use BF16 weights and BF16 layer
+inputs with FP32 sums, but in a different order: the tensor cores' sums
+differ from the CPU's by about 1e-6 relative, which rounds some activations
+to the neighbouring BF16 value (one part in 256).  Replaying the CPU network
+with its pre-activations scaled by 1 + 1e-6 N(0,1) moves the loss by up to
+4e-6 and single gradient groups by up to 1.7e-4 of their norm on the
+216-cell grid; a wrong operand, a missing rounding or a wrong bias moves
+them by 1e-3 or more.
 """
 import numpy as np
 import pytest
@@ -105,7 +112,8 @@ def test_loss_and_gradient_match_autograd(need_gpu, mesh):
     assert abs(loss - loss_o) <= 1e-5 * loss_o
     for name, lo, hi in G.groups():
         go, gg = grad_o[lo:hi], grad[lo:hi]
-        assert np.abs(gg - go).max() <= 1e-4 * np.abs(go).max() + 1e-12, name
+        assert np.linalg.norm(gg - go) <= 1e-3 * np.linalg.norm(go) + 1e-12, name
+        assert np.abs(gg - go).max() <= 3e-3 * np.abs(go).max() + 1e-12, name
 
 
 def test_minibatch_gradient_is_the_batch_mean(need_gpu):
