@@ -115,27 +115,9 @@ __device__ __forceinline__ float gelu_grad(float x) {
   return cdf + x * pdf;
 }
 
-__device__ __forceinline__ float to_f(float v) { return v; }
-__device__ __forceinline__ float to_f(__nv_bfloat16 v) { return __bfloat162float(v); }
 // a layer input as the tensor cores multiply it (FP32 features rounded to BF16)
 __device__ __forceinline__ float as_operand(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
 __device__ __forceinline__ float as_operand(__nv_bfloat16 v) { return __bfloat162float(v); }
-
-// agg[c] = mean over neighbours of h[n] (width fin), summed in FP32 and
-// rounded to BF16
-template <class TIn>
-__global__ void k_aggregate(int64_t nc, int fin, const int32_t* __restrict__ off,
-                            const int32_t* __restrict__ nb, const TIn* __restrict__ h,
-                            __nv_bfloat16* __restrict__ agg) {
-  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= nc * fin) return;
-  const int64_t c = i / fin;
-  const int k = int(i % fin);
-  const int32_t a = off[c], b = off[c + 1];
-  float s = 0.f;
-  for (int32_t e = a; e < b; ++e) s += to_f(h[int64_t(nb[e]) * fin + k]);
-  agg[i] = __float2bfloat16_rn(b > a ? s / float(b - a) : 0.f);
-}
 
 // ---- tcgen05 helpers (single-CTA MMA, no multicast) ----------------------
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -182,68 +164,132 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   }
   return false;
 }
-// this warp's 32 lanes x 64 FP32 columns of the accumulator
-__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float* v) {
-  uint32_t r[64];
+// 32 lanes x 32 FP32 columns of the accumulator for this warp
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
-      "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, "
-      "%32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, "
-      "%51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];\n"
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+      "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+      "[%32];\n"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
         "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
         "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
         "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
-        "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]),
-        "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]),
-        "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]),
-        "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]),
-        "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+        "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
       : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-  for (int j = 0; j < 64; ++j) v[j] = __uint_as_float(r[j]);
+  for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
 }
 
-constexpr int TC_ROWS = 128;  // cells per tile (the MMA's M)
-constexpr int TC_COLS = 64;   // tensor-memory columns held per CTA (the MMA's N)
-// dynamic shared memory of k_mp_tc for input width fin
-inline size_t tc_smem_bytes(int fin) {
-  const int nch = 2 * fin / 8;  // 16 B chunks of one operand row
-  return size_t(nch) * TC_ROWS * 16 + size_t(nch) * W * 16 + 16 + W * sizeof(float);
+// 8 consecutive elements of a layer input (one 16 B operand chunk), held
+// as loaded so that many loads can be in flight before they are used
+template <class T>
+struct Chunk8;
+template <>
+struct Chunk8<__nv_bfloat16> {
+  uint4 u;
+  __device__ __forceinline__ void load(const __nv_bfloat16* p) { u = __ldg(reinterpret_cast<const uint4*>(p)); }
+  __device__ __forceinline__ void get(float* v) const {
+    const __nv_bfloat162* q = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float2 f = __bfloat1622float2(q[k]);
+      v[2 * k] = f.x;
+      v[2 * k + 1] = f.y;
+    }
+  }
+};
+template <>
+struct Chunk8<float> {
+  float4 a, b;
+  __device__ __forceinline__ void load(const float* p) {
+    a = __ldg(reinterpret_cast<const float4*>(p));
+    b = __ldg(reinterpret_cast<const float4*>(p) + 1);
+  }
+  __device__ __forceinline__ void get(float* v) const {
+    v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+  }
+};
+__device__ __forceinline__ uint4 pack8(const float* v) {
+  uint4 u;
+  __nv_bfloat162* q = reinterpret_cast<__nv_bfloat162*>(&u);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) q[k] = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
+  return u;
 }
 
-// One message-passing layer on the tensor cores, persistent over 128-cell
-// tiles:  z = [h | agg] [Ws | Wn]^T + b  (BF16 operands, FP32 accumulate in
-// tensor memory), out = GELU(z) in BF16, z kept in FP32 when asked.
+constexpr int TC_ROWS = 128;     // cells per tile (the MMA's M)
+constexpr int TC_COLS = 64;      // tensor-memory columns held per CTA (the MMA's N)
+constexpr int TC_THREADS = 256;  // 8 warps: two per accumulator lane quarter
+constexpr int TC_OSTRIDE = 144;  // bytes per row of the staged BF16 output tile (128 + 16 pad)
+constexpr int NB_FAST = 6;       // neighbours per cell gathered with all loads in flight
+
+struct TcSmem {  // byte offsets of the layer kernel's dynamic shared memory
+  size_t a, b, o, y, wo, bar, slot, bias, total;
+};
+__host__ __device__ inline TcSmem tc_smem(int fin) {
+  const size_t nch = size_t(2 * fin / 8);  // 16 B chunks of one operand row
+  TcSmem s;
+  s.a = 0;
+  s.b = s.a + nch * TC_ROWS * 16;
+  s.o = s.b + nch * W * 16;
+  s.y = s.o + size_t(TC_ROWS) * TC_OSTRIDE;
+  s.wo = s.y + size_t(TC_ROWS) * 8 * sizeof(float);
+  s.bar = s.wo + size_t(NOUT * W + 8) * sizeof(float);
+  s.slot = s.bar + 8;
+  s.bias = s.slot + 8;
+  s.total = s.bias + W * sizeof(float);
+  return s;
+}
+
+// One message-passing layer, aggregation included, on the tensor cores,
+// persistent over 128-cell tiles:
+//   A = [h | mean over graph neighbours of h]   (BF16, staged from global)
+//   z = A [Ws | Wn]^T + b                         (tcgen05, FP32 in tensor memory)
+//   h_out = BF16(GELU(z))
+// and, for the last layer, the head y = Wo h_out + bo.  z, the neighbour
+// means and h_out are written only where the caller asks (training keeps
+// them for the backward pass).
 // Operands sit in shared memory chunk-major: chunk c (8 K-elements, 16 B)
 // of row r at (c * rows + r) * 16, so one MMA (K = 16) reads chunks 2s and
 // 2s+1 with SBO = 128 B and LBO = rows * 16 B.  fin is 40 or 64 (K = 80 or
-// 128, whole 16-element steps).  Every wait is bounded; a wait that gives
-// up sets bit 1 of err, waits once more for the MMAs in flight and frees the
-// tensor memory.
-template <class TIn>
-__global__ void __launch_bounds__(TC_ROWS, 1)
-k_mp_tc(int64_t nc, int fin, const TIn* __restrict__ h, const __nv_bfloat16* __restrict__ agg,
-        const __nv_bfloat16* __restrict__ ws, const __nv_bfloat16* __restrict__ wn,
-        const __nv_bfloat16* __restrict__ bias, float* __restrict__ z,
-        __nv_bfloat16* __restrict__ hout, int32_t* __restrict__ err) {
+// 128).  Staging: warp w fills rows 16w..16w+15, lane = (row 0..7, chunk
+// group 0..3); the epilogue's warp w reads accumulator lanes 32(w%4).. and
+// columns 32(w/4)...  Every wait is bounded; a wait that gives up sets bit 1
+// of err, waits once more for the MMAs in flight and frees the tensor memory.
+template <class TIn, bool HEAD>
+__global__ void __launch_bounds__(TC_THREADS, 2)
+k_layer_tc(int64_t nc, int fin, const TIn* __restrict__ h, const int32_t* __restrict__ off,
+           const int32_t* __restrict__ nb, const __nv_bfloat16* __restrict__ ws,
+           const __nv_bfloat16* __restrict__ wn, const __nv_bfloat16* __restrict__ bias,
+           const __nv_bfloat16* __restrict__ wo, const __nv_bfloat16* __restrict__ bo,
+           __nv_bfloat16* __restrict__ agg_out, float* __restrict__ z, __nv_bfloat16* __restrict__ hout,
+           float* __restrict__ y, int32_t* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char tsm[];
+  const TcSmem L = tc_smem(fin);
   const int nch = 2 * fin / 8, hch = fin / 8;
-  unsigned char* sA = tsm;
-  unsigned char* sB = tsm + size_t(nch) * TC_ROWS * 16;
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(sB + size_t(nch) * W * 16);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
-  float* sbias = reinterpret_cast<float*>(mbar + 2);
-  const int tid = threadIdx.x, warp = tid >> 5;
+  unsigned char* sA = tsm + L.a;
+  unsigned char* sB = tsm + L.b;
+  unsigned char* sO = tsm + L.o;
+  float* sY = reinterpret_cast<float*>(tsm + L.y);
+  float* sWo = reinterpret_cast<float*>(tsm + L.wo);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(tsm + L.bar);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(tsm + L.slot);
+  float* sbias = reinterpret_cast<float*>(tsm + L.bias);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   // B = [Ws | Wn]: row j (output feature), chunk c of 8 elements
-  for (int idx = tid; idx < W * nch; idx += TC_ROWS) {
+  for (int idx = tid; idx < W * nch; idx += TC_THREADS) {
     const int j = idx / nch, c = idx - nch * (idx / nch);
     const __nv_bfloat16* src = c < hch ? ws + j * fin + 8 * c : wn + j * fin + 8 * (c - hch);
     *reinterpret_cast<uint4*>(sB + (size_t(c) * W + j) * 16) = *reinterpret_cast<const uint4*>(src);
   }
   if (tid < W) sbias[tid] = __bfloat162float(bias[tid]);
+  if (HEAD) {
+    for (int i = tid; i < NOUT * W; i += TC_THREADS) sWo[i] = __bfloat162float(wo[i]);
+    if (tid < NOUT) sWo[NOUT * W + tid] = __bfloat162float(bo[tid]);
+  }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
                  "r"(uint32_t(TC_COLS))
@@ -262,29 +308,87 @@ k_mp_tc(int64_t nc, int fin, const TIn* __restrict__ h, const __nv_bfloat16* __r
   uint32_t phase = 0;
   bool ok = true, pending = false;
   const int64_t ntiles = (nc + TC_ROWS - 1) / TC_ROWS;
+  const int rs = lane & 7, cg = lane >> 3;     // staging: row within 8, chunk group
+  const int q = warp & 3, hf = warp >> 2;      // epilogue: lane quarter, column half
+  constexpr int CPI = sizeof(TIn) == 2 ? 2 : 1;  // chunks of a row gathered together
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const int64_t row = t * TC_ROWS + tid;
-    // A row tid = [bf16(h[row]) | agg[row]]
-    if (row < nc) {
-      const TIn* hr = h + row * fin;
-      for (int c = 0; c < hch; ++c) {
-        __align__(16) __nv_bfloat16 v[8];
+    const int64_t row0 = t * TC_ROWS;
+    // ---- stage A = [h | neighbour mean] for rows 16 warp .. 16 warp + 15.
+    // The row bounds and the first NB_FAST neighbour ids of both rows are
+    // loaded first, then every chunk of a row at once, so that each lane has
+    // up to 2 (NB_FAST + 1) loads in flight.
+    int32_t e0[2], e1[2], nbi[2][NB_FAST];
 #pragma unroll
-        for (int e = 0; e < 8; ++e) v[e] = __float2bfloat16_rn(to_f(hr[8 * c + e]));
-        *reinterpret_cast<uint4*>(sA + (size_t(c) * TC_ROWS + tid) * 16) = *reinterpret_cast<uint4*>(v);
+    for (int p = 0; p < 2; ++p) {
+      const int64_t cell = row0 + 16 * warp + 8 * p + rs;
+      e0[p] = e1[p] = 0;
+      if (cell < nc) {
+        e0[p] = __ldg(off + cell);
+        e1[p] = __ldg(off + cell + 1);
       }
-      const __nv_bfloat16* ar = agg + row * fin;
-      for (int c = 0; c < hch; ++c)
-        *reinterpret_cast<uint4*>(sA + (size_t(hch + c) * TC_ROWS + tid) * 16) =
-            *reinterpret_cast<const uint4*>(ar + 8 * c);
-    } else {
-      for (int c = 0; c < nch; ++c)
-        *reinterpret_cast<uint4*>(sA + (size_t(c) * TC_ROWS + tid) * 16) = make_uint4(0, 0, 0, 0);
+    }
+#pragma unroll
+    for (int p = 0; p < 2; ++p)
+#pragma unroll
+      for (int k = 0; k < NB_FAST; ++k) nbi[p][k] = e0[p] + k < e1[p] ? __ldg(nb + e0[p] + k) : -1;
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      const int r = 16 * warp + 8 * p + rs;
+      const int64_t cell = row0 + r;
+      if (cell < nc) {
+        const float inv = e1[p] > e0[p] ? 1.0f / float(e1[p] - e0[p]) : 0.f;
+#pragma unroll 1
+        for (int c = cg; c < hch; c += 4 * CPI) {
+          // chunks c + 4 i, i < CPI, of the row and of its neighbours
+          Chunk8<TIn> own[CPI], u[NB_FAST][CPI];
+#pragma unroll
+          for (int i = 0; i < CPI; ++i)
+            if (c + 4 * i < hch) own[i].load(h + cell * fin + 8 * (c + 4 * i));
+#pragma unroll
+          for (int k = 0; k < NB_FAST; ++k)
+#pragma unroll
+            for (int i = 0; i < CPI; ++i)
+              if (nbi[p][k] >= 0 && c + 4 * i < hch) u[k][i].load(h + int64_t(nbi[p][k]) * fin + 8 * (c + 4 * i));
+#pragma unroll
+          for (int i = 0; i < CPI; ++i) {
+            const int ci = c + 4 * i;
+            if (ci >= hch) break;
+            float v[8], sum[8];
+            own[i].get(v);
+            *reinterpret_cast<uint4*>(sA + (size_t(ci) * TC_ROWS + r) * 16) = pack8(v);
+#pragma unroll
+            for (int q8 = 0; q8 < 8; ++q8) sum[q8] = 0.f;
+#pragma unroll
+            for (int k = 0; k < NB_FAST; ++k)
+              if (nbi[p][k] >= 0) {
+                u[k][i].get(v);
+#pragma unroll
+                for (int q8 = 0; q8 < 8; ++q8) sum[q8] += v[q8];
+              }
+            for (int32_t e = e0[p] + NB_FAST; e < e1[p]; ++e) {  // cells with many neighbours
+              Chunk8<TIn> x;
+              x.load(h + int64_t(__ldg(nb + e)) * fin + 8 * ci);
+              x.get(v);
+#pragma unroll
+              for (int q8 = 0; q8 < 8; ++q8) sum[q8] += v[q8];
+            }
+#pragma unroll
+            for (int q8 = 0; q8 < 8; ++q8) sum[q8] *= inv;
+            const uint4 m = pack8(sum);
+            *reinterpret_cast<uint4*>(sA + (size_t(hch + ci) * TC_ROWS + r) * 16) = m;
+            if (agg_out) *reinterpret_cast<uint4*>(agg_out + cell * fin + 8 * ci) = m;
+          }
+        }
+      } else {
+        for (int c = cg; c < nch; c += 4)
+          *reinterpret_cast<uint4*>(sA + (size_t(c) * TC_ROWS + r) * 16) = make_uint4(0, 0, 0, 0);
+      }
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    // ---- z = A B^T on the tensor cores
     if (tid == 0) {
       for (int st = 0; st < nch / 2; ++st) {
         const uint64_t ad = umma_desc(sA + size_t(2 * st) * TC_ROWS * 16, TC_ROWS * 16, 128);
@@ -295,39 +399,67 @@ k_mp_tc(int64_t nc, int fin, const TIn* __restrict__ h, const __nv_bfloat16* __r
     }
     pending = true;
     __syncwarp();
-    const bool got = mbar_wait_bounded(mbar, phase);
+    // warp 0 polls the barrier, the others wait at the thread barrier
+    const bool got = warp == 0 ? mbar_wait_bounded(mbar, phase) : true;
     ok = __syncthreads_and(got) != 0;
     if (!ok) break;
     pending = false;
     phase ^= 1u;
     tc_fence_after();
-    float v[64];
-    tmem_ld64(tmem + (uint32_t(warp * 32) << 16), v);
-    if (row < nc) {
-      __align__(16) __nv_bfloat16 o[64];
+    // ---- epilogue: row 32 q + lane, columns 32 hf .. 32 hf + 31
+    const int r = 32 * q + lane;
+    const int64_t cell = row0 + r;
+    float v[32];
+    tmem_ld32(tmem + (uint32_t(32 * q) << 16) + uint32_t(32 * hf), v);
 #pragma unroll
-      for (int j = 0; j < 64; ++j) {
-        const float zz = v[j] + sbias[j];
-        v[j] = zz;
-        o[j] = __float2bfloat16_rn(gelu(zz));
-      }
-      if (z) {
-        float4* zo = reinterpret_cast<float4*>(z + row * W);
+    for (int j = 0; j < 32; ++j) v[j] += sbias[32 * hf + j];
+    if (z && cell < nc) {
+      float4* zo = reinterpret_cast<float4*>(z + cell * W + 32 * hf);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) zo[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
-      }
-      uint4* ho = reinterpret_cast<uint4*>(hout + row * W);
-#pragma unroll
-      for (int j = 0; j < 8; ++j) ho[j] = reinterpret_cast<uint4*>(o)[j];
+      for (int j = 0; j < 8; ++j) zo[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
     }
-    // tensor memory and the A tile are reused by the next tile
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = __bfloat162float(__float2bfloat16_rn(gelu(v[j])));
+    if (hout) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        *reinterpret_cast<uint4*>(sO + size_t(r) * TC_OSTRIDE + 64 * hf + 16 * j) = pack8(v + 8 * j);
+    }
+    if (HEAD) {
+      float yp[NOUT];
+#pragma unroll
+      for (int k = 0; k < NOUT; ++k) {
+        float s = 0.f;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) s += sWo[k * W + 32 * hf + j] * v[j];
+        yp[k] = s;
+      }
+      if (hf == 1)
+#pragma unroll
+        for (int k = 0; k < NOUT; ++k) sY[r * 8 + k] = yp[k];
+      __syncthreads();
+      if (hf == 0 && cell < nc)
+#pragma unroll
+        for (int k = 0; k < NOUT; ++k) y[cell * NOUT + k] = (yp[k] + sY[r * 8 + k]) + sWo[NOUT * W + k];
+    }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    // ---- coalesced copy of the BF16 output tile
+    if (hout) {
+      const int64_t nrow = nc - row0 < TC_ROWS ? nc - row0 : int64_t(TC_ROWS);
+      for (int idx = tid; idx < TC_ROWS * 8; idx += TC_THREADS) {
+        const int rr = idx >> 3, c16 = idx & 7;
+        if (rr < nrow)
+          *reinterpret_cast<uint4*>(hout + (row0 + rr) * W + 8 * c16) =
+              *reinterpret_cast<const uint4*>(sO + size_t(rr) * TC_OSTRIDE + 16 * c16);
+      }
+    }
+    // sO is rewritten only after the next tile's staging barrier
   }
   if (!ok) {
     if (tid == 0) atomicOr(err, 2);
-    if (pending) mbar_wait_bounded(mbar, phase);  // let the MMAs in flight finish
+    if (pending && warp == 0) mbar_wait_bounded(mbar, phase);  // let the MMAs in flight finish
   }
   tc_fence_before();
   __syncthreads();
@@ -335,27 +467,6 @@ k_mp_tc(int64_t nc, int fin, const TIn* __restrict__ h, const __nv_bfloat16* __r
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(uint32_t(TC_COLS))
                  : "memory");
-}
-
-__global__ void __launch_bounds__(GT) k_head_forward(int64_t nc, const __nv_bfloat16* __restrict__ wo,
-                                                     const __nv_bfloat16* __restrict__ bo,
-                                                     const __nv_bfloat16* __restrict__ h, float* __restrict__ y) {
-  __shared__ float sw[NOUT * W], sb[NOUT];
-  for (int i = threadIdx.x; i < NOUT * W; i += GT) sw[i] = __bfloat162float(wo[i]);
-  if (threadIdx.x < NOUT) sb[threadIdx.x] = __bfloat162float(bo[threadIdx.x]);
-  __syncthreads();
-  const int64_t c = int64_t(blockIdx.x) * GT + threadIdx.x;
-  if (c >= nc) return;
-  float acc[NOUT];
-#pragma unroll
-  for (int k = 0; k < NOUT; ++k) acc[k] = sb[k];
-  for (int i = 0; i < W; ++i) {
-    const float hv = __bfloat162float(h[c * W + i]);
-#pragma unroll
-    for (int k = 0; k < NOUT; ++k) acc[k] += sw[k * W + i] * hv;
-  }
-#pragma unroll
-  for (int k = 0; k < NOUT; ++k) y[c * NOUT + k] = acc[k];
 }
 
 // batch membership: a counter-based hash of (seed, cell) below the threshold
@@ -522,6 +633,8 @@ __global__ void k_to_bf16(int64_t n, const float* __restrict__ w, __nv_bfloat16*
   if (i < n) wb[i] = __float2bfloat16_rn(w[i]);
 }
 
+constexpr int FCB = 128;  // cells per block of the feature kernels
+
 // features of one assembled system (RCM order): B = float(src), D, x_J
 // gathered from the colour-order iterate right after assembly, dq_prev from
 // the colour-order copy of the last update (null: zero)
@@ -529,15 +642,36 @@ template <class TB, class TX>
 __global__ void k_features_raw(int64_t nc, const double* __restrict__ src, const TB* __restrict__ D,
                                const TX* __restrict__ xj_ci, const TX* __restrict__ xprev_ci,
                                const int32_t* __restrict__ ci,
-                               float* __restrict__ raw /* [nc][40]: B, D, unused, dq_prev */,
+                               float* __restrict__ raw /* [nc][40]: B, D, zero, dq_prev */,
                                float* __restrict__ xj) {
-  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (c >= nc) return;
-  for (int k = 0; k < 5; ++k) raw[c * NIN + k] = float(src[5 * c + k]);
-  for (int k = 0; k < 25; ++k) raw[c * NIN + 5 + k] = float(D[25 * c + k]);
-  const int64_t x = ci[c];
-  for (int k = 0; k < 5; ++k) xj[c * 5 + k] = float(xj_ci[5 * x + k]);
-  for (int k = 0; k < 5; ++k) raw[c * NIN + 35 + k] = xprev_ci ? float(xprev_ci[5 * x + k]) : 0.f;
+  // a block per FCB cells, a thread per 4 feature elements (float4 stores;
+  // 40 = 10 x 4, so a float4 never straddles two cells), unrolled so that
+  // each thread has several loads in flight
+  const int64_t c0 = int64_t(blockIdx.x) * FCB;
+  const int ncb = int(nc - c0 < FCB ? nc - c0 : FCB);
+  float4* raw4 = reinterpret_cast<float4*>(raw + c0 * NIN);
+#pragma unroll 5
+  for (int j = threadIdx.x; j < ncb * (NIN / 4); j += blockDim.x) {
+    const int cl = j / (NIN / 4), k0 = 4 * (j - (NIN / 4) * cl);
+    const int64_t c = c0 + cl;
+    float v[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int k = k0 + e;
+      v[e] = 0.f;
+      if (k < 5)
+        v[e] = float(src[5 * c + k]);
+      else if (k < 30)
+        v[e] = float(D[25 * c + k - 5]);
+      else if (k >= 35 && xprev_ci)
+        v[e] = float(xprev_ci[5 * int64_t(ci[c]) + k - 35]);
+    }
+    raw4[j] = make_float4(v[0], v[1], v[2], v[3]);
+  }
+  for (int j = threadIdx.x; j < ncb * 5; j += blockDim.x) {
+    const int cl = j / 5, k = j - 5 * cl;
+    xj[c0 * 5 + j] = float(xj_ci[5 * int64_t(ci[c0 + cl]) + k]);
+  }
 }
 
 // per-component sums of squares of B (raw[:,0:5]) and x_J, block partials
@@ -561,46 +695,79 @@ __global__ void k_rms_partial(int64_t nc, const float* __restrict__ raw, const f
     for (int k = 0; k < 10; ++k) part[10 * blockIdx.x + k] = sh[k][0];
 }
 
-// normalise: B/rs, D_ij xs_j / rs_i, x_J/xs, dq_prev/xs
+// normalise: B/rs, D_ij xs_j / rs_i, x_J/xs, dq_prev/xs, each as one
+// multiplication by a per-feature factor (feature 30..34 read from x_J)
 __global__ void k_features_norm(int64_t nc, const float* __restrict__ raw, const float* __restrict__ xj,
                                 const float* __restrict__ scl /*rs[5],xs[5]*/, float* __restrict__ feat) {
-  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (c >= nc) return;
-  const float* rs = scl;
-  const float* xs = scl + 5;
-  for (int k = 0; k < 5; ++k) feat[c * NIN + k] = raw[c * NIN + k] / rs[k];
-  for (int i = 0; i < 5; ++i)
-    for (int j = 0; j < 5; ++j)
-      feat[c * NIN + 5 + 5 * i + j] = raw[c * NIN + 5 + 5 * i + j] * xs[j] / rs[i];
-  for (int k = 0; k < 5; ++k) feat[c * NIN + 30 + k] = xj[c * 5 + k] / xs[k];
-  for (int k = 0; k < 5; ++k) feat[c * NIN + 35 + k] = raw[c * NIN + 35 + k] / xs[k];
+  // a block per FCB cells, a thread per 4 feature elements (float4 loads
+  // and stores), unrolled so that each thread has several loads in flight;
+  // no branch depends on the feature index
+  const int64_t c0 = int64_t(blockIdx.x) * FCB;
+  const int ncb = int(nc - c0 < FCB ? nc - c0 : FCB);
+  __shared__ float fac[NIN];
+  if (threadIdx.x < NIN) {
+    const int k = threadIdx.x;
+    const float* rs = scl;
+    const float* xs = scl + 5;
+    float f;
+    if (k < 5)
+      f = 1.0f / rs[k];
+    else if (k < 30)
+      f = xs[(k - 5) % 5] / rs[(k - 5) / 5];
+    else if (k < 35)
+      f = 1.0f / xs[k - 30];
+    else
+      f = 1.0f / xs[k - 35];
+    fac[k] = f;
+  }
+  __syncthreads();
+  const float4* raw4 = reinterpret_cast<const float4*>(raw + c0 * NIN);
+  float4* feat4 = reinterpret_cast<float4*>(feat + c0 * NIN);
+#pragma unroll 5
+  for (int j = threadIdx.x; j < ncb * (NIN / 4); j += blockDim.x) {
+    const int cl = j / (NIN / 4), k0 = 4 * (j - (NIN / 4) * cl);
+    const float4 r4 = raw4[j];
+    float v[4] = {r4.x, r4.y, r4.z, r4.w};
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int k = k0 + e;
+      if (k >= 30 && k < 35) v[e] = xj[(c0 + cl) * 5 + k - 30];
+      v[e] *= fac[k];
+    }
+    feat4[j] = make_float4(v[0], v[1], v[2], v[3]);
+  }
 }
 
 inline unsigned nb_(int64_t n, int t) { return unsigned((n + t - 1) / t); }
 
 // forward over the whole graph from features; returns head output in
-// m->d_y.  keep_z stores the FP32 pre-activations the backward pass needs.
-int forward(fpsi_gnn* m, const Graph& G, const float* feat, bool keep_z) {
+// m->d_y.  keep stores what the backward pass needs: neighbour means, FP32
+// pre-activations and every layer's activations.
+static_assert(NLAYER >= 2, "the head is fused into the last hidden layer");
+int forward(fpsi_gnn* m, const Graph& G, const float* feat, bool keep) {
   cudaStream_t s = m->stream;
   const int64_t nc = G.nc;
   const int64_t ntiles = (nc + TC_ROWS - 1) / TC_ROWS;
   const unsigned grid = unsigned(std::max<int64_t>(1, std::min<int64_t>(ntiles, 2 * int64_t(m->nsm))));
+  const __nv_bfloat16 *wo = m->d_wb + m->L.wo, *bo = m->d_wb + m->L.bo;
   for (int l = 0; l < NLAYER; ++l) {
     const int fin = m->L.fan_in[l];
+    const size_t smem = tc_smem(fin).total;
     const __nv_bfloat16 *ws = m->d_wb + m->L.ws[l], *wn = m->d_wb + m->L.wn[l], *b = m->d_wb + m->L.b[l];
-    float* z = keep_z ? m->d_z[l] : nullptr;
-    if (l == 0) {
-      k_aggregate<float><<<nb_(nc * fin, 256), 256, 0, s>>>(nc, fin, G.off, G.nb, feat, m->d_agg[l]);
-      k_mp_tc<float><<<grid, TC_ROWS, tc_smem_bytes(fin), s>>>(nc, fin, feat, m->d_agg[l], ws, wn, b, z,
-                                                               m->d_h[l + 1], m->d_err);
-    } else {
-      k_aggregate<__nv_bfloat16><<<nb_(nc * fin, 256), 256, 0, s>>>(nc, fin, G.off, G.nb, m->d_h[l],
-                                                                    m->d_agg[l]);
-      k_mp_tc<__nv_bfloat16><<<grid, TC_ROWS, tc_smem_bytes(fin), s>>>(nc, fin, m->d_h[l], m->d_agg[l], ws,
-                                                                       wn, b, z, m->d_h[l + 1], m->d_err);
-    }
+    __nv_bfloat16* agg = keep ? m->d_agg[l] : nullptr;
+    float* z = keep ? m->d_z[l] : nullptr;
+    const bool last = l == NLAYER - 1;
+    __nv_bfloat16* hout = (last && !keep) ? nullptr : m->d_h[l + 1];
+    if (l == 0)
+      k_layer_tc<float, false><<<grid, TC_THREADS, smem, s>>>(nc, fin, feat, G.off, G.nb, ws, wn, b, wo, bo, agg,
+                                                              z, hout, nullptr, m->d_err);
+    else if (!last)
+      k_layer_tc<__nv_bfloat16, false><<<grid, TC_THREADS, smem, s>>>(nc, fin, m->d_h[l], G.off, G.nb, ws, wn, b,
+                                                                      wo, bo, agg, z, hout, nullptr, m->d_err);
+    else
+      k_layer_tc<__nv_bfloat16, true><<<grid, TC_THREADS, smem, s>>>(nc, fin, m->d_h[l], G.off, G.nb, ws, wn, b,
+                                                                     wo, bo, agg, z, hout, m->d_y, m->d_err);
   }
-  k_head_forward<<<nb_(nc, GT), GT, 0, s>>>(nc, m->d_wb + m->L.wo, m->d_wb + m->L.bo, m->d_h[NLAYER], m->d_y);
   FPSI_CUDA_TRY(cudaGetLastError());
   return FPSI_OK;
 }
@@ -779,10 +946,13 @@ int fpsi_gnn_create(fpsi_gnn** out, uint64_t seed) {
   int dev = 0;
   if (!rc && (cudaGetDevice(&dev) != cudaSuccess ||
               cudaDeviceGetAttribute(&m->nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-              cudaFuncSetAttribute(k_mp_tc<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   int(tc_smem_bytes(W))) != cudaSuccess ||
-              cudaFuncSetAttribute(k_mp_tc<__nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   int(tc_smem_bytes(W))) != cudaSuccess)) {
+              cudaFuncSetAttribute(k_layer_tc<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(tc_smem(W).total)) != cudaSuccess ||
+              cudaFuncSetAttribute(k_layer_tc<__nv_bfloat16, false>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(tc_smem(W).total)) != cudaSuccess ||
+              cudaFuncSetAttribute(k_layer_tc<__nv_bfloat16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(tc_smem(W).total)) != cudaSuccess)) {
     fpsi::set_error("learned start: device query failed");
     rc = FPSI_E_CUDA;
   }
@@ -883,14 +1053,14 @@ static int make_features(fpsi_gnn* m, fpsi_ctx* x, float* feat, float* xj, float
   FPSI_CUDA_TRY(cudaStreamSynchronize(x->stream));
   float* raw = m->d_dagg;  // [nc][40] scratch inside an [nc][64] buffer
   if (x->P.precision == FPSI_PREC_FP64)
-    k_features_raw<double, double><<<nb_(nc, 256), 256, 0, m->stream>>>(
+    k_features_raw<double, double><<<nb_(nc, FCB), 256, 0, m->stream>>>(
         nc, x->d_src, (const double*)x->d_D, (const double*)x->d_x, (const double*)xprev, x->d_ci, raw,
         xj);
   else if (x->P.precision == FPSI_PREC_MIXED)
-    k_features_raw<float, float><<<nb_(nc, 256), 256, 0, m->stream>>>(
+    k_features_raw<float, float><<<nb_(nc, FCB), 256, 0, m->stream>>>(
         nc, x->d_src, (const float*)x->d_D, (const float*)x->d_x, (const float*)xprev, x->d_ci, raw, xj);
   else
-    k_features_raw<float, double><<<nb_(nc, 256), 256, 0, m->stream>>>(
+    k_features_raw<float, double><<<nb_(nc, FCB), 256, 0, m->stream>>>(
         nc, x->d_src, (const float*)x->d_D, (const double*)x->d_x, (const double*)xprev, x->d_ci, raw,
         xj);
   const int nblk = int(nb_(nc, GT));
@@ -907,7 +1077,7 @@ static int make_features(fpsi_gnn* m, fpsi_ctx* x, float* feat, float* xj, float
   for (int k = 0; k < 5; ++k) rs[k] = scl[k], xs[k] = scl[5 + k];
   float* dscl = reinterpret_cast<float*>(m->d_lpart);
   FPSI_CUDA_TRY(cudaMemcpyAsync(dscl, scl, sizeof(scl), cudaMemcpyHostToDevice, m->stream));
-  k_features_norm<<<nb_(nc, 256), 256, 0, m->stream>>>(nc, raw, xj, dscl, feat);
+  k_features_norm<<<nb_(nc, FCB), 256, 0, m->stream>>>(nc, raw, xj, dscl, feat);
   FPSI_CUDA_TRY(cudaGetLastError());
   return FPSI_OK;
 }
@@ -1085,13 +1255,10 @@ int fpsi_gnn_predict(fpsi_gnn* m, fpsi_ctx* x, double* x0) {
   int rc = ensure_capacity(m, nc);
   if (!rc) rc = ctx_graph(x, &G);
   if (rc) return rc;
-  float* fbuf = nullptr;
-  if ((rc = galloc(&fbuf, nc * NIN))) return rc;
-  float* xjb = nullptr;
-  if ((rc = galloc(&xjb, nc * 5))) {
-    cudaFree(fbuf);
-    return rc;
-  }
+  // features and Jacobi start in the backward pass's buffers, which an
+  // inference pass does not use ([nc][64] FP32 each)
+  float* fbuf = m->d_dz;
+  float* xjb = m->d_dh;
   rc = make_features(m, x, fbuf, xjb, rs, xs);
   if (!rc) rc = forward(m, G, fbuf, false);
   double* dx0 = nullptr;
@@ -1114,8 +1281,6 @@ int fpsi_gnn_predict(fpsi_gnn* m, fpsi_ctx* x, double* x0) {
     for (int64_t i = 0; !rc && i < nc; ++i)
       for (int k = 0; k < 5; ++k) x0[5 * int64_t(x->H.perm[i]) + k] = h[5 * i + k];
   }
-  cudaFree(fbuf);
-  cudaFree(xjb);
   cudaFree(dx0);
   if (!rc) x->x_preset = true;
   return rc;

@@ -137,3 +137,52 @@ def sweeps_to_tolerance(solver: FlowPsi, start: str, rtol: float = 1e-3,
     else:
         raise ValueError(start)
     return solver.sweeps_to_tolerance(rtol, max_sweeps)
+
+
+def _time_inference(argv=None) -> dict:
+    """Wall time of the learned start's inference (features, the three
+    tensor-core layers with the head, the start written into the solver's
+    iterate) on an assembled Taylor-Green tet system of n^3 x 6 cells, and
+    of training steps on one snapshot of it."""
+    import argparse
+    import json
+    import time
+
+    from . import cases
+
+    ap = argparse.ArgumentParser(prog="python -m flowpsi_b200.learned")
+    ap.add_argument("--n", type=int, default=64, help="hexes per direction (x6 tets)")
+    ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--train-steps", type=int, default=0)
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "ref", "mixed"])
+    a = ap.parse_args(argv)
+    case = cases.taylor_green_tets(a.n, precision=a.precision)
+    s = FlowPsi(case.mesh, case.params)
+    s.keep_blocks(True)
+    s.set_state(*case.initial_state(s.geometry()["cellcenter"]))
+    s.residual(want_src=False)
+    s.assemble()
+    m = LearnedStart(seed=1)
+    m.predict(s)  # first pass allocates the activations
+    ts = []
+    for _ in range(a.reps):
+        t0 = time.perf_counter()
+        m.predict(s)
+        ts.append(time.perf_counter() - t0)
+    out = {"cells": s.ncells, "predict_ms_min": 1e3 * min(ts), "predict_ms_median": 1e3 * float(np.median(ts)),
+           "precision": a.precision}
+    if a.train_steps > 0:
+        s.sweeps(4)
+        m.add_snapshot(s, s.get_iterate())
+        m.train(1, batch=s.ncells)
+        t0 = time.perf_counter()
+        m.train(a.train_steps, batch=s.ncells)
+        out["train_step_ms"] = 1e3 * (time.perf_counter() - t0) / a.train_steps
+    m.close()
+    s.close()
+    print(json.dumps(out), flush=True)
+    return out
+
+
+if __name__ == "__main__":
+    _time_inference()
