@@ -143,11 +143,11 @@ def sgs_launch_sequence(ncolours, sweeps):
     return seq
 
 
-def sgs_colour_bytes(colour, nint, tb, tx):
+def sgs_colour_bytes(colour, nint, tb, tx, slot=25):
     """algorithmic bytes of one launch of each colour: per cell LU 25*tb +
-    B 5*tb + x write 5*tx; per interior face side block 25*tb + index 4 +
-    neighbour x 5*tx"""
-    per_cell = (30 * tb + 5 * tx) + nint * (25 * tb + 4 + 5 * tx)
+    B 5*tb + x write 5*tx; per interior face side the off-diagonal slot
+    (25 values, or 15 in the compact Roe form) + index 4 + neighbour x 5*tx"""
+    per_cell = (30 * tb + 5 * tx) + nint * (slot * tb + 4 + 5 * tx)
     return np.bincount(colour, weights=per_cell.astype(np.float64))
 
 
@@ -156,11 +156,20 @@ def sgs_bytes_per_step(colour_bytes, sweeps):
     return float(sum(colour_bytes[k] for k in seq)), len(seq)
 
 
-def kernel_bytes(name, nc, nfi, nbf, sweeps, tb, tx, sgs_step_bytes=None):
+def kernel_bytes(name, nc, nfi, nbf, sweeps, tb, tx, sgs_step_bytes=None, compact=False):
     """algorithmic bytes of one step of each kernel (every array the kernel
-    must touch counted once: FP64 8 B, FP32 4 B, index 4 B)"""
+    must touch counted once: FP64 8 B, FP32 4 B, index 4 B).  compact: the
+    inviscid SGS system keeps its face Jacobians as 24-value face records
+    (9 coefficients per direction + U + n) and 15-value sweep slots"""
     nf = nfi + nbf
     geo_face = 8 + 32 + 48  # cl,cr + n*A + rL,rR
+    if compact:
+        jac_out = nf * 24 * tb
+        # each face side needs its direction's 9 coefficients and U, n
+        asm_faces = (2 * nfi + nbf) * 15 * tb + 2 * nfi * 15 * tb
+    else:
+        jac_out = (nfi * 2 + nbf) * 25 * tb
+        asm_faces = (2 * nfi + nbf) * 25 * tb + 2 * nfi * 25 * tb
     return {
         "bc_state": nbf * (4 + 24 + 40 + 40),
         # q + Minv + vol + grad/limiter writes; face geometry and indices
@@ -168,12 +177,11 @@ def kernel_bytes(name, nc, nfi, nbf, sweeps, tb, tx, sgs_step_bytes=None):
         # survey K3: q 40 + grad 120 + phi 40 per cell, 88 per face, flux write 40 + mev 8
         "face_flux": nc * (40 + 120 + 40) + nf * (geo_face + 48),
         "cell_residual": nc * (40 + 8 + 40 + 8) + nf * 48,
-        "face_jacobian": nc * (40 + 120 + 40) + nf * geo_face + (nfi * 2 + nbf) * 25 * tb,
+        "face_jacobian": nc * (40 + 120 + 40) + nf * geo_face + jac_out,
         # q, src, dtau, vol; LU + B slots, pivots, Jacobi start; each face
         # block read once for the diagonal sum, interior ones written once
         # more into the off-diagonal slots
-        "assemble_lu": (nc * (40 + 40 + 8 + 8 + 30 * tb + 4 + 5 * tx) + (2 * nfi + nbf) * 25 * tb
-                        + 2 * nfi * 25 * tb),
+        "assemble_lu": nc * (40 + 40 + 8 + 8 + 30 * tb + 4 + 5 * tx) + asm_faces,
         "sgs_colour": sgs_step_bytes,
         "update": nc * (80 + 5 * tx),
     }.get(name)
@@ -359,22 +367,25 @@ def run_fpsi(args, ws, rank, local):
     kt = solver.kernel_times(args.profile_steps)
     tb = 4 if args.precision in ("ref", "mixed") else 8
     tx = 4 if args.precision == "mixed" else 8
+    # inviscid systems relaxed by multi-colour SGS keep compact face Jacobians
+    compact = case.params.viscous == 0 and case.params.solver == 0
     peaks, src = load_peaks()
     peak = float(peaks["hbm_gbs"])
     kernels = {}
     sgs_step = None
     if case.params.solver == 0:
-        cb = sgs_colour_bytes(solver.colours(), nint, tb, tx)
+        cb = sgs_colour_bytes(solver.colours(), nint, tb, tx, slot=15 if compact else 25)
         sgs_step, _ = sgs_bytes_per_step(cb, case.params.gauss_seidel_iter)
     for name, (kms, launches) in kt.items():
-        b = kernel_bytes(name, nc, nfi, nbf, args.sweeps, tb, tx, sgs_step)
+        b = kernel_bytes(name, nc, nfi, nbf, args.sweeps, tb, tx, sgs_step, compact)
         per_step_ms = kms / args.profile_steps
         kernels[name] = {"ms_per_step": per_step_ms, "launches_per_step": launches / args.profile_steps,
                          "gbs": None if b is None else b / (per_step_ms / 1e3) / 1e9}
     dom = max((k for k in kernels if kernels[k]["gbs"] is not None),
               key=lambda k: kernels[k]["ms_per_step"])
     dk = kernels[dom]
-    b_launch = kernel_bytes(dom, nc, nfi, nbf, args.sweeps, tb, tx, sgs_step) / dk["launches_per_step"]
+    b_launch = (kernel_bytes(dom, nc, nfi, nbf, args.sweeps, tb, tx, sgs_step, compact)
+                / dk["launches_per_step"])
     avg_launch_s = dk["ms_per_step"] / dk["launches_per_step"] / 1e3
     achieved = b_launch / avg_launch_s / 1e9
     traffic = None

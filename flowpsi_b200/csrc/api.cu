@@ -69,10 +69,10 @@ std::vector<double> soa3(const std::vector<double>& a, int64_t n) {
 }
 
 void free_system(fpsi_ctx* x) {
-  void* ps[] = {x->d_fjp, x->d_fjm, x->d_D, x->d_x, x->d_luc, x->d_bc, x->d_pv, x->d_aoff};
+  void* ps[] = {x->d_fjp, x->d_fjm, x->d_fjc, x->d_D, x->d_x, x->d_luc, x->d_bc, x->d_pv, x->d_aoff};
   for (void* p : ps)
     if (p) cudaFree(p);
-  x->d_fjp = x->d_fjm = x->d_D = x->d_x = x->d_luc = x->d_bc = x->d_aoff = nullptr;
+  x->d_fjp = x->d_fjm = x->d_fjc = x->d_D = x->d_x = x->d_luc = x->d_bc = x->d_aoff = nullptr;
   x->d_pv = nullptr;
 }
 
@@ -87,6 +87,7 @@ int alloc_system(fpsi_ctx* x) {
   int rc;
   if ((rc = dalloc(x, (char**)&x->d_fjp, nf * 25 * tb))) return rc;
   if ((rc = dalloc(x, (char**)&x->d_fjm, nf * 25 * tb))) return rc;
+  if ((rc = dalloc(x, (char**)&x->d_fjc, nf * 24 * tb))) return rc;
   const size_t ncp = size_t(x->H.ncp);
   if ((rc = dalloc(x, (char**)&x->d_luc, ncp * 25 * tb))) return rc;
   if ((rc = dalloc(x, (char**)&x->d_bc, ncp * 5 * tb))) return rc;
@@ -751,6 +752,10 @@ int fpsi_get_blocks(fpsi_ctx* x, void* D, void* fjp, void* fjm, void* B) {
     FPSI_CUDA_TRY(cudaMemcpy(h.data(), x->d_D, h.size(), cudaMemcpyDeviceToHost));
     for (int64_t i = 0; i < nc; ++i)
       std::memcpy((char*)D + size_t(x->H.perm[i]) * 25 * tb, h.data() + size_t(i) * 25 * tb, 25 * tb);
+  }
+  if ((fjp || fjm) && !x->have_explicit) {
+    const int rc = fpsi::ensure_explicit_blocks(x);
+    if (rc) return rc;
   }
   for (int w = 0; w < 2; ++w) {
     void* dst = w ? fjm : fjp;

@@ -132,12 +132,17 @@ struct fpsi_ctx {
   // implicit system (block type depends on precision)
   void* d_fjp = nullptr;       // [nf][25] TB
   void* d_fjm = nullptr;       // [nf][25] TB
+  // compact face Jacobians (inviscid SGS): per face [+ (9) | - (9) | U | n] TB;
+  // the explicit fjp/fjm are then filled only on request
+  void* d_fjc = nullptr;       // [nf][24] TB
+  bool asm_compact = false;    // the assembled system's slots are compact
+  bool have_explicit = false;  // fjp/fjm hold the assembled system's blocks
   void* d_D = nullptr;         // [nc][25] TB (only when keep_D)
   // colour-order arrays of the sweeps (see HostMesh)
   void* d_luc = nullptr;       // per colour [25][n_k] TB: LU factors of fluid_D
   void* d_bc = nullptr;        // per colour [5][n_k] TB: fluid_B
   int32_t* d_pv = nullptr;     // [nc] packed pivots, colour order
-  void* d_aoff = nullptr;      // per colour [m_k][25][n_k] TB: off-diagonal blocks
+  void* d_aoff = nullptr;      // per colour [m_k][25 or 15][n_k] TB: off-diagonal blocks
   int32_t* d_nbr = nullptr;    // per colour [m_k][n_k] neighbour ci
   int32_t* d_ci = nullptr;     // RCM cell -> ci
   int32_t* d_ccol = nullptr;   // RCM cell -> colour

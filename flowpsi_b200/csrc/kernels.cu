@@ -643,6 +643,66 @@ k_face_jacobian(MeshView M, const double* __restrict__ q, const double* __restri
   for (int64_t k = threadIdx.x; k < cnt; k += JAC_THREADS) fjm[25 * f0 + k] = stage[k];
 }
 
+// Compact face Jacobians of an inviscid system: per face the coefficients of
+// fjp (+) and fjm (-) and the shared U, n (CK_FACE values), staged and
+// written back like the explicit blocks.  A viscous-wall face's pressure
+// block d(p n A)/dpg is c1 = -A with every other coefficient zero.
+template <class TB>
+__global__ void __launch_bounds__(JAC_THREADS)
+k_face_jacobian_c(MeshView M, const double* __restrict__ q, const double* __restrict__ qb,
+                  const double* __restrict__ grad, const double* __restrict__ phi, Gas g,
+                  TB* __restrict__ fjc) {
+  __shared__ TB stage[JAC_THREADS * CK_FACE];
+  const int64_t f0 = int64_t(blockIdx.x) * JAC_THREADS;
+  const int64_t f = f0 + threadIdx.x;
+  const int64_t cnt = min(int64_t(JAC_THREADS), M.nf - f0) * CK_FACE;
+  if (f < M.nf) {
+    FaceStates s;
+    reconstruct(M, q, qb, grad, phi, f, g.pamb, s);
+    const double nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
+    const double A = M.area[f];
+    const RoeAvg ra = roe_average(s.L, s.R, nx, ny, nz, g, 0.0, 1.0);
+    TB* st = stage + CK_FACE * threadIdx.x;
+    if (bc_kind(M, f) == FPSI_BC_VISCOUS_WALL) {
+#pragma unroll
+      for (int k = 0; k < CK_DIR; ++k) st[k] = TB(0);
+      st[CK_C1] = TB(-A);
+    } else {
+      jac_roe_compact<TB>(ra, A, g, +1, st);
+    }
+    if (f < M.nfi) {
+      jac_roe_compact<TB>(ra, A, g, -1, st + CK_DIR);
+    } else {
+#pragma unroll
+      for (int k = 0; k < CK_DIR; ++k) st[CK_DIR + k] = TB(0);
+    }
+    st[2 * CK_DIR] = TB(ra.U), st[2 * CK_DIR + 1] = TB(ra.V), st[2 * CK_DIR + 2] = TB(ra.W);
+    st[2 * CK_DIR + 3] = TB(nx), st[2 * CK_DIR + 4] = TB(ny), st[2 * CK_DIR + 5] = TB(nz);
+  }
+  __syncthreads();
+  for (int64_t k = threadIdx.x; k < cnt; k += JAC_THREADS) fjc[CK_FACE * f0 + k] = stage[k];
+}
+
+// explicit fjp/fjm from the compact face records (boundary faces: fjp only)
+template <class TB>
+__global__ void k_expand_blocks(int64_t nf, int64_t nfi, const TB* __restrict__ fjc,
+                                TB* __restrict__ fjp, TB* __restrict__ fjm) {
+  const int64_t f = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (f >= nf) return;
+  TB r[CK_FACE];
+#pragma unroll
+  for (int k = 0; k < CK_FACE; ++k) r[k] = fjc[CK_FACE * f + k];
+  TB Mb[25];
+  compact_expand<TB>(r, r + 2 * CK_DIR, r + 2 * CK_DIR + 3, Mb);
+#pragma unroll
+  for (int k = 0; k < 25; ++k) fjp[25 * f + k] = Mb[k];
+  if (f < nfi) {
+    compact_expand<TB>(r + CK_DIR, r + 2 * CK_DIR, r + 2 * CK_DIR + 3, Mb);
+#pragma unroll
+    for (int k = 0; k < 25; ++k) fjm[25 * f + k] = Mb[k];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // 5x5 LU with partial pivoting and its solve
 // ---------------------------------------------------------------------------
@@ -748,12 +808,18 @@ constexpr size_t asm_smem_bytes() {
   return size_t(ASM_THREADS / 32) * 50 * ASM_STRIDE * sizeof(TB);
 }
 
-template <class TB, class TX>
+// CPT: the face blocks come as compact records (fjc, CK_FACE values per
+// face) and the slots are written compact (CK_SLOT values); otherwise as
+// explicit (fjp, fjm) pairs into 25-value slots.
+template <class TB, class TX, bool CPT>
 __global__ void __launch_bounds__(ASM_THREADS, sizeof(TB) == 4 ? 6 : 4)
 k_assemble(MeshView M, SweepView S, const double* __restrict__ q, const double* __restrict__ src,
            const double* __restrict__ dtau, const TB* __restrict__ fjp, const TB* __restrict__ fjm,
-           Gas g, TB* __restrict__ luc, TB* __restrict__ bcv, int32_t* __restrict__ pvv,
-           TB* __restrict__ aoff, TB* __restrict__ Dout, TX* __restrict__ x, int32_t* __restrict__ err) {
+           const TB* __restrict__ fjc, Gas g, TB* __restrict__ luc, TB* __restrict__ bcv,
+           int32_t* __restrict__ pvv, TB* __restrict__ aoff, TB* __restrict__ Dout, TX* __restrict__ x,
+           int32_t* __restrict__ err) {
+  constexpr int RW = CPT ? CK_FACE : 50;        // words staged per face
+  constexpr int BATCH = CPT ? 8 : ASM_BATCH;    // RW / BATCH rounds per lane
   extern __shared__ __align__(16) unsigned char asm_smem[];
   TB* st = reinterpret_cast<TB*>(asm_smem) + (threadIdx.x >> 5) * (50 * ASM_STRIDE);
   const int lane = threadIdx.x & 31;
@@ -777,29 +843,67 @@ k_assemble(MeshView M, SweepView S, const double* __restrict__ q, const double* 
   int64_t slot = 0;
   for (int e = 0; e < maxdeg; ++e) {
     const int32_t my_ent = e < deg ? M.cf[e0 + e] : -1;
-    // 1600 words per round, 50 per lane, in batches of ASM_BATCH independent
+    // 32 RW words per round, RW per lane, in batches of BATCH independent
     // loads (fjm is allocated for every face, so every address is valid;
     // lanes without an entry read face 0 and their words are never used)
 #pragma unroll 1
-    for (int b = 0; b < 50 / ASM_BATCH; ++b) {
-      TB v[ASM_BATCH];
+    for (int b = 0; b < RW / BATCH; ++b) {
+      TB v[BATCH];
 #pragma unroll
-      for (int u = 0; u < ASM_BATCH; ++u) {
-        const int idx = lane + 32 * (ASM_BATCH * b + u);
-        const int L = idx / 50, k = idx - 50 * L;
+      for (int u = 0; u < BATCH; ++u) {
+        const int idx = lane + 32 * (BATCH * b + u);
+        const int L = idx / RW, k = idx - RW * L;
         const int32_t ent = __shfl_sync(0xffffffffu, my_ent, L);
         const int64_t f = ent >= 0 ? int64_t(ent >> 1) : 0;
-        v[u] = k < 25 ? __ldg(fjp + 25 * f + k) : __ldg(fjm + 25 * f + (k - 25));
+        if constexpr (CPT)
+          v[u] = __ldg(fjc + CK_FACE * f + k);
+        else
+          v[u] = k < 25 ? __ldg(fjp + 25 * f + k) : __ldg(fjm + 25 * f + (k - 25));
       }
 #pragma unroll
-      for (int u = 0; u < ASM_BATCH; ++u) {
-        const int idx = lane + 32 * (ASM_BATCH * b + u);
-        const int L = idx / 50, k = idx - 50 * L;
+      for (int u = 0; u < BATCH; ++u) {
+        const int idx = lane + 32 * (BATCH * b + u);
+        const int L = idx / RW, k = idx - RW * L;
         st[k * ASM_STRIDE + L] = v[u];
       }
     }
     __syncwarp();
-    if (my_ent >= 0) {
+    if (CPT && my_ent >= 0) {
+      // L = -fjp to the lower neighbour, U = fjm to the upper one, as below,
+      // with the slots written compact
+      const int64_t f = my_ent >> 1;
+      TB r[CK_FACE];
+#pragma unroll
+      for (int k = 0; k < CK_FACE; ++k) r[k] = st[k * ASM_STRIDE + lane];
+      TB* ao = aoff ? aoff + CK_SLOT * ck.ebp + slot * CK_SLOT * ld + i : nullptr;
+      TB Mb[25];
+      if (my_ent & 1) {
+        compact_expand<TB>(r + CK_DIR, r + 2 * CK_DIR, r + 2 * CK_DIR + 3, Mb);
+#pragma unroll
+        for (int k = 0; k < 25; ++k) sJ[k] += Mb[k];
+        if (ao) {
+#pragma unroll
+          for (int k = 0; k < CK_DIR; ++k) ao[k * ld] = -r[k];
+#pragma unroll
+          for (int k = 0; k < 6; ++k) ao[(CK_DIR + k) * ld] = r[2 * CK_DIR + k];
+        }
+        ++slot;
+      } else {
+        compact_expand<TB>(r, r + 2 * CK_DIR, r + 2 * CK_DIR + 3, Mb);
+#pragma unroll
+        for (int k = 0; k < 25; ++k) sJ[k] -= Mb[k];
+        if (f < M.nfi) {
+          if (ao) {
+#pragma unroll
+            for (int k = 0; k < CK_DIR; ++k) ao[k * ld] = r[CK_DIR + k];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) ao[(CK_DIR + k) * ld] = r[2 * CK_DIR + k];
+          }
+          ++slot;
+        }
+      }
+    }
+    if (!CPT && my_ent >= 0) {
       const int64_t f = my_ent >> 1;
       const TB* sp = st + lane;                    // fjp of the face
       const TB* sm = st + 25 * ASM_STRIDE + lane;  // fjm of the face
@@ -911,7 +1015,9 @@ __global__ void k_jacobi_start(ColInfo ck, const TB* __restrict__ luc,
 // addresses; only the neighbours' iterates are gathered.  The one-pass
 // streams are loaded with the streaming hint (evict first) so that the
 // iterate, which every colour re-reads, stays resident in L2.
-template <class TB, class TX>
+// CPT: slots hold the compact form (CK_SLOT values), applied without
+// spelling out the 25 entries.
+template <class TB, class TX, bool CPT>
 __global__ void k_sgs_colour(ColInfo ck, const int32_t* __restrict__ nbr,
                              const TB* __restrict__ aoff, const TB* __restrict__ luc,
                              const TB* __restrict__ bcv, const int32_t* __restrict__ pvv,
@@ -928,11 +1034,19 @@ __global__ void k_sgs_colour(ColInfo ck, const int32_t* __restrict__ nbr,
     TX xv[5];
 #pragma unroll
     for (int k = 0; k < 5; ++k) xv[k] = x[5 * int64_t(o) + k];
-    const TB* A = aoff + 25 * ck.ebp + s * 25 * ld + i;
+    if constexpr (CPT) {
+      const TB* A = aoff + CK_SLOT * ck.ebp + s * CK_SLOT * ld + i;
+      TB c[CK_SLOT];
 #pragma unroll
-    for (int r = 0; r < 5; ++r)
+      for (int k = 0; k < CK_SLOT; ++k) c[k] = __ldcs(A + k * ld);
+      compact_apply<TB, TX>(c, xv, t);
+    } else {
+      const TB* A = aoff + 25 * ck.ebp + s * 25 * ld + i;
 #pragma unroll
-      for (int j = 0; j < 5; ++j) t[r] += TX(__ldcs(A + (5 * r + j) * ld)) * xv[j];
+      for (int r = 0; r < 5; ++r)
+#pragma unroll
+        for (int j = 0; j < 5; ++j) t[r] += TX(__ldcs(A + (5 * r + j) * ld)) * xv[j];
+    }
   }
   TB LU[25];
 #pragma unroll
@@ -1195,6 +1309,26 @@ static dev::SweepView sweep_view(const fpsi_ctx* x) {
   return S;
 }
 
+// Inviscid systems relaxed by multi-colour SGS keep their face Jacobians in
+// the compact Roe form (15 values per sweep slot instead of 25); viscous
+// terms and the line solver need the explicit blocks.
+static bool compact_blocks(const fpsi_ctx* x) {
+  return !x->P.viscous && x->P.solver == FPSI_SOLVER_SGS;
+}
+
+template <class TB, class TX, bool CPT>
+static void launch_assemble_kernel(fpsi_ctx* x, const dev::MeshView& M, const dev::Gas& g) {
+  constexpr size_t smem = dev::asm_smem_bytes<TB>();
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(dev::k_assemble<TB, TX, CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(smem));
+  dev::k_assemble<TB, TX, CPT><<<blocks_for(M.nc, dev::ASM_THREADS), dev::ASM_THREADS, smem, x->stream>>>(
+      M, sweep_view(x), x->d_q, x->d_src, x->d_dtau, (const TB*)x->d_fjp, (const TB*)x->d_fjm,
+      (const TB*)x->d_fjc, g, (TB*)x->d_luc, (TB*)x->d_bc, x->d_pv,
+      x->P.solver == FPSI_SOLVER_LSGS ? nullptr : (TB*)x->d_aoff, x->keep_D ? (TB*)x->d_D : nullptr,
+      (TX*)x->d_x, x->d_err);
+}
+
 template <class TB, class TX>
 static int launch_assemble_t(fpsi_ctx* x) {
   const dev::MeshView M = view(x);
@@ -1202,8 +1336,14 @@ static int launch_assemble_t(fpsi_ctx* x) {
   cudaStream_t s = x->stream;
   TB* fjp = (TB*)x->d_fjp;
   TB* fjm = (TB*)x->d_fjm;
+  const bool cpt = compact_blocks(x);
+  x->asm_compact = cpt;
+  x->have_explicit = !cpt;
   prof_begin(x, "face_jacobian");
-  if (x->P.viscous)
+  if (cpt)
+    dev::k_face_jacobian_c<TB><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
+        M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, (TB*)x->d_fjc);
+  else if (x->P.viscous)
     dev::k_face_jacobian<TB, true><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
         M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, visc(x), fjp, fjm);
   else
@@ -1211,14 +1351,10 @@ static int launch_assemble_t(fpsi_ctx* x) {
         M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, visc(x), fjp, fjm);
   prof_end(x);
   prof_begin(x, "assemble_lu");
-  constexpr size_t smem = dev::asm_smem_bytes<TB>();
-  if (smem > 48 * 1024)
-    FPSI_CUDA_TRY(cudaFuncSetAttribute(dev::k_assemble<TB, TX>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  dev::k_assemble<TB, TX><<<blocks_for(M.nc, dev::ASM_THREADS), dev::ASM_THREADS, smem, s>>>(
-      M, sweep_view(x), x->d_q, x->d_src, x->d_dtau, fjp, fjm, g, (TB*)x->d_luc, (TB*)x->d_bc,
-      x->d_pv, x->P.solver == FPSI_SOLVER_LSGS ? nullptr : (TB*)x->d_aoff,
-      x->keep_D ? (TB*)x->d_D : nullptr, (TX*)x->d_x, x->d_err);
+  if (cpt)
+    launch_assemble_kernel<TB, TX, true>(x, M, g);
+  else
+    launch_assemble_kernel<TB, TX, false>(x, M, g);
   prof_end(x);
   FPSI_CUDA_TRY(cudaGetLastError());
   return FPSI_OK;
@@ -1277,9 +1413,14 @@ static int launch_sgs_t(fpsi_ctx* x, int sweeps) {
         if (ck.n == 0 || k == last) continue;
         last = k;
         prof_begin(x, "sgs_colour");
-        dev::k_sgs_colour<TB, TX><<<blocks_for(ck.n, T), T, 0, s>>>(
-            ck, x->d_nbr, (const TB*)x->d_aoff, (const TB*)x->d_luc, (const TB*)x->d_bc, x->d_pv,
-            (TX*)x->d_x);
+        if (x->asm_compact)
+          dev::k_sgs_colour<TB, TX, true><<<blocks_for(ck.n, T), T, 0, s>>>(
+              ck, x->d_nbr, (const TB*)x->d_aoff, (const TB*)x->d_luc, (const TB*)x->d_bc, x->d_pv,
+              (TX*)x->d_x);
+        else
+          dev::k_sgs_colour<TB, TX, false><<<blocks_for(ck.n, T), T, 0, s>>>(
+              ck, x->d_nbr, (const TB*)x->d_aoff, (const TB*)x->d_luc, (const TB*)x->d_bc, x->d_pv,
+              (TX*)x->d_x);
         prof_end(x);
       }
   }
@@ -1298,8 +1439,25 @@ int launch_sgs(fpsi_ctx* x, int sweeps) {
   }
 }
 
+template <class TB>
+static int expand_blocks_t(fpsi_ctx* x) {
+  dev::k_expand_blocks<TB><<<blocks_for(x->H.nf, 128), 128, 0, x->stream>>>(
+      x->H.nf, x->H.nfi, (const TB*)x->d_fjc, (TB*)x->d_fjp, (TB*)x->d_fjm);
+  FPSI_CUDA_TRY(cudaGetLastError());
+  FPSI_CUDA_TRY(cudaStreamSynchronize(x->stream));
+  x->have_explicit = true;
+  return FPSI_OK;
+}
+
+int ensure_explicit_blocks(fpsi_ctx* x) {
+  if (x->have_explicit || !x->asm_compact) return FPSI_OK;
+  return x->P.precision == FPSI_PREC_FP64 ? expand_blocks_t<double>(x) : expand_blocks_t<float>(x);
+}
+
 template <class TB, class TX>
 static int launch_linres_t(fpsi_ctx* x, double* out2) {
+  const int rc = ensure_explicit_blocks(x);
+  if (rc) return rc;
   const dev::MeshView M = view(x);
   const bool lsgs = x->P.solver == FPSI_SOLVER_LSGS;
   dev::k_linres<TB, TX><<<x->nblk_norm, dev::NORM_THREADS, 0, x->stream>>>(

@@ -20,6 +20,9 @@ int launch_jacobi_start(fpsi_ctx* x);
 int launch_sgs(fpsi_ctx* x, int sweeps);
 // out2[0] = ||B||, out2[1] = ||B - A x|| (device)
 int launch_linres(fpsi_ctx* x, double* out2);
+// fills fjp/fjm from the compact face records of the assembled system (a
+// no-op when they already hold it)
+int ensure_explicit_blocks(fpsi_ctx* x);
 // clipped Newton update; per-block minimum alpha into d_amin
 int launch_update(fpsi_ctx* x);
 // caller-order staging buffer <-> device state (in = staging -> q)

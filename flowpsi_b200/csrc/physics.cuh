@@ -198,9 +198,7 @@ __device__ __forceinline__ void flux_roe(const Q5& L, const Q5& R, double nx, do
 
 // Smoothed one-sided eigenvalue Jacobian, roeCT_jacobian (:1141-1167):
 // l -> (l +- sqrt(l^2 + (0.02 (lmax - lmin))^2)) / 2.
-template <class TB>
-__device__ __forceinline__ void jac_roe(const RoeAvg& s, double nx, double ny, double nz,
-                                        double area, const Gas& g, int dir, TB* M) {
+__device__ __forceinline__ RoeK roe_k_smoothed(const RoeAvg& s, const Gas& g, int dir) {
   const double ep = s.eta + 1.0;
   double l1 = s.un;
   double l2 = 0.5 * (s.un * ep - s.sigma);
@@ -212,8 +210,90 @@ __device__ __forceinline__ void jac_roe(const RoeAvg& s, double nx, double ny, d
   l1 = 0.5 * (l1 + d * sqrt(l1 * l1 + e2));
   l2 = 0.5 * (l2 + d * sqrt(l2 * l2 + e2));
   l3 = 0.5 * (l3 + d * sqrt(l3 * l3 + e2));
-  const RoeK k = roe_k(l1, l2, l3, s, g);
-  roe_k_matrix<TB>(k, s, nx, ny, nz, area, M);
+  return roe_k(l1, l2, l3, s, g);
+}
+
+template <class TB>
+__device__ __forceinline__ void jac_roe(const RoeAvg& s, double nx, double ny, double nz,
+                                        double area, const Gas& g, int dir, TB* M) {
+  roe_k_matrix<TB>(roe_k_smoothed(s, g, dir), s, nx, ny, nz, area, M);
+}
+
+// Compact form of area * K: nine per-direction coefficients (area folded in)
+// with which, for x = (x0, x_m, x4) and dun = n . x_m,
+//   y0  = a1 x0 + c7 dun + c8 x4
+//   y_r = U_r y0 + n_r (c4 dun - c1 x4) + lr x_r          (r = 1..3)
+//   y4  = l9 x0 + c10 dun + lr (U . x_m) + c11 x4
+// is y = area K x.  With U and n, which both directions of a face share,
+// 15 numbers hold the matrix that roe_k_matrix spells out in 25.
+// A face record holds both directions: [+ (9) | - (9) | U (3) | n (3)];
+// a sweep slot holds one: [dir (9) | U (3) | n (3)].
+enum { CK_A1, CK_C7, CK_C8, CK_C4, CK_C1, CK_LR, CK_L9, CK_C10, CK_C11, CK_DIR };
+constexpr int CK_FACE = 2 * CK_DIR + 6;  // 24
+constexpr int CK_SLOT = CK_DIR + 6;      // 15
+
+template <class TB>
+__device__ __forceinline__ void jac_roe_compact(const RoeAvg& s, double area, const Gas& g, int dir,
+                                                TB* c) {
+  const RoeK k = roe_k_smoothed(s, g, dir);
+  c[CK_A1] = TB(area * (k.l1 * k.rT));
+  c[CK_C7] = TB(area * k.c7);
+  c[CK_C8] = TB(area * k.c8);
+  c[CK_C4] = TB(area * k.c4);
+  c[CK_C1] = TB(area * k.c1);
+  c[CK_LR] = TB(area * (k.l1 * k.rho));
+  c[CK_L9] = TB(area * (k.l1 * k.c9));
+  c[CK_C10] = TB(area * k.c10);
+  c[CK_C11] = TB(area * k.c11);
+}
+
+// The 25 entries (row-major) of the matrix held by direction coefficients
+// c[9] and the face's U[3], n[3]; each entry evaluated in FP64 and rounded
+// once, as roe_k_matrix does.
+template <class TB>
+__device__ __forceinline__ void compact_expand(const TB* c, const TB* Uf, const TB* nf, TB* M) {
+  const double a1 = c[CK_A1], c7 = c[CK_C7], c8 = c[CK_C8], c4 = c[CK_C4], c1 = c[CK_C1];
+  const double lr = c[CK_LR], l9 = c[CK_L9], c10 = c[CK_C10], c11 = c[CK_C11];
+  const double U[3] = {double(Uf[0]), double(Uf[1]), double(Uf[2])};
+  const double n[3] = {double(nf[0]), double(nf[1]), double(nf[2])};
+  M[0] = TB(a1);
+#pragma unroll
+  for (int m = 0; m < 3; ++m) M[1 + m] = TB(n[m] * c7);
+  M[4] = TB(c8);
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    M[5 * (1 + r)] = TB(a1 * U[r]);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      double v = n[m] * (c7 * U[r] + n[r] * c4);
+      if (r == m) v += lr;
+      M[5 * (1 + r) + 1 + m] = TB(v);
+    }
+    M[5 * (1 + r) + 4] = TB(c8 * U[r] - n[r] * c1);
+  }
+  M[20] = TB(l9);
+#pragma unroll
+  for (int m = 0; m < 3; ++m) M[21 + m] = TB(n[m] * c10 + lr * U[m]);
+  M[24] = TB(c11);
+}
+
+// y += M x for the matrix of one sweep slot s[15] (coefficients, U, n), in
+// the iterate's precision
+template <class TB, class TX>
+__device__ __forceinline__ void compact_apply(const TB* s, const TX* x, TX* y) {
+  const TX a1 = TX(s[CK_A1]), c7 = TX(s[CK_C7]), c8 = TX(s[CK_C8]), c4 = TX(s[CK_C4]);
+  const TX c1 = TX(s[CK_C1]), lr = TX(s[CK_LR]), l9 = TX(s[CK_L9]), c10 = TX(s[CK_C10]);
+  const TX c11 = TX(s[CK_C11]);
+  const TX U0 = TX(s[CK_DIR]), U1 = TX(s[CK_DIR + 1]), U2 = TX(s[CK_DIR + 2]);
+  const TX n0 = TX(s[CK_DIR + 3]), n1 = TX(s[CK_DIR + 4]), n2 = TX(s[CK_DIR + 5]);
+  const TX dun = n0 * x[1] + n1 * x[2] + n2 * x[3];
+  const TX y0 = a1 * x[0] + c7 * dun + c8 * x[4];
+  const TX w = c4 * dun - c1 * x[4];
+  y[0] += y0;
+  y[1] += U0 * y0 + n0 * w + lr * x[1];
+  y[2] += U1 * y0 + n1 * w + lr * x[2];
+  y[3] += U2 * y0 + n2 * w + lr * x[3];
+  y[4] += l9 * x[0] + c10 * dun + lr * (U0 * x[1] + U1 * x[2] + U2 * x[3]) + c11 * x[4];
 }
 
 // hllc_flux (fluxInviscid.loci:157-256) and the HLL two-wave flux built on
