@@ -243,7 +243,11 @@ int fpsi_get_dtau(fpsi_ctx* ctx, double* dtau);
 int fpsi_assemble(fpsi_ctx* ctx);
 /* optional export of the assembled blocks (caller order, row-major 25 per
  * entity, as float in REF/MIXED and as double in FP64 precision):
- * D (nc*25, before factorisation), fjp and fjm (nfaces*25), B (nc*5). */
+ * D (nc*25, before factorisation), fjp and fjm (nfaces*25), B (nc*5).
+ * An inviscid system relaxed by multi-colour SGS keeps its face Jacobians
+ * in the compact Roe form (9 coefficients per direction plus the face's
+ * Roe velocity and normal); fjp and fjm are then expanded from it on this
+ * call, each entry evaluated in FP64 and rounded once. */
 int fpsi_get_blocks(fpsi_ctx* ctx, void* D, void* fjp, void* fjm, void* B);
 
 /* relaxation of  A dq = B.  x0 (nc*5 AoS) NULL selects the reference start
