@@ -115,13 +115,16 @@ __global__ void k_bc_state(MeshView M, const double* __restrict__ q, const fpsi_
 }
 
 // ---------------------------------------------------------------------------
-// least-squares gradient + limiter, one thread per cell
+// least-squares gradient + limiter, one thread per cell.  The CTA's 128
+// gradient (120 B) and limiter (40 B) records are contiguous: they are
+// staged in shared memory and written back with consecutive threads on
+// consecutive addresses.
 // ---------------------------------------------------------------------------
-__global__ void k_grad_limiter(MeshView M, const double* __restrict__ q,
-                               const double* __restrict__ qb, int limiter, double Kl,
-                               double* __restrict__ grad, double* __restrict__ phi) {
-  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (c >= M.nc) return;
+constexpr int GRAD_THREADS = 128;
+
+__device__ __forceinline__ void grad_limiter_cell(const MeshView& M, const double* __restrict__ q,
+                                                  const double* __restrict__ qb, int limiter,
+                                                  double Kl, int64_t c, double* go, double* po) {
   double qc[5];
   q_arr(load_q(q, c), qc);
   double b[15];
@@ -186,27 +189,41 @@ __global__ void k_grad_limiter(MeshView M, const double* __restrict__ q,
 #pragma unroll
       for (int k = 0; k < 5; ++k) {
         const double d2 = g[3 * k] * rx + g[3 * k + 1] * ry + g[3 * k + 2] * rz;
+        // min(1, a / b) divides only where the ratio is below 1 (a
+        // correctly rounded quotient is >= 1 exactly when a >= b for b > 0),
+        // so the result is the same bit for bit
         double p = 1.0;
         if (d2 != 0.0) {
           const double d1 = d2 > 0 ? qmax[k] - qc[k] : qmin[k] - qc[k];
           if (limiter == FPSI_LIMITER_BARTH) {
-            p = dmin(1.0, d1 / d2);
+            if (d2 > 0 ? d1 < d2 : d1 > d2) p = d1 / d2;
           } else {
             const double num = (d1 * d1 + eps2) + 2.0 * d2 * d1;
             const double den = d1 * d1 + 2.0 * d2 * d2 + d1 * d2 + eps2;
-            p = dmin(1.0, num / den);
+            if (num < den) p = num / den;
           }
         }
         ph[k] = dmin(ph[k], p);
       }
     }
   }
-  double* go = grad + 15 * c;
 #pragma unroll
   for (int k = 0; k < 15; ++k) go[k] = g[k];
-  double* po = phi + 5 * c;
 #pragma unroll
   for (int k = 0; k < 5; ++k) po[k] = ph[k];
+}
+
+__global__ void __launch_bounds__(GRAD_THREADS)
+k_grad_limiter(MeshView M, const double* __restrict__ q, const double* __restrict__ qb, int limiter,
+               double Kl, double* __restrict__ grad, double* __restrict__ phi) {
+  __shared__ double sg[GRAD_THREADS * 15], sp[GRAD_THREADS * 5];
+  const int64_t c0 = int64_t(blockIdx.x) * GRAD_THREADS;
+  const int64_t c = c0 + threadIdx.x;
+  const int cnt = int(min(int64_t(GRAD_THREADS), M.nc - c0));
+  if (c < M.nc) grad_limiter_cell(M, q, qb, limiter, Kl, c, sg + 15 * threadIdx.x, sp + 5 * threadIdx.x);
+  __syncthreads();
+  for (int i = threadIdx.x; i < 15 * cnt; i += GRAD_THREADS) grad[15 * c0 + i] = sg[i];
+  for (int i = threadIdx.x; i < 5 * cnt; i += GRAD_THREADS) phi[5 * c0 + i] = sp[i];
 }
 
 // MUSCL states of one face: q_c + phi*grad.(x_f - x_c), floors 0.1*min(T),
@@ -1273,7 +1290,7 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
     prof_end(x);
   }
   prof_begin(x, "grad_limiter");
-  dev::k_grad_limiter<<<blocks_for(M.nc, 128), 128, 0, s>>>(M, x->d_q, x->d_qb, x->P.limiter,
+  dev::k_grad_limiter<<<blocks_for(M.nc, dev::GRAD_THREADS), dev::GRAD_THREADS, 0, s>>>(M, x->d_q, x->d_qb, x->P.limiter,
                                                              x->P.Kl, x->d_grad, x->d_phi);
   prof_end(x);
   prof_begin(x, "face_flux");
