@@ -829,7 +829,7 @@ constexpr size_t asm_smem_bytes() {
 // face) and the slots are written compact (CK_SLOT values); otherwise as
 // explicit (fjp, fjm) pairs into 25-value slots.
 template <class TB, class TX, bool CPT>
-__global__ void __launch_bounds__(ASM_THREADS, sizeof(TB) == 4 ? 6 : 4)
+__global__ void __launch_bounds__(ASM_THREADS, sizeof(TB) == 4 ? (CPT ? 5 : 6) : 4)
 k_assemble(MeshView M, SweepView S, const double* __restrict__ q, const double* __restrict__ src,
            const double* __restrict__ dtau, const TB* __restrict__ fjp, const TB* __restrict__ fjm,
            const TB* __restrict__ fjc, Gas g, TB* __restrict__ luc, TB* __restrict__ bcv,
