@@ -312,7 +312,7 @@ int fpsi_destroy(fpsi_ctx* x) {
   free_sa(x);
   void* ps[] = {x->d_cl, x->d_cr, x->d_n, x->d_area, x->d_rL, x->d_rR, x->d_vol, x->d_cc,
                 x->d_Minv, x->d_cf_off, x->d_cf, x->d_colour_cells, x->d_bcs, x->d_q,
-                x->d_qb, x->d_grad, x->d_phi, x->d_F, x->d_mev, x->d_src, x->d_dtau, x->d_tmu,
+                x->d_qb, x->d_grad, x->d_phi, x->d_F, x->d_src, x->d_dtau, x->d_tmu,
                 x->d_part, x->d_resid, x->d_amin, x->d_err, x->d_perm, x->d_stage, x->d_ci, x->d_ccol,
                 x->d_nbr, x->d_colinfo, x->d_cnb_off, x->d_cnb, x->d_xprev};
   for (void* p : ps)
@@ -401,8 +401,7 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
   TRY(dalloc(x, &x->d_qb, std::max<int64_t>(H.nbf, 1) * 5));
   TRY(dalloc(x, &x->d_grad, nc * 15));
   TRY(dalloc(x, &x->d_phi, nc * 5));
-  TRY(dalloc(x, &x->d_F, nf * 5));
-  TRY(dalloc(x, &x->d_mev, nf));
+  TRY(dalloc(x, &x->d_F, nf * fpsi::FREC));
   TRY(dalloc(x, &x->d_src, nc * 5));
   TRY(dalloc(x, &x->d_dtau, nc));
   TRY(dalloc(x, &x->d_tmu, nc));

@@ -10,6 +10,10 @@
 
 namespace fpsi {
 
+// doubles per face record of the flux array: the flux (5) and maxev_f*area,
+// 48 B so that the record is three aligned 16 B accesses
+constexpr int FREC = 6;
+
 void set_error(const char* fmt, ...);
 
 #define FPSI_CUDA_TRY(expr)                                                          \
@@ -120,8 +124,7 @@ struct fpsi_ctx {
   double* d_qb = nullptr;      // [nbf][5] boundary face states
   double* d_grad = nullptr;    // [nc][15]
   double* d_phi = nullptr;     // [nc][5]
-  double* d_F = nullptr;       // [nf][5] face fluxes
-  double* d_mev = nullptr;     // [nf] maxev_f * area
+  double* d_F = nullptr;       // [nf][FREC]: face flux (5) and maxev_f * area
   double* d_src = nullptr;     // [nc][5]
   double* d_dtau = nullptr;    // [nc]
   double* d_tmu = nullptr;     // [nc] eddy viscosity (flowRegime turbulent)

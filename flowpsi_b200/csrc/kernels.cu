@@ -4,7 +4,8 @@
 //   q      [nc][5]  FP64  T,u,v,w,pg          (AoS: every gather is one 40 B record)
 //   grad   [nc][15] FP64  dT/dx.. dpg/dz
 //   phi    [nc][5]  FP64  limiter per variable
-//   F      [nf][5]  FP64  face flux, mev [nf] maxev_f*area
+//   F      [nf][6]  FP64  face flux (5) and maxev_f*area: one 48 B record,
+//                         three 16 B accesses
 //   src    [nc][5]  FP64, dtau [nc]
 //   fjp/fjm [nf][25] TB   (TB = float in REF/MIXED precision, double in FP64)
 //   sweeps, colour order (ci = position of the cell in its colour's list):
@@ -418,7 +419,7 @@ template <bool VIS>
 __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
                             const double* __restrict__ qb, const double* __restrict__ grad,
                             const double* __restrict__ phi, Gas g, int kind, Visc V,
-                            double* __restrict__ F, double* __restrict__ mev) {
+                            double* __restrict__ F) {
   const int64_t f = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (f >= M.nf) return;
   FaceStates s;
@@ -438,9 +439,6 @@ __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
 #pragma unroll
     for (int k = 0; k < 4; ++k) fl[1 + k] -= v.vf[k];
   }
-  double* o = F + 5 * f;
-#pragma unroll
-  for (int k = 0; k < 5; ++k) o[k] = fl[k];
   // maxev_f (solverSetup.loci:81-105), eta == 1: |u.n| + a of each side
   const double utr = s.qr[1] * nx + s.qr[2] * ny + s.qr[3] * nz;
   const double ar = sqrt(g.gamma * g.Rt * s.qr[0]);
@@ -452,7 +450,10 @@ __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
     const double sl = sqrt(4.0 * al * al);
     m = dmax(0.5 * dmax(fabs(2.0 * utl - sl), fabs(2.0 * utl + sl)), m);
   }
-  mev[f] = m * A;
+  double2* o = reinterpret_cast<double2*>(F + FREC * f);
+  o[0] = make_double2(fl[0], fl[1]);
+  o[1] = make_double2(fl[2], fl[3]);
+  o[2] = make_double2(fl[4], m * A);
 }
 
 // ---------------------------------------------------------------------------
@@ -462,7 +463,7 @@ constexpr int NORM_THREADS = 256;
 
 __global__ void __launch_bounds__(NORM_THREADS)
 k_cell_residual(MeshView M, const double* __restrict__ q, const double* __restrict__ F,
-                const double* __restrict__ mev, Gas g, double urelax, double dtmax,
+                Gas g, double urelax, double dtmax,
                 double cflmax, double vol_tot, double* __restrict__ src,
                 double* __restrict__ dtau, double* __restrict__ part) {
   const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -474,7 +475,9 @@ k_cell_residual(MeshView M, const double* __restrict__ q, const double* __restri
     for (int32_t e = M.cf_off[c]; e < M.cf_off[c + 1]; ++e) {
       const int32_t ent = M.cf[e];
       const int64_t f = ent >> 1;
-      const double* p = F + 5 * f;
+      const double2* p2 = reinterpret_cast<const double2*>(F + FREC * f);
+      const double2 a = p2[0], b = p2[1], c = p2[2];
+      const double p[5] = {a.x, a.y, b.x, b.y, c.x};
       if (ent & 1) {
 #pragma unroll
         for (int k = 0; k < 5; ++k) s[k] += p[k];
@@ -482,7 +485,7 @@ k_cell_residual(MeshView M, const double* __restrict__ q, const double* __restri
 #pragma unroll
         for (int k = 0; k < 5; ++k) s[k] -= p[k];
       }
-      meva += mev[f];
+      meva += c.y;
     }
     double* so = src + 5 * c;
 #pragma unroll
@@ -1298,14 +1301,14 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
   // does not carry their registers
   if (x->P.viscous)
     dev::k_face_flux<true><<<blocks_for(M.nf, 128), 128, 0, s>>>(
-        M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, x->P.flux, visc(x), x->d_F, x->d_mev);
+        M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, x->P.flux, visc(x), x->d_F);
   else
     dev::k_face_flux<false><<<blocks_for(M.nf, 128), 128, 0, s>>>(
-        M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, x->P.flux, visc(x), x->d_F, x->d_mev);
+        M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, x->P.flux, visc(x), x->d_F);
   prof_end(x);
   prof_begin(x, "cell_residual");
   dev::k_cell_residual<<<x->nblk_norm, dev::NORM_THREADS, 0, s>>>(
-      M, x->d_q, x->d_F, x->d_mev, g, x->P.urelax, x->P.dtmax, x->P.cflmax, x->H.vol_tot,
+      M, x->d_q, x->d_F, g, x->P.urelax, x->P.dtmax, x->P.cflmax, x->H.vol_tot,
       x->d_src, x->d_dtau, x->d_part);
   dev::k_norm_final<<<1, dev::NORM_THREADS, 0, s>>>(x->d_part, x->nblk_norm, resid_slot);
   prof_end(x);

@@ -156,7 +156,7 @@ __global__ void k_sa_face(Geo G, const double* __restrict__ q, const double* __r
   if (f >= nf) return;
   const double n0 = G.n[f], n1 = G.n[nf + f], n2 = G.n[2 * nf + f];
   const double A = G.area[f];
-  const double mdot = F[5 * f];  // scalar_mdot_f = iflux[0]
+  const double mdot = F[FREC * f];  // scalar_mdot_f = iflux[0]
   const int64_t a = G.cl[f];
   const double* ga = sgrad + 3 * a;
   const double rl0 = G.rL[f], rl1 = G.rL[nf + f], rl2 = G.rL[2 * nf + f];
@@ -254,7 +254,7 @@ __global__ void k_sa_cell(Geo G, const double* __restrict__ q, const double* __r
   for (int32_t e = G.cf_off[c]; e < G.cf_off[c + 1]; ++e) {
     const int32_t ent = G.cf[e];
     const int64_t f = ent >> 1;
-    const double mdot = F[5 * f];
+    const double mdot = F[FREC * f];
     if (ent & 1) {  // lower face: this cell is cr
       src += fo[f];
       rhodot += mdot;
