@@ -258,8 +258,15 @@ __host__ __device__ inline TcSmem tc_smem(int fin) {
 // group 0..3); the epilogue's warp w reads accumulator lanes 32(w%4).. and
 // columns 32(w/4)...  Every wait is bounded; a wait that gives up sets bit 1
 // of err, waits once more for the MMAs in flight and frees the tensor memory.
+// CTAs per SM: three for the BF16 layers (80 registers), two for the
+// first layer, whose FP32 input chunks need more registers
+template <class TIn>
+constexpr int tc_ctas_per_sm() {
+  return sizeof(TIn) == 2 ? 3 : 2;
+}
+
 template <class TIn, bool HEAD>
-__global__ void __launch_bounds__(TC_THREADS, 2)
+__global__ void __launch_bounds__(TC_THREADS, tc_ctas_per_sm<TIn>())
 k_layer_tc(int64_t nc, int fin, const TIn* __restrict__ h, const int32_t* __restrict__ off,
            const int32_t* __restrict__ nb, const __nv_bfloat16* __restrict__ ws,
            const __nv_bfloat16* __restrict__ wn, const __nv_bfloat16* __restrict__ bias,
@@ -310,7 +317,7 @@ k_layer_tc(int64_t nc, int fin, const TIn* __restrict__ h, const int32_t* __rest
   const int64_t ntiles = (nc + TC_ROWS - 1) / TC_ROWS;
   const int rs = lane & 7, cg = lane >> 3;     // staging: row within 8, chunk group
   const int q = warp & 3, hf = warp >> 2;      // epilogue: lane quarter, column half
-  constexpr int CPI = sizeof(TIn) == 2 ? 2 : 1;  // chunks of a row gathered together
+  constexpr int CPI = 1;  // chunks of a row gathered together
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int64_t row0 = t * TC_ROWS;
     // ---- stage A = [h | neighbour mean] for rows 16 warp .. 16 warp + 15.
@@ -748,7 +755,11 @@ int forward(fpsi_gnn* m, const Graph& G, const float* feat, bool keep) {
   cudaStream_t s = m->stream;
   const int64_t nc = G.nc;
   const int64_t ntiles = (nc + TC_ROWS - 1) / TC_ROWS;
-  const unsigned grid = unsigned(std::max<int64_t>(1, std::min<int64_t>(ntiles, 2 * int64_t(m->nsm))));
+  auto grid_for = [&](int per_sm) {
+    return unsigned(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(per_sm) * m->nsm)));
+  };
+  const unsigned grid = grid_for(tc_ctas_per_sm<__nv_bfloat16>());
+  const unsigned grid0 = grid_for(tc_ctas_per_sm<float>());
   const __nv_bfloat16 *wo = m->d_wb + m->L.wo, *bo = m->d_wb + m->L.bo;
   for (int l = 0; l < NLAYER; ++l) {
     const int fin = m->L.fan_in[l];
@@ -759,7 +770,7 @@ int forward(fpsi_gnn* m, const Graph& G, const float* feat, bool keep) {
     const bool last = l == NLAYER - 1;
     __nv_bfloat16* hout = (last && !keep) ? nullptr : m->d_h[l + 1];
     if (l == 0)
-      k_layer_tc<float, false><<<grid, TC_THREADS, smem, s>>>(nc, fin, feat, G.off, G.nb, ws, wn, b, wo, bo, agg,
+      k_layer_tc<float, false><<<grid0, TC_THREADS, smem, s>>>(nc, fin, feat, G.off, G.nb, ws, wn, b, wo, bo, agg,
                                                               z, hout, nullptr, m->d_err);
     else if (!last)
       k_layer_tc<__nv_bfloat16, false><<<grid, TC_THREADS, smem, s>>>(nc, fin, m->d_h[l], G.off, G.nb, ws, wn, b,
