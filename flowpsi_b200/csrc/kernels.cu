@@ -442,12 +442,12 @@ __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
   // maxev_f (solverSetup.loci:81-105), eta == 1: |u.n| + a of each side
   const double utr = s.qr[1] * nx + s.qr[2] * ny + s.qr[3] * nz;
   const double ar = sqrt(g.gamma * g.Rt * s.qr[0]);
-  const double sr = sqrt(4.0 * ar * ar);
+  const double sr = 2.0 * ar;  // sqrt(4 a^2) of the reference, to an ulp
   double m = 0.5 * dmax(fabs(2.0 * utr - sr), fabs(2.0 * utr + sr));
   if (f < M.nfi) {
     const double utl = s.ql[1] * nx + s.ql[2] * ny + s.ql[3] * nz;
     const double al = sqrt(g.gamma * g.Rt * s.ql[0]);
-    const double sl = sqrt(4.0 * al * al);
+    const double sl = 2.0 * al;  // sqrt(4 a^2) of the reference, to an ulp
     m = dmax(0.5 * dmax(fabs(2.0 * utl - sl), fabs(2.0 * utl + sl)), m);
   }
   double2* o = reinterpret_cast<double2*>(F + FREC * f);

@@ -176,15 +176,15 @@ __device__ __forceinline__ void flux_roe(const Q5& L, const Q5& R, double nx, do
   const double dT = R.T - L.T, dp = R.p - L.p;
   const double du = R.u - L.u, dv = R.v - L.v, dw = R.w - L.w;
   const double uj = du * nx + dv * ny + dw * nz;
-  const double i2s = 2.0 * s.sigma;
+  // the six quotients by sigma and 2 sigma share one reciprocal (each term
+  // moves by at most an ulp against the division)
+  const double isg = 1.0 / s.sigma;
+  const double dsg = k.d23 * isg, tsg = s.r * k.t4 * uj * (0.5 * isg);
   double d[5];
   d[0] = dp * k.c8 + uj * k.c7 + l1 * dT * k.rT;
-  d[1] = s.U * k.c7 * uj + l1 * (s.U * dT * k.rT + s.r * du) + dp * (k.c8 * s.U - nx * k.d23 / s.sigma) +
-         nx * s.r * k.t4 * uj / i2s;
-  d[2] = s.V * k.c7 * uj + l1 * (s.V * dT * k.rT + s.r * dv) + dp * (k.c8 * s.V - ny * k.d23 / s.sigma) +
-         ny * s.r * k.t4 * uj / i2s;
-  d[3] = s.W * k.c7 * uj + l1 * (s.W * dT * k.rT + s.r * dw) + dp * (k.c8 * s.W - nz * k.d23 / s.sigma) +
-         nz * s.r * k.t4 * uj / i2s;
+  d[1] = s.U * k.c7 * uj + l1 * (s.U * dT * k.rT + s.r * du) + dp * (k.c8 * s.U - nx * dsg) + nx * tsg;
+  d[2] = s.V * k.c7 * uj + l1 * (s.V * dT * k.rT + s.r * dv) + dp * (k.c8 * s.V - ny * dsg) + ny * tsg;
+  d[3] = s.W * k.c7 * uj + l1 * (s.W * dT * k.rT + s.r * dw) + dp * (k.c8 * s.W - nz * dsg) + nz * tsg;
   d[4] = dp * k.c11 + k.c10 * uj + l1 * (k.c9 * dT + s.r * (s.U * du + s.V * dv + s.W * dw));
   const double ah = 0.5 * area;
   const double ml = s.rl * unl, mr = s.rr * unr;
