@@ -69,14 +69,11 @@ std::vector<double> soa3(const std::vector<double>& a, int64_t n) {
 }
 
 void free_system(fpsi_ctx* x) {
-  // a side-stream Jacobian may still write the face records
-  if (x->jstream) cudaStreamSynchronize(x->jstream);
   void* ps[] = {x->d_fjp, x->d_fjm, x->d_fjc, x->d_D, x->d_x, x->d_luc, x->d_bc, x->d_pv, x->d_aoff};
   for (void* p : ps)
     if (p) cudaFree(p);
   x->d_fjp = x->d_fjm = x->d_fjc = x->d_D = x->d_x = x->d_luc = x->d_bc = x->d_aoff = nullptr;
   x->d_pv = nullptr;
-  x->fjc_ready = false;
 }
 
 int alloc_system(fpsi_ctx* x) {
@@ -322,12 +319,6 @@ int fpsi_destroy(fpsi_ctx* x) {
     if (p) cudaFree(p);
   if (x->h_resid) cudaFreeHost(x->h_resid);
   for (cudaEvent_t e : x->evpool) cudaEventDestroy(e);
-  if (x->jstream) {
-    cudaStreamSynchronize(x->jstream);
-    cudaStreamDestroy(x->jstream);
-  }
-  if (x->ev_grad) cudaEventDestroy(x->ev_grad);
-  if (x->ev_jac) cudaEventDestroy(x->ev_jac);
   if (x->stream) cudaStreamDestroy(x->stream);
   delete x;
   return FPSI_OK;
@@ -958,7 +949,7 @@ int fpsi_newton_step(fpsi_ctx* x, fpsi_stepinfo* info) {
   int rc;
   const bool sa = fpsi::sa_active(x);
   if (sa && (rc = fpsi::sa_launch_tmu(x))) return rc;
-  if ((rc = fpsi::launch_residual(x, x->d_resid, true))) return rc;
+  if ((rc = fpsi::launch_residual(x, x->d_resid))) return rc;
   if (sa && ((rc = fpsi::sa_launch_residual(x)) || (rc = fpsi::sa_launch_solve(x)))) return rc;
   if ((rc = fpsi::launch_assemble(x))) return rc;
   if (is_lsgs(x)) {
@@ -992,7 +983,7 @@ static int run_steps(fpsi_ctx* x, int32_t nsteps, double* hist) {
   const bool sa = fpsi::sa_active(x);
   for (int32_t s = 0; s < nsteps && !rc; ++s) {
     if (sa) rc = fpsi::sa_launch_tmu(x);
-    if (!rc) rc = fpsi::launch_residual(x, hist + 8 * s, true);
+    if (!rc) rc = fpsi::launch_residual(x, hist + 8 * s);
     if (!rc && sa) rc = fpsi::sa_launch_residual(x);
     if (!rc && sa) rc = fpsi::sa_launch_solve(x);
     if (!rc) rc = fpsi::launch_assemble(x);

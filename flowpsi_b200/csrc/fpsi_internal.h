@@ -109,11 +109,6 @@ struct fpsi_ctx {
   std::vector<fpsi_bc> bcs;
   int device = 0;
   cudaStream_t stream = nullptr;
-  // side stream of the chained step: a compact system's face Jacobians run
-  // on it beside the flux and residual kernels (ev_grad: gradients ready;
-  // ev_jac: records written)
-  cudaStream_t jstream = nullptr;
-  cudaEvent_t ev_grad = nullptr, ev_jac = nullptr;
   // ---- device arrays (new numbering) ----
   // geometry
   int32_t *d_cl = nullptr, *d_cr = nullptr;
@@ -145,7 +140,6 @@ struct fpsi_ctx {
   void* d_fjc = nullptr;       // [nf][24] TB
   bool asm_compact = false;    // the assembled system's slots are compact
   bool have_explicit = false;  // fjp/fjm hold the assembled system's blocks
-  bool fjc_ready = false;      // fjc for the last residual's state is on jstream (ev_jac)
   void* d_D = nullptr;         // [nc][25] TB (only when keep_D)
   // colour-order arrays of the sweeps (see HostMesh)
   void* d_luc = nullptr;       // per colour [25][n_k] TB: LU factors of fluid_D

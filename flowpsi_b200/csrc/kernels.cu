@@ -1282,29 +1282,7 @@ dev::Gas gas(const fpsi_ctx* x) {
 }
 }  // namespace
 
-// Inviscid systems relaxed by multi-colour SGS keep their face Jacobians in
-// the compact Roe form (15 values per sweep slot instead of 25); viscous
-// terms and the line solver need the explicit blocks.
-static bool compact_blocks(const fpsi_ctx* x) {
-  return !x->P.viscous && x->P.solver == FPSI_SOLVER_SGS;
-}
-
-static int side_stream(fpsi_ctx* x) {
-  if (x->jstream) return FPSI_OK;
-  FPSI_CUDA_TRY(cudaStreamCreateWithFlags(&x->jstream, cudaStreamNonBlocking));
-  FPSI_CUDA_TRY(cudaEventCreateWithFlags(&x->ev_grad, cudaEventDisableTiming));
-  FPSI_CUDA_TRY(cudaEventCreateWithFlags(&x->ev_jac, cudaEventDisableTiming));
-  return FPSI_OK;
-}
-
-template <class TB>
-static void launch_jacobian_c(fpsi_ctx* x, cudaStream_t s) {
-  const dev::MeshView M = view(x);
-  dev::k_face_jacobian_c<TB><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
-      M, x->d_q, x->d_qb, x->d_grad, x->d_phi, gas(x), (TB*)x->d_fjc);
-}
-
-int launch_residual(fpsi_ctx* x, double* resid_slot, bool early_jac) {
+int launch_residual(fpsi_ctx* x, double* resid_slot) {
   const dev::MeshView M = view(x);
   const dev::Gas g = gas(x);
   cudaStream_t s = x->stream;
@@ -1318,24 +1296,6 @@ int launch_residual(fpsi_ctx* x, double* resid_slot, bool early_jac) {
   dev::k_grad_limiter<<<blocks_for(M.nc, dev::GRAD_THREADS), dev::GRAD_THREADS, 0, s>>>(M, x->d_q, x->d_qb, x->P.limiter,
                                                              x->P.Kl, x->d_grad, x->d_phi);
   prof_end(x);
-  // per-kernel profiling keeps every launch on the one stream.  A side-stream
-  // Jacobian of an earlier residual that was never assembled may still be
-  // writing the records: this stream waits for it first.
-  if (x->jstream) FPSI_CUDA_TRY(cudaStreamWaitEvent(s, x->ev_jac, 0));
-  x->fjc_ready = false;
-  if (early_jac && compact_blocks(x) && !x->profiling) {
-    int rc = side_stream(x);
-    if (rc) return rc;
-    FPSI_CUDA_TRY(cudaEventRecord(x->ev_grad, s));
-    FPSI_CUDA_TRY(cudaStreamWaitEvent(x->jstream, x->ev_grad, 0));
-    if (x->P.precision == FPSI_PREC_FP64)
-      launch_jacobian_c<double>(x, x->jstream);
-    else
-      launch_jacobian_c<float>(x, x->jstream);
-    FPSI_CUDA_TRY(cudaGetLastError());
-    FPSI_CUDA_TRY(cudaEventRecord(x->ev_jac, x->jstream));
-    x->fjc_ready = true;
-  }
   prof_begin(x, "face_flux");
   // the viscous terms are a separate instantiation: the inviscid kernel
   // does not carry their registers
@@ -1369,6 +1329,12 @@ static dev::SweepView sweep_view(const fpsi_ctx* x) {
   return S;
 }
 
+// Inviscid systems relaxed by multi-colour SGS keep their face Jacobians in
+// the compact Roe form (15 values per sweep slot instead of 25); viscous
+// terms and the line solver need the explicit blocks.
+static bool compact_blocks(const fpsi_ctx* x) {
+  return !x->P.viscous && x->P.solver == FPSI_SOLVER_SGS;
+}
 
 template <class TB, class TX, bool CPT>
 static void launch_assemble_kernel(fpsi_ctx* x, const dev::MeshView& M, const dev::Gas& g) {
@@ -1393,22 +1359,17 @@ static int launch_assemble_t(fpsi_ctx* x) {
   const bool cpt = compact_blocks(x);
   x->asm_compact = cpt;
   x->have_explicit = !cpt;
-  if (cpt && x->fjc_ready) {
-    // started on the side stream by the residual of this state
-    FPSI_CUDA_TRY(cudaStreamWaitEvent(s, x->ev_jac, 0));
-    x->fjc_ready = false;
-  } else {
-    prof_begin(x, "face_jacobian");
-    if (cpt)
-      launch_jacobian_c<TB>(x, s);
-    else if (x->P.viscous)
-      dev::k_face_jacobian<TB, true><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
-          M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, visc(x), fjp, fjm);
-    else
-      dev::k_face_jacobian<TB, false><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
-          M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, visc(x), fjp, fjm);
-    prof_end(x);
-  }
+  prof_begin(x, "face_jacobian");
+  if (cpt)
+    dev::k_face_jacobian_c<TB><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
+        M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, (TB*)x->d_fjc);
+  else if (x->P.viscous)
+    dev::k_face_jacobian<TB, true><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
+        M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, visc(x), fjp, fjm);
+  else
+    dev::k_face_jacobian<TB, false><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
+        M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, visc(x), fjp, fjm);
+  prof_end(x);
   prof_begin(x, "assemble_lu");
   if (cpt)
     launch_assemble_kernel<TB, TX, true>(x, M, g);

@@ -10,9 +10,7 @@ namespace fpsi {
 
 // residual chain: boundary states, gradient+limiter, face flux, per-cell
 // gather (src, dtau), norms into resid_slot[8] (device)
-// early_jac: the caller assembles next; a compact system's face Jacobians
-// then start on the side stream as soon as the gradients are ready
-int launch_residual(fpsi_ctx* x, double* resid_slot, bool early_jac = false);
+int launch_residual(fpsi_ctx* x, double* resid_slot);
 // face Jacobians, diagonal blocks, LU, B and the starting iterate
 // (the starting iterate is the block Jacobi start D^-1 B)
 int launch_assemble(fpsi_ctx* x);
