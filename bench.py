@@ -45,28 +45,67 @@ def load_peaks():
 
 
 class Clocks:
-    """nvidia-smi sampler over the timed region"""
+    """SM clocks and clock-event reasons sampled over the timed region: NVML
+    read every 20 ms from a thread (the same counters nvidia-smi prints),
+    or an nvidia-smi sampler when NVML is unavailable.  Read-only."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index: int):
-        self.index = index
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        self.p = None
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        parts = [p for p in vis.split(",") if p.strip()]
+        # the CUDA index maps to the NVML index through CUDA_VISIBLE_DEVICES
+        self.index = int(parts[index]) if index < len(parts) and parts[index].strip().isdigit() else index
+        self.samples, self.stop, self.thread, self.p, self.f = [], None, None, None, None
+
+    def _nvml_loop(self, h, nv):
+        bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while True:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), float(mx), [n for n, b in zip(self.NAMES, bits) if r & b]))
+            except Exception:  # noqa: BLE001
+                pass
+            if self.stop.wait(0.02):
+                break
 
     def __enter__(self):
         try:
+            import threading
+
+            import pynvml as nv
+
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._nvml_loop, args=(h, nv), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:  # noqa: BLE001
+            self.thread = None
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.p = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=self.f, stderr=subprocess.DEVNULL)
+            t0 = time.time()  # wait for the first sample before the timed region
+            while time.time() - t0 < 3 and not Path(self.f.name).read_text().strip():
+                time.sleep(0.02)
         except OSError:
             self.p = None
         return self
 
     def __exit__(self, *a):
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(2)
         if self.p:
             self.p.terminate()
             try:
@@ -75,24 +114,27 @@ class Clocks:
                 self.p.kill()
 
     def summary(self):
-        if self.p is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.f.flush()
-        rows = [r.split(",") for r in Path(self.f.name).read_text().splitlines() if r.strip()]
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
-            try:
-                sm.append(float(r[1]))
-                mx.append(float(r[2]))
-                for nm, v in zip(names, r[5:9]):
-                    if v.strip().lower() == "active":
-                        reasons.add(nm)
-            except (ValueError, IndexError):
-                continue
+        if self.thread is not None:
+            rows = self.samples
+            src = "nvml"
+        elif self.p is not None:
+            self.f.flush()
+            rows = []
+            for r in Path(self.f.name).read_text().splitlines():
+                r = r.split(",")
+                try:
+                    rows.append((float(r[1]), float(r[2]),
+                                 [nm for nm, v in zip(self.NAMES, r[5:9]) if v.strip().lower() == "active"]))
+                except (ValueError, IndexError):
+                    continue
+            src = "nvidia-smi"
+        else:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        sm = [r[0] for r in rows]
+        reasons = sorted({n for r in rows for n in r[2]})
         return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "sm_max_mhz": max(r[1] for r in rows) if rows else None, "reasons": reasons,
+                "samples": len(sm), "source": src}
 
 
 def dist_setup():
