@@ -527,35 +527,53 @@ k_cell_residual(MeshView M, const double* __restrict__ q, const double* __restri
     rmax = a0, emax = a4;
     rloc = double(c), eloc = double(c);
   }
-  // fixed-shape block tree: sums and signed max-abs with lowest-index ties
-  __shared__ double sh[8][NORM_THREADS];
-  const int t = threadIdx.x;
-  sh[0][t] = rt, sh[1][t] = et, sh[2][t] = mt;
-  sh[3][t] = rmax, sh[4][t] = rloc, sh[5][t] = emax, sh[6][t] = eloc, sh[7][t] = mmax;
-  __syncthreads();
-  for (int st = NORM_THREADS / 2; st > 0; st >>= 1) {
-    if (t < st) {
-      sh[0][t] += sh[0][t + st];
-      sh[1][t] += sh[1][t + st];
-      sh[2][t] += sh[2][t + st];
-      if (fabs(sh[3][t + st]) > fabs(sh[3][t]) ||
-          (fabs(sh[3][t + st]) == fabs(sh[3][t]) && sh[4][t] < 0)) {
-        sh[3][t] = sh[3][t + st];
-        sh[4][t] = sh[4][t + st];
-      }
-      if (fabs(sh[5][t + st]) > fabs(sh[5][t]) ||
-          (fabs(sh[5][t + st]) == fabs(sh[5][t]) && sh[6][t] < 0)) {
-        sh[5][t] = sh[5][t + st];
-        sh[6][t] = sh[6][t + st];
-      }
-      if (fabs(sh[7][t + st]) > fabs(sh[7][t])) sh[7][t] = sh[7][t + st];
-    }
-    __syncthreads();
-  }
-  if (t == 0) {
-    double* o = part + 8 * int64_t(blockIdx.x);
+  // fixed-shape reduction: sums and signed max-abs with lowest-index ties,
+  // first across each warp's lanes (shuffles), then across the 8 warps
+  const unsigned full = 0xffffffffu;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  auto combine = [&](double& v, double& loc, double ov, double oloc) {
+    if (fabs(ov) > fabs(v) || (fabs(ov) == fabs(v) && loc < 0)) v = ov, loc = oloc;
+  };
 #pragma unroll
-    for (int k = 0; k < 8; ++k) o[k] = sh[k][0];
+  for (int off = 16; off > 0; off >>= 1) {
+    rt += __shfl_down_sync(full, rt, off);
+    et += __shfl_down_sync(full, et, off);
+    mt += __shfl_down_sync(full, mt, off);
+    const double orm = __shfl_down_sync(full, rmax, off), orl = __shfl_down_sync(full, rloc, off);
+    const double oem = __shfl_down_sync(full, emax, off), oel = __shfl_down_sync(full, eloc, off);
+    const double omm = __shfl_down_sync(full, mmax, off);
+    combine(rmax, rloc, orm, orl);
+    combine(emax, eloc, oem, oel);
+    if (fabs(omm) > fabs(mmax)) mmax = omm;
+  }
+  constexpr int NW = NORM_THREADS / 32;
+  __shared__ double sw[8][NW];
+  if (lane == 0) {
+    sw[0][warp] = rt, sw[1][warp] = et, sw[2][warp] = mt, sw[3][warp] = rmax;
+    sw[4][warp] = rloc, sw[5][warp] = emax, sw[6][warp] = eloc, sw[7][warp] = mmax;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const bool in = lane < NW;
+    rt = in ? sw[0][lane] : 0.0, et = in ? sw[1][lane] : 0.0, mt = in ? sw[2][lane] : 0.0;
+    rmax = in ? sw[3][lane] : 0.0, rloc = in ? sw[4][lane] : -1.0;
+    emax = in ? sw[5][lane] : 0.0, eloc = in ? sw[6][lane] : -1.0, mmax = in ? sw[7][lane] : 0.0;
+#pragma unroll
+    for (int off = NW / 2; off > 0; off >>= 1) {
+      rt += __shfl_down_sync(full, rt, off);
+      et += __shfl_down_sync(full, et, off);
+      mt += __shfl_down_sync(full, mt, off);
+      const double orm = __shfl_down_sync(full, rmax, off), orl = __shfl_down_sync(full, rloc, off);
+      const double oem = __shfl_down_sync(full, emax, off), oel = __shfl_down_sync(full, eloc, off);
+      const double omm = __shfl_down_sync(full, mmax, off);
+      combine(rmax, rloc, orm, orl);
+      combine(emax, eloc, oem, oel);
+      if (fabs(omm) > fabs(mmax)) mmax = omm;
+    }
+    if (lane == 0) {
+      double* o = part + 8 * int64_t(blockIdx.x);
+      o[0] = rt, o[1] = et, o[2] = mt, o[3] = rmax, o[4] = rloc, o[5] = emax, o[6] = eloc, o[7] = mmax;
+    }
   }
 }
 
