@@ -136,6 +136,8 @@ __device__ __forceinline__ void grad_limiter_cell(const MeshView& M, const doubl
   for (int k = 0; k < 5; ++k) qmax[k] = qmin[k] = qc[k];
   const int32_t e0 = M.cf_off[c], e1 = M.cf_off[c + 1];
   const int64_t nf = M.nf;
+  // unrolled so that the loads of several faces are in flight together
+#pragma unroll 4
   for (int32_t e = e0; e < e1; ++e) {
     const int32_t ent = M.cf[e];
     const int64_t f = ent >> 1;
@@ -1185,15 +1187,19 @@ k_update(int64_t nc, double pamb, const int32_t* __restrict__ ci, const TX* __re
     qc[3] += alpha * double(d[3]);
     qc[4] += alpha * dp;
   }
-  __shared__ double sh[NORM_THREADS];
-  const int t = threadIdx.x;
-  sh[t] = alpha;
+  // block minimum: warp shuffles, then one exchange across the warps
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) alpha = dmin(alpha, __shfl_down_sync(0xffffffffu, alpha, off));
+  __shared__ double sw[NORM_THREADS / 32];
+  if (lane == 0) sw[warp] = alpha;
   __syncthreads();
-  for (int st = NORM_THREADS / 2; st > 0; st >>= 1) {
-    if (t < st) sh[t] = dmin(sh[t], sh[t + st]);
-    __syncthreads();
+  if (t == 0) {
+    double a = sw[0];
+#pragma unroll
+    for (int w = 1; w < NORM_THREADS / 32; ++w) a = dmin(a, sw[w]);
+    amin_part[blockIdx.x] = a;
   }
-  if (t == 0) amin_part[blockIdx.x] = sh[0];
 }
 
 // caller-order state (T[nc], pg[nc], u[3nc]) <-> device q[nc][5] (RCM order)
