@@ -858,10 +858,16 @@ k_assemble(MeshView M, SweepView S, const double* __restrict__ q, const double* 
            const TB* __restrict__ fjc, Gas g, TB* __restrict__ luc, TB* __restrict__ bcv,
            int32_t* __restrict__ pvv, TB* __restrict__ aoff, TB* __restrict__ Dout, TX* __restrict__ x,
            int32_t* __restrict__ err) {
-  constexpr int RW = CPT ? CK_FACE : 50;        // words staged per face
-  constexpr int BATCH = CPT ? 8 : ASM_BATCH;    // RW / BATCH rounds per lane
+  constexpr int RW = 50;  // words staged per face (explicit blocks)
+  // compact records move in 16 B units: U16 per record, stored record-major
+  // with an odd stride of RS16 units so that a quarter warp's 16 B accesses
+  // hit distinct banks
+  constexpr int U16 = int(CK_FACE * sizeof(TB) / 16), RS16 = U16 + 1;
+  static_assert(CK_FACE * sizeof(TB) % 16 == 0, "a compact record is whole 16 B units");
+  static_assert(32 * RS16 * 16 <= 50 * ASM_STRIDE * sizeof(TB), "fits the warp's staging area");
   extern __shared__ __align__(16) unsigned char asm_smem[];
   TB* st = reinterpret_cast<TB*>(asm_smem) + (threadIdx.x >> 5) * (50 * ASM_STRIDE);
+  uint4* st4 = reinterpret_cast<uint4*>(asm_smem + (threadIdx.x >> 5) * size_t(32 * RS16 * 16));
   const int lane = threadIdx.x & 31;
   const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const bool active = c < M.nc;
@@ -883,28 +889,51 @@ k_assemble(MeshView M, SweepView S, const double* __restrict__ q, const double* 
   int64_t slot = 0;
   for (int e = 0; e < maxdeg; ++e) {
     const int32_t my_ent = e < deg ? M.cf[e0 + e] : -1;
-    // 32 RW words per round, RW per lane, in batches of BATCH independent
-    // loads (fjm is allocated for every face, so every address is valid;
-    // lanes without an entry read face 0 and their words are never used)
-#pragma unroll 1
-    for (int b = 0; b < RW / BATCH; ++b) {
-      TB v[BATCH];
+    if constexpr (CPT) {
+      // the warp's 32 records as 32 * U16 units of 16 B, U16 per lane, all
+      // in flight together (lanes without an entry read face 0; their units
+      // are never used)
+      constexpr int HALF = U16 > 6 ? U16 / 2 : U16;  // units held in registers at once
 #pragma unroll
-      for (int u = 0; u < BATCH; ++u) {
-        const int idx = lane + 32 * (BATCH * b + u);
-        const int L = idx / RW, k = idx - RW * L;
-        const int32_t ent = __shfl_sync(0xffffffffu, my_ent, L);
-        const int64_t f = ent >= 0 ? int64_t(ent >> 1) : 0;
-        if constexpr (CPT)
-          v[u] = __ldg(fjc + CK_FACE * f + k);
-        else
-          v[u] = k < 25 ? __ldg(fjp + 25 * f + k) : __ldg(fjm + 25 * f + (k - 25));
+      for (int h = 0; h < U16; h += HALF) {
+        uint4 v[HALF];
+#pragma unroll
+        for (int u = 0; u < HALF; ++u) {
+          const int idx = lane + 32 * (h + u);
+          const int L = idx / U16, j = idx - U16 * L;
+          const int32_t ent = __shfl_sync(0xffffffffu, my_ent, L);
+          const int64_t f = ent >= 0 ? int64_t(ent >> 1) : 0;
+          v[u] = __ldg(reinterpret_cast<const uint4*>(fjc + CK_FACE * f) + j);
+        }
+#pragma unroll
+        for (int u = 0; u < HALF; ++u) {
+          const int idx = lane + 32 * (h + u);
+          const int L = idx / U16, j = idx - U16 * L;
+          st4[L * RS16 + j] = v[u];
+        }
       }
+    } else {
+      // 32 RW words per round, RW per lane, in batches of ASM_BATCH
+      // independent loads (fjm is allocated for every face, so every address
+      // is valid; lanes without an entry read face 0 and their words are
+      // never used)
+#pragma unroll 1
+      for (int b = 0; b < RW / ASM_BATCH; ++b) {
+        TB v[ASM_BATCH];
 #pragma unroll
-      for (int u = 0; u < BATCH; ++u) {
-        const int idx = lane + 32 * (BATCH * b + u);
-        const int L = idx / RW, k = idx - RW * L;
-        st[k * ASM_STRIDE + L] = v[u];
+        for (int u = 0; u < ASM_BATCH; ++u) {
+          const int idx = lane + 32 * (ASM_BATCH * b + u);
+          const int L = idx / RW, k = idx - RW * L;
+          const int32_t ent = __shfl_sync(0xffffffffu, my_ent, L);
+          const int64_t f = ent >= 0 ? int64_t(ent >> 1) : 0;
+          v[u] = k < 25 ? __ldg(fjp + 25 * f + k) : __ldg(fjm + 25 * f + (k - 25));
+        }
+#pragma unroll
+        for (int u = 0; u < ASM_BATCH; ++u) {
+          const int idx = lane + 32 * (ASM_BATCH * b + u);
+          const int L = idx / RW, k = idx - RW * L;
+          st[k * ASM_STRIDE + L] = v[u];
+        }
       }
     }
     __syncwarp();
@@ -914,7 +943,7 @@ k_assemble(MeshView M, SweepView S, const double* __restrict__ q, const double* 
       const int64_t f = my_ent >> 1;
       TB r[CK_FACE];
 #pragma unroll
-      for (int k = 0; k < CK_FACE; ++k) r[k] = st[k * ASM_STRIDE + lane];
+      for (int j = 0; j < U16; ++j) reinterpret_cast<uint4*>(r)[j] = st4[lane * RS16 + j];
       TB* ao = aoff ? aoff + CK_SLOT * ck.ebp + slot * CK_SLOT * ld + i : nullptr;
       TB Mb[25];
       if (my_ent & 1) {
