@@ -1094,12 +1094,19 @@ __global__ void k_sgs_colour(ColInfo ck, const int32_t* __restrict__ nbr,
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t n = ck.n, ld = ck.ld;
   if (i >= n) return;
+  // the cell's LU factors and pivots are loaded first, so that they are in
+  // flight while the slots are walked; each slot's neighbour id is read one
+  // slot ahead
+  TB LU[25];
+#pragma unroll
+  for (int k = 0; k < 25; ++k) LU[k] = __ldcs(luc + 25 * ck.cbp + k * ld + i);
+  const int32_t pv = __ldcs(pvv + ck.cb + i);
   TX t[5];
 #pragma unroll
   for (int k = 0; k < 5; ++k) t[k] = -TX(__ldcs(bcv + 5 * ck.cbp + k * ld + i));
-  for (int64_t s = 0; s < ck.m; ++s) {
-    const int32_t o = __ldcs(nbr + ck.ebp + s * ld + i);
-    if (o < 0) break;
+  int32_t o = ck.m > 0 ? __ldcs(nbr + ck.ebp + i) : -1;
+  for (int64_t s = 0; s < ck.m && o >= 0; ++s) {
+    const int32_t onext = s + 1 < ck.m ? __ldcs(nbr + ck.ebp + (s + 1) * ld + i) : -1;
     TX xv[5];
 #pragma unroll
     for (int k = 0; k < 5; ++k) xv[k] = x[5 * int64_t(o) + k];
@@ -1116,14 +1123,12 @@ __global__ void k_sgs_colour(ColInfo ck, const int32_t* __restrict__ nbr,
 #pragma unroll
         for (int j = 0; j < 5; ++j) t[r] += TX(__ldcs(A + (5 * r + j) * ld)) * xv[j];
     }
+    o = onext;
   }
-  TB LU[25];
-#pragma unroll
-  for (int k = 0; k < 25; ++k) LU[k] = __ldcs(luc + 25 * ck.cbp + k * ld + i);
   TX y[5];
 #pragma unroll
   for (int k = 0; k < 5; ++k) y[k] = -t[k];
-  lu5_solve<TB, TX>(LU, __ldcs(pvv + ck.cb + i), y);
+  lu5_solve<TB, TX>(LU, pv, y);
   TX* xo = x + 5 * (ck.cb + i);
 #pragma unroll
   for (int k = 0; k < 5; ++k) xo[k] = y[k];
