@@ -171,8 +171,9 @@ __device__ __forceinline__ void flux_roe(const Q5& L, const Q5& R, double nx, do
   if (l2 < w2) l2 = 0.5 * ((l2s * l2s) / w2 + w2);
   if (l3 < w3) l3 = 0.5 * ((l3s * l3s) / w3 + w3);
   const RoeK k = roe_k(l1, l2, l3, s, g);
-  // K(|l|) dq with the association of fluxInviscid.loci:985-1004 so the
-  // FP64 flux agrees with the reference to rounding
+  // K(|l|) dq with the association of fluxInviscid.loci:985-1004 (the
+  // quotients by sigma below share one reciprocal), so the FP64 flux agrees
+  // with the reference to within a few ulp of its terms
   const double dT = R.T - L.T, dp = R.p - L.p;
   const double du = R.u - L.u, dv = R.v - L.v, dw = R.w - L.w;
   const double uj = du * nx + dv * ny + dw * nz;
