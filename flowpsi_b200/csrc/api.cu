@@ -312,7 +312,7 @@ int fpsi_destroy(fpsi_ctx* x) {
   free_sa(x);
   void* ps[] = {x->d_cl, x->d_cr, x->d_n, x->d_area, x->d_rL, x->d_rR, x->d_vol, x->d_cc,
                 x->d_Minv, x->d_cf_off, x->d_cf, x->d_colour_cells, x->d_bcs, x->d_q,
-                x->d_qb, x->d_grad, x->d_phi, x->d_F, x->d_src, x->d_dtau, x->d_tmu,
+                x->d_qb, x->d_grad, x->d_F, x->d_src, x->d_dtau, x->d_tmu,
                 x->d_part, x->d_resid, x->d_amin, x->d_err, x->d_perm, x->d_stage, x->d_ci, x->d_ccol,
                 x->d_nbr, x->d_colinfo, x->d_cnb_off, x->d_cnb, x->d_xprev};
   for (void* p : ps)
@@ -399,8 +399,8 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
   TRY(upload(x, &x->d_bcs, x->bcs));
   TRY(dalloc(x, &x->d_q, nc * 5));
   TRY(dalloc(x, &x->d_qb, std::max<int64_t>(H.nbf, 1) * 5));
-  TRY(dalloc(x, &x->d_grad, nc * 15));
-  TRY(dalloc(x, &x->d_phi, nc * 5));
+  TRY(dalloc(x, &x->d_grad, nc * fpsi::GPREC));
+  x->d_phi = x->d_grad + 15;
   TRY(dalloc(x, &x->d_F, nf * fpsi::FREC));
   TRY(dalloc(x, &x->d_src, nc * 5));
   TRY(dalloc(x, &x->d_dtau, nc));
@@ -687,17 +687,18 @@ int fpsi_get_reconstruction(fpsi_ctx* x, double* grad, double* limiter) {
   if (!x) return FPSI_E_INVALID;
   if (!x->have_resid) return FPSI_E_STATE;
   const int64_t nc = x->H.nc;
-  std::vector<double> g;
-  if (grad) {
-    g.resize(15 * nc);
-    FPSI_CUDA_TRY(cudaMemcpy(g.data(), x->d_grad, g.size() * sizeof(double), cudaMemcpyDeviceToHost));
-    unpermute_cells(x, g.data(), 15, grad);
-  }
-  if (limiter) {
-    g.resize(5 * nc);
-    FPSI_CUDA_TRY(cudaMemcpy(g.data(), x->d_phi, 5 * nc * sizeof(double), cudaMemcpyDeviceToHost));
-    unpermute_cells(x, g.data(), 5, limiter);
-  }
+  // device records hold the gradient (15) and the limiter (5) of a cell
+  std::vector<double> rec(size_t(nc) * fpsi::GPREC), part;
+  if (grad || limiter)
+    FPSI_CUDA_TRY(cudaMemcpy(rec.data(), x->d_grad, rec.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  auto split = [&](int k0, int w, double* out) {
+    part.resize(size_t(nc) * w);
+    for (int64_t i = 0; i < nc; ++i)
+      for (int k = 0; k < w; ++k) part[size_t(i) * w + k] = rec[size_t(i) * fpsi::GPREC + k0 + k];
+    unpermute_cells(x, part.data(), w, out);
+  };
+  if (grad) split(0, 15, grad);
+  if (limiter) split(15, 5, limiter);
   return FPSI_OK;
 }
 

@@ -13,6 +13,10 @@ namespace fpsi {
 // doubles per face record of the flux array: the flux (5) and maxev_f*area,
 // 48 B so that the record is three aligned 16 B accesses
 constexpr int FREC = 6;
+// doubles per cell record of the reconstruction array: the gradient (15,
+// d(T,u,v,w,pg)/dx, y, z) then the limiter (5); 160 B, ten aligned 16 B
+// accesses
+constexpr int GPREC = 20;
 
 void set_error(const char* fmt, ...);
 
@@ -122,8 +126,8 @@ struct fpsi_ctx {
   // state and residual
   double* d_q = nullptr;       // [nc][5]  T,u,v,w,pg
   double* d_qb = nullptr;      // [nbf][5] boundary face states
-  double* d_grad = nullptr;    // [nc][15]
-  double* d_phi = nullptr;     // [nc][5]
+  double* d_grad = nullptr;    // [nc][GPREC]: gradient (15) and limiter (5) per cell
+  double* d_phi = nullptr;     // d_grad + 15: the limiter inside each record (not allocated)
   double* d_F = nullptr;       // [nf][FREC]: face flux (5) and maxev_f * area
   double* d_src = nullptr;     // [nc][5]
   double* d_dtau = nullptr;    // [nc]

@@ -2,8 +2,8 @@
 //
 // Data layout in HBM (RCM cell order, faces sorted by cl, interior first):
 //   q      [nc][5]  FP64  T,u,v,w,pg          (AoS: every gather is one 40 B record)
-//   grad   [nc][15] FP64  dT/dx.. dpg/dz
-//   phi    [nc][5]  FP64  limiter per variable
+//   grad   [nc][20] FP64  dT/dx.. dpg/dz (15), then the limiter per variable
+//                         (5, phi = grad + 15): one 160 B record per cell
 //   F      [nf][6]  FP64  face flux (5) and maxev_f*area: one 48 B record,
 //                         three 16 B accesses
 //   src    [nc][5]  FP64, dtau [nc]
@@ -116,10 +116,10 @@ __global__ void k_bc_state(MeshView M, const double* __restrict__ q, const fpsi_
 }
 
 // ---------------------------------------------------------------------------
-// least-squares gradient + limiter, one thread per cell.  The CTA's 128
-// gradient (120 B) and limiter (40 B) records are contiguous: they are
-// staged in shared memory and written back with consecutive threads on
-// consecutive addresses.
+// least-squares gradient + limiter, one thread per cell.  Each cell's
+// gradient (15) and limiter (5) form one 160 B record; the CTA's 128
+// records are contiguous, staged in shared memory and written back with
+// consecutive threads on consecutive addresses.
 // ---------------------------------------------------------------------------
 constexpr int GRAD_THREADS = 128;
 
@@ -219,14 +219,27 @@ __device__ __forceinline__ void grad_limiter_cell(const MeshView& M, const doubl
 __global__ void __launch_bounds__(GRAD_THREADS)
 k_grad_limiter(MeshView M, const double* __restrict__ q, const double* __restrict__ qb, int limiter,
                double Kl, double* __restrict__ grad, double* __restrict__ phi) {
-  __shared__ double sg[GRAD_THREADS * 15], sp[GRAD_THREADS * 5];
+  __shared__ double sr[GRAD_THREADS * GPREC];
   const int64_t c0 = int64_t(blockIdx.x) * GRAD_THREADS;
   const int64_t c = c0 + threadIdx.x;
   const int cnt = int(min(int64_t(GRAD_THREADS), M.nc - c0));
-  if (c < M.nc) grad_limiter_cell(M, q, qb, limiter, Kl, c, sg + 15 * threadIdx.x, sp + 5 * threadIdx.x);
+  double* my = sr + GPREC * threadIdx.x;
+  if (c < M.nc) grad_limiter_cell(M, q, qb, limiter, Kl, c, my, my + 15);
   __syncthreads();
-  for (int i = threadIdx.x; i < 15 * cnt; i += GRAD_THREADS) grad[15 * c0 + i] = sg[i];
-  for (int i = threadIdx.x; i < 5 * cnt; i += GRAD_THREADS) phi[5 * c0 + i] = sp[i];
+  // gradient and limiter records are interleaved: phi == grad + 15
+  (void)phi;
+  for (int i = threadIdx.x; i < GPREC * cnt; i += GRAD_THREADS) grad[GPREC * c0 + i] = sr[i];
+}
+
+// one cell's gradient-and-limiter record (GPREC doubles, 16 B aligned)
+__device__ __forceinline__ void load_rec20(const double* p, double* v) {
+  const double2* p2 = reinterpret_cast<const double2*>(p);
+#pragma unroll
+  for (int j = 0; j < GPREC / 2; ++j) {
+    const double2 t = __ldg(p2 + j);
+    v[2 * j] = t.x;
+    v[2 * j + 1] = t.y;
+  }
 }
 
 // MUSCL states of one face: q_c + phi*grad.(x_f - x_c), floors 0.1*min(T),
@@ -257,12 +270,11 @@ __device__ __forceinline__ void reconstruct(const MeshView& M, const double* __r
   double l[5], r[5];
   {
     const double rx = M.rL[f], ry = M.rL[nf + f], rz = M.rL[2 * nf + f];
-    const double* g = grad + 15 * int64_t(a);
-    const double* ph = phi + 5 * int64_t(a);
+    double gp[GPREC];  // gradient then limiter, ten 16 B loads
+    load_rec20(grad + GPREC * int64_t(a), gp);
 #pragma unroll
     for (int k = 0; k < 5; ++k)
-      l[k] = s.ql[k] + __ldg(ph + k) * (__ldg(g + 3 * k) * rx + __ldg(g + 3 * k + 1) * ry +
-                                        __ldg(g + 3 * k + 2) * rz);
+      l[k] = s.ql[k] + gp[15 + k] * (gp[3 * k] * rx + gp[3 * k + 1] * ry + gp[3 * k + 2] * rz);
   }
   l[0] = dmax(l[0], tlim);
   l[4] = dmax(l[4], plim);
@@ -272,12 +284,11 @@ __device__ __forceinline__ void reconstruct(const MeshView& M, const double* __r
   } else {
     const int64_t d = M.cr[f];
     const double rx = M.rR[f], ry = M.rR[nf + f], rz = M.rR[2 * nf + f];
-    const double* g = grad + 15 * d;
-    const double* ph = phi + 5 * d;
+    double gp[GPREC];
+    load_rec20(grad + GPREC * d, gp);
 #pragma unroll
     for (int k = 0; k < 5; ++k)
-      r[k] = s.qr[k] + __ldg(ph + k) * (__ldg(g + 3 * k) * rx + __ldg(g + 3 * k + 1) * ry +
-                                        __ldg(g + 3 * k + 2) * rz);
+      r[k] = s.qr[k] + gp[15 + k] * (gp[3 * k] * rx + gp[3 * k + 1] * ry + gp[3 * k + 2] * rz);
     r[0] = dmax(r[0], tlim);
     r[4] = dmax(r[4], plim);
   }
@@ -322,7 +333,7 @@ __device__ VFace viscous_face(const MeshView& M, const double* __restrict__ q,
   const int64_t a = M.cl[f];
   double qa[5];
   q_arr(load_q(q, a), qa);
-  const double* ga = grad + 15 * a;
+  const double* ga = grad + GPREC * a;
   // face gradients of T, u, v, w (rows 0..3 of the cell gradient)
   double gf[4][3];
   double muf, kf, tmuf = 0.0;
@@ -331,7 +342,7 @@ __device__ VFace viscous_face(const MeshView& M, const double* __restrict__ q,
     const int64_t b = M.cr[f];
     double qc[5];
     q_arr(load_q(q, b), qc);
-    const double* gb = grad + 15 * b;
+    const double* gb = grad + GPREC * b;
     const double vl = M.vol[a], vr = M.vol[b];
     const double iv = 1.0 / (vl + vr);
     muf = (vl * suth(qc[0], V.a1, V.a2, V.a3) + vr * suth(qa[0], V.a1, V.a2, V.a3)) / (vl + vr);

@@ -271,7 +271,7 @@ __global__ void k_sa_cell(Geo G, const double* __restrict__ q, const double* __r
   }
   const double nu = nut[c], V = G.vol[c], y = wdist[c];
   const double mu = suth(q[5 * c], g);
-  const double* gu = grad + 15 * c + 3;  // rows u, v, w: d u_i / d x_j
+  const double* gu = grad + GPREC * c + 3;  // rows u, v, w: d u_i / d x_j
   const double wx = gu[3 * 2 + 1] - gu[3 * 1 + 2];
   const double wy = gu[3 * 0 + 2] - gu[3 * 2 + 0];
   const double wz = gu[3 * 1 + 0] - gu[3 * 0 + 1];
