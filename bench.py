@@ -256,11 +256,23 @@ def workload_name(args) -> str:
     return f"taylor_green_tets_{args.n}"
 
 
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 class OracleSample:
     """the oracle (the C++ restatement) on a smaller grid of the same
-    workload, multi-colour SGS order, every requested host thread"""
+    workload with every requested host thread (residual, Jacobians and
+    assembly in parallel), its SGS in the reference's sequential cell order
+    (linearSolverSGS.loci:150-329, one thread) or multi-colour (parallel)"""
 
-    def __init__(self, args, threads: int, n_sample: int):
+    def __init__(self, args, threads: int, n_sample: int, order: str = "sequential"):
         from flowpsi_b200 import cases
         from oracle import Oracle
         from oracle.oracle import set_threads
@@ -272,7 +284,8 @@ class OracleSample:
         self.o = Oracle(case.mesh, case.params)
         T, p, u = case.initial_state(self.o.geometry()["cellcenter"])
         self.o.set_state(T, p, u)
-        self.colour = greedy_colours(case.mesh)
+        self.colour = greedy_colours(case.mesh) if order == "multicolour" else None
+        self.order = order
         self.ncells = self.o.ncells
 
     def step(self) -> float:
@@ -281,11 +294,17 @@ class OracleSample:
         return time.perf_counter() - t0
 
 
-def cpu_oracle_rate(args, threads: int, n_sample: int, steps: int):
-    s = OracleSample(args, threads, n_sample)
+def cpu_oracle_rate(args, threads: int, n_sample: int, order: str, budget_s: float,
+                    min_steps: int = 2):
+    """cell-iterations per second of the oracle over steps until budget_s
+    of CPU time (at least min_steps), after one warm-up step"""
+    s = OracleSample(args, threads, n_sample, order)
     s.step()  # warm-up
-    dt = sum(s.step() for _ in range(steps))
-    return s.ncells * steps / dt, s.ncells, dt
+    dt, steps = 0.0, 0
+    while steps < min_steps or dt < budget_s:
+        dt += s.step()
+        steps += 1
+    return s.ncells * steps / dt, s.ncells, dt, steps
 
 
 def greedy_colours(mesh) -> np.ndarray:
@@ -313,7 +332,7 @@ def run_reference(args, ws, rank):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    smp = OracleSample(args, threads, args.cpu_n)
+    smp = OracleSample(args, threads, args.cpu_n, "sequential")
     for _ in range(args.warmup):
         smp.step()
     times = [smp.step() for _ in range(args.steps)]
@@ -321,7 +340,8 @@ def run_reference(args, ws, rank):
     rates = [smp.ncells / t for t in times]
     value = statistics.median(rates)
     sample = (f"taylor_green_tets {args.cpu_n}^3 x 6 = {6 * args.cpu_n ** 3} cells, "
-              f"one implicit step per timed step, {args.sweeps} multi-colour SGS sweeps")
+              f"one implicit step per timed step, {args.sweeps} SGS sweeps in the reference's "
+              f"sequential cell order; CPU {cpu_model()}")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-iters/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -337,34 +357,99 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
-def time_to_drop(n: int, precision: str, drop: float = 1e-8, max_steps: int = 2000,
-                 chunk: int = 25, seed: int = 0):
-    """device time and implicit steps until the density residual (rtrms)
-    falls below drop x its step-0 value, on the steady farfield cube
-    (freestream M=0.5 with 1% noise, Roe + MUSCL + Venkatakrishnan, 5 SGS
-    sweeps, CFL 50)"""
+RT_AIR, GAMMA = 8314.4621 / 28.96, 1.4
+
+
+def _rho_energy(T, p, u):
+    rho = p / (RT_AIR * T)
+    return rho, rho * (RT_AIR * T / (GAMMA - 1.0) + 0.5 * (u * u).sum(1))
+
+
+def _drop_arm(solver, case, drop, max_steps, chunk, model=None):
+    """device ms and steps until the density residual (rtrms) falls below
+    drop x its step-0 value.  Without a model: fpsi_run_timed in chunks
+    (CUDA events on the library's stream).  With a model: one
+    fpsi_newton_step_ex per step from the learned start with the rejection
+    rule, timed by the host clock around the steps (its host decisions and
+    copies are part of the cost)."""
+    solver.set_state(*case.initial_state(solver.geometry()["cellcenter"]))
+    r0, done, ms_tot, reached, rejected = None, 0, 0.0, None, 0
+    if model is None:
+        while done < max_steps and reached is None:
+            hist, ms = solver.run_timed(chunk)
+            if r0 is None:
+                r0 = hist[0]["rtrms"]
+            for k, h in enumerate(hist):
+                if h["rtrms"] < drop * r0:
+                    reached = done + k
+                    ms_tot += ms * k / chunk
+                    break
+            else:
+                ms_tot += ms
+            done += chunk
+    else:
+        t0 = time.perf_counter()
+        for k in range(max_steps):
+            r = solver.newton_step_ex(start="learned", model=model, reject=True)
+            rejected += int(r["rejected"])
+            if r0 is None:
+                r0 = r["rtrms"]
+            if r["after"]["rtrms"] < drop * r0:
+                reached = k + 1
+                break
+        ms_tot = 1e3 * (time.perf_counter() - t0)
+    return {"steps": reached, "ms": ms_tot if reached is not None else None,
+            "rejected": rejected if model is not None else None,
+            "timer": "host clock, per-step decisions" if model is not None else
+            "CUDA events on the library stream"}, solver.get_state()
+
+
+def time_to_drop(n: int, drop: float = 1e-8, max_steps: int = 400, chunk: int = 10,
+                 seed: int = 0, learned: bool = True):
+    """Time to a 1e-8 drop of the density residual on the steady split-tet
+    case (farfield_tets: the 128^3 x 6 jittered Kuhn grid of the
+    Taylor-Green workload with farfield sides, M=0.5 freestream with 1%
+    noise, Roe + MUSCL + Venkatakrishnan, 8 SGS sweeps, CFL 50): plain FP64,
+    MIXED from the reference's Jacobi start, and MIXED from the learned start
+    (a model trained first on 16^3 x 6 grids of the same case, seeds 1-4).
+    Each arm reports steps, ms and the largest density and energy difference
+    of its final state from the FP64 arm's."""
     from flowpsi_b200 import FlowPsi, cases
 
-    case = cases.farfield_cube(n, seed=seed, precision=precision)
-    s = FlowPsi(case.mesh, case.params)
+    out = {"case": f"farfield_tets_{n}", "cells": 6 * n ** 3, "drop": drop}
+    c64 = cases.farfield_tets(n, seed=seed, precision="fp64")
+    s = FlowPsi(c64.mesh, c64.params)
     s.keep_blocks(False)
-    s.set_state(*case.initial_state(s.geometry()["cellcenter"]))
-    r0, done, ms_tot, reached = None, 0, 0.0, None
-    while done < max_steps and reached is None:
-        hist, ms = s.run_timed(chunk)
-        if r0 is None:
-            r0 = hist[0]["rtrms"]
-        for k, h in enumerate(hist):
-            if h["rtrms"] < drop * r0:
-                reached = done + k
-                ms_tot += ms * k / chunk
-                break
-        else:
-            ms_tot += ms
-        done += chunk
+    out["fp64"], st64 = _drop_arm(s, c64, drop, max_steps, chunk)
     s.close()
-    return {"steps": reached, "ms": ms_tot if reached is not None else None,
-            "cells": n ** 3}
+    del s
+    rho64, e64 = _rho_energy(*st64)
+    c32 = cases.farfield_tets(n, seed=seed, precision="mixed")
+    s = FlowPsi(c32.mesh, c32.params)
+    s.keep_blocks(learned)
+    arms = [("mixed", None)]
+    if learned:
+        from flowpsi_b200.learned import train_on_case
+
+        model, info = train_on_case(lambda sd: cases.farfield_tets(16, seed=sd, precision="fp64"),
+                                    seeds=(1, 2, 3, 4), steps_per_seed=12, train_steps=1500,
+                                    batch=16384)
+        out["training"] = info
+        arms.append(("mixed_learned", model))
+    for name, model in arms:
+        out[name], st = _drop_arm(s, c32, drop, max_steps, chunk, model)
+        rho, e = _rho_energy(*st)
+        out[name]["max_rel_diff_vs_fp64"] = {
+            "rho": float(np.abs(rho - rho64).max() / np.abs(rho64).max()),
+            "rho_e0": float(np.abs(e - e64).max() / np.abs(e64).max())}
+    if learned:
+        model.close()
+    s.close()
+    f = out["fp64"]["ms"]
+    for name, _ in arms:
+        m = out[name]["ms"]
+        out[name]["speedup_vs_fp64"] = (f / m) if f and m else None
+    return out
 
 
 def run_fpsi(args, ws, rank, local):
@@ -465,20 +550,23 @@ def run_fpsi(args, ws, rank, local):
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        r, ncs, dt = cpu_oracle_rate(args, threads, args.cpu_n, args.cpu_steps)
+        r, ncs, dt, k = cpu_oracle_rate(args, threads, args.cpu_n, "sequential", args.cpu_budget)
+        r2, _, dt2, k2 = cpu_oracle_rate(args, threads, args.cpu_n, "multicolour", args.cpu_budget)
         cpu = {"value": r, "unit": "cell-iters/s", "cores": threads, "kind": "port",
-               "sample": f"taylor_green_tets {args.cpu_n}^3 x 6 = {ncs} cells, "
-                         f"{args.cpu_steps} implicit steps ({dt:.1f} s), multi-colour SGS"}
+               "cpu": cpu_model(),
+               "sample": f"taylor_green_tets {args.cpu_n}^3 x 6 = {ncs} cells, {k} implicit "
+                         f"steps ({dt:.1f} s); residual, Jacobians and assembly on {threads} "
+                         f"threads, SGS in the reference's sequential cell order (one thread)",
+               "multicolour": {"value": r2, "steps": k2, "seconds": dt2,
+                               "sample": "the same grid with multi-colour SGS on every thread"}}
 
     converge = None
-    if args.converge_n > 0:
-        # second half of the metric: time to a 1e-8 residual drop on a steady
-        # case, FP64 against FP32 relaxation (MIXED)
-        c64 = time_to_drop(args.converge_n, "fp64")
-        c32 = time_to_drop(args.converge_n, "mixed")
-        converge = {"case": f"farfield_cube_{args.converge_n}", "drop": 1e-8, "fp64": c64,
-                    "mixed": c32,
-                    "speedup": (c64["ms"] / c32["ms"]) if c64["ms"] and c32["ms"] else None}
+    if args.converge_n > 0 and rank == 0 and ws == 1:
+        # second half of the metric: time to a 1e-8 residual drop on the
+        # steady split-tet case, FP64 against FP32 relaxation (MIXED) from
+        # the reference's start and from the learned start
+        solver.close()
+        converge = time_to_drop(args.converge_n, learned=not args.no_learned)
 
     launches = sum(v[1] for v in kt.values()) / args.profile_steps * args.steps
     line = {
@@ -525,7 +613,8 @@ def main():
     ap.add_argument("--profile-steps", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-n", type=int, default=48)
-    ap.add_argument("--cpu-steps", type=int, default=40)
+    ap.add_argument("--cpu-budget", type=float, default=12.0,
+                    help="seconds of CPU time per cpu_baseline variant")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="tgv", choices=["tgv", "bl", "shock"])
     ap.add_argument("--bl-nx", type=int, default=256)
@@ -535,7 +624,9 @@ def main():
     ap.add_argument("--turb", default="sa", choices=["sa", "frozen"],
                     help="bl turbulent: SA nu~ transport or a frozen eddy viscosity")
     ap.add_argument("--converge-n", type=int, default=128,
-                    help="farfield cube size for the time-to-1e-8 runs (0: skip)")
+                    help="split-tet farfield grid (n^3 x 6) of the time-to-1e-8 runs (0: skip)")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="time-to-1e-8 without the learned-start arm")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warning: fewer than 3 warm-up steps")

@@ -85,7 +85,16 @@ class LsInfo(C.Structure):
 
 class StepInfo(C.Structure):
     _fields_ = [("resid", Resid), ("ls", LsInfo), ("min_alpha", C.c_double),
-                ("dtau_min", C.c_double), ("dtau_max", C.c_double)]
+                ("dtau_min", C.c_double), ("dtau_max", C.c_double),
+                ("resid_after", Resid), ("start_used", C.c_int32), ("rejected", C.c_int32)]
+
+
+START = {"jacobi": 0, "zero": 1, "learned": 2}
+
+
+class StepOpts(C.Structure):
+    _fields_ = [("start", C.c_int32), ("reject", C.c_int32), ("lin_rtol", C.c_double),
+                ("max_sweeps", C.c_int32), ("check_every", C.c_int32)]
 
 
 _dp = C.POINTER(C.c_double)
@@ -148,6 +157,7 @@ _SIGS = {
     "fpsi_gnn_predict": (C.c_int, [C.c_void_p, _ctx, _dp]),
     "fpsi_update": (C.c_int, [_ctx, _dp]),
     "fpsi_newton_step": (C.c_int, [_ctx, C.POINTER(StepInfo)]),
+    "fpsi_newton_step_ex": (C.c_int, [_ctx, C.c_void_p, C.POINTER(StepOpts), C.POINTER(StepInfo)]),
     "fpsi_run": (C.c_int, [_ctx, C.c_int32, C.POINTER(Resid)]),
     "fpsi_run_timed": (C.c_int, [_ctx, C.c_int32, C.POINTER(Resid), _dp]),
     "fpsi_kernel_times": (C.c_int, [_ctx, C.c_int32, C.c_int32, C.c_char_p, _dp,

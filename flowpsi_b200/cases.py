@@ -15,6 +15,9 @@ inputs for the same seed.
   taylorGreenIC.loci:26-31: constant density, pressure from the analytic
   field); Roe + MUSCL + Venkatakrishnan, 8 multi-colour SGS sweeps (128^3:
   12.58M cells, 25.2M faces).
+* ``farfield_tets``: the split-tet grid of ``taylor_green_tets`` with
+  farfield sides and the freestream-plus-noise start of ``farfield_cube``:
+  the steady case on which the 1e-8 residual drop is timed.
 * ``oblique_shock_cube``: n^3 hex cube, Mach-2 flow with a Rankine-Hugoniot
   jump across a plane tilted 30 degrees, 0.5% noise, supersonic inflow /
   outflow, HLLE + Barth.
@@ -115,6 +118,39 @@ def taylor_green_tets(n: int = 128, seed: int = 0, sweeps: int = 8, jitter: floa
         return T, p, u
 
     return Case(f"taylor_green_tets_{n}", mesh, params, 200, init)
+
+
+def farfield_tets(n: int = 128, seed: int = 0, sweeps: int = 8, jitter: float = 0.1,
+                  precision: str = "mixed", flux: str = "roe",
+                  limiter: str = "venkatakrishnan", L: float = 2.0 * math.pi) -> Case:
+    """Steady case on the Taylor-Green split-tet grid: n^3 hexes of the box
+    [0,L]^3 split into 6 Kuhn tetrahedra, nodes jittered by +-10% of the
+    spacing (the sides stay plane), farfield on all six sides at M=0.5
+    along +x, p=1e5 Pa, T=300 K; initial state the freestream with 1%
+    Gaussian noise in rho, u, v, w and p (as farfield_cube).  Roe + MUSCL +
+    Venkatakrishnan, 8 SGS sweeps, CFL 50.  The noise leaves through the
+    farfield sides, so the residual falls to machine level."""
+    T0, p0, M = 300.0, 1e5, 0.5
+    U0 = M * math.sqrt(GAMMA * RTILDE * T0)
+    ff = bc("farfield", T=T0, pg=p0, u=(U0, 0.0, 0.0))
+    mesh = GeneratedMesh("kuhn", n=(n, n, n), L=(L, L, L), jitter=jitter, seed=seed,
+                         bc_side=(0,) * 6, bcs=[ff])
+    params = default_params(flux=flux, limiter=limiter, Kl=1.0, solver="sgs",
+                            gauss_seidel_iter=sweeps, cflmax=50.0, precision=precision)
+
+    def init(cc):
+        nc = cc.shape[0]
+        rho0 = p0 / (RTILDE * T0)
+        rho = rho0 * (1.0 + 0.01 * normal(seed, 0, nc))
+        p = p0 * (1.0 + 0.01 * normal(seed, 1, nc))
+        u = np.empty((nc, 3))
+        u[:, 0] = U0 + 0.01 * U0 * normal(seed, 2, nc)
+        u[:, 1] = 0.01 * U0 * normal(seed, 3, nc)
+        u[:, 2] = 0.01 * U0 * normal(seed, 4, nc)
+        T = p / (RTILDE * rho)
+        return T, p, u
+
+    return Case(f"farfield_tets_{n}", mesh, params, 400, init)
 
 
 MU_A = (1.458e-6, 1.5, 110.4)  # Sutherland, fluxViscous.loci:58-80

@@ -184,6 +184,27 @@ int alloc_lsgs(fpsi_ctx* x) {
   return FPSI_OK;
 }
 
+// residual history for runs of up to n steps (8 doubles per step)
+int ensure_hist(fpsi_ctx* x, int64_t n) {
+  if (n <= x->hist_cap) return FPSI_OK;
+  if (x->d_hist) {
+    x->device_bytes -= x->hist_cap * 8 * int64_t(sizeof(double));
+    cudaFree(x->d_hist);
+    x->d_hist = nullptr;
+  }
+  if (x->h_hist) cudaFreeHost(x->h_hist);
+  x->h_hist = nullptr;
+  x->hist_cap = 0;
+  int rc = dalloc(x, &x->d_hist, size_t(n) * 8);
+  if (rc) return rc;
+  if (cudaMallocHost((void**)&x->h_hist, size_t(n) * 8 * sizeof(double)) != cudaSuccess) {
+    fpsi::set_error("cudaMallocHost of the residual history failed");
+    return FPSI_E_NOMEM;
+  }
+  x->hist_cap = n;
+  return FPSI_OK;
+}
+
 bool is_lsgs(const fpsi_ctx* x) { return x->P.solver == FPSI_SOLVER_LSGS; }
 
 int check_params(const fpsi_params* p) {
@@ -314,10 +335,12 @@ int fpsi_destroy(fpsi_ctx* x) {
                 x->d_Minv, x->d_cf_off, x->d_cf, x->d_colour_cells, x->d_bcs, x->d_q,
                 x->d_qb, x->d_grad, x->d_F, x->d_src, x->d_dtau, x->d_tmu,
                 x->d_part, x->d_resid, x->d_amin, x->d_err, x->d_perm, x->d_stage, x->d_ci, x->d_ccol,
-                x->d_nbr, x->d_colinfo, x->d_cnb_off, x->d_cnb, x->d_xprev};
+                x->d_nbr, x->d_colinfo, x->d_cnb_off, x->d_cnb, x->d_xprev, x->d_qsave};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (x->h_resid) cudaFreeHost(x->h_resid);
+  if (x->d_hist) cudaFree(x->d_hist);
+  if (x->h_hist) cudaFreeHost(x->h_hist);
   for (cudaEvent_t e : x->evpool) cudaEventDestroy(e);
   if (x->stream) cudaStreamDestroy(x->stream);
   delete x;
@@ -400,7 +423,6 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
   TRY(dalloc(x, &x->d_q, nc * 5));
   TRY(dalloc(x, &x->d_qb, std::max<int64_t>(H.nbf, 1) * 5));
   TRY(dalloc(x, &x->d_grad, nc * fpsi::GPREC));
-  x->d_phi = x->d_grad + 15;
   TRY(dalloc(x, &x->d_F, nf * fpsi::FREC));
   TRY(dalloc(x, &x->d_src, nc * 5));
   TRY(dalloc(x, &x->d_dtau, nc));
@@ -422,6 +444,7 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
     fpsi_destroy(x);
     return FPSI_E_CUDA;
   }
+  TRY(ensure_hist(x, 4096));
   if (params->solver == FPSI_SOLVER_LSGS) x->keep_D = true;
   TRY(alloc_system(x));
   TRY(alloc_lsgs(x));
@@ -619,7 +642,7 @@ int fpsi_sa_solve(fpsi_ctx* x, double* dq) {
 int fpsi_sa_update(fpsi_ctx* x) {
   if (!x) return FPSI_E_INVALID;
   if (!x->have_sa_dq) return FPSI_E_STATE;
-  int rc = fpsi::sa_launch_update(x);
+  int rc = fpsi::sa_launch_update(x, x->d_resid);
   if (rc) return rc;
   if ((rc = sync(x))) return rc;
   x->have_sa = x->have_sa_dq = false;
@@ -934,7 +957,7 @@ int fpsi_linear_residual(fpsi_ctx* x, double* norm_b, double* norm_r) {
 int fpsi_update(fpsi_ctx* x, double* min_alpha) {
   if (!x) return FPSI_E_INVALID;
   if (!x->have_dq) return FPSI_E_STATE;
-  int rc = fpsi::launch_update(x);
+  int rc = fpsi::launch_update(x, x->d_resid);
   if (rc) return rc;
   std::vector<double> a(x->nblk_norm);
   FPSI_CUDA_TRY(cudaMemcpyAsync(a.data(), x->d_amin, a.size() * sizeof(double),
@@ -959,14 +982,14 @@ int fpsi_newton_step(fpsi_ctx* x, fpsi_stepinfo* info) {
   } else if ((rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter))) {
     return rc;
   }
-  if ((rc = fpsi::launch_update(x))) return rc;
-  if (sa && (rc = fpsi::sa_launch_update(x))) return rc;
+  if ((rc = fpsi::launch_update(x, x->d_resid))) return rc;
+  if (sa && (rc = fpsi::sa_launch_update(x, x->d_resid))) return rc;
   FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid, x->d_resid, 8 * sizeof(double),
                                 cudaMemcpyDeviceToHost, x->stream));
   std::vector<double> a(x->nblk_norm);
   FPSI_CUDA_TRY(cudaMemcpyAsync(a.data(), x->d_amin, a.size() * sizeof(double),
                                 cudaMemcpyDeviceToHost, x->stream));
-  if ((rc = finish_assemble(x))) return rc;
+  if ((rc = sync(x))) return rc;
   x->have_resid = x->have_asm = x->have_dq = false;
   if (info) {
     std::memset(info, 0, sizeof(*info));
@@ -974,17 +997,172 @@ int fpsi_newton_step(fpsi_ctx* x, fpsi_stepinfo* info) {
     info->ls.iterations = x->P.gauss_seidel_iter;
     info->min_alpha = *std::min_element(a.begin(), a.end());
   }
-  return has_nan(x->h_resid) ? FPSI_E_NAN : FPSI_OK;
+  if (has_nan(x->h_resid)) {
+    // the state was left unchanged; a system built from NaN norms may have
+    // flagged zero pivots too
+    FPSI_CUDA_TRY(cudaMemset(x->d_err, 0, sizeof(int32_t)));
+    fpsi::set_error("NaN residual norms; the state is unchanged");
+    return FPSI_E_NAN;
+  }
+  return finish_assemble(x);
+}
+
+// ---- one step with a chosen start, a linear tolerance and rejection -----
+namespace {
+// sweeps of the assembled system: exactly gauss_seidel_iter, or until the
+// linear residual falls below lin_rtol ||B|| (checked every check_every
+// sweeps); info gets the count and the residuals measured
+int ex_sweeps(fpsi_ctx* x, const fpsi_step_opts& o, fpsi_lsinfo* info) {
+  int rc;
+  info->status = FPSI_OK;
+  info->resid0 = info->resid = 0;
+  if (o.lin_rtol <= 0) {
+    if ((rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter))) return rc;
+    info->iterations = x->P.gauss_seidel_iter;
+    return FPSI_OK;
+  }
+  const int every = std::max(1, o.check_every);
+  int done = 0;
+  for (bool first = true;; first = false) {
+    if ((rc = fpsi::launch_linres(x, x->d_resid + 8))) return rc;
+    FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid + 8, x->d_resid + 8, 2 * sizeof(double),
+                                  cudaMemcpyDeviceToHost, x->stream));
+    if ((rc = sync(x))) return rc;
+    const double nb = x->h_resid[8], nr = x->h_resid[9];
+    if (first) info->resid0 = nr;
+    info->resid = nr;
+    if (!(nr > o.lin_rtol * nb) || done >= o.max_sweeps) break;
+    const int k = std::min(every, o.max_sweeps - done);
+    if ((rc = fpsi::launch_sgs(x, k))) return rc;
+    done += k;
+  }
+  info->iterations = done;
+  return FPSI_OK;
+}
+
+// residual of the current state into d_resid and h_resid
+int ex_residual(fpsi_ctx* x) {
+  int rc = fpsi::launch_residual(x, x->d_resid);
+  if (rc) return rc;
+  FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid, x->d_resid, 8 * sizeof(double),
+                                cudaMemcpyDeviceToHost, x->stream));
+  if ((rc = sync(x))) return rc;
+  x->have_resid = true;
+  x->have_asm = x->have_dq = x->x_preset = false;
+  return FPSI_OK;
+}
+
+// assemble, start, relax and update from the residual in d_resid
+int ex_attempt(fpsi_ctx* x, fpsi_gnn* model, const fpsi_step_opts& o, int start,
+               fpsi_stepinfo* info) {
+  int rc = fpsi::launch_assemble(x);
+  if (rc) return rc;
+  if ((rc = finish_assemble(x))) return rc;
+  x->have_asm = true;
+  if (start == FPSI_START_ZERO) {
+    FPSI_CUDA_TRY(cudaMemsetAsync(x->d_x, 0, size_t(x->H.nc) * 5 * x->x_bytes, x->stream));
+  } else if (start == FPSI_START_LEARNED) {
+    if ((rc = fpsi_gnn_predict(model, x, nullptr))) return rc;
+  }
+  if ((rc = ex_sweeps(x, o, &info->ls))) return rc;
+  if ((rc = fpsi::launch_update(x, x->d_resid))) return rc;
+  std::vector<double> a(x->nblk_norm);
+  FPSI_CUDA_TRY(cudaMemcpyAsync(a.data(), x->d_amin, a.size() * sizeof(double),
+                                cudaMemcpyDeviceToHost, x->stream));
+  if ((rc = sync(x))) return rc;
+  info->min_alpha = *std::min_element(a.begin(), a.end());
+  x->have_resid = x->have_asm = x->have_dq = x->x_preset = false;
+  return FPSI_OK;
+}
+}  // namespace
+
+int fpsi_newton_step_ex(fpsi_ctx* x, fpsi_gnn* model, const fpsi_step_opts* opts,
+                        fpsi_stepinfo* info) {
+  if (!x || !opts) return FPSI_E_INVALID;
+  const fpsi_step_opts o = *opts;
+  if (o.start < FPSI_START_JACOBI || o.start > FPSI_START_LEARNED ||
+      (o.start == FPSI_START_LEARNED && !model) || (o.lin_rtol > 0 && o.max_sweeps < 0)) {
+    fpsi::set_error("fpsi_newton_step_ex: bad options");
+    return FPSI_E_INVALID;
+  }
+  if (is_lsgs(x) || fpsi::sa_active(x)) {
+    fpsi::set_error("fpsi_newton_step_ex: multi-colour SGS without the SA model only");
+    return FPSI_E_UNSUPPORTED;
+  }
+  if ((o.start == FPSI_START_LEARNED || o.lin_rtol > 0) && !x->d_D) {
+    fpsi::set_error("fpsi_newton_step_ex: keep the diagonal blocks (fpsi_keep_blocks)");
+    return FPSI_E_STATE;
+  }
+  const int64_t nc = x->H.nc;
+  const size_t qb = size_t(nc) * 5 * sizeof(double);
+  const bool may_reject = o.reject && o.start != FPSI_START_JACOBI;
+  int rc;
+  if (may_reject && !x->d_qsave && (rc = dalloc(x, &x->d_qsave, size_t(nc) * 5))) return rc;
+  fpsi_stepinfo si;
+  std::memset(&si, 0, sizeof(si));
+  // the residual of the current state: kept from the previous call, or new
+  if (!x->have_resid && (rc = ex_residual(x))) return rc;
+  double r_start[8];
+  std::memcpy(r_start, x->h_resid, sizeof(r_start));
+  fill_norms(x, r_start, &si.resid);
+  if (has_nan(r_start)) {
+    fpsi::set_error("NaN residual norms; the state is unchanged");
+    return FPSI_E_NAN;
+  }
+  if (may_reject)
+    FPSI_CUDA_TRY(cudaMemcpyAsync(x->d_qsave, x->d_q, qb, cudaMemcpyDeviceToDevice, x->stream));
+  si.start_used = o.start;
+  if ((rc = ex_attempt(x, model, o, o.start, &si))) return rc;
+  if ((rc = ex_residual(x))) return rc;
+  if (may_reject && !(x->h_resid[0] < r_start[0])) {
+    // the step did not lower the FP64 density residual: undo it and take
+    // the reference's step from D^-1 B
+    FPSI_CUDA_TRY(cudaMemcpyAsync(x->d_q, x->d_qsave, qb, cudaMemcpyDeviceToDevice, x->stream));
+    if ((rc = ex_residual(x))) return rc;
+    si.rejected = 1;
+    si.start_used = FPSI_START_JACOBI;
+    if ((rc = ex_attempt(x, model, o, FPSI_START_JACOBI, &si))) return rc;
+    if ((rc = ex_residual(x))) return rc;
+  }
+  fill_norms(x, x->h_resid, &si.resid_after);
+  if (info) *info = si;
+  if (has_nan(x->h_resid)) {
+    fpsi::set_error("NaN residual norms after the step");
+    return FPSI_E_NAN;
+  }
+  return FPSI_OK;
 }
 
 // nsteps implicit steps on the stream; with the SA model nu~ is advanced in
-// each step from the same residual state, after the mean flow's solve
-static int run_steps(fpsi_ctx* x, int32_t nsteps, double* hist) {
+// each step from the same residual state, after the mean flow's solve.  The
+// norms of step s go to d_hist[8s] and, by a 64-byte copy queued behind the
+// residual, to the pinned h_hist[8s] (whose rtrms slot starts at -1).  Before
+// each launch the host looks at the copies that have landed and stops
+// launching once one holds NaN norms; steps already queued behind it leave
+// the state alone (the update kernels test their step's norms), so the state
+// is the one of the first NaN step.  Returns the number of steps launched.
+static int run_steps(fpsi_ctx* x, int32_t nsteps, int32_t* launched) {
   int rc = FPSI_OK;
   const bool sa = fpsi::sa_active(x);
-  for (int32_t s = 0; s < nsteps && !rc; ++s) {
+  volatile double* hh = x->h_hist;
+  for (int32_t s = 0; s < nsteps; ++s) hh[8 * int64_t(s)] = -1.0;
+  int32_t seen = 0, s = 0;
+  for (; s < nsteps && !rc; ++s) {
+    bool nan = false;
+    while (seen < s && !nan) {
+      const double r = hh[8 * int64_t(seen)];
+      if (r == -1.0) break;  // not landed yet
+      nan = r != r || hh[8 * int64_t(seen) + 1] != hh[8 * int64_t(seen) + 1] ||
+            hh[8 * int64_t(seen) + 2] != hh[8 * int64_t(seen) + 2];
+      ++seen;
+    }
+    if (nan) break;
+    double* slot = x->d_hist + 8 * int64_t(s);
     if (sa) rc = fpsi::sa_launch_tmu(x);
-    if (!rc) rc = fpsi::launch_residual(x, hist + 8 * s);
+    if (!rc) rc = fpsi::launch_residual(x, slot);
+    if (!rc && cudaMemcpyAsync(x->h_hist + 8 * int64_t(s), slot, 8 * sizeof(double),
+                               cudaMemcpyDeviceToHost, x->stream) != cudaSuccess)
+      rc = FPSI_E_CUDA;
     if (!rc && sa) rc = fpsi::sa_launch_residual(x);
     if (!rc && sa) rc = fpsi::sa_launch_solve(x);
     if (!rc) rc = fpsi::launch_assemble(x);
@@ -994,87 +1172,89 @@ static int run_steps(fpsi_ctx* x, int32_t nsteps, double* hist) {
     } else if (!rc) {
       rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter);
     }
-    if (!rc) rc = fpsi::launch_update(x);
-    if (!rc && sa) rc = fpsi::sa_launch_update(x);
+    if (!rc) rc = fpsi::launch_update(x, slot);
+    if (!rc && sa) rc = fpsi::sa_launch_update(x, slot);
   }
+  *launched = s;
   x->have_sa = x->have_sa_dq = false;
   return rc;
+}
+
+// norms of a finished run; a NaN step ends the history (later entries NaN)
+static int finish_run(fpsi_ctx* x, int32_t nsteps, int32_t launched, fpsi_resid* norms) {
+  int32_t first_nan = -1;
+  for (int32_t s = 0; s < launched && first_nan < 0; ++s)
+    if (has_nan(&x->h_hist[8 * int64_t(s)])) first_nan = s;
+  if (launched < nsteps && first_nan < 0) {
+    fpsi::set_error("the run stopped after %d of %d steps without a NaN residual", launched, nsteps);
+    return FPSI_E_STATE;
+  }
+  const int32_t last = first_nan < 0 ? nsteps : first_nan + 1;
+  if (norms) {
+    for (int32_t s = 0; s < last; ++s) fill_norms(x, &x->h_hist[8 * int64_t(s)], &norms[s]);
+    const double q = std::nan("");
+    const double nanrec[8] = {q, q, q, q, -1, q, -1, q};
+    for (int32_t s = last; s < nsteps; ++s) fill_norms(x, nanrec, &norms[s]);
+  }
+  if (first_nan >= 0) {
+    // the systems built from NaN norms may have flagged zero pivots too
+    FPSI_CUDA_TRY(cudaMemset(x->d_err, 0, sizeof(int32_t)));
+    fpsi::set_error("NaN residual norms at step %d of %d; the state is that step's", first_nan,
+                    nsteps);
+    return FPSI_E_NAN;
+  }
+  return finish_assemble(x);
 }
 
 int fpsi_run(fpsi_ctx* x, int32_t nsteps, fpsi_resid* norms) {
   if (!x || nsteps < 0) return FPSI_E_INVALID;
   if (nsteps == 0) return FPSI_OK;
-  double* hist = nullptr;
-  if (cudaMalloc((void**)&hist, size_t(nsteps) * 8 * sizeof(double)) != cudaSuccess) {
-    fpsi::set_error("cudaMalloc of the residual history failed");
-    return FPSI_E_NOMEM;
-  }
-  int rc = run_steps(x, nsteps, hist);
-  std::vector<double> h(size_t(nsteps) * 8);
-  if (!rc && cudaMemcpyAsync(h.data(), hist, h.size() * sizeof(double), cudaMemcpyDeviceToHost,
-                             x->stream) != cudaSuccess)
-    rc = FPSI_E_CUDA;
-  if (!rc) rc = finish_assemble(x);
-  cudaFree(hist);
+  int rc = ensure_hist(x, nsteps);
+  if (rc) return rc;
+  int32_t launched = 0;
+  rc = run_steps(x, nsteps, &launched);
+  if (!rc) rc = sync(x);
   x->have_resid = x->have_asm = x->have_dq = false;
   if (rc) return rc;
-  bool nan = false;
-  for (int32_t s = 0; s < nsteps; ++s) {
-    if (norms) fill_norms(x, &h[8 * s], &norms[s]);
-    nan = nan || has_nan(&h[8 * s]);
-  }
-  return nan ? FPSI_E_NAN : FPSI_OK;
+  return finish_run(x, nsteps, launched, norms);
 }
 
 int fpsi_run_timed(fpsi_ctx* x, int32_t nsteps, fpsi_resid* norms, double* device_ms) {
   if (!x || nsteps <= 0 || !device_ms) return FPSI_E_INVALID;
-  double* hist = nullptr;
-  if (cudaMalloc((void**)&hist, size_t(nsteps) * 8 * sizeof(double)) != cudaSuccess) {
-    fpsi::set_error("cudaMalloc of the residual history failed");
-    return FPSI_E_NOMEM;
-  }
+  int rc = ensure_hist(x, nsteps);
+  if (rc) return rc;
   cudaEvent_t a = nullptr, b = nullptr;
-  int rc = FPSI_OK;
   if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) rc = FPSI_E_CUDA;
   if (!rc && cudaEventRecord(a, x->stream) != cudaSuccess) rc = FPSI_E_CUDA;
-  if (!rc) rc = run_steps(x, nsteps, hist);
+  int32_t launched = 0;
+  if (!rc) rc = run_steps(x, nsteps, &launched);
   if (!rc && cudaEventRecord(b, x->stream) != cudaSuccess) rc = FPSI_E_CUDA;
-  std::vector<double> h(size_t(nsteps) * 8);
-  if (!rc && cudaMemcpyAsync(h.data(), hist, h.size() * sizeof(double), cudaMemcpyDeviceToHost,
-                             x->stream) != cudaSuccess)
-    rc = FPSI_E_CUDA;
-  if (!rc) rc = finish_assemble(x);
+  if (!rc) rc = sync(x);
   float ms = 0;
   if (!rc && cudaEventElapsedTime(&ms, a, b) != cudaSuccess) rc = FPSI_E_CUDA;
   if (a) cudaEventDestroy(a);
   if (b) cudaEventDestroy(b);
-  cudaFree(hist);
   x->have_resid = x->have_asm = x->have_dq = false;
   if (rc) return rc;
   *device_ms = ms;
-  bool nan = false;
-  for (int32_t s = 0; s < nsteps; ++s) {
-    if (norms) fill_norms(x, &h[8 * s], &norms[s]);
-    nan = nan || has_nan(&h[8 * s]);
-  }
-  return nan ? FPSI_E_NAN : FPSI_OK;
+  return finish_run(x, nsteps, launched, norms);
 }
 
 int fpsi_kernel_times(fpsi_ctx* x, int32_t nsteps, int32_t cap, char* names, double* ms,
                       int64_t* launches, int32_t* count) {
   if (!x || nsteps <= 0 || cap < 0 || !count) return FPSI_E_INVALID;
-  double* hist = nullptr;
-  if (cudaMalloc((void**)&hist, size_t(nsteps) * 8 * sizeof(double)) != cudaSuccess)
-    return FPSI_E_NOMEM;
+  int rc = ensure_hist(x, nsteps);
+  if (rc) return rc;
   x->prof.clear();
   x->evnext = 0;
   x->profiling = true;
-  int rc = run_steps(x, nsteps, hist);
+  int32_t launched = 0;
+  rc = run_steps(x, nsteps, &launched);
   x->profiling = false;
   if (!rc) rc = sync(x);
-  cudaFree(hist);
   x->have_resid = x->have_asm = x->have_dq = false;
   if (rc) return rc;
+  if ((rc = finish_run(x, nsteps, launched, nullptr))) return rc;
   std::vector<std::string> keys;
   std::vector<double> tot;
   std::vector<int64_t> cnt;

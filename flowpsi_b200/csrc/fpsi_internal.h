@@ -127,7 +127,6 @@ struct fpsi_ctx {
   double* d_q = nullptr;       // [nc][5]  T,u,v,w,pg
   double* d_qb = nullptr;      // [nbf][5] boundary face states
   double* d_grad = nullptr;    // [nc][GPREC]: gradient (15) and limiter (5) per cell
-  double* d_phi = nullptr;     // d_grad + 15: the limiter inside each record (not allocated)
   double* d_F = nullptr;       // [nf][FREC]: face flux (5) and maxev_f * area
   double* d_src = nullptr;     // [nc][5]
   double* d_dtau = nullptr;    // [nc]
@@ -135,6 +134,14 @@ struct fpsi_ctx {
   double* d_part = nullptr;    // per-block partial norms
   double* d_resid = nullptr;   // 16 doubles: final norms
   double* h_resid = nullptr;   // pinned mirror
+  // residual history of fpsi_run / fpsi_run_timed: 8 norms per step on the
+  // device and their pinned host mirror, kept for the context's life (grown
+  // only for a longer run than any before)
+  double* d_hist = nullptr;
+  double* h_hist = nullptr;
+  int64_t hist_cap = 0;
+  // state copy of fpsi_newton_step_ex, to undo a rejected update
+  double* d_qsave = nullptr;   // [nc][5]
   int nblk_norm = 0;
   // implicit system (block type depends on precision)
   void* d_fjp = nullptr;       // [nf][25] TB
@@ -213,5 +220,5 @@ bool sa_active(const fpsi_ctx* x);
 int sa_launch_tmu(fpsi_ctx* x);
 int sa_launch_residual(fpsi_ctx* x);
 int sa_launch_solve(fpsi_ctx* x);
-int sa_launch_update(fpsi_ctx* x);
+int sa_launch_update(fpsi_ctx* x, const double* guard);
 }  // namespace fpsi

@@ -218,7 +218,7 @@ __device__ __forceinline__ void grad_limiter_cell(const MeshView& M, const doubl
 
 __global__ void __launch_bounds__(GRAD_THREADS)
 k_grad_limiter(MeshView M, const double* __restrict__ q, const double* __restrict__ qb, int limiter,
-               double Kl, double* __restrict__ grad, double* __restrict__ phi) {
+               double Kl, double* __restrict__ grad) {
   __shared__ double sr[GRAD_THREADS * GPREC];
   const int64_t c0 = int64_t(blockIdx.x) * GRAD_THREADS;
   const int64_t c = c0 + threadIdx.x;
@@ -226,8 +226,7 @@ k_grad_limiter(MeshView M, const double* __restrict__ q, const double* __restric
   double* my = sr + GPREC * threadIdx.x;
   if (c < M.nc) grad_limiter_cell(M, q, qb, limiter, Kl, c, my, my + 15);
   __syncthreads();
-  // gradient and limiter records are interleaved: phi == grad + 15
-  (void)phi;
+  // one record per cell: the gradient (15) then the limiter (5)
   for (int i = threadIdx.x; i < GPREC * cnt; i += GRAD_THREADS) grad[GPREC * c0 + i] = sr[i];
 }
 
@@ -251,8 +250,7 @@ struct FaceStates {
 
 __device__ __forceinline__ void reconstruct(const MeshView& M, const double* __restrict__ q,
                                             const double* __restrict__ qb,
-                                            const double* __restrict__ grad,
-                                            const double* __restrict__ phi, int64_t f,
+                                            const double* __restrict__ grad, int64_t f,
                                             double pamb, FaceStates& s) {
   const int64_t nf = M.nf;
   const int32_t a = M.cl[f];
@@ -431,12 +429,11 @@ __device__ __forceinline__ void add_visc_jac(TB* M, const VFace& v, const double
 template <bool VIS>
 __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
                             const double* __restrict__ qb, const double* __restrict__ grad,
-                            const double* __restrict__ phi, Gas g, int kind, Visc V,
-                            double* __restrict__ F) {
+                            Gas g, int kind, Visc V, double* __restrict__ F) {
   const int64_t f = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (f >= M.nf) return;
   FaceStates s;
-  reconstruct(M, q, qb, grad, phi, f, g.pamb, s);
+  reconstruct(M, q, qb, grad, f, g.pamb, s);
   const double nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
   const double A = M.area[f];
   double fl[5];
@@ -445,7 +442,7 @@ __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
     const double p = s.qr[4];
     fl[0] = 0.0, fl[1] = p * nx * A, fl[2] = p * ny * A, fl[3] = p * nz * A, fl[4] = 0.0;
   } else {
-    riemann(kind, s.L, s.R, nx, ny, nz, A, g, 0.0, 1.0, fl);
+    riemann1(kind, s.L, s.R, nx, ny, nz, A, g, fl);
   }
   if constexpr (VIS) {
     const VFace v = viscous_face(M, q, qb, grad, V, f);
@@ -649,7 +646,7 @@ constexpr int JAC_THREADS = 128;
 template <class TB, bool VIS>
 __global__ void __launch_bounds__(JAC_THREADS)
 k_face_jacobian(MeshView M, const double* __restrict__ q, const double* __restrict__ qb,
-                const double* __restrict__ grad, const double* __restrict__ phi, Gas g, Visc V,
+                const double* __restrict__ grad, Gas g, Visc V,
                 TB* __restrict__ fjp, TB* __restrict__ fjm) {
   __shared__ TB stage[JAC_THREADS * 25];
   const int64_t f0 = int64_t(blockIdx.x) * JAC_THREADS;
@@ -660,10 +657,10 @@ k_face_jacobian(MeshView M, const double* __restrict__ q, const double* __restri
   double nx = 0, ny = 0, nz = 0, A = 0;
   if (live) {
     FaceStates s;
-    reconstruct(M, q, qb, grad, phi, f, g.pamb, s);
+    reconstruct(M, q, qb, grad, f, g.pamb, s);
     nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
     A = M.area[f];
-    ra = roe_average(s.L, s.R, nx, ny, nz, g, 0.0, 1.0);
+    ra = roe_average1(s.L, s.R, nx, ny, nz, g);
     TB* st = stage + 25 * threadIdx.x;
     if (bc_kind(M, f) == FPSI_BC_VISCOUS_WALL) {
       // d(pressure flux)/dq of the wall (bcViscousWall.loci:232-240); u_f.n = 0
@@ -671,7 +668,7 @@ k_face_jacobian(MeshView M, const double* __restrict__ q, const double* __restri
       for (int k = 0; k < 25; ++k) st[k] = TB(0);
       st[9] = TB(nx * A), st[14] = TB(ny * A), st[19] = TB(nz * A);
     } else {
-      jac_roe<TB>(ra, nx, ny, nz, A, g, +1, st);
+      jac_roe1<TB>(ra, nx, ny, nz, A, g, +1, st);
     }
     if constexpr (VIS) {
       const double nn[3] = {nx, ny, nz};
@@ -682,7 +679,7 @@ k_face_jacobian(MeshView M, const double* __restrict__ q, const double* __restri
   for (int64_t k = threadIdx.x; k < cnt; k += JAC_THREADS) fjp[25 * f0 + k] = stage[k];
   __syncthreads();
   if (live && f < M.nfi) {
-    jac_roe<TB>(ra, nx, ny, nz, A, g, -1, stage + 25 * threadIdx.x);
+    jac_roe1<TB>(ra, nx, ny, nz, A, g, -1, stage + 25 * threadIdx.x);
     if constexpr (VIS) {
       const double nn[3] = {nx, ny, nz};
       add_visc_jac<TB>(stage + 25 * threadIdx.x, viscous_face(M, q, qb, grad, V, f), nn, A, -1.0);
@@ -701,7 +698,7 @@ k_face_jacobian(MeshView M, const double* __restrict__ q, const double* __restri
 template <class TB>
 __global__ void __launch_bounds__(JAC_THREADS)
 k_face_jacobian_c(MeshView M, const double* __restrict__ q, const double* __restrict__ qb,
-                  const double* __restrict__ grad, const double* __restrict__ phi, Gas g,
+                  const double* __restrict__ grad, Gas g,
                   TB* __restrict__ fjc) {
   __shared__ TB stage[JAC_THREADS * CK_FACE];
   const int64_t f0 = int64_t(blockIdx.x) * JAC_THREADS;
@@ -709,20 +706,20 @@ k_face_jacobian_c(MeshView M, const double* __restrict__ q, const double* __rest
   const int64_t cnt = min(int64_t(JAC_THREADS), M.nf - f0) * CK_FACE;
   if (f < M.nf) {
     FaceStates s;
-    reconstruct(M, q, qb, grad, phi, f, g.pamb, s);
+    reconstruct(M, q, qb, grad, f, g.pamb, s);
     const double nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
     const double A = M.area[f];
-    const RoeAvg ra = roe_average(s.L, s.R, nx, ny, nz, g, 0.0, 1.0);
+    const RoeAvg ra = roe_average1(s.L, s.R, nx, ny, nz, g);
     TB* st = stage + CK_FACE * threadIdx.x;
     if (bc_kind(M, f) == FPSI_BC_VISCOUS_WALL) {
 #pragma unroll
       for (int k = 0; k < CK_DIR; ++k) st[k] = TB(0);
       st[CK_C1] = TB(-A);
     } else {
-      jac_roe_compact<TB>(ra, A, g, +1, st);
+      jac_roe_compact<TB, true>(ra, A, g, +1, st);
     }
     if (f < M.nfi) {
-      jac_roe_compact<TB>(ra, A, g, -1, st + CK_DIR);
+      jac_roe_compact<TB, true>(ra, A, g, -1, st + CK_DIR);
     } else {
 #pragma unroll
       for (int k = 0; k < CK_DIR; ++k) st[CK_DIR + k] = TB(0);
@@ -1214,13 +1211,18 @@ __global__ void k_sum2(const double* __restrict__ part, int nblk, double* __rest
 // ---------------------------------------------------------------------------
 // clipped Newton update (solverNewton.loci:62-78)
 // ---------------------------------------------------------------------------
+// guard (may be null): the norms of the residual this system was built
+// from; when they are NaN the state is left as it is, so a run that meets a
+// NaN residual keeps the state of that step (solverResidual.loci:203-208
+// aborts there)
 template <class TX>
 __global__ void __launch_bounds__(NORM_THREADS)
 k_update(int64_t nc, double pamb, const int32_t* __restrict__ ci, const TX* __restrict__ x, double* __restrict__ q,
-         double* __restrict__ amin_part) {
+         double* __restrict__ amin_part, const double* __restrict__ guard) {
   const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   double alpha = 1.0;
-  if (c < nc) {
+  const bool halt = guard && (isnan(guard[0]) || isnan(guard[1]) || isnan(guard[2]));
+  if (c < nc && !halt) {
     double* qc = q + 5 * c;
     const TX* d = x + 5 * int64_t(ci[c]);
     const double dT = double(d[0]), dp = double(d[4]);
@@ -1363,17 +1365,17 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
   }
   prof_begin(x, "grad_limiter");
   dev::k_grad_limiter<<<blocks_for(M.nc, dev::GRAD_THREADS), dev::GRAD_THREADS, 0, s>>>(M, x->d_q, x->d_qb, x->P.limiter,
-                                                             x->P.Kl, x->d_grad, x->d_phi);
+                                                             x->P.Kl, x->d_grad);
   prof_end(x);
   prof_begin(x, "face_flux");
   // the viscous terms are a separate instantiation: the inviscid kernel
   // does not carry their registers
   if (x->P.viscous)
     dev::k_face_flux<true><<<blocks_for(M.nf, 128), 128, 0, s>>>(
-        M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, x->P.flux, visc(x), x->d_F);
+        M, x->d_q, x->d_qb, x->d_grad, g, x->P.flux, visc(x), x->d_F);
   else
     dev::k_face_flux<false><<<blocks_for(M.nf, 128), 128, 0, s>>>(
-        M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, x->P.flux, visc(x), x->d_F);
+        M, x->d_q, x->d_qb, x->d_grad, g, x->P.flux, visc(x), x->d_F);
   prof_end(x);
   prof_begin(x, "cell_residual");
   dev::k_cell_residual<<<x->nblk_norm, dev::NORM_THREADS, 0, s>>>(
@@ -1431,13 +1433,13 @@ static int launch_assemble_t(fpsi_ctx* x) {
   prof_begin(x, "face_jacobian");
   if (cpt)
     dev::k_face_jacobian_c<TB><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
-        M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, (TB*)x->d_fjc);
+        M, x->d_q, x->d_qb, x->d_grad, g, (TB*)x->d_fjc);
   else if (x->P.viscous)
     dev::k_face_jacobian<TB, true><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
-        M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, visc(x), fjp, fjm);
+        M, x->d_q, x->d_qb, x->d_grad, g, visc(x), fjp, fjm);
   else
     dev::k_face_jacobian<TB, false><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
-        M, x->d_q, x->d_qb, x->d_grad, x->d_phi, g, visc(x), fjp, fjm);
+        M, x->d_q, x->d_qb, x->d_grad, g, visc(x), fjp, fjm);
   prof_end(x);
   prof_begin(x, "assemble_lu");
   if (cpt)
@@ -1568,7 +1570,7 @@ int launch_linres(fpsi_ctx* x, double* out2) {
   }
 }
 
-int launch_update(fpsi_ctx* x) {
+int launch_update(fpsi_ctx* x, const double* guard) {
   const int64_t nc = x->H.nc;
   const bool lsgs = x->P.solver == FPSI_SOLVER_LSGS;
   const int32_t* map = lsgs ? x->d_lt : x->d_ci;
@@ -1576,10 +1578,10 @@ int launch_update(fpsi_ctx* x) {
   prof_begin(x, "update");
   if (x->P.precision == FPSI_PREC_MIXED)
     dev::k_update<float><<<x->nblk_norm, dev::NORM_THREADS, 0, x->stream>>>(
-        nc, x->P.Pambient, map, (const float*)xv, x->d_q, x->d_amin);
+        nc, x->P.Pambient, map, (const float*)xv, x->d_q, x->d_amin, guard);
   else
     dev::k_update<double><<<x->nblk_norm, dev::NORM_THREADS, 0, x->stream>>>(
-        nc, x->P.Pambient, map, (const double*)xv, x->d_q, x->d_amin);
+        nc, x->P.Pambient, map, (const double*)xv, x->d_q, x->d_amin, guard);
   prof_end(x);
   FPSI_CUDA_TRY(cudaGetLastError());
   if (x->keep_prev && x->d_xprev && !lsgs) {

@@ -23,8 +23,10 @@ int launch_linres(fpsi_ctx* x, double* out2);
 // fills fjp/fjm from the compact face records of the assembled system (a
 // no-op when they already hold it)
 int ensure_explicit_blocks(fpsi_ctx* x);
-// clipped Newton update; per-block minimum alpha into d_amin
-int launch_update(fpsi_ctx* x);
+// clipped Newton update; per-block minimum alpha into d_amin.  guard
+// (device, may be null): the norms of the residual the system came from;
+// NaN norms leave the state unchanged
+int launch_update(fpsi_ctx* x, const double* guard);
 // caller-order staging buffer <-> device state (in = staging -> q)
 int launch_state(fpsi_ctx* x, bool in);
 

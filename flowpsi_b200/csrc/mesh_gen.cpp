@@ -1,8 +1,9 @@
 // mesh_gen.cpp -- synthetic grids for the benchmark configurations.
 //
 // kind 0: structured hex box (configs: 32^3 farfield cube, 256^3 shock cube)
-// kind 1: periodic hex box, each hex split into 6 Kuhn tetrahedra along its
-//         main diagonal, nodes jittered (128^3 Taylor-Green case)
+// kind 1: hex box, each hex split into 6 Kuhn tetrahedra along its main
+//         diagonal, nodes jittered; periodic (128^3 Taylor-Green case) or
+//         bounded sides (the steady farfield tet case)
 // kind 2: boundary-layer hex block with geometric wall-normal stretching
 // kind 3: hex box (as kind 0, periodic sides allowed) with each hex split
 //         into two triangular prisms across the diagonal v000-v110 of its
@@ -207,44 +208,65 @@ int gen_hex(const fpsi_mesh_spec* s, OwnedMesh* o, bool stretched, bool prism = 
   return FPSI_OK;
 }
 
-// Kuhn split of each hex of a periodic box into 6 tetrahedra.  For the
-// permutation (a,b,c) of the axes, tet = {v0, v0+e_a, v0+e_a+e_b, v0+1}.
-// Face sharing is analytic:
+// Kuhn split of each hex of a box into 6 tetrahedra.  For the permutation
+// (a,b,c) of the axes, tet = {v0, v0+e_a, v0+e_a+e_b, v0+1}.  Face sharing
+// is analytic:
 //   opposite v7         <-> tet (c,a,b) of the hex at -e_c   (cube-face)
 //   opposite v0         <-> tet (b,c,a) of the hex at +e_a   (cube-face)
 //   opposite v0+e_a     <-> tet (b,a,c) of the same hex      (internal)
 //   opposite v0+e_a+e_b <-> tet (a,c,b) of the same hex      (internal)
+// The split conforms across opposite sides of the box, so every direction
+// may be periodic (bc_side < 0: the neighbour hex wraps around) or bounded
+// (a cube-face tet face on the side becomes a boundary face of that side's
+// condition).  Node coordinates are jittered by U(-jitter,+jitter) of the
+// spacing, except the normal component of nodes on a bounded side, so the
+// sides stay plane.  A periodic direction has one node layer per hex layer
+// (periodic images share their node and its jitter).
 int gen_kuhn(const fpsi_mesh_spec* s, OwnedMesh* o) {
   const int64_t nx = s->nx, ny = s->ny, nz = s->nz;
   if (nx < 2 || ny < 2 || nz < 2) return FPSI_E_INVALID;
+  bool per[3];
+  for (int d = 0; d < 3; ++d) {
+    per[d] = s->bc_side[2 * d] < 0;
+    if ((s->bc_side[2 * d] < 0) != (s->bc_side[2 * d + 1] < 0)) return FPSI_E_INVALID;
+  }
+  const bool anyper = per[0] || per[1] || per[2];
   static const int PERM[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
   auto perm_id = [&](int a, int b, int c) {
     for (int p = 0; p < 6; ++p)
       if (PERM[p][0] == a && PERM[p][1] == b && PERM[p][2] == c) return p;
     return -1;
   };
-  const int64_t nn = nx * ny * nz;  // periodic: one node per (i,j,k)
   const double h[3] = {s->Lx / nx, s->Ly / ny, s->Lz / nz};
   const double L[3] = {s->Lx, s->Ly, s->Lz};
   const int64_t N[3] = {nx, ny, nz};
+  // node layers per direction: n (periodic) or n + 1 (bounded)
+  const int64_t NN[3] = {per[0] ? nx : nx + 1, per[1] ? ny : ny + 1, per[2] ? nz : nz + 1};
+  const int64_t nn = NN[0] * NN[1] * NN[2];
   o->xyz.resize(size_t(nn * 3));
-  for (int64_t k = 0; k < nz; ++k)
-    for (int64_t j = 0; j < ny; ++j)
-      for (int64_t i = 0; i < nx; ++i) {
-        int64_t id = i + nx * (j + ny * k);
+  for (int64_t k = 0; k < NN[2]; ++k)
+    for (int64_t j = 0; j < NN[1]; ++j)
+      for (int64_t i = 0; i < NN[0]; ++i) {
+        int64_t id = i + NN[0] * (j + NN[1] * k);
         int64_t ijk[3] = {i, j, k};
         for (int d = 0; d < 3; ++d) {
-          double jt = s->jitter * h[d] * (2.0 * u01(s->seed, uint64_t(3 * id + d)) - 1.0);
+          const bool on_side = !per[d] && (ijk[d] == 0 || ijk[d] == N[d]);
+          double jt = on_side ? 0.0
+                              : s->jitter * h[d] * (2.0 * u01(s->seed, uint64_t(3 * id + d)) - 1.0);
           o->xyz[3 * id + d] = h[d] * ijk[d] + jt;
         }
       }
+  auto nodeid = [&](int64_t i, int64_t j, int64_t k) {
+    if (per[0]) i = (i + nx) % nx;
+    if (per[1]) j = (j + ny) % ny;
+    if (per[2]) k = (k + nz) % nz;
+    return i + NN[0] * (j + NN[1] * k);
+  };
   auto hexid = [&](int64_t i, int64_t j, int64_t k) {
     i = (i + nx) % nx, j = (j + ny) % ny, k = (k + nz) % nz;
     return i + nx * (j + ny * k);
   };
-  const int64_t ncell = 6 * nn;
-  // vertex v of a tet in hex (i,j,k) with offset o[3] -> node id + shift
-  // (shift = the periodic wrap in physical units, relative to the hex frame)
+  const int64_t ncell = 6 * nx * ny * nz;
   o->face_off.push_back(0);
   for (int64_t k = 0; k < nz; ++k)
     for (int64_t j = 0; j < ny; ++j)
@@ -260,7 +282,6 @@ int gen_kuhn(const fpsi_mesh_spec* s, OwnedMesh* o) {
           const int32_t me = int32_t(6 * hx + p);
           // the four faces: (opposite vertex, neighbour tet, shift of neighbour hex)
           for (int opp = 0; opp < 4; ++opp) {
-            int64_t nh;
             int np;
             int dshift[3] = {0, 0, 0};
             if (opp == 3) {
@@ -274,19 +295,27 @@ int gen_kuhn(const fpsi_mesh_spec* s, OwnedMesh* o) {
             } else {
               np = perm_id(a, c, b);
             }
-            nh = hexid(i + dshift[0], j + dshift[1], k + dshift[2]);
-            const int32_t other = int32_t(6 * nh + np);
-            // emit each face once, from the smaller cell id (cl < cr)
-            if (other < me) continue;
-            if (other == me) return FPSI_E_INVALID;
-            // nodes of the face (the three vertices other than opp) and
-            // their positions in this hex's frame
+            // a neighbour hex across a bounded side: boundary face
+            int32_t bcode = 0;
+            for (int d = 0; d < 3; ++d) {
+              const int64_t u = base[d] + dshift[d];
+              if (!per[d] && u < 0) bcode = -1 - s->bc_side[2 * d];
+              if (!per[d] && u >= N[d]) bcode = -1 - s->bc_side[2 * d + 1];
+            }
+            int32_t other = bcode;
+            if (!bcode) {
+              const int64_t nh = hexid(i + dshift[0], j + dshift[1], k + dshift[2]);
+              other = int32_t(6 * nh + np);
+              // emit each interior face once, from the smaller cell id (cl < cr)
+              if (other < me) continue;
+              if (other == me) return FPSI_E_INVALID;
+            }
+            // nodes of the face (the three vertices other than opp)
             int32_t ids[3];
             int q = 0;
             for (int v = 0; v < 4; ++v) {
               if (v == opp) continue;
-              int64_t ii = base[0] + off[v][0], jj = base[1] + off[v][1], kk = base[2] + off[v][2];
-              ids[q++] = int32_t(hexid(ii, jj, kk));
+              ids[q++] = int32_t(nodeid(base[0] + off[v][0], base[1] + off[v][1], base[2] + off[v][2]));
             }
             // orientation: normal must point away from the opposite vertex.
             // positions (unjittered is enough for the sign; jitter < h/2)
@@ -310,59 +339,49 @@ int gen_kuhn(const fpsi_mesh_spec* s, OwnedMesh* o) {
             double sd = 0;
             for (int d = 0; d < 3; ++d) sd += nrm[d] * (P[0][d] - Vo[d]);
             if (sd < 0) std::swap(ids[1], ids[2]);
-            // node coordinates are stored wrapped into the box; the face's
-            // vertices in this tet's frame may sit one period above: record
-            // per face the frame via pshift, and place nodes in cl's frame
-            // by storing the face with cl = me.  The wrap of each vertex
-            // is handled in the geometry through pshift only if the face
-            // vertices themselves wrap, which we avoid by writing explicit
-            // per-face node copies below.
             o->cl.push_back(me);
             o->cr.push_back(other);
-            double sh[3];
-            for (int d = 0; d < 3; ++d) sh[d] = dshift[d] * L[d];
-            // cr's image next to me: x_other + pshift, where the neighbour hex
-            // was wrapped; unwrapped hex index = base + dshift.
-            for (int d = 0; d < 3; ++d) {
-              int64_t unwrapped = base[d] + dshift[d];
-              double s2 = 0;
-              if (unwrapped < 0) s2 = -L[d];
-              if (unwrapped >= N[d]) s2 = L[d];
-              o->pshift.push_back(s2);
-            }
-            (void)sh;
+            // x_cr_image = x_cr + pshift: the wrap of the neighbour hex
+            if (anyper)
+              for (int d = 0; d < 3; ++d) {
+                const int64_t u = base[d] + dshift[d];
+                double s2 = 0;
+                if (!bcode && u < 0) s2 = -L[d];
+                if (!bcode && u >= N[d]) s2 = L[d];
+                o->pshift.push_back(s2);
+              }
             for (int v = 0; v < 3; ++v) o->face_nodes.push_back(ids[v]);
             o->face_off.push_back(int64_t(o->face_nodes.size()));
           }
         }
       }
-  // Faces reference wrapped node ids; a face whose vertices straddle the
-  // periodic seam must be expressed in cl's frame.  Emit private node copies
-  // for those faces (nodes appended after the shared ones).
+  // Faces reference wrapped node ids; a face whose vertices straddle a
+  // periodic seam is expressed in cl's frame through private node copies
+  // (appended after the shared nodes).
   const int64_t nf = int64_t(o->cl.size());
-  for (int64_t f = 0; f < nf; ++f) {
-    // recover cl's hex base
-    int64_t hx = o->cl[f] / 6;
-    int64_t bi = hx % nx, bj = (hx / nx) % ny, bk = hx / (nx * ny);
-    int64_t b = o->face_off[f];
-    for (int q = 0; q < 3; ++q) {
-      int64_t nd = o->face_nodes[b + q];
-      int64_t ii = nd % nx, jj = (nd / nx) % ny, kk = nd / (nx * ny);
-      // the vertex belongs to hex base + {0,1}: unwrap relative to base
-      double add[3] = {0, 0, 0};
-      int64_t v[3] = {ii, jj, kk}, bb[3] = {bi, bj, bk};
-      bool wrap = false;
-      for (int d = 0; d < 3; ++d)
-        if (v[d] < bb[d]) {
-          add[d] = L[d];
-          wrap = true;
-        }
-      if (!wrap) continue;
-      int64_t newid = int64_t(o->xyz.size() / 3);
-      for (int d = 0; d < 3; ++d) o->xyz.push_back(o->xyz[3 * nd + d] + add[d]);
-      o->face_nodes[b + q] = int32_t(newid);
+  if (anyper)
+    for (int64_t f = 0; f < nf; ++f) {
+      const int64_t hx = o->cl[f] / 6;
+      const int64_t bb[3] = {hx % nx, (hx / nx) % ny, hx / (nx * ny)};
+      const int64_t b = o->face_off[f];
+      for (int q = 0; q < 3; ++q) {
+        const int64_t nd = o->face_nodes[b + q];
+        const int64_t v[3] = {nd % NN[0], (nd / NN[0]) % NN[1], nd / (NN[0] * NN[1])};
+        // the vertex belongs to hex base + {0,1}: unwrap relative to base
+        double add[3] = {0, 0, 0};
+        bool wrap = false;
+        for (int d = 0; d < 3; ++d)
+          if (per[d] && v[d] < bb[d]) {
+            add[d] = L[d];
+            wrap = true;
+          }
+        if (!wrap) continue;
+        const int64_t newid = int64_t(o->xyz.size() / 3);
+        for (int d = 0; d < 3; ++d) o->xyz.push_back(o->xyz[3 * nd + d] + add[d]);
+        o->face_nodes[b + q] = int32_t(newid);
+      }
     }
-  }
+  o->bcs.assign(s->bcs, s->bcs + s->nbc);
   o->m.ncells = ncell;
   finish(o);
   o->m.ncells = ncell;

@@ -112,22 +112,32 @@ k_norm_combine(const double* __restrict__ scratch, int64_t nblk, double* __restr
   }
 }
 
-// Device address of g_norm_scratch, looked up once per device.  In host
-// code the symbol itself is only a host-side stand-in: a kernel given it
-// would fault or silently use the wrong memory.
+// Device address of g_norm_scratch.  In host code the symbol itself is
+// only a host-side stand-in: a kernel given it would fault or silently use
+// the wrong memory.  The address is looked up on every call made outside a
+// stream capture (the lookup allocates nothing), so a module reloaded after
+// cudaDeviceReset is followed; a call inside a capture uses the address the
+// last uncaptured call on that device found.
 constexpr int NA_MAX_DEVICES = 64;
 std::mutex g_mu;
 double* g_scratch_ptr[NA_MAX_DEVICES] = {nullptr};
 
-int scratch_for_current_device(double** out) {
+int scratch_for_current_device(cudaStream_t s, double** out) {
   int dev = 0;
   FPSI_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= NA_MAX_DEVICES) {
     fpsi::set_error("device ordinal %d beyond the %d supported", dev, NA_MAX_DEVICES);
     return FPSI_E_UNSUPPORTED;
   }
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  FPSI_CUDA_TRY(cudaStreamIsCapturing(s, &cap));
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_scratch_ptr[dev]) {
+  if (cap != cudaStreamCaptureStatusNone && !g_scratch_ptr[dev]) {
+    fpsi::set_error("fpsi_residual_norms_noalloc: the first call on a device must come before "
+                    "any stream capture");
+    return FPSI_E_STATE;
+  }
+  if (cap == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_norm_scratch);
     if (e != cudaSuccess || !p) {
@@ -153,10 +163,10 @@ extern "C" int fpsi_residual_norms_noalloc(const double* d_src, const double* d_
                     "of %lld cells", (long long)nc, (long long)NA_MAX_CELLS);
     return FPSI_E_INVALID;
   }
-  double* scratch = nullptr;
-  int rc = scratch_for_current_device(&scratch);
-  if (rc) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* scratch = nullptr;
+  int rc = scratch_for_current_device(s, &scratch);
+  if (rc) return rc;
   const int64_t nblk = (nc + NA_CELLS_PER_BLOCK - 1) / NA_CELLS_PER_BLOCK;
   k_norm_partial<<<unsigned(nblk), NA_THREADS, 0, s>>>(d_src, d_vol, nc, vol_tot, scratch);
   k_norm_combine<<<1, NA_THREADS, 0, s>>>(scratch, nblk, d_out);

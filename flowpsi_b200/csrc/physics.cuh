@@ -71,6 +71,82 @@ struct RoeK {
   double l1, rT, c7, c8, c9, c10, c11, c4, c1, rho, t4, d23;
 };
 
+// ---- eta == 1 with a fixed grid (us_n == 0): the form every mesh kernel
+// evaluates.  The preconditioning parameter is 1 for Minf >= 0.5
+// (fluxInviscid.loci:97-112), the only range the library accepts, and the
+// grid does not move.  Then sigma = sqrt(4 a^2) = 2 a and every (beta - 1)
+// term of roeCT_flux / RoeJacobian vanishes, so the coefficient set needs
+// the reciprocals of a and of rT instead of a dozen divisions.  Results
+// differ from the general form by a few ulp of their terms.
+__device__ __forceinline__ RoeAvg roe_average1(const Q5& L, const Q5& R, double nx, double ny,
+                                               double nz, const Gas& g) {
+  RoeAvg s;
+  const double gm1 = g.gamma - 1.0;
+  const double pl = L.p + g.pamb, pr = R.p + g.pamb;
+  const double RTl = g.Rt * L.T, RTr = g.Rt * R.T;
+  s.rl = pl / RTl;
+  s.rr = pr / RTr;
+  const double kl = 0.5 * (L.u * L.u + L.v * L.v + L.w * L.w);
+  const double kr = 0.5 * (R.u * R.u + R.v * R.v + R.w * R.w);
+  const double igm1 = 1.0 / gm1;
+  s.rel = s.rl * (RTl * igm1 + kl);
+  s.rer = s.rr * (RTr * igm1 + kr);
+  // h0 = (rho e0 + p) / rho = gamma R T / (gamma - 1) + |u|^2 / 2
+  const double h0l = g.gamma * RTl * igm1 + kl;
+  const double h0r = g.gamma * RTr * igm1 + kr;
+  const double wl = sqrt(s.rl), wr = sqrt(s.rr);
+  s.r = wl * wr;
+  const double iw = 1.0 / (wl + wr);
+  s.U = (L.u * wl + R.u * wr) * iw;
+  s.V = (L.v * wl + R.v * wr) * iw;
+  s.W = (L.w * wl + R.w * wr) * iw;
+  s.unA = s.U * nx + s.V * ny + s.W * nz;
+  s.un = s.unA;
+  s.h0 = (h0l * wl + h0r * wr) * iw;
+  const double h = s.h0 - 0.5 * (s.U * s.U + s.V * s.V + s.W * s.W);
+  s.eta = 1.0;
+  s.a = sqrt(dmax(gm1 * h, 1e-30));
+  s.sigma = 2.0 * s.a;
+  return s;
+}
+
+// roe_k at eta == 1; isg receives 1/sigma for the flux's dissipation
+__device__ __forceinline__ RoeK roe_k1(double l1, double l2, double l3, const RoeAvg& s,
+                                       const Gas& g, double& isg) {
+  const double gm1 = g.gamma - 1.0;
+  const double ia = 1.0 / s.a;
+  const double ia2 = ia * ia;
+  isg = 0.5 * ia;
+  const double d23 = l2 - l3;
+  const double s23 = l2 + l3 - 2.0 * l1;
+  const double t3 = -0.25 * s.r * s.sigma;  // r (0 - sigma^2) / (4 sigma)
+  const double t5 = 0.5 * s23;              // (s23 sigma) / (2 sigma)
+  const double t6 = 0.5 * (l2 + l3);
+  const double cp = g.gamma * g.Rt / gm1;
+  const double rT = -g.gamma * g.Rt * s.r * ia2;  // -gamma R rho / ((gamma - 1) h)
+  const double irT = 1.0 / rT;
+  RoeK k;
+  k.l1 = l1;
+  k.rT = rT;
+  k.rho = s.r;
+  const double dt3 = d23 * t3 * ia2;
+  k.c7 = dt3;
+  k.c8 = (g.gamma * t6 - gm1 * t5) * ia2;
+  k.c9 = cp * s.r + s.h0 * rT;
+  const double x1 = g.gamma * s.h0 * dt3;
+  const double x2 = -gm1 * dt3 * k.c9 * irT;
+  const double x3 = -d23 * t3;
+  const double x4 = 0.5 * s.r * s23 * s.unA;  // r t4 unA / (2 sigma), t4 = s23 sigma
+  k.c10 = (x1 + x2 + x3 + x4);
+  k.c11 = (ia2 * s.h0 + (k.c9 - s.r * cp) * ia2 * gm1 * irT - 1.0) * t6 -
+          gm1 * ia2 * k.c9 * t5 * irT - s.unA * d23 * isg;
+  k.c4 = 0.5 * s.r * s23;  // r t4 / (2 sigma)
+  k.c1 = d23 * isg;
+  k.t4 = s23 * s.sigma;
+  k.d23 = d23;
+  return k;
+}
+
 __device__ __forceinline__ RoeK roe_k(double l1, double l2, double l3, const RoeAvg& s,
                                       const Gas& g) {
   const double beta = s.eta, sg = s.sigma, un = s.un;
@@ -197,6 +273,57 @@ __device__ __forceinline__ void flux_roe(const Q5& L, const Q5& R, double nx, do
   F[4] = ah * ((s.rel * unl + pl * unlA) + (s.rer * unr + pr * unrA) - d[4]);
 }
 
+// roeCT_flux at eta == 1 on a fixed grid (see roe_average1)
+__device__ __forceinline__ void flux_roe1(const Q5& L, const Q5& R, double nx, double ny,
+                                          double nz, double area, const Gas& g, double F[5]) {
+  const RoeAvg s = roe_average1(L, R, nx, ny, nz, g);
+  const double l2s = s.un - s.a;  // (un (eta + 1) - sigma) / 2
+  const double l3s = s.un + s.a;
+  double l1 = fabs(s.un), l2 = fabs(l2s), l3 = fabs(l3s);
+  const double unl = L.u * nx + L.v * ny + L.w * nz, unr = R.u * nx + R.v * ny + R.w * nz;
+  const double hl = sqrt(g.gamma * g.Rt * L.T), hr = sqrt(g.gamma * g.Rt * R.T);  // sigma / 2
+  const double w2 = dmax(0.0, dmax(l2s - (unl - hl), (unr - hr) - l2s));
+  const double w3 = dmax(0.0, dmax(l3s - (unl + hl), (unr + hr) - l3s));
+  if (l2 < w2) l2 = 0.5 * ((l2s * l2s) / w2 + w2);
+  if (l3 < w3) l3 = 0.5 * ((l3s * l3s) / w3 + w3);
+  double isg;
+  const RoeK k = roe_k1(l1, l2, l3, s, g, isg);
+  const double dT = R.T - L.T, dp = R.p - L.p;
+  const double du = R.u - L.u, dv = R.v - L.v, dw = R.w - L.w;
+  const double uj = du * nx + dv * ny + dw * nz;
+  const double dsg = k.d23 * isg, tsg = s.r * k.t4 * uj * (0.5 * isg);
+  double d[5];
+  d[0] = dp * k.c8 + uj * k.c7 + l1 * dT * k.rT;
+  d[1] = s.U * k.c7 * uj + l1 * (s.U * dT * k.rT + s.r * du) + dp * (k.c8 * s.U - nx * dsg) + nx * tsg;
+  d[2] = s.V * k.c7 * uj + l1 * (s.V * dT * k.rT + s.r * dv) + dp * (k.c8 * s.V - ny * dsg) + ny * tsg;
+  d[3] = s.W * k.c7 * uj + l1 * (s.W * dT * k.rT + s.r * dw) + dp * (k.c8 * s.W - nz * dsg) + nz * tsg;
+  d[4] = dp * k.c11 + k.c10 * uj + l1 * (k.c9 * dT + s.r * (s.U * du + s.V * dv + s.W * dw));
+  const double ah = 0.5 * area;
+  const double ml = s.rl * unl, mr = s.rr * unr;
+  const double pl = L.p + g.pamb, pr = R.p + g.pamb;
+  F[0] = ah * (ml + mr - d[0]);
+  F[1] = ah * (L.u * ml + R.u * mr + nx * (L.p + R.p) - d[1]);
+  F[2] = ah * (L.v * ml + R.v * mr + ny * (L.p + R.p) - d[2]);
+  F[3] = ah * (L.w * ml + R.w * mr + nz * (L.p + R.p) - d[3]);
+  F[4] = ah * ((s.rel * unl + pl * unl) + (s.rer * unr + pr * unr) - d[4]);
+}
+
+// smoothed eigenvalue Jacobian coefficients at eta == 1 (roe_k_smoothed)
+__device__ __forceinline__ RoeK roe_k_smoothed1(const RoeAvg& s, const Gas& g, int dir) {
+  double l1 = s.un;
+  double l2 = s.un - s.a;
+  double l3 = s.un + s.a;
+  const double hi = dmax(l1, dmax(l2, l3)), lo = dmin(l1, dmin(l2, l3));
+  const double e = 0.02 * (hi - lo);
+  const double e2 = e * e;
+  const double d = dir < 0 ? -1.0 : 1.0;
+  l1 = 0.5 * (l1 + d * sqrt(l1 * l1 + e2));
+  l2 = 0.5 * (l2 + d * sqrt(l2 * l2 + e2));
+  l3 = 0.5 * (l3 + d * sqrt(l3 * l3 + e2));
+  double isg;
+  return roe_k1(l1, l2, l3, s, g, isg);
+}
+
 // Smoothed one-sided eigenvalue Jacobian, roeCT_jacobian (:1141-1167):
 // l -> (l +- sqrt(l^2 + (0.02 (lmax - lmin))^2)) / 2.
 __device__ __forceinline__ RoeK roe_k_smoothed(const RoeAvg& s, const Gas& g, int dir) {
@@ -220,6 +347,12 @@ __device__ __forceinline__ void jac_roe(const RoeAvg& s, double nx, double ny, d
   roe_k_matrix<TB>(roe_k_smoothed(s, g, dir), s, nx, ny, nz, area, M);
 }
 
+template <class TB>
+__device__ __forceinline__ void jac_roe1(const RoeAvg& s, double nx, double ny, double nz,
+                                         double area, const Gas& g, int dir, TB* M) {
+  roe_k_matrix<TB>(roe_k_smoothed1(s, g, dir), s, nx, ny, nz, area, M);
+}
+
 // Compact form of area * K: nine per-direction coefficients (area folded in)
 // with which, for x = (x0, x_m, x4) and dun = n . x_m,
 //   y0  = a1 x0 + c7 dun + c8 x4
@@ -233,10 +366,10 @@ enum { CK_A1, CK_C7, CK_C8, CK_C4, CK_C1, CK_LR, CK_L9, CK_C10, CK_C11, CK_DIR }
 constexpr int CK_FACE = 2 * CK_DIR + 6;  // 24
 constexpr int CK_SLOT = CK_DIR + 6;      // 15
 
-template <class TB>
+template <class TB, bool ETA1 = false>
 __device__ __forceinline__ void jac_roe_compact(const RoeAvg& s, double area, const Gas& g, int dir,
                                                 TB* c) {
-  const RoeK k = roe_k_smoothed(s, g, dir);
+  const RoeK k = ETA1 ? roe_k_smoothed1(s, g, dir) : roe_k_smoothed(s, g, dir);
   c[CK_A1] = TB(area * (k.l1 * k.rT));
   c[CK_C7] = TB(area * k.c7);
   c[CK_C8] = TB(area * k.c8);
@@ -360,18 +493,14 @@ __device__ __forceinline__ void flux_hllc(const Q5& L, const Q5& R, double nx, d
   const double ps = pgs + g.pamb;
   const double CR = SR - fabs(SM), CL = SL + fabs(SM);
   const double fl = (SL - unl) * rl, fr = (SR - unr) * rr;
-  // star states U*_L, U*_R (conserved), weighted by CL, CR
-  F[0] += AM * (CR * (fr / (SR - SM)) + CL * (fl / (SL - SM)));
-  F[1] += AM * (CR * ((fr * R.u + (pgs - R.p) * nx) / (SR - SM)) +
-                CL * ((fl * L.u + (pgs - L.p) * nx) / (SL - SM)));
-  F[2] += AM * (CR * ((fr * R.v + (pgs - R.p) * ny) / (SR - SM)) +
-                CL * ((fl * L.v + (pgs - L.p) * ny) / (SL - SM)));
-  F[3] += AM * (CR * ((fr * R.w + (pgs - R.p) * nz) / (SR - SM)) +
-                CL * ((fl * L.w + (pgs - L.p) * nz) / (SL - SM)));
-  F[4] += AM * (CR * ((fr * w.er - pr * unr + ps * SM) / (SR - SM)) +
-                CL * ((fl * w.el - pl * unl + ps * SM) / (SL - SM)));
-  (void)il;
-  (void)ir;
+  // star states U*_L, U*_R (conserved), weighted by CL, CR; the ten
+  // quotients by SR - SM and SL - SM share two reciprocals
+  F[0] += AM * (CR * (fr * ir) + CL * (fl * il));
+  F[1] += AM * (CR * ((fr * R.u + (pgs - R.p) * nx) * ir) + CL * ((fl * L.u + (pgs - L.p) * nx) * il));
+  F[2] += AM * (CR * ((fr * R.v + (pgs - R.p) * ny) * ir) + CL * ((fl * L.v + (pgs - L.p) * ny) * il));
+  F[3] += AM * (CR * ((fr * R.w + (pgs - R.p) * nz) * ir) + CL * ((fl * L.w + (pgs - L.p) * nz) * il));
+  F[4] += AM * (CR * ((fr * w.er - pr * unr + ps * SM) * ir) +
+                CL * ((fl * w.el - pl * unl + ps * SM) * il));
 }
 
 __device__ __forceinline__ void analytic_flux(const Q5& q, double rho, double e0, double unA,
@@ -419,6 +548,18 @@ __device__ __forceinline__ void riemann(int kind, const Q5& L, const Q5& R, doub
     flux_hlle(L, R, nx, ny, nz, area, g, us_n, eta, F);
   else
     flux_hllc(L, R, nx, ny, nz, area, g, us_n, eta, F);
+}
+
+// the face flux of the mesh kernels: eta == 1, fixed grid
+__device__ __forceinline__ void riemann1(int kind, const Q5& L, const Q5& R, double nx,
+                                         double ny, double nz, double area, const Gas& g,
+                                         double F[5]) {
+  if (kind == 1)
+    flux_roe1(L, R, nx, ny, nz, area, g, F);
+  else if (kind == 2)
+    flux_hlle(L, R, nx, ny, nz, area, g, 0.0, 1.0, F);
+  else
+    flux_hllc(L, R, nx, ny, nz, area, g, 0.0, 1.0, F);
 }
 
 // Characteristic boundary states, cv_inflow / cv_outflow (bcTools.h:25-81).

@@ -357,10 +357,13 @@ __global__ void k_sa_gs(Geo G, const int32_t* __restrict__ cells, int64_t n,
 
 // X_next = max(X + min(1, urelax X / (|dq| + 1e-15)) dq, 1e-15)
 // (solverScalarTransport.loci:397-405)
+// guard (may be null): the mean flow's norms of this step; NaN norms leave
+// nu~ unchanged, as the mean-flow update does
 __global__ void k_sa_update(int64_t nc, double urelax, const double* __restrict__ dq,
-                            double* __restrict__ nut) {
+                            double* __restrict__ nut, const double* __restrict__ guard) {
   const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (c >= nc) return;
+  if (guard && (isnan(guard[0]) || isnan(guard[1]) || isnan(guard[2]))) return;
   double tscale = 1.0;
   tscale = fmin(tscale, urelax * nut[c] / (fabs(dq[c]) + 1e-15));
   const double xn = nut[c] + tscale * dq[c];
@@ -446,10 +449,10 @@ int sa_launch_solve(fpsi_ctx* x) {
   return FPSI_OK;
 }
 
-int sa_launch_update(fpsi_ctx* x) {
+int sa_launch_update(fpsi_ctx* x, const double* guard) {
   prof_begin(x, "sa_update");
   sa::k_sa_update<<<nblk(x->H.nc, 256), 256, 0, x->stream>>>(x->H.nc, x->P.urelax, x->d_sa_x,
-                                                             x->d_nut);
+                                                             x->d_nut, guard);
   prof_end(x);
   FPSI_CUDA_TRY(cudaGetLastError());
   return FPSI_OK;

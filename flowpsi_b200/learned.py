@@ -3,9 +3,11 @@
 No counterpart in the reference; the hook is the relaxation's starting
 iterate (linearSolverSGS.loci:57-69).  The network, its training and its
 inference run in the library's CUDA kernels (flowpsi_b200/csrc/gnn.cu); this
-module drives them: snapshot generation from the solver itself, training,
-and the start used inside a Newton step with the reference's Jacobi start
-as the fallback and a rejection of steps whose FP64 residual does not drop.
+module drives them: snapshot generation from the solver itself and
+training.  Inside a Newton step the start is used through
+FlowPsi.newton_step_ex(start="learned", model=...), which runs in the
+library (fpsi_newton_step_ex): a step that does not lower the FP64 density
+residual is undone and redone from the reference's Jacobi start D^-1 B.
 """
 from __future__ import annotations
 
@@ -122,6 +124,28 @@ def make_snapshots(model: LearnedStart, case, steps: int, rtol: float = 1e-10,
         s.update()
     s.close()
     return hist
+
+
+def train_on_case(make_case, seeds, steps_per_seed: int, train_steps: int,
+                  batch: int = 65536, rtol: float = 1e-8, lr: float = 1e-3,
+                  model_seed: int = 0) -> tuple[LearnedStart, dict]:
+    """A model trained on (system, converged dq) snapshots of the first
+    steps_per_seed implicit steps of make_case(seed) for every seed (FP64
+    systems, dq swept to rtol), then train_steps Adam steps.  Returns the
+    model and a summary (snapshots, final loss, seconds)."""
+    import time
+
+    m = LearnedStart(seed=model_seed)
+    t0 = time.perf_counter()
+    for sd in seeds:
+        make_snapshots(m, make_case(sd), steps_per_seed, rtol=rtol)
+    t1 = time.perf_counter()
+    losses = m.train(train_steps, batch=batch, seed=model_seed, lr=lr)
+    t2 = time.perf_counter()
+    return m, {"snapshots": m.n_snapshots, "train_steps": train_steps, "batch": batch,
+               "loss_first": float(losses[0]) if len(losses) else None,
+               "loss_last": float(np.mean(losses[-50:])) if len(losses) else None,
+               "snapshot_s": t1 - t0, "train_s": t2 - t1}
 
 
 def sweeps_to_tolerance(solver: FlowPsi, start: str, rtol: float = 1e-3,

@@ -369,18 +369,58 @@ class FlowPsi:
         d["min_alpha"] = si.min_alpha
         return d
 
+    def newton_step_ex(self, start: str = "jacobi", model=None, reject: bool = True,
+                       lin_rtol: float = 0.0, max_sweeps: int = 200,
+                       check_every: int = 2) -> dict:
+        """One steady step (fpsi_newton_step_ex) from a chosen starting
+        iterate: 'jacobi' (the reference's D^-1 B, linearSolverSGS.loci:57-69),
+        'zero' or 'learned' (model: a learned.LearnedStart).  With reject, a
+        step that did not start from D^-1 B and does not lower the FP64
+        density residual is undone and redone from D^-1 B.  lin_rtol > 0
+        sweeps to ||B - A x|| <= lin_rtol ||B|| instead of
+        gauss_seidel_iter sweeps.  Returns the starting norms, the norms of
+        the new state ('after'), the sweeps, the start kept and whether the
+        first attempt was rejected."""
+        o = N.StepOpts()
+        o.start = N.START[start]
+        o.reject = 1 if reject else 0
+        o.lin_rtol, o.max_sweeps, o.check_every = lin_rtol, max_sweeps, check_every
+        si = N.StepInfo()
+        h = None if model is None else model._h
+        N.check(N.lib().fpsi_newton_step_ex(self._ctx, h, C.byref(o), C.byref(si)),
+                "fpsi_newton_step_ex")
+        d = si.resid.as_dict()
+        d.update(min_alpha=si.min_alpha, after=si.resid_after.as_dict(), sweeps=si.ls.iterations,
+                 lin_resid0=si.ls.resid0, lin_resid=si.ls.resid,
+                 start={v: k for k, v in N.START.items()}[si.start_used],
+                 rejected=bool(si.rejected))
+        return d
+
     def run(self, nsteps: int) -> list[dict]:
+        """nsteps implicit steps on the device.  A NaN residual stops the run
+        at that step (solverResidual.loci:203-208) and raises FpsiError with
+        the norm history so far as its ``history``."""
         arr = (N.Resid * max(nsteps, 1))()
-        N.check(N.lib().fpsi_run(self._ctx, nsteps, arr), "fpsi_run")
-        return [arr[i].as_dict() for i in range(nsteps)]
+        rc = N.lib().fpsi_run(self._ctx, nsteps, arr)
+        hist = [arr[i].as_dict() for i in range(nsteps)]
+        if rc != N.FPSI_OK:
+            e = N.FpsiError(rc, "fpsi_run")
+            e.history = hist
+            raise e
+        return hist
 
     def run_timed(self, nsteps: int):
         """(norm history, device milliseconds) of nsteps steps, timed with
         CUDA events on the library's stream"""
         arr = (N.Resid * max(nsteps, 1))()
         ms = C.c_double()
-        N.check(N.lib().fpsi_run_timed(self._ctx, nsteps, arr, C.byref(ms)), "fpsi_run_timed")
-        return [arr[i].as_dict() for i in range(nsteps)], ms.value
+        rc = N.lib().fpsi_run_timed(self._ctx, nsteps, arr, C.byref(ms))
+        hist = [arr[i].as_dict() for i in range(nsteps)]
+        if rc != N.FPSI_OK:
+            e = N.FpsiError(rc, "fpsi_run_timed")
+            e.history = hist
+            raise e
+        return hist, ms.value
 
     def kernel_times(self, nsteps: int = 1) -> dict:
         """{kernel: (total ms, launches)} over nsteps steps"""

@@ -153,9 +153,14 @@ typedef struct fpsi_stepinfo {
   fpsi_lsinfo ls;
   double min_alpha;            /* smallest Newton clip factor applied */
   double dtau_min, dtau_max;
+  /* fpsi_newton_step_ex only: */
+  fpsi_resid resid_after;      /* norms of the residual of the new state */
+  int32_t start_used;          /* fpsi_start_kind the accepted update started from */
+  int32_t rejected;            /* 1: the first attempt's update was rejected */
 } fpsi_stepinfo;
 
 typedef struct fpsi_ctx fpsi_ctx;
+typedef struct fpsi_gnn fpsi_gnn;   /* learned starting iterate, below */
 
 /* ---- parameters / errors -------------------------------------------------- */
 void        fpsi_default_params(fpsi_params* p);
@@ -167,8 +172,10 @@ int         fpsi_device_available(void);
  * kind 0: nx*ny*nz hex box [0,Lx]x[0,Ly]x[0,Lz], boundary condition of the six
  *         sides bc_side[0..5] = (xmin, xmax, ymin, ymax, zmin, zmax); an entry
  *         of -1 makes that direction periodic (both sides).
- * kind 1: nx*ny*nz hexes each split into 6 Kuhn tetrahedra on the periodic
- *         box [0,Lx]x[0,Ly]x[0,Lz]; nodes jittered by U(-jitter,+jitter)*h.
+ * kind 1: nx*ny*nz hexes each split into 6 Kuhn tetrahedra on the box
+ *         [0,Lx]x[0,Ly]x[0,Lz], sides periodic (-1) or bounded as kind 0;
+ *         nodes jittered by U(-jitter,+jitter)*h (not normal to a bounded
+ *         side, so the sides stay plane).
  * kind 2: boundary-layer hex block: y spacing dy0*growth^j.
  * kind 3: the kind-0 box with each hex split into two triangular prisms
  *         across the diagonal of its z-faces (cells 2c and 2c+1 of hex c):
@@ -267,9 +274,47 @@ int fpsi_linear_residual(fpsi_ctx* ctx, double* norm_b, double* norm_r);
 /* clipped Newton update with the device dq (solverNewton.loci:62-78) */
 int fpsi_update(fpsi_ctx* ctx, double* min_alpha);
 
-/* one steady implicit step: residual -> dtau -> assemble -> solve -> update */
+/* one steady implicit step: residual -> dtau -> assemble -> solve -> update.
+ * NaN residual norms return FPSI_E_NAN and leave the state unchanged. */
 int fpsi_newton_step(fpsi_ctx* ctx, fpsi_stepinfo* info);
-/* nsteps steps without host round trips; norms[k] of each step (may be NULL) */
+/* Starting iterate of the relaxation and the rule that keeps a step.
+ *   start       FPSI_START_JACOBI: the reference's D^-1 B
+ *               (linearSolverSGS.loci:57-69); FPSI_START_ZERO; or
+ *               FPSI_START_LEARNED: the model's start (fpsi_gnn_predict).
+ *   reject      1: when the FP64 density residual (rtrms) of the new state is
+ *               not below the one the step started from, a step that did not
+ *               start from D^-1 B is undone and redone from D^-1 B, which is
+ *               kept whatever its residual (the reference's step).
+ *   lin_rtol    > 0: sweep until ||B - A x|| <= lin_rtol ||B||, measured every
+ *               check_every sweeps, at most max_sweeps; <= 0: exactly
+ *               gauss_seidel_iter sweeps. */
+enum fpsi_start_kind {
+  FPSI_START_JACOBI = 0,
+  FPSI_START_ZERO = 1,
+  FPSI_START_LEARNED = 2
+};
+typedef struct fpsi_step_opts {
+  int32_t start;               /* fpsi_start_kind */
+  int32_t reject;
+  double lin_rtol;
+  int32_t max_sweeps;
+  int32_t check_every;
+} fpsi_step_opts;
+/* one steady implicit step as fpsi_newton_step, with a chosen starting
+ * iterate, an optional linear tolerance and the rejection rule above.  The
+ * step ends with the residual of the new state (info->resid_after), which
+ * the next call reuses as its starting residual.  model may be NULL unless
+ * start is FPSI_START_LEARNED.  Multi-colour SGS without the SA model; the
+ * learned start and a linear tolerance need the diagonal blocks kept
+ * (fpsi_keep_blocks). */
+int fpsi_newton_step_ex(fpsi_ctx* ctx, fpsi_gnn* model, const fpsi_step_opts* opts,
+                        fpsi_stepinfo* info);
+/* nsteps steps without host round trips; norms[k] of each step (may be NULL).
+ * A step whose residual norms are NaN ends the run there, as
+ * solverResidual.loci:203-208 aborts: the state stays the one that step
+ * started from, norms[] is filled up to that step and NaN after it, and
+ * the call returns FPSI_E_NAN (fpsi_last_error names the step).  The norm
+ * history lives in the context (no allocation per call up to 4096 steps). */
 int fpsi_run(fpsi_ctx* ctx, int32_t nsteps, fpsi_resid* norms);
 /* fpsi_run timed on the device: CUDA events recorded on the library's
  * stream around the nsteps steps; device_ms receives the elapsed time. */
@@ -293,7 +338,6 @@ int fpsi_kernel_times(fpsi_ctx* ctx, int32_t nsteps, int32_t cap, char* names, d
  * context.  Training pairs come from the solver: fpsi_gnn_add_snapshot takes
  * the features of an assembled system, its cell graph and its converged dq
  * (caller order).  The model runs on its own stream. */
-typedef struct fpsi_gnn fpsi_gnn;
 int fpsi_gnn_create(fpsi_gnn** out, uint64_t seed);
 int fpsi_gnn_destroy(fpsi_gnn* m);
 int64_t fpsi_gnn_num_params(const fpsi_gnn* m);
@@ -356,9 +400,12 @@ int fpsi_sa_update(fpsi_ctx* ctx);
  * cell of etmax, mtmax).  stream is a cudaStream_t or NULL.
  * Allocates nothing: the block partials live in a static 1 MiB __device__
  * array that every GPU loading the library keeps until exit, so nc is
- * limited to 16,777,216 cells (larger sizes return FPSI_E_INVALID).  The
- * first call on a device looks the array's address up (no allocation);
- * make that first call before any stream capture.  Every call overwrites
+ * limited to 16,777,216 cells (larger sizes return FPSI_E_INVALID).  Each
+ * call outside a stream capture looks the array's address up on the current
+ * device (no allocation), which also follows a module reloaded after
+ * cudaDeviceReset; a call inside a capture reuses the address found last,
+ * so make the first call on a device before any stream capture (else
+ * FPSI_E_STATE).  Every call overwrites
  * the partials it reads, so nothing must start at zero; calls that overlap
  * on the GPU share the array and race. */
 int fpsi_residual_norms_noalloc(const double* d_src, const double* d_vol, int64_t nc,

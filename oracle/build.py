@@ -21,7 +21,14 @@ HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
 REF_DIR = HERE / "_ref"
 REF_LIB = REF_DIR / "libfpsiref.so"
-REFERENCE = Path(os.environ.get("FLOWPSI_REFERENCE", "/root/reference"))
+
+
+def reference_tree(path: str | os.PathLike | None = None) -> Path | None:
+    """The flowPsi source tree to cut the face functions from: the caller's
+    path, else the FLOWPSI_REFERENCE environment variable, else none."""
+    p = path if path is not None else os.environ.get("FLOWPSI_REFERENCE")
+    return Path(p) if p else None
+
 
 # (file, first line, last line, what) -- ranges of plain C++ in the reference
 REF_RANGES = [
@@ -52,10 +59,15 @@ def build_oracle(force: bool = False) -> Path:
     return LIB
 
 
-def build_ref(force: bool = False) -> Path | None:
-    """Compile the reference face functions; None when the tree is absent."""
+def build_ref(force: bool = False, reference: str | os.PathLike | None = None) -> Path | None:
+    """Compile the reference face functions from the flowPsi tree at
+    `reference` (or FLOWPSI_REFERENCE); without a tree the library built
+    before is kept, else None."""
     shim = HERE / "ref_shim.h"
     glue = HERE / "ref_glue.inc"
+    REFERENCE = reference_tree(reference)
+    if REFERENCE is None:
+        return REF_LIB if REF_LIB.exists() else None
     srcs = [REFERENCE / f for f, *_ in REF_RANGES]
     if not all(s.exists() for s in srcs):
         return REF_LIB if REF_LIB.exists() else None
@@ -81,11 +93,13 @@ def build_ref(force: bool = False) -> Path | None:
     return REF_LIB
 
 
-def build(force: bool = False) -> None:
+def build(force: bool = False, reference: str | os.PathLike | None = None) -> None:
     build_oracle(force)
-    build_ref(force)
+    build_ref(force, reference)
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv)
+    # python oracle/build.py [--force] [path of the flowPsi source tree]
+    args = [a for a in sys.argv[1:] if a != "--force"]
+    build(force="--force" in sys.argv, reference=args[0] if args else None)
     print(LIB, REF_LIB if REF_LIB.exists() else "(no reference tree)")

@@ -85,3 +85,33 @@ def test_no_cpu_fallback_without_device():
     rc = N.lib().fpsi_face_flux(1, 1, N.dptr(qL), N.dptr(qL), N.dptr(np.ones(3)),
                                 N.dptr(np.ones(1)), 0.0, 287.0, 1.4, 0.0, 1.0, N.dptr(np.empty(5)))
     assert rc == -2
+
+
+def test_bounded_kuhn_mesh_closes():
+    """Kuhn tets with bounded sides: face counts, and the oracle's geometry
+    fills the box and closes every cell (sum of outward area vectors 0)"""
+    from oracle import Oracle
+
+    m = GeneratedMesh("kuhn", n=(3, 4, 5), L=(1.0, 2.0, 3.0), jitter=0.1, seed=2,
+                      bc_side=(0,) * 6, bcs=[bc("farfield")])
+    a = m.arrays()
+    assert a.ncells == 6 * 60
+    nb = int((a.cr < 0).sum())
+    assert nb == 2 * 2 * (3 * 4 + 4 * 5 + 3 * 5)  # two triangles per boundary quad
+    assert 4 * a.ncells == 2 * (a.nfaces - nb) + nb
+    assert np.all(a.cl < np.where(a.cr >= 0, a.cr, a.ncells))
+    o = Oracle(m, default_params(solver="sgs"))
+    g = o.geometry()
+    assert abs(g["vol"].sum() - 6.0) < 1e-12 and g["vol"].min() > 0
+    s = np.zeros((a.ncells, 3))
+    np.add.at(s, a.cl, g["area_vec"])
+    inner = a.cr >= 0
+    np.add.at(s, a.cr[inner], -g["area_vec"][inner])
+    assert np.abs(s).max() < 1e-13
+    # boundary faces lie on the sides and point out of the box
+    fc, an = g["facecenter"][~inner], g["area_vec"][~inner]
+    L = np.array([1.0, 2.0, 3.0])
+    on_side = (np.abs(fc) < 1e-12) | (np.abs(fc - L) < 1e-12)
+    assert np.all(on_side.sum(1) == 1)
+    out = np.where(np.abs(fc) < 1e-12, -1.0, 1.0)
+    assert np.all((an * out * on_side).sum(1) > 0)

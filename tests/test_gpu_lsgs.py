@@ -110,3 +110,43 @@ def test_lsgs_newton_step_matches_oracle(need_gpu):
         o.update()
     for a, b in zip(g.get_state(), o.get_state()):
         assert np.abs(a - b).max() <= 1e-9 * np.abs(b).max()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_single_cell_lines_match_oracle(need_gpu, prec):
+    """The reference's own line set.  Its connection pass
+    (linearSolverLSGS.loci:642-664) runs over equation numbers after unique()
+    has removed every duplicate (:626-631), so it never links two cells and
+    every line is one cell: LSGS is then the relaxed block iteration over
+    single cells.  fpsi_set_lines expresses that set; the GPU result must
+    match the oracle's restatement on the same lines and colours."""
+    case = _bl(prec)
+    g = FlowPsi(case.mesh, case.params)
+    o = Oracle(case.mesh, case.params)
+    g.set_lines([np.array([c], np.int32) for c in range(g.ncells)])
+    T, p, u = case.initial_state(o.geometry()["cellcenter"])
+    g.set_state(T, p, u)
+    o.set_state(T, p, u)
+    lines, colours = g.line_list()
+    assert len(lines) == g.ncells and all(len(l) == 1 for l in lines)
+    g.residual()
+    o.residual()
+    g.assemble()
+    o.assemble()
+    dg, ig = g.linear_solve(info=True)
+    do, io = o.lsgs_solve(lines, colours)
+    if prec == "fp64":
+        assert ig["iterations"] == io["iterations"]
+        for k in range(5):
+            assert np.abs(dg[:, k] - do[:, k]).max() <= 1e-8 * np.abs(do[:, k]).max(), k
+    else:
+        c64 = _bl("fp64")
+        o64 = Oracle(c64.mesh, c64.params)
+        o64.set_state(*o.get_state())
+        o64.residual()
+        o64.assemble()
+        d64, _ = o64.lsgs_solve(lines, colours)
+        for k in range(5):
+            e_orc = np.abs(do[:, k] - d64[:, k]).max()
+            e_gpu = np.abs(dg[:, k] - d64[:, k]).max()
+            assert e_gpu <= 2.0 * e_orc + 1e-6 * np.abs(d64[:, k]).max(), k
