@@ -23,7 +23,7 @@ LIMITER = {"venkatakrishnan": 0, "barth": 1, "none": 2, "zero": 3}
 SOLVER = {"sgs": 0, "lsgs": 1}
 PRECISION = {"fp64": 0, "ref": 1, "mixed": 2}
 BC = {"farfield": 1, "supersonicInflow": 2, "supersonicOutflow": 3, "extrapolate": 4,
-      "reflecting": 5, "viscousWall": 6}
+      "reflecting": 5, "viscousWall": 6, "outflow": 7, "outflowMean": 8}
 
 
 class Params(C.Structure):
@@ -75,7 +75,9 @@ class Resid(C.Structure):
     ]
 
     def as_dict(self) -> dict:
-        return {k: getattr(self, k) for k in ("rtrms", "etrms", "mtrms", "rtmax", "etmax", "mtmax")}
+        d = {k: getattr(self, k) for k in ("rtrms", "etrms", "mtrms", "rtmax", "etmax", "mtmax")}
+        d["bcErrorCode"] = int(self.bcErrorCode)
+        return d
 
 
 class LsInfo(C.Structure):

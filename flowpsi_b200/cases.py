@@ -15,6 +15,8 @@ inputs for the same seed.
   taylorGreenIC.loci:26-31: constant density, pressure from the analytic
   field); Roe + MUSCL + Venkatakrishnan, 8 multi-colour SGS sweeps (128^3:
   12.58M cells, 25.2M faces).
+* ``outflow_duct``: hex duct from a farfield inflow to an outflow held at
+  a back pressure ('p' or 'pMean'), periodic sides.
 * ``farfield_tets``: the split-tet grid of ``taylor_green_tets`` with
   farfield sides and the freestream-plus-noise start of ``farfield_cube``:
   the steady case on which the 1e-8 residual drop is timed.
@@ -94,6 +96,38 @@ def farfield_cube(n: int = 32, seed: int = 0, sweeps: int = 5, flux: str = "roe"
         return T, p, u
 
     return Case(f"farfield_cube_{n}", mesh, params, 20, init)
+
+
+def outflow_duct(n: int = 16, seed: int = 0, sweeps: int = 5, mean: bool = False,
+                 back_pressure: float = 1.02e5, flux: str = "roe",
+                 limiter: str = "venkatakrishnan", precision: str = "ref") -> Case:
+    """Subsonic duct: n^3 hex cube [0,1]^3, farfield inflow at x-min (M=0.5
+    along +x, p=1e5 Pa, T=300 K), outflow at x-max held at a back pressure
+    (bcOutflow.loci:174-273; with mean=True the pMean form, where the
+    area-weighted mean of the boundary pressure is held instead), periodic
+    in y and z.  Initial state the freestream with 1% noise (farfield_cube)."""
+    T0, p0, M = 300.0, 1e5, 0.5
+    U0 = M * math.sqrt(GAMMA * RTILDE * T0)
+    ff = bc("farfield", T=T0, pg=p0, u=(U0, 0.0, 0.0))
+    out = bc("outflowMean" if mean else "outflow", T=T0, pg=back_pressure)
+    mesh = GeneratedMesh("hex", n=(n, n, n), L=(1.0, 1.0, 1.0), bc_side=(0, 1, -1, -1, -1, -1),
+                         bcs=[ff, out])
+    params = default_params(flux=flux, limiter=limiter, Kl=1.0, solver="sgs",
+                            gauss_seidel_iter=sweeps, cflmax=50.0, precision=precision)
+
+    def init(cc):
+        nc = cc.shape[0]
+        rho0 = p0 / (RTILDE * T0)
+        rho = rho0 * (1.0 + 0.01 * normal(seed, 0, nc))
+        p = p0 * (1.0 + 0.01 * normal(seed, 1, nc))
+        u = np.empty((nc, 3))
+        u[:, 0] = U0 + 0.01 * U0 * normal(seed, 2, nc)
+        u[:, 1] = 0.01 * U0 * normal(seed, 3, nc)
+        u[:, 2] = 0.01 * U0 * normal(seed, 4, nc)
+        T = p / (RTILDE * rho)
+        return T, p, u
+
+    return Case(f"outflow_duct_{n}", mesh, params, 100, init)
 
 
 def taylor_green_tets(n: int = 128, seed: int = 0, sweeps: int = 8, jitter: float = 0.1,

@@ -188,16 +188,16 @@ int alloc_lsgs(fpsi_ctx* x) {
 int ensure_hist(fpsi_ctx* x, int64_t n) {
   if (n <= x->hist_cap) return FPSI_OK;
   if (x->d_hist) {
-    x->device_bytes -= x->hist_cap * 8 * int64_t(sizeof(double));
+    x->device_bytes -= x->hist_cap * fpsi::NREC * int64_t(sizeof(double));
     cudaFree(x->d_hist);
     x->d_hist = nullptr;
   }
   if (x->h_hist) cudaFreeHost(x->h_hist);
   x->h_hist = nullptr;
   x->hist_cap = 0;
-  int rc = dalloc(x, &x->d_hist, size_t(n) * 8);
+  int rc = dalloc(x, &x->d_hist, size_t(n) * fpsi::NREC);
   if (rc) return rc;
-  if (cudaMallocHost((void**)&x->h_hist, size_t(n) * 8 * sizeof(double)) != cudaSuccess) {
+  if (cudaMallocHost((void**)&x->h_hist, size_t(n) * fpsi::NREC * sizeof(double)) != cudaSuccess) {
     fpsi::set_error("cudaMallocHost of the residual history failed");
     return FPSI_E_NOMEM;
   }
@@ -251,6 +251,7 @@ void fill_norms(const fpsi_ctx* x, const double* r, fpsi_resid* n) {
   n->rtmax = r[3];
   n->etmax = r[5];
   n->mtmax = r[7];
+  n->bcErrorCode = uint64_t(r[8]);
   const int64_t cr = int64_t(r[4]), ce = int64_t(r[6]);
   if (cr >= 0 && cr < x->H.nc)
     for (int d = 0; d < 3; ++d) n->ccmaxr_center[d] = x->H.cc[3 * cr + d];
@@ -332,7 +333,7 @@ int fpsi_destroy(fpsi_ctx* x) {
   free_lsgs(x);
   free_sa(x);
   void* ps[] = {x->d_cl, x->d_cr, x->d_n, x->d_area, x->d_rL, x->d_rR, x->d_vol, x->d_cc,
-                x->d_Minv, x->d_cf_off, x->d_cf, x->d_colour_cells, x->d_bcs, x->d_q,
+                x->d_Minv, x->d_cf_off, x->d_cf, x->d_colour_cells, x->d_bcs, x->d_bcmean, x->d_q,
                 x->d_qb, x->d_grad, x->d_F, x->d_src, x->d_dtau, x->d_tmu,
                 x->d_part, x->d_resid, x->d_amin, x->d_err, x->d_perm, x->d_stage, x->d_ci, x->d_ccol,
                 x->d_nbr, x->d_colinfo, x->d_cnb_off, x->d_cnb, x->d_xprev, x->d_qsave};
@@ -370,7 +371,7 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
   }
   x->bcs.assign(mesh->bcs, mesh->bcs + mesh->nbc);
   for (const fpsi_bc& b : x->bcs)
-    if (b.kind < FPSI_BC_FARFIELD || b.kind > FPSI_BC_VISCOUS_WALL) {
+    if (b.kind < FPSI_BC_FARFIELD || b.kind > FPSI_BC_OUTFLOW_MEAN) {
       fpsi::set_error("boundary condition kind %d is not on the device path", b.kind);
       delete x;
       return FPSI_E_UNSUPPORTED;
@@ -420,6 +421,8 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
   }
   TRY(dalloc(x, &x->d_stage, nc * 5));
   TRY(upload(x, &x->d_bcs, x->bcs));
+  TRY(dalloc(x, &x->d_bcmean, std::max<size_t>(x->bcs.size(), 1) * 2));
+  for (const fpsi_bc& b : x->bcs) x->any_pmean = x->any_pmean || b.kind == FPSI_BC_OUTFLOW_MEAN;
   TRY(dalloc(x, &x->d_q, nc * 5));
   TRY(dalloc(x, &x->d_qb, std::max<int64_t>(H.nbf, 1) * 5));
   TRY(dalloc(x, &x->d_grad, nc * fpsi::GPREC));
@@ -433,10 +436,10 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
   }
   x->nblk_norm = int((nc + 255) / 256);
   TRY(dalloc(x, &x->d_part, size_t(x->nblk_norm) * 8));
-  TRY(dalloc(x, &x->d_resid, 16));
+  TRY(dalloc(x, &x->d_resid, 32));
   TRY(dalloc(x, &x->d_amin, size_t(x->nblk_norm)));
   TRY(dalloc(x, &x->d_err, 4));
-  if (cudaMallocHost((void**)&x->h_resid, 16 * sizeof(double)) != cudaSuccess) {
+  if (cudaMallocHost((void**)&x->h_resid, 32 * sizeof(double)) != cudaSuccess) {
     fpsi_destroy(x);
     return FPSI_E_NOMEM;
   }
@@ -690,7 +693,7 @@ int fpsi_residual(fpsi_ctx* x, double* src, fpsi_resid* norms) {
   if (fpsi::sa_active(x) && (rc = fpsi::sa_launch_tmu(x))) return rc;
   rc = fpsi::launch_residual(x, x->d_resid);
   if (rc) return rc;
-  FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid, x->d_resid, 8 * sizeof(double),
+  FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid, x->d_resid, fpsi::NREC * sizeof(double),
                                 cudaMemcpyDeviceToHost, x->stream));
   std::vector<double> s;
   if (src) {
@@ -944,13 +947,13 @@ int fpsi_linear_sweeps(fpsi_ctx* x, int32_t nsweeps) {
 int fpsi_linear_residual(fpsi_ctx* x, double* norm_b, double* norm_r) {
   if (!x) return FPSI_E_INVALID;
   if (!x->have_asm || !x->d_D) return FPSI_E_STATE;
-  int rc = fpsi::launch_linres(x, x->d_resid + 8);
+  int rc = fpsi::launch_linres(x, x->d_resid + 16);
   if (rc) return rc;
-  FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid + 8, x->d_resid + 8, 2 * sizeof(double),
+  FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid + 16, x->d_resid + 16, 2 * sizeof(double),
                                 cudaMemcpyDeviceToHost, x->stream));
   if ((rc = sync(x))) return rc;
-  if (norm_b) *norm_b = x->h_resid[8];
-  if (norm_r) *norm_r = x->h_resid[9];
+  if (norm_b) *norm_b = x->h_resid[16];
+  if (norm_r) *norm_r = x->h_resid[17];
   return FPSI_OK;
 }
 
@@ -984,7 +987,7 @@ int fpsi_newton_step(fpsi_ctx* x, fpsi_stepinfo* info) {
   }
   if ((rc = fpsi::launch_update(x, x->d_resid))) return rc;
   if (sa && (rc = fpsi::sa_launch_update(x, x->d_resid))) return rc;
-  FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid, x->d_resid, 8 * sizeof(double),
+  FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid, x->d_resid, fpsi::NREC * sizeof(double),
                                 cudaMemcpyDeviceToHost, x->stream));
   std::vector<double> a(x->nblk_norm);
   FPSI_CUDA_TRY(cudaMemcpyAsync(a.data(), x->d_amin, a.size() * sizeof(double),
@@ -1024,11 +1027,11 @@ int ex_sweeps(fpsi_ctx* x, const fpsi_step_opts& o, fpsi_lsinfo* info) {
   const int every = std::max(1, o.check_every);
   int done = 0;
   for (bool first = true;; first = false) {
-    if ((rc = fpsi::launch_linres(x, x->d_resid + 8))) return rc;
-    FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid + 8, x->d_resid + 8, 2 * sizeof(double),
+    if ((rc = fpsi::launch_linres(x, x->d_resid + 16))) return rc;
+    FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid + 16, x->d_resid + 16, 2 * sizeof(double),
                                   cudaMemcpyDeviceToHost, x->stream));
     if ((rc = sync(x))) return rc;
-    const double nb = x->h_resid[8], nr = x->h_resid[9];
+    const double nb = x->h_resid[16], nr = x->h_resid[17];
     if (first) info->resid0 = nr;
     info->resid = nr;
     if (!(nr > o.lin_rtol * nb) || done >= o.max_sweeps) break;
@@ -1044,7 +1047,7 @@ int ex_sweeps(fpsi_ctx* x, const fpsi_step_opts& o, fpsi_lsinfo* info) {
 int ex_residual(fpsi_ctx* x) {
   int rc = fpsi::launch_residual(x, x->d_resid);
   if (rc) return rc;
-  FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid, x->d_resid, 8 * sizeof(double),
+  FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_resid, x->d_resid, fpsi::NREC * sizeof(double),
                                 cudaMemcpyDeviceToHost, x->stream));
   if ((rc = sync(x))) return rc;
   x->have_resid = true;
@@ -1102,7 +1105,7 @@ int fpsi_newton_step_ex(fpsi_ctx* x, fpsi_gnn* model, const fpsi_step_opts* opts
   std::memset(&si, 0, sizeof(si));
   // the residual of the current state: kept from the previous call, or new
   if (!x->have_resid && (rc = ex_residual(x))) return rc;
-  double r_start[8];
+  double r_start[fpsi::NREC];
   std::memcpy(r_start, x->h_resid, sizeof(r_start));
   fill_norms(x, r_start, &si.resid);
   if (has_nan(r_start)) {
@@ -1145,22 +1148,22 @@ static int run_steps(fpsi_ctx* x, int32_t nsteps, int32_t* launched) {
   int rc = FPSI_OK;
   const bool sa = fpsi::sa_active(x);
   volatile double* hh = x->h_hist;
-  for (int32_t s = 0; s < nsteps; ++s) hh[8 * int64_t(s)] = -1.0;
+  for (int32_t s = 0; s < nsteps; ++s) hh[fpsi::NREC * int64_t(s)] = -1.0;
   int32_t seen = 0, s = 0;
   for (; s < nsteps && !rc; ++s) {
     bool nan = false;
     while (seen < s && !nan) {
-      const double r = hh[8 * int64_t(seen)];
+      const double r = hh[fpsi::NREC * int64_t(seen)];
       if (r == -1.0) break;  // not landed yet
-      nan = r != r || hh[8 * int64_t(seen) + 1] != hh[8 * int64_t(seen) + 1] ||
-            hh[8 * int64_t(seen) + 2] != hh[8 * int64_t(seen) + 2];
+      const int64_t o = fpsi::NREC * int64_t(seen);
+      nan = r != r || hh[o + 1] != hh[o + 1] || hh[o + 2] != hh[o + 2];
       ++seen;
     }
     if (nan) break;
-    double* slot = x->d_hist + 8 * int64_t(s);
+    double* slot = x->d_hist + fpsi::NREC * int64_t(s);
     if (sa) rc = fpsi::sa_launch_tmu(x);
     if (!rc) rc = fpsi::launch_residual(x, slot);
-    if (!rc && cudaMemcpyAsync(x->h_hist + 8 * int64_t(s), slot, 8 * sizeof(double),
+    if (!rc && cudaMemcpyAsync(x->h_hist + fpsi::NREC * int64_t(s), slot, fpsi::NREC * sizeof(double),
                                cudaMemcpyDeviceToHost, x->stream) != cudaSuccess)
       rc = FPSI_E_CUDA;
     if (!rc && sa) rc = fpsi::sa_launch_residual(x);
@@ -1184,16 +1187,16 @@ static int run_steps(fpsi_ctx* x, int32_t nsteps, int32_t* launched) {
 static int finish_run(fpsi_ctx* x, int32_t nsteps, int32_t launched, fpsi_resid* norms) {
   int32_t first_nan = -1;
   for (int32_t s = 0; s < launched && first_nan < 0; ++s)
-    if (has_nan(&x->h_hist[8 * int64_t(s)])) first_nan = s;
+    if (has_nan(&x->h_hist[fpsi::NREC * int64_t(s)])) first_nan = s;
   if (launched < nsteps && first_nan < 0) {
     fpsi::set_error("the run stopped after %d of %d steps without a NaN residual", launched, nsteps);
     return FPSI_E_STATE;
   }
   const int32_t last = first_nan < 0 ? nsteps : first_nan + 1;
   if (norms) {
-    for (int32_t s = 0; s < last; ++s) fill_norms(x, &x->h_hist[8 * int64_t(s)], &norms[s]);
+    for (int32_t s = 0; s < last; ++s) fill_norms(x, &x->h_hist[fpsi::NREC * int64_t(s)], &norms[s]);
     const double q = std::nan("");
-    const double nanrec[8] = {q, q, q, q, -1, q, -1, q};
+    const double nanrec[fpsi::NREC] = {q, q, q, q, -1, q, -1, q, 0, 0};
     for (int32_t s = last; s < nsteps; ++s) fill_norms(x, nanrec, &norms[s]);
   }
   if (first_nan >= 0) {

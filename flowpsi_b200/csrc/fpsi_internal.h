@@ -17,6 +17,10 @@ constexpr int FREC = 6;
 // d(T,u,v,w,pg)/dx, y, z) then the limiter (5); 160 B, ten aligned 16 B
 // accesses
 constexpr int GPREC = 20;
+// doubles per residual-norm record: rtrms, etrms, mtrms, rtmax, its cell,
+// etmax, its cell, mtmax, the boundary-condition error bits of that
+// residual (flowPsiIO.h:212-215), one spare
+constexpr int NREC = 10;
 
 void set_error(const char* fmt, ...);
 
@@ -123,6 +127,8 @@ struct fpsi_ctx {
   int32_t *d_cf_off = nullptr, *d_cf = nullptr;
   int32_t* d_colour_cells = nullptr;
   fpsi_bc* d_bcs = nullptr;
+  double* d_bcmean = nullptr;  // [nbc][2]: sum of A pg and of A over each condition's faces
+  bool any_pmean = false;      // a pMean outflow is present
   // state and residual
   double* d_q = nullptr;       // [nc][5]  T,u,v,w,pg
   double* d_qb = nullptr;      // [nbf][5] boundary face states

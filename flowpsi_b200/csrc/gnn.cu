@@ -104,15 +104,36 @@ struct fpsi_gnn {
   cudaStream_t stream = nullptr;
   int nsm = 148;                  // multiprocessors of the device (grid of the layer GEMM)
   int32_t* d_err = nullptr;       // bit 1: a tensor-core wait gave up
+  float* d_fac = nullptr;         // inference: scales rs|xs (10) then the 40 feature factors
 };
 
 namespace {
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+// GELU in the tanh form of Hendrycks and Gimpel ("Gaussian Error Linear
+// Units", 2016):  0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))).  Since
+// 1 + tanh(u) = 2 / (1 + exp(-2u)) it is x / (1 + exp(-2u)): one base-2
+// exponential and one fast division on the special-function unit, against
+// the twenty-odd instructions of erff.  The tanh form differs from the erf
+// form by at most 4.8e-4 (at |x| = 2.7); the network is trained with it.
+constexpr float GELU_K = 0.7978845608028654f;  // sqrt(2/pi)
+constexpr float GELU_C = 0.044715f;
+// -2 sqrt(2/pi) log2(e): exp(-2u) = 2^(GELU_T x (1 + GELU_C x^2))
+constexpr float GELU_T = -2.0f * 0.7978845608028654f * 1.4426950408889634f;
+__device__ __forceinline__ float ex2_approx(float t) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(t));
+  return r;
+}
+__device__ __forceinline__ float gelu(float x) {
+  const float e = ex2_approx(GELU_T * x * fmaf(GELU_C, x * x, 1.0f));
+  return __fdividef(x, 1.0f + e);
+}
+// d/dx [x s(x)], s = 1 / (1 + exp(-2u)):  s + x s (1 - s) 2 sqrt(2/pi) (1 + 3 GELU_C x^2)
 __device__ __forceinline__ float gelu_grad(float x) {
-  const float cdf = 0.5f * (1.0f + erff(x * 0.70710678118654752f));
-  const float pdf = expf(-0.5f * x * x) * 0.39894228040143268f;
-  return cdf + x * pdf;
+  const float x2 = x * x;
+  const float e = ex2_approx(GELU_T * x * fmaf(GELU_C, x2, 1.0f));
+  const float sg = __fdividef(1.0f, 1.0f + e);
+  return sg + x * sg * (1.0f - sg) * (2.0f * GELU_K) * fmaf(3.0f * GELU_C, x2, 1.0f);
 }
 
 // a layer input as the tensor cores multiply it (FP32 features rounded to BF16)
@@ -751,8 +772,11 @@ inline unsigned nb_(int64_t n, int t) { return unsigned((n + t - 1) / t); }
 // m->d_y.  keep stores what the backward pass needs: neighbour means, FP32
 // pre-activations and every layer's activations.
 static_assert(NLAYER >= 2, "the head is fused into the last hidden layer");
-int forward(fpsi_gnn* m, const Graph& G, const float* feat, bool keep) {
-  cudaStream_t s = m->stream;
+// feat16 (BF16 [nc][40], inference): used instead of feat by the first
+// layer, which rounds its input to BF16 anyway, so the result is the same
+int forward(fpsi_gnn* m, const Graph& G, const float* feat, bool keep,
+            const __nv_bfloat16* feat16 = nullptr, cudaStream_t stream = nullptr) {
+  cudaStream_t s = stream ? stream : m->stream;
   const int64_t nc = G.nc;
   const int64_t ntiles = (nc + TC_ROWS - 1) / TC_ROWS;
   auto grid_for = [&](int per_sm) {
@@ -769,7 +793,10 @@ int forward(fpsi_gnn* m, const Graph& G, const float* feat, bool keep) {
     float* z = keep ? m->d_z[l] : nullptr;
     const bool last = l == NLAYER - 1;
     __nv_bfloat16* hout = (last && !keep) ? nullptr : m->d_h[l + 1];
-    if (l == 0)
+    if (l == 0 && feat16)
+      k_layer_tc<__nv_bfloat16, false><<<grid, TC_THREADS, smem, s>>>(nc, fin, feat16, G.off, G.nb, ws, wn, b,
+                                                                      wo, bo, agg, z, hout, nullptr, m->d_err);
+    else if (l == 0)
       k_layer_tc<float, false><<<grid0, TC_THREADS, smem, s>>>(nc, fin, feat, G.off, G.nb, ws, wn, b, wo, bo, agg,
                                                               z, hout, nullptr, m->d_err);
     else if (!last)
@@ -952,6 +979,7 @@ int fpsi_gnn_create(fpsi_gnn** out, uint64_t seed) {
   G(galloc(&m->d_g, np));
   G(galloc(&m->d_wb, np));
   G(galloc(&m->d_err, 1));
+  G(galloc(&m->d_fac, 64));
 #undef G
   if (!rc && cudaMemset(m->d_err, 0, sizeof(int32_t)) != cudaSuccess) rc = FPSI_E_CUDA;
   int dev = 0;
@@ -1010,7 +1038,7 @@ int fpsi_gnn_destroy(fpsi_gnn* m) {
   if (!m) return FPSI_OK;
   fpsi_gnn_clear_snapshots(m);
   free_activations(m);
-  void* ps[] = {m->d_w, m->d_m, m->d_v, m->d_g, m->d_wb, m->d_err};
+  void* ps[] = {m->d_w, m->d_m, m->d_v, m->d_g, m->d_wb, m->d_err, m->d_fac};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (m->stream) cudaStreamDestroy(m->stream);
@@ -1239,53 +1267,172 @@ int fpsi_gnn_train(fpsi_gnn* m, int32_t nsteps, int64_t batch, uint64_t seed, do
 }  // extern "C"
 
 namespace {
-// x0 = x_J + xs * d into ctx's colour-order iterate (the next linear solve
-// starts from it); x0_out (caller order) optional
+// ---- inference features in two passes, with no host round trip ----------
+// Per-block sums of squares of B (= float(src)) and x_J (= float of the
+// colour-order iterate), GT cells per block and the same tree as
+// k_rms_partial, so the partials are the ones the training features use.
 template <class TX>
-__global__ void k_apply_start(int64_t nc, const float* __restrict__ xj, const float* __restrict__ y,
-                              const float* __restrict__ scl, const int32_t* __restrict__ ci,
-                              TX* __restrict__ x, double* __restrict__ x0) {
+__global__ void k_feat_stats(int64_t nc, const double* __restrict__ src, const TX* __restrict__ x_ci,
+                             const int32_t* __restrict__ ci, double* __restrict__ part) {
+  const int64_t c = int64_t(blockIdx.x) * GT + threadIdx.x;
+  __shared__ double sh[10][GT];
+  const int64_t i = c < nc ? int64_t(ci[c]) : 0;
+  for (int k = 0; k < 5; ++k) {
+    const double b = c < nc ? double(float(src[5 * c + k])) : 0.0;
+    const double x = c < nc ? double(float(x_ci[5 * i + k])) : 0.0;
+    sh[k][threadIdx.x] = b * b;
+    sh[5 + k][threadIdx.x] = x * x;
+  }
+  __syncthreads();
+  for (int st = GT / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int k = 0; k < 10; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 10; ++k) part[10 * blockIdx.x + k] = sh[k][0];
+}
+
+// scales rs, xs (the blocks summed in order, as the host does for the
+// training features) and the 40 per-feature factors of k_features_norm
+__global__ void k_feat_scales(const double* __restrict__ part, int nblk, int64_t nc,
+                              float* __restrict__ fac) {
+  __shared__ float scl[10];
+  const int k = threadIdx.x;
+  if (k < 10) {
+    double sum = 0;
+    for (int b = 0; b < nblk; ++b) sum += part[10 * b + k];
+    scl[k] = float(sqrt(sum / double(nc)) + 1e-30);
+    fac[k] = scl[k];
+  }
+  __syncthreads();
+  if (k < NIN) {
+    const float* rs = scl;
+    const float* xs = scl + 5;
+    float f;
+    if (k < 5)
+      f = 1.0f / rs[k];
+    else if (k < 30)
+      f = xs[(k - 5) % 5] / rs[(k - 5) / 5];
+    else if (k < 35)
+      f = 1.0f / xs[k - 30];
+    else
+      f = 1.0f / xs[k - 35];
+    fac[10 + k] = f;
+  }
+}
+
+// the 40 normalised features of a cell straight from the system, rounded
+// to BF16 (B, D, x_J, dq_prev; the same float products as
+// k_features_raw + k_features_norm), one 16 B chunk of 8 per thread
+template <class TB, class TX>
+__global__ void k_features_bf16(int64_t nc, const double* __restrict__ src, const TB* __restrict__ D,
+                                const TX* __restrict__ x_ci, const TX* __restrict__ xprev_ci,
+                                const int32_t* __restrict__ ci, const float* __restrict__ fac,
+                                __nv_bfloat16* __restrict__ feat) {
+  __shared__ float f[NIN];
+  if (threadIdx.x < NIN) f[threadIdx.x] = fac[10 + threadIdx.x];
+  __syncthreads();
+  const int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;  // chunk
+  if (j >= nc * (NIN / 8)) return;
+  const int64_t c = j / (NIN / 8);
+  const int k0 = 8 * int(j - (NIN / 8) * c);
+  const int64_t i = ci[c];
+  float v[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    const int k = k0 + e;
+    float r;
+    if (k < 5)
+      r = float(src[5 * c + k]);
+    else if (k < 30)
+      r = float(D[25 * c + k - 5]);
+    else if (k < 35)
+      r = float(x_ci[5 * i + k - 30]);
+    else
+      r = xprev_ci ? float(xprev_ci[5 * i + k - 35]) : 0.f;
+    v[e] = r * f[k];
+  }
+  *reinterpret_cast<uint4*>(feat + c * NIN + k0) = pack8(v);
+}
+
+// x0 = x_J + xs * d into ctx's colour-order iterate, which holds x_J (the
+// next linear solve starts from it); x0_out (RCM order) optional
+template <class TX>
+__global__ void k_apply_start(int64_t nc, const float* __restrict__ y, const float* __restrict__ fac,
+                              const int32_t* __restrict__ ci, TX* __restrict__ x, double* __restrict__ x0) {
   const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (c >= nc) return;
   const int64_t i = ci[c];
   for (int k = 0; k < 5; ++k) {
-    const double v = double(xj[c * 5 + k]) + double(scl[k]) * double(y[c * 5 + k]);
+    const float xj = float(x[5 * i + k]);
+    const double v = double(xj) + double(fac[5 + k]) * double(y[c * 5 + k]);
     x[5 * i + k] = TX(v);
     if (x0) x0[5 * c + k] = v;
   }
+}
+
+template <class TB, class TX>
+void launch_features16(fpsi_gnn* m, fpsi_ctx* x, __nv_bfloat16* feat, cudaStream_t s) {
+  const int64_t nc = x->H.nc;
+  const int nblk = int(nb_(nc, GT));
+  const TX* xv = static_cast<const TX*>(x->d_x);
+  const TX* xp = x->have_xprev ? static_cast<const TX*>(x->d_xprev) : nullptr;
+  k_feat_stats<TX><<<nblk, GT, 0, s>>>(nc, x->d_src, xv, x->d_ci, m->d_lpart);
+  k_feat_scales<<<1, 64, 0, s>>>(m->d_lpart, nblk, nc, m->d_fac);
+  k_features_bf16<TB, TX><<<nb_(nc * (NIN / 8), 256), 256, 0, s>>>(
+      nc, x->d_src, static_cast<const TB*>(x->d_D), xv, xp, x->d_ci, m->d_fac, feat);
 }
 }  // namespace
 
 extern "C" {
 
+// Inference runs on the context's stream: the Jacobi start D^-1 B, the
+// features (two kernels and a one-block scale kernel, no host round trip),
+// the three layers with the head, and the start written over D^-1 B.
 int fpsi_gnn_predict(fpsi_gnn* m, fpsi_ctx* x, double* x0) {
   if (!m || !x) return FPSI_E_INVALID;
+  if (!x->have_asm || !x->d_D || x->P.solver != FPSI_SOLVER_SGS) {
+    fpsi::set_error("learned start: needs an assembled SGS system with the diagonal blocks kept");
+    return FPSI_E_STATE;
+  }
   const int64_t nc = x->H.nc;
-  float rs[5], xs[5];
   Graph G;
   int rc = ensure_capacity(m, nc);
   if (!rc) rc = ctx_graph(x, &G);
   if (rc) return rc;
-  // features and Jacobi start in the backward pass's buffers, which an
-  // inference pass does not use ([nc][64] FP32 each)
-  float* fbuf = m->d_dz;
-  float* xjb = m->d_dh;
-  rc = make_features(m, x, fbuf, xjb, rs, xs);
-  if (!rc) rc = forward(m, G, fbuf, false);
-  double* dx0 = nullptr;
-  if (!rc && x0) rc = galloc(&dx0, nc * 5);
-  if (!rc) {
-    float* dscl = reinterpret_cast<float*>(m->d_lpart);
-    cudaMemcpyAsync(dscl, xs, sizeof(xs), cudaMemcpyHostToDevice, m->stream);
-    if (x->P.precision == FPSI_PREC_MIXED)
-      k_apply_start<float><<<nb_(nc, 256), 256, 0, m->stream>>>(nc, xjb, m->d_y, dscl, x->d_ci,
-                                                               (float*)x->d_x, dx0);
-    else
-      k_apply_start<double><<<nb_(nc, 256), 256, 0, m->stream>>>(nc, xjb, m->d_y, dscl, x->d_ci,
-                                                                (double*)x->d_x, dx0);
-    if (cudaStreamSynchronize(m->stream) != cudaSuccess) rc = FPSI_E_CUDA;
-    if (!rc) rc = take_error(m);
+  // from now on the context keeps a copy of each applied update
+  if (!x->d_xprev) {
+    if (cudaMalloc(&x->d_xprev, size_t(nc) * 5 * 8) != cudaSuccess) {
+      x->d_xprev = nullptr;
+      fpsi::set_error("cudaMalloc failed for the previous-update copy");
+      return FPSI_E_NOMEM;
+    }
+    x->have_xprev = false;
   }
+  x->keep_prev = true;
+  FPSI_CUDA_TRY(cudaStreamSynchronize(m->stream));  // no training pass in flight
+  cudaStream_t s = x->stream;
+  // x_J = D^-1 B from the factored blocks (the iterate may hold a solve)
+  if ((rc = fpsi::launch_jacobi_start(x))) return rc;
+  // BF16 features [nc][40] in a backward-pass buffer an inference pass does
+  // not use ([nc][64] FP32)
+  __nv_bfloat16* feat16 = reinterpret_cast<__nv_bfloat16*>(m->d_dz);
+  if (x->P.precision == FPSI_PREC_FP64)
+    launch_features16<double, double>(m, x, feat16, s);
+  else if (x->P.precision == FPSI_PREC_MIXED)
+    launch_features16<float, float>(m, x, feat16, s);
+  else
+    launch_features16<float, double>(m, x, feat16, s);
+  if ((rc = forward(m, G, nullptr, false, feat16, s))) return rc;
+  double* dx0 = nullptr;
+  if (x0 && (rc = galloc(&dx0, nc * 5))) return rc;
+  if (x->P.precision == FPSI_PREC_MIXED)
+    k_apply_start<float><<<nb_(nc, 256), 256, 0, s>>>(nc, m->d_y, m->d_fac, x->d_ci, (float*)x->d_x, dx0);
+  else
+    k_apply_start<double><<<nb_(nc, 256), 256, 0, s>>>(nc, m->d_y, m->d_fac, x->d_ci, (double*)x->d_x, dx0);
+  if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) rc = FPSI_E_CUDA;
+  if (!rc) rc = take_error(m);
   if (!rc && x0) {
     std::vector<double> h(nc * 5);
     if (cudaMemcpy(h.data(), dx0, h.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess) rc = FPSI_E_CUDA;

@@ -61,8 +61,37 @@ __device__ __forceinline__ void q_arr(const Q5& q, double a[5]) {
 // boundary face states (bcInflow.loci:270-344, bcOutflow.loci:84-142,
 // bcImpermeable.loci:48-140); eta == 1
 // ---------------------------------------------------------------------------
+// Area-weighted mean gauge pressure of the cells next to each boundary
+// condition (areaPressure / boundary_area, bcOutflow.loci:178-198), for the
+// pMean outflow: block b sums over the faces of condition b in a fixed
+// order (per-thread strided sums, then a tree), out[2b] = sum A pg,
+// out[2b+1] = sum A.
+constexpr int BCM_THREADS = 256;
+__global__ void __launch_bounds__(BCM_THREADS)
+k_bc_mean(MeshView M, const double* __restrict__ q, double* __restrict__ out) {
+  const int b = blockIdx.x;
+  __shared__ double sp[BCM_THREADS], sa[BCM_THREADS];
+  double ap = 0, aa = 0;
+  for (int64_t f = M.nfi + threadIdx.x; f < M.nf; f += BCM_THREADS) {
+    if (-M.cr[f] - 1 != b) continue;
+    const double A = M.area[f];
+    ap += A * q[5 * int64_t(M.cl[f]) + 4];
+    aa += A;
+  }
+  sp[threadIdx.x] = ap, sa[threadIdx.x] = aa;
+  __syncthreads();
+  for (int st = BCM_THREADS / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) sp[threadIdx.x] += sp[threadIdx.x + st], sa[threadIdx.x] += sa[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[2 * b] = sp[0], out[2 * b + 1] = sa[0];
+}
+
+// bcmean: k_bc_mean's sums (read by pMean outflows only); bcflags: error
+// bits of this residual (OUTFLOW_BECAME_INFLOW)
 __global__ void k_bc_state(MeshView M, const double* __restrict__ q, const fpsi_bc* __restrict__ bcs,
-                           Gas g, double* __restrict__ qb) {
+                           Gas g, const double* __restrict__ bcmean, int32_t* __restrict__ bcflags,
+                           double* __restrict__ qb) {
   const int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t nbf = M.nf - M.nfi;
   if (b >= nbf) return;
@@ -106,6 +135,30 @@ __global__ void k_bc_state(MeshView M, const double* __restrict__ q, const fpsi_
       r.u = qi.u - 2.0 * un * nx;
       r.v = qi.v - 2.0 * un * ny;
       r.w = qi.w - 2.0 * un * nz;
+      break;
+    }
+    case FPSI_BC_OUTFLOW:
+    case FPSI_BC_OUTFLOW_MEAN: {  // bcOutflow.loci:206-244, us_n = 0
+      // back pressure (gauge): 'p', or the cell's pressure shifted so that
+      // the boundary's area-weighted mean becomes 'pMean' (:200-204)
+      double pref = bc.pg;
+      if (bc.kind == FPSI_BC_OUTFLOW_MEAN) {
+        const int bi = -M.cr[f] - 1;
+        pref = qi.p + (bc.pg - bcmean[2 * bi] / bcmean[2 * bi + 1]);
+      }
+      const double uit = qi.u * nx + qi.v * ny + qi.w * nz;
+      const double ai = sqrt(g.gamma * g.Rt * qi.T);
+      const double rhoi = (qi.p + g.pamb) / (g.Rt * qi.T);
+      if (uit >= 0) {
+        if (!(uit > ai)) {  // subsonic: the back pressure at the cell's density
+          r.p = pref;
+          r.T = (pref + g.pamb) / (g.Rt * rhoi);
+        }
+      } else {  // the outflow became an inflow
+        r.u = r.v = r.w = 0.0;
+        r.p = qi.p - 0.05 * (qi.p + g.pamb);
+        atomicOr(bcflags, FPSI_BCERR_OUTFLOW_BECAME_INFLOW);
+      }
       break;
     }
     default:
@@ -590,7 +643,7 @@ k_cell_residual(MeshView M, const double* __restrict__ q, const double* __restri
 // out[0..2] = rms (sqrt of sums), out[3..4] rtmax/loc, out[5..6] etmax/loc,
 // out[7] mtmax; written to slot `step` of a per-run history
 __global__ void k_norm_final(const double* __restrict__ part, int nblk,
-                             double* __restrict__ out) {
+                             int32_t* __restrict__ bcflags, double* __restrict__ out) {
   __shared__ double sh[8][NORM_THREADS];
   const int t = threadIdx.x;
   double a[8] = {0, 0, 0, 0, -1, 0, -1, 0};
@@ -631,6 +684,10 @@ __global__ void k_norm_final(const double* __restrict__ part, int nblk,
     out[2] = sqrt(sh[2][0]);
 #pragma unroll
     for (int k = 3; k < 8; ++k) out[k] = sh[k][0];
+    // the boundary-condition error bits of this residual, cleared for the next
+    out[8] = double(*bcflags);
+    out[9] = 0.0;
+    *bcflags = 0;
   }
 }
 
@@ -1360,7 +1417,10 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
   const int T = 256;
   if (x->H.nbf > 0) {
     prof_begin(x, "bc_state");
-    dev::k_bc_state<<<blocks_for(x->H.nbf, T), T, 0, s>>>(M, x->d_q, x->d_bcs, g, x->d_qb);
+    if (x->any_pmean)
+      dev::k_bc_mean<<<unsigned(x->bcs.size()), dev::BCM_THREADS, 0, s>>>(M, x->d_q, x->d_bcmean);
+    dev::k_bc_state<<<blocks_for(x->H.nbf, T), T, 0, s>>>(M, x->d_q, x->d_bcs, g, x->d_bcmean,
+                                                         x->d_err + 1, x->d_qb);
     prof_end(x);
   }
   prof_begin(x, "grad_limiter");
@@ -1381,7 +1441,7 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
   dev::k_cell_residual<<<x->nblk_norm, dev::NORM_THREADS, 0, s>>>(
       M, x->d_q, x->d_F, g, x->P.urelax, x->P.dtmax, x->P.cflmax, x->H.vol_tot,
       x->d_src, x->d_dtau, x->d_part);
-  dev::k_norm_final<<<1, dev::NORM_THREADS, 0, s>>>(x->d_part, x->nblk_norm, resid_slot);
+  dev::k_norm_final<<<1, dev::NORM_THREADS, 0, s>>>(x->d_part, x->nblk_norm, x->d_err + 1, resid_slot);
   prof_end(x);
   FPSI_CUDA_TRY(cudaGetLastError());
   return FPSI_OK;

@@ -79,8 +79,14 @@ enum fpsi_bc_kind {
   FPSI_BC_SUPERSONIC_OUTFLOW = 3,  /* bcOutflow.loci:127-165 */
   FPSI_BC_EXTRAPOLATE = 4,         /* bcOutflow.loci:84-120 */
   FPSI_BC_REFLECTING = 5,          /* symmetry / slip wall, bcImpermeable.loci:48-140 */
-  FPSI_BC_VISCOUS_WALL = 6         /* adiabatic no-slip wall, bcViscousWall.loci:146-240 */
+  FPSI_BC_VISCOUS_WALL = 6,        /* adiabatic no-slip wall, bcViscousWall.loci:146-240 */
+  FPSI_BC_OUTFLOW = 7,             /* subsonic outflow at back pressure 'p' (gauge: fpsi_bc.pg),
+                                      bcOutflow.loci:174-273 */
+  FPSI_BC_OUTFLOW_MEAN = 8         /* outflow whose area-weighted mean pressure is 'pMean'
+                                      (gauge: fpsi_bc.pg), bcOutflow.loci:178-204 */
 };
+/* fpsi_resid.bcErrorCode bits (flowPsiIO.h:212-215) */
+#define FPSI_BCERR_OUTFLOW_BECAME_INFLOW 1
 
 typedef struct fpsi_params {
   double gamma;            /* 1.4                                  solverEoS.loci:31 */

@@ -57,7 +57,8 @@ def loss_and_grad(w: np.ndarray, feat: np.ndarray, target: np.ndarray, A: torch.
     for l in range(NLAYER):
         ws, wn, b = p[3 * l], p[3 * l + 1], p[3 * l + 2]
         agg = bf16(torch.sparse.mm(A, h))  # mean of the layer input, rounded
-        h = bf16(torch.nn.functional.gelu(bf16(h) @ ws.T + agg @ wn.T + b))
+        # GELU in its tanh form (Hendrycks and Gimpel 2016), as the device
+        h = bf16(torch.nn.functional.gelu(bf16(h) @ ws.T + agg @ wn.T + b, approximate="tanh"))
     y = h @ p[-2].T + p[-1]
     t = torch.from_numpy(np.ascontiguousarray(target, np.float32))
     loss = ((y - t) ** 2).mean()

@@ -477,6 +477,8 @@ struct orc_ctx {
   std::vector<double> T, pg, u;         // nc, nc, nc*3
   std::vector<double> tmu;              // nc eddy viscosity (turbulent regime)
   std::vector<double> qb;               // nbf... stored per face (nf*5): boundary face state
+  std::vector<double> bc_pmean;         // per condition: area-weighted mean gauge pressure
+  uint64_t bc_err = 0;                  // boundary-condition error bits of the last residual
   std::vector<double> grad, phi;        // nc*15, nc*5
   std::vector<double> F, maxev;         // nf*5, nf
   std::vector<double> src, dtau;        // nc*5, nc
@@ -725,9 +727,10 @@ extern "C" int orc_get_state(orc_ctx* o, double* T, double* pg, double* u) {
 
 // boundary face state (gagePressure_f, temperature_f, u_f) from the cell
 // centre state: farfield bcInflow.loci:311-344, supersonicInflow :270-278,
-// extrapolate bcOutflow.loci:84-95, supersonicOutflow :127-142, reflecting
-// (mirror of the normal velocity) bcImpermeable.loci:48-140.
-static void bc_face_state(const orc_ctx* o, int64_t f, double q[5]) {
+// extrapolate bcOutflow.loci:84-95, supersonicOutflow :127-142, outflow at a
+// back pressure :206-244, reflecting (mirror of the normal velocity)
+// bcImpermeable.loci:48-140.  Returns the boundary-condition error bits.
+static uint64_t bc_face_state(const orc_ctx* o, int64_t f, double q[5]) {
   const fpsi_params& P = o->P;
   int c = o->cl[f];
   const fpsi_bc& bc = o->bcs[-o->cr[f] - 1];
@@ -779,10 +782,35 @@ static void bc_face_state(const orc_ctx* o, int64_t f, double q[5]) {
     case FPSI_BC_VISCOUS_WALL:  // stationary adiabatic wall (bcViscousWall.loci:148-218)
       ub = mk(0, 0, 0);
       break;
+    case FPSI_BC_OUTFLOW:
+    case FPSI_BC_OUTFLOW_MEAN: {
+      // pBoundary - Pambient: p_BC, or (pMean) the cell's pressure plus the
+      // difference of pMean and the boundary's mean pressure (:174-204)
+      const double pref = bc.kind == FPSI_BC_OUTFLOW
+                              ? bc.pg
+                              : pgi + (bc.pg - o->bc_pmean[-o->cr[f] - 1]);
+      const double uit = dot(ui, n) - us_n;
+      const double ai = std::sqrt(P.gamma * P.Rtilde * Ti);
+      const double rhoi = (pgi + P.Pambient) / (P.Rtilde * Ti);
+      if (uit >= 0) {
+        if (!(uit > ai)) {
+          pgb = pref;
+          Tb = (pgb + P.Pambient) / (P.Rtilde * rhoi);
+        }
+      } else {
+        ub = mk(0, 0, 0);
+        pgb = pgi - .05 * (pgi + P.Pambient);
+        Tb = Ti;
+        q[0] = Tb, q[1] = ub.x, q[2] = ub.y, q[3] = ub.z, q[4] = pgb;
+        return FPSI_BCERR_OUTFLOW_BECAME_INFLOW;
+      }
+      break;
+    }
     default:  // extrapolate
       break;
   }
   q[0] = Tb, q[1] = ub.x, q[2] = ub.y, q[3] = ub.z, q[4] = pgb;
+  return 0;
 }
 
 static inline void cell_q(const orc_ctx* o, int64_t c, double q[5]) {
@@ -1035,8 +1063,22 @@ extern "C" int orc_residual(orc_ctx* o, double* src_out, fpsi_resid* norms) {
   if (P.viscous == 2 && P.turbulence == FPSI_TURB_SA) sa_tmu(o);
   o->have_sa = o->have_sa_dq = false;
   o->qb.assign(nf * 5, 0);
+  // area-weighted mean gauge pressure next to each condition (areaPressure /
+  // boundary_area, bcOutflow.loci:178-198), in face order
+  {
+    std::vector<double> ap(o->bcs.size(), 0.0), aa(o->bcs.size(), 0.0);
+    for (int64_t f = 0; f < nf; ++f)
+      if (o->cr[f] < 0) {
+        const int b = -o->cr[f] - 1;
+        ap[b] += o->area[f] * o->pg[o->cl[f]];
+        aa[b] += o->area[f];
+      }
+    o->bc_pmean.assign(o->bcs.size(), 0.0);
+    for (size_t b = 0; b < o->bcs.size(); ++b) o->bc_pmean[b] = aa[b] > 0 ? ap[b] / aa[b] : 0.0;
+  }
+  o->bc_err = 0;
   for (int64_t f = 0; f < nf; ++f)
-    if (o->cr[f] < 0) bc_face_state(o, f, &o->qb[5 * f]);
+    if (o->cr[f] < 0) o->bc_err |= bc_face_state(o, f, &o->qb[5 * f]);
   gradients_and_limiters(o);
   o->F.assign(nf * 5, 0);
   o->maxev.assign(nf, 0);
@@ -1174,6 +1216,7 @@ extern "C" int orc_residual(orc_ctx* o, double* src_out, fpsi_resid* norms) {
   o->have_resid = true;
   o->have_asm = false;
   if (src_out) std::memcpy(src_out, o->src.data(), sizeof(double) * nc * 5);
+  r.bcErrorCode = o->bc_err;
   if (norms) *norms = r;
   if (r.rtrms != r.rtrms || r.etrms != r.etrms || r.mtrms != r.mtrms) return FPSI_E_NAN;
   return FPSI_OK;

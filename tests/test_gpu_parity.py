@@ -68,6 +68,8 @@ CASES = {
     "shock_hex": lambda prec: cases.oblique_shock_cube(8, precision=prec),
     "farfield_hllc": lambda prec: cases.farfield_cube(6, precision=prec, flux="hllc",
                                                       limiter="barth"),
+    "outflow_p": lambda prec: cases.outflow_duct(6, precision=prec),
+    "outflow_pmean": lambda prec: cases.outflow_duct(6, precision=prec, mean=True),
 }
 
 
@@ -206,7 +208,7 @@ def test_sgs_converges_on_gpu(need_gpu):
 
 
 @pytest.mark.parametrize("prec", ["fp64", "ref", "mixed"])
-@pytest.mark.parametrize("name", ["farfield_hex", "tgv_tets", "shock_hex"])
+@pytest.mark.parametrize("name", ["farfield_hex", "tgv_tets", "shock_hex", "outflow_pmean"])
 def test_newton_steps_match_oracle(need_gpu, name, prec):
     case = CASES[name](prec)
     g, o = _pair(case)
@@ -290,6 +292,28 @@ def test_run_stops_at_the_nan_step(need_gpu):
     g.set_state(*good)
     h = g.run(2)
     assert all(np.isfinite(x["rtrms"]) for x in h)
+
+
+@pytest.mark.parametrize("mean", [False, True])
+def test_outflow_that_became_inflow_is_flagged(need_gpu, mean):
+    """bcOutflow.loci:238-243: a face of an outflow whose flow enters sets
+    OUTFLOW_BECAME_INFLOW in the residual's bcErrorCode (flowPsiIO.h:212)"""
+    case = cases.outflow_duct(6, precision="fp64", mean=mean)
+    g, o = _pair(case)
+    _, ng = g.residual()
+    assert ng["bcErrorCode"] == 0
+    T, p, u = g.get_state()
+    u[:, 0] = -np.abs(u[:, 0])
+    g.set_state(T, p, u)
+    o.set_state(T, p, u)
+    sg, ng = g.residual()
+    so, no = o.residual()
+    assert ng["bcErrorCode"] == no["bcErrorCode"] == 1
+    assert np.max(np.abs(sg - so) / cell_scale(o, T, p, u)) < 1e-12
+    # the bit belongs to that residual only
+    u[:, 0] = np.abs(u[:, 0])
+    g.set_state(T, p, u)
+    assert g.residual()[1]["bcErrorCode"] == 0
 
 
 def test_call_order_enforced(need_gpu):
