@@ -334,7 +334,7 @@ int fpsi_destroy(fpsi_ctx* x) {
   free_sa(x);
   void* ps[] = {x->d_cl, x->d_cr, x->d_n, x->d_area, x->d_rL, x->d_rR, x->d_vol, x->d_cc,
                 x->d_Minv, x->d_cf_off, x->d_cf, x->d_colour_cells, x->d_bcs, x->d_bcmean, x->d_q,
-                x->d_qb, x->d_grad, x->d_F, x->d_src, x->d_dtau, x->d_tmu,
+                x->d_qb, x->d_grad, x->d_qf, x->d_F, x->d_src, x->d_dtau, x->d_tmu,
                 x->d_part, x->d_resid, x->d_amin, x->d_err, x->d_perm, x->d_stage, x->d_ci, x->d_ccol,
                 x->d_nbr, x->d_colinfo, x->d_cnb_off, x->d_cnb, x->d_xprev, x->d_qsave};
   for (void* p : ps)
@@ -426,6 +426,7 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
   TRY(dalloc(x, &x->d_q, nc * 5));
   TRY(dalloc(x, &x->d_qb, std::max<int64_t>(H.nbf, 1) * 5));
   TRY(dalloc(x, &x->d_grad, nc * fpsi::GPREC));
+  TRY(dalloc(x, &x->d_qf, nf * fpsi::QFREC));
   TRY(dalloc(x, &x->d_F, nf * fpsi::FREC));
   TRY(dalloc(x, &x->d_src, nc * 5));
   TRY(dalloc(x, &x->d_dtau, nc));
@@ -713,7 +714,13 @@ int fpsi_get_reconstruction(fpsi_ctx* x, double* grad, double* limiter) {
   if (!x) return FPSI_E_INVALID;
   if (!x->have_resid) return FPSI_E_STATE;
   const int64_t nc = x->H.nc;
-  // device records hold the gradient (15) and the limiter (5) of a cell
+  // device records hold the gradient (15) and the limiter (5) of a cell;
+  // an inviscid residual does not write them, so they are made on request
+  if (!x->grad_valid) {
+    int rc = fpsi::launch_grad_records(x);
+    if (!rc) rc = sync(x);
+    if (rc) return rc;
+  }
   std::vector<double> rec(size_t(nc) * fpsi::GPREC), part;
   if (grad || limiter)
     FPSI_CUDA_TRY(cudaMemcpy(rec.data(), x->d_grad, rec.size() * sizeof(double), cudaMemcpyDeviceToHost));

@@ -17,6 +17,10 @@ constexpr int FREC = 6;
 // d(T,u,v,w,pg)/dx, y, z) then the limiter (5); 160 B, ten aligned 16 B
 // accesses
 constexpr int GPREC = 20;
+// doubles per face of the reconstructed face states: per side (cl, then cr
+// or the boundary state) T, u, v, w, pg at the face and the side's spectral
+// radius |u.n| + a of its cell-centre state; 96 B, six aligned 16 B accesses
+constexpr int QFREC = 12;
 // doubles per residual-norm record: rtrms, etrms, mtrms, rtmax, its cell,
 // etmax, its cell, mtmax, the boundary-condition error bits of that
 // residual (flowPsiIO.h:212-215), one spare
@@ -133,6 +137,9 @@ struct fpsi_ctx {
   double* d_q = nullptr;       // [nc][5]  T,u,v,w,pg
   double* d_qb = nullptr;      // [nbf][5] boundary face states
   double* d_grad = nullptr;    // [nc][GPREC]: gradient (15) and limiter (5) per cell
+  bool grad_valid = false;     // d_grad holds the last residual's records (viscous runs
+                               // write them every residual, others on request)
+  double* d_qf = nullptr;      // [nf][QFREC]: reconstructed face states of the last residual
   double* d_F = nullptr;       // [nf][FREC]: face flux (5) and maxev_f * area
   double* d_src = nullptr;     // [nc][5]
   double* d_dtau = nullptr;    // [nc]

@@ -269,82 +269,103 @@ __device__ __forceinline__ void grad_limiter_cell(const MeshView& M, const doubl
   for (int k = 0; k < 5; ++k) po[k] = ph[k];
 }
 
+// The face states of one cell's faces: MUSCL q_c + phi grad.(x_f - x_c)
+// with the floors 0.1 min(T) and 0.1 min(pg) - 0.9 Pambient over the face's
+// two cells (the form of fluxLowDiss.loci:338-356), and the side's spectral
+// radius 0.5 max(|2 u.n - 2a|, |2 u.n + 2a|) of the cell-centre state
+// (maxev_f, solverSetup.loci:81-105, eta == 1).  The cell writes its own
+// side of every face; on a boundary face also the other side, the boundary
+// state (not reconstructed) and its spectral radius.
+__device__ __forceinline__ void side_record(double* o, const double l[5], double m) {
+  double2* o2 = reinterpret_cast<double2*>(o);
+  o2[0] = make_double2(l[0], l[1]);
+  o2[1] = make_double2(l[2], l[3]);
+  o2[2] = make_double2(l[4], m);
+}
+__device__ __forceinline__ double side_maxev(const double s[5], double nx, double ny, double nz,
+                                             const Gas& gas) {
+  const double ut = s[1] * nx + s[2] * ny + s[3] * nz;
+  const double a2 = 2.0 * sqrt(gas.gamma * gas.Rt * s[0]);  // sqrt(4 a^2) of the reference, to an ulp
+  return 0.5 * dmax(fabs(2.0 * ut - a2), fabs(2.0 * ut + a2));
+}
+__device__ __forceinline__ void face_states_cell(const MeshView& M, const double* __restrict__ q,
+                                                 const double* __restrict__ qb, const Gas& gas,
+                                                 int64_t c, const double g[15], const double ph[5],
+                                                 double* __restrict__ qf) {
+  double qc[5];
+  q_arr(load_q(q, c), qc);
+  const int32_t e0 = M.cf_off[c], e1 = M.cf_off[c + 1];
+  const int64_t nf = M.nf;
+#pragma unroll 2
+  for (int32_t e = e0; e < e1; ++e) {
+    const int32_t ent = M.cf[e];
+    const int64_t f = ent >> 1;
+    const int side = ent & 1;
+    const bool bnd = f >= M.nfi;
+    double Tn, pn;
+    double qbs[5];
+    if (bnd) {
+      const double* p = qb + 5 * (f - M.nfi);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) qbs[k] = __ldg(p + k);
+      Tn = qbs[0], pn = qbs[4];
+    } else {
+      const double* p = q + 5 * int64_t(side ? M.cl[f] : M.cr[f]);
+      Tn = __ldg(p), pn = __ldg(p + 4);
+    }
+    const double* r = side ? M.rR : M.rL;
+    const double rx = r[f], ry = r[nf + f], rz = r[2 * nf + f];
+    double l[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) l[k] = qc[k] + ph[k] * (g[3 * k] * rx + g[3 * k + 1] * ry + g[3 * k + 2] * rz);
+    l[0] = dmax(l[0], 0.1 * dmin(side ? Tn : qc[0], side ? qc[0] : Tn));
+    l[4] = dmax(l[4], 0.1 * dmin(side ? pn : qc[4], side ? qc[4] : pn) - 0.9 * gas.pamb);
+    const double nx = M.n[f], ny = M.n[nf + f], nz = M.n[2 * nf + f];
+    double* o = qf + int64_t(QFREC) * f;
+    side_record(o + (QFREC / 2) * side, l, side_maxev(qc, nx, ny, nz, gas));
+    if (bnd) side_record(o + QFREC / 2, qbs, side_maxev(qbs, nx, ny, nz, gas));
+  }
+}
+
+// WREC: also the cell's gradient-and-limiter record (viscous terms, the SA
+// model and fpsi_get_reconstruction read it)
+template <bool WREC>
 __global__ void __launch_bounds__(GRAD_THREADS)
 k_grad_limiter(MeshView M, const double* __restrict__ q, const double* __restrict__ qb, int limiter,
-               double Kl, double* __restrict__ grad) {
-  __shared__ double sr[GRAD_THREADS * GPREC];
+               double Kl, Gas gas, double* __restrict__ grad, double* __restrict__ qf) {
+  __shared__ double sr[WREC ? GRAD_THREADS * GPREC : 1];
   const int64_t c0 = int64_t(blockIdx.x) * GRAD_THREADS;
   const int64_t c = c0 + threadIdx.x;
-  const int cnt = int(min(int64_t(GRAD_THREADS), M.nc - c0));
-  double* my = sr + GPREC * threadIdx.x;
-  if (c < M.nc) grad_limiter_cell(M, q, qb, limiter, Kl, c, my, my + 15);
-  __syncthreads();
-  // one record per cell: the gradient (15) then the limiter (5)
-  for (int i = threadIdx.x; i < GPREC * cnt; i += GRAD_THREADS) grad[GPREC * c0 + i] = sr[i];
-}
-
-// one cell's gradient-and-limiter record (GPREC doubles, 16 B aligned)
-__device__ __forceinline__ void load_rec20(const double* p, double* v) {
-  const double2* p2 = reinterpret_cast<const double2*>(p);
+  if (c < M.nc) {
+    double rec[GPREC];
+    grad_limiter_cell(M, q, qb, limiter, Kl, c, rec, rec + 15);
+    face_states_cell(M, q, qb, gas, c, rec, rec + 15, qf);
+    if (WREC) {
 #pragma unroll
-  for (int j = 0; j < GPREC / 2; ++j) {
-    const double2 t = __ldg(p2 + j);
-    v[2 * j] = t.x;
-    v[2 * j + 1] = t.y;
+      for (int k = 0; k < GPREC; ++k) sr[GPREC * threadIdx.x + k] = rec[k];
+    }
+  }
+  if (WREC) {
+    __syncthreads();
+    // one record per cell: the gradient (15) then the limiter (5)
+    const int cnt = int(min(int64_t(GRAD_THREADS), M.nc - c0));
+    for (int i = threadIdx.x; i < GPREC * cnt; i += GRAD_THREADS) grad[GPREC * c0 + i] = sr[i];
   }
 }
 
-// MUSCL states of one face: q_c + phi*grad.(x_f - x_c), floors 0.1*min(T),
-// 0.1*min(pg) - 0.9*Pambient (the form of fluxLowDiss.loci:338-356).
+// The two reconstructed states of a face and their spectral radii, from
+// the face record the gradient kernel wrote (six aligned 16 B loads).
 struct FaceStates {
   Q5 L, R;
-  double ql[5], qr[5];  // cell-centre (unreconstructed) values of both sides
+  double mL, mR;
 };
-
-__device__ __forceinline__ void reconstruct(const MeshView& M, const double* __restrict__ q,
-                                            const double* __restrict__ qb,
-                                            const double* __restrict__ grad, int64_t f,
-                                            double pamb, FaceStates& s) {
-  const int64_t nf = M.nf;
-  const int32_t a = M.cl[f];
-  const bool bnd = f >= M.nfi;
-  q_arr(load_q(q, a), s.ql);
-  if (bnd) {
-    const double* p = qb + 5 * (f - M.nfi);
-#pragma unroll
-    for (int k = 0; k < 5; ++k) s.qr[k] = __ldg(p + k);
-  } else {
-    q_arr(load_q(q, M.cr[f]), s.qr);
-  }
-  const double tlim = 0.1 * dmin(s.ql[0], s.qr[0]);
-  const double plim = 0.1 * dmin(s.ql[4], s.qr[4]) - 0.9 * pamb;
-  double l[5], r[5];
-  {
-    const double rx = M.rL[f], ry = M.rL[nf + f], rz = M.rL[2 * nf + f];
-    double gp[GPREC];  // gradient then limiter, ten 16 B loads
-    load_rec20(grad + GPREC * int64_t(a), gp);
-#pragma unroll
-    for (int k = 0; k < 5; ++k)
-      l[k] = s.ql[k] + gp[15 + k] * (gp[3 * k] * rx + gp[3 * k + 1] * ry + gp[3 * k + 2] * rz);
-  }
-  l[0] = dmax(l[0], tlim);
-  l[4] = dmax(l[4], plim);
-  if (bnd) {
-#pragma unroll
-    for (int k = 0; k < 5; ++k) r[k] = s.qr[k];
-  } else {
-    const int64_t d = M.cr[f];
-    const double rx = M.rR[f], ry = M.rR[nf + f], rz = M.rR[2 * nf + f];
-    double gp[GPREC];
-    load_rec20(grad + GPREC * d, gp);
-#pragma unroll
-    for (int k = 0; k < 5; ++k)
-      r[k] = s.qr[k] + gp[15 + k] * (gp[3 * k] * rx + gp[3 * k + 1] * ry + gp[3 * k + 2] * rz);
-    r[0] = dmax(r[0], tlim);
-    r[4] = dmax(r[4], plim);
-  }
-  s.L.T = l[0], s.L.u = l[1], s.L.v = l[2], s.L.w = l[3], s.L.p = l[4];
-  s.R.T = r[0], s.R.u = r[1], s.R.v = r[2], s.R.w = r[3], s.R.p = r[4];
+__device__ __forceinline__ void load_face_states(const double* __restrict__ qf, int64_t f,
+                                                 FaceStates& s) {
+  const double2* p = reinterpret_cast<const double2*>(qf + int64_t(QFREC) * f);
+  const double2 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+  const double2 d = __ldg(p + 3), e = __ldg(p + 4), h = __ldg(p + 5);
+  s.L.T = a.x, s.L.u = a.y, s.L.v = b.x, s.L.w = b.y, s.L.p = c.x, s.mL = c.y;
+  s.R.T = d.x, s.R.u = d.y, s.R.v = e.x, s.R.w = e.y, s.R.p = h.x, s.mR = h.y;
 }
 
 // ---------------------------------------------------------------------------
@@ -479,40 +500,35 @@ __device__ __forceinline__ void add_visc_jac(TB* M, const VFace& v, const double
 // ---------------------------------------------------------------------------
 // face flux + spectral radius, one thread per face
 // ---------------------------------------------------------------------------
-template <bool VIS>
+// KIND: the Riemann solver (fpsi_flux_kind), a template parameter so that
+// each instantiation holds only its own solver's registers
+template <bool VIS, int KIND>
 __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
                             const double* __restrict__ qb, const double* __restrict__ grad,
-                            Gas g, int kind, Visc V, double* __restrict__ F) {
+                            const double* __restrict__ qf, Gas g, Visc V, double* __restrict__ F) {
   const int64_t f = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (f >= M.nf) return;
   FaceStates s;
-  reconstruct(M, q, qb, grad, f, g.pamb, s);
+  load_face_states(qf, f, s);
   const double nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
   const double A = M.area[f];
   double fl[5];
   if (bc_kind(M, f) == FPSI_BC_VISCOUS_WALL) {
-    // pressure only, from the cell-centre pressure (bcViscousWall.loci:220-230)
-    const double p = s.qr[4];
+    // pressure only, from the cell-centre pressure (bcViscousWall.loci:220-230),
+    // which the wall's boundary state carries
+    const double p = s.R.p;
     fl[0] = 0.0, fl[1] = p * nx * A, fl[2] = p * ny * A, fl[3] = p * nz * A, fl[4] = 0.0;
   } else {
-    riemann1(kind, s.L, s.R, nx, ny, nz, A, g, fl);
+    riemann1(KIND, s.L, s.R, nx, ny, nz, A, g, fl);
   }
   if constexpr (VIS) {
     const VFace v = viscous_face(M, q, qb, grad, V, f);
 #pragma unroll
     for (int k = 0; k < 4; ++k) fl[1 + k] -= v.vf[k];
   }
-  // maxev_f (solverSetup.loci:81-105), eta == 1: |u.n| + a of each side
-  const double utr = s.qr[1] * nx + s.qr[2] * ny + s.qr[3] * nz;
-  const double ar = sqrt(g.gamma * g.Rt * s.qr[0]);
-  const double sr = 2.0 * ar;  // sqrt(4 a^2) of the reference, to an ulp
-  double m = 0.5 * dmax(fabs(2.0 * utr - sr), fabs(2.0 * utr + sr));
-  if (f < M.nfi) {
-    const double utl = s.ql[1] * nx + s.ql[2] * ny + s.ql[3] * nz;
-    const double al = sqrt(g.gamma * g.Rt * s.ql[0]);
-    const double sl = 2.0 * al;  // sqrt(4 a^2) of the reference, to an ulp
-    m = dmax(0.5 * dmax(fabs(2.0 * utl - sl), fabs(2.0 * utl + sl)), m);
-  }
+  // maxev_f (solverSetup.loci:81-105): the larger spectral radius of the
+  // two sides; a boundary face has only its boundary state's
+  const double m = f < M.nfi ? dmax(s.mL, s.mR) : s.mR;
   double2* o = reinterpret_cast<double2*>(F + FREC * f);
   o[0] = make_double2(fl[0], fl[1]);
   o[1] = make_double2(fl[2], fl[3]);
@@ -703,7 +719,7 @@ constexpr int JAC_THREADS = 128;
 template <class TB, bool VIS>
 __global__ void __launch_bounds__(JAC_THREADS)
 k_face_jacobian(MeshView M, const double* __restrict__ q, const double* __restrict__ qb,
-                const double* __restrict__ grad, Gas g, Visc V,
+                const double* __restrict__ grad, const double* __restrict__ qf, Gas g, Visc V,
                 TB* __restrict__ fjp, TB* __restrict__ fjm) {
   __shared__ TB stage[JAC_THREADS * 25];
   const int64_t f0 = int64_t(blockIdx.x) * JAC_THREADS;
@@ -714,7 +730,7 @@ k_face_jacobian(MeshView M, const double* __restrict__ q, const double* __restri
   double nx = 0, ny = 0, nz = 0, A = 0;
   if (live) {
     FaceStates s;
-    reconstruct(M, q, qb, grad, f, g.pamb, s);
+    load_face_states(qf, f, s);
     nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
     A = M.area[f];
     ra = roe_average1(s.L, s.R, nx, ny, nz, g);
@@ -754,16 +770,14 @@ k_face_jacobian(MeshView M, const double* __restrict__ q, const double* __restri
 // block d(p n A)/dpg is c1 = -A with every other coefficient zero.
 template <class TB>
 __global__ void __launch_bounds__(JAC_THREADS)
-k_face_jacobian_c(MeshView M, const double* __restrict__ q, const double* __restrict__ qb,
-                  const double* __restrict__ grad, Gas g,
-                  TB* __restrict__ fjc) {
+k_face_jacobian_c(MeshView M, const double* __restrict__ qf, Gas g, TB* __restrict__ fjc) {
   __shared__ TB stage[JAC_THREADS * CK_FACE];
   const int64_t f0 = int64_t(blockIdx.x) * JAC_THREADS;
   const int64_t f = f0 + threadIdx.x;
   const int64_t cnt = min(int64_t(JAC_THREADS), M.nf - f0) * CK_FACE;
   if (f < M.nf) {
     FaceStates s;
-    reconstruct(M, q, qb, grad, f, g.pamb, s);
+    load_face_states(qf, f, s);
     const double nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
     const double A = M.area[f];
     const RoeAvg ra = roe_average1(s.L, s.R, nx, ny, nz, g);
@@ -1410,6 +1424,15 @@ dev::Gas gas(const fpsi_ctx* x) {
 }
 }  // namespace
 
+int launch_grad_records(fpsi_ctx* x) {
+  const dev::MeshView M = view(x);
+  dev::k_grad_limiter<true><<<blocks_for(M.nc, dev::GRAD_THREADS), dev::GRAD_THREADS, 0, x->stream>>>(
+      M, x->d_q, x->d_qb, x->P.limiter, x->P.Kl, gas(x), x->d_grad, x->d_qf);
+  FPSI_CUDA_TRY(cudaGetLastError());
+  x->grad_valid = true;
+  return FPSI_OK;
+}
+
 int launch_residual(fpsi_ctx* x, double* resid_slot) {
   const dev::MeshView M = view(x);
   const dev::Gas g = gas(x);
@@ -1424,18 +1447,36 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
     prof_end(x);
   }
   prof_begin(x, "grad_limiter");
-  dev::k_grad_limiter<<<blocks_for(M.nc, dev::GRAD_THREADS), dev::GRAD_THREADS, 0, s>>>(M, x->d_q, x->d_qb, x->P.limiter,
-                                                             x->P.Kl, x->d_grad);
+  // the gradient records are written every residual only where the viscous
+  // terms (and the SA model) read them
+  x->grad_valid = x->P.viscous != 0;
+  if (x->grad_valid)
+    dev::k_grad_limiter<true><<<blocks_for(M.nc, dev::GRAD_THREADS), dev::GRAD_THREADS, 0, s>>>(
+        M, x->d_q, x->d_qb, x->P.limiter, x->P.Kl, g, x->d_grad, x->d_qf);
+  else
+    dev::k_grad_limiter<false><<<blocks_for(M.nc, dev::GRAD_THREADS), dev::GRAD_THREADS, 0, s>>>(
+        M, x->d_q, x->d_qb, x->P.limiter, x->P.Kl, g, x->d_grad, x->d_qf);
   prof_end(x);
   prof_begin(x, "face_flux");
-  // the viscous terms are a separate instantiation: the inviscid kernel
-  // does not carry their registers
-  if (x->P.viscous)
-    dev::k_face_flux<true><<<blocks_for(M.nf, 128), 128, 0, s>>>(
-        M, x->d_q, x->d_qb, x->d_grad, g, x->P.flux, visc(x), x->d_F);
-  else
-    dev::k_face_flux<false><<<blocks_for(M.nf, 128), 128, 0, s>>>(
-        M, x->d_q, x->d_qb, x->d_grad, g, x->P.flux, visc(x), x->d_F);
+  // the viscous terms and each Riemann solver are separate instantiations:
+  // the inviscid Roe kernel does not carry the others' registers
+  {
+    const unsigned nb = blocks_for(M.nf, 128);
+    const dev::Visc Vv = visc(x);
+    double* F = x->d_F;
+#define FPSI_FLUX(VIS, K) \
+  dev::k_face_flux<VIS, K><<<nb, 128, 0, s>>>(M, x->d_q, x->d_qb, x->d_grad, x->d_qf, g, Vv, F)
+    if (x->P.viscous) {
+      if (x->P.flux == FPSI_FLUX_ROE) FPSI_FLUX(true, FPSI_FLUX_ROE);
+      else if (x->P.flux == FPSI_FLUX_HLLE) FPSI_FLUX(true, FPSI_FLUX_HLLE);
+      else FPSI_FLUX(true, FPSI_FLUX_HLLC);
+    } else {
+      if (x->P.flux == FPSI_FLUX_ROE) FPSI_FLUX(false, FPSI_FLUX_ROE);
+      else if (x->P.flux == FPSI_FLUX_HLLE) FPSI_FLUX(false, FPSI_FLUX_HLLE);
+      else FPSI_FLUX(false, FPSI_FLUX_HLLC);
+    }
+#undef FPSI_FLUX
+  }
   prof_end(x);
   prof_begin(x, "cell_residual");
   dev::k_cell_residual<<<x->nblk_norm, dev::NORM_THREADS, 0, s>>>(
@@ -1493,13 +1534,13 @@ static int launch_assemble_t(fpsi_ctx* x) {
   prof_begin(x, "face_jacobian");
   if (cpt)
     dev::k_face_jacobian_c<TB><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
-        M, x->d_q, x->d_qb, x->d_grad, g, (TB*)x->d_fjc);
+        M, x->d_qf, g, (TB*)x->d_fjc);
   else if (x->P.viscous)
     dev::k_face_jacobian<TB, true><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
-        M, x->d_q, x->d_qb, x->d_grad, g, visc(x), fjp, fjm);
+        M, x->d_q, x->d_qb, x->d_grad, x->d_qf, g, visc(x), fjp, fjm);
   else
     dev::k_face_jacobian<TB, false><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
-        M, x->d_q, x->d_qb, x->d_grad, g, visc(x), fjp, fjm);
+        M, x->d_q, x->d_qb, x->d_grad, x->d_qf, g, visc(x), fjp, fjm);
   prof_end(x);
   prof_begin(x, "assemble_lu");
   if (cpt)

@@ -11,6 +11,9 @@ namespace fpsi {
 // residual chain: boundary states, gradient+limiter, face flux, per-cell
 // gather (src, dtau), norms into resid_slot[8] (device)
 int launch_residual(fpsi_ctx* x, double* resid_slot);
+// the gradient-and-limiter records of the last residual's state (written
+// by the residual itself only for viscous runs)
+int launch_grad_records(fpsi_ctx* x);
 // face Jacobians, diagonal blocks, LU, B and the starting iterate
 // (the starting iterate is the block Jacobi start D^-1 B)
 int launch_assemble(fpsi_ctx* x);
