@@ -37,7 +37,7 @@ class Params(C.Structure):
         ("precision", C.c_int32), ("viscous", C.c_int32), ("turbulence", C.c_int32),
         ("Prt", C.c_double), ("mu_a1", C.c_double), ("mu_a2", C.c_double),
         ("mu_a3", C.c_double), ("k_a1", C.c_double), ("k_a2", C.c_double),
-        ("k_a3", C.c_double),
+        ("k_a3", C.c_double), ("time_accurate", C.c_int32), ("newton_iters", C.c_int32),
     ]
 
 
@@ -161,6 +161,7 @@ _SIGS = {
     "fpsi_newton_step": (C.c_int, [_ctx, C.POINTER(StepInfo)]),
     "fpsi_newton_step_ex": (C.c_int, [_ctx, C.c_void_p, C.POINTER(StepOpts), C.POINTER(StepInfo)]),
     "fpsi_run": (C.c_int, [_ctx, C.c_int32, C.POINTER(Resid)]),
+    "fpsi_time_step": (C.c_int, [_ctx, C.POINTER(Resid)]),
     "fpsi_run_timed": (C.c_int, [_ctx, C.c_int32, C.POINTER(Resid), _dp]),
     "fpsi_kernel_times": (C.c_int, [_ctx, C.c_int32, C.c_int32, C.c_char_p, _dp,
                                     C.POINTER(C.c_int64), _ip]),

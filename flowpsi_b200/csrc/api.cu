@@ -235,6 +235,14 @@ int check_params(const fpsi_params* p) {
     fpsi::set_error("turbulence: 0 (given eddy viscosity) or 1 (SA, needs viscous = 2)");
     return FPSI_E_INVALID;
   }
+  if (p->time_accurate < 0 || p->time_accurate > 1 || (p->time_accurate && p->newton_iters < 1)) {
+    fpsi::set_error("time_accurate: 0 (steady) or 1 (BDF2, newton_iters >= 1)");
+    return FPSI_E_INVALID;
+  }
+  if (p->time_accurate && p->turbulence == FPSI_TURB_SA && p->viscous == 2) {
+    fpsi::set_error("the SA model is advanced in steady mode only");
+    return FPSI_E_UNSUPPORTED;
+  }
   return FPSI_OK;
 }
 
@@ -302,6 +310,8 @@ void fpsi_default_params(fpsi_params* p) {
   p->k_a1 = 2.495e-3;
   p->k_a2 = 1.5;
   p->k_a3 = 194.0;
+  p->time_accurate = 0;
+  p->newton_iters = 6;
 }
 
 const char* fpsi_strerror(int code) {
@@ -334,7 +344,7 @@ int fpsi_destroy(fpsi_ctx* x) {
   free_sa(x);
   void* ps[] = {x->d_cl, x->d_cr, x->d_n, x->d_area, x->d_rL, x->d_rR, x->d_vol, x->d_cc,
                 x->d_Minv, x->d_cf_off, x->d_cf, x->d_colour_cells, x->d_bcs, x->d_bcmean, x->d_q,
-                x->d_qb, x->d_grad, x->d_qf, x->d_F, x->d_src, x->d_dtau, x->d_tmu,
+                x->d_qn, x->d_qnm1, x->d_qb, x->d_grad, x->d_qf, x->d_F, x->d_src, x->d_dtau, x->d_tmu,
                 x->d_part, x->d_resid, x->d_amin, x->d_err, x->d_perm, x->d_stage, x->d_ci, x->d_ccol,
                 x->d_nbr, x->d_colinfo, x->d_cnb_off, x->d_cnb, x->d_xprev, x->d_qsave};
   for (void* p : ps)
@@ -424,6 +434,8 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
   TRY(dalloc(x, &x->d_bcmean, std::max<size_t>(x->bcs.size(), 1) * 2));
   for (const fpsi_bc& b : x->bcs) x->any_pmean = x->any_pmean || b.kind == FPSI_BC_OUTFLOW_MEAN;
   TRY(dalloc(x, &x->d_q, nc * 5));
+  TRY(dalloc(x, &x->d_qn, nc * 5));
+  TRY(dalloc(x, &x->d_qnm1, nc * 5));
   TRY(dalloc(x, &x->d_qb, std::max<int64_t>(H.nbf, 1) * 5));
   TRY(dalloc(x, &x->d_grad, nc * fpsi::GPREC));
   TRY(dalloc(x, &x->d_qf, nf * fpsi::QFREC));
@@ -465,6 +477,7 @@ int fpsi_set_params(fpsi_ctx* x, const fpsi_params* p) {
   if (rc) return rc;
   x->P = *p;
   x->have_asm = x->have_dq = x->have_xprev = false;
+  x->have_levels = false;
   if (is_lsgs(x) && !x->keep_D) {
     x->keep_D = true;
     x->alloc_prec = -1;
@@ -663,6 +676,7 @@ int fpsi_set_state(fpsi_ctx* x, const double* T, const double* pg, const double*
   int rc = fpsi::launch_state(x, true);
   if (rc) return rc;
   x->have_resid = x->have_asm = x->have_dq = x->have_xprev = false;
+  x->have_levels = false;
   return sync(x);
 }
 
@@ -1227,6 +1241,28 @@ int fpsi_run(fpsi_ctx* x, int32_t nsteps, fpsi_resid* norms) {
   x->have_resid = x->have_asm = x->have_dq = false;
   if (rc) return rc;
   return finish_run(x, nsteps, launched, norms);
+}
+
+int fpsi_time_step(fpsi_ctx* x, fpsi_resid* norms) {
+  if (!x) return FPSI_E_INVALID;
+  if (!x->P.time_accurate) {
+    fpsi::set_error("fpsi_time_step needs params.time_accurate = 1");
+    return FPSI_E_STATE;
+  }
+  const int32_t nit = x->P.newton_iters;
+  int rc = ensure_hist(x, nit);
+  if (rc) return rc;
+  int32_t launched = 0;
+  rc = run_steps(x, nit, &launched);
+  if (!rc) rc = sync(x);
+  x->have_resid = x->have_asm = x->have_dq = false;
+  if (rc) return rc;
+  if ((rc = finish_run(x, nit, launched, norms))) return rc;
+  // the converged state becomes time level n+1: Q(n-1) = Q(n), Q(n) = Q(n+1)
+  const size_t b = size_t(x->H.nc) * 5 * sizeof(double);
+  std::swap(x->d_qn, x->d_qnm1);
+  FPSI_CUDA_TRY(cudaMemcpyAsync(x->d_qn, x->d_q, b, cudaMemcpyDeviceToDevice, x->stream));
+  return sync(x);
 }
 
 int fpsi_run_timed(fpsi_ctx* x, int32_t nsteps, fpsi_resid* norms, double* device_ms) {

@@ -135,6 +135,10 @@ struct fpsi_ctx {
   bool any_pmean = false;      // a pMean outflow is present
   // state and residual
   double* d_q = nullptr;       // [nc][5]  T,u,v,w,pg
+  // time-accurate mode: the states of time levels n and n-1 (as d_q)
+  double* d_qn = nullptr;
+  double* d_qnm1 = nullptr;
+  bool have_levels = false;
   double* d_qb = nullptr;      // [nbf][5] boundary face states
   double* d_grad = nullptr;    // [nc][GPREC]: gradient (15) and limiter (5) per cell
   bool grad_valid = false;     // d_grad holds the last residual's records (viscous runs

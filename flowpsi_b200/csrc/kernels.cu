@@ -541,9 +541,14 @@ __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
 constexpr int NORM_THREADS = 256;
 
 __global__ void __launch_bounds__(NORM_THREADS)
+// qn, qnm1 (time-accurate BDF2, else null): the states of time levels n
+// and n-1; src then receives the rhs with the time terms
+// (solverTimestep.loci:397-428), and the norms are the rhs's
+// (solverResidual.loci:113-150), while dtau is still the spatial src's
 k_cell_residual(MeshView M, const double* __restrict__ q, const double* __restrict__ F,
                 Gas g, double urelax, double dtmax,
-                double cflmax, double vol_tot, double* __restrict__ src,
+                double cflmax, double vol_tot, const double* __restrict__ qn,
+                const double* __restrict__ qnm1, double* __restrict__ src,
                 double* __restrict__ dtau, double* __restrict__ part) {
   const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   double rt = 0, et = 0, mt = 0, rmax = 0, emax = 0, mmax = 0;
@@ -566,9 +571,6 @@ k_cell_residual(MeshView M, const double* __restrict__ q, const double* __restri
       }
       meva += c.y;
     }
-    double* so = src + 5 * c;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) so[k] = s[k];
     const double V = M.vol[c];
     const double cflpdt = 0.5 * meva / V;
     double dt = dtmax;
@@ -590,6 +592,30 @@ k_cell_residual(MeshView M, const double* __restrict__ q, const double* __restri
     const double dp = rvol * (rT * (2.0 * qk * s[0] - dsu + s[4]) - fT * s[0]);
     dt = dmin(dt, urelax * p / (fabs(dp) + 1e-30));
     dtau[c] = dt;
+    if (qn) {
+      // BDF2: s - 1.5 (Q(n+1) - Q(n)) V/dt + 0.5 (Q(n) - Q(n-1)) V/dt
+      const Q5 a = load_q(qn, c), b = load_q(qnm1, c);
+      const double rdtvol = V / dtmax;
+      const double w1 = 1.5 * rdtvol, w2 = 0.5 * rdtvol;
+      const double rhon = (a.p + g.pamb) / (g.Rt * a.T);
+      const double rhonm1 = (b.p + g.pamb) / (g.Rt * b.T);
+      const double rhonp1 = rho;
+      s[0] = s[0] - w1 * (rhonp1 - rhon) + w2 * (rhon - rhonm1);
+      const double up1[3] = {qc.u, qc.v, qc.w}, un[3] = {a.u, a.v, a.w}, um1[3] = {b.u, b.v, b.w};
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const double r1 = rhonp1 * up1[i], r0 = rhon * un[i], rm = rhonm1 * um1[i];
+        s[1 + i] = s[1 + i] - w1 * (r1 - r0) + w2 * (r0 - rm);
+      }
+      const double igm1 = 1.0 / (g.gamma - 1.0);
+      const double e1 = rhonp1 * (g.Rt * qc.T * igm1 + qk);
+      const double e0 = rhon * (g.Rt * a.T * igm1 + 0.5 * (a.u * a.u + a.v * a.v + a.w * a.w));
+      const double em = rhonm1 * (g.Rt * b.T * igm1 + 0.5 * (b.u * b.u + b.v * b.v + b.w * b.w));
+      s[4] = s[4] - w1 * (e1 - e0) + w2 * (e0 - em);
+    }
+    double* so = src + 5 * c;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) so[k] = s[k];
     // norms (solverResidual.loci:74-112)
     const double w = V / vol_tot;
     const double a0 = rvol * s[0], a4 = rvol * s[4];
@@ -936,7 +962,7 @@ k_assemble(MeshView M, SweepView S, const double* __restrict__ q, const double* 
            const double* __restrict__ dtau, const TB* __restrict__ fjp, const TB* __restrict__ fjm,
            const TB* __restrict__ fjc, Gas g, TB* __restrict__ luc, TB* __restrict__ bcv,
            int32_t* __restrict__ pvv, TB* __restrict__ aoff, TB* __restrict__ Dout, TX* __restrict__ x,
-           int32_t* __restrict__ err) {
+           int32_t* __restrict__ err, double dcoef) {
   constexpr int RW = 50;  // words staged per face (explicit blocks)
   // compact records move in 16 B units: U16 per record, stored record-major
   // with an odd stride of RS16 units so that a quarter warp's 16 B accesses
@@ -1083,7 +1109,8 @@ k_assemble(MeshView M, SweepView S, const double* __restrict__ q, const double* 
 #pragma unroll
   for (int i = 0; i < 25; ++i) D[i] = -sJ[i];
   const Q5 qc = load_q(q, c);
-  const double coef = M.vol[c] / dtau[c];
+  // V / dtau (steady, solverLinearSystem.loci:176-215), 1.5 V / dtau (BDF2, :376-435)
+  const double coef = dcoef * M.vol[c] / dtau[c];
   const double T = qc.T, rP = 1.0 / (g.Rt * T);
   const double rho = (qc.p + g.pamb) * rP;
   const double rT = -rho / T;
@@ -1288,8 +1315,10 @@ __global__ void k_sum2(const double* __restrict__ part, int nblk, double* __rest
 // aborts there)
 template <class TX>
 __global__ void __launch_bounds__(NORM_THREADS)
+// relax: 0.9 (steady, solverNewton.loci:62-78) or 0.75 of T and p (BDF2,
+// :163-182, whose floor is max(|d|, 1e-30) instead of |d| + 1e-30)
 k_update(int64_t nc, double pamb, const int32_t* __restrict__ ci, const TX* __restrict__ x, double* __restrict__ q,
-         double* __restrict__ amin_part, const double* __restrict__ guard) {
+         double* __restrict__ amin_part, const double* __restrict__ guard, bool bdf) {
   const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   double alpha = 1.0;
   const bool halt = guard && (isnan(guard[0]) || isnan(guard[1]) || isnan(guard[2]));
@@ -1297,8 +1326,13 @@ k_update(int64_t nc, double pamb, const int32_t* __restrict__ ci, const TX* __re
     double* qc = q + 5 * c;
     const TX* d = x + 5 * int64_t(ci[c]);
     const double dT = double(d[0]), dp = double(d[4]);
-    alpha = dmin(alpha, 0.9 * qc[0] / (fabs(dT) + 1e-30));
-    alpha = dmin(alpha, 0.9 * (qc[4] + pamb) / (fabs(dp) + 1e-30));
+    if (bdf) {
+      alpha = dmin(alpha, 0.75 * (qc[4] + pamb) / dmax(fabs(dp), 1e-30));
+      alpha = dmin(alpha, 0.75 * qc[0] / dmax(fabs(dT), 1e-30));
+    } else {
+      alpha = dmin(alpha, 0.9 * qc[0] / (fabs(dT) + 1e-30));
+      alpha = dmin(alpha, 0.9 * (qc[4] + pamb) / (fabs(dp) + 1e-30));
+    }
     qc[0] += alpha * dT;
     qc[1] += alpha * double(d[1]);
     qc[2] += alpha * double(d[2]);
@@ -1479,9 +1513,18 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
   }
   prof_end(x);
   prof_begin(x, "cell_residual");
+  const bool bdf = x->P.time_accurate != 0;
+  if (bdf && !x->have_levels) {
+    // the first time step after a new state: Q(n-1) = Q(n) = that state
+    FPSI_CUDA_TRY(cudaMemcpyAsync(x->d_qn, x->d_q, size_t(M.nc) * 5 * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, s));
+    FPSI_CUDA_TRY(cudaMemcpyAsync(x->d_qnm1, x->d_q, size_t(M.nc) * 5 * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, s));
+    x->have_levels = true;
+  }
   dev::k_cell_residual<<<x->nblk_norm, dev::NORM_THREADS, 0, s>>>(
       M, x->d_q, x->d_F, g, x->P.urelax, x->P.dtmax, x->P.cflmax, x->H.vol_tot,
-      x->d_src, x->d_dtau, x->d_part);
+      bdf ? x->d_qn : nullptr, bdf ? x->d_qnm1 : nullptr, x->d_src, x->d_dtau, x->d_part);
   dev::k_norm_final<<<1, dev::NORM_THREADS, 0, s>>>(x->d_part, x->nblk_norm, x->d_err + 1, resid_slot);
   prof_end(x);
   FPSI_CUDA_TRY(cudaGetLastError());
@@ -1518,7 +1561,7 @@ static void launch_assemble_kernel(fpsi_ctx* x, const dev::MeshView& M, const de
       M, sweep_view(x), x->d_q, x->d_src, x->d_dtau, (const TB*)x->d_fjp, (const TB*)x->d_fjm,
       (const TB*)x->d_fjc, g, (TB*)x->d_luc, (TB*)x->d_bc, x->d_pv,
       x->P.solver == FPSI_SOLVER_LSGS ? nullptr : (TB*)x->d_aoff, x->keep_D ? (TB*)x->d_D : nullptr,
-      (TX*)x->d_x, x->d_err);
+      (TX*)x->d_x, x->d_err, x->P.time_accurate ? 1.5 : 1.0);
 }
 
 template <class TB, class TX>
@@ -1679,10 +1722,10 @@ int launch_update(fpsi_ctx* x, const double* guard) {
   prof_begin(x, "update");
   if (x->P.precision == FPSI_PREC_MIXED)
     dev::k_update<float><<<x->nblk_norm, dev::NORM_THREADS, 0, x->stream>>>(
-        nc, x->P.Pambient, map, (const float*)xv, x->d_q, x->d_amin, guard);
+        nc, x->P.Pambient, map, (const float*)xv, x->d_q, x->d_amin, guard, x->P.time_accurate != 0);
   else
     dev::k_update<double><<<x->nblk_norm, dev::NORM_THREADS, 0, x->stream>>>(
-        nc, x->P.Pambient, map, (const double*)xv, x->d_q, x->d_amin, guard);
+        nc, x->P.Pambient, map, (const double*)xv, x->d_q, x->d_amin, guard, x->P.time_accurate != 0);
   prof_end(x);
   FPSI_CUDA_TRY(cudaGetLastError());
   if (x->keep_prev && x->d_xprev && !lsgs) {

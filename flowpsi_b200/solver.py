@@ -409,6 +409,21 @@ class FlowPsi:
             raise e
         return hist
 
+    def time_step(self) -> list[dict]:
+        """One BDF2 time step of size dtmax (params.time_accurate = 1):
+        params.newton_iters Newton iterations, then the time levels shift
+        (solverTimestep.loci:397-428, solverNewton.loci:163-198).  Returns
+        the norms of each iteration's rhs."""
+        nit = self.params.newton_iters
+        arr = (N.Resid * max(nit, 1))()
+        rc = N.lib().fpsi_time_step(self._ctx, arr)
+        hist = [arr[i].as_dict() for i in range(nit)]
+        if rc != N.FPSI_OK:
+            e = N.FpsiError(rc, "fpsi_time_step")
+            e.history = hist
+            raise e
+        return hist
+
     def run_timed(self, nsteps: int):
         """(norm history, device milliseconds) of nsteps steps, timed with
         CUDA events on the library's stream"""

@@ -113,6 +113,11 @@ typedef struct fpsi_params {
   double mu_a1, mu_a2, mu_a3; /* Sutherland mu = a1 T^a2/(T+a3): 1.458e-6, 1.5, 110.4 */
   double k_a1, k_a2, k_a3;    /* conductivity k = k1 T^k2/(T+k3): 2.495e-3, 1.5, 194
                                  (sutherlandParameters, fluxViscous.loci:58-80) */
+  int32_t time_accurate;   /* timeSteppingMode: 0 steady (pseudo-time, one Newton
+                              iteration per step), 1 time accurate with the BDF2 scheme
+                              (solverTimestep.loci:397-428); dtmax is then the time step */
+  int32_t newton_iters;    /* newtonMaxIter: Newton iterations per time step, 6
+                                                                   solverNewton.loci:200-210 */
 } fpsi_params;
 
 typedef struct fpsi_bc {
@@ -322,6 +327,19 @@ int fpsi_newton_step_ex(fpsi_ctx* ctx, fpsi_gnn* model, const fpsi_step_opts* op
  * the call returns FPSI_E_NAN (fpsi_last_error names the step).  The norm
  * history lives in the context (no allocation per call up to 4096 steps). */
 int fpsi_run(fpsi_ctx* ctx, int32_t nsteps, fpsi_resid* norms);
+/* ---- time-accurate stepping (params.time_accurate = 1, BDF2) -------------
+ * One time step of size dtmax: params.newton_iters Newton iterations on the
+ * state q(n+1), each with the residual rhs = src - (1.5 (Q(n+1) - Q(n)) -
+ * 0.5 (Q(n) - Q(n-1))) V / dtmax of the conserved variables Q = (rho, rho u,
+ * rho e0) (solverTimestep.loci:397-428), the diagonal blocks -srcJ +
+ * 1.5 V / dtau dQ/dq (solverLinearSystem.loci:376-435), the linear solve and
+ * the update clipped at 0.75 of T and p (solverNewton.loci:163-198); then
+ * Q(n-1) = Q(n), Q(n) = Q(n+1).  The first step after fpsi_set_state takes
+ * Q(n-1) = Q(n) = the set state.  norms (newton_iters entries, may be NULL)
+ * receive the norms of each iteration's rhs.  In this mode fpsi_residual's
+ * src is that rhs, and fpsi_newton_step is one Newton iteration of the
+ * current time step. */
+int fpsi_time_step(fpsi_ctx* ctx, fpsi_resid* norms);
 /* fpsi_run timed on the device: CUDA events recorded on the library's
  * stream around the nsteps steps; device_ms receives the elapsed time. */
 int fpsi_run_timed(fpsi_ctx* ctx, int32_t nsteps, fpsi_resid* norms, double* device_ms);

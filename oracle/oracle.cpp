@@ -482,6 +482,9 @@ struct orc_ctx {
   std::vector<double> grad, phi;        // nc*15, nc*5
   std::vector<double> F, maxev;         // nf*5, nf
   std::vector<double> src, dtau;        // nc*5, nc
+  // time-accurate BDF2: primitive states of time levels n and n-1
+  std::vector<double> Tn, pgn, un, Tm, pgm, um;
+  bool have_levels = false;
   bool have_resid = false, have_asm = false, have_dq = false;
   // blocks (both precisions kept; the active one is selected by P.precision)
   std::vector<float> fjp32, fjm32, D32, LU32, B32;
@@ -696,6 +699,7 @@ extern "C" void orc_destroy(orc_ctx* o) { delete o; }
 extern "C" int orc_set_params(orc_ctx* o, const fpsi_params* p) {
   o->P = *p;
   o->have_asm = false;
+  o->have_levels = false;
   return FPSI_OK;
 }
 
@@ -716,6 +720,7 @@ extern "C" int orc_set_state(orc_ctx* o, const double* T, const double* pg, cons
   std::memcpy(o->pg.data(), pg, sizeof(double) * o->nc);
   std::memcpy(o->u.data(), u, sizeof(double) * o->nc * 3);
   o->have_resid = o->have_asm = o->have_dq = false;
+  o->have_levels = false;
   return FPSI_OK;
 }
 extern "C" int orc_get_state(orc_ctx* o, double* T, double* pg, double* u) {
@@ -1062,6 +1067,12 @@ extern "C" int orc_residual(orc_ctx* o, double* src_out, fpsi_resid* norms) {
   if (P.Minf < 0.5) return FPSI_E_UNSUPPORTED;
   if (P.viscous == 2 && P.turbulence == FPSI_TURB_SA) sa_tmu(o);
   o->have_sa = o->have_sa_dq = false;
+  if (P.time_accurate && !o->have_levels) {  // first time step: Q(n-1) = Q(n) = Q
+    o->Tn = o->Tm = o->T;
+    o->pgn = o->pgm = o->pg;
+    o->un = o->um = o->u;
+    o->have_levels = true;
+  }
   o->qb.assign(nf * 5, 0);
   // area-weighted mean gauge pressure next to each condition (areaPressure /
   // boundary_area, bcOutflow.loci:178-198), in face order
@@ -1180,6 +1191,26 @@ extern "C" int orc_residual(orc_ctx* o, double* src_out, fpsi_resid* norms) {
     const double dp = rvol * (rT * (q2 * s[0] - dsu + s[4]) - fT * s[0]);
     dt = std::min(dt, P.urelax * p / (std::fabs(dp) + 1e-30));
     o->dtau[c] = dt;
+    if (P.time_accurate) {
+      // rhs of the BDF2 Newton iteration (solverTimestep.loci:397-428)
+      const double Pa = P.Pambient;
+      const double rhon = (o->pgn[c] + Pa) / (Rt * o->Tn[c]);
+      const double rhonm1 = (o->pgm[c] + Pa) / (Rt * o->Tm[c]);
+      const double rhonp1 = (o->pg[c] + Pa) / (Rt * o->T[c]);
+      const double rdtvol = o->vol[c] / P.dtmax;
+      const double w = 0.5, w1 = (1.0 + w) * rdtvol, w2 = w * rdtvol;
+      double* r = &o->src[5 * c];
+      r[0] = (r[0] - w1 * (rhonp1 - rhon) + w2 * (rhon - rhonm1));
+      const V3 Un = v3(&o->un[3 * c]), Um = v3(&o->um[3 * c]);
+      const V3 runp1 = rhonp1 * U, run = rhon * Un, runm1 = rhonm1 * Um;
+      r[1] = (r[1] - w1 * (runp1.x - run.x) + w2 * (run.x - runm1.x));
+      r[2] = (r[2] - w1 * (runp1.y - run.y) + w2 * (run.y - runm1.y));
+      r[3] = (r[3] - w1 * (runp1.z - run.z) + w2 * (run.z - runm1.z));
+      const double re0np1 = rhonp1 * (Rt * o->T[c] / (g - 1.) + .5 * dot(U, U));
+      const double re0n = rhon * (Rt * o->Tn[c] / (g - 1.) + .5 * dot(Un, Un));
+      const double re0nm1 = rhonm1 * (Rt * o->Tm[c] / (g - 1.) + .5 * dot(Um, Um));
+      r[4] = (r[4] - w1 * (re0np1 - re0n) + w2 * (re0n - re0nm1));
+    }
   }
   // residual norms, solverResidual.loci:74-112 joined in cell order
   fpsi_resid r;
@@ -1285,7 +1316,8 @@ static int assemble_t(orc_ctx* o, std::vector<TB>& fjp, std::vector<TB>& fjm,
       for (int i = 0; i < 25; ++i) sJ[i] -= fjp[25 * o->bd[k] + i];
     TB* d = &D[25 * c];
     for (int i = 0; i < 25; ++i) d[i] = -sJ[i];
-    const double coef = o->vol[c] / o->dtau[c];
+    // V / dtau (steady), 1.5 V / dtau (BDF2, solverLinearSystem.loci:389)
+    const double coef = (o->P.time_accurate ? 1.5 : 1.0) * o->vol[c] / o->dtau[c];
     const double Rt = P.Rtilde, T = o->T[c];
     const double rP = 1. / (Rt * T);
     const double rho = (o->pg[c] + P.Pambient) * rP;
@@ -1702,8 +1734,14 @@ extern "C" int orc_update(orc_ctx* o, double* min_alpha) {
   for (int64_t c = 0; c < o->nc; ++c) {
     const double* d = &o->dq[5 * c];
     double alpha = 1.0;
-    alpha = std::min(alpha, 0.9 * o->T[c] / (std::fabs(d[0]) + 1e-30));
-    alpha = std::min(alpha, 0.9 * (o->pg[c] + o->P.Pambient) / (std::fabs(d[4]) + 1e-30));
+    if (o->P.time_accurate) {  // BDF2, solverNewton.loci:163-182
+      const double relax = 0.75;
+      alpha = std::min(alpha, relax * (o->pg[c] + o->P.Pambient) / std::max(std::fabs(d[4]), 1e-30));
+      alpha = std::min(alpha, relax * o->T[c] / std::max(std::fabs(d[0]), 1e-30));
+    } else {
+      alpha = std::min(alpha, 0.9 * o->T[c] / (std::fabs(d[0]) + 1e-30));
+      alpha = std::min(alpha, 0.9 * (o->pg[c] + o->P.Pambient) / (std::fabs(d[4]) + 1e-30));
+    }
     o->T[c] += alpha * d[0];
     o->pg[c] += alpha * d[4];
     for (int i = 0; i < 3; ++i) o->u[3 * c + i] += alpha * d[1 + i];
@@ -1740,6 +1778,22 @@ extern "C" int orc_newton_step(orc_ctx* o, const int32_t* colour, fpsi_stepinfo*
   if (!rc && sa) rc = orc_sa_update(o);
   if (info) *info = si;
   return rc;
+}
+
+// One BDF2 time step (timeStepAccurate, timeStepSchemeBDF2): newton_iters
+// Newton iterations (solverNewton.loci:200-219), then the time levels move
+// on (the in-place copy of :190-198).
+extern "C" int orc_time_step(orc_ctx* o, const int32_t* colour, fpsi_resid* norms) {
+  if (!o->P.time_accurate) return FPSI_E_STATE;
+  for (int it = 0; it < o->P.newton_iters; ++it) {
+    fpsi_stepinfo si;
+    const int rc = orc_newton_step(o, colour, &si);
+    if (norms) norms[it] = si.resid;
+    if (rc) return rc;
+  }
+  o->Tm = o->Tn, o->pgm = o->pgn, o->um = o->un;
+  o->Tn = o->T, o->pgn = o->pg, o->un = o->u;
+  return FPSI_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -40,6 +40,7 @@ _SIGS = {
                                  C.POINTER(N.LsInfo)]),
     "orc_update": (C.c_int, [C.c_void_p, _dp]),
     "orc_newton_step": (C.c_int, [C.c_void_p, _ip, C.POINTER(N.StepInfo)]),
+    "orc_time_step": (C.c_int, [C.c_void_p, _ip, C.POINTER(N.Resid)]),
     "orc_set_threads": (C.c_int, [C.c_int]),
     "orc_set_nutilde": (C.c_int, [C.c_void_p, _dp]),
     "orc_get_nutilde": (C.c_int, [C.c_void_p, _dp]),
@@ -294,6 +295,16 @@ class Oracle:
         d = si.resid.as_dict()
         d["min_alpha"] = si.min_alpha
         return d
+
+    def time_step(self, colour=None):
+        """one BDF2 time step: newton_iters Newton iterations, then the
+        time levels move on; norms of each iteration"""
+        col = None if colour is None else np.ascontiguousarray(colour, np.int32)
+        nit = self.params.newton_iters
+        arr = (N.Resid * max(nit, 1))()
+        _chk(olib().orc_time_step(self._h, None if col is None else col.ctypes.data_as(_ip), arr),
+             "orc_time_step")
+        return [arr[i].as_dict() for i in range(nit)]
 
     # -- Spalart-Allmaras nu~ (turbulence/SA/SA_turb.loci) -------------------
     def set_nutilde(self, nut):

@@ -186,3 +186,25 @@ def test_viscous_linear_shear_has_no_net_force_inside():
     scale = mu * 2.0e3 * o.geometry()["area"].max()
     d = np.abs(res[1][inner, 1:4] - res[0][inner, 1:4]).max()
     assert d < 1e-10 * scale, (d, scale)
+
+
+def test_bdf2_oracle_properties():
+    """The oracle's BDF2 step (solverTimestep.loci:397-428): a uniform state
+    on a periodic grid is an exact solution (rhs zero, state kept), and on
+    the Taylor-Green state the Newton iterations of one step converge."""
+    from flowpsi_b200 import cases
+    from oracle import Oracle
+
+    c = cases.taylor_green_tets(3, precision="fp64")
+    c.params.time_accurate, c.params.newton_iters, c.params.dtmax = 1, 12, 0.005
+    o = Oracle(c.mesh, c.params)
+    nc = o.ncells
+    T, p, u = np.full(nc, 300.0), np.full(nc, 1e5), np.tile([30.0, -10.0, 5.0], (nc, 1))
+    o.set_state(T, p, u)
+    h = o.time_step()
+    assert max(x["rtrms"] for x in h) < 1e-9
+    for a, b in zip(o.get_state(), (T, p, u)):
+        np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-9)
+    o.set_state(*c.initial_state(o.geometry()["cellcenter"]))
+    h = o.time_step()
+    assert h[-1]["rtrms"] < 1e-3 * h[0]["rtrms"]
