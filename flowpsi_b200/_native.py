@@ -23,7 +23,8 @@ LIMITER = {"venkatakrishnan": 0, "barth": 1, "none": 2, "zero": 3}
 SOLVER = {"sgs": 0, "lsgs": 1}
 PRECISION = {"fp64": 0, "ref": 1, "mixed": 2}
 BC = {"farfield": 1, "supersonicInflow": 2, "supersonicOutflow": 3, "extrapolate": 4,
-      "reflecting": 5, "viscousWall": 6, "outflow": 7, "outflowMean": 8}
+      "reflecting": 5, "viscousWall": 6, "outflow": 7, "outflowMean": 8,
+      "isentropicInflow": 9, "fixedMass": 10, "fixedMassOutflow": 11}
 
 
 class Params(C.Structure):
@@ -43,7 +44,8 @@ class Params(C.Structure):
 
 class BCSpec(C.Structure):
     _fields_ = [("kind", C.c_int32), ("reserved", C.c_int32), ("T", C.c_double),
-                ("pg", C.c_double), ("u", C.c_double * 3), ("nu_t", C.c_double)]
+                ("pg", C.c_double), ("u", C.c_double * 3), ("nu_t", C.c_double),
+                ("mass_flux", C.c_double), ("mdot", C.c_double), ("mass_relax", C.c_double)]
 
 
 class Mesh(C.Structure):

@@ -100,16 +100,32 @@ def farfield_cube(n: int = 32, seed: int = 0, sweeps: int = 5, flux: str = "roe"
 
 def outflow_duct(n: int = 16, seed: int = 0, sweeps: int = 5, mean: bool = False,
                  back_pressure: float = 1.02e5, flux: str = "roe",
-                 limiter: str = "venkatakrishnan", precision: str = "ref") -> Case:
-    """Subsonic duct: n^3 hex cube [0,1]^3, farfield inflow at x-min (M=0.5
-    along +x, p=1e5 Pa, T=300 K), outflow at x-max held at a back pressure
-    (bcOutflow.loci:174-273; with mean=True the pMean form, where the
-    area-weighted mean of the boundary pressure is held instead), periodic
-    in y and z.  Initial state the freestream with 1% noise (farfield_cube)."""
+                 limiter: str = "venkatakrishnan", precision: str = "ref",
+                 inflow: str = "farfield", outflow: str = "outflow") -> Case:
+    """Subsonic duct: n^3 hex cube [0,1]^3, inflow at x-min, outflow at
+    x-max, periodic in y and z; initial state the freestream (M=0.5 along
+    +x, p=1e5 Pa, T=300 K) with 1% noise (farfield_cube).  inflow:
+    'farfield' at the freestream, 'isentropic' at its total pressure and
+    temperature (bcIsentropic.loci), or 'fixedMass' at its mass flux and
+    total temperature (bcFixedMass.loci).  outflow: 'outflow' at a back
+    pressure (bcOutflow.loci:174-273; with mean=True the pMean form, where
+    the area-weighted mean of the boundary pressure is held instead), or
+    'fixedMassOutflow' at 1.01 times the freestream mass flux, massRelax 0.5
+    (bcFixedMassOutflow.loci)."""
     T0, p0, M = 300.0, 1e5, 0.5
     U0 = M * math.sqrt(GAMMA * RTILDE * T0)
     ff = bc("farfield", T=T0, pg=p0, u=(U0, 0.0, 0.0))
-    out = bc("outflowMean" if mean else "outflow", T=T0, pg=back_pressure)
+    if inflow == "isentropic":  # total conditions of the freestream
+        f = 1.0 + 0.5 * (GAMMA - 1.0) * M * M
+        ff = bc("isentropicInflow", T=T0 * f, pg=p0 * f ** (GAMMA / (GAMMA - 1.0)))
+    elif inflow == "fixedMass":  # the freestream's mass flux at its total temperature
+        f = 1.0 + 0.5 * (GAMMA - 1.0) * M * M
+        ff = bc("fixedMass", T=T0 * f, mass_flux=p0 / (RTILDE * T0) * U0)
+    if outflow == "fixedMassOutflow":
+        out = bc("fixedMassOutflow", T=T0, mass_flux=1.01 * p0 / (RTILDE * T0) * U0,
+                 mass_relax=0.5)
+    else:
+        out = bc("outflowMean" if mean else "outflow", T=T0, pg=back_pressure)
     mesh = GeneratedMesh("hex", n=(n, n, n), L=(1.0, 1.0, 1.0), bc_side=(0, 1, -1, -1, -1, -1),
                          bcs=[ff, out])
     params = default_params(flux=flux, limiter=limiter, Kl=1.0, solver="sgs",

@@ -69,10 +69,12 @@ std::vector<double> soa3(const std::vector<double>& a, int64_t n) {
 }
 
 void free_system(fpsi_ctx* x) {
-  void* ps[] = {x->d_fjp, x->d_fjm, x->d_fjc, x->d_D, x->d_x, x->d_luc, x->d_bc, x->d_pv, x->d_aoff};
+  void* ps[] = {x->d_fjp, x->d_fjm, x->d_fjc, x->d_D, x->d_x, x->d_luc, x->d_bc, x->d_pv, x->d_aoff,
+                x->d_bjac};
   for (void* p : ps)
     if (p) cudaFree(p);
   x->d_fjp = x->d_fjm = x->d_fjc = x->d_D = x->d_x = x->d_luc = x->d_bc = x->d_aoff = nullptr;
+  x->d_bjac = nullptr;
   x->d_pv = nullptr;
 }
 
@@ -96,6 +98,8 @@ int alloc_system(fpsi_ctx* x) {
   if (x->keep_D)
     if ((rc = dalloc(x, (char**)&x->d_D, nc * 25 * tb))) return rc;
   if ((rc = dalloc(x, (char**)&x->d_x, nc * 5 * tx))) return rc;
+  if (x->any_fdbc && (rc = dalloc(x, (char**)&x->d_bjac, size_t(std::max<int64_t>(x->H.nbf, 1)) * 25 * tb)))
+    return rc;
   x->alloc_prec = x->P.precision;
   x->have_asm = x->have_dq = false;
   return FPSI_OK;
@@ -381,7 +385,7 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
   }
   x->bcs.assign(mesh->bcs, mesh->bcs + mesh->nbc);
   for (const fpsi_bc& b : x->bcs)
-    if (b.kind < FPSI_BC_FARFIELD || b.kind > FPSI_BC_OUTFLOW_MEAN) {
+    if (b.kind < FPSI_BC_FARFIELD || b.kind > FPSI_BC_FIXED_MASS_OUTFLOW) {
       fpsi::set_error("boundary condition kind %d is not on the device path", b.kind);
       delete x;
       return FPSI_E_UNSUPPORTED;
@@ -430,6 +434,19 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
     TRY(upload(x, &x->d_colinfo, ci));
   }
   TRY(dalloc(x, &x->d_stage, nc * 5));
+  // fixed-mass conditions given by mdot: the mass flux over the condition's
+  // area (massFlux_BC = mdot_BC / boundary_area, bcFixedMass.loci:227-230)
+  {
+    std::vector<double> barea(x->bcs.size(), 0.0);
+    for (int64_t f = H.nfi; f < H.nf; ++f) barea[-H.cr[f] - 1] += H.area[f];
+    for (size_t b = 0; b < x->bcs.size(); ++b) {
+      fpsi_bc& bc = x->bcs[b];
+      const bool fm = bc.kind == FPSI_BC_FIXED_MASS_INFLOW || bc.kind == FPSI_BC_FIXED_MASS_OUTFLOW;
+      if (fm && !(bc.mass_flux > 0) && barea[b] > 0) bc.mass_flux = bc.mdot / barea[b];
+      x->any_fdbc = x->any_fdbc || bc.kind == FPSI_BC_ISENTROPIC_INFLOW ||
+                    bc.kind == FPSI_BC_FIXED_MASS_INFLOW;
+    }
+  }
   TRY(upload(x, &x->d_bcs, x->bcs));
   TRY(dalloc(x, &x->d_bcmean, std::max<size_t>(x->bcs.size(), 1) * 2));
   for (const fpsi_bc& b : x->bcs) x->any_pmean = x->any_pmean || b.kind == FPSI_BC_OUTFLOW_MEAN;
@@ -804,6 +821,11 @@ int fpsi_get_blocks(fpsi_ctx* x, void* D, void* fjp, void* fjm, void* B) {
     const int rc = fpsi::ensure_explicit_blocks(x);
     if (rc) return rc;
   }
+  std::vector<char> hb;  // difference blocks of the total-pressure and fixed-mass inflows
+  if (fjp && x->any_fdbc) {
+    hb.resize(size_t(std::max<int64_t>(x->H.nbf, 1)) * 25 * tb);
+    FPSI_CUDA_TRY(cudaMemcpy(hb.data(), x->d_bjac, hb.size(), cudaMemcpyDeviceToHost));
+  }
   for (int w = 0; w < 2; ++w) {
     void* dst = w ? fjm : fjp;
     if (!dst) continue;
@@ -811,10 +833,24 @@ int fpsi_get_blocks(fpsi_ctx* x, void* D, void* fjp, void* fjm, void* B) {
     FPSI_CUDA_TRY(cudaMemcpy(h.data(), w ? x->d_fjm : x->d_fjp, h.size(), cudaMemcpyDeviceToHost));
     for (int64_t i = 0; i < nf; ++i) {
       char* o = (char*)dst + size_t(x->H.fperm[i]) * 25 * tb;
-      if (w && i >= x->H.nfi)
+      if (w && i >= x->H.nfi) {
         std::memset(o, 0, 25 * tb);  // no fjm on boundary faces
-      else
+      } else if (!w && i >= x->H.nfi && !hb.empty()) {
+        const int kind = x->bcs[-x->H.cr[i] - 1].kind;
+        const bool fd = kind == FPSI_BC_ISENTROPIC_INFLOW || kind == FPSI_BC_FIXED_MASS_INFLOW;
+        const char* a = h.data() + size_t(i) * 25 * tb;
+        const char* b = hb.data() + size_t(i - x->H.nfi) * 25 * tb;
+        std::memcpy(o, a, 25 * tb);
+        // the block srcJ loses is the face's (viscous part, if any) plus the difference block
+        for (int k = 0; fd && k < 25; ++k) {
+          if (tb == 4)
+            reinterpret_cast<float*>(o)[k] += reinterpret_cast<const float*>(b)[k];
+          else
+            reinterpret_cast<double*>(o)[k] += reinterpret_cast<const double*>(b)[k];
+        }
+      } else {
         std::memcpy(o, h.data() + size_t(i) * 25 * tb, 25 * tb);
+      }
     }
   }
   if (B) {

@@ -133,6 +133,8 @@ struct fpsi_ctx {
   fpsi_bc* d_bcs = nullptr;
   double* d_bcmean = nullptr;  // [nbc][2]: sum of A pg and of A over each condition's faces
   bool any_pmean = false;      // a pMean outflow is present
+  bool any_fdbc = false;       // a total-pressure or fixed-mass inflow is present
+  void* d_bjac = nullptr;      // [nbf][25] TB: their difference Jacobian blocks
   // state and residual
   double* d_q = nullptr;       // [nc][5]  T,u,v,w,pg
   // time-accurate mode: the states of time levels n and n-1 (as d_q)

@@ -161,6 +161,16 @@ __global__ void k_bc_state(MeshView M, const double* __restrict__ q, const fpsi_
       }
       break;
     }
+    case FPSI_BC_ISENTROPIC_INFLOW:  // total conditions: p0 = pg + Pambient, T0 = T
+      isentropic_state(qi, nx, ny, nz, bc.pg + g.pamb, bc.T, g, r);
+      break;
+    case FPSI_BC_FIXED_MASS_INFLOW:
+      if (!fixed_mass_state(qi, nx, ny, nz, bc.mass_flux, bc.T, g, r))
+        atomicOr(bcflags, FPSI_BCERR_FIXED_MASS_FAILED_CONVERGENCE);
+      break;
+    case FPSI_BC_FIXED_MASS_OUTFLOW:
+      fixed_mass_outflow_state(qi, nx, ny, nz, bc.mass_flux, bc.mass_relax, g, r);
+      break;
     default:
       break;
   }
@@ -513,11 +523,17 @@ __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
   const double nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
   const double A = M.area[f];
   double fl[5];
-  if (bc_kind(M, f) == FPSI_BC_VISCOUS_WALL) {
+  const int bk = bc_kind(M, f);
+  if (bk == FPSI_BC_VISCOUS_WALL) {
     // pressure only, from the cell-centre pressure (bcViscousWall.loci:220-230),
     // which the wall's boundary state carries
     const double p = s.R.p;
     fl[0] = 0.0, fl[1] = p * nx * A, fl[2] = p * ny * A, fl[3] = p * nz * A, fl[4] = 0.0;
+  } else if (bk >= FPSI_BC_ISENTROPIC_INFLOW) {
+    // the total-pressure and fixed-mass conditions take the analytic flux of
+    // their boundary state (bcIsentropic.loci:162-167, bcFixedMass.loci:155-160,
+    // bcFixedMassOutflow.loci:152-157)
+    state_flux(s.R, nx, ny, nz, A, g, fl);
   } else {
     riemann1(KIND, s.L, s.R, nx, ny, nz, A, g, fl);
   }
@@ -734,6 +750,55 @@ __global__ void k_norm_final(const double* __restrict__ part, int nblk,
 }
 
 // ---------------------------------------------------------------------------
+// Boundary conditions whose state comes from total conditions or a mass
+// flux and whose flux is the state's analytic flux: the Jacobian block of a
+// face is the one-sided difference of that flux in the cell-centre state,
+// steps 1e-5 of T, a, a, a and a^2 (bcIsentropic.loci:196-239,
+// bcFixedMass.loci:163-224); bjac[b] receives the block that srcJ loses.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool fd_jacobian_kind(int kind) {
+  return kind == FPSI_BC_ISENTROPIC_INFLOW || kind == FPSI_BC_FIXED_MASS_INFLOW;
+}
+__device__ __forceinline__ void fd_bc_flux(const fpsi_bc& bc, const double v[5], double nx,
+                                           double ny, double nz, double A, const Gas& g,
+                                           double F[5]) {
+  Q5 qi, qb;
+  qi.T = v[0], qi.u = v[1], qi.v = v[2], qi.w = v[3], qi.p = v[4];
+  if (bc.kind == FPSI_BC_ISENTROPIC_INFLOW)
+    isentropic_state(qi, nx, ny, nz, bc.pg + g.pamb, bc.T, g, qb);
+  else
+    fixed_mass_state(qi, nx, ny, nz, bc.mass_flux, bc.T, g, qb);
+  state_flux(qb, nx, ny, nz, A, g, F);
+}
+template <class TB>
+__global__ void k_bc_fdjac(MeshView M, const double* __restrict__ q, Gas g, TB* __restrict__ bjac) {
+  const int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b >= M.nf - M.nfi) return;
+  const int64_t f = M.nfi + b;
+  const fpsi_bc bc = M.bcs[-M.cr[f] - 1];
+  if (!fd_jacobian_kind(bc.kind)) return;
+  const double nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f], A = M.area[f];
+  double v[5];
+  q_arr(load_q(q, M.cl[f]), v);
+  double F[5], F2[5];
+  fd_bc_flux(bc, v, nx, ny, nz, A, g, F);
+  const double ai = sqrt(g.gamma * g.Rt * v[0]);
+  const double eps = 1e-5;
+  const double d[5] = {v[0] * eps, ai * eps, ai * eps, ai * eps, ai * ai * eps};
+  TB* J = bjac + 25 * b;
+  for (int j = 0; j < 5; ++j) {
+    const double t = v[j];
+    v[j] += d[j];
+    fd_bc_flux(bc, v, nx, ny, nz, A, g, F2);
+    const double rh = 1.0 / (t - v[j]);
+#pragma unroll
+    for (int i = 0; i < 5; ++i) J[5 * i + j] = TB((F[i] - F2[i]) * rh);
+    v[j] = t;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// face Jacobians fjp (dir +1) and fjm (dir -1), one thread per face// ---------------------------------------------------------------------------
 // face Jacobians fjp (dir +1) and fjm (dir -1), one thread per face
 // ---------------------------------------------------------------------------
 // The 25 entries of each thread's block are staged in shared memory and the
@@ -761,11 +826,15 @@ k_face_jacobian(MeshView M, const double* __restrict__ q, const double* __restri
     A = M.area[f];
     ra = roe_average1(s.L, s.R, nx, ny, nz, g);
     TB* st = stage + 25 * threadIdx.x;
-    if (bc_kind(M, f) == FPSI_BC_VISCOUS_WALL) {
+    const int bk = bc_kind(M, f);
+    if (bk == FPSI_BC_VISCOUS_WALL) {
       // d(pressure flux)/dq of the wall (bcViscousWall.loci:232-240); u_f.n = 0
 #pragma unroll
       for (int k = 0; k < 25; ++k) st[k] = TB(0);
       st[9] = TB(nx * A), st[14] = TB(ny * A), st[19] = TB(nz * A);
+    } else if (fd_jacobian_kind(bk)) {  // the difference block comes from k_bc_fdjac
+#pragma unroll
+      for (int k = 0; k < 25; ++k) st[k] = TB(0);
     } else {
       jac_roe1<TB>(ra, nx, ny, nz, A, g, +1, st);
     }
@@ -808,10 +877,14 @@ k_face_jacobian_c(MeshView M, const double* __restrict__ qf, Gas g, TB* __restri
     const double A = M.area[f];
     const RoeAvg ra = roe_average1(s.L, s.R, nx, ny, nz, g);
     TB* st = stage + CK_FACE * threadIdx.x;
-    if (bc_kind(M, f) == FPSI_BC_VISCOUS_WALL) {
+    const int bk = bc_kind(M, f);
+    if (bk == FPSI_BC_VISCOUS_WALL) {
 #pragma unroll
       for (int k = 0; k < CK_DIR; ++k) st[k] = TB(0);
       st[CK_C1] = TB(-A);
+    } else if (fd_jacobian_kind(bk)) {  // the difference block comes from k_bc_fdjac
+#pragma unroll
+      for (int k = 0; k < CK_DIR; ++k) st[k] = TB(0);
     } else {
       jac_roe_compact<TB, true>(ra, A, g, +1, st);
     }
@@ -962,7 +1035,7 @@ k_assemble(MeshView M, SweepView S, const double* __restrict__ q, const double* 
            const double* __restrict__ dtau, const TB* __restrict__ fjp, const TB* __restrict__ fjm,
            const TB* __restrict__ fjc, Gas g, TB* __restrict__ luc, TB* __restrict__ bcv,
            int32_t* __restrict__ pvv, TB* __restrict__ aoff, TB* __restrict__ Dout, TX* __restrict__ x,
-           int32_t* __restrict__ err, double dcoef) {
+           int32_t* __restrict__ err, double dcoef, const TB* __restrict__ bjac) {
   constexpr int RW = 50;  // words staged per face (explicit blocks)
   // compact records move in 16 B units: U16 per record, stored record-major
   // with an odd stride of RS16 units so that a quarter warp's 16 B accesses
@@ -1105,6 +1178,15 @@ k_assemble(MeshView M, SweepView S, const double* __restrict__ q, const double* 
     __syncwarp();
   }
   if (!active) return;
+  if (bjac) {  // difference blocks of the total-pressure and fixed-mass inflows
+    for (int e = 0; e < deg; ++e) {
+      const int64_t f = M.cf[e0 + e] >> 1;
+      if (f < M.nfi || !fd_jacobian_kind(M.bcs[-M.cr[f] - 1].kind)) continue;
+      const TB* J = bjac + 25 * (f - M.nfi);
+#pragma unroll
+      for (int k = 0; k < 25; ++k) sJ[k] -= J[k];
+    }
+  }
   TB D[25];
 #pragma unroll
   for (int i = 0; i < 25; ++i) D[i] = -sJ[i];
@@ -1561,7 +1643,8 @@ static void launch_assemble_kernel(fpsi_ctx* x, const dev::MeshView& M, const de
       M, sweep_view(x), x->d_q, x->d_src, x->d_dtau, (const TB*)x->d_fjp, (const TB*)x->d_fjm,
       (const TB*)x->d_fjc, g, (TB*)x->d_luc, (TB*)x->d_bc, x->d_pv,
       x->P.solver == FPSI_SOLVER_LSGS ? nullptr : (TB*)x->d_aoff, x->keep_D ? (TB*)x->d_D : nullptr,
-      (TX*)x->d_x, x->d_err, x->P.time_accurate ? 1.5 : 1.0);
+      (TX*)x->d_x, x->d_err, x->P.time_accurate ? 1.5 : 1.0,
+      x->any_fdbc ? (const TB*)x->d_bjac : nullptr);
 }
 
 template <class TB, class TX>
@@ -1575,6 +1658,8 @@ static int launch_assemble_t(fpsi_ctx* x) {
   x->asm_compact = cpt;
   x->have_explicit = !cpt;
   prof_begin(x, "face_jacobian");
+  if (x->any_fdbc)
+    dev::k_bc_fdjac<TB><<<blocks_for(x->H.nbf, 128), 128, 0, s>>>(M, x->d_q, g, (TB*)x->d_bjac);
   if (cpt)
     dev::k_face_jacobian_c<TB><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
         M, x->d_qf, g, (TB*)x->d_fjc);

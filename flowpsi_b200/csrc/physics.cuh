@@ -562,7 +562,151 @@ __device__ __forceinline__ void riemann1(int kind, const Q5& L, const Q5& R, dou
     flux_hllc(L, R, nx, ny, nz, area, g, 0.0, 1.0, F);
 }
 
-// Characteristic boundary states, cv_inflow / cv_outflow (bcTools.h:25-81).
+// ---- boundary states from total conditions or a mass flux ---------------
+// Each returns the face state (T, u, v, w, pg) from the cell-centre state qi
+// of the face's cell; n is the outward unit normal, the flow direction of
+// the inflows is -n, the grid does not move.
+
+// The analytic flux of one state through a face (inviscidFlux,
+// inviscidFlux.h:25-45): momentum with the gauge pressure, energy with the
+// absolute one.
+__device__ __forceinline__ void state_flux(const Q5& q, double nx, double ny, double nz,
+                                           double area, const Gas& g, double F[5]) {
+  const double gm1 = g.gamma - 1.0;
+  const double rho = (q.p + g.pamb) / (g.Rt * q.T);
+  const double h0 = g.Rt * q.T * g.gamma / gm1 + 0.5 * (q.u * q.u + q.v * q.v + q.w * q.w);
+  const double e0 = h0 - g.Rt * q.T;
+  const double ut = q.u * nx + q.v * ny + q.w * nz;
+  const double m = area * rho * ut;
+  F[0] = m;
+  F[1] = m * q.u + area * q.p * nx;
+  F[2] = m * q.v + area * q.p * ny;
+  F[3] = m * q.w + area * q.p * nz;
+  F[4] = m * e0 + area * (q.p + g.pamb) * ut;
+}
+
+// Isentropic inflow at total pressure p0 (absolute) and temperature T0
+// (bcIsentropic.loci:52-160): the boundary sound speed from the outgoing
+// Riemann invariant, the Mach number capped at 1, isentropic relations, and a
+// blend towards the inside sound speed when the boundary would be much
+// hotter than the inside.
+__device__ __forceinline__ void isentropic_state(const Q5& qi, double nx, double ny, double nz,
+                                                 double p0, double T0, const Gas& g, Q5& qb) {
+  const double gm1 = g.gamma - 1.0;
+  const double a0 = sqrt(g.gamma * g.Rt * T0);
+  const double ai = sqrt(g.gamma * g.Rt * qi.T);
+  const double dx = -nx, dy = -ny, dz = -nz;  // flow direction
+  const double uit = qi.u * dx + qi.v * dy + qi.w * dz;
+  // boundary sound speed ab and normal velocity unb: the root of a quadratic
+  const double rim = uit - 2.0 * ai / gm1;
+  const double qa = 2.0 / gm1 + 1.0, qb2 = 2.0 * rim, qc = 0.5 * gm1 * rim * rim - a0 * a0;
+  const double D = qb2 * qb2 - 4.0 * qa * qc;
+  double ab, unb;
+  if (D < 0) {
+    ab = a0;
+  } else {
+    ab = (-qb2 + sqrt(D)) / (2.0 * qa);
+    ab = dmax(ab, 0.25 * a0);
+  }
+  unb = rim + 2.0 * ab / gm1;
+  auto finish = [&](double ab_, double unb_, double& Tb, double& pb, double& un_out) {
+    double M = fabs(unb_) / ab_;
+    un_out = unb_;
+    if (M > 1.0) {  // choked: Mach 1 from the total conditions
+      M = 1.0;
+      const double utot = M * a0 / sqrt(1.0 + 0.5 * gm1 * M * M);
+      un_out = sqrt(dmax(utot * utot, 0.0));
+    }
+    const double fm = 1.0 + 0.5 * gm1 * M * M;
+    Tb = T0 / fm;
+    pb = p0 * pow(fm, -g.gamma / gm1);
+  };
+  double Tb, pb, un;
+  finish(ab, unb, Tb, pb, un);
+  double f = (Tb - qi.T) / dmax(qi.T, Tb) - 0.1;
+  if (f > 0) {
+    f = sqrt(f);
+    ab = (1.0 - f) * ab + f * a0;
+    unb = (1.0 - f) * unb + f * uit;
+    finish(ab, unb, Tb, pb, un);
+  }
+  qb.u = un * dx, qb.v = un * dy, qb.w = un * dz;
+  qb.T = Tb;
+  qb.p = pb - g.pamb;
+}
+
+// Fixed mass-flux inflow at total temperature T0 (bcFixedMass.loci:84-135):
+// the boundary temperature by fixed-point iteration (at most 1000 steps, to
+// 1e-9 of the inside temperature) at the inside pressure.  Returns false
+// when the iteration did not converge.
+__device__ __forceinline__ bool fixed_mass_state(const Q5& qi, double nx, double ny, double nz,
+                                                 double mflux, double T0, const Gas& g, Q5& qb) {
+  const double pin = qi.p + g.pamb;
+  const double gp1 = g.gamma + 1.0, gm1 = g.gamma - 1.0;
+  double T = qi.T;
+  const double eps = qi.T * 1e-9;
+  bool ok = false;
+  for (int it = 0; it < 1000; ++it) {
+    const double rho = pin / (g.Rt * T);
+    const double a = sqrt(g.gamma * g.Rt * T);
+    const double M = (mflux / rho) / a;
+    const double lam = sqrt((gp1 * M * M) / (gm1 * M * M + 2.0));
+    const double base = 1.0 - (gm1 / gp1) * lam * lam;
+    const double p0 = pin * pow(base, -g.gamma / gm1);
+    const double rho0 = p0 / (g.Rt * T0);
+    const double rho1 = rho0 * pow(base, 1.0 / gm1);
+    const double T1 = pin / (rho1 * g.Rt);
+    if (fabs(T1 - T) < eps) {
+      ok = true;
+      break;
+    }
+    T = T1;
+  }
+  const double vel = mflux / (pin / (g.Rt * T));
+  // u = d (-vel / (d . n)) with the flow direction d = -n: -vel n
+  qb.u = -vel * nx, qb.v = -vel * ny, qb.w = -vel * nz;
+  qb.T = T;
+  qb.p = qi.p;
+  return ok;
+}
+
+// Fixed mass-flux outflow (bcFixedMassOutflow.loci:86-132): the target
+// mass flux (1 - relax) rho_i u_i.n + relax mflux, bounded by the choked
+// flux, reached by the normal velocity at the inside total conditions.
+__device__ __forceinline__ void fixed_mass_outflow_state(const Q5& qi, double nx, double ny,
+                                                         double nz, double mflux, double relax,
+                                                         const Gas& g, Q5& qb) {
+  const double gm1 = g.gamma - 1.0, gp1 = g.gamma + 1.0;
+  const double pin = qi.p + g.pamb;
+  const double rhoin = pin / (g.Rt * qi.T);
+  const double cin = sqrt(g.gamma * g.Rt * qi.T);
+  const double uin_n = qi.u * nx + qi.v * ny + qi.w * nz;
+  const double target = (1.0 - relax) * rhoin * uin_n + relax * mflux;
+  const double M2 = (qi.u * qi.u + qi.v * qi.v + qi.w * qi.w) / (cin * cin);
+  double fm = 1.0 + 0.5 * gm1 * M2;
+  const double p0 = pin * pow(fm, g.gamma / gm1);
+  const double T0 = qi.T * fm;
+  const double rho0 = rhoin * pow(fm, 1.0 / gm1);
+  const double rhos = rho0 * pow(2.0 / gp1, 1.0 / gm1);
+  double cstar = cin * sqrt(2.0 * fm / gp1);
+  double u = dmin(target, rhos * cstar) / rhoin;
+  fm = 1.0 + 0.5 * gm1 * (u / cin) * (u / cin);
+  cstar = cin * sqrt(2.0 * fm / gp1);
+  u = dmin(u, cstar);
+  const double lam = u / cstar;
+  const double fl = 1.0 - (gm1 / gp1) * lam * lam;
+  const double p = p0 * pow(fl, g.gamma / gm1);
+  if (u < cin) {
+    const double du = u - uin_n;
+    qb.u = qi.u + du * nx, qb.v = qi.v + du * ny, qb.w = qi.w + du * nz;
+    qb.T = T0 * fl;
+    qb.p = p - g.pamb;
+  } else {
+    qb = qi;
+  }
+}
+
+// Characteristic boundary states, cv_inflow / cv_outflow (bcTools.h:25-81).// Characteristic boundary states, cv_inflow / cv_outflow (bcTools.h:25-81).
 __device__ __forceinline__ void cv_state(bool outflow, const Q5& qi, const Q5& q0, double nx,
                                          double ny, double nz, double us_n, const Gas& g,
                                          double beta, Q5& qb) {

@@ -40,11 +40,17 @@ def default_params(**kw) -> N.Params:
 
 
 def bc(kind: str, T: float = 300.0, pg: float = 1e5, u=(0.0, 0.0, 0.0),
-       nu_t: float = 0.0) -> N.BCSpec:
-    """boundary condition; nu_t: SA nu~ entering through it (<= 0: 5e-9)"""
+       nu_t: float = 0.0, mass_flux: float = 0.0, mdot: float = 0.0,
+       mass_relax: float = 1.0) -> N.BCSpec:
+    """boundary condition; nu_t: SA nu~ entering through it (<= 0: 5e-9);
+    for the total-pressure and fixed-mass conditions T is the total
+    temperature T0, pg the total gauge pressure p0 - Pambient
+    (isentropicInflow), mass_flux (or mdot over the condition's area) the
+    prescribed mass flux"""
     b = N.BCSpec()
     b.kind = N.BC[kind]
     b.T, b.pg, b.nu_t = T, pg, nu_t
+    b.mass_flux, b.mdot, b.mass_relax = mass_flux, mdot, mass_relax
     for i in range(3):
         b.u[i] = u[i]
     return b

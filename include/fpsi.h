@@ -82,11 +82,18 @@ enum fpsi_bc_kind {
   FPSI_BC_VISCOUS_WALL = 6,        /* adiabatic no-slip wall, bcViscousWall.loci:146-240 */
   FPSI_BC_OUTFLOW = 7,             /* subsonic outflow at back pressure 'p' (gauge: fpsi_bc.pg),
                                       bcOutflow.loci:174-273 */
-  FPSI_BC_OUTFLOW_MEAN = 8         /* outflow whose area-weighted mean pressure is 'pMean'
+  FPSI_BC_OUTFLOW_MEAN = 8,        /* outflow whose area-weighted mean pressure is 'pMean'
                                       (gauge: fpsi_bc.pg), bcOutflow.loci:178-204 */
+  FPSI_BC_ISENTROPIC_INFLOW = 9,   /* total pressure p0 (gauge: fpsi_bc.pg) and temperature
+                                      T0 (fpsi_bc.T), bcIsentropic.loci:40-240 */
+  FPSI_BC_FIXED_MASS_INFLOW = 10,  /* mass flux (fpsi_bc.mass_flux) at total temperature T0
+                                      (fpsi_bc.T), bcFixedMass.loci:84-235 */
+  FPSI_BC_FIXED_MASS_OUTFLOW = 11  /* mass flux (fpsi_bc.mass_flux) relaxed by mass_relax,
+                                      bcFixedMassOutflow.loci:72-186 */
 };
 /* fpsi_resid.bcErrorCode bits (flowPsiIO.h:212-215) */
 #define FPSI_BCERR_OUTFLOW_BECAME_INFLOW 1
+#define FPSI_BCERR_FIXED_MASS_FAILED_CONVERGENCE 4
 
 typedef struct fpsi_params {
   double gamma;            /* 1.4                                  solverEoS.loci:31 */
@@ -126,6 +133,10 @@ typedef struct fpsi_bc {
   double T, pg, u[3];      /* reference state (temperatureRef, gagePressureRef, uRef) */
   double nu_t;             /* SA nu~ entering through the boundary (BC option nu_t,
                               SA_turb.loci:167-179); <= 0 selects the default 5e-9 */
+  double mass_flux;        /* fixed-mass conditions: 'massFlux' (kg/s/m^2), or <= 0 to use
+                              mdot over the condition's area (massFlux_BC, bcFixedMass.loci:227-230) */
+  double mdot;             /* fixed-mass conditions: 'mdot' (kg/s) */
+  double mass_relax;       /* fixedMassOutflow 'massRelax' (default 1, bcFixedMassOutflow.loci:72-78) */
 } fpsi_bc;
 
 /* Unstructured mesh in the caller's numbering.  Face nodes are ordered so

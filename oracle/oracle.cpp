@@ -478,6 +478,7 @@ struct orc_ctx {
   std::vector<double> tmu;              // nc eddy viscosity (turbulent regime)
   std::vector<double> qb;               // nbf... stored per face (nf*5): boundary face state
   std::vector<double> bc_pmean;         // per condition: area-weighted mean gauge pressure
+  bool bcs_from_mdot = false;           // fixed-mass mass fluxes still to derive from mdot
   uint64_t bc_err = 0;                  // boundary-condition error bits of the last residual
   std::vector<double> grad, phi;        // nc*15, nc*5
   std::vector<double> F, maxev;         // nf*5, nf
@@ -624,6 +625,7 @@ extern "C" int orc_create(orc_ctx** out, const fpsi_mesh* m, const fpsi_params* 
   o->cl.assign(m->cl, m->cl + m->nfaces);
   o->cr.assign(m->cr, m->cr + m->nfaces);
   o->bcs.assign(m->bcs, m->bcs + m->nbc);
+  o->bcs_from_mdot = true;
   compute_geometry(o, m);
   const int64_t nc = o->nc, nf = o->nf;
   // cell -> face lists in face order (the order Loci's upper/lower maps keep)
@@ -730,6 +732,119 @@ extern "C" int orc_get_state(orc_ctx* o, double* T, double* pg, double* u) {
   return FPSI_OK;
 }
 
+// ---- total-pressure and fixed-mass conditions (their own form) ----------
+// analytic flux of one state, inviscidFlux (inviscidFlux.h:25-45)
+static void state_flux(double F[5], double pg, double T, V3 U, V3 an, double area, double pamb,
+                       double Rt, double gamma) {
+  const double gm1 = gamma - 1;
+  const double rho = (pg + pamb) / (Rt * T);
+  const double h0 = Rt * T * gamma / gm1 + 0.5 * dot(U, U);
+  const double e0 = h0 - Rt * T;
+  const double uta = dot(U, an);
+  const double mdot = area * rho * uta;
+  F[0] = mdot;
+  F[1] = mdot * U.x + area * pg * an.x;
+  F[2] = mdot * U.y + area * pg * an.y;
+  F[3] = mdot * U.z + area * pg * an.z;
+  F[4] = mdot * e0 + area * (pg + pamb) * uta;
+}
+
+// isentropic inflow from p0 (absolute), T0 and the inside state, flow along
+// dir (= -n): bcIsentropic.loci:52-160
+static void isentropic_bc(double& pb, double& Tb, V3& ub, double T0, double p0, double gamma,
+                          double Rt, V3 ui, double Ti, V3 dir) {
+  const double gm1 = gamma - 1.;
+  const double a0 = std::sqrt(gamma * Rt * T0), ai = std::sqrt(gamma * Rt * Ti);
+  const double uit = dot(ui, dir);
+  double unb = uit, ab = a0;
+  {  // fixed_p0t0_bc: outgoing invariant and the energy equation
+    const double rim = uit - 2. * ai / gm1;
+    const double a = 2. / gm1 + 1, b = 2. * rim, c = 0.5 * gm1 * rim * rim - a0 * a0;
+    const double D = b * b - 4. * a * c;
+    if (D < 0) {
+      ab = a0;
+      unb = rim + 2. * ab / gm1;
+    } else {
+      ab = std::max((-b + std::sqrt(D)) / (2. * a), .25 * a0);
+      unb = rim + 2. * ab / gm1;
+    }
+  }
+  auto relations = [&](double abx, double unx) {
+    ub = unx * dir;
+    double M = norm(ub) / abx;
+    if (M > 1.0) {
+      M = 1.0;
+      const double utot = M * a0 / std::sqrt(1 + .5 * gm1 * M * M);
+      ub = std::sqrt(std::max(utot * utot, 0.0)) * dir;
+    }
+    Tb = T0 / (1 + .5 * gm1 * M * M);
+    pb = p0 * std::pow(1. + .5 * gm1 * M * M, -gamma / gm1);
+  };
+  relations(ab, unb);
+  double f = (Tb - Ti) / std::max(Ti, Tb) - .1;
+  if (f > 0) {
+    f = std::pow(f, .5);
+    ab = (1 - f) * ab + f * a0;
+    unb = (1 - f) * unb + f * uit;
+    relations(ab, unb);
+  }
+}
+
+// fixed mass-flux inflow at total temperature Tstag: bcFixedMass.loci:84-135;
+// returns false when the temperature iteration did not converge
+static bool fixed_mass_bc(V3& ub, double& Tb, double& pgb, double pin, double Tin, double mflux,
+                          V3 dir, V3 n, double Tstag, double pamb, double gamma, double Rt) {
+  double T = Tin;
+  const double eps = Tin * 1e-9;
+  int iter;
+  for (iter = 0; iter < 1000; ++iter) {
+    const double rho = pin / (Rt * T);
+    const double a = std::sqrt(gamma * Rt * T);
+    const double M = (mflux / rho) / a;
+    const double lam = std::sqrt(((gamma + 1.0) * M * M) / ((gamma - 1.0) * M * M + 2));
+    const double p0 = pin * std::pow((1. - ((gamma - 1.) / (gamma + 1.)) * lam * lam), -gamma / (gamma - 1.0));
+    const double rho0 = p0 / (Rt * Tstag);
+    const double rho1 = rho0 * std::pow((1. - (gamma - 1.0) / (gamma + 1.0) * lam * lam), 1.0 / (gamma - 1.0));
+    const double T1 = pin / (rho1 * Rt);
+    if (std::fabs(T1 - T) < eps) break;
+    T = T1;
+  }
+  const double vel = mflux / (pin / (Rt * T));
+  ub = dir * (-vel / dot(dir, n));
+  Tb = T;
+  pgb = pin - pamb;
+  return iter < 1000;
+}
+
+// fixed mass-flux outflow: bcFixedMassOutflow.loci:86-132
+static void fixed_mass_outflow_bc(V3& ub, double& Tb, double& pgb, double rhoin, double pin,
+                                  double Tin, V3 uin, double gam, double cin, double mflux,
+                                  double pamb, V3 n) {
+  const double M2 = dot(uin, uin) / (cin * cin);
+  double fm = 1. + 0.5 * (gam - 1.) * M2;
+  const double p0 = pin * std::pow(fm, gam / (gam - 1.));
+  const double T0 = Tin * fm;
+  const double rho0 = rhoin * std::pow(fm, 1. / (gam - 1.));
+  const double rhos = rho0 * std::pow(2. / (gam + 1.), 1. / (gam - 1.));
+  double cstar = cin * std::sqrt(2. * fm / (gam + 1.));
+  double u = std::min(mflux, rhos * cstar) / rhoin;
+  fm = 1. + 0.5 * (gam - 1.) * (u / cin) * (u / cin);
+  cstar = cin * std::sqrt(2. * fm / (gam + 1.));
+  u = std::min(u, cstar);
+  const double lambda = u / cstar;
+  const double fl = 1. - ((gam - 1.) / (gam + 1.)) * lambda * lambda;
+  const double p = p0 * std::pow(fl, gam / (gam - 1.));
+  if (u < cin) {
+    ub = uin + (u - dot(uin, n)) * n;
+    Tb = T0 * fl;
+    pgb = p - pamb;
+  } else {
+    ub = uin;
+    Tb = Tin;
+    pgb = pin - pamb;
+  }
+}
+
 // boundary face state (gagePressure_f, temperature_f, u_f) from the cell
 // centre state: farfield bcInflow.loci:311-344, supersonicInflow :270-278,
 // extrapolate bcOutflow.loci:84-95, supersonicOutflow :127-142, outflow at a
@@ -809,6 +924,26 @@ static uint64_t bc_face_state(const orc_ctx* o, int64_t f, double q[5]) {
         q[0] = Tb, q[1] = ub.x, q[2] = ub.y, q[3] = ub.z, q[4] = pgb;
         return FPSI_BCERR_OUTFLOW_BECAME_INFLOW;
       }
+      break;
+    }
+    case FPSI_BC_ISENTROPIC_INFLOW: {
+      double pb;
+      isentropic_bc(pb, Tb, ub, bc.T, bc.pg + P.Pambient, P.gamma, P.Rtilde, ui, Ti, -1.0 * n);
+      pgb = pb - P.Pambient;
+      break;
+    }
+    case FPSI_BC_FIXED_MASS_INFLOW: {
+      const bool ok = fixed_mass_bc(ub, Tb, pgb, pgi + P.Pambient, Ti, bc.mass_flux, -1.0 * n, n,
+                                    bc.T, P.Pambient, P.gamma, P.Rtilde);
+      q[0] = Tb, q[1] = ub.x, q[2] = ub.y, q[3] = ub.z, q[4] = pgb;
+      return ok ? 0 : FPSI_BCERR_FIXED_MASS_FAILED_CONVERGENCE;
+    }
+    case FPSI_BC_FIXED_MASS_OUTFLOW: {
+      const double pin = pgi + P.Pambient, rhoin = pin / (P.Rtilde * Ti);
+      const double t = bc.mass_relax;
+      const double mfb = (1. - t) * rhoin * dot(ui, n) + t * bc.mass_flux;
+      fixed_mass_outflow_bc(ub, Tb, pgb, rhoin, pin, Ti, ui, P.gamma,
+                            std::sqrt(P.gamma * P.Rtilde * Ti), mfb, P.Pambient, n);
       break;
     }
     default:  // extrapolate
@@ -1073,6 +1208,17 @@ extern "C" int orc_residual(orc_ctx* o, double* src_out, fpsi_resid* norms) {
     o->un = o->um = o->u;
     o->have_levels = true;
   }
+  if (o->bcs_from_mdot) {  // massFlux_BC = mdot_BC / boundary_area (bcFixedMass.loci:227-230)
+    std::vector<double> barea(o->bcs.size(), 0.0);
+    for (int64_t f = 0; f < nf; ++f)
+      if (o->cr[f] < 0) barea[-o->cr[f] - 1] += o->area[f];
+    for (size_t b = 0; b < o->bcs.size(); ++b) {
+      fpsi_bc& bc = o->bcs[b];
+      const bool fm = bc.kind == FPSI_BC_FIXED_MASS_INFLOW || bc.kind == FPSI_BC_FIXED_MASS_OUTFLOW;
+      if (fm && !(bc.mass_flux > 0) && barea[b] > 0) bc.mass_flux = bc.mdot / barea[b];
+    }
+    o->bcs_from_mdot = false;
+  }
   o->qb.assign(nf * 5, 0);
   // area-weighted mean gauge pressure next to each condition (areaPressure /
   // boundary_area, bcOutflow.loci:178-198), in face order
@@ -1104,6 +1250,12 @@ extern "C" int orc_residual(orc_ctx* o, double* src_out, fpsi_resid* norms) {
       const V3 a = n * o->area[f];
       double* F = &o->F[5 * f];
       F[0] = 0, F[1] = p * a.x, F[2] = p * a.y, F[3] = p * a.z, F[4] = 0;
+    } else if (bc_kind_of(o, f) >= FPSI_BC_ISENTROPIC_INFLOW) {
+      // analytic flux of the boundary state (bcIsentropic.loci:162-167,
+      // bcFixedMass.loci:155-160, bcFixedMassOutflow.loci:152-157)
+      const double* b = &o->qb[5 * f];
+      state_flux(&o->F[5 * f], b[4], b[0], mk(b[1], b[2], b[3]), n, o->area[f], P.Pambient,
+                 P.Rtilde, P.gamma);
     } else {
       riemann_flux(P.flux, &o->F[5 * f], qL[4], qL[0], mk(qL[1], qL[2], qL[3]), qR[4], qR[0],
                    mk(qR[1], qR[2], qR[3]), n, o->area[f], P.Pambient, P.Rtilde, P.gamma, 0.0,
@@ -1284,6 +1436,40 @@ static int assemble_t(orc_ctx* o, std::vector<TB>& fjp, std::vector<TB>& fjm,
       // srcJ -= d(wall pressure flux)/dq (bcViscousWall.loci:232-240), u_f.n = 0
       TB* J = &fjp[25 * f];
       J[9] = TB(n.x * o->area[f]), J[14] = TB(n.y * o->area[f]), J[19] = TB(n.z * o->area[f]);
+    } else if (bc_kind_of(o, f) == FPSI_BC_ISENTROPIC_INFLOW ||
+               bc_kind_of(o, f) == FPSI_BC_FIXED_MASS_INFLOW) {
+      // one-sided differences of the boundary flux in the cell-centre state
+      // (bcIsentropic.loci:196-239, bcFixedMass.loci:163-224)
+      const fpsi_bc& bc = o->bcs[-o->cr[f] - 1];
+      const int c = o->cl[f];
+      double vals[5] = {o->T[c], o->u[3 * c], o->u[3 * c + 1], o->u[3 * c + 2], o->pg[c]};
+      auto bflux = [&](double F[5]) {
+        double pgb, Tb;
+        V3 ub;
+        const V3 ui = mk(vals[1], vals[2], vals[3]);
+        if (bc.kind == FPSI_BC_ISENTROPIC_INFLOW) {
+          double pb;
+          isentropic_bc(pb, Tb, ub, bc.T, bc.pg + P.Pambient, P.gamma, P.Rtilde, ui, vals[0],
+                        -1.0 * n);
+          pgb = pb - P.Pambient;
+        } else {
+          fixed_mass_bc(ub, Tb, pgb, vals[4] + P.Pambient, vals[0], bc.mass_flux, -1.0 * n, n,
+                        bc.T, P.Pambient, P.gamma, P.Rtilde);
+        }
+        state_flux(F, pgb, Tb, ub, n, o->area[f], P.Pambient, P.Rtilde, P.gamma);
+      };
+      double F[5], F2[5];
+      bflux(F);
+      const double eps = 1e-5, ai = std::sqrt(P.gamma * P.Rtilde * vals[0]);
+      const double deltas[5] = {vals[0] * eps, ai * eps, ai * eps, ai * eps, ai * ai * eps};
+      for (int j = 0; j < 5; ++j) {
+        const double tmp = vals[j];
+        vals[j] += deltas[j];
+        bflux(F2);
+        const double rh = 1. / (tmp - vals[j]);
+        for (int i = 0; i < 5; ++i) fjp[25 * f + 5 * i + j] = TB((F[i] - F2[i]) * rh);
+        vals[j] = tmp;
+      }
     } else {
       roe_jacobian<TB>(&fjp[25 * f], qL[4], qL[0], mk(qL[1], qL[2], qL[3]), qR[4], qR[0],
                        mk(qR[1], qR[2], qR[3]), n, o->area[f], P.Pambient, P.Rtilde, P.gamma,

@@ -70,6 +70,9 @@ CASES = {
                                                       limiter="barth"),
     "outflow_p": lambda prec: cases.outflow_duct(6, precision=prec),
     "outflow_pmean": lambda prec: cases.outflow_duct(6, precision=prec, mean=True),
+    "isentropic_in": lambda prec: cases.outflow_duct(6, precision=prec, inflow="isentropic"),
+    "fixedmass_in": lambda prec: cases.outflow_duct(6, precision=prec, inflow="fixedMass"),
+    "fixedmass_out": lambda prec: cases.outflow_duct(6, precision=prec, outflow="fixedMassOutflow"),
 }
 
 
@@ -133,7 +136,8 @@ def test_residual_matches_oracle(need_gpu, name):
 
 
 @pytest.mark.parametrize("prec", ["fp64", "ref", "mixed"])
-@pytest.mark.parametrize("name", ["farfield_hex", "tgv_tets", "shock_hex"])
+@pytest.mark.parametrize("name", ["farfield_hex", "tgv_tets", "shock_hex", "isentropic_in",
+                                  "fixedmass_in", "fixedmass_out"])
 def test_blocks_match_oracle(need_gpu, name, prec):
     g, o = _pair(CASES[name](prec))
     g.residual()
@@ -208,7 +212,8 @@ def test_sgs_converges_on_gpu(need_gpu):
 
 
 @pytest.mark.parametrize("prec", ["fp64", "ref", "mixed"])
-@pytest.mark.parametrize("name", ["farfield_hex", "tgv_tets", "shock_hex", "outflow_pmean"])
+@pytest.mark.parametrize("name", ["farfield_hex", "tgv_tets", "shock_hex", "outflow_pmean",
+                                  "isentropic_in", "fixedmass_in", "fixedmass_out"])
 def test_newton_steps_match_oracle(need_gpu, name, prec):
     case = CASES[name](prec)
     g, o = _pair(case)
