@@ -149,6 +149,7 @@ _SIGS = {
     "fpsi_gnn_get_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     "fpsi_gnn_set_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     "fpsi_gnn_add_snapshot": (C.c_int, [C.c_void_p, _ctx, _dp]),
+    "fpsi_gnn_add_snapshot_region": (C.c_int, [C.c_void_p, _ctx, _dp, _dp, _dp, C.c_int32]),
     "fpsi_gnn_clear_snapshots": (C.c_int, [C.c_void_p]),
     "fpsi_gnn_num_snapshots": (C.c_int, [C.c_void_p]),
     "fpsi_gnn_snapshot_cells": (C.c_int64, [C.c_void_p, C.c_int32]),

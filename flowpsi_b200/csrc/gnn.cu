@@ -80,6 +80,7 @@ struct Snapshot {
   float* feat = nullptr;    // [nc][40]
   float* target = nullptr;  // [nc][5]  (dq - xJ)/xs
   float* xj = nullptr;      // [nc][5]
+  float* mask = nullptr;    // [nc] 1 where the loss counts (region snapshots), or null: all
   float xs[5], rs[5];
   Graph graph() const { return Graph{nc, d_off, d_nb}; }
 };
@@ -510,11 +511,12 @@ __device__ __forceinline__ bool in_batch(uint64_t seed, int64_t c, uint64_t thr)
 // the squared error and of the batch count
 __global__ void __launch_bounds__(GT) k_loss(int64_t nc, const float* __restrict__ y,
                                              const float* __restrict__ t, uint64_t seed, uint64_t thr,
-                                             float* __restrict__ dy, double* __restrict__ part) {
+                                             const float* __restrict__ mask, float* __restrict__ dy,
+                                             double* __restrict__ part) {
   const int64_t c = int64_t(blockIdx.x) * GT + threadIdx.x;
   double se = 0, cnt = 0;
   if (c < nc) {
-    const bool m = in_batch(seed, c, thr);
+    const bool m = in_batch(seed, c, thr) && (!mask || mask[c] > 0.f);
 #pragma unroll
     for (int k = 0; k < NOUT; ++k) {
       const float d = y[c * NOUT + k] - t[c * NOUT + k];
@@ -822,13 +824,13 @@ int take_error(fpsi_gnn* m) {
 }
 
 // loss over the batch and full gradient into m->d_g; loss_out (device) [2]
-int backward(fpsi_gnn* m, const Graph& G, const float* feat, const float* target, uint64_t seed,
-             uint64_t thr, double* loss_out) {
+int backward(fpsi_gnn* m, const Graph& G, const float* feat, const float* target, const float* mask,
+             uint64_t seed, uint64_t thr, double* loss_out) {
   cudaStream_t s = m->stream;
   const int64_t nc = G.nc;
   const int nblk = int(nb_(nc, GT));
   float* dy = m->d_dz;  // [nc][5] fits in the [nc][64] buffer
-  k_loss<<<nblk, GT, 0, s>>>(nc, m->d_y, target, seed, thr, dy, m->d_lpart);
+  k_loss<<<nblk, GT, 0, s>>>(nc, m->d_y, target, seed, thr, mask, dy, m->d_lpart);
   k_loss_final<<<1, 256, 0, s>>>(m->d_lpart, nblk, loss_out);
   k_scale<<<nb_(nc * NOUT, 256), 256, 0, s>>>(nc * NOUT, dy, loss_out);
   const int rb = int(nb_(nc, RB));
@@ -947,11 +949,11 @@ int ctx_graph(fpsi_ctx* x, Graph* G) {
 }
 
 void free_snapshot(Snapshot& s) {
-  void* ps[] = {s.d_off, s.d_nb, s.feat, s.target, s.xj};
+  void* ps[] = {s.d_off, s.d_nb, s.feat, s.target, s.xj, s.mask};
   for (void* p : ps)
     if (p) cudaFree(p);
   s.d_off = s.d_nb = nullptr;
-  s.feat = s.target = s.xj = nullptr;
+  s.feat = s.target = s.xj = s.mask = nullptr;
 }
 
 }  // namespace
@@ -1174,6 +1176,122 @@ int fpsi_gnn_add_snapshot(fpsi_gnn* m, fpsi_ctx* x, const double* dq) {
   return FPSI_OK;
 }
 
+__global__ void k_gather_rows(int64_t n, const int32_t* __restrict__ idx, int w,
+                              const float* __restrict__ src, float* __restrict__ dst) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n * w) return;
+  const int64_t r = i / w;
+  dst[i] = src[int64_t(idx[r]) * w + (i - r * w)];
+}
+
+int fpsi_gnn_add_snapshot_region(fpsi_gnn* m, fpsi_ctx* x, const double* dq, const double* lo,
+                                 const double* hi, int32_t halo) {
+  if (!m || !x || !dq || !lo || !hi || halo < 0) return FPSI_E_INVALID;
+  const int64_t nc = x->H.nc;
+  Graph G;
+  int rc = ensure_capacity(m, nc);
+  if (!rc) rc = ctx_graph(x, &G);
+  if (rc) return rc;
+  // features of the whole system in the backward pass's scratch
+  float* ffull = m->d_dz;
+  float* xfull = m->d_dh;
+  float rs[5], xs[5];
+  if ((rc = make_features(m, x, ffull, xfull, rs, xs))) return rc;
+  // cells of the box (RCM order) and their interior-face neighbours
+  const fpsi::HostMesh& H = x->H;
+  std::vector<int32_t> sel, newid(nc, -1);
+  for (int64_t c = 0; c < nc; ++c) {
+    bool in = true;
+    for (int d = 0; d < 3; ++d) in = in && H.cc[3 * c + d] >= lo[d] && H.cc[3 * c + d] < hi[d];
+    if (in) {
+      newid[c] = int32_t(sel.size());
+      sel.push_back(int32_t(c));
+    }
+  }
+  const int64_t ns = int64_t(sel.size());
+  if (ns == 0) {
+    fpsi::set_error("learned start: no cell centre inside the snapshot box");
+    return FPSI_E_INVALID;
+  }
+  auto nbrs = [&](int64_t c, auto&& fn) {
+    for (int32_t e = H.cf_off[c]; e < H.cf_off[c + 1]; ++e) {
+      const int64_t f = H.cf[e] >> 1;
+      if (H.cr[f] < 0) continue;
+      fn(int64_t((H.cf[e] & 1) ? H.cl[f] : H.cr[f]));
+    }
+  };
+  // hops from each box cell to the nearest cell outside the box (up to halo+1)
+  std::vector<int32_t> dist(nc, -1), front, next;
+  for (int64_t c = 0; c < nc; ++c)
+    if (newid[c] < 0) dist[c] = 0;
+  for (int64_t c : sel) {
+    bool edge = false;
+    nbrs(c, [&](int64_t o) { edge = edge || newid[o] < 0; });
+    if (edge) dist[c] = 1, front.push_back(int32_t(c));
+  }
+  for (int h = 2; h <= halo + 1 && !front.empty(); ++h) {
+    next.clear();
+    for (int32_t c : front)
+      nbrs(c, [&](int64_t o) {
+        if (dist[o] < 0) dist[o] = h, next.push_back(int32_t(o));
+      });
+    front.swap(next);
+  }
+  std::vector<float> mask(ns);
+  std::vector<int32_t> off(ns + 1, 0), nb;
+  for (int64_t j = 0; j < ns; ++j) {
+    const int64_t c = sel[j];
+    mask[j] = (dist[c] < 0 || dist[c] > halo) ? 1.f : 0.f;
+    nbrs(c, [&](int64_t o) {
+      if (newid[o] >= 0) nb.push_back(newid[o]);
+    });
+    off[j + 1] = int32_t(nb.size());
+  }
+  Snapshot s;
+  int32_t* didx = nullptr;
+  double* dd = nullptr;
+  rc = galloc(&s.d_off, ns + 1);
+  if (!rc) rc = galloc(&s.d_nb, std::max<size_t>(nb.size(), 1));
+  if (!rc) rc = galloc(&s.feat, ns * NIN);
+  if (!rc) rc = galloc(&s.target, ns * 5);
+  if (!rc) rc = galloc(&s.xj, ns * 5);
+  if (!rc) rc = galloc(&s.mask, ns);
+  if (!rc) rc = galloc(&didx, ns);
+  if (!rc) rc = galloc(&dd, ns * 5);
+  std::vector<double> d(ns * 5);
+  for (int64_t j = 0; j < ns; ++j)
+    for (int k = 0; k < 5; ++k) d[5 * j + k] = dq[5 * int64_t(H.perm[sel[j]]) + k];
+  float* dscl = reinterpret_cast<float*>(m->d_lpart);
+  bool ok = !rc;
+  cudaStream_t st = m->stream;
+  ok = ok && cudaMemcpyAsync(s.d_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  ok = ok && (nb.empty() ||
+              cudaMemcpyAsync(s.d_nb, nb.data(), nb.size() * 4, cudaMemcpyHostToDevice, st) == cudaSuccess);
+  ok = ok && cudaMemcpyAsync(s.mask, mask.data(), ns * 4, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(didx, sel.data(), ns * 4, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(dd, d.data(), d.size() * 8, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(dscl, xs, 5 * sizeof(float), cudaMemcpyHostToDevice, st) == cudaSuccess;
+  if (ok) {
+    k_gather_rows<<<nb_(ns * NIN, 256), 256, 0, st>>>(ns, didx, NIN, ffull, s.feat);
+    k_gather_rows<<<nb_(ns * 5, 256), 256, 0, st>>>(ns, didx, 5, xfull, s.xj);
+    k_target<<<nb_(ns * 5, 256), 256, 0, st>>>(ns, dd, s.xj, dscl, s.target);
+    ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(st) == cudaSuccess;
+  }
+  cudaFree(didx);
+  cudaFree(dd);
+  if (!ok) {
+    free_snapshot(s);
+    if (!rc) fpsi::set_error("learned start: region snapshot upload failed");
+    return rc ? rc : FPSI_E_CUDA;
+  }
+  s.nc = ns;
+  s.perm.resize(ns);
+  for (int64_t j = 0; j < ns; ++j) s.perm[j] = int32_t(j);  // snapshot order
+  for (int k = 0; k < 5; ++k) s.rs[k] = rs[k], s.xs[k] = xs[k];
+  m->snaps.push_back(std::move(s));
+  return FPSI_OK;
+}
+
 int fpsi_gnn_num_snapshots(const fpsi_gnn* m) { return m ? int(m->snaps.size()) : 0; }
 
 int64_t fpsi_gnn_snapshot_cells(const fpsi_gnn* m, int32_t si) {
@@ -1216,7 +1334,7 @@ int fpsi_gnn_loss_grad(fpsi_gnn* m, int32_t si, int64_t batch, uint64_t seed, do
   if (!rc) rc = forward(m, s.graph(), s.feat, true);
   if (rc) return rc;
   double* dl = m->d_lpart + ((s.nc + GT - 1) / GT) * 2 + 2;
-  if ((rc = backward(m, s.graph(), s.feat, s.target, seed, threshold(s.nc, batch), dl))) return rc;
+  if ((rc = backward(m, s.graph(), s.feat, s.target, s.mask, seed, threshold(s.nc, batch), dl))) return rc;
   double h[2];
   FPSI_CUDA_TRY(cudaMemcpyAsync(h, dl, sizeof(h), cudaMemcpyDeviceToHost, m->stream));
   FPSI_CUDA_TRY(cudaStreamSynchronize(m->stream));
@@ -1242,7 +1360,7 @@ int fpsi_gnn_train(fpsi_gnn* m, int32_t nsteps, int64_t batch, uint64_t seed, do
     const Snapshot& s = m->snaps[size_t(sd % uint64_t(ns))];
     double* dl = m->d_lpart + ((s.nc + GT - 1) / GT) * 2 + 2;
     int rc = forward(m, s.graph(), s.feat, true);
-    if (!rc) rc = backward(m, s.graph(), s.feat, s.target, sd, threshold(s.nc, batch), dl);
+    if (!rc) rc = backward(m, s.graph(), s.feat, s.target, s.mask, sd, threshold(s.nc, batch), dl);
     if (rc) {
       cudaFree(dhist);
       return rc;

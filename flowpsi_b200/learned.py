@@ -55,6 +55,16 @@ class LearnedStart:
         N.check(N.lib().fpsi_gnn_add_snapshot(self._h, solver._ctx, N.dptr(d)),
                 "fpsi_gnn_add_snapshot")
 
+    def add_snapshot_region(self, solver: FlowPsi, dq, lo, hi, halo: int = 3) -> None:
+        """a snapshot of the cells whose centroids lie in the box [lo, hi);
+        the loss counts only cells more than `halo` hops inside it"""
+        d = np.ascontiguousarray(dq, np.float64).reshape(-1)
+        lo = np.ascontiguousarray(lo, np.float64)
+        hi = np.ascontiguousarray(hi, np.float64)
+        N.check(N.lib().fpsi_gnn_add_snapshot_region(self._h, solver._ctx, N.dptr(d), N.dptr(lo),
+                                                     N.dptr(hi), halo),
+                "fpsi_gnn_add_snapshot_region")
+
     @property
     def n_snapshots(self) -> int:
         return int(N.lib().fpsi_gnn_num_snapshots(self._h))
@@ -163,6 +173,111 @@ def sweeps_to_tolerance(solver: FlowPsi, start: str, rtol: float = 1e-3,
     return solver.sweeps_to_tolerance(rtol, max_sweeps)
 
 
+def _solve_to(solver: FlowPsi, rtol: float, max_sweeps: int, every: int = 10) -> int:
+    """symmetric sweeps from the current iterate, checked every `every`
+    sweeps, until ||B - A x|| <= rtol ||B||; returns the sweeps made"""
+    done = 0
+    while done < max_sweeps:
+        nb, nr = solver.linear_residual()
+        if nr <= rtol * nb:
+            break
+        k = min(every, max_sweeps - done)
+        solver.sweeps(k)
+        done += k
+    return done
+
+
+def tgv_state(cellcenter: np.ndarray, seed: int):
+    """Taylor-Green state at M = 0.1 x amplitude, amplitude 0.5 + U(0,1)
+    from the seed, with 1% seeded noise in every variable: the family of
+    states the learned start is trained and evaluated on"""
+    from . import cases
+
+    amp = 0.5 + float(cases.uniform(seed, 17, 1)[0])
+    T, p, u = cases.taylor_green_tets(2, amplitude=amp).initial_state(cellcenter)
+    nc = cellcenter.shape[0]
+    T = T * (1.0 + 0.01 * cases.normal(seed, 20, nc))
+    p = p * (1.0 + 0.01 * cases.normal(seed, 21, nc))
+    u = u + 0.01 * np.abs(u).max() * np.stack([cases.normal(seed, 22 + k, nc) for k in range(3)], 1)
+    return T, p, u
+
+
+def config4(n: int = 128, train_seeds=range(40), eval_seeds=range(40, 50), snaps_per_seed: int = 10,
+            train_steps: int = 20000, batch: int = 65536, box_hex: int = 32, rtol: float = 1e-6,
+            max_sweeps: int = 300, lin_tol: float = 1e-3, eval_steps: int = 6,
+            precision: str = "ref", log=print) -> dict:
+    """The learned start at the training scale of the specification: the
+    n^3 x 6 jittered split-tet grid, Taylor-Green states from train_seeds
+    (tgv_state), snaps_per_seed Newton systems each from the first steps,
+    dq swept to rtol, kept as region snapshots of box_hex^3 hexes (random
+    corners) so that 400 of them fit in memory; train_steps Adam steps
+    (lr 1e-3) on batches of `batch` cells; then, on the states of
+    eval_seeds, the sweeps to lin_tol and their wall time from the zero,
+    Jacobi and learned starts on the same systems (the run takes the
+    reference's steps).  Returns a summary."""
+    import time
+
+    from . import cases
+
+    case = cases.taylor_green_tets(n, seed=0, precision=precision)
+    s = FlowPsi(case.mesh, case.params)
+    s.keep_blocks(True)
+    cc = s.geometry()["cellcenter"]
+    L = 2.0 * np.pi
+    hb = box_hex * L / n
+    m = LearnedStart(seed=0)
+    t0 = time.perf_counter()
+    for sd in train_seeds:
+        s.set_state(*tgv_state(cc, sd))
+        for k in range(snaps_per_seed):
+            s.residual(want_src=False)
+            s.assemble()
+            _solve_to(s, rtol, max_sweeps)
+            dq = s.get_iterate()
+            lo = cases.uniform(sd, 100 + k, 3) * (L - hb)
+            m.add_snapshot_region(s, dq, lo, lo + hb, 3)
+            s.assemble()
+            s.sweeps(case.params.gauss_seidel_iter)
+            s.update()
+        log(f"seed {sd}: {m.n_snapshots} snapshots, {time.perf_counter() - t0:.0f} s")
+    t1 = time.perf_counter()
+    losses = m.train(train_steps, batch=batch, seed=0, lr=1e-3)
+    t2 = time.perf_counter()
+    log(f"trained: loss {losses[:20].mean():.4g} -> {losses[-200:].mean():.4g} in {t2 - t1:.0f} s")
+    res = {k: {"sweeps": 0, "ms": 0.0} for k in ("zero", "jacobi", "learned")}
+    r0 = {"jacobi": [], "learned": []}
+    for sd in eval_seeds:
+        s.set_state(*tgv_state(cc, sd))
+        for k in range(eval_steps):
+            s.residual(want_src=False)
+            s.assemble()
+            for start in ("zero", "jacobi", "learned"):
+                ta = time.perf_counter()
+                if start == "zero":
+                    s.set_iterate(np.zeros((s.ncells, 5)))
+                elif start == "jacobi":
+                    s.assemble()
+                else:
+                    m.predict(s)
+                if start != "zero":
+                    nb, nr = s.linear_residual()
+                    r0[start].append(nr / nb)
+                sw = _solve_to(s, lin_tol, max_sweeps, every=1)
+                res[start]["ms"] += 1e3 * (time.perf_counter() - ta)
+                res[start]["sweeps"] += sw
+            s.assemble()
+            s.sweeps(case.params.gauss_seidel_iter)
+            s.update()
+    out = {"cells": s.ncells, "snapshots": m.n_snapshots, "box_hex": box_hex,
+           "snapshot_s": t1 - t0, "train_s": t2 - t1, "train_steps": train_steps, "batch": batch,
+           "loss_first": float(losses[:20].mean()), "loss_last": float(losses[-200:].mean()),
+           "eval": res, "initial_residual": {k: float(np.mean(v)) for k, v in r0.items()},
+           "lin_tol": lin_tol, "eval_seeds": [int(x) for x in eval_seeds], "eval_steps": eval_steps}
+    m.close()
+    s.close()
+    return out
+
+
 def _time_inference(argv=None) -> dict:
     """Wall time of the learned start's inference (features, the three
     tensor-core layers with the head, the start written into the solver's
@@ -209,4 +324,16 @@ def _time_inference(argv=None) -> dict:
 
 
 if __name__ == "__main__":
-    _time_inference()
+    import sys
+
+    if "--config4" in sys.argv:
+        import json
+
+        args = [a for a in sys.argv[1:] if a != "--config4"]
+        kw = {}
+        for a in args:  # key=value overrides, e.g. n=64 train_steps=2000
+            k, v = a.split("=")
+            kw[k] = range(*map(int, v.split(":"))) if ":" in v else (float(v) if "." in v or "e" in v else int(v))
+        print(json.dumps(config4(**kw)), flush=True)
+    else:
+        _time_inference()

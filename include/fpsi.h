@@ -381,6 +381,15 @@ int64_t fpsi_gnn_num_params(const fpsi_gnn* m);
 int fpsi_gnn_get_params(fpsi_gnn* m, float* w);
 int fpsi_gnn_set_params(fpsi_gnn* m, const float* w);
 int fpsi_gnn_add_snapshot(fpsi_gnn* m, fpsi_ctx* ctx, const double* dq);
+/* a snapshot of the cells of ctx's assembled system whose centroids lie in
+ * the box lo <= x < hi: their features (those of the whole system), the
+ * graph among them, dq and the Jacobi start; the loss counts only cells
+ * more than `halo` hops from every cell outside the box, whose network
+ * inputs the box holds in full (halo = 3 for the three layers).  Keeps the
+ * training set of a large grid small; its cells are listed in the
+ * library's order (fpsi_gnn_get_snapshot). */
+int fpsi_gnn_add_snapshot_region(fpsi_gnn* m, fpsi_ctx* ctx, const double* dq, const double* lo,
+                                 const double* hi, int32_t halo);
 int fpsi_gnn_clear_snapshots(fpsi_gnn* m);
 int fpsi_gnn_num_snapshots(const fpsi_gnn* m);
 /* cells of snapshot s (-1 when s is out of range) */

@@ -51,7 +51,10 @@ def bf16(x: torch.Tensor) -> torch.Tensor:
     return x + (x.to(torch.bfloat16).to(torch.float32) - x).detach()
 
 
-def loss_and_grad(w: np.ndarray, feat: np.ndarray, target: np.ndarray, A: torch.Tensor):
+def loss_and_grad(w: np.ndarray, feat: np.ndarray, target: np.ndarray, A: torch.Tensor,
+                  mask: np.ndarray | None = None):
+    """mean squared error over all cells, or over the cells where mask is
+    true, and its gradient"""
     flat, p = unpack(w)
     h = torch.from_numpy(np.ascontiguousarray(feat, np.float32))
     for l in range(NLAYER):
@@ -61,7 +64,11 @@ def loss_and_grad(w: np.ndarray, feat: np.ndarray, target: np.ndarray, A: torch.
         h = bf16(torch.nn.functional.gelu(bf16(h) @ ws.T + agg @ wn.T + b, approximate="tanh"))
     y = h @ p[-2].T + p[-1]
     t = torch.from_numpy(np.ascontiguousarray(target, np.float32))
-    loss = ((y - t) ** 2).mean()
+    if mask is None:
+        loss = ((y - t) ** 2).mean()
+    else:
+        mk = torch.from_numpy(np.asarray(mask, bool))
+        loss = ((y - t)[mk] ** 2).mean()
     loss.backward()
     return float(loss), flat.grad.numpy().copy(), y.detach().numpy()
 

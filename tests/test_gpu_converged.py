@@ -115,3 +115,26 @@ def test_converged_state_matches_oracle(need_gpu, name, prec):
     rho_g, E_g = _rho_energy(*g.get_state())
     assert _rel(rho_g, rho_o) < 1e-8, _rel(rho_g, rho_o)
     assert _rel(E_g, E_o) < 1e-8, _rel(E_g, E_o)
+
+
+def test_oblique_shock_history_matches_oracle(need_gpu):
+    """The oblique-shock cube (HLLE + Barth, CFL 50) does not settle: its
+    supersonic-outflow sides lower the face pressure by 10% wherever the
+    normal velocity is subsonic (bcOutflow.loci:127-133), which holds on the
+    side the post-shock flow enters and where the flow is tangential.  The
+    oracle and the GPU take the same wild first steps (temperatures leave
+    [283, 483] K), so the behaviour is the method's on this configuration,
+    not the device path's: 10 FP64 steps on 16^3 agree to 1e-6 per step."""
+    case = cases.oblique_shock_cube(16, precision="fp64")
+    g = FlowPsi(case.mesh, case.params)
+    o = Oracle(case.mesh, case.params)
+    T, p, u = case.initial_state(o.geometry()["cellcenter"])
+    g.set_state(T, p, u)
+    o.set_state(T, p, u)
+    col = g.colours()
+    hg = g.run(10)
+    ho = [o.newton_step(colour=col) for _ in range(10)]
+    for k, (a, b) in enumerate(zip(hg, ho)):
+        assert abs(a["rtrms"] - b["rtrms"]) <= 1e-6 * b["rtrms"], (k, a["rtrms"], b["rtrms"])
+    Tg = g.get_state()[0]
+    assert Tg.min() < 250.0 or Tg.max() > 500.0  # the excursion itself

@@ -116,6 +116,63 @@ def test_loss_and_gradient_match_autograd(need_gpu, mesh):
         assert np.abs(gg - go).max() <= 3e-3 * np.abs(go).max() + 1e-12, name
 
 
+def test_region_snapshot_matches_the_replica(need_gpu):
+    """A region snapshot keeps the cells whose centroids lie in a box, the
+    graph among them, and counts the loss only on cells more than 3 hops
+    from the box's outside: its rows are the whole system's rows of those
+    cells, and its loss and gradient are the replica's on that subgraph
+    with that mask."""
+    case, g, _ = _system(n=8)
+    dq = converged_update(g, 1e-10, 400)
+    model = LearnedStart(seed=5)
+    model.add_snapshot(g, dq)
+    L = 2.0 * np.pi
+    lo, hi = np.array([0.1, 0.0, 0.2]) * L, np.array([0.85, 0.8, 0.95]) * L
+    model.add_snapshot_region(g, dq, lo, hi, halo=3)
+    w = _random_head(model)
+    f0, t0, x0, _ = model.snapshot(0)
+    f1, t1, x1, _ = model.snapshot(1)
+    cc = g.geometry()["cellcenter"]
+    inbox = np.all((cc >= lo) & (cc < hi), axis=1)
+    assert f1.shape[0] == inbox.sum()
+    key = {f0[i].tobytes(): i for i in np.where(inbox)[0]}
+    assert len(key) == inbox.sum()  # feature rows identify the cells
+    idx = np.array([key[r.tobytes()] for r in f1])
+    np.testing.assert_array_equal(t1, t0[idx])
+    np.testing.assert_array_equal(x1, x0[idx])
+    # the subgraph in snapshot order and the mask: hops to the nearest outside cell
+    a = case.mesh.arrays()
+    inner = a.cr >= 0
+    cl, cr = np.asarray(a.cl)[inner], np.asarray(a.cr)[inner]
+    pos = -np.ones(a.ncells, np.int64)
+    pos[idx] = np.arange(len(idx))
+    keep = (pos[cl] >= 0) & (pos[cr] >= 0)
+    A = G.neighbour_mean_matrix(len(idx), pos[cl[keep]], pos[cr[keep]])
+    nbr = [[] for _ in range(a.ncells)]
+    for x, y in zip(cl.tolist(), cr.tolist()):
+        nbr[x].append(y)
+        nbr[y].append(x)
+    dist = np.where(inbox, -1, 0)
+    front = [c for c in np.where(inbox)[0] if any(not inbox[o] for o in nbr[c])]
+    dist[front] = 1
+    for h in range(2, 5):
+        nxt = []
+        for c in front:
+            for o in nbr[c]:
+                if dist[o] < 0:
+                    dist[o] = h
+                    nxt.append(o)
+        front = nxt
+    mask = (dist[idx] < 0) | (dist[idx] > 3)
+    assert 0 < mask.sum() < len(idx)
+    loss, grad = model.loss_grad(1)
+    loss_o, grad_o, _ = G.loss_and_grad(w, f1, t1, A, mask=mask)
+    assert abs(loss - loss_o) <= 1e-5 * loss_o
+    for name, lo_, hi_ in G.groups():
+        go, gg = grad_o[lo_:hi_], grad[lo_:hi_]
+        assert np.linalg.norm(gg - go) <= 1e-3 * np.linalg.norm(go) + 1e-12, name
+
+
 def test_minibatch_gradient_is_the_batch_mean(need_gpu):
     """the batch is a hashed subset of cells: its loss and gradient are those
     of the masked mean squared error"""
