@@ -20,7 +20,7 @@ ERRORS = {
 
 FLUX = {"hllc": 0, "roe": 1, "hlle": 2}
 LIMITER = {"venkatakrishnan": 0, "barth": 1, "none": 2, "zero": 3}
-SOLVER = {"sgs": 0, "lsgs": 1}
+SOLVER = {"sgs": 0, "lsgs": 1, "fsgs": 2}
 PRECISION = {"fp64": 0, "ref": 1, "mixed": 2}
 BC = {"farfield": 1, "supersonicInflow": 2, "supersonicOutflow": 3, "extrapolate": 4,
       "reflecting": 5, "viscousWall": 6, "outflow": 7, "outflowMean": 8,

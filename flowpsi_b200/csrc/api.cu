@@ -222,8 +222,8 @@ int check_params(const fpsi_params* p) {
     fpsi::set_error("low-Mach preconditioning (Minf < 0.5) is not on the device path");
     return FPSI_E_UNSUPPORTED;
   }
-  if (p->solver != FPSI_SOLVER_SGS && p->solver != FPSI_SOLVER_LSGS) {
-    fpsi::set_error("fluidLinearSolver: 'sgs' or 'lsgs'");
+  if (p->solver != FPSI_SOLVER_SGS && p->solver != FPSI_SOLVER_LSGS && p->solver != FPSI_SOLVER_FSGS) {
+    fpsi::set_error("fluidLinearSolver: 'sgs', 'lsgs' or 'fsgs'");
     return FPSI_E_INVALID;
   }
   if (p->solver == FPSI_SOLVER_LSGS && (p->lsgs_max_iter < 0 || !(p->lsgs_relaxation > 0))) {
@@ -958,8 +958,12 @@ int fpsi_linear_solve(fpsi_ctx* x, const double* x0, double* dq, fpsi_lsinfo* in
   if (x0) {
     if ((rc = upload_x(x, x0))) return rc;
   } else if (x->have_dq && !x->x_preset) {
-    // iterate was consumed by an earlier solve: rebuild the block Jacobi start
-    if ((rc = fpsi::launch_jacobi_start(x))) return rc;
+    // iterate was consumed by an earlier solve: rebuild the reference start
+    if (x->P.solver == FPSI_SOLVER_FSGS) {
+      FPSI_CUDA_TRY(cudaMemsetAsync(x->d_x, 0, size_t(x->H.nc) * 5 * x->x_bytes, x->stream));
+    } else if ((rc = fpsi::launch_jacobi_start(x))) {
+      return rc;
+    }
   }
   x->x_preset = false;
   if ((rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter))) return rc;

@@ -1070,7 +1070,7 @@ int fpsi_gnn_set_params(fpsi_gnn* m, const float* w) {
 // features of ctx's assembled system into (feat, xj, scales)
 // (activation buffers must hold x's cells)
 static int make_features(fpsi_gnn* m, fpsi_ctx* x, float* feat, float* xj, float* rs, float* xs) {
-  if (!x->have_asm || !x->d_D || x->P.solver != FPSI_SOLVER_SGS) {
+  if (!x->have_asm || !x->d_D || x->P.solver == FPSI_SOLVER_LSGS) {
     fpsi::set_error("learned start: needs an assembled SGS system with the diagonal blocks kept");
     return FPSI_E_STATE;
   }
@@ -1510,7 +1510,7 @@ extern "C" {
 // the three layers with the head, and the start written over D^-1 B.
 int fpsi_gnn_predict(fpsi_gnn* m, fpsi_ctx* x, double* x0) {
   if (!m || !x) return FPSI_E_INVALID;
-  if (!x->have_asm || !x->d_D || x->P.solver != FPSI_SOLVER_SGS) {
+  if (!x->have_asm || !x->d_D || x->P.solver == FPSI_SOLVER_LSGS) {
     fpsi::set_error("learned start: needs an assembled SGS system with the diagonal blocks kept");
     return FPSI_E_STATE;
   }

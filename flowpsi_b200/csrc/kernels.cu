@@ -1630,7 +1630,7 @@ static dev::SweepView sweep_view(const fpsi_ctx* x) {
 // the compact Roe form (15 values per sweep slot instead of 25); viscous
 // terms and the line solver need the explicit blocks.
 static bool compact_blocks(const fpsi_ctx* x) {
-  return !x->P.viscous && x->P.solver == FPSI_SOLVER_SGS;
+  return !x->P.viscous && x->P.solver != FPSI_SOLVER_LSGS;
 }
 
 template <class TB, class TX, bool CPT>
@@ -1681,14 +1681,22 @@ static int launch_assemble_t(fpsi_ctx* x) {
 }
 
 int launch_assemble(fpsi_ctx* x) {
+  int rc;
   switch (x->P.precision) {
     case FPSI_PREC_FP64:
-      return launch_assemble_t<double, double>(x);
+      rc = launch_assemble_t<double, double>(x);
+      break;
     case FPSI_PREC_MIXED:
-      return launch_assemble_t<float, float>(x);
+      rc = launch_assemble_t<float, float>(x);
+      break;
     default:
-      return launch_assemble_t<float, double>(x);
+      rc = launch_assemble_t<float, double>(x);
   }
+  // FSGS starts its sweeps from zero (linearSolverFSGS.loci:1611), the
+  // others from the block Jacobi solution the assembly left in x
+  if (!rc && x->P.solver == FPSI_SOLVER_FSGS)
+    FPSI_CUDA_TRY(cudaMemsetAsync(x->d_x, 0, size_t(x->H.nc) * 5 * x->x_bytes, x->stream));
+  return rc;
 }
 
 template <class TB, class TX>

@@ -62,7 +62,11 @@ enum fpsi_limiter_kind {       /* vars 'limiter' (guide.tex:495-518) */
 };
 enum fpsi_solver_kind {        /* vars 'fluidLinearSolver' (solverNewton.loci:222-249) */
   FPSI_SOLVER_SGS = 0,         /* multi-colour block SGS */
-  FPSI_SOLVER_LSGS = 1         /* line SGS (batched block-tridiagonal lines) */
+  FPSI_SOLVER_LSGS = 1,        /* line SGS (batched block-tridiagonal lines) */
+  FPSI_SOLVER_FSGS = 2         /* 'fsgs' (linearSolverFSGS.loci:1601-1700): gauss_seidel_iter
+                                  symmetric sweeps from a zero start; the reference sweeps
+                                  single cells in breadth-first order with an unpivoted block
+                                  LU, this path the colours with the pivoted LU of SGS */
 };
 enum fpsi_precision {
   FPSI_PREC_FP64 = 0,          /* every block and iterate in FP64 */

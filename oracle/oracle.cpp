@@ -1591,8 +1591,12 @@ static int solve_t(orc_ctx* o, const int32_t* colour, const double* x0,
                    const std::vector<TB>& LU, const std::vector<TB>& B) {
   const int64_t nc = o->nc;
   std::vector<TX> x(nc * 5);
+  const bool fsgs = o->P.solver == FPSI_SOLVER_FSGS;
   if (x0) {
     for (int64_t i = 0; i < nc * 5; ++i) x[i] = TX(x0[i]);
+  } else if (fsgs) {
+    // FSGS starts from zero (linearSolverFSGS.loci:1611)
+    std::fill(x.begin(), x.end(), TX(0));
   } else {
     // block Jacobi start D x = B (linearSolverSGS.loci:57-69)
     for (int64_t c = 0; c < nc; ++c) {
@@ -1603,9 +1607,39 @@ static int solve_t(orc_ctx* o, const int32_t* colour, const double* x0,
   }
   const int nit = o->P.gauss_seidel_iter;
   if (!colour) {
+    // the sequential order: cell order for SGS; for FSGS the breadth-first
+    // order of its single-cell lines (linearSolverFSGS.loci:808-845): from
+    // the lowest unvisited cell, level by level, each level in increasing
+    // cell number
+    std::vector<int64_t> order(nc);
+    if (fsgs) {
+      std::vector<char> seen(nc, 0);
+      int64_t cnt = 0, sp = 0;
+      std::vector<int64_t> level, next;
+      while (cnt < nc) {
+        if (level.empty()) {
+          while (seen[sp]) ++sp;
+          level.push_back(sp);
+          seen[sp] = 1;
+        }
+        next.clear();
+        for (int64_t c : level) {
+          order[cnt++] = c;
+          auto visit = [&](int64_t n) {
+            if (!seen[n]) seen[n] = 1, next.push_back(n);
+          };
+          for (int64_t k = o->lo_off[c]; k < o->lo_off[c + 1]; ++k) visit(o->cl[o->lo[k]]);
+          for (int64_t k = o->up_off[c]; k < o->up_off[c + 1]; ++k) visit(o->cr[o->up[k]]);
+        }
+        std::sort(next.begin(), next.end());
+        level.swap(next);
+      }
+    } else {
+      for (int64_t c = 0; c < nc; ++c) order[c] = c;
+    }
     for (int it = 0; it < nit; ++it) {
-      for (int64_t c = 0; c < nc; ++c) gs_cell<TB, TX>(o, c, fjp, fjm, LU, B, x.data());
-      for (int64_t c = nc - 1; c >= 0; --c) gs_cell<TB, TX>(o, c, fjp, fjm, LU, B, x.data());
+      for (int64_t i = 0; i < nc; ++i) gs_cell<TB, TX>(o, order[i], fjp, fjm, LU, B, x.data());
+      for (int64_t i = nc - 1; i >= 0; --i) gs_cell<TB, TX>(o, order[i], fjp, fjm, LU, B, x.data());
     }
   } else {
     int ncol = 0;

@@ -208,3 +208,28 @@ def test_bdf2_oracle_properties():
     o.set_state(*c.initial_state(o.geometry()["cellcenter"]))
     h = o.time_step()
     assert h[-1]["rtrms"] < 1e-3 * h[0]["rtrms"]
+
+
+def test_fsgs_reaches_the_sgs_steady_state():
+    """FSGS (zero start, breadth-first order, linearSolverFSGS.loci) and SGS
+    (Jacobi start, cell order) relax the same systems, so the steady state
+    they converge to is the same"""
+    from flowpsi_b200 import cases
+    from oracle import Oracle
+
+    out = []
+    for solver in (0, 2):
+        c = cases.farfield_cube(6, precision="fp64")
+        c.params.solver = solver
+        o = Oracle(c.mesh, c.params)
+        o.set_state(*c.initial_state(o.geometry()["cellcenter"]))
+        r0 = None
+        for _ in range(200):
+            r = o.newton_step()
+            r0 = r0 or r["rtrms"]
+            if r["rtrms"] < 1e-11 * r0:
+                break
+        assert r["rtrms"] < 1e-10 * r0
+        out.append(o.get_state())
+    for a, b in zip(*out):
+        assert np.abs(a - b).max() <= 1e-9 * np.abs(b).max()
