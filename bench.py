@@ -204,7 +204,7 @@ def kernel_bytes(name, nc, nfi, nbf, sweeps, tb, tx, sgs_step_bytes=None, compac
     inviscid SGS system keeps its face Jacobians as 24-value face records
     (9 coefficients per direction + U + n) and 15-value sweep slots"""
     nf = nfi + nbf
-    geo_face = 8 + 32 + 48  # cl,cr + n*A + rL,rR
+    qf = 96  # reconstructed face states of both sides (+ spectral radii) per face
     if compact:
         jac_out = nf * 24 * tb
         # each face side needs its direction's 9 coefficients and U, n
@@ -214,12 +214,13 @@ def kernel_bytes(name, nc, nfi, nbf, sweeps, tb, tx, sgs_step_bytes=None, compac
         asm_faces = (2 * nfi + nbf) * 25 * tb + 2 * nfi * 25 * tb
     return {
         "bc_state": nbf * (4 + 24 + 40 + 40),
-        # q + Minv + vol + grad/limiter writes; face geometry and indices
-        "grad_limiter": nc * (40 + 48 + 8 + 120 + 40) + nf * (8 + 48),
-        # survey K3: q 40 + grad 120 + phi 40 per cell, 88 per face, flux write 40 + mev 8
-        "face_flux": nc * (40 + 120 + 40) + nf * (geo_face + 48),
+        # q + Minv + vol per cell; per face cl,cr 8 + rL,rR 48 + n 24, the
+        # two face-list entries 8 and the face-state write; boundary states
+        "grad_limiter": nc * (40 + 48 + 8) + nf * (8 + 48 + 24 + 8 + qf) + nbf * 40,
+        # face states, n and area in, the 48 B flux record out
+        "face_flux": nf * (qf + 32 + 48),
         "cell_residual": nc * (40 + 8 + 40 + 8) + nf * 48,
-        "face_jacobian": nc * (40 + 120 + 40) + nf * geo_face + jac_out,
+        "face_jacobian": nf * (qf + 32) + jac_out,
         # q, src, dtau, vol; LU + B slots, pivots, Jacobi start; each face
         # block read once for the diagonal sum, interior ones written once
         # more into the off-diagonal slots

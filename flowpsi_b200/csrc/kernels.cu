@@ -572,20 +572,40 @@ k_cell_residual(MeshView M, const double* __restrict__ q, const double* __restri
   if (c < M.nc) {
     double s[5] = {0, 0, 0, 0, 0};
     double meva = 0;
-    for (int32_t e = M.cf_off[c]; e < M.cf_off[c + 1]; ++e) {
-      const int32_t ent = M.cf[e];
-      const int64_t f = ent >> 1;
-      const double2* p2 = reinterpret_cast<const double2*>(F + FREC * f);
-      const double2 a = p2[0], b = p2[1], c = p2[2];
-      const double p[5] = {a.x, a.y, b.x, b.y, c.x};
-      if (ent & 1) {
+    const int32_t e0 = M.cf_off[c], e1 = M.cf_off[c + 1];
+    // the first NPF face records are all requested before any is summed
+    // (a tet has 4 faces), then summed in the cell's face order; faces
+    // beyond NPF follow one by one in the same order
+    constexpr int NPF = 4;
+    int32_t ent[NPF];
+#pragma unroll
+    for (int j = 0; j < NPF; ++j) ent[j] = e0 + j < e1 ? __ldg(M.cf + e0 + j) : -1;
+    double2 rec[NPF][3];
+#pragma unroll
+    for (int j = 0; j < NPF; ++j)
+      if (ent[j] >= 0) {
+        const double2* p2 = reinterpret_cast<const double2*>(F + FREC * int64_t(ent[j] >> 1));
+        rec[j][0] = __ldg(p2), rec[j][1] = __ldg(p2 + 1), rec[j][2] = __ldg(p2 + 2);
+      }
+    auto add = [&](int32_t en, const double2* r3) {
+      const double p[5] = {r3[0].x, r3[0].y, r3[1].x, r3[1].y, r3[2].x};
+      if (en & 1) {
 #pragma unroll
         for (int k = 0; k < 5; ++k) s[k] += p[k];
       } else {
 #pragma unroll
         for (int k = 0; k < 5; ++k) s[k] -= p[k];
       }
-      meva += c.y;
+      meva += r3[2].y;
+    };
+#pragma unroll
+    for (int j = 0; j < NPF; ++j)
+      if (ent[j] >= 0) add(ent[j], rec[j]);
+    for (int32_t e = e0 + NPF; e < e1; ++e) {
+      const int32_t en = __ldg(M.cf + e);
+      const double2* p2 = reinterpret_cast<const double2*>(F + FREC * int64_t(en >> 1));
+      const double2 r3[3] = {__ldg(p2), __ldg(p2 + 1), __ldg(p2 + 2)};
+      add(en, r3);
     }
     const double V = M.vol[c];
     const double cflpdt = 0.5 * meva / V;

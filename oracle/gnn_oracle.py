@@ -51,6 +51,15 @@ def bf16(x: torch.Tensor) -> torch.Tensor:
     return x + (x.to(torch.bfloat16).to(torch.float32) - x).detach()
 
 
+def gelu_tanh(z: torch.Tensor) -> torch.Tensor:
+    """GELU in its tanh form (Hendrycks and Gimpel 2016),
+    0.5 z (1 + tanh(u)) with u = sqrt(2/pi) (z + 0.044715 z^3), evaluated as
+    the device does, z sigmoid(2u): the same function without the
+    cancellation of 1 + tanh(u) for negative z"""
+    u = 0.7978845608028654 * (z + 0.044715 * z * z * z)
+    return z * torch.sigmoid(2.0 * u)
+
+
 def loss_and_grad(w: np.ndarray, feat: np.ndarray, target: np.ndarray, A: torch.Tensor,
                   mask: np.ndarray | None = None):
     """mean squared error over all cells, or over the cells where mask is
@@ -60,8 +69,7 @@ def loss_and_grad(w: np.ndarray, feat: np.ndarray, target: np.ndarray, A: torch.
     for l in range(NLAYER):
         ws, wn, b = p[3 * l], p[3 * l + 1], p[3 * l + 2]
         agg = bf16(torch.sparse.mm(A, h))  # mean of the layer input, rounded
-        # GELU in its tanh form (Hendrycks and Gimpel 2016), as the device
-        h = bf16(torch.nn.functional.gelu(bf16(h) @ ws.T + agg @ wn.T + b, approximate="tanh"))
+        h = bf16(gelu_tanh(bf16(h) @ ws.T + agg @ wn.T + b))
     y = h @ p[-2].T + p[-1]
     t = torch.from_numpy(np.ascontiguousarray(target, np.float32))
     if mask is None:

@@ -138,6 +138,18 @@ def test_residual_matches_oracle(need_gpu, name):
 @pytest.mark.parametrize("prec", ["fp64", "ref", "mixed"])
 @pytest.mark.parametrize("name", ["farfield_hex", "tgv_tets", "shock_hex", "isentropic_in",
                                   "fixedmass_in", "fixedmass_out"])
+# The total-pressure and fixed-mass inflows take one-sided differences of
+# their boundary flux with steps of 1e-5 of the state (bcIsentropic.loci:
+# 219-239, bcFixedMass.loci:199-224): a difference of the flux in its last
+# digits is divided by 1e-5.  The isentropic state is closed-form, so device
+# and oracle (whose pow and sqrt differ by an ulp) agree to ~1e-16/1e-5 of
+# the block scale; the fixed-mass state comes from a fixed-point iteration
+# that stops within 1e-9 of T, so the two agree to ~1e-9/1e-5.  These
+# tolerances hold for those faces' blocks and for the diagonal blocks that
+# sum them.
+FD_TOL = {"isentropic_in": 1e-8, "fixedmass_in": 1e-3}
+
+
 def test_blocks_match_oracle(need_gpu, name, prec):
     g, o = _pair(CASES[name](prec))
     g.residual()
@@ -146,13 +158,19 @@ def test_blocks_match_oracle(need_gpu, name, prec):
     o.assemble()
     bg, bo = g.blocks(), o.blocks()
     tol = 1e-11 if prec == "fp64" else 1e-6
+    a = o._mesh.arrays()
+    fd = np.zeros(a.nfaces, bool)
+    if name in FD_TOL:  # the inflow is condition 0 of the duct
+        fd = np.asarray(a.cr) == -1
     for k in ("fjp", "fjm"):
         assert bg[k].dtype == bo[k].dtype
-        inner = np.abs(bo[k]).reshape(len(bo[k]), -1).max(1) > 0
+        inner = (np.abs(bo[k]).reshape(len(bo[k]), -1).max(1) > 0) & ~fd
         assert block_rel(bg[k][inner], bo[k][inner]) < tol, k
+    if fd.any():
+        assert block_rel(bg["fjp"][fd], bo["fjp"][fd]) < FD_TOL[name]
+        tol = max(tol, FD_TOL[name])
     # fluid_D sums the cell's face blocks (srcJ, solverLinearSystem.loci:106-121)
     # with cancellation; its error is measured against the size of the summands
-    a = o._mesh.arrays()
     mx = lambda b: np.abs(b.astype(np.float64)).reshape(len(b), -1).max(1)  # noqa: E731
     scale = mx(bo["fluid_D"])
     np.add.at(scale, a.cl, mx(bo["fjp"]))
