@@ -725,7 +725,56 @@ __global__ void k_rms_partial(int64_t nc, const float* __restrict__ raw, const f
     for (int k = 0; k < 10; ++k) part[10 * blockIdx.x + k] = sh[k][0];
 }
 
-// normalise: B/rs, D_ij xs_j / rs_i, x_J/xs, dq_prev/xs, each as one
+// Scales rs, xs from the per-block sums of squares, and the 40 per-feature
+// factors of k_features_norm, in one block: thread t sums blocks t, t + T,
+// ... in order, then a fixed tree combines the threads, so the scales are
+// the same on every call for the same system (training features and
+// inference features use this one kernel).  fac[0..9] = rs|xs,
+// fac[10..49] the factors.
+constexpr int FS_THREADS = 512;
+__global__ void __launch_bounds__(FS_THREADS) k_feat_scales(const double* __restrict__ part, int nblk,
+                                                         int64_t nc, float* __restrict__ fac) {
+  __shared__ double sh[10][FS_THREADS];
+  __shared__ float scl[10];
+  const int t = threadIdx.x;
+  double a[10];
+#pragma unroll
+  for (int k = 0; k < 10; ++k) a[k] = 0.0;
+  for (int b = t; b < nblk; b += FS_THREADS) {
+#pragma unroll
+    for (int k = 0; k < 10; ++k) a[k] += part[10 * int64_t(b) + k];
+  }
+#pragma unroll
+  for (int k = 0; k < 10; ++k) sh[k][t] = a[k];
+  __syncthreads();
+  for (int st = FS_THREADS / 2; st > 0; st >>= 1) {
+    if (t < st)
+#pragma unroll
+      for (int k = 0; k < 10; ++k) sh[k][t] += sh[k][t + st];
+    __syncthreads();
+  }
+  if (t < 10) {
+    scl[t] = float(sqrt(sh[t][0] / double(nc)) + 1e-30);
+    fac[t] = scl[t];
+  }
+  __syncthreads();
+  if (t < NIN) {
+    const float* rs = scl;
+    const float* xs = scl + 5;
+    float f;
+    if (t < 5)
+      f = 1.0f / rs[t];
+    else if (t < 30)
+      f = xs[(t - 5) % 5] / rs[(t - 5) / 5];
+    else if (t < 35)
+      f = 1.0f / xs[t - 30];
+    else
+      f = 1.0f / xs[t - 35];
+    fac[10 + t] = f;
+  }
+}
+
+// normalise: B/rs, D_ij xs_j / rs_i, x_J/xs, dq_prev/xs, each as one// normalise: B/rs, D_ij xs_j / rs_i, x_J/xs, dq_prev/xs, each as one
 // multiplication by a per-feature factor (feature 30..34 read from x_J)
 __global__ void k_features_norm(int64_t nc, const float* __restrict__ raw, const float* __restrict__ xj,
                                 const float* __restrict__ scl /*rs[5],xs[5]*/, float* __restrict__ feat) {
@@ -1106,19 +1155,12 @@ static int make_features(fpsi_gnn* m, fpsi_ctx* x, float* feat, float* xj, float
         xj);
   const int nblk = int(nb_(nc, GT));
   k_rms_partial<<<nblk, GT, 0, m->stream>>>(nc, raw, xj, m->d_lpart);
-  std::vector<double> part(size_t(nblk) * 10);
-  FPSI_CUDA_TRY(cudaMemcpyAsync(part.data(), m->d_lpart, part.size() * 8, cudaMemcpyDeviceToHost, m->stream));
-  FPSI_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  k_feat_scales<<<1, FS_THREADS, 0, m->stream>>>(m->d_lpart, nblk, nc, m->d_fac);
   float scl[10];
-  for (int k = 0; k < 10; ++k) {
-    double s = 0;
-    for (int b = 0; b < nblk; ++b) s += part[10 * b + k];
-    scl[k] = float(std::sqrt(s / double(nc)) + 1e-30);
-  }
+  FPSI_CUDA_TRY(cudaMemcpyAsync(scl, m->d_fac, sizeof(scl), cudaMemcpyDeviceToHost, m->stream));
+  k_features_norm<<<nb_(nc, FCB), 256, 0, m->stream>>>(nc, raw, xj, m->d_fac, feat);
+  FPSI_CUDA_TRY(cudaStreamSynchronize(m->stream));
   for (int k = 0; k < 5; ++k) rs[k] = scl[k], xs[k] = scl[5 + k];
-  float* dscl = reinterpret_cast<float*>(m->d_lpart);
-  FPSI_CUDA_TRY(cudaMemcpyAsync(dscl, scl, sizeof(scl), cudaMemcpyHostToDevice, m->stream));
-  k_features_norm<<<nb_(nc, FCB), 256, 0, m->stream>>>(nc, raw, xj, dscl, feat);
   FPSI_CUDA_TRY(cudaGetLastError());
   return FPSI_OK;
 }
@@ -1411,35 +1453,6 @@ __global__ void k_feat_stats(int64_t nc, const double* __restrict__ src, const T
     for (int k = 0; k < 10; ++k) part[10 * blockIdx.x + k] = sh[k][0];
 }
 
-// scales rs, xs (the blocks summed in order, as the host does for the
-// training features) and the 40 per-feature factors of k_features_norm
-__global__ void k_feat_scales(const double* __restrict__ part, int nblk, int64_t nc,
-                              float* __restrict__ fac) {
-  __shared__ float scl[10];
-  const int k = threadIdx.x;
-  if (k < 10) {
-    double sum = 0;
-    for (int b = 0; b < nblk; ++b) sum += part[10 * b + k];
-    scl[k] = float(sqrt(sum / double(nc)) + 1e-30);
-    fac[k] = scl[k];
-  }
-  __syncthreads();
-  if (k < NIN) {
-    const float* rs = scl;
-    const float* xs = scl + 5;
-    float f;
-    if (k < 5)
-      f = 1.0f / rs[k];
-    else if (k < 30)
-      f = xs[(k - 5) % 5] / rs[(k - 5) / 5];
-    else if (k < 35)
-      f = 1.0f / xs[k - 30];
-    else
-      f = 1.0f / xs[k - 35];
-    fac[10 + k] = f;
-  }
-}
-
 // the 40 normalised features of a cell straight from the system, rounded
 // to BF16 (B, D, x_J, dq_prev; the same float products as
 // k_features_raw + k_features_norm), one 16 B chunk of 8 per thread
@@ -1497,7 +1510,7 @@ void launch_features16(fpsi_gnn* m, fpsi_ctx* x, __nv_bfloat16* feat, cudaStream
   const TX* xv = static_cast<const TX*>(x->d_x);
   const TX* xp = x->have_xprev ? static_cast<const TX*>(x->d_xprev) : nullptr;
   k_feat_stats<TX><<<nblk, GT, 0, s>>>(nc, x->d_src, xv, x->d_ci, m->d_lpart);
-  k_feat_scales<<<1, 64, 0, s>>>(m->d_lpart, nblk, nc, m->d_fac);
+  k_feat_scales<<<1, FS_THREADS, 0, s>>>(m->d_lpart, nblk, nc, m->d_fac);
   k_features_bf16<TB, TX><<<nb_(nc * (NIN / 8), 256), 256, 0, s>>>(
       nc, x->d_src, static_cast<const TB*>(x->d_D), xv, xp, x->d_ci, m->d_fac, feat);
 }

@@ -340,7 +340,7 @@ __device__ __forceinline__ void face_states_cell(const MeshView& M, const double
 // WREC: also the cell's gradient-and-limiter record (viscous terms, the SA
 // model and fpsi_get_reconstruction read it)
 template <bool WREC>
-__global__ void __launch_bounds__(GRAD_THREADS)
+__global__ void __launch_bounds__(GRAD_THREADS, 5)
 k_grad_limiter(MeshView M, const double* __restrict__ q, const double* __restrict__ qb, int limiter,
                double Kl, Gas gas, double* __restrict__ grad, double* __restrict__ qf) {
   __shared__ double sr[WREC ? GRAD_THREADS * GPREC : 1];
