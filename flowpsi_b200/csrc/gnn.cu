@@ -498,6 +498,256 @@ k_layer_tc(int64_t nc, int fin, const TIn* __restrict__ h, const int32_t* __rest
                  : "memory");
 }
 
+// ---- inference layer, warp-specialised ------------------------------------
+// The same layer as k_layer_tc (A = [h | neighbour mean] in BF16, z = A
+// [Ws | Wn]^T + b on the tensor cores, GELU, BF16 out; the last layer also
+// the head), with the roles split and two tiles in flight:
+//   warps 0..WS_PROD-1   gather A of tile k into shared buffer k % 2;
+//   warp WS_PROD         one thread issues the tile's MMAs into tensor-memory
+//                        accumulator k % 2 and commits them;
+//   warps WS_PROD+1..+4  read accumulator k % 2 (one lane quarter each), apply
+//                        bias and GELU and store the tile (or the head).
+// Hand-offs are mbarriers: full[b] (gatherers -> MMA), done[b] (MMA
+// completion -> epilogue, and -> gatherers: buffer b may be refilled),
+// tfree[b] (epilogue has read accumulator b -> MMA may overwrite it).  A
+// phase of done[b] cannot complete twice before both of its waiters saw it,
+// because the next MMA on b needs both of them first.  Every wait is
+// bounded: a wait that gives up sets the CTA's abort flag and bit 1 of err,
+// every role then leaves its loop, the MMA thread lets its last commits
+// land (bounded) and the tensor memory is freed.
+constexpr int WS_PROD = 8;                         // gathering warps
+constexpr int WS_EPI = 4;                          // epilogue warps
+constexpr int WS_THREADS = 32 * (WS_PROD + 1 + WS_EPI);
+constexpr int WS_NB = 4;                           // neighbour rows per cell in flight
+
+struct WsSmem {
+  size_t a0, a1, b, o, wo, bias, bar, slot, abort, total;
+};
+__host__ __device__ inline WsSmem ws_smem(int fin) {
+  const size_t nch = size_t(2 * fin / 8);
+  WsSmem s;
+  s.a0 = 0;
+  s.a1 = s.a0 + nch * TC_ROWS * 16;
+  s.b = s.a1 + nch * TC_ROWS * 16;
+  s.o = s.b + nch * W * 16;
+  s.wo = s.o + size_t(WS_EPI) * 32 * TC_OSTRIDE;
+  s.bias = s.wo + size_t(NOUT * W + 8) * sizeof(float);
+  s.bar = s.bias + W * sizeof(float);
+  s.slot = s.bar + 6 * 8;
+  s.abort = s.slot + 8;
+  s.total = s.abort + 8;
+  return s;
+}
+
+__device__ __forceinline__ void mbar_init_n(uint64_t* bar, uint32_t n) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(n) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+template <bool HEAD>
+__global__ void __launch_bounds__(WS_THREADS, 1)
+k_layer_ws(int64_t nc, int fin, const __nv_bfloat16* __restrict__ h, const int32_t* __restrict__ off,
+           const int32_t* __restrict__ nb, const __nv_bfloat16* __restrict__ ws,
+           const __nv_bfloat16* __restrict__ wn, const __nv_bfloat16* __restrict__ bias,
+           const __nv_bfloat16* __restrict__ wo, const __nv_bfloat16* __restrict__ bo,
+           __nv_bfloat16* __restrict__ hout, float* __restrict__ y, int32_t* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char wsm[];
+  const WsSmem L = ws_smem(fin);
+  const int nch = 2 * fin / 8, hch = fin / 8;
+  unsigned char* sA[2] = {wsm + L.a0, wsm + L.a1};
+  unsigned char* sB = wsm + L.b;
+  float* sWo = reinterpret_cast<float*>(wsm + L.wo);
+  float* sbias = reinterpret_cast<float*>(wsm + L.bias);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(wsm + L.bar);  // full[2], done[2], tfree[2]
+  uint64_t *full = bar, *done = bar + 2, *tfree = bar + 4;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(wsm + L.slot);
+  volatile int32_t* abort_flag = reinterpret_cast<volatile int32_t*>(wsm + L.abort);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  for (int idx = tid; idx < W * nch; idx += WS_THREADS) {
+    const int j = idx / nch, c = idx - nch * (idx / nch);
+    const __nv_bfloat16* src = c < hch ? ws + j * fin + 8 * c : wn + j * fin + 8 * (c - hch);
+    *reinterpret_cast<uint4*>(sB + (size_t(c) * W + j) * 16) = *reinterpret_cast<const uint4*>(src);
+  }
+  if (tid < W) sbias[tid] = __bfloat162float(bias[tid]);
+  if (HEAD) {
+    for (int i = tid; i < NOUT * W; i += WS_THREADS) sWo[i] = __bfloat162float(wo[i]);
+    if (tid < NOUT) sWo[NOUT * W + tid] = __bfloat162float(bo[tid]);
+  }
+  if (warp == WS_PROD) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(uint32_t(2 * TC_COLS))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int b = 0; b < 2; ++b) {
+      mbar_init_n(full + b, 32 * WS_PROD);
+      mbar_init_n(done + b, 1);
+      mbar_init_n(tfree + b, 32 * WS_EPI);
+    }
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const int64_t ntiles = (nc + TC_ROWS - 1) / TC_ROWS;
+  auto give_up = [&]() {
+    *abort_flag = 1;
+    atomicOr(err, 2);
+  };
+
+  if (warp < WS_PROD) {
+    // ---- gather: warp w fills rows 16 w .. 16 w + 15; lane = (row 0..15,
+    // chunk parity 0..1), two chunks (own and neighbour rows) in flight
+    const int r = 16 * warp + (lane & 15), cp = lane >> 4;
+    int k = 0;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+      const int b = k & 1;
+      if (k >= 2 && !mbar_wait_bounded(done + b, uint32_t(((k >> 1) - 1) & 1))) give_up();
+      if (*abort_flag) break;
+      unsigned char* A = sA[b];
+      const int64_t cell = t * TC_ROWS + r;
+      if (cell < nc) {
+        const int32_t e0 = __ldg(off + cell), e1 = __ldg(off + cell + 1);
+        int32_t nbi[WS_NB];
+#pragma unroll
+        for (int j = 0; j < WS_NB; ++j) nbi[j] = e0 + j < e1 ? __ldg(nb + e0 + j) : -1;
+        const float inv = e1 > e0 ? 1.0f / float(e1 - e0) : 0.f;
+        for (int c0 = cp; c0 < hch; c0 += 4) {
+          // chunks c0 and c0 + 2 of the row and of its neighbours
+          Chunk8<__nv_bfloat16> own[2], u[2][WS_NB];
+#pragma unroll
+          for (int i = 0; i < 2; ++i) {
+            const int c = c0 + 2 * i;
+            if (c < hch) {
+              own[i].load(h + cell * fin + 8 * c);
+#pragma unroll
+              for (int j = 0; j < WS_NB; ++j)
+                if (nbi[j] >= 0) u[i][j].load(h + int64_t(nbi[j]) * fin + 8 * c);
+            }
+          }
+#pragma unroll
+          for (int i = 0; i < 2; ++i) {
+            const int c = c0 + 2 * i;
+            if (c >= hch) break;
+            float v[8], sum[8];
+            own[i].get(v);
+            *reinterpret_cast<uint4*>(A + (size_t(c) * TC_ROWS + r) * 16) = pack8(v);
+#pragma unroll
+            for (int q8 = 0; q8 < 8; ++q8) sum[q8] = 0.f;
+#pragma unroll
+            for (int j = 0; j < WS_NB; ++j)
+              if (nbi[j] >= 0) {
+                u[i][j].get(v);
+#pragma unroll
+                for (int q8 = 0; q8 < 8; ++q8) sum[q8] += v[q8];
+              }
+            for (int32_t e = e0 + WS_NB; e < e1; ++e) {  // cells with more neighbours
+              Chunk8<__nv_bfloat16> x;
+              x.load(h + int64_t(__ldg(nb + e)) * fin + 8 * c);
+              x.get(v);
+#pragma unroll
+              for (int q8 = 0; q8 < 8; ++q8) sum[q8] += v[q8];
+            }
+#pragma unroll
+            for (int q8 = 0; q8 < 8; ++q8) sum[q8] *= inv;
+            *reinterpret_cast<uint4*>(A + (size_t(hch + c) * TC_ROWS + r) * 16) = pack8(sum);
+          }
+        }
+      } else {
+        for (int c = cp; c < nch; c += 2)
+          *reinterpret_cast<uint4*>(A + (size_t(c) * TC_ROWS + r) * 16) = make_uint4(0, 0, 0, 0);
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(full + b);
+    }
+  } else if (warp == WS_PROD) {
+    // ---- MMA issue (one thread)
+    int k = 0;
+    int last[2] = {-1, -1};  // last tile index committed on each accumulator
+    if (lane == 0) {
+      for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+        const int b = k & 1;
+        if (!mbar_wait_bounded(full + b, uint32_t((k >> 1) & 1))) give_up();
+        if (!*abort_flag && k >= 2 && !mbar_wait_bounded(tfree + b, uint32_t(((k >> 1) - 1) & 1)))
+          give_up();
+        if (*abort_flag) break;
+        tc_fence_after();
+        for (int st = 0; st < nch / 2; ++st) {
+          const uint64_t ad = umma_desc(sA[b] + size_t(2 * st) * TC_ROWS * 16, TC_ROWS * 16, 128);
+          const uint64_t bd = umma_desc(sB + size_t(2 * st) * W * 16, W * 16, 128);
+          umma_bf16(tmem + uint32_t(TC_COLS * b), ad, bd, st > 0 ? 1u : 0u);
+        }
+        umma_commit(done + b);
+        last[b] = k;
+      }
+      // let every committed MMA land before the tensor memory is freed
+      for (int b = 0; b < 2; ++b)
+        if (last[b] >= 0) mbar_wait_bounded(done + b, uint32_t((last[b] >> 1) & 1));
+    }
+    __syncwarp();
+  } else {
+    // ---- epilogue: warp quarter q holds accumulator lanes 32 q .. 32 q + 31
+    const int ew = warp - WS_PROD - 1;
+    const int q = warp & 3;
+    unsigned char* sO = wsm + L.o + size_t(ew) * 32 * TC_OSTRIDE;
+    int k = 0;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+      const int b = k & 1;
+      if (!mbar_wait_bounded(done + b, uint32_t((k >> 1) & 1))) give_up();
+      if (*abort_flag) break;
+      tc_fence_after();
+      float v[64];
+      const uint32_t ta = tmem + (uint32_t(32 * q) << 16) + uint32_t(TC_COLS * b);
+      tmem_ld32(ta, v);
+      tmem_ld32(ta + 32, v + 32);
+      tc_fence_before();
+      mbar_arrive(tfree + b);
+      const int64_t cell = t * TC_ROWS + 32 * q + lane;
+#pragma unroll
+      for (int j = 0; j < 64; ++j) v[j] = __bfloat162float(__float2bfloat16_rn(gelu(v[j] + sbias[j])));
+      if (HEAD) {
+        if (cell < nc) {
+#pragma unroll
+          for (int o = 0; o < NOUT; ++o) {
+            float sacc = 0.f, sacc2 = 0.f;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) sacc += sWo[o * W + j] * v[j];
+#pragma unroll
+            for (int j = 32; j < 64; ++j) sacc2 += sWo[o * W + j] * v[j];
+            y[cell * NOUT + o] = (sacc + sacc2) + sWo[NOUT * W + o];
+          }
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          *reinterpret_cast<uint4*>(sO + size_t(lane) * TC_OSTRIDE + 16 * j) = pack8(v + 8 * j);
+        __syncwarp();
+        const int64_t row0 = t * TC_ROWS + 32 * q;
+        for (int idx = lane; idx < 32 * 8; idx += 32) {
+          const int rr = idx >> 3, c16 = idx & 7;
+          if (row0 + rr < nc)
+            *reinterpret_cast<uint4*>(hout + (row0 + rr) * W + 8 * c16) =
+                *reinterpret_cast<const uint4*>(sO + size_t(rr) * TC_OSTRIDE + 16 * c16);
+        }
+        __syncwarp();
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == WS_PROD)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(uint32_t(2 * TC_COLS))
+                 : "memory");
+}
+
 // batch membership: a counter-based hash of (seed, cell) below the threshold
 __device__ __forceinline__ bool in_batch(uint64_t seed, int64_t c, uint64_t thr) {
   uint64_t x = seed * 0x9E3779B97F4A7C15ull + uint64_t(c) + 0x632BE59BD9B4E019ull;
@@ -830,6 +1080,25 @@ int forward(fpsi_gnn* m, const Graph& G, const float* feat, bool keep,
   cudaStream_t s = stream ? stream : m->stream;
   const int64_t nc = G.nc;
   const int64_t ntiles = (nc + TC_ROWS - 1) / TC_ROWS;
+  if (!keep && feat16) {
+    // inference: the warp-specialised layer, one CTA per SM
+    const unsigned gws = unsigned(std::max<int64_t>(1, std::min<int64_t>(ntiles, m->nsm)));
+    const __nv_bfloat16 *wo = m->d_wb + m->L.wo, *bo = m->d_wb + m->L.bo;
+    for (int l = 0; l < NLAYER; ++l) {
+      const int fin = m->L.fan_in[l];
+      const size_t smem = ws_smem(fin).total;
+      const __nv_bfloat16 *ws = m->d_wb + m->L.ws[l], *wn = m->d_wb + m->L.wn[l], *b = m->d_wb + m->L.b[l];
+      const __nv_bfloat16* hin = l == 0 ? feat16 : m->d_h[l];
+      if (l == NLAYER - 1)
+        k_layer_ws<true><<<gws, WS_THREADS, smem, s>>>(nc, fin, hin, G.off, G.nb, ws, wn, b, wo, bo, nullptr,
+                                                      m->d_y, m->d_err);
+      else
+        k_layer_ws<false><<<gws, WS_THREADS, smem, s>>>(nc, fin, hin, G.off, G.nb, ws, wn, b, wo, bo,
+                                                       m->d_h[l + 1], nullptr, m->d_err);
+    }
+    FPSI_CUDA_TRY(cudaGetLastError());
+    return FPSI_OK;
+  }
   auto grid_for = [&](int per_sm) {
     return unsigned(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(per_sm) * m->nsm)));
   };
@@ -1042,7 +1311,11 @@ int fpsi_gnn_create(fpsi_gnn** out, uint64_t seed) {
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(tc_smem(W).total)) != cudaSuccess ||
               cudaFuncSetAttribute(k_layer_tc<__nv_bfloat16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   int(tc_smem(W).total)) != cudaSuccess)) {
+                                   int(tc_smem(W).total)) != cudaSuccess ||
+              cudaFuncSetAttribute(k_layer_ws<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(ws_smem(W).total)) != cudaSuccess ||
+              cudaFuncSetAttribute(k_layer_ws<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(ws_smem(W).total)) != cudaSuccess)) {
     fpsi::set_error("learned start: device query failed");
     rc = FPSI_E_CUDA;
   }

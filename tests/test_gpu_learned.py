@@ -173,6 +173,27 @@ def test_region_snapshot_matches_the_replica(need_gpu):
         assert np.linalg.norm(gg - go) <= 1e-3 * np.linalg.norm(go) + 1e-12, name
 
 
+def test_inference_matches_the_training_forward(need_gpu):
+    """fpsi_gnn_predict runs the warp-specialised inference layers on BF16
+    features made in one pass; a snapshot of the same system runs the
+    training forward on FP32 features, which its first layer rounds to BF16.
+    Both must give the same network output: the loss of predict's output
+    against the snapshot's target is the snapshot's own loss."""
+    for n, prec in ((8, "fp64"), (6, "mixed")):
+        case, g, _ = _system(n=n, prec=prec)
+        model = LearnedStart(seed=5)
+        _random_head(model)
+        model.add_snapshot(g, g.get_iterate())
+        x0 = model.predict(g, want=True)
+        f, t, xj, sc = model.snapshot(0)
+        y = (x0 - xj.astype(np.float64)) / sc[5:].astype(np.float64)
+        loss_py = float(np.mean((y - t) ** 2))
+        loss_dev, _ = model.loss_grad(0)
+        assert abs(loss_dev - loss_py) <= 1e-5 * loss_py, (n, prec, loss_dev, loss_py)
+        model.close()
+        g.close()
+
+
 def test_minibatch_gradient_is_the_batch_mean(need_gpu):
     """the batch is a hashed subset of cells: its loss and gradient are those
     of the masked mean squared error"""
