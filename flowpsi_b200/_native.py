@@ -18,7 +18,7 @@ ERRORS = {
     -5: "FPSI_E_SINGULAR", -6: "FPSI_E_NAN", -7: "FPSI_E_TIMEOUT", -8: "FPSI_E_STATE",
 }
 
-FLUX = {"hllc": 0, "roe": 1, "hlle": 2}
+FLUX = {"hllc": 0, "roe": 1, "hlle": 2, "kec": 3}
 LIMITER = {"venkatakrishnan": 0, "barth": 1, "none": 2, "zero": 3}
 SOLVER = {"sgs": 0, "lsgs": 1, "fsgs": 2}
 PRECISION = {"fp64": 0, "ref": 1, "mixed": 2}
@@ -39,6 +39,9 @@ class Params(C.Structure):
         ("Prt", C.c_double), ("mu_a1", C.c_double), ("mu_a2", C.c_double),
         ("mu_a3", C.c_double), ("k_a1", C.c_double), ("k_a2", C.c_double),
         ("k_a3", C.c_double), ("time_accurate", C.c_int32), ("newton_iters", C.c_int32),
+        ("lds_comp_factor", C.c_double), ("lds_dissipation_limit", C.c_double),
+        ("lds_ducros_factor", C.c_double), ("lds_use_upwind", C.c_double),
+        ("lds_nonsym_coeff", C.c_double), ("lds_nonsym_factor", C.c_double),
     ]
 
 

@@ -213,7 +213,7 @@ bool is_lsgs(const fpsi_ctx* x) { return x->P.solver == FPSI_SOLVER_LSGS; }
 
 int check_params(const fpsi_params* p) {
   if (!p) return FPSI_E_INVALID;
-  if (!(p->gamma > 1.0) || !(p->Rtilde > 0) || p->flux < 0 || p->flux > 2 || p->limiter < 0 ||
+  if (!(p->gamma > 1.0) || !(p->Rtilde > 0) || p->flux < 0 || p->flux > FPSI_FLUX_KEC || p->limiter < 0 ||
       p->limiter > 3 || p->precision < 0 || p->precision > 2 || p->gauss_seidel_iter < 0) {
     fpsi::set_error("invalid parameter value");
     return FPSI_E_INVALID;
@@ -246,6 +246,12 @@ int check_params(const fpsi_params* p) {
   if (p->time_accurate && p->turbulence == FPSI_TURB_SA && p->viscous == 2) {
     fpsi::set_error("the SA model is advanced in steady mode only");
     return FPSI_E_UNSUPPORTED;
+  }
+  if (p->flux == FPSI_FLUX_KEC &&
+      (!(p->lds_comp_factor >= 0) || !(p->lds_dissipation_limit >= 0) || !(p->lds_ducros_factor >= 0) ||
+       !(p->lds_use_upwind >= 0) || !(p->lds_nonsym_coeff > 0) || !(p->lds_nonsym_factor >= 0))) {
+    fpsi::set_error("low-dissipation flux switches out of range");
+    return FPSI_E_INVALID;
   }
   return FPSI_OK;
 }
@@ -316,6 +322,12 @@ void fpsi_default_params(fpsi_params* p) {
   p->k_a3 = 194.0;
   p->time_accurate = 0;
   p->newton_iters = 6;
+  p->lds_comp_factor = 5.0;
+  p->lds_dissipation_limit = 1.0;
+  p->lds_ducros_factor = 0.0;
+  p->lds_use_upwind = 0.0;
+  p->lds_nonsym_coeff = 2.0;
+  p->lds_nonsym_factor = 1.0;
 }
 
 const char* fpsi_strerror(int code) {
@@ -347,10 +359,10 @@ int fpsi_destroy(fpsi_ctx* x) {
   free_lsgs(x);
   free_sa(x);
   void* ps[] = {x->d_cl, x->d_cr, x->d_n, x->d_area, x->d_rL, x->d_rR, x->d_vol, x->d_cc,
-                x->d_Minv, x->d_cf_off, x->d_cf, x->d_colour_cells, x->d_bcs, x->d_bcmean, x->d_q,
+                x->d_Minv, x->d_cf_off, x->d_cf, x->d_ecf, x->d_enb, x->d_colour_cells, x->d_bcs, x->d_bcmean, x->d_q,
                 x->d_qn, x->d_qnm1, x->d_qb, x->d_grad, x->d_qf, x->d_F, x->d_src, x->d_dtau, x->d_tmu,
                 x->d_part, x->d_resid, x->d_amin, x->d_err, x->d_perm, x->d_stage, x->d_ci, x->d_ccol,
-                x->d_nbr, x->d_colinfo, x->d_cnb_off, x->d_cnb, x->d_xprev, x->d_qsave};
+                x->d_nbr, x->d_colinfo, x->d_cnb_off, x->d_cnb, x->d_xprev, x->d_qsave, x->d_adiss, x->d_ageom};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (x->h_resid) cudaFreeHost(x->h_resid);
@@ -421,6 +433,8 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
   }
   TRY(upload(x, &x->d_cf_off, H.cf_off));
   TRY(upload(x, &x->d_cf, H.cf));
+  TRY(upload(x, &x->d_ecf, H.ecf));
+  TRY(upload(x, &x->d_enb, H.enb));
   TRY(upload(x, &x->d_colour_cells, H.colour_cells));
   TRY(upload(x, &x->d_perm, H.perm));
   TRY(upload(x, &x->d_ci, H.ci_of));

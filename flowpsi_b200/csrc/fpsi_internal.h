@@ -52,6 +52,12 @@ struct HostMesh {
   std::vector<double> an_caller, area_caller, fc_caller;  // caller order, for export
   std::vector<int32_t> cf_off;   // nc+1
   std::vector<int32_t> cf;       // (face << 1) | side ; upper, lower, boundary order
+  // the same lists entry-major: entry j of cell c at [j * nc + c], j below
+  // ell_k (the largest face count of a cell), -1 past a cell's last face;
+  // a warp's 32 consecutive cells read entry j as one coalesced 128 B line
+  int32_t ell_k = 0;
+  std::vector<int32_t> ecf;      // ell_k * nc: cf entries
+  std::vector<int32_t> enb;      // ell_k * nc: the interior neighbour, -1 on boundary faces
   std::vector<int32_t> colour;   // nc (new numbering)
   int ncolours = 0;
   std::vector<int32_t> colour_off;   // ncolours+1 into colour_cells
@@ -129,6 +135,12 @@ struct fpsi_ctx {
   double *d_vol = nullptr, *d_cc = nullptr;      // vol[nc], cc[3][nc]
   double* d_Minv = nullptr;                      // [6][nc]
   int32_t *d_cf_off = nullptr, *d_cf = nullptr;
+  int32_t *d_ecf = nullptr, *d_enb = nullptr;  // entry-major cell-face lists
+  // low-dissipation (KEC) flux: alpha_diss per cell, alpha_geom_f per
+  // interior face (FP32) and the switches it was computed with
+  double* d_adiss = nullptr;
+  float* d_ageom = nullptr;
+  double ageom_coeff = -1.0, ageom_factor = -1.0;
   int32_t* d_colour_cells = nullptr;
   fpsi_bc* d_bcs = nullptr;
   double* d_bcmean = nullptr;  // [nbc][2]: sum of A pg and of A over each condition's faces

@@ -31,6 +31,7 @@
 #include <cstdint>
 #include <cstring>
 #include <new>
+#include <type_traits>
 #include <vector>
 
 #include "fpsi_internal.h"
@@ -71,6 +72,9 @@ struct Graph {
   int64_t nc = 0;
   const int32_t* off = nullptr;
   const int32_t* nb = nullptr;
+  // the same graph entry-major (a context's mesh): [K][nc], -1 = no neighbour
+  const int32_t* ell = nullptr;
+  int K = 0;
 };
 
 struct Snapshot {
@@ -233,6 +237,13 @@ struct Chunk8<float> {
     v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
   }
 };
+// a layer input value as the network sees it: FP32 features are rounded to
+// BF16 (the own row and every neighbour row before their mean), BF16
+// activations are already
+template <class TIn>
+__device__ __forceinline__ float as_input(float x) {
+  return std::is_same<TIn, float>::value ? __bfloat162float(__float2bfloat16_rn(x)) : x;
+}
 __device__ __forceinline__ uint4 pack8(const float* v) {
   uint4 u;
   __nv_bfloat162* q = reinterpret_cast<__nv_bfloat162*>(&u);
@@ -392,14 +403,14 @@ k_layer_tc(int64_t nc, int fin, const TIn* __restrict__ h, const int32_t* __rest
               if (nbi[p][k] >= 0) {
                 u[k][i].get(v);
 #pragma unroll
-                for (int q8 = 0; q8 < 8; ++q8) sum[q8] += v[q8];
+                for (int q8 = 0; q8 < 8; ++q8) sum[q8] += as_input<TIn>(v[q8]);
               }
             for (int32_t e = e0[p] + NB_FAST; e < e1[p]; ++e) {  // cells with many neighbours
               Chunk8<TIn> x;
               x.load(h + int64_t(__ldg(nb + e)) * fin + 8 * ci);
               x.get(v);
 #pragma unroll
-              for (int q8 = 0; q8 < 8; ++q8) sum[q8] += v[q8];
+              for (int q8 = 0; q8 < 8; ++q8) sum[q8] += as_input<TIn>(v[q8]);
             }
 #pragma unroll
             for (int q8 = 0; q8 < 8; ++q8) sum[q8] *= inv;
@@ -515,7 +526,7 @@ k_layer_tc(int64_t nc, int fin, const TIn* __restrict__ h, const int32_t* __rest
 // bounded: a wait that gives up sets the CTA's abort flag and bit 1 of err,
 // every role then leaves its loop, the MMA thread lets its last commits
 // land (bounded) and the tensor memory is freed.
-constexpr int WS_PROD = 8;                         // gathering warps
+constexpr int WS_PROD = 8;                         // gathering warps, 16 rows each
 constexpr int WS_EPI = 4;                          // epilogue warps
 constexpr int WS_THREADS = 32 * (WS_PROD + 1 + WS_EPI);
 constexpr int WS_NB = 4;                           // neighbour rows per cell in flight
@@ -547,9 +558,9 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 }
 
 template <bool HEAD>
-__global__ void __launch_bounds__(WS_THREADS, 1)
-k_layer_ws(int64_t nc, int fin, const __nv_bfloat16* __restrict__ h, const int32_t* __restrict__ off,
-           const int32_t* __restrict__ nb, const __nv_bfloat16* __restrict__ ws,
+__global__ void __launch_bounds__(WS_THREADS, 2)
+k_layer_ws(int64_t nc, int fin, const __nv_bfloat16* __restrict__ h, const int32_t* __restrict__ ell,
+           int K, const __nv_bfloat16* __restrict__ ws,
            const __nv_bfloat16* __restrict__ wn, const __nv_bfloat16* __restrict__ bias,
            const __nv_bfloat16* __restrict__ wo, const __nv_bfloat16* __restrict__ bo,
            __nv_bfloat16* __restrict__ hout, float* __restrict__ y, int32_t* __restrict__ err) {
@@ -604,21 +615,33 @@ k_layer_ws(int64_t nc, int fin, const __nv_bfloat16* __restrict__ h, const int32
 
   if (warp < WS_PROD) {
     // ---- gather: warp w fills rows 16 w .. 16 w + 15; lane = (row 0..15,
-    // chunk parity 0..1), two chunks (own and neighbour rows) in flight
+    // chunk parity 0..1), two chunks of the row and of its first WS_NB
+    // neighbour rows in flight together; the next tile's neighbour ids are
+    // requested before this tile's rows.  The neighbours come from the
+    // entry-major lists in the cell's face order (boundary entries are -1
+    // and skipped), so the mean sums them in the order of the face graph.
     const int r = 16 * warp + (lane & 15), cp = lane >> 4;
+    auto ids = [&](int64_t t, int32_t* o) {
+      const int64_t cell = t * TC_ROWS + r;
+#pragma unroll
+      for (int j = 0; j < WS_NB; ++j) o[j] = cell < nc && j < K ? __ldg(ell + j * nc + cell) : -1;
+    };
+    int32_t nbi[WS_NB], nbn[WS_NB];
+    ids(blockIdx.x, nbi);
     int k = 0;
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
       const int b = k & 1;
+      ids(t + gridDim.x, nbn);
       if (k >= 2 && !mbar_wait_bounded(done + b, uint32_t(((k >> 1) - 1) & 1))) give_up();
       if (*abort_flag) break;
       unsigned char* A = sA[b];
       const int64_t cell = t * TC_ROWS + r;
       if (cell < nc) {
-        const int32_t e0 = __ldg(off + cell), e1 = __ldg(off + cell + 1);
-        int32_t nbi[WS_NB];
+        int deg = 0;
 #pragma unroll
-        for (int j = 0; j < WS_NB; ++j) nbi[j] = e0 + j < e1 ? __ldg(nb + e0 + j) : -1;
-        const float inv = e1 > e0 ? 1.0f / float(e1 - e0) : 0.f;
+        for (int j = 0; j < WS_NB; ++j) deg += nbi[j] >= 0;
+        for (int j = WS_NB; j < K; ++j) deg += __ldg(ell + j * nc + cell) >= 0;
+        const float inv = deg > 0 ? 1.0f / float(deg) : 0.f;
         for (int c0 = cp; c0 < hch; c0 += 4) {
           // chunks c0 and c0 + 2 of the row and of its neighbours
           Chunk8<__nv_bfloat16> own[2], u[2][WS_NB];
@@ -648,9 +671,11 @@ k_layer_ws(int64_t nc, int fin, const __nv_bfloat16* __restrict__ h, const int32
 #pragma unroll
                 for (int q8 = 0; q8 < 8; ++q8) sum[q8] += v[q8];
               }
-            for (int32_t e = e0 + WS_NB; e < e1; ++e) {  // cells with more neighbours
+            for (int j = WS_NB; j < K; ++j) {  // cells with more faces
+              const int32_t o = __ldg(ell + j * nc + cell);
+              if (o < 0) continue;
               Chunk8<__nv_bfloat16> x;
-              x.load(h + int64_t(__ldg(nb + e)) * fin + 8 * c);
+              x.load(h + int64_t(o) * fin + 8 * c);
               x.get(v);
 #pragma unroll
               for (int q8 = 0; q8 < 8; ++q8) sum[q8] += v[q8];
@@ -666,6 +691,8 @@ k_layer_ws(int64_t nc, int fin, const __nv_bfloat16* __restrict__ h, const int32
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(full + b);
+#pragma unroll
+      for (int j = 0; j < WS_NB; ++j) nbi[j] = nbn[j];
     }
   } else if (warp == WS_PROD) {
     // ---- MMA issue (one thread)
@@ -703,31 +730,41 @@ k_layer_ws(int64_t nc, int fin, const __nv_bfloat16* __restrict__ h, const int32
       if (!mbar_wait_bounded(done + b, uint32_t((k >> 1) & 1))) give_up();
       if (*abort_flag) break;
       tc_fence_after();
-      float v[64];
+      // the accumulator's two 32-column halves in turn (fewer registers:
+      // two CTAs share an SM); it is released after the second is read
       const uint32_t ta = tmem + (uint32_t(32 * q) << 16) + uint32_t(TC_COLS * b);
-      tmem_ld32(ta, v);
-      tmem_ld32(ta + 32, v + 32);
-      tc_fence_before();
-      mbar_arrive(tfree + b);
       const int64_t cell = t * TC_ROWS + 32 * q + lane;
+      float ys[2][NOUT];
 #pragma unroll
-      for (int j = 0; j < 64; ++j) v[j] = __bfloat162float(__float2bfloat16_rn(gelu(v[j] + sbias[j])));
-      if (HEAD) {
-        if (cell < nc) {
+      for (int hf = 0; hf < 2; ++hf) {
+        float v[32];
+        tmem_ld32(ta + 32 * hf, v);
+        if (hf == 1) {
+          tc_fence_before();
+          mbar_arrive(tfree + b);
+        }
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          v[j] = __bfloat162float(__float2bfloat16_rn(gelu(v[j] + sbias[32 * hf + j])));
+        if (HEAD) {
 #pragma unroll
           for (int o = 0; o < NOUT; ++o) {
-            float sacc = 0.f, sacc2 = 0.f;
+            float sacc = 0.f;
 #pragma unroll
-            for (int j = 0; j < 32; ++j) sacc += sWo[o * W + j] * v[j];
-#pragma unroll
-            for (int j = 32; j < 64; ++j) sacc2 += sWo[o * W + j] * v[j];
-            y[cell * NOUT + o] = (sacc + sacc2) + sWo[NOUT * W + o];
+            for (int j = 0; j < 32; ++j) sacc += sWo[o * W + 32 * hf + j] * v[j];
+            ys[hf][o] = sacc;
           }
-        }
-      } else {
+        } else {
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
-          *reinterpret_cast<uint4*>(sO + size_t(lane) * TC_OSTRIDE + 16 * j) = pack8(v + 8 * j);
+          for (int j = 0; j < 4; ++j)
+            *reinterpret_cast<uint4*>(sO + size_t(lane) * TC_OSTRIDE + 64 * hf + 16 * j) = pack8(v + 8 * j);
+        }
+      }
+      if (HEAD) {
+        if (cell < nc)
+#pragma unroll
+          for (int o = 0; o < NOUT; ++o) y[cell * NOUT + o] = (ys[0][o] + ys[1][o]) + sWo[NOUT * W + o];
+      } else {
         __syncwarp();
         const int64_t row0 = t * TC_ROWS + 32 * q;
         for (int idx = lane; idx < 32 * 8; idx += 32) {
@@ -1074,15 +1111,16 @@ inline unsigned nb_(int64_t n, int t) { return unsigned((n + t - 1) / t); }
 // pre-activations and every layer's activations.
 static_assert(NLAYER >= 2, "the head is fused into the last hidden layer");
 // feat16 (BF16 [nc][40], inference): used instead of feat by the first
-// layer, which rounds its input to BF16 anyway, so the result is the same
+// layer, which rounds every input row to BF16 anyway (its own and each
+// neighbour's before their mean), so the result is the same
 int forward(fpsi_gnn* m, const Graph& G, const float* feat, bool keep,
             const __nv_bfloat16* feat16 = nullptr, cudaStream_t stream = nullptr) {
   cudaStream_t s = stream ? stream : m->stream;
   const int64_t nc = G.nc;
   const int64_t ntiles = (nc + TC_ROWS - 1) / TC_ROWS;
-  if (!keep && feat16) {
-    // inference: the warp-specialised layer, one CTA per SM
-    const unsigned gws = unsigned(std::max<int64_t>(1, std::min<int64_t>(ntiles, m->nsm)));
+  if (!keep && feat16 && G.ell) {
+    // inference: the warp-specialised layer, two CTAs per SM
+    const unsigned gws = unsigned(std::max<int64_t>(1, std::min<int64_t>(ntiles, 2 * int64_t(m->nsm))));
     const __nv_bfloat16 *wo = m->d_wb + m->L.wo, *bo = m->d_wb + m->L.bo;
     for (int l = 0; l < NLAYER; ++l) {
       const int fin = m->L.fan_in[l];
@@ -1090,10 +1128,10 @@ int forward(fpsi_gnn* m, const Graph& G, const float* feat, bool keep,
       const __nv_bfloat16 *ws = m->d_wb + m->L.ws[l], *wn = m->d_wb + m->L.wn[l], *b = m->d_wb + m->L.b[l];
       const __nv_bfloat16* hin = l == 0 ? feat16 : m->d_h[l];
       if (l == NLAYER - 1)
-        k_layer_ws<true><<<gws, WS_THREADS, smem, s>>>(nc, fin, hin, G.off, G.nb, ws, wn, b, wo, bo, nullptr,
+        k_layer_ws<true><<<gws, WS_THREADS, smem, s>>>(nc, fin, hin, G.ell, G.K, ws, wn, b, wo, bo, nullptr,
                                                       m->d_y, m->d_err);
       else
-        k_layer_ws<false><<<gws, WS_THREADS, smem, s>>>(nc, fin, hin, G.off, G.nb, ws, wn, b, wo, bo,
+        k_layer_ws<false><<<gws, WS_THREADS, smem, s>>>(nc, fin, hin, G.ell, G.K, ws, wn, b, wo, bo,
                                                        m->d_h[l + 1], nullptr, m->d_err);
     }
     FPSI_CUDA_TRY(cudaGetLastError());
@@ -1262,7 +1300,7 @@ int ctx_graph(fpsi_ctx* x, Graph* G) {
       FPSI_CUDA_TRY(cudaMemcpy(x->d_cnb, nb.data(), nb.size() * 4, cudaMemcpyHostToDevice));
     x->cnb_n = int64_t(nb.size());
   }
-  *G = Graph{nc, x->d_cnb_off, x->d_cnb};
+  *G = Graph{nc, x->d_cnb_off, x->d_cnb, x->d_enb, x->H.ell_k};
   return FPSI_OK;
 }
 

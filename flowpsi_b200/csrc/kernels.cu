@@ -40,6 +40,9 @@ struct MeshView {
   const double* Minv;  // [6][nc]
   const int32_t* cf_off;
   const int32_t* cf;
+  int32_t K;           // largest face count of a cell
+  const int32_t* ecf;  // [K][nc] cf entries entry-major, -1 past the last
+  const int32_t* enb;  // [K][nc] interior neighbour of the entry, -1 on boundary faces
   const fpsi_bc* bcs;
 };
 
@@ -185,6 +188,33 @@ __global__ void k_bc_state(MeshView M, const double* __restrict__ q, const fpsi_
 // consecutive threads on consecutive addresses.
 // ---------------------------------------------------------------------------
 constexpr int GRAD_THREADS = 128;
+// The cell's faces are taken four at a time from the entry-major lists:
+// the four entries and neighbours are loaded together (entry j of a warp's
+// 32 cells is one coalesced line), then the four neighbour states and face
+// vectors, then they are summed in the cell's face order.  Padding entries
+// (-1) read cell 0 and face 0 and are not summed.
+constexpr int ECH = 4;
+struct EChunk {
+  int32_t ent[ECH];
+  int64_t f[ECH];
+  int32_t nb[ECH];
+};
+__device__ __forceinline__ void load_chunk(const MeshView& M, int64_t c, int j0, EChunk& k,
+                                           bool with_nb) {
+#pragma unroll
+  for (int i = 0; i < ECH; ++i) {
+    const bool in = j0 + i < M.K;
+    k.ent[i] = in ? __ldg(M.ecf + int64_t(j0 + i) * M.nc + c) : -1;
+    k.nb[i] = in && with_nb ? __ldg(M.enb + int64_t(j0 + i) * M.nc + c) : -1;
+  }
+#pragma unroll
+  for (int i = 0; i < ECH; ++i) k.f[i] = k.ent[i] >= 0 ? int64_t(k.ent[i] >> 1) : 0;
+}
+// the state across face i of the chunk: the neighbour's, or the boundary state
+__device__ __forceinline__ const double* across(const MeshView& M, const double* q,
+                                                const double* qb, const EChunk& k, int i) {
+  return k.f[i] >= M.nfi ? qb + 5 * (k.f[i] - M.nfi) : q + 5 * int64_t(k.nb[i] < 0 ? 0 : k.nb[i]);
+}
 
 __device__ __forceinline__ void grad_limiter_cell(const MeshView& M, const double* __restrict__ q,
                                                   const double* __restrict__ qb, int limiter,
@@ -197,37 +227,36 @@ __device__ __forceinline__ void grad_limiter_cell(const MeshView& M, const doubl
   for (int k = 0; k < 15; ++k) b[k] = 0.0;
 #pragma unroll
   for (int k = 0; k < 5; ++k) qmax[k] = qmin[k] = qc[k];
-  const int32_t e0 = M.cf_off[c], e1 = M.cf_off[c + 1];
   const int64_t nf = M.nf;
-  // unrolled so that the loads of several faces are in flight together
-#pragma unroll 4
-  for (int32_t e = e0; e < e1; ++e) {
-    const int32_t ent = M.cf[e];
-    const int64_t f = ent >> 1;
-    const int side = ent & 1;
-    double qn[5];
-    double d[3];
-    if (f >= M.nfi) {
-      const double* p = qb + 5 * (f - M.nfi);
+  for (int j0 = 0; j0 < M.K; j0 += ECH) {
+    EChunk ch;
+    load_chunk(M, c, j0, ch, true);
+    double qn[ECH][5], d[ECH][3];
 #pragma unroll
-      for (int k = 0; k < 5; ++k) qn[k] = __ldg(p + k);
+    for (int i = 0; i < ECH; ++i) {
+      const double* p = across(M, q, qb, ch, i);
 #pragma unroll
-      for (int k = 0; k < 3; ++k) d[k] = M.rL[k * nf + f];
-    } else {
-      const int32_t o = side ? M.cl[f] : M.cr[f];
-      q_arr(load_q(q, o), qn);
-      const double sg = side ? -1.0 : 1.0;
+      for (int k = 0; k < 5; ++k) qn[i][k] = __ldg(p + k);
+      const bool bnd = ch.f[i] >= M.nfi;
+      const double sg = (ch.ent[i] & 1) ? -1.0 : 1.0;
 #pragma unroll
-      for (int k = 0; k < 3; ++k) d[k] = sg * (M.rL[k * nf + f] - M.rR[k * nf + f]);
+      for (int k = 0; k < 3; ++k) {
+        const double l = M.rL[k * nf + ch.f[i]], r = M.rR[k * nf + ch.f[i]];
+        d[i][k] = bnd ? l : sg * (l - r);
+      }
     }
 #pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      const double dq = qn[k] - qc[k];
-      b[3 * k] += d[0] * dq;
-      b[3 * k + 1] += d[1] * dq;
-      b[3 * k + 2] += d[2] * dq;
-      qmax[k] = dmax(qmax[k], qn[k]);
-      qmin[k] = dmin(qmin[k], qn[k]);
+    for (int i = 0; i < ECH; ++i) {
+      if (ch.ent[i] < 0) continue;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        const double dq = qn[i][k] - qc[k];
+        b[3 * k] += d[i][0] * dq;
+        b[3 * k + 1] += d[i][1] * dq;
+        b[3 * k + 2] += d[i][2] * dq;
+        qmax[k] = dmax(qmax[k], qn[i][k]);
+        qmin[k] = dmin(qmin[k], qn[i][k]);
+      }
     }
   }
   const double m0 = M.Minv[c], m1 = M.Minv[M.nc + c], m2 = M.Minv[2 * M.nc + c],
@@ -247,29 +276,38 @@ __device__ __forceinline__ void grad_limiter_cell(const MeshView& M, const doubl
     const double h = cbrt(M.vol[c]);
     const double kh = Kl * h;
     const double eps2 = kh * kh * kh;
-    for (int32_t e = e0; e < e1; ++e) {
-      const int32_t ent = M.cf[e];
-      const int64_t f = ent >> 1;
-      const double* r = (ent & 1) ? M.rR : M.rL;
-      const double rx = r[f], ry = r[nf + f], rz = r[2 * nf + f];
+    for (int j0 = 0; j0 < M.K; j0 += ECH) {
+      EChunk ch;
+      load_chunk(M, c, j0, ch, false);
+      double rv[ECH][3];
 #pragma unroll
-      for (int k = 0; k < 5; ++k) {
-        const double d2 = g[3 * k] * rx + g[3 * k + 1] * ry + g[3 * k + 2] * rz;
-        // min(1, a / b) divides only where the ratio is below 1 (a
-        // correctly rounded quotient is >= 1 exactly when a >= b for b > 0),
-        // so the result is the same bit for bit
-        double p = 1.0;
-        if (d2 != 0.0) {
-          const double d1 = d2 > 0 ? qmax[k] - qc[k] : qmin[k] - qc[k];
-          if (limiter == FPSI_LIMITER_BARTH) {
-            if (d2 > 0 ? d1 < d2 : d1 > d2) p = d1 / d2;
-          } else {
-            const double num = (d1 * d1 + eps2) + 2.0 * d2 * d1;
-            const double den = d1 * d1 + 2.0 * d2 * d2 + d1 * d2 + eps2;
-            if (num < den) p = num / den;
+      for (int i = 0; i < ECH; ++i) {
+        const double* r = (ch.ent[i] & 1) ? M.rR : M.rL;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) rv[i][k] = r[k * nf + ch.f[i]];
+      }
+#pragma unroll
+      for (int i = 0; i < ECH; ++i) {
+        if (ch.ent[i] < 0) continue;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+          const double d2 = g[3 * k] * rv[i][0] + g[3 * k + 1] * rv[i][1] + g[3 * k + 2] * rv[i][2];
+          // min(1, a / b) divides only where the ratio is below 1 (a
+          // correctly rounded quotient is >= 1 exactly when a >= b for b > 0),
+          // so the result is the same bit for bit
+          double p = 1.0;
+          if (d2 != 0.0) {
+            const double d1 = d2 > 0 ? qmax[k] - qc[k] : qmin[k] - qc[k];
+            if (limiter == FPSI_LIMITER_BARTH) {
+              if (d2 > 0 ? d1 < d2 : d1 > d2) p = d1 / d2;
+            } else {
+              const double num = (d1 * d1 + eps2) + 2.0 * d2 * d1;
+              const double den = d1 * d1 + 2.0 * d2 * d2 + d1 * d2 + eps2;
+              if (num < den) p = num / den;
+            }
           }
+          ph[k] = dmin(ph[k], p);
         }
-        ph[k] = dmin(ph[k], p);
       }
     }
   }
@@ -304,43 +342,47 @@ __device__ __forceinline__ void face_states_cell(const MeshView& M, const double
                                                  double* __restrict__ qf) {
   double qc[5];
   q_arr(load_q(q, c), qc);
-  const int32_t e0 = M.cf_off[c], e1 = M.cf_off[c + 1];
   const int64_t nf = M.nf;
-#pragma unroll 2
-  for (int32_t e = e0; e < e1; ++e) {
-    const int32_t ent = M.cf[e];
-    const int64_t f = ent >> 1;
-    const int side = ent & 1;
-    const bool bnd = f >= M.nfi;
-    double Tn, pn;
-    double qbs[5];
-    if (bnd) {
-      const double* p = qb + 5 * (f - M.nfi);
+  for (int j0 = 0; j0 < M.K; j0 += ECH) {
+    EChunk ch;
+    load_chunk(M, c, j0, ch, true);
+    double Tn[ECH], pn[ECH], rv[ECH][3], nv[ECH][3];
 #pragma unroll
-      for (int k = 0; k < 5; ++k) qbs[k] = __ldg(p + k);
-      Tn = qbs[0], pn = qbs[4];
-    } else {
-      const double* p = q + 5 * int64_t(side ? M.cl[f] : M.cr[f]);
-      Tn = __ldg(p), pn = __ldg(p + 4);
+    for (int i = 0; i < ECH; ++i) {
+      const double* p = across(M, q, qb, ch, i);
+      Tn[i] = __ldg(p), pn[i] = __ldg(p + 4);
+      const double* r = (ch.ent[i] & 1) ? M.rR : M.rL;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) rv[i][k] = r[k * nf + ch.f[i]], nv[i][k] = M.n[k * nf + ch.f[i]];
     }
-    const double* r = side ? M.rR : M.rL;
-    const double rx = r[f], ry = r[nf + f], rz = r[2 * nf + f];
-    double l[5];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) l[k] = qc[k] + ph[k] * (g[3 * k] * rx + g[3 * k + 1] * ry + g[3 * k + 2] * rz);
-    l[0] = dmax(l[0], 0.1 * dmin(side ? Tn : qc[0], side ? qc[0] : Tn));
-    l[4] = dmax(l[4], 0.1 * dmin(side ? pn : qc[4], side ? qc[4] : pn) - 0.9 * gas.pamb);
-    const double nx = M.n[f], ny = M.n[nf + f], nz = M.n[2 * nf + f];
-    double* o = qf + int64_t(QFREC) * f;
-    side_record(o + (QFREC / 2) * side, l, side_maxev(qc, nx, ny, nz, gas));
-    if (bnd) side_record(o + QFREC / 2, qbs, side_maxev(qbs, nx, ny, nz, gas));
+    for (int i = 0; i < ECH; ++i) {
+      if (ch.ent[i] < 0) continue;
+      const int64_t f = ch.f[i];
+      const int side = ch.ent[i] & 1;
+      double l[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k)
+        l[k] = qc[k] + ph[k] * (g[3 * k] * rv[i][0] + g[3 * k + 1] * rv[i][1] + g[3 * k + 2] * rv[i][2]);
+      l[0] = dmax(l[0], 0.1 * dmin(side ? Tn[i] : qc[0], side ? qc[0] : Tn[i]));
+      l[4] = dmax(l[4], 0.1 * dmin(side ? pn[i] : qc[4], side ? qc[4] : pn[i]) - 0.9 * gas.pamb);
+      double* o = qf + int64_t(QFREC) * f;
+      side_record(o + (QFREC / 2) * side, l, side_maxev(qc, nv[i][0], nv[i][1], nv[i][2], gas));
+      if (f >= M.nfi) {
+        double qbs[5];
+        const double* p = qb + 5 * (f - M.nfi);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) qbs[k] = __ldg(p + k);
+        side_record(o + QFREC / 2, qbs, side_maxev(qbs, nv[i][0], nv[i][1], nv[i][2], gas));
+      }
+    }
   }
 }
 
 // WREC: also the cell's gradient-and-limiter record (viscous terms, the SA
 // model and fpsi_get_reconstruction read it)
 template <bool WREC>
-__global__ void __launch_bounds__(GRAD_THREADS, 5)
+__global__ void __launch_bounds__(GRAD_THREADS, 4)
 k_grad_limiter(MeshView M, const double* __restrict__ q, const double* __restrict__ qb, int limiter,
                double Kl, Gas gas, double* __restrict__ grad, double* __restrict__ qf) {
   __shared__ double sr[WREC ? GRAD_THREADS * GPREC : 1];
@@ -515,7 +557,8 @@ __device__ __forceinline__ void add_visc_jac(TB* M, const VFace& v, const double
 template <bool VIS, int KIND>
 __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
                             const double* __restrict__ qb, const double* __restrict__ grad,
-                            const double* __restrict__ qf, Gas g, Visc V, double* __restrict__ F) {
+                            const double* __restrict__ qf, Gas g, Visc V, double* __restrict__ F,
+                            const double* __restrict__ adiss, const float* __restrict__ ageom) {
   const int64_t f = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (f >= M.nf) return;
   FaceStates s;
@@ -534,6 +577,16 @@ __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
     // their boundary state (bcIsentropic.loci:162-167, bcFixedMass.loci:155-160,
     // bcFixedMassOutflow.loci:152-157)
     state_flux(s.R, nx, ny, nz, A, g, fl);
+  } else if (KIND == FPSI_FLUX_KEC) {
+    if (f < M.nfi) {
+      const int64_t a = M.cl[f], b = M.cr[f];
+      const double dvx = 0.5 * (M.rL[f] + M.rR[f]), dvy = 0.5 * (M.rL[M.nf + f] + M.rR[M.nf + f]),
+                   dvz = 0.5 * (M.rL[2 * M.nf + f] + M.rR[2 * M.nf + f]);
+      kec_face(s.L, s.R, load_q(q, a), load_q(q, b), grad + GPREC * a, grad + GPREC * b, dvx, dvy,
+               dvz, adiss[a], adiss[b], double(ageom[f]), nx, ny, nz, A, g, fl);
+    } else {
+      riemann1(FPSI_FLUX_HLLC, s.L, s.R, nx, ny, nz, A, g, fl);  // inviscidRiemannFlux
+    }
   } else {
     riemann1(KIND, s.L, s.R, nx, ny, nz, A, g, fl);
   }
@@ -552,10 +605,126 @@ __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
 }
 
 // ---------------------------------------------------------------------------
+// low-dissipation (KEC) switches
+// ---------------------------------------------------------------------------
+struct Lds {
+  double comp, dlim, ducros, upwind, nscoeff, nsfactor;
+};
+
+// alpha_geom_f (fluxLowDiss.loci:122-138) of each interior face, stored in
+// FP32 like the reference's store<realF>: with df = x_r - x_l and dv = x_f -
+// (x_l + x_r)/2, cos a = min(sqrt(max(1 - 2|dv|/|df|, 0)), n.df/|df|),
+// x = min(c (1 - cos a), 1), alpha = x^2 + s (x^3 - 2 x^2 + x), s = factor/max(c, 1)
+__global__ void k_alpha_geom(MeshView M, Lds P, float* __restrict__ ag) {
+  const int64_t f = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (f >= M.nfi) return;
+  const int64_t nf = M.nf;
+  double df[3], dv[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double l = M.rL[k * nf + f], r = M.rR[k * nf + f];
+    df[k] = l - r;
+    dv[k] = 0.5 * (l + r);
+  }
+  const double ndv = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+  const double ndf = sqrt(df[0] * df[0] + df[1] * df[1] + df[2] * df[2]);
+  const double ndotdf = M.n[f] * df[0] + M.n[nf + f] * df[1] + M.n[2 * nf + f] * df[2];
+  const double cosa = dmin(sqrt(dmax(1. - 2. * ndv / ndf, 0.0)), ndotdf / ndf);
+  const double scale = P.nscoeff;
+  const double sf = P.nsfactor / dmax(scale, 1.0);
+  const double x = dmin(scale * (1. - cosa), 1.0);
+  const double x2 = x * x, x3 = x2 * x;
+  ag[f] = float(x2 + sf * (x3 - 2. * x2 + x));
+}
+
+// alpha_diss (fluxLowDiss.loci:141-176) of each cell from its velocity
+// divergence veldiv, the sum over its faces of +-ufn (fluxLowDiss.loci:61-78;
+// interior faces: the mean velocity plus the face gradient of u times dv =
+// x_f - (x_l + x_r)/2, boundary faces: the boundary velocity; dotted with the
+// area vector, + on the cl side), the vorticity magnitude of the cell
+// gradient (solverTurbulence.loci:45-79), the sound speed and twice the
+// largest distance from the cell centre to its face centres.
+constexpr int AD_THREADS = 128;
+__global__ void __launch_bounds__(AD_THREADS)
+k_alpha_diss(MeshView M, const double* __restrict__ q, const double* __restrict__ qb,
+             const double* __restrict__ grad, Gas g, Lds P, double* __restrict__ adiss) {
+  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c >= M.nc) return;
+  const int64_t nf = M.nf;
+  double veldiv = 0.0, maxd2 = 0.0;
+  for (int j0 = 0; j0 < M.K; j0 += ECH) {
+    EChunk ch;
+    load_chunk(M, c, j0, ch, true);
+#pragma unroll
+    for (int i = 0; i < ECH; ++i) {
+      if (ch.ent[i] < 0) continue;
+      const int64_t f = ch.f[i];
+      const int side = ch.ent[i] & 1;
+      double rl[3], rr[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) rl[k] = M.rL[k * nf + f], rr[k] = M.rR[k * nf + f];
+      const double* ro = side ? rr : rl;
+      maxd2 = dmax(maxd2, ro[0] * ro[0] + ro[1] * ro[1] + ro[2] * ro[2]);
+      const double n[3] = {M.n[f], M.n[nf + f], M.n[2 * nf + f]};
+      const double A = M.area[f];
+      double ufn;
+      if (f < M.nfi) {
+        const int64_t a = side ? ch.nb[i] : c, b = side ? c : ch.nb[i];
+        double ua[5], ub[5];
+        q_arr(load_q(q, a), ua);
+        q_arr(load_q(q, b), ub);
+        const double* ga = grad + GPREC * a;
+        const double* gb = grad + GPREC * b;
+        double d[3], d2 = 0.0, dv[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          d[k] = rl[k] - rr[k];
+          d2 += d[k] * d[k];
+          dv[k] = 0.5 * (rl[k] + rr[k]);
+        }
+        double un = 0.0;
+#pragma unroll
+        for (int v = 1; v < 4; ++v) {
+          double gm[3];
+#pragma unroll
+          for (int k = 0; k < 3; ++k) gm[k] = 0.5 * (ga[3 * v + k] + gb[3 * v + k]);
+          const double cq = ((ub[v] - ua[v]) - (gm[0] * d[0] + gm[1] * d[1] + gm[2] * d[2])) / d2;
+          double gf[3];
+#pragma unroll
+          for (int k = 0; k < 3; ++k) gf[k] = gm[k] + cq * d[k];
+          const double uf = 0.5 * (ua[v] + ub[v]) + (gf[0] * dv[0] + gf[1] * dv[1] + gf[2] * dv[2]);
+          un += uf * n[v - 1];
+        }
+        ufn = un * A;
+      } else {
+        const double* pb = qb + 5 * (f - M.nfi);
+        ufn = (pb[1] * n[0] + pb[2] * n[1] + pb[3] * n[2]) * A;
+      }
+      veldiv += side ? -ufn : ufn;
+    }
+  }
+  const Q5 qc = load_q(q, c);
+  const double* gc = grad + GPREC * c;
+  const double V = M.vol[c];
+  const double len = 2. * sqrt(maxd2);
+  const double snd = sqrt(g.gamma * g.Rt * qc.T);
+  const double factor = P.comp * fabs(veldiv) * len / (snd * V);
+  const double alpha_comp = factor * factor;
+  const double theta2 = veldiv * veldiv / (V * V);
+  const double wx = gc[10] - gc[8], wy = gc[5] - gc[9], wz = gc[6] - gc[4];
+  const double vm = sqrt(wx * wx + wy * wy + wz * wz);
+  const double alpha_ducro = P.ducros * theta2 / (theta2 + vm * vm + 1e-10);
+  double al = dmax(alpha_ducro, alpha_comp);
+  al = dmin(al, P.dlim);
+  adiss[c] = dmax(al, P.upwind);
+}
+
+// ---------------------------------------------------------------------------
 // per-cell residual gather, local time step and norm partials
 // ---------------------------------------------------------------------------
 constexpr int NORM_THREADS = 256;
 
+template <bool BDF>
 __global__ void __launch_bounds__(NORM_THREADS)
 // qn, qnm1 (time-accurate BDF2, else null): the states of time levels n
 // and n-1; src then receives the rhs with the time terms
@@ -572,21 +741,8 @@ k_cell_residual(MeshView M, const double* __restrict__ q, const double* __restri
   if (c < M.nc) {
     double s[5] = {0, 0, 0, 0, 0};
     double meva = 0;
-    const int32_t e0 = M.cf_off[c], e1 = M.cf_off[c + 1];
-    // the first NPF face records are all requested before any is summed
-    // (a tet has 4 faces), then summed in the cell's face order; faces
-    // beyond NPF follow one by one in the same order
-    constexpr int NPF = 4;
-    int32_t ent[NPF];
-#pragma unroll
-    for (int j = 0; j < NPF; ++j) ent[j] = e0 + j < e1 ? __ldg(M.cf + e0 + j) : -1;
-    double2 rec[NPF][3];
-#pragma unroll
-    for (int j = 0; j < NPF; ++j)
-      if (ent[j] >= 0) {
-        const double2* p2 = reinterpret_cast<const double2*>(F + FREC * int64_t(ent[j] >> 1));
-        rec[j][0] = __ldg(p2), rec[j][1] = __ldg(p2 + 1), rec[j][2] = __ldg(p2 + 2);
-      }
+    // the face records four at a time from the entry-major lists, all four
+    // requested before any is summed, then summed in the cell's face order
     auto add = [&](int32_t en, const double2* r3) {
       const double p[5] = {r3[0].x, r3[0].y, r3[1].x, r3[1].y, r3[2].x};
       if (en & 1) {
@@ -598,14 +754,21 @@ k_cell_residual(MeshView M, const double* __restrict__ q, const double* __restri
       }
       meva += r3[2].y;
     };
+    for (int j0 = 0; j0 < M.K; j0 += ECH) {
+      int32_t ent[ECH];
 #pragma unroll
-    for (int j = 0; j < NPF; ++j)
-      if (ent[j] >= 0) add(ent[j], rec[j]);
-    for (int32_t e = e0 + NPF; e < e1; ++e) {
-      const int32_t en = __ldg(M.cf + e);
-      const double2* p2 = reinterpret_cast<const double2*>(F + FREC * int64_t(en >> 1));
-      const double2 r3[3] = {__ldg(p2), __ldg(p2 + 1), __ldg(p2 + 2)};
-      add(en, r3);
+      for (int i = 0; i < ECH; ++i)
+        ent[i] = j0 + i < M.K ? __ldg(M.ecf + int64_t(j0 + i) * M.nc + c) : -1;
+      double2 rec[ECH][3];
+#pragma unroll
+      for (int i = 0; i < ECH; ++i) {
+        const double2* p2 =
+            reinterpret_cast<const double2*>(F + FREC * int64_t(ent[i] >= 0 ? ent[i] >> 1 : 0));
+        rec[i][0] = __ldg(p2), rec[i][1] = __ldg(p2 + 1), rec[i][2] = __ldg(p2 + 2);
+      }
+#pragma unroll
+      for (int i = 0; i < ECH; ++i)
+        if (ent[i] >= 0) add(ent[i], rec[i]);
     }
     const double V = M.vol[c];
     const double cflpdt = 0.5 * meva / V;
@@ -628,7 +791,7 @@ k_cell_residual(MeshView M, const double* __restrict__ q, const double* __restri
     const double dp = rvol * (rT * (2.0 * qk * s[0] - dsu + s[4]) - fT * s[0]);
     dt = dmin(dt, urelax * p / (fabs(dp) + 1e-30));
     dtau[c] = dt;
-    if (qn) {
+    if (BDF) {
       // BDF2: s - 1.5 (Q(n+1) - Q(n)) V/dt + 0.5 (Q(n) - Q(n-1)) V/dt
       const Q5 a = load_q(qn, c), b = load_q(qnm1, c);
       const double rdtvol = V / dtmax;
@@ -1539,6 +1702,9 @@ dev::MeshView view(const fpsi_ctx* x) {
   M.Minv = x->d_Minv;
   M.cf_off = x->d_cf_off;
   M.cf = x->d_cf;
+  M.K = x->H.ell_k;
+  M.ecf = x->d_ecf;
+  M.enb = x->d_enb;
   M.bcs = x->d_bcs;
   return M;
 }
@@ -1550,6 +1716,16 @@ dev::Visc visc(const fpsi_ctx* x) {
   V.cp_prt = x->P.gamma * x->P.Rtilde / (x->P.gamma - 1.0) / x->P.Prt;
   V.tmu = x->d_tmu;
   return V;
+}
+dev::Lds lds(const fpsi_ctx* x) {
+  dev::Lds L;
+  L.comp = x->P.lds_comp_factor;
+  L.dlim = x->P.lds_dissipation_limit;
+  L.ducros = x->P.lds_ducros_factor;
+  L.upwind = x->P.lds_use_upwind;
+  L.nscoeff = x->P.lds_nonsym_coeff;
+  L.nsfactor = x->P.lds_nonsym_factor;
+  return L;
 }
 dev::Gas gas(const fpsi_ctx* x) {
   dev::Gas g;
@@ -1582,16 +1758,32 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
                                                          x->d_err + 1, x->d_qb);
     prof_end(x);
   }
+  const bool kec = x->P.flux == FPSI_FLUX_KEC;
+  if (kec) {
+    if (!x->d_adiss) {
+      FPSI_CUDA_TRY(cudaMalloc(&x->d_adiss, size_t(M.nc) * sizeof(double)));
+      FPSI_CUDA_TRY(cudaMalloc(&x->d_ageom, size_t(std::max<int64_t>(M.nfi, 1)) * sizeof(float)));
+    }
+    if (x->ageom_coeff != x->P.lds_nonsym_coeff || x->ageom_factor != x->P.lds_nonsym_factor) {
+      if (M.nfi > 0)
+        dev::k_alpha_geom<<<blocks_for(M.nfi, T), T, 0, s>>>(M, lds(x), x->d_ageom);
+      x->ageom_coeff = x->P.lds_nonsym_coeff;
+      x->ageom_factor = x->P.lds_nonsym_factor;
+    }
+  }
   prof_begin(x, "grad_limiter");
   // the gradient records are written every residual only where the viscous
-  // terms (and the SA model) read them
-  x->grad_valid = x->P.viscous != 0;
+  // terms, the SA model and the KEC flux read them
+  x->grad_valid = x->P.viscous != 0 || kec;
   if (x->grad_valid)
     dev::k_grad_limiter<true><<<blocks_for(M.nc, dev::GRAD_THREADS), dev::GRAD_THREADS, 0, s>>>(
         M, x->d_q, x->d_qb, x->P.limiter, x->P.Kl, g, x->d_grad, x->d_qf);
   else
     dev::k_grad_limiter<false><<<blocks_for(M.nc, dev::GRAD_THREADS), dev::GRAD_THREADS, 0, s>>>(
         M, x->d_q, x->d_qb, x->P.limiter, x->P.Kl, g, x->d_grad, x->d_qf);
+  if (kec)
+    dev::k_alpha_diss<<<blocks_for(M.nc, dev::AD_THREADS), dev::AD_THREADS, 0, s>>>(
+        M, x->d_q, x->d_qb, x->d_grad, g, lds(x), x->d_adiss);
   prof_end(x);
   prof_begin(x, "face_flux");
   // the viscous terms and each Riemann solver are separate instantiations:
@@ -1600,15 +1792,18 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
     const unsigned nb = blocks_for(M.nf, 128);
     const dev::Visc Vv = visc(x);
     double* F = x->d_F;
-#define FPSI_FLUX(VIS, K) \
-  dev::k_face_flux<VIS, K><<<nb, 128, 0, s>>>(M, x->d_q, x->d_qb, x->d_grad, x->d_qf, g, Vv, F)
+#define FPSI_FLUX(VIS, K)                                                                     \
+  dev::k_face_flux<VIS, K><<<nb, 128, 0, s>>>(M, x->d_q, x->d_qb, x->d_grad, x->d_qf, g, Vv, F, \
+                                              x->d_adiss, x->d_ageom)
     if (x->P.viscous) {
       if (x->P.flux == FPSI_FLUX_ROE) FPSI_FLUX(true, FPSI_FLUX_ROE);
       else if (x->P.flux == FPSI_FLUX_HLLE) FPSI_FLUX(true, FPSI_FLUX_HLLE);
+      else if (kec) FPSI_FLUX(true, FPSI_FLUX_KEC);
       else FPSI_FLUX(true, FPSI_FLUX_HLLC);
     } else {
       if (x->P.flux == FPSI_FLUX_ROE) FPSI_FLUX(false, FPSI_FLUX_ROE);
       else if (x->P.flux == FPSI_FLUX_HLLE) FPSI_FLUX(false, FPSI_FLUX_HLLE);
+      else if (kec) FPSI_FLUX(false, FPSI_FLUX_KEC);
       else FPSI_FLUX(false, FPSI_FLUX_HLLC);
     }
 #undef FPSI_FLUX
@@ -1624,9 +1819,14 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
                                   cudaMemcpyDeviceToDevice, s));
     x->have_levels = true;
   }
-  dev::k_cell_residual<<<x->nblk_norm, dev::NORM_THREADS, 0, s>>>(
-      M, x->d_q, x->d_F, g, x->P.urelax, x->P.dtmax, x->P.cflmax, x->H.vol_tot,
-      bdf ? x->d_qn : nullptr, bdf ? x->d_qnm1 : nullptr, x->d_src, x->d_dtau, x->d_part);
+  if (bdf)
+    dev::k_cell_residual<true><<<x->nblk_norm, dev::NORM_THREADS, 0, s>>>(
+        M, x->d_q, x->d_F, g, x->P.urelax, x->P.dtmax, x->P.cflmax, x->H.vol_tot, x->d_qn, x->d_qnm1,
+        x->d_src, x->d_dtau, x->d_part);
+  else
+    dev::k_cell_residual<false><<<x->nblk_norm, dev::NORM_THREADS, 0, s>>>(
+        M, x->d_q, x->d_F, g, x->P.urelax, x->P.dtmax, x->P.cflmax, x->H.vol_tot, nullptr, nullptr,
+        x->d_src, x->d_dtau, x->d_part);
   dev::k_norm_final<<<1, dev::NORM_THREADS, 0, s>>>(x->d_part, x->nblk_norm, x->d_err + 1, resid_slot);
   prof_end(x);
   FPSI_CUDA_TRY(cudaGetLastError());

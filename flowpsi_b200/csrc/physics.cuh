@@ -562,6 +562,78 @@ __device__ __forceinline__ void riemann1(int kind, const Q5& L, const Q5& R, dou
     flux_hllc(L, R, nx, ny, nz, area, g, 0.0, 1.0, F);
 }
 
+// ---- low-dissipation (KEC) flux, fluxLowDiss.loci -----------------------
+// The central kinetic-energy-consistent flux of two states through a face of
+// area A (kec_flux, fluxLowDiss.loci:258-298), added to F: the mean velocity
+// and gauge pressure, the density-averaged temperature, the internal energy
+// of the mean temperature and the kinetic energy |u_f|^2 - (|u_l|^2 + |u_r|^2)/4.
+__device__ __forceinline__ void kec_flux_add(const Q5& l, const Q5& r, double nx, double ny,
+                                             double nz, double A, const Gas& g, double F[5]) {
+  const double ux = 0.5 * (l.u + r.u), uy = 0.5 * (l.v + r.v), uz = 0.5 * (l.w + r.w);
+  const double ufn = ux * nx + uy * ny + uz * nz;
+  const double pgf = 0.5 * (l.p + r.p);
+  const double tf =
+      l.T * r.T * (l.p + r.p + 2 * g.pamb) / ((l.p + g.pamb) * r.T + (r.p + g.pamb) * l.T);
+  const double rf = (pgf + g.pamb) / (g.Rt * tf);
+  const double mdot = rf * ufn;
+  F[0] += A * mdot;
+  F[1] += A * (mdot * ux + pgf * nx);
+  F[2] += A * (mdot * uy + pgf * ny);
+  F[3] += A * (mdot * uz + pgf * nz);
+  const double ei = 0.5 * g.Rt * (l.T + r.T) / (g.gamma - 1);
+  const double ke = (ux * ux + uy * uy + uz * uz) -
+                    0.25 * ((l.u * l.u + l.v * l.v + l.w * l.w) + (r.u * r.u + r.v * r.v + r.w * r.w));
+  F[4] += A * (mdot * (ke + ei) + ufn * (pgf + g.pamb));
+}
+
+// KEC::iflux of an interior face (fluxLowDiss.loci:320-431).  L, R: the
+// MUSCL face states with their floors; qa, qb: the two cell states; ga, gb:
+// their gradient (15) and limiter (5) records; dv = x_f - (x_l + x_r) / 2;
+// aa, ab: the cells' alpha_diss; ag: the face's alpha_geom_f.  The upwind
+// part is hllc_flux (inviscidRiemannFlux, inviscidFlux.h:82-90) of the
+// Thornber-preconditioned states on the area A alpha, the central part
+// kec_flux of the states reconstructed to dv on the area A (1 - alpha).
+__device__ __forceinline__ void kec_face(const Q5& L, const Q5& R, const Q5& qa, const Q5& qb,
+                                         const double* ga, const double* gb, double dvx,
+                                         double dvy, double dvz, double aa, double ab, double ag,
+                                         double nx, double ny, double nz, double A, const Gas& g,
+                                         double F[5]) {
+  const double pglim = 0.1 * dmin(qa.p, qb.p) + -0.9 * g.pamb;
+  const double tlim = 0.1 * dmin(qa.T, qb.T);
+  const double rl = (L.p + g.pamb) / (g.Rt * L.T), rr = (R.p + g.pamb) / (g.Rt * R.T);
+  const double al2 = g.gamma * g.Rt * L.T, ar2 = g.gamma * g.Rt * R.T;
+  const double dp = 2. * fabs(L.p - R.p) / dmax(rl * al2, rr * ar2);
+  const double alpha_c = dmax(dmax(aa, ab), dmin(1.0, dp * 1.0 - 0.5));
+  const double alpha = dmax(alpha_c, ag);
+#pragma unroll
+  for (int i = 0; i < 5; ++i) F[i] = 0.0;
+  if (alpha > 1e-10) {
+    const double amin = sqrt(dmin(al2, ar2));
+    const double utmax = dmax(fabs(L.u * nx + L.v * ny + L.w * nz), fabs(R.u * nx + R.v * ny + R.w * nz));
+    const double Ma = dmax(alpha_c, dmin(1.0, utmax / amin + 1e-4));
+    const double h = 0.5 * (1. - Ma);
+    Q5 Lp = L, Rp = R;
+    Lp.u = L.u + h * (R.u - L.u), Lp.v = L.v + h * (R.v - L.v), Lp.w = L.w + h * (R.w - L.w);
+    Rp.u = R.u + h * (L.u - R.u), Rp.v = R.v + h * (L.v - R.v), Rp.w = R.w + h * (L.w - R.w);
+    flux_hllc(Lp, Rp, nx, ny, nz, A * alpha, g, 0.0, 1.0, F);
+  }
+  auto at = [&](const Q5& c, const double* gr, Q5& o) {
+    const double* ph = gr + 15;
+    double d[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) d[k] = gr[3 * k] * dvx + gr[3 * k + 1] * dvy + gr[3 * k + 2] * dvz;
+    o.p = dmax(c.p + ph[4] * d[4], pglim);
+    o.T = dmax(c.T + ph[0] * d[0], tlim);
+    o.u = c.u + ph[1] * d[1];
+    o.v = c.v + ph[2] * d[2];
+    o.w = c.w + ph[3] * d[3];
+  };
+  Q5 l, r;
+  at(qa, ga, l);
+  at(qb, gb, r);
+  kec_flux_add(l, r, nx, ny, nz, A * (1. - alpha), g, F);
+}
+
 // ---- boundary states from total conditions or a mass flux ---------------
 // Each returns the face state (T, u, v, w, pg) from the cell-centre state qi
 // of the face's cell; n is the outward unit normal, the flow direction of

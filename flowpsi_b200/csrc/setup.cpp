@@ -314,6 +314,18 @@ int build_host_mesh(const fpsi_mesh* m, HostMesh& h) {
       }
     }
   }
+  // ---- the same lists entry-major ----
+  h.ell_k = 0;
+  for (int64_t c = 0; c < nc; ++c) h.ell_k = std::max(h.ell_k, h.cf_off[c + 1] - h.cf_off[c]);
+  h.ecf.assign(size_t(h.ell_k) * nc, -1);
+  h.enb.assign(size_t(h.ell_k) * nc, -1);
+  for (int64_t c = 0; c < nc; ++c)
+    for (int32_t e = h.cf_off[c]; e < h.cf_off[c + 1]; ++e) {
+      const size_t at = size_t(e - h.cf_off[c]) * nc + c;
+      const int64_t f = h.cf[e] >> 1;
+      h.ecf[at] = h.cf[e];
+      if (h.cr[f] >= 0) h.enb[at] = (h.cf[e] & 1) ? h.cl[f] : h.cr[f];
+    }
   // ---- least-squares normal matrices (inverse, symmetric 6 entries) ----
   h.Minv.assign(nc * 6, 0.0);
   for (int64_t c = 0; c < nc; ++c) {

@@ -52,7 +52,10 @@ extern "C" {
 enum fpsi_flux_kind {          /* inviscidRiemannFlux, inviscidFlux.h:82-90 */
   FPSI_FLUX_HLLC = 0,          /* hllc_flux, fluxInviscid.loci:157-256 (reference default) */
   FPSI_FLUX_ROE  = 1,          /* roeCT_flux, fluxInviscid.loci:869-1014 */
-  FPSI_FLUX_HLLE = 2           /* two-wave HLL with hllc_flux's SL/SR (no reference counterpart) */
+  FPSI_FLUX_HLLE = 2,          /* two-wave HLL with hllc_flux's SL/SR (no reference counterpart) */
+  FPSI_FLUX_KEC  = 3           /* inviscidFlux "KEC": kinetic-energy-consistent low-dissipation
+                                  flux on interior faces (KEC::iflux, fluxLowDiss.loci:320-431),
+                                  hllc_flux on boundary faces */
 };
 enum fpsi_limiter_kind {       /* vars 'limiter' (guide.tex:495-518) */
   FPSI_LIMITER_VENKATAKRISHNAN = 0,
@@ -129,6 +132,13 @@ typedef struct fpsi_params {
                               (solverTimestep.loci:397-428); dtmax is then the time step */
   int32_t newton_iters;    /* newtonMaxIter: Newton iterations per time step, 6
                                                                    solverNewton.loci:200-210 */
+  /* the low-dissipation (KEC) flux's switches, fluxLowDiss.loci:82-120 */
+  double lds_comp_factor;       /* LDS_compFactor 5 */
+  double lds_dissipation_limit; /* LDS_dissipationLimit 1 */
+  double lds_ducros_factor;     /* LDS_ducrosFactor 0 */
+  double lds_use_upwind;        /* LDS_useUpwind 0 */
+  double lds_nonsym_coeff;      /* LDS_nonSymmetricCoeff 2 */
+  double lds_nonsym_factor;     /* LDS_nonSymmetricFactor 1 */
 } fpsi_params;
 
 typedef struct fpsi_bc {

@@ -36,14 +36,30 @@ def unpack(w: np.ndarray):
     return t, [t[a:b].view(*shape) for a, b, shape in parts]
 
 
-def neighbour_mean_matrix(nc: int, cl: np.ndarray, cr: np.ndarray) -> torch.Tensor:
-    inner = cr >= 0
-    a, b = cl[inner].astype(np.int64), cr[inner].astype(np.int64)
-    rows = np.concatenate([a, b])
-    cols = np.concatenate([b, a])
-    deg = np.bincount(rows, minlength=nc).astype(np.float32)
-    vals = 1.0 / deg[rows]
-    return torch.sparse_coo_tensor(np.vstack([rows, cols]), vals, (nc, nc)).coalesce()
+class NeighbourMean:
+    """mean of the face neighbours' rows as the device forms it: the rows
+    summed in FP32, then multiplied by the FP32 reciprocal of the degree
+    (k_layer_tc / k_layer_ws: sum * (1.0f / deg)); for degrees that are not
+    powers of two this differs in the last bits from summing rows / deg"""
+
+    def __init__(self, nc: int, cl: np.ndarray, cr: np.ndarray):
+        inner = cr >= 0
+        a, b = cl[inner].astype(np.int64), cr[inner].astype(np.int64)
+        rows = np.concatenate([a, b])
+        cols = np.concatenate([b, a])
+        deg = np.bincount(rows, minlength=nc).astype(np.float32)
+        with np.errstate(divide="ignore"):
+            inv = np.where(deg > 0, np.float32(1.0) / deg, np.float32(0.0)).astype(np.float32)
+        self.S = torch.sparse_coo_tensor(np.vstack([rows, cols]), np.ones(len(rows), np.float32),
+                                         (nc, nc)).coalesce()
+        self.inv = torch.from_numpy(inv)
+
+    def __call__(self, h: torch.Tensor) -> torch.Tensor:
+        return torch.sparse.mm(self.S, h) * self.inv[:, None]
+
+
+def neighbour_mean_matrix(nc: int, cl: np.ndarray, cr: np.ndarray) -> NeighbourMean:
+    return NeighbourMean(nc, cl, cr)
 
 
 def bf16(x: torch.Tensor) -> torch.Tensor:
@@ -68,8 +84,9 @@ def loss_and_grad(w: np.ndarray, feat: np.ndarray, target: np.ndarray, A: torch.
     h = torch.from_numpy(np.ascontiguousarray(feat, np.float32))
     for l in range(NLAYER):
         ws, wn, b = p[3 * l], p[3 * l + 1], p[3 * l + 2]
-        agg = bf16(torch.sparse.mm(A, h))  # mean of the layer input, rounded
-        h = bf16(gelu_tanh(bf16(h) @ ws.T + agg @ wn.T + b))
+        hb = bf16(h)  # the layer input as the network sees it (FP32 features rounded)
+        agg = bf16(A(hb))  # mean of the neighbours' inputs, rounded
+        h = bf16(gelu_tanh(hb @ ws.T + agg @ wn.T + b))
     y = h @ p[-2].T + p[-1]
     t = torch.from_numpy(np.ascontiguousarray(target, np.float32))
     if mask is None:

@@ -1196,6 +1196,146 @@ extern "C" int orc_set_eddy_viscosity(orc_ctx* o, const double* tmu) {
   return FPSI_OK;
 }
 
+// ---- low-dissipation (KEC) flux, fluxLowDiss.loci ----------------------
+// alpha_geom_f (fluxLowDiss.loci:122-138), rounded to FP32 (store<realF>).
+// With rL = x_f - x_l and rR = x_f - x_r: df = x_r - x_l = rL - rR and
+// dv = x_f - (x_l + x_r)/2 = (rL + rR)/2.
+static float alpha_geom(const orc_ctx* o, int64_t f) {
+  const V3 rl = v3(&o->rL[3 * f]), rr = v3(&o->rR[3 * f]);
+  const V3 df = rl - rr, dv = 0.5 * (rl + rr);
+  const double ndv = norm(dv), ndf = norm(df);
+  const double cosa = std::min(std::sqrt(std::max(1. - 2. * ndv / ndf, 0.0)),
+                               dot(v3(&o->an[3 * f]), df) / ndf);
+  const double scale = o->P.lds_nonsym_coeff;
+  const double s = o->P.lds_nonsym_factor / std::max(scale, 1.0);
+  const double x = std::min(scale * (1. - cosa), 1.0);
+  const double x2 = x * x, x3 = x2 * x;
+  return float(x2 + s * (x3 - 2. * x2 + x));
+}
+
+// alpha_diss of every cell (fluxLowDiss.loci:141-176): veldiv from ufn
+// (fluxLowDiss.loci:61-78) summed over the cell's faces, + on the cl side,
+// in the cell's face order (upper, lower, boundary); interior faces use the
+// face gradient of u of the viscous terms (viscous_face), boundary faces the
+// boundary velocity.  vortMag from the cell gradient (solverTurbulence.loci:45-79).
+static void alpha_diss(const orc_ctx* o, std::vector<double>& ad) {
+  const int64_t nc = o->nc;
+  const fpsi_params& P = o->P;
+  ad.assign(nc, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < nc; ++c) {
+    double veldiv = 0.0, maxd2 = 0.0;
+    auto interior = [&](int64_t f, double sign) {
+      const int64_t a = o->cl[f], b = o->cr[f];
+      const V3 rl = v3(&o->rL[3 * f]), rr = v3(&o->rR[3 * f]);
+      const V3 d = rl - rr, dv = 0.5 * (rl + rr);
+      const double d2 = dot(d, d);
+      const double* ga = &o->grad[15 * a];
+      const double* gb = &o->grad[15 * b];
+      double uf[3];
+      for (int v = 1; v < 4; ++v) {
+        const V3 gm = 0.5 * (v3(ga + 3 * v) + v3(gb + 3 * v));
+        const double ua = o->u[3 * a + v - 1], ub = o->u[3 * b + v - 1];
+        const double cq = ((ub - ua) - dot(gm, d)) / d2;
+        const V3 gf = gm + cq * d;
+        uf[v - 1] = 0.5 * (ua + ub) + dot(gf, dv);
+      }
+      const double ufn = dot(mk(uf[0], uf[1], uf[2]), v3(&o->an[3 * f])) * o->area[f];
+      veldiv += sign * ufn;
+    };
+    for (int64_t k = o->up_off[c]; k < o->up_off[c + 1]; ++k) {
+      const int64_t f = o->up[k];
+      maxd2 = std::max(maxd2, dot(v3(&o->rL[3 * f]), v3(&o->rL[3 * f])));
+      interior(f, 1.0);
+    }
+    for (int64_t k = o->lo_off[c]; k < o->lo_off[c + 1]; ++k) {
+      const int64_t f = o->lo[k];
+      maxd2 = std::max(maxd2, dot(v3(&o->rR[3 * f]), v3(&o->rR[3 * f])));
+      interior(f, -1.0);
+    }
+    for (int64_t k = o->bd_off[c]; k < o->bd_off[c + 1]; ++k) {
+      const int64_t f = o->bd[k];
+      maxd2 = std::max(maxd2, dot(v3(&o->rL[3 * f]), v3(&o->rL[3 * f])));
+      const double* qb = &o->qb[5 * f];
+      veldiv += dot(mk(qb[1], qb[2], qb[3]), v3(&o->an[3 * f])) * o->area[f];
+    }
+    const double V = o->vol[c];
+    const double len = 2. * std::sqrt(maxd2);
+    const double a = std::sqrt(P.gamma * P.Rtilde * o->T[c]);
+    const double factor = P.lds_comp_factor * std::fabs(veldiv) * len / (a * V);
+    const double alpha_comp = factor * factor;
+    const double theta_2 = veldiv * veldiv / (V * V);
+    const double* g = &o->grad[15 * c];
+    const V3 w = mk(g[10] - g[8], g[5] - g[9], g[6] - g[4]);
+    const double vm = norm(w);
+    const double alpha_ducro = P.lds_ducros_factor * theta_2 / (theta_2 + vm * vm + 1e-10);
+    double al = std::max(alpha_ducro, alpha_comp);
+    al = std::min(al, P.lds_dissipation_limit);
+    ad[c] = std::max(al, P.lds_use_upwind);
+  }
+}
+
+// kec_flux (fluxLowDiss.loci:258-298), added to F
+static void kec_flux(double F[5], double pgl, double Tl, V3 Ul, double pgr, double Tr, V3 Ur,
+                     V3 an, double area, double pamb, double Rt, double gamma) {
+  const V3 uf = 0.5 * (Ul + Ur);
+  const double ufn = dot(uf, an);
+  const double pgf = 0.5 * (pgl + pgr);
+  const double tf = Tl * Tr * (pgl + pgr + 2 * pamb) / ((pgl + pamb) * Tr + (pgr + pamb) * Tl);
+  const double rf = (pgf + pamb) / (Rt * tf);
+  const double mdot = rf * ufn;
+  F[0] += area * mdot;
+  F[1] += area * (mdot * uf.x + pgf * an.x);
+  F[2] += area * (mdot * uf.y + pgf * an.y);
+  F[3] += area * (mdot * uf.z + pgf * an.z);
+  const double e_internalf = 0.5 * Rt * (Tl + Tr) / (gamma - 1);
+  const double ke_f = dot(uf, uf) - 0.25 * (dot(Ul, Ul) + dot(Ur, Ur));
+  F[4] += area * (mdot * (ke_f + e_internalf) + ufn * (pgf + pamb));
+}
+
+// KEC::iflux of interior face f (fluxLowDiss.loci:320-431); qL, qR are the
+// MUSCL face states with their floors (face_states)
+static void kec_iflux(const orc_ctx* o, int64_t f, const double qL[5], const double qR[5],
+                      const std::vector<double>& ad, double F[5]) {
+  const fpsi_params& P = o->P;
+  const int64_t a = o->cl[f], b = o->cr[f];
+  const V3 an = v3(&o->an[3 * f]);
+  const double A = o->area[f];
+  const double pglim = 0.1 * std::min(o->pg[a], o->pg[b]) + -0.9 * P.Pambient;
+  const double tlim = 0.1 * std::min(o->T[a], o->T[b]);
+  const double pgL = qL[4], pgR = qR[4], tL = qL[0], tR = qR[0];
+  const double rL = (pgL + P.Pambient) / (P.Rtilde * tL);
+  const double rR = (pgR + P.Pambient) / (P.Rtilde * tR);
+  const double al2 = P.gamma * P.Rtilde * tL, ar2 = P.gamma * P.Rtilde * tR;
+  const double dp = 2. * std::fabs(pgL - pgR) / std::max(rL * al2, rR * ar2);
+  const double alpha_c = std::max(std::max(ad[a], ad[b]), std::min(1.0, dp * 1.0 - 0.5));
+  const double alpha = std::max(alpha_c, double(alpha_geom(o, f)));
+  for (int i = 0; i < 5; ++i) F[i] = 0;
+  if (alpha > 1e-10) {
+    const V3 uL = mk(qL[1], qL[2], qL[3]), uR = mk(qR[1], qR[2], qR[3]);
+    const double amin = std::sqrt(std::min(al2, ar2));
+    const double utmax = std::max(std::fabs(dot(uL, an)), std::fabs(dot(uR, an)));
+    const double Ma = std::max(alpha_c, std::min(1.0, utmax / amin + 1e-4));
+    const V3 uLp = uL + 0.5 * (1. - Ma) * (uR - uL);
+    const V3 uRp = uR + 0.5 * (1. - Ma) * (uL - uR);
+    hllc_flux(F, pgL, tL, uLp, pgR, tR, uRp, an, A * alpha, P.Pambient, P.Rtilde, P.gamma, 0.0, 1.0);
+  }
+  const V3 dv = 0.5 * (v3(&o->rL[3 * f]) + v3(&o->rR[3 * f]));
+  auto at = [&](int64_t c, double& pg, double& t, V3& u) {
+    const double* g = &o->grad[15 * c];
+    const double* ph = &o->phi[5 * c];
+    pg = std::max(o->pg[c] + ph[4] * dot(v3(g + 12), dv), pglim);
+    t = std::max(o->T[c] + ph[0] * dot(v3(g), dv), tlim);
+    u = mk(o->u[3 * c] + ph[1] * dot(v3(g + 3), dv), o->u[3 * c + 1] + ph[2] * dot(v3(g + 6), dv),
+           o->u[3 * c + 2] + ph[3] * dot(v3(g + 9), dv));
+  };
+  double pg_l, t_l, pg_r, t_r;
+  V3 u_l, u_r;
+  at(a, pg_l, t_l, u_l);
+  at(b, pg_r, t_r, u_r);
+  kec_flux(F, pg_l, t_l, u_l, pg_r, t_r, u_r, an, A * (1. - alpha), P.Pambient, P.Rtilde, P.gamma);
+}
+
 extern "C" int orc_residual(orc_ctx* o, double* src_out, fpsi_resid* norms) {
   const int64_t nc = o->nc, nf = o->nf;
   const fpsi_params& P = o->P;
@@ -1237,6 +1377,9 @@ extern "C" int orc_residual(orc_ctx* o, double* src_out, fpsi_resid* norms) {
   for (int64_t f = 0; f < nf; ++f)
     if (o->cr[f] < 0) o->bc_err |= bc_face_state(o, f, &o->qb[5 * f]);
   gradients_and_limiters(o);
+  const bool kec = P.flux == FPSI_FLUX_KEC;
+  std::vector<double> adiss;
+  if (kec) alpha_diss(o, adiss);
   o->F.assign(nf * 5, 0);
   o->maxev.assign(nf, 0);
 #pragma omp parallel for schedule(static)
@@ -1256,10 +1399,13 @@ extern "C" int orc_residual(orc_ctx* o, double* src_out, fpsi_resid* norms) {
       const double* b = &o->qb[5 * f];
       state_flux(&o->F[5 * f], b[4], b[0], mk(b[1], b[2], b[3]), n, o->area[f], P.Pambient,
                  P.Rtilde, P.gamma);
+    } else if (kec && o->cr[f] >= 0) {
+      kec_iflux(o, f, qL, qR, adiss, &o->F[5 * f]);
     } else {
-      riemann_flux(P.flux, &o->F[5 * f], qL[4], qL[0], mk(qL[1], qL[2], qL[3]), qR[4], qR[0],
-                   mk(qR[1], qR[2], qR[3]), n, o->area[f], P.Pambient, P.Rtilde, P.gamma, 0.0,
-                   1.0);
+      // boundary faces of the KEC scheme: inviscidRiemannFlux (inviscidFlux.h:82-90)
+      riemann_flux(kec ? FPSI_FLUX_HLLC : P.flux, &o->F[5 * f], qL[4], qL[0],
+                   mk(qL[1], qL[2], qL[3]), qR[4], qR[0], mk(qR[1], qR[2], qR[3]), n, o->area[f],
+                   P.Pambient, P.Rtilde, P.gamma, 0.0, 1.0);
     }
     if (P.viscous) {
       // src[cl] += vflux, src[cr] -= vflux (fluxViscous.loci:299-310)

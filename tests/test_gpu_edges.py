@@ -102,7 +102,7 @@ def test_malformed_meshes_are_refused(need_gpu):
 
 
 @pytest.mark.parametrize("field,value", [("flux", 3), ("limiter", -1), ("precision", 5),
-                                         ("gauss_seidel_iter", -1), ("solver", 2),
+                                         ("gauss_seidel_iter", -1), ("solver", 3),
                                          ("viscous", 3), ("turbulence", 2)])
 def test_bad_parameters_are_refused(need_gpu, field, value):
     p = default_params(precision="fp64")

@@ -62,6 +62,12 @@ def test_face_functions_vs_oracle(need_gpu):
 # --------------------------------------------------------------------------
 # mesh level
 # --------------------------------------------------------------------------
+def _kec(case):
+    """the same case with the low-dissipation KEC flux (fluxLowDiss.loci:320-431)"""
+    case.params.flux = 3
+    return case
+
+
 CASES = {
     "farfield_hex": lambda prec: cases.farfield_cube(8, precision=prec),
     "tgv_tets": lambda prec: cases.taylor_green_tets(5, precision=prec),
@@ -73,6 +79,9 @@ CASES = {
     "isentropic_in": lambda prec: cases.outflow_duct(6, precision=prec, inflow="isentropic"),
     "fixedmass_in": lambda prec: cases.outflow_duct(6, precision=prec, inflow="fixedMass"),
     "fixedmass_out": lambda prec: cases.outflow_duct(6, precision=prec, outflow="fixedMassOutflow"),
+    "kec_tgv_tets": lambda prec: _kec(cases.taylor_green_tets(5, precision=prec)),
+    "kec_farfield_hex": lambda prec: _kec(cases.farfield_cube(6, precision=prec)),
+    "kec_shock_hex": lambda prec: _kec(cases.oblique_shock_cube(8, precision=prec)),
 }
 
 

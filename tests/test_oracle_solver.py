@@ -233,3 +233,63 @@ def test_fsgs_reaches_the_sgs_steady_state():
         out.append(o.get_state())
     for a, b in zip(*out):
         assert np.abs(a - b).max() <= 1e-9 * np.abs(b).max()
+
+
+def _kec_case(**lds):
+    case = cases.taylor_green_tets(5, precision="fp64")
+    case.params.flux = 3  # KEC
+    for k, v in lds.items():
+        setattr(case.params, k, v)
+    return case
+
+
+def test_kec_preserves_uniform_flow():
+    """uniform flow on the jittered periodic tet grid: alpha_diss is 0 (no
+    divergence), the upwind part sees equal states and the central kinetic-
+    energy-consistent flux (fluxLowDiss.loci:258-298) of equal states is the
+    analytic flux, so the residual is round-off"""
+    case = _kec_case()
+    o = Oracle(case.mesh, case.params)
+    nc = o.ncells
+    o.set_state(np.full(nc, 300.0), np.full(nc, 1e5), np.tile([30.0, -20.0, 10.0], (nc, 1)))
+    src, _ = o.residual()
+    rho, a = 1e5 / (287.05 * 300.0), 347.0
+    scale = rho * (40.0 + a) * (287.05 * 300.0 / 0.4) * o.geometry()["area"].max()
+    assert np.abs(src).max() < 1e-14 * scale
+
+
+def test_kec_with_full_upwinding_is_hllc():
+    """LDS_useUpwind = 1 makes alpha_diss = 1 on every cell, so alpha = 1,
+    the Thornber factor Ma = 1 and the central part has zero area: the KEC
+    flux is hllc_flux of the face states (fluxLowDiss.loci:371-399)"""
+    c_kec = _kec_case(lds_use_upwind=1.0)
+    c_hllc = cases.taylor_green_tets(5, precision="fp64")
+    c_hllc.params.flux = 0
+    a, b = Oracle(c_kec.mesh, c_kec.params), Oracle(c_hllc.mesh, c_hllc.params)
+    st = c_kec.initial_state(a.geometry()["cellcenter"])
+    a.set_state(*st)
+    b.set_state(*st)
+    sa, _ = a.residual()
+    sb, _ = b.residual()
+    assert np.array_equal(sa, sb)
+
+
+def test_kec_differs_from_hllc_and_steps():
+    """on the Taylor-Green state (M = 0.1, smooth) alpha_diss and the
+    geometric switch stay small, so the KEC residual is mostly the central
+    flux and differs from HLLC's; an implicit step with it (the Jacobians
+    stay the Roe ones, inviscidFlux.h:92-107) lowers the residual"""
+    case = _kec_case()
+    o = Oracle(case.mesh, case.params)
+    st = case.initial_state(o.geometry()["cellcenter"])
+    o.set_state(*st)
+    c_hllc = cases.taylor_green_tets(5, precision="fp64")
+    c_hllc.params.flux = 0
+    h = Oracle(c_hllc.mesh, c_hllc.params)
+    h.set_state(*st)
+    sk, _ = o.residual()
+    sh, _ = h.residual()
+    assert np.abs(sk - sh).max() > 1e-6 * np.abs(sh).max()
+    r0 = o.newton_step()
+    r1 = o.newton_step()
+    assert np.isfinite(r1["rtrms"]) and r1["rtrms"] < r0["rtrms"]
