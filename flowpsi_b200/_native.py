@@ -18,7 +18,7 @@ ERRORS = {
     -5: "FPSI_E_SINGULAR", -6: "FPSI_E_NAN", -7: "FPSI_E_TIMEOUT", -8: "FPSI_E_STATE",
 }
 
-FLUX = {"hllc": 0, "roe": 1, "hlle": 2, "kec": 3}
+FLUX = {"hllc": 0, "roe": 1, "hlle": 2, "kec": 3, "ssf": 4}
 LIMITER = {"venkatakrishnan": 0, "barth": 1, "none": 2, "zero": 3}
 SOLVER = {"sgs": 0, "lsgs": 1, "fsgs": 2}
 PRECISION = {"fp64": 0, "ref": 1, "mixed": 2}
@@ -42,6 +42,7 @@ class Params(C.Structure):
         ("lds_comp_factor", C.c_double), ("lds_dissipation_limit", C.c_double),
         ("lds_ducros_factor", C.c_double), ("lds_use_upwind", C.c_double),
         ("lds_nonsym_coeff", C.c_double), ("lds_nonsym_factor", C.c_double),
+        ("lds_miles_filter", C.c_double), ("ssf_coeff", C.c_double),
     ]
 
 

@@ -213,7 +213,7 @@ bool is_lsgs(const fpsi_ctx* x) { return x->P.solver == FPSI_SOLVER_LSGS; }
 
 int check_params(const fpsi_params* p) {
   if (!p) return FPSI_E_INVALID;
-  if (!(p->gamma > 1.0) || !(p->Rtilde > 0) || p->flux < 0 || p->flux > FPSI_FLUX_KEC || p->limiter < 0 ||
+  if (!(p->gamma > 1.0) || !(p->Rtilde > 0) || p->flux < 0 || p->flux > FPSI_FLUX_SSF || p->limiter < 0 ||
       p->limiter > 3 || p->precision < 0 || p->precision > 2 || p->gauss_seidel_iter < 0) {
     fpsi::set_error("invalid parameter value");
     return FPSI_E_INVALID;
@@ -247,9 +247,10 @@ int check_params(const fpsi_params* p) {
     fpsi::set_error("the SA model is advanced in steady mode only");
     return FPSI_E_UNSUPPORTED;
   }
-  if (p->flux == FPSI_FLUX_KEC &&
+  if ((p->flux == FPSI_FLUX_KEC || p->flux == FPSI_FLUX_SSF) &&
       (!(p->lds_comp_factor >= 0) || !(p->lds_dissipation_limit >= 0) || !(p->lds_ducros_factor >= 0) ||
-       !(p->lds_use_upwind >= 0) || !(p->lds_nonsym_coeff > 0) || !(p->lds_nonsym_factor >= 0))) {
+       !(p->lds_use_upwind >= 0) || !(p->lds_nonsym_coeff > 0) || !(p->lds_nonsym_factor >= 0) ||
+       !(p->lds_miles_filter >= 0) || !(p->ssf_coeff == p->ssf_coeff))) {
     fpsi::set_error("low-dissipation flux switches out of range");
     return FPSI_E_INVALID;
   }
@@ -328,6 +329,8 @@ void fpsi_default_params(fpsi_params* p) {
   p->lds_use_upwind = 0.0;
   p->lds_nonsym_coeff = 2.0;
   p->lds_nonsym_factor = 1.0;
+  p->lds_miles_filter = 0.1;
+  p->ssf_coeff = 1.0;
 }
 
 const char* fpsi_strerror(int code) {

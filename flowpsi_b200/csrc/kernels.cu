@@ -554,11 +554,17 @@ __device__ __forceinline__ void add_visc_jac(TB* M, const VFace& v, const double
 // ---------------------------------------------------------------------------
 // KIND: the Riemann solver (fpsi_flux_kind), a template parameter so that
 // each instantiation holds only its own solver's registers
+// the low-dissipation fluxes' switches (fluxLowDiss.loci:82-120, 434-437)
+struct Lds {
+  double comp, dlim, ducros, upwind, nscoeff, nsfactor, filter, ssf;
+};
+
 template <bool VIS, int KIND>
 __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
                             const double* __restrict__ qb, const double* __restrict__ grad,
                             const double* __restrict__ qf, Gas g, Visc V, double* __restrict__ F,
-                            const double* __restrict__ adiss, const float* __restrict__ ageom) {
+                            const double* __restrict__ adiss, const float* __restrict__ ageom,
+                            Lds P) {
   const int64_t f = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (f >= M.nf) return;
   FaceStates s;
@@ -577,13 +583,20 @@ __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
     // their boundary state (bcIsentropic.loci:162-167, bcFixedMass.loci:155-160,
     // bcFixedMassOutflow.loci:152-157)
     state_flux(s.R, nx, ny, nz, A, g, fl);
-  } else if (KIND == FPSI_FLUX_KEC) {
+  } else if (KIND == FPSI_FLUX_KEC || KIND == FPSI_FLUX_SSF) {
     if (f < M.nfi) {
       const int64_t a = M.cl[f], b = M.cr[f];
-      const double dvx = 0.5 * (M.rL[f] + M.rR[f]), dvy = 0.5 * (M.rL[M.nf + f] + M.rR[M.nf + f]),
-                   dvz = 0.5 * (M.rL[2 * M.nf + f] + M.rR[2 * M.nf + f]);
-      kec_face(s.L, s.R, load_q(q, a), load_q(q, b), grad + GPREC * a, grad + GPREC * b, dvx, dvy,
-               dvz, adiss[a], adiss[b], double(ageom[f]), nx, ny, nz, A, g, fl);
+      const double lx = M.rL[f], ly = M.rL[M.nf + f], lz = M.rL[2 * M.nf + f];
+      const double rx = M.rR[f], ry = M.rR[M.nf + f], rz = M.rR[2 * M.nf + f];
+      // dv = x_f - (x_l + x_r)/2, d2 = x_r - x_l
+      const double dvx = 0.5 * (lx + rx), dvy = 0.5 * (ly + ry), dvz = 0.5 * (lz + rz);
+      if (KIND == FPSI_FLUX_KEC)
+        kec_face(s.L, s.R, load_q(q, a), load_q(q, b), grad + GPREC * a, grad + GPREC * b, dvx, dvy,
+                 dvz, adiss[a], adiss[b], double(ageom[f]), nx, ny, nz, A, g, fl);
+      else
+        ssf_face(s.L, s.R, load_q(q, a), load_q(q, b), grad + GPREC * a, grad + GPREC * b, dvx, dvy,
+                 dvz, lx - rx, ly - ry, lz - rz, adiss[a], adiss[b], double(ageom[f]), P.ssf,
+                 P.filter, nx, ny, nz, A, g, fl);
     } else {
       riemann1(FPSI_FLUX_HLLC, s.L, s.R, nx, ny, nz, A, g, fl);  // inviscidRiemannFlux
     }
@@ -607,9 +620,6 @@ __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
 // ---------------------------------------------------------------------------
 // low-dissipation (KEC) switches
 // ---------------------------------------------------------------------------
-struct Lds {
-  double comp, dlim, ducros, upwind, nscoeff, nsfactor;
-};
 
 // alpha_geom_f (fluxLowDiss.loci:122-138) of each interior face, stored in
 // FP32 like the reference's store<realF>: with df = x_r - x_l and dv = x_f -
@@ -1725,6 +1735,8 @@ dev::Lds lds(const fpsi_ctx* x) {
   L.upwind = x->P.lds_use_upwind;
   L.nscoeff = x->P.lds_nonsym_coeff;
   L.nsfactor = x->P.lds_nonsym_factor;
+  L.filter = x->P.lds_miles_filter;
+  L.ssf = x->P.ssf_coeff;
   return L;
 }
 dev::Gas gas(const fpsi_ctx* x) {
@@ -1758,7 +1770,7 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
                                                          x->d_err + 1, x->d_qb);
     prof_end(x);
   }
-  const bool kec = x->P.flux == FPSI_FLUX_KEC;
+  const bool kec = x->P.flux == FPSI_FLUX_KEC || x->P.flux == FPSI_FLUX_SSF;
   if (kec) {
     if (!x->d_adiss) {
       FPSI_CUDA_TRY(cudaMalloc(&x->d_adiss, size_t(M.nc) * sizeof(double)));
@@ -1794,16 +1806,18 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
     double* F = x->d_F;
 #define FPSI_FLUX(VIS, K)                                                                     \
   dev::k_face_flux<VIS, K><<<nb, 128, 0, s>>>(M, x->d_q, x->d_qb, x->d_grad, x->d_qf, g, Vv, F, \
-                                              x->d_adiss, x->d_ageom)
+                                              x->d_adiss, x->d_ageom, lds(x))
     if (x->P.viscous) {
       if (x->P.flux == FPSI_FLUX_ROE) FPSI_FLUX(true, FPSI_FLUX_ROE);
       else if (x->P.flux == FPSI_FLUX_HLLE) FPSI_FLUX(true, FPSI_FLUX_HLLE);
-      else if (kec) FPSI_FLUX(true, FPSI_FLUX_KEC);
+      else if (x->P.flux == FPSI_FLUX_KEC) FPSI_FLUX(true, FPSI_FLUX_KEC);
+      else if (x->P.flux == FPSI_FLUX_SSF) FPSI_FLUX(true, FPSI_FLUX_SSF);
       else FPSI_FLUX(true, FPSI_FLUX_HLLC);
     } else {
       if (x->P.flux == FPSI_FLUX_ROE) FPSI_FLUX(false, FPSI_FLUX_ROE);
       else if (x->P.flux == FPSI_FLUX_HLLE) FPSI_FLUX(false, FPSI_FLUX_HLLE);
-      else if (kec) FPSI_FLUX(false, FPSI_FLUX_KEC);
+      else if (x->P.flux == FPSI_FLUX_KEC) FPSI_FLUX(false, FPSI_FLUX_KEC);
+      else if (x->P.flux == FPSI_FLUX_SSF) FPSI_FLUX(false, FPSI_FLUX_SSF);
       else FPSI_FLUX(false, FPSI_FLUX_HLLC);
     }
 #undef FPSI_FLUX

@@ -634,6 +634,143 @@ __device__ __forceinline__ void kec_face(const Q5& L, const Q5& R, const Q5& qa,
   kec_flux_add(l, r, nx, ny, nz, A * (1. - alpha), g, F);
 }
 
+// The Roe-type dissipation of two states (roedis, fluxLowDiss.loci:180-270)
+// on the area `area`, subtracted from F: eigenvalues of the Roe-averaged
+// state with the face sound speed a^2 = 2 a_l^2 a_r^2 / (a_l^2 + a_r^2),
+// applied to the jumps in p, u and T.
+__device__ __forceinline__ void roe_dissipation_sub(const Q5& l, const Q5& r, double nx, double ny,
+                                                    double nz, double area, const Gas& g,
+                                                    double F[5]) {
+  const double pl = l.p + g.pamb, pr = r.p + g.pamb;
+  const double rl = pl / (g.Rt * l.T), rr = pr / (g.Rt * r.T);
+  const double rgm1 = 1. / (g.gamma - 1);
+  const double el = g.Rt * rgm1 * l.T, er = g.Rt * rgm1 * r.T;
+  const double re0l = rl * el + 0.5 * rl * (l.u * l.u + l.v * l.v + l.w * l.w);
+  const double re0r = rr * er + 0.5 * rr * (r.u * r.u + r.v * r.v + r.w * r.w);
+  const double h0l = (re0l + pl) / rl, h0r = (re0r + pr) / rr;
+  const double rho = sqrt(rl * rr);
+  const double wl = sqrt(rl), wr = sqrt(rr), iw = 1. / (wl + wr);
+  const double U = (l.u * wl + r.u * wr) * iw, V = (l.v * wl + r.v * wr) * iw,
+               W = (l.w * wl + r.w * wr) * iw;
+  const double un = U * nx + V * ny + W * nz;  // fixed grid: the relative and absolute speeds agree
+  const double h0 = (h0l * wl + h0r * wr) * iw;
+  const double al2 = g.gamma * g.Rt * l.T, ar2 = g.gamma * g.Rt * r.T;
+  const double af2 = dmax(2. * al2 * ar2 / (al2 + ar2), 1e-30);
+  const double cp = g.Rt * g.gamma * rgm1;
+  const double Tm = (l.T * ar2 + r.T * al2) * af2 / (2. * ar2 * al2);
+  const double rT = -rho / Tm;
+  const double a = sqrt(af2);
+  const double ev1 = fabs(un), ev2 = fabs(un - a), ev3 = fabs(un + a);
+  const double ujx = r.u - l.u, ujy = r.v - l.v, ujz = r.w - l.w;
+  const double utj = ujx * nx + ujy * ny + ujz * nz;
+  const double pj = r.p - l.p, Tj = r.T - l.T;
+  const double t1 = ev2 - ev3, t2 = (ev2 + ev3 - 2 * ev1), t3 = -rho * a / 2.;
+  const double t4 = 2. * t2 * a, t5 = t2 / 2., t6 = (ev2 + ev3) / 2.;
+  const double c1 = (1 - g.gamma) / rT;
+  const double ra2 = 1. / (a * a);
+  const double gm1 = g.gamma - 1;
+  const double t7 = (1 + gm1 + c1 * rT) * t1 * t3 * ra2;
+  const double t8 = (g.gamma * t6 + c1 * rT * t5) * ra2;
+  const double t9 = cp * rho + h0 * rT;
+  const double x1 = g.gamma * h0 * t1 * t3 * ra2;
+  const double x2 = c1 * t1 * t3 * t9 * ra2;
+  const double x3 = rT * Tm * t1 * t3 * 1 / rho;
+  const double x4 = .25 * rho * t4 * un / a;
+  const double t10 = (x1 + x2 + x3 + x4);
+  const double t11 = (ra2 * h0 + (t9 - rho * cp) * ra2 * gm1 / rT + rT * Tm / rho) * t6 +
+                     ra2 * t9 * t5 * c1 - .5 * un * t1 / a;
+  const double coef = 0.5 * area;
+  const double md = coef * (pj * t8 + utj * t7 + ev1 * Tj * rT);
+  F[0] -= md;
+  const double fp = .5 * (.5 * rho * t4 * utj - pj * t1) / a;
+  F[1] -= md * U + coef * (ev1 * rho * ujx + fp * nx);
+  F[2] -= md * V + coef * (ev1 * rho * ujy + fp * ny);
+  F[3] -= md * W + coef * (ev1 * rho * ujz + fp * nz);
+  F[4] -= coef * (pj * t11 + t10 * utj + ev1 * (t9 * Tj + rho * (U * ujx + V * ujy + W * ujz)));
+}
+
+// SSF::iflux of an interior face (fluxLowDiss.loci:436-640): the 4th-order
+// skew-symmetric scheme.  Arguments as kec_face, plus d2 = x_r - x_l, the
+// SSF coefficient and the MILES filter level.  Upwind part as KEC's but
+// switched by alpha_c alone; central part: kec_flux of (l, r) on (1 + 2C)
+// A (1 - alpha) and of (l, rr) and (ll, r) on -C A (1 - alpha), C = coeff/6,
+// with ll, rr extrapolated along d2; then the Roe dissipation of the cubic
+// face values (1/3, 5/6, -1/6), Thornber-preconditioned, on the area
+// max(alpha_geom_f, filter) A (1 - alpha).
+__device__ __forceinline__ void ssf_face(const Q5& L, const Q5& R, const Q5& qa, const Q5& qb,
+                                         const double* ga, const double* gb, double dvx,
+                                         double dvy, double dvz, double d2x, double d2y, double d2z,
+                                         double aa, double ab, double ag, double coeff,
+                                         double filter, double nx, double ny, double nz, double A,
+                                         const Gas& g, double F[5]) {
+  const double pglim = 0.1 * dmin(qa.p, qb.p) + -0.9 * g.pamb;
+  const double tlim = 0.1 * dmin(qa.T, qb.T);
+  const double rl = (L.p + g.pamb) / (g.Rt * L.T), rr = (R.p + g.pamb) / (g.Rt * R.T);
+  const double al2 = g.gamma * g.Rt * L.T, ar2 = g.gamma * g.Rt * R.T;
+  const double dp = 2. * fabs(L.p - R.p) / dmax(rl * al2, rr * ar2);
+  const double alpha_c = dmax(dmax(aa, ab), dmin(1.0, dp * 1.0 - 0.5));
+  const double alpha = alpha_c;
+  const double amin = sqrt(dmin(al2, ar2));
+#pragma unroll
+  for (int i = 0; i < 5; ++i) F[i] = 0.0;
+  if (alpha > 1e-10) {
+    const double utmax = dmax(fabs(L.u * nx + L.v * ny + L.w * nz), fabs(R.u * nx + R.v * ny + R.w * nz));
+    const double Ma = dmax(alpha_c, dmin(1.0, utmax / amin + 1e-4));
+    const double h = 0.5 * (1. - Ma);
+    Q5 Lp = L, Rp = R;
+    Lp.u = L.u + h * (R.u - L.u), Lp.v = L.v + h * (R.v - L.v), Lp.w = L.w + h * (R.w - L.w);
+    Rp.u = R.u + h * (L.u - R.u), Rp.v = R.v + h * (L.v - R.v), Rp.w = R.w + h * (L.w - R.w);
+    flux_hllc(Lp, Rp, nx, ny, nz, A * alpha, g, 0.0, 1.0, F);
+  }
+  auto dot3 = [](const double* gr, double x, double y, double z) { return gr[0] * x + gr[1] * y + gr[2] * z; };
+  auto at = [&](const Q5& c, const double* gr, Q5& o) {
+    const double* ph = gr + 15;
+    o.p = dmax(c.p + ph[4] * dot3(gr + 12, dvx, dvy, dvz), pglim);
+    o.T = dmax(c.T + ph[0] * dot3(gr, dvx, dvy, dvz), tlim);
+    o.u = c.u + ph[1] * dot3(gr + 3, dvx, dvy, dvz);
+    o.v = c.v + ph[2] * dot3(gr + 6, dvx, dvy, dvz);
+    o.w = c.w + ph[3] * dot3(gr + 9, dvx, dvy, dvz);
+  };
+  Q5 l, r, ll, rx;
+  at(qa, ga, l);
+  at(qb, gb, r);
+  // ll from r with the left cell's gradient, rr from l with the right one's
+  ll.p = dmax(r.p - 2. * dot3(ga + 12, d2x, d2y, d2z), pglim);
+  rx.p = dmax(l.p + 2. * dot3(gb + 12, d2x, d2y, d2z), pglim);
+  ll.T = dmax(r.T - 2. * dot3(ga, d2x, d2y, d2z), tlim);
+  rx.T = dmax(l.T + 2. * dot3(gb, d2x, d2y, d2z), tlim);
+  ll.u = r.u - 2. * dot3(ga + 3, d2x, d2y, d2z);
+  ll.v = r.v - 2. * dot3(ga + 6, d2x, d2y, d2z);
+  ll.w = r.w - 2. * dot3(ga + 9, d2x, d2y, d2z);
+  rx.u = l.u + 2. * dot3(gb + 3, d2x, d2y, d2z);
+  rx.v = l.v + 2. * dot3(gb + 6, d2x, d2y, d2z);
+  rx.w = l.w + 2. * dot3(gb + 9, d2x, d2y, d2z);
+  const double CC = coeff / 6.0;
+  const double sada = A * (1. - alpha);
+  kec_flux_add(l, r, nx, ny, nz, (1. + 2. * CC) * sada, g, F);
+  kec_flux_add(l, rx, nx, ny, nz, -CC * sada, g, F);
+  kec_flux_add(ll, r, nx, ny, nz, -CC * sada, g, F);
+  // cubic extrapolation to the face
+  const double a0 = 1. / 3., a1 = 5. / 6., a2 = -1. / 6.;
+  Q5 lq, rq;
+  lq.p = dmax(pglim, a0 * r.p + a1 * l.p + a2 * ll.p);
+  rq.p = dmax(pglim, a0 * l.p + a1 * r.p + a2 * rx.p);
+  lq.T = dmax(tlim, a0 * r.T + a1 * l.T + a2 * ll.T);
+  rq.T = dmax(tlim, a0 * l.T + a1 * r.T + a2 * rx.T);
+  lq.u = a0 * r.u + a1 * l.u + a2 * ll.u, lq.v = a0 * r.v + a1 * l.v + a2 * ll.v,
+  lq.w = a0 * r.w + a1 * l.w + a2 * ll.w;
+  rq.u = a0 * l.u + a1 * r.u + a2 * rx.u, rq.v = a0 * l.v + a1 * r.v + a2 * rx.v,
+  rq.w = a0 * l.w + a1 * r.w + a2 * rx.w;
+  const double cf = dmax(ag, filter) * sada;
+  const double utmax = dmax(fabs(lq.u * nx + lq.v * ny + lq.w * nz), fabs(rq.u * nx + rq.v * ny + rq.w * nz));
+  const double Ma = dmin(1.0, utmax / amin + 1e-4);
+  const double h = 0.5 * (1. - Ma);
+  Q5 lp = lq, rp = rq;
+  lp.u = lq.u + h * (rq.u - lq.u), lp.v = lq.v + h * (rq.v - lq.v), lp.w = lq.w + h * (rq.w - lq.w);
+  rp.u = rq.u + h * (lq.u - rq.u), rp.v = rq.v + h * (lq.v - rq.v), rp.w = rq.w + h * (lq.w - rq.w);
+  roe_dissipation_sub(lp, rp, nx, ny, nz, cf, g, F);
+}
+
 // ---- boundary states from total conditions or a mass flux ---------------
 // Each returns the face state (T, u, v, w, pg) from the cell-centre state qi
 // of the face's cell; n is the outward unit normal, the flow direction of

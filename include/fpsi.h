@@ -53,9 +53,12 @@ enum fpsi_flux_kind {          /* inviscidRiemannFlux, inviscidFlux.h:82-90 */
   FPSI_FLUX_HLLC = 0,          /* hllc_flux, fluxInviscid.loci:157-256 (reference default) */
   FPSI_FLUX_ROE  = 1,          /* roeCT_flux, fluxInviscid.loci:869-1014 */
   FPSI_FLUX_HLLE = 2,          /* two-wave HLL with hllc_flux's SL/SR (no reference counterpart) */
-  FPSI_FLUX_KEC  = 3           /* inviscidFlux "KEC": kinetic-energy-consistent low-dissipation
+  FPSI_FLUX_KEC  = 3,          /* inviscidFlux "KEC": kinetic-energy-consistent low-dissipation
                                   flux on interior faces (KEC::iflux, fluxLowDiss.loci:320-431),
                                   hllc_flux on boundary faces */
+  FPSI_FLUX_SSF  = 4           /* inviscidFlux "SSF": 4th-order skew-symmetric low-dissipation
+                                  flux with a Roe-type MILES filter on interior faces
+                                  (SSF::iflux, fluxLowDiss.loci:436-640), hllc_flux on boundary faces */
 };
 enum fpsi_limiter_kind {       /* vars 'limiter' (guide.tex:495-518) */
   FPSI_LIMITER_VENKATAKRISHNAN = 0,
@@ -139,6 +142,8 @@ typedef struct fpsi_params {
   double lds_use_upwind;        /* LDS_useUpwind 0 */
   double lds_nonsym_coeff;      /* LDS_nonSymmetricCoeff 2 */
   double lds_nonsym_factor;     /* LDS_nonSymmetricFactor 1 */
+  double lds_miles_filter;      /* LDS_MILES_filter 0.1 (SSF) */
+  double ssf_coeff;             /* SSF_Coeff 1 (SSF) */
 } fpsi_params;
 
 typedef struct fpsi_bc {

@@ -1336,6 +1336,121 @@ static void kec_iflux(const orc_ctx* o, int64_t f, const double qL[5], const dou
   kec_flux(F, pg_l, t_l, u_l, pg_r, t_r, u_r, an, A * (1. - alpha), P.Pambient, P.Rtilde, P.gamma);
 }
 
+// roedis (fluxLowDiss.loci:180-270): Roe-type dissipation of two states on
+// the area `sada`, subtracted from F
+static void roe_dissipation(double F[5], double pg_l, V3 Ul, double Tl, double pg_r, V3 Ur,
+                            double Tr, double Rt, double gamma, double pamb, V3 an, double sada) {
+  const double pl = pg_l + pamb, pr = pg_r + pamb;
+  const double rl = pl / (Rt * Tl), rr = pr / (Rt * Tr);
+  const double rgm1 = 1. / (gamma - 1);
+  const double el = Rt * rgm1 * Tl, er = Rt * rgm1 * Tr;
+  const double re0l = rl * el + 0.5 * rl * dot(Ul, Ul);
+  const double re0r = rr * er + 0.5 * rr * dot(Ur, Ur);
+  const double h0l = (re0l + pl) / rl, h0r = (re0r + pr) / rr;
+  const double rho = std::sqrt(rl * rr);
+  const double srl = std::sqrt(rl), srr = std::sqrt(rr), f = 1. / (srl + srr);
+  const V3 U = (Ul * srl + Ur * srr) * f;
+  const double un = dot(U, an);
+  const double h0 = (h0l * srl + h0r * srr) * f;
+  const double al2 = gamma * Rt * Tl, ar2 = gamma * Rt * Tr;
+  const double af2 = std::max(2. * al2 * ar2 / (al2 + ar2), 1e-30);
+  const double cp = Rt * gamma * rgm1;
+  const double Tm = (Tl * ar2 + Tr * al2) * af2 / (2. * ar2 * al2);
+  const double rT = -rho / Tm;
+  const double a = std::sqrt(af2);
+  const double ev1 = std::fabs(un), ev2 = std::fabs(un - a), ev3 = std::fabs(un + a);
+  const V3 Uj = Ur - Ul;
+  const double utj = dot(Uj, an), pj = pg_r - pg_l, Tj = Tr - Tl;
+  const double t1 = ev2 - ev3, t2 = (ev2 + ev3 - 2 * ev1), t3 = -rho * a / 2.;
+  const double t4 = 2. * t2 * a, t5 = t2 / 2., t6 = (ev2 + ev3) / 2.;
+  const double c1 = (1 - gamma) / rT, ra2 = 1. / (a * a), gm1 = gamma - 1;
+  const double t7 = (1 + gm1 + c1 * rT) * t1 * t3 * ra2;
+  const double t8 = (gamma * t6 + c1 * rT * t5) * ra2;
+  const double t9 = cp * rho + h0 * rT;
+  const double x1 = gamma * h0 * t1 * t3 * ra2, x2 = c1 * t1 * t3 * t9 * ra2;
+  const double x3 = rT * Tm * t1 * t3 * 1 / rho, x4 = .25 * rho * t4 * un / a;
+  const double t10 = (x1 + x2 + x3 + x4);
+  const double t11 = (ra2 * h0 + (t9 - rho * cp) * ra2 * gm1 / rT + rT * Tm / rho) * t6 +
+                     ra2 * t9 * t5 * c1 - .5 * un * t1 / a;
+  const double coef = 0.5 * sada;
+  const double md = coef * (pj * t8 + utj * t7 + ev1 * Tj * rT);
+  F[0] -= md;
+  const double fp = .5 * (.5 * rho * t4 * utj - pj * t1) / a;
+  F[1] -= md * U.x + coef * (ev1 * rho * Uj.x + fp * an.x);
+  F[2] -= md * U.y + coef * (ev1 * rho * Uj.y + fp * an.y);
+  F[3] -= md * U.z + coef * (ev1 * rho * Uj.z + fp * an.z);
+  F[4] -= coef * (pj * t11 + t10 * utj + ev1 * (t9 * Tj + rho * dot(U, Uj)));
+}
+
+// SSF::iflux of interior face f (fluxLowDiss.loci:436-640, the cubic
+// extrapolation variant that the file compiles)
+static void ssf_iflux(const orc_ctx* o, int64_t f, const double qL[5], const double qR[5],
+                      const std::vector<double>& ad, double F[5]) {
+  const fpsi_params& P = o->P;
+  const int64_t a = o->cl[f], b = o->cr[f];
+  const V3 an = v3(&o->an[3 * f]);
+  const double A = o->area[f];
+  const double pglim = 0.1 * std::min(o->pg[a], o->pg[b]) + -0.9 * P.Pambient;
+  const double tlim = 0.1 * std::min(o->T[a], o->T[b]);
+  const double pgL = qL[4], pgR = qR[4], tL = qL[0], tR = qR[0];
+  const double rL = (pgL + P.Pambient) / (P.Rtilde * tL);
+  const double rR = (pgR + P.Pambient) / (P.Rtilde * tR);
+  const double al2 = P.gamma * P.Rtilde * tL, ar2 = P.gamma * P.Rtilde * tR;
+  const double dp = 2. * std::fabs(pgL - pgR) / std::max(rL * al2, rR * ar2);
+  const double alpha_c = std::max(std::max(ad[a], ad[b]), std::min(1.0, dp * 1.0 - 0.5));
+  const double alpha = alpha_c;
+  const double amin = std::sqrt(std::min(al2, ar2));
+  for (int i = 0; i < 5; ++i) F[i] = 0;
+  if (alpha > 1e-10) {
+    const V3 uL = mk(qL[1], qL[2], qL[3]), uR = mk(qR[1], qR[2], qR[3]);
+    const double utmax = std::max(std::fabs(dot(uL, an)), std::fabs(dot(uR, an)));
+    const double Ma = std::max(alpha_c, std::min(1.0, utmax / amin + 1e-4));
+    const V3 uLp = uL + 0.5 * (1. - Ma) * (uR - uL);
+    const V3 uRp = uR + 0.5 * (1. - Ma) * (uL - uR);
+    hllc_flux(F, pgL, tL, uLp, pgR, tR, uRp, an, A * alpha, P.Pambient, P.Rtilde, P.gamma, 0.0, 1.0);
+  }
+  const V3 rl = v3(&o->rL[3 * f]), rr = v3(&o->rR[3 * f]);
+  const V3 dv = 0.5 * (rl + rr), dv2 = rl - rr;
+  const double* ga = &o->grad[15 * a];
+  const double* gb = &o->grad[15 * b];
+  auto at = [&](int64_t c, double& pg, double& t, V3& u) {
+    const double* g = &o->grad[15 * c];
+    const double* ph = &o->phi[5 * c];
+    pg = std::max(o->pg[c] + ph[4] * dot(v3(g + 12), dv), pglim);
+    t = std::max(o->T[c] + ph[0] * dot(v3(g), dv), tlim);
+    u = mk(o->u[3 * c] + ph[1] * dot(v3(g + 3), dv), o->u[3 * c + 1] + ph[2] * dot(v3(g + 6), dv),
+           o->u[3 * c + 2] + ph[3] * dot(v3(g + 9), dv));
+  };
+  double pg_l, t_l, pg_r, t_r;
+  V3 u_l, u_r;
+  at(a, pg_l, t_l, u_l);
+  at(b, pg_r, t_r, u_r);
+  const double pg_ll = std::max(pg_r - 2. * dot(v3(ga + 12), dv2), pglim);
+  const double pg_rr = std::max(pg_l + 2. * dot(v3(gb + 12), dv2), pglim);
+  const double t_ll = std::max(t_r - 2. * dot(v3(ga), dv2), tlim);
+  const double t_rr = std::max(t_l + 2. * dot(v3(gb), dv2), tlim);
+  const V3 u_ll = u_r - mk(2. * dot(v3(ga + 3), dv2), 2. * dot(v3(ga + 6), dv2), 2. * dot(v3(ga + 9), dv2));
+  const V3 u_rr = u_l + mk(2. * dot(v3(gb + 3), dv2), 2. * dot(v3(gb + 6), dv2), 2. * dot(v3(gb + 9), dv2));
+  const double CC = P.ssf_coeff / 6.0;
+  const double sada = A * (1. - alpha);
+  kec_flux(F, pg_l, t_l, u_l, pg_r, t_r, u_r, an, (1. + 2. * CC) * sada, P.Pambient, P.Rtilde, P.gamma);
+  kec_flux(F, pg_l, t_l, u_l, pg_rr, t_rr, u_rr, an, -CC * sada, P.Pambient, P.Rtilde, P.gamma);
+  kec_flux(F, pg_ll, t_ll, u_ll, pg_r, t_r, u_r, an, -CC * sada, P.Pambient, P.Rtilde, P.gamma);
+  const double a0 = 1. / 3., a1 = 5. / 6., a2 = -1. / 6.;
+  const double pg_lq = std::max(pglim, a0 * pg_r + a1 * pg_l + a2 * pg_ll);
+  const double pg_rq = std::max(pglim, a0 * pg_l + a1 * pg_r + a2 * pg_rr);
+  const double t_lq = std::max(tlim, a0 * t_r + a1 * t_l + a2 * t_ll);
+  const double t_rq = std::max(tlim, a0 * t_l + a1 * t_r + a2 * t_rr);
+  const V3 u_lq = a0 * u_r + a1 * u_l + a2 * u_ll;
+  const V3 u_rq = a0 * u_l + a1 * u_r + a2 * u_rr;
+  const double coef = std::max(double(alpha_geom(o, f)), P.lds_miles_filter) * sada;
+  const double utmax = std::max(std::fabs(dot(u_lq, an)), std::fabs(dot(u_rq, an)));
+  const double Ma = std::min(1.0, utmax / amin + 1e-4);
+  const V3 u_lqp = u_lq + 0.5 * (1. - Ma) * (u_rq - u_lq);
+  const V3 u_rqp = u_rq + 0.5 * (1. - Ma) * (u_lq - u_rq);
+  roe_dissipation(F, pg_lq, u_lqp, t_lq, pg_rq, u_rqp, t_rq, P.Rtilde, P.gamma, P.Pambient, an, coef);
+}
+
 extern "C" int orc_residual(orc_ctx* o, double* src_out, fpsi_resid* norms) {
   const int64_t nc = o->nc, nf = o->nf;
   const fpsi_params& P = o->P;
@@ -1377,7 +1492,7 @@ extern "C" int orc_residual(orc_ctx* o, double* src_out, fpsi_resid* norms) {
   for (int64_t f = 0; f < nf; ++f)
     if (o->cr[f] < 0) o->bc_err |= bc_face_state(o, f, &o->qb[5 * f]);
   gradients_and_limiters(o);
-  const bool kec = P.flux == FPSI_FLUX_KEC;
+  const bool kec = P.flux == FPSI_FLUX_KEC || P.flux == FPSI_FLUX_SSF;
   std::vector<double> adiss;
   if (kec) alpha_diss(o, adiss);
   o->F.assign(nf * 5, 0);
@@ -1400,7 +1515,10 @@ extern "C" int orc_residual(orc_ctx* o, double* src_out, fpsi_resid* norms) {
       state_flux(&o->F[5 * f], b[4], b[0], mk(b[1], b[2], b[3]), n, o->area[f], P.Pambient,
                  P.Rtilde, P.gamma);
     } else if (kec && o->cr[f] >= 0) {
-      kec_iflux(o, f, qL, qR, adiss, &o->F[5 * f]);
+      if (P.flux == FPSI_FLUX_KEC)
+        kec_iflux(o, f, qL, qR, adiss, &o->F[5 * f]);
+      else
+        ssf_iflux(o, f, qL, qR, adiss, &o->F[5 * f]);
     } else {
       // boundary faces of the KEC scheme: inviscidRiemannFlux (inviscidFlux.h:82-90)
       riemann_flux(kec ? FPSI_FLUX_HLLC : P.flux, &o->F[5 * f], qL[4], qL[0],

@@ -101,7 +101,7 @@ def test_malformed_meshes_are_refused(need_gpu):
     assert _code(lambda: FlowPsi(empty.m, p)) == -1
 
 
-@pytest.mark.parametrize("field,value", [("flux", 3), ("limiter", -1), ("precision", 5),
+@pytest.mark.parametrize("field,value", [("flux", 5), ("limiter", -1), ("precision", 5),
                                          ("gauss_seidel_iter", -1), ("solver", 3),
                                          ("viscous", 3), ("turbulence", 2)])
 def test_bad_parameters_are_refused(need_gpu, field, value):

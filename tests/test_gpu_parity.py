@@ -62,9 +62,10 @@ def test_face_functions_vs_oracle(need_gpu):
 # --------------------------------------------------------------------------
 # mesh level
 # --------------------------------------------------------------------------
-def _kec(case):
-    """the same case with the low-dissipation KEC flux (fluxLowDiss.loci:320-431)"""
-    case.params.flux = 3
+def _kec(case, flux=3):
+    """the same case with a low-dissipation flux: 3 KEC (fluxLowDiss.loci:320-431),
+    4 SSF (fluxLowDiss.loci:436-640)"""
+    case.params.flux = flux
     return case
 
 
@@ -82,6 +83,8 @@ CASES = {
     "kec_tgv_tets": lambda prec: _kec(cases.taylor_green_tets(5, precision=prec)),
     "kec_farfield_hex": lambda prec: _kec(cases.farfield_cube(6, precision=prec)),
     "kec_shock_hex": lambda prec: _kec(cases.oblique_shock_cube(8, precision=prec)),
+    "ssf_tgv_tets": lambda prec: _kec(cases.taylor_green_tets(5, precision=prec), 4),
+    "ssf_shock_hex": lambda prec: _kec(cases.oblique_shock_cube(8, precision=prec), 4),
 }
 
 

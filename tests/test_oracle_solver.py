@@ -235,20 +235,21 @@ def test_fsgs_reaches_the_sgs_steady_state():
         assert np.abs(a - b).max() <= 1e-9 * np.abs(b).max()
 
 
-def _kec_case(**lds):
+def _kec_case(flux=3, **lds):
     case = cases.taylor_green_tets(5, precision="fp64")
-    case.params.flux = 3  # KEC
+    case.params.flux = flux  # 3 KEC, 4 SSF
     for k, v in lds.items():
         setattr(case.params, k, v)
     return case
 
 
-def test_kec_preserves_uniform_flow():
+@pytest.mark.parametrize("flux", [3, 4])
+def test_kec_preserves_uniform_flow(flux):
     """uniform flow on the jittered periodic tet grid: alpha_diss is 0 (no
     divergence), the upwind part sees equal states and the central kinetic-
     energy-consistent flux (fluxLowDiss.loci:258-298) of equal states is the
     analytic flux, so the residual is round-off"""
-    case = _kec_case()
+    case = _kec_case(flux)
     o = Oracle(case.mesh, case.params)
     nc = o.ncells
     o.set_state(np.full(nc, 300.0), np.full(nc, 1e5), np.tile([30.0, -20.0, 10.0], (nc, 1)))
@@ -258,11 +259,13 @@ def test_kec_preserves_uniform_flow():
     assert np.abs(src).max() < 1e-14 * scale
 
 
-def test_kec_with_full_upwinding_is_hllc():
+@pytest.mark.parametrize("flux", [3, 4])
+def test_kec_with_full_upwinding_is_hllc(flux):
     """LDS_useUpwind = 1 makes alpha_diss = 1 on every cell, so alpha = 1,
-    the Thornber factor Ma = 1 and the central part has zero area: the KEC
-    flux is hllc_flux of the face states (fluxLowDiss.loci:371-399)"""
-    c_kec = _kec_case(lds_use_upwind=1.0)
+    the Thornber factor Ma = 1 and the central parts (and SSF's filter) have
+    zero area: both low-dissipation fluxes are hllc_flux of the face states
+    (fluxLowDiss.loci:371-399, 492-512)"""
+    c_kec = _kec_case(flux, lds_use_upwind=1.0)
     c_hllc = cases.taylor_green_tets(5, precision="fp64")
     c_hllc.params.flux = 0
     a, b = Oracle(c_kec.mesh, c_kec.params), Oracle(c_hllc.mesh, c_hllc.params)
@@ -292,4 +295,20 @@ def test_kec_differs_from_hllc_and_steps():
     assert np.abs(sk - sh).max() > 1e-6 * np.abs(sh).max()
     r0 = o.newton_step()
     r1 = o.newton_step()
+    assert np.isfinite(r1["rtrms"]) and r1["rtrms"] < r0["rtrms"]
+
+
+def test_ssf_differs_from_kec():
+    """the skew-symmetric scheme's extrapolated states and MILES filter
+    (fluxLowDiss.loci:556-640) change the residual of the Taylor-Green state"""
+    a, b = _kec_case(3), _kec_case(4)
+    oa, ob = Oracle(a.mesh, a.params), Oracle(b.mesh, b.params)
+    st = a.initial_state(oa.geometry()["cellcenter"])
+    oa.set_state(*st)
+    ob.set_state(*st)
+    sa, _ = oa.residual()
+    sb, _ = ob.residual()
+    assert np.abs(sa - sb).max() > 1e-8 * np.abs(sa).max()
+    r0 = ob.newton_step()
+    r1 = ob.newton_step()
     assert np.isfinite(r1["rtrms"]) and r1["rtrms"] < r0["rtrms"]
