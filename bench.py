@@ -399,7 +399,7 @@ def _drop_arm(solver, case, drop, max_steps, chunk, model=None):
                 reached = k + 1
                 break
         ms_tot = 1e3 * (time.perf_counter() - t0)
-    return {"steps": reached, "ms": ms_tot if reached is not None else None,
+    return {"steps": reached, "ms": ms_tot if reached is not None else None, "r0": r0,
             "rejected": rejected if model is not None else None,
             "timer": "host clock, per-step decisions" if model is not None else
             "CUDA events on the library stream"}, solver.get_state()
@@ -414,7 +414,8 @@ def time_to_drop(n: int, drop: float = 1e-8, max_steps: int = 400, chunk: int = 
     MIXED from the reference's Jacobi start, and MIXED from the learned start
     (a model trained first on 16^3 x 6 grids of the same case, seeds 1-4).
     Each arm reports steps, ms and the largest density and energy difference
-    of its final state from the FP64 arm's."""
+    of its final state from the FP64 arm's and from the converged state (the
+    FP64 run continued, untimed, to a 1e-12 drop)."""
     from flowpsi_b200 import FlowPsi, cases
 
     out = {"case": f"farfield_tets_{n}", "cells": 6 * n ** 3, "drop": drop}
@@ -422,9 +423,23 @@ def time_to_drop(n: int, drop: float = 1e-8, max_steps: int = 400, chunk: int = 
     s = FlowPsi(c64.mesh, c64.params)
     s.keep_blocks(False)
     out["fp64"], st64 = _drop_arm(s, c64, drop, max_steps, chunk)
+    r0, extra = out["fp64"]["r0"], 0
+    while extra < 400:
+        hist = s.run(chunk)
+        extra += chunk
+        if hist[-1]["rtrms"] < 1e-12 * r0:
+            break
+    out["converged"] = {"extra_fp64_steps": extra, "drop": hist[-1]["rtrms"] / r0}
+    rho_c, e_c = _rho_energy(*s.get_state())
     s.close()
     del s
     rho64, e64 = _rho_energy(*st64)
+
+    def vs_converged(rho, e):
+        return {"rho": float(np.abs(rho - rho_c).max() / np.abs(rho_c).max()),
+                "rho_e0": float(np.abs(e - e_c).max() / np.abs(e_c).max())}
+
+    out["fp64"]["max_rel_diff_vs_converged"] = vs_converged(rho64, e64)
     c32 = cases.farfield_tets(n, seed=seed, precision="mixed")
     s = FlowPsi(c32.mesh, c32.params)
     s.keep_blocks(learned)
@@ -443,6 +458,7 @@ def time_to_drop(n: int, drop: float = 1e-8, max_steps: int = 400, chunk: int = 
         out[name]["max_rel_diff_vs_fp64"] = {
             "rho": float(np.abs(rho - rho64).max() / np.abs(rho64).max()),
             "rho_e0": float(np.abs(e - e64).max() / np.abs(e64).max())}
+        out[name]["max_rel_diff_vs_converged"] = vs_converged(rho, e)
     if learned:
         model.close()
     s.close()
