@@ -614,40 +614,46 @@ k_layer_ws(int64_t nc, int fin, const __nv_bfloat16* __restrict__ h, const int32
   };
 
   if (warp < WS_PROD) {
-    // ---- gather: warp w fills rows 16 w .. 16 w + 15; lane = (row 0..15,
-    // chunk parity 0..1), two chunks of the row and of its first WS_NB
-    // neighbour rows in flight together; the next tile's neighbour ids are
-    // requested before this tile's rows.  The neighbours come from the
-    // entry-major lists in the cell's face order (boundary entries are -1
-    // and skipped), so the mean sums them in the order of the face graph.
-    const int r = 16 * warp + (lane & 15), cp = lane >> 4;
-    auto ids = [&](int64_t t, int32_t* o) {
-      const int64_t cell = t * TC_ROWS + r;
-#pragma unroll
-      for (int j = 0; j < WS_NB; ++j) o[j] = cell < nc && j < K ? __ldg(ell + j * nc + cell) : -1;
-    };
-    int32_t nbi[WS_NB], nbn[WS_NB];
-    ids(blockIdx.x, nbi);
+    // ---- gather: warp w fills rows 16 w .. 16 w + 15, eight rows at a
+    // time; lane = 8 quarter + row slot (0..7) holds chunks quarter and
+    // quarter + 4 of its row and of the row's first WS_NB neighbours, all
+    // loading at once.  A load instruction reads half of eight 128 B rows;
+    // the eight lanes of a quarter warp store one chunk of eight
+    // consecutive rows, 128 contiguous bytes of the K-major tile, so each
+    // 16 B store phase hits every bank once.  The
+    // neighbours come from the entry-major lists in the cell's face order
+    // (boundary entries are -1 and skipped), so the mean sums them in the
+    // order of the face graph.
+    const int sl = lane & 7, qc = lane >> 3;
     int k = 0;
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
       const int b = k & 1;
-      ids(t + gridDim.x, nbn);
       if (k >= 2 && !mbar_wait_bounded(done + b, uint32_t(((k >> 1) - 1) & 1))) give_up();
       if (*abort_flag) break;
       unsigned char* A = sA[b];
-      const int64_t cell = t * TC_ROWS + r;
-      if (cell < nc) {
+#pragma unroll 1
+      for (int g = 0; g < 2; ++g) {
+        const int r = 16 * warp + 8 * g + sl;
+        const int64_t cell = t * TC_ROWS + r;
+        int32_t nbi[WS_NB];
+#pragma unroll
+        for (int j = 0; j < WS_NB; ++j) nbi[j] = cell < nc && j < K ? __ldg(ell + j * nc + cell) : -1;
+        if (cell >= nc) {
+          for (int c = qc; c < nch; c += 4)
+            *reinterpret_cast<uint4*>(A + (size_t(c) * TC_ROWS + r) * 16) = make_uint4(0, 0, 0, 0);
+          continue;
+        }
         int deg = 0;
 #pragma unroll
         for (int j = 0; j < WS_NB; ++j) deg += nbi[j] >= 0;
         for (int j = WS_NB; j < K; ++j) deg += __ldg(ell + j * nc + cell) >= 0;
         const float inv = deg > 0 ? 1.0f / float(deg) : 0.f;
-        for (int c0 = cp; c0 < hch; c0 += 4) {
-          // chunks c0 and c0 + 2 of the row and of its neighbours
+        for (int c0 = qc; c0 < hch; c0 += 8) {
+          // chunks c0 and c0 + 4 of the row and of its neighbours
           Chunk8<__nv_bfloat16> own[2], u[2][WS_NB];
 #pragma unroll
           for (int i = 0; i < 2; ++i) {
-            const int c = c0 + 2 * i;
+            const int c = c0 + 4 * i;
             if (c < hch) {
               own[i].load(h + cell * fin + 8 * c);
 #pragma unroll
@@ -657,7 +663,7 @@ k_layer_ws(int64_t nc, int fin, const __nv_bfloat16* __restrict__ h, const int32
           }
 #pragma unroll
           for (int i = 0; i < 2; ++i) {
-            const int c = c0 + 2 * i;
+            const int c = c0 + 4 * i;
             if (c >= hch) break;
             float v[8], sum[8];
             own[i].get(v);
@@ -685,14 +691,9 @@ k_layer_ws(int64_t nc, int fin, const __nv_bfloat16* __restrict__ h, const int32
             *reinterpret_cast<uint4*>(A + (size_t(hch + c) * TC_ROWS + r) * 16) = pack8(sum);
           }
         }
-      } else {
-        for (int c = cp; c < nch; c += 2)
-          *reinterpret_cast<uint4*>(A + (size_t(c) * TC_ROWS + r) * 16) = make_uint4(0, 0, 0, 0);
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(full + b);
-#pragma unroll
-      for (int j = 0; j < WS_NB; ++j) nbi[j] = nbn[j];
     }
   } else if (warp == WS_PROD) {
     // ---- MMA issue (one thread)
@@ -743,15 +744,30 @@ k_layer_ws(int64_t nc, int fin, const __nv_bfloat16* __restrict__ h, const int32
           tc_fence_before();
           mbar_arrive(tfree + b);
         }
+        // bias and head weights are read as 16 B vectors (one shared load
+        // per four values, the same address in every lane)
+        const float4* b4 = reinterpret_cast<const float4*>(sbias + 32 * hf);
 #pragma unroll
-        for (int j = 0; j < 32; ++j)
-          v[j] = __bfloat162float(__float2bfloat16_rn(gelu(v[j] + sbias[32 * hf + j])));
+        for (int j4 = 0; j4 < 8; ++j4) {
+          const float4 bb = b4[j4];
+          v[4 * j4] = __bfloat162float(__float2bfloat16_rn(gelu(v[4 * j4] + bb.x)));
+          v[4 * j4 + 1] = __bfloat162float(__float2bfloat16_rn(gelu(v[4 * j4 + 1] + bb.y)));
+          v[4 * j4 + 2] = __bfloat162float(__float2bfloat16_rn(gelu(v[4 * j4 + 2] + bb.z)));
+          v[4 * j4 + 3] = __bfloat162float(__float2bfloat16_rn(gelu(v[4 * j4 + 3] + bb.w)));
+        }
         if (HEAD) {
 #pragma unroll
           for (int o = 0; o < NOUT; ++o) {
+            const float4* w4 = reinterpret_cast<const float4*>(sWo + o * W + 32 * hf);
             float sacc = 0.f;
 #pragma unroll
-            for (int j = 0; j < 32; ++j) sacc += sWo[o * W + 32 * hf + j] * v[j];
+            for (int j4 = 0; j4 < 8; ++j4) {
+              const float4 ww = w4[j4];
+              sacc += ww.x * v[4 * j4];
+              sacc += ww.y * v[4 * j4 + 1];
+              sacc += ww.z * v[4 * j4 + 2];
+              sacc += ww.w * v[4 * j4 + 3];
+            }
             ys[hf][o] = sacc;
           }
         } else {
