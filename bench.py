@@ -469,6 +469,43 @@ def time_to_drop(n: int, drop: float = 1e-8, max_steps: int = 400, chunk: int = 
     return out
 
 
+def bl_time_to_drop(drop: float = 1e-8, max_steps: int = 16000, chunk: int = 100) -> dict:
+    """Config 3 to a 1e-8 drop: the 256x128x64 flat-plate boundary layer
+    (first spacing 1e-6, growth 1.15, M 0.3, Re 1e6), Spalart-Allmaras,
+    line SGS over the wall-normal lines, CFL 50; plain FP64 and MIXED, each
+    timed with CUDA events in chunks of `chunk` steps"""
+    from flowpsi_b200 import FlowPsi, cases
+
+    out = {"case": "boundary_layer_256x128x64_sa", "cells": 256 * 128 * 64, "drop": drop}
+    for prec in ("fp64", "mixed"):
+        case = cases.boundary_layer_block(256, 128, 64, precision=prec, viscous=2, solver="lsgs",
+                                          sa=True)
+        s = FlowPsi(case.mesh, case.params)
+        s.set_lines(case.lines)
+        s.set_state(*case.initial_state(s.geometry()["cellcenter"]))
+        s.set_nutilde(case.nut0)
+        r0, done, ms, reached, hist_out = None, 0, 0.0, None, []
+        while done < max_steps and reached is None:
+            hist, dt = s.run_timed(chunk)
+            r0 = r0 or hist[0]["rtrms"]
+            for k, h in enumerate(hist):
+                if h["rtrms"] < drop * r0:
+                    reached = done + k
+                    ms += dt * k / chunk
+                    break
+            else:
+                ms += dt
+            done += chunk
+            if done % 1000 == 0:
+                hist_out.append((done, hist[-1]["rtrms"] / r0))
+        out[prec] = {"steps": reached, "ms": ms if reached is not None else None,
+                     "drop_every_1000": hist_out, "timer": "CUDA events on the library stream"}
+        s.close()
+    f, m = out["fp64"]["ms"], out["mixed"]["ms"]
+    out["mixed"]["speedup_vs_fp64"] = (f / m) if f and m else None
+    return out
+
+
 def run_fpsi(args, ws, rank, local):
     from flowpsi_b200 import FlowPsi
     from flowpsi_b200 import _native as N
@@ -642,9 +679,14 @@ def main():
                     help="bl turbulent: SA nu~ transport or a frozen eddy viscosity")
     ap.add_argument("--converge-n", type=int, default=128,
                     help="split-tet farfield grid (n^3 x 6) of the time-to-1e-8 runs (0: skip)")
+    ap.add_argument("--bl-drop", action="store_true",
+                    help="only config 3 to a 1e-8 drop (boundary layer, SA, line SGS), FP64 and MIXED")
     ap.add_argument("--no-learned", action="store_true",
                     help="time-to-1e-8 without the learned-start arm")
     args = ap.parse_args()
+    if args.bl_drop:
+        print(json.dumps({"time_to_1e-8": bl_time_to_drop()}), flush=True)
+        return
     if args.warmup < 3:
         log("warning: fewer than 3 warm-up steps")
     ws, rank, local = dist_setup()

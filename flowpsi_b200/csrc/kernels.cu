@@ -405,6 +405,163 @@ k_grad_limiter(MeshView M, const double* __restrict__ q, const double* __restric
   }
 }
 
+// The same three passes with the per-face data of the last two staged in
+// shared memory by the first: the first pass loads, for every face of the
+// cell, the neighbour state, rL, rR and the normal, and keeps the cell's own
+// face vector x_f - x_c, the normal and the neighbour's T and pg; the
+// limiter and face-state passes then read those instead of walking the
+// face lists again (two rounds of dependent gathers fewer).  Layout
+// [entry][value][thread], so a warp's accesses are consecutive doubles.
+// For cells of at most KS_MAX faces (the launcher falls back to
+// k_grad_limiter otherwise).
+constexpr int KS_MAX = 8;
+constexpr int KS_VALS = 8;  // r_own 3, n 3, T and pg across the face
+__host__ __device__ inline size_t grad_staged_smem(int K, bool wrec) {
+  return size_t(K) * GRAD_THREADS * (KS_VALS * sizeof(double) + sizeof(int32_t)) +
+         (wrec ? size_t(GRAD_THREADS) * GPREC * sizeof(double) : 0);
+}
+template <bool WREC>
+__global__ void __launch_bounds__(GRAD_THREADS, 4)
+k_grad_staged(MeshView M, const double* __restrict__ q, const double* __restrict__ qb, int limiter,
+              double Kl, Gas gas, double* __restrict__ grad, double* __restrict__ qf) {
+  extern __shared__ __align__(16) unsigned char gsm[];
+  const int K = M.K;
+  const int t = threadIdx.x;
+  double* sv = reinterpret_cast<double*>(gsm);                                 // [K][8][T]
+  int32_t* se = reinterpret_cast<int32_t*>(sv + size_t(K) * KS_VALS * GRAD_THREADS);  // [K][T]
+  double* sr = WREC ? reinterpret_cast<double*>(gsm + size_t(K) * GRAD_THREADS * (KS_VALS * 8 + 4)) : nullptr;
+  auto V = [&](int j, int v) -> double& { return sv[(size_t(j) * KS_VALS + v) * GRAD_THREADS + t]; };
+  const int64_t c0 = int64_t(blockIdx.x) * GRAD_THREADS;
+  const int64_t c = c0 + t;
+  const int64_t nf = M.nf;
+  if (c < M.nc) {
+    double qc[5];
+    q_arr(load_q(q, c), qc);
+    double b[15], qmax[5], qmin[5];
+#pragma unroll
+    for (int k = 0; k < 15; ++k) b[k] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) qmax[k] = qmin[k] = qc[k];
+    // ---- pass 1: gradient sums and bounds; stage the face data.  All
+    // entries and neighbours first (coalesced), then the faces two at a time
+    int32_t ents[KS_MAX], nbs[KS_MAX];
+#pragma unroll
+    for (int j = 0; j < KS_MAX; ++j) {
+      const bool in = j < K;
+      ents[j] = in ? __ldg(M.ecf + int64_t(j) * M.nc + c) : -1;
+      nbs[j] = in ? __ldg(M.enb + int64_t(j) * M.nc + c) : -1;
+    }
+#pragma unroll
+    for (int j = 0; j < KS_MAX; ++j) {
+      if (j >= K) break;
+      const int32_t ent = ents[j];
+      se[size_t(j) * GRAD_THREADS + t] = ent;
+      if (ent < 0) continue;
+      const int64_t f = ent >> 1;
+      const int side = ent & 1;
+      const bool bnd = f >= M.nfi;
+      const double* p = bnd ? qb + 5 * (f - M.nfi) : q + 5 * int64_t(nbs[j] < 0 ? 0 : nbs[j]);
+      double qn[5], d[3];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) qn[k] = __ldg(p + k);
+      const double sg = side ? -1.0 : 1.0;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const double l = M.rL[k * nf + f], r = M.rR[k * nf + f];
+        d[k] = bnd ? l : sg * (l - r);
+        V(j, k) = side ? r : l;
+        V(j, 3 + k) = M.n[k * nf + f];
+      }
+      V(j, 6) = qn[0];
+      V(j, 7) = qn[4];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        const double dq = qn[k] - qc[k];
+        b[3 * k] += d[0] * dq;
+        b[3 * k + 1] += d[1] * dq;
+        b[3 * k + 2] += d[2] * dq;
+        qmax[k] = dmax(qmax[k], qn[k]);
+        qmin[k] = dmin(qmin[k], qn[k]);
+      }
+    }
+    const double m0 = M.Minv[c], m1 = M.Minv[M.nc + c], m2 = M.Minv[2 * M.nc + c],
+                 m3 = M.Minv[3 * M.nc + c], m4 = M.Minv[4 * M.nc + c], m5 = M.Minv[5 * M.nc + c];
+    double g[15];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const double bx = b[3 * k], by = b[3 * k + 1], bz = b[3 * k + 2];
+      g[3 * k] = m0 * bx + m1 * by + m2 * bz;
+      g[3 * k + 1] = m1 * bx + m3 * by + m4 * bz;
+      g[3 * k + 2] = m2 * bx + m4 * by + m5 * bz;
+    }
+    // ---- pass 2: limiter over the staged face vectors
+    double ph[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) ph[k] = limiter == FPSI_LIMITER_ZERO ? 0.0 : 1.0;
+    if (limiter == FPSI_LIMITER_VENKATAKRISHNAN || limiter == FPSI_LIMITER_BARTH) {
+      const double h = cbrt(M.vol[c]);
+      const double kh = Kl * h;
+      const double eps2 = kh * kh * kh;
+      for (int j = 0; j < K; ++j) {
+        if (se[size_t(j) * GRAD_THREADS + t] < 0) continue;
+        const double rx = V(j, 0), ry = V(j, 1), rz = V(j, 2);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+          const double d2 = g[3 * k] * rx + g[3 * k + 1] * ry + g[3 * k + 2] * rz;
+          // min(1, a / b) divides only where the ratio is below 1
+          double p = 1.0;
+          if (d2 != 0.0) {
+            const double d1 = d2 > 0 ? qmax[k] - qc[k] : qmin[k] - qc[k];
+            if (limiter == FPSI_LIMITER_BARTH) {
+              if (d2 > 0 ? d1 < d2 : d1 > d2) p = d1 / d2;
+            } else {
+              const double num = (d1 * d1 + eps2) + 2.0 * d2 * d1;
+              const double den = d1 * d1 + 2.0 * d2 * d2 + d1 * d2 + eps2;
+              if (num < den) p = num / den;
+            }
+          }
+          ph[k] = dmin(ph[k], p);
+        }
+      }
+    }
+    // ---- pass 3: face states from the staged data
+    for (int j = 0; j < K; ++j) {
+      const int32_t ent = se[size_t(j) * GRAD_THREADS + t];
+      if (ent < 0) continue;
+      const int64_t f = ent >> 1;
+      const int side = ent & 1;
+      const double rx = V(j, 0), ry = V(j, 1), rz = V(j, 2);
+      const double nx = V(j, 3), ny = V(j, 4), nz = V(j, 5);
+      const double Tn = V(j, 6), pn = V(j, 7);
+      double l[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) l[k] = qc[k] + ph[k] * (g[3 * k] * rx + g[3 * k + 1] * ry + g[3 * k + 2] * rz);
+      l[0] = dmax(l[0], 0.1 * dmin(side ? Tn : qc[0], side ? qc[0] : Tn));
+      l[4] = dmax(l[4], 0.1 * dmin(side ? pn : qc[4], side ? qc[4] : pn) - 0.9 * gas.pamb);
+      double* o = qf + int64_t(QFREC) * f;
+      side_record(o + (QFREC / 2) * side, l, side_maxev(qc, nx, ny, nz, gas));
+      if (f >= M.nfi) {
+        double qbs[5];
+        const double* p = qb + 5 * (f - M.nfi);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) qbs[k] = __ldg(p + k);
+        side_record(o + QFREC / 2, qbs, side_maxev(qbs, nx, ny, nz, gas));
+      }
+    }
+    if (WREC) {
+#pragma unroll
+      for (int k = 0; k < 15; ++k) sr[GPREC * t + k] = g[k];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) sr[GPREC * t + 15 + k] = ph[k];
+    }
+  }
+  if (WREC) {
+    __syncthreads();
+    const int cnt = int(min(int64_t(GRAD_THREADS), M.nc - c0));
+    for (int i = t; i < GPREC * cnt; i += GRAD_THREADS) grad[GPREC * c0 + i] = sr[i];
+  }
+}
+
 // The two reconstructed states of a face and their spectral radii, from
 // the face record the gradient kernel wrote (six aligned 16 B loads).
 struct FaceStates {
@@ -1748,10 +1905,29 @@ dev::Gas gas(const fpsi_ctx* x) {
 }
 }  // namespace
 
+// the gradient, limiter and face-state kernel: the shared-memory staged
+// form for cells of at most KS_MAX faces, else the general one
+template <bool WREC>
+void launch_grad(fpsi_ctx* x, const dev::MeshView& M, cudaStream_t s) {
+  const unsigned nb = blocks_for(M.nc, dev::GRAD_THREADS);
+  if (M.K <= dev::KS_MAX) {
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(dev::k_grad_staged<WREC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           int(dev::grad_staged_smem(dev::KS_MAX, true)));
+      attr = true;
+    }
+    dev::k_grad_staged<WREC><<<nb, dev::GRAD_THREADS, dev::grad_staged_smem(M.K, WREC), s>>>(
+        M, x->d_q, x->d_qb, x->P.limiter, x->P.Kl, gas(x), x->d_grad, x->d_qf);
+  } else {
+    dev::k_grad_limiter<WREC><<<nb, dev::GRAD_THREADS, 0, s>>>(M, x->d_q, x->d_qb, x->P.limiter,
+                                                               x->P.Kl, gas(x), x->d_grad, x->d_qf);
+  }
+}
+
 int launch_grad_records(fpsi_ctx* x) {
   const dev::MeshView M = view(x);
-  dev::k_grad_limiter<true><<<blocks_for(M.nc, dev::GRAD_THREADS), dev::GRAD_THREADS, 0, x->stream>>>(
-      M, x->d_q, x->d_qb, x->P.limiter, x->P.Kl, gas(x), x->d_grad, x->d_qf);
+  launch_grad<true>(x, M, x->stream);
   FPSI_CUDA_TRY(cudaGetLastError());
   x->grad_valid = true;
   return FPSI_OK;
@@ -1788,11 +1964,9 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
   // terms, the SA model and the KEC flux read them
   x->grad_valid = x->P.viscous != 0 || kec;
   if (x->grad_valid)
-    dev::k_grad_limiter<true><<<blocks_for(M.nc, dev::GRAD_THREADS), dev::GRAD_THREADS, 0, s>>>(
-        M, x->d_q, x->d_qb, x->P.limiter, x->P.Kl, g, x->d_grad, x->d_qf);
+    launch_grad<true>(x, M, s);
   else
-    dev::k_grad_limiter<false><<<blocks_for(M.nc, dev::GRAD_THREADS), dev::GRAD_THREADS, 0, s>>>(
-        M, x->d_q, x->d_qb, x->P.limiter, x->P.Kl, g, x->d_grad, x->d_qf);
+    launch_grad<false>(x, M, s);
   if (kec)
     dev::k_alpha_diss<<<blocks_for(M.nc, dev::AD_THREADS), dev::AD_THREADS, 0, s>>>(
         M, x->d_q, x->d_qb, x->d_grad, g, lds(x), x->d_adiss);

@@ -175,12 +175,20 @@ def test_region_snapshot_matches_the_replica(need_gpu):
 
 def test_inference_matches_the_training_forward(need_gpu):
     """fpsi_gnn_predict runs the warp-specialised inference layers on BF16
-    features made in one pass; a snapshot of the same system runs the
+    features made in one pass (tets and hexes); a snapshot of the same system runs the
     training forward on FP32 features, which its first layer rounds to BF16.
     Both must give the same network output: the loss of predict's output
     against the snapshot's target is the snapshot's own loss."""
-    for n, prec in ((8, "fp64"), (6, "mixed")):
-        case, g, _ = _system(n=n, prec=prec)
+    for n, prec in ((8, "fp64"), (6, "mixed"), ("hex", "fp64")):
+        if n == "hex":  # six faces per cell: two of them gathered past the first four
+            case = cases.farfield_cube(6, precision=prec)
+            g = FlowPsi(case.mesh, case.params)
+            g.keep_blocks(True)
+            g.set_state(*case.initial_state(g.geometry()["cellcenter"]))
+            g.residual()
+            g.assemble()
+        else:
+            case, g, _ = _system(n=n, prec=prec)
         model = LearnedStart(seed=5)
         _random_head(model)
         model.add_snapshot(g, g.get_iterate())
