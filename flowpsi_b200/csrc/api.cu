@@ -369,6 +369,8 @@ int fpsi_destroy(fpsi_ctx* x) {
   for (void* p : ps)
     if (p) cudaFree(p);
   if (x->h_resid) cudaFreeHost(x->h_resid);
+  if (x->h_flags) cudaFreeHost(x->h_flags);
+  if (x->h_amin) cudaFreeHost(x->h_amin);
   if (x->d_hist) cudaFree(x->d_hist);
   if (x->h_hist) cudaFreeHost(x->h_hist);
   for (cudaEvent_t e : x->evpool) cudaEventDestroy(e);
@@ -486,7 +488,9 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
   TRY(dalloc(x, &x->d_resid, 32));
   TRY(dalloc(x, &x->d_amin, size_t(x->nblk_norm)));
   TRY(dalloc(x, &x->d_err, 4));
-  if (cudaMallocHost((void**)&x->h_resid, 32 * sizeof(double)) != cudaSuccess) {
+  if (cudaMallocHost((void**)&x->h_resid, 32 * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost((void**)&x->h_flags, 4 * sizeof(int32_t)) != cudaSuccess ||
+      cudaMallocHost((void**)&x->h_amin, size_t(x->nblk_norm) * sizeof(double)) != cudaSuccess) {
     fpsi_destroy(x);
     return FPSI_E_NOMEM;
   }
@@ -1133,26 +1137,55 @@ int ex_residual(fpsi_ctx* x) {
   return FPSI_OK;
 }
 
-// assemble, start, relax and update from the residual in d_resid
+// assemble, start, relax and update from the residual in d_resid, queued
+// with no host synchronisation (unless the sweeps run to a tolerance).  The
+// update leaves the state alone when the assembly (a zero pivot) or the
+// learned start (a wait that gave up) raised an error bit; the bits and the
+// update's step fractions are copied to pinned memory behind the kernels
+// and checked by ex_finish after the next residual's synchronisation.
 int ex_attempt(fpsi_ctx* x, fpsi_gnn* model, const fpsi_step_opts& o, int start,
                fpsi_stepinfo* info) {
+  x->h_flags[0] = x->h_flags[1] = 0;
   int rc = fpsi::launch_assemble(x);
   if (rc) return rc;
-  if ((rc = finish_assemble(x))) return rc;
   x->have_asm = true;
+  int32_t* merr = nullptr;
   if (start == FPSI_START_ZERO) {
     FPSI_CUDA_TRY(cudaMemsetAsync(x->d_x, 0, size_t(x->H.nc) * 5 * x->x_bytes, x->stream));
   } else if (start == FPSI_START_LEARNED) {
-    if ((rc = fpsi_gnn_predict(model, x, nullptr))) return rc;
+    if ((rc = fpsi::gnn_predict_launch(model, x, nullptr))) return rc;
+    merr = fpsi::gnn_error_bits(model);
   }
   if ((rc = ex_sweeps(x, o, &info->ls))) return rc;
-  if ((rc = fpsi::launch_update(x, x->d_resid))) return rc;
-  std::vector<double> a(x->nblk_norm);
-  FPSI_CUDA_TRY(cudaMemcpyAsync(a.data(), x->d_amin, a.size() * sizeof(double),
+  if ((rc = fpsi::launch_update(x, x->d_resid, x->d_err, merr))) return rc;
+  FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_flags, x->d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, x->stream));
+  FPSI_CUDA_TRY(cudaMemsetAsync(x->d_err, 0, sizeof(int32_t), x->stream));
+  if (merr) {
+    FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_flags + 1, merr, sizeof(int32_t), cudaMemcpyDeviceToHost, x->stream));
+    FPSI_CUDA_TRY(cudaMemsetAsync(merr, 0, sizeof(int32_t), x->stream));
+  }
+  FPSI_CUDA_TRY(cudaMemcpyAsync(x->h_amin, x->d_amin, size_t(x->nblk_norm) * sizeof(double),
                                 cudaMemcpyDeviceToHost, x->stream));
-  if ((rc = sync(x))) return rc;
-  info->min_alpha = *std::min_element(a.begin(), a.end());
   x->have_resid = x->have_asm = x->have_dq = x->x_preset = false;
+  return FPSI_OK;
+}
+
+// after ex_attempt and the synchronisation of the residual that follows it
+int ex_finish(fpsi_ctx* x, fpsi_stepinfo* info) {
+  const int32_t ea = x->h_flags[0], em = x->h_flags[1];
+  if (ea & 4) {
+    fpsi::set_error("a line solve gave up waiting for its staged rows");
+    return FPSI_E_TIMEOUT;
+  }
+  if (ea) {
+    fpsi::set_error("zero pivot in a diagonal block LU");
+    return FPSI_E_SINGULAR;
+  }
+  if (em) {
+    fpsi::set_error("learned start: a tensor-core wait timed out");
+    return FPSI_E_TIMEOUT;
+  }
+  info->min_alpha = *std::min_element(x->h_amin, x->h_amin + x->nblk_norm);
   return FPSI_OK;
 }
 }  // namespace
@@ -1195,6 +1228,7 @@ int fpsi_newton_step_ex(fpsi_ctx* x, fpsi_gnn* model, const fpsi_step_opts* opts
   si.start_used = o.start;
   if ((rc = ex_attempt(x, model, o, o.start, &si))) return rc;
   if ((rc = ex_residual(x))) return rc;
+  if ((rc = ex_finish(x, &si))) return rc;
   if (may_reject && !(x->h_resid[0] < r_start[0])) {
     // the step did not lower the FP64 density residual: undo it and take
     // the reference's step from D^-1 B
@@ -1204,6 +1238,7 @@ int fpsi_newton_step_ex(fpsi_ctx* x, fpsi_gnn* model, const fpsi_step_opts* opts
     si.start_used = FPSI_START_JACOBI;
     if ((rc = ex_attempt(x, model, o, FPSI_START_JACOBI, &si))) return rc;
     if ((rc = ex_residual(x))) return rc;
+    if ((rc = ex_finish(x, &si))) return rc;
   }
   fill_norms(x, x->h_resid, &si.resid_after);
   if (info) *info = si;

@@ -165,6 +165,10 @@ struct fpsi_ctx {
   double* d_part = nullptr;    // per-block partial norms
   double* d_resid = nullptr;   // 16 doubles: final norms
   double* h_resid = nullptr;   // pinned mirror
+  // pinned: a learned step's error bits ([0] assembly, [1] the model) and
+  // the update's per-block step fractions, read after its one synchronisation
+  int32_t* h_flags = nullptr;
+  double* h_amin = nullptr;
   // residual history of fpsi_run / fpsi_run_timed: 8 norms per step on the
   // device and their pinned host mirror, kept for the context's life (grown
   // only for a longer run than any before)
@@ -250,6 +254,8 @@ void wall_distance(const fpsi_mesh* m, const HostMesh& H, std::vector<double>& o
 bool sa_active(const fpsi_ctx* x);
 int sa_launch_tmu(fpsi_ctx* x);
 int sa_launch_residual(fpsi_ctx* x);
+int gnn_predict_launch(fpsi_gnn* m, fpsi_ctx* x, double* dx0);
+int32_t* gnn_error_bits(fpsi_gnn* m);  // the model's device error word
 int sa_launch_solve(fpsi_ctx* x);
 int sa_launch_update(fpsi_ctx* x, const double* guard);
 }  // namespace fpsi

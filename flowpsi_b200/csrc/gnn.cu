@@ -1851,8 +1851,33 @@ extern "C" {
 // the three layers with the head, and the start written over D^-1 B.
 int fpsi_gnn_predict(fpsi_gnn* m, fpsi_ctx* x, double* x0) {
   if (!m || !x) return FPSI_E_INVALID;
+  const int64_t nc = x->H.nc;
+  double* dx0 = nullptr;
+  int rc = FPSI_OK;
+  if (x0 && (rc = galloc(&dx0, nc * 5))) return rc;
+  rc = fpsi::gnn_predict_launch(m, x, dx0);
+  if (!rc && cudaStreamSynchronize(x->stream) != cudaSuccess) rc = FPSI_E_CUDA;
+  if (!rc) rc = take_error(m);
+  if (!rc && x0) {
+    std::vector<double> h(nc * 5);
+    if (cudaMemcpy(h.data(), dx0, h.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess) rc = FPSI_E_CUDA;
+    for (int64_t i = 0; !rc && i < nc; ++i)
+      for (int k = 0; k < 5; ++k) x0[5 * int64_t(x->H.perm[i]) + k] = h[5 * i + k];
+  }
+  cudaFree(dx0);
+  return rc;
+}
+
+}  // extern "C"
+namespace fpsi {
+// Inference queued on the context's stream with no host synchronisation:
+// the Jacobi start, the features, the layers and the start written into the
+// iterate (and, with dx0, a copy in RCM order).  The model's error bits
+// (gnn_error_bits) are left for the caller to read.
+int32_t* gnn_error_bits(fpsi_gnn* m) { return m->d_err; }
+int gnn_predict_launch(fpsi_gnn* m, fpsi_ctx* x, double* dx0) {
   if (!x->have_asm || !x->d_D || x->P.solver == FPSI_SOLVER_LSGS) {
-    fpsi::set_error("learned start: needs an assembled SGS system with the diagonal blocks kept");
+    set_error("learned start: needs an assembled SGS system with the diagonal blocks kept");
     return FPSI_E_STATE;
   }
   const int64_t nc = x->H.nc;
@@ -1864,7 +1889,7 @@ int fpsi_gnn_predict(fpsi_gnn* m, fpsi_ctx* x, double* x0) {
   if (!x->d_xprev) {
     if (cudaMalloc(&x->d_xprev, size_t(nc) * 5 * 8) != cudaSuccess) {
       x->d_xprev = nullptr;
-      fpsi::set_error("cudaMalloc failed for the previous-update copy");
+      set_error("cudaMalloc failed for the previous-update copy");
       return FPSI_E_NOMEM;
     }
     x->have_xprev = false;
@@ -1873,7 +1898,7 @@ int fpsi_gnn_predict(fpsi_gnn* m, fpsi_ctx* x, double* x0) {
   FPSI_CUDA_TRY(cudaStreamSynchronize(m->stream));  // no training pass in flight
   cudaStream_t s = x->stream;
   // x_J = D^-1 B from the factored blocks (the iterate may hold a solve)
-  if ((rc = fpsi::launch_jacobi_start(x))) return rc;
+  if ((rc = launch_jacobi_start(x))) return rc;
   // BF16 features [nc][40] in a backward-pass buffer an inference pass does
   // not use ([nc][64] FP32)
   __nv_bfloat16* feat16 = reinterpret_cast<__nv_bfloat16*>(m->d_dz);
@@ -1884,23 +1909,13 @@ int fpsi_gnn_predict(fpsi_gnn* m, fpsi_ctx* x, double* x0) {
   else
     launch_features16<float, double>(m, x, feat16, s);
   if ((rc = forward(m, G, nullptr, false, feat16, s))) return rc;
-  double* dx0 = nullptr;
-  if (x0 && (rc = galloc(&dx0, nc * 5))) return rc;
   if (x->P.precision == FPSI_PREC_MIXED)
     k_apply_start<float><<<nb_(nc, 256), 256, 0, s>>>(nc, m->d_y, m->d_fac, x->d_ci, (float*)x->d_x, dx0);
   else
     k_apply_start<double><<<nb_(nc, 256), 256, 0, s>>>(nc, m->d_y, m->d_fac, x->d_ci, (double*)x->d_x, dx0);
-  if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) rc = FPSI_E_CUDA;
-  if (!rc) rc = take_error(m);
-  if (!rc && x0) {
-    std::vector<double> h(nc * 5);
-    if (cudaMemcpy(h.data(), dx0, h.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess) rc = FPSI_E_CUDA;
-    for (int64_t i = 0; !rc && i < nc; ++i)
-      for (int k = 0; k < 5; ++k) x0[5 * int64_t(x->H.perm[i]) + k] = h[5 * i + k];
-  }
-  cudaFree(dx0);
-  if (!rc) x->x_preset = true;
-  return rc;
+  FPSI_CUDA_TRY(cudaGetLastError());
+  x->x_preset = true;
+  return FPSI_OK;
 }
+}  // namespace fpsi
 
-}  // extern "C"

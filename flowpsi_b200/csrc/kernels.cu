@@ -906,6 +906,9 @@ k_cell_residual(MeshView M, const double* __restrict__ q, const double* __restri
   double rt = 0, et = 0, mt = 0, rmax = 0, emax = 0, mmax = 0;
   double rloc = -1, eloc = -1;
   if (c < M.nc) {
+    // the cell's own state and volume are requested before its face records
+    const Q5 qc = load_q(q, c);
+    const double V = M.vol[c];
     double s[5] = {0, 0, 0, 0, 0};
     double meva = 0;
     // the face records four at a time from the entry-major lists, all four
@@ -937,11 +940,9 @@ k_cell_residual(MeshView M, const double* __restrict__ q, const double* __restri
       for (int i = 0; i < ECH; ++i)
         if (ent[i] >= 0) add(ent[i], rec[i]);
     }
-    const double V = M.vol[c];
     const double cflpdt = 0.5 * meva / V;
     double dt = dtmax;
     if (cflmax > 0) dt = dmin(dt, cflmax / cflpdt);
-    const Q5 qc = load_q(q, c);
     // dtau, solverTimestep.loci:302-329 with eta == 1
     const double rvol = 1.0 / V;
     const double p = qc.p + g.pamb, T = qc.T;
@@ -1750,10 +1751,14 @@ __global__ void __launch_bounds__(NORM_THREADS)
 // relax: 0.9 (steady, solverNewton.loci:62-78) or 0.75 of T and p (BDF2,
 // :163-182, whose floor is max(|d|, 1e-30) instead of |d| + 1e-30)
 k_update(int64_t nc, double pamb, const int32_t* __restrict__ ci, const TX* __restrict__ x, double* __restrict__ q,
-         double* __restrict__ amin_part, const double* __restrict__ guard, bool bdf) {
+         double* __restrict__ amin_part, const double* __restrict__ guard, bool bdf,
+         const int32_t* __restrict__ flag0, const int32_t* __restrict__ flag1) {
   const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   double alpha = 1.0;
-  const bool halt = guard && (isnan(guard[0]) || isnan(guard[1]) || isnan(guard[2]));
+  // the state stays as it is for a step with NaN norms, or (flags given)
+  // whose assembly or learned start raised an error bit
+  const bool halt = (guard && (isnan(guard[0]) || isnan(guard[1]) || isnan(guard[2]))) ||
+                    (flag0 && *flag0 != 0) || (flag1 && *flag1 != 0);
   if (c < nc && !halt) {
     double* qc = q + 5 * c;
     const TX* d = x + 5 * int64_t(ci[c]);
@@ -2215,7 +2220,7 @@ int launch_linres(fpsi_ctx* x, double* out2) {
   }
 }
 
-int launch_update(fpsi_ctx* x, const double* guard) {
+int launch_update(fpsi_ctx* x, const double* guard, const int32_t* flag0, const int32_t* flag1) {
   const int64_t nc = x->H.nc;
   const bool lsgs = x->P.solver == FPSI_SOLVER_LSGS;
   const int32_t* map = lsgs ? x->d_lt : x->d_ci;
@@ -2223,10 +2228,12 @@ int launch_update(fpsi_ctx* x, const double* guard) {
   prof_begin(x, "update");
   if (x->P.precision == FPSI_PREC_MIXED)
     dev::k_update<float><<<x->nblk_norm, dev::NORM_THREADS, 0, x->stream>>>(
-        nc, x->P.Pambient, map, (const float*)xv, x->d_q, x->d_amin, guard, x->P.time_accurate != 0);
+        nc, x->P.Pambient, map, (const float*)xv, x->d_q, x->d_amin, guard, x->P.time_accurate != 0,
+        flag0, flag1);
   else
     dev::k_update<double><<<x->nblk_norm, dev::NORM_THREADS, 0, x->stream>>>(
-        nc, x->P.Pambient, map, (const double*)xv, x->d_q, x->d_amin, guard, x->P.time_accurate != 0);
+        nc, x->P.Pambient, map, (const double*)xv, x->d_q, x->d_amin, guard, x->P.time_accurate != 0,
+        flag0, flag1);
   prof_end(x);
   FPSI_CUDA_TRY(cudaGetLastError());
   if (x->keep_prev && x->d_xprev && !lsgs) {

@@ -29,7 +29,8 @@ int ensure_explicit_blocks(fpsi_ctx* x);
 // clipped Newton update; per-block minimum alpha into d_amin.  guard
 // (device, may be null): the norms of the residual the system came from;
 // NaN norms leave the state unchanged
-int launch_update(fpsi_ctx* x, const double* guard);
+int launch_update(fpsi_ctx* x, const double* guard, const int32_t* flag0 = nullptr,
+                  const int32_t* flag1 = nullptr);
 // caller-order staging buffer <-> device state (in = staging -> q)
 int launch_state(fpsi_ctx* x, bool in);
 
