@@ -389,6 +389,12 @@ def _drop_arm(solver, case, drop, max_steps, chunk, model=None):
                 ms_tot += ms
             done += chunk
     else:
+        # one untimed learned step first: the context builds its cell graph
+        # for the network and allocates the inference and rejection buffers
+        # once per mesh, as the other arms' setup does; then the state is
+        # reset, which also drops that step's update from the features
+        solver.newton_step_ex(start="learned", model=model, reject=True)
+        solver.set_state(*case.initial_state(solver.geometry()["cellcenter"]))
         t0 = time.perf_counter()
         for k in range(max_steps):
             r = solver.newton_step_ex(start="learned", model=model, reject=True)

@@ -1153,7 +1153,7 @@ int ex_attempt(fpsi_ctx* x, fpsi_gnn* model, const fpsi_step_opts& o, int start,
   if (start == FPSI_START_ZERO) {
     FPSI_CUDA_TRY(cudaMemsetAsync(x->d_x, 0, size_t(x->H.nc) * 5 * x->x_bytes, x->stream));
   } else if (start == FPSI_START_LEARNED) {
-    if ((rc = fpsi::gnn_predict_launch(model, x, nullptr))) return rc;
+    if ((rc = fpsi::gnn_predict_launch(model, x, nullptr, x->P.solver == FPSI_SOLVER_SGS))) return rc;
     merr = fpsi::gnn_error_bits(model);
   }
   if ((rc = ex_sweeps(x, o, &info->ls))) return rc;

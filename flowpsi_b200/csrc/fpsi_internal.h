@@ -254,7 +254,7 @@ void wall_distance(const fpsi_mesh* m, const HostMesh& H, std::vector<double>& o
 bool sa_active(const fpsi_ctx* x);
 int sa_launch_tmu(fpsi_ctx* x);
 int sa_launch_residual(fpsi_ctx* x);
-int gnn_predict_launch(fpsi_gnn* m, fpsi_ctx* x, double* dx0);
+int gnn_predict_launch(fpsi_gnn* m, fpsi_ctx* x, double* dx0, bool jacobi_in_iterate = false);
 int32_t* gnn_error_bits(fpsi_gnn* m);  // the model's device error word
 int sa_launch_solve(fpsi_ctx* x);
 int sa_launch_update(fpsi_ctx* x, const double* guard);

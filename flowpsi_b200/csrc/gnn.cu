@@ -1873,9 +1873,10 @@ namespace fpsi {
 // Inference queued on the context's stream with no host synchronisation:
 // the Jacobi start, the features, the layers and the start written into the
 // iterate (and, with dx0, a copy in RCM order).  The model's error bits
-// (gnn_error_bits) are left for the caller to read.
+// (gnn_error_bits) are left for the caller to read.  jacobi_in_iterate: the
+// iterate already holds D^-1 B (an SGS assembly has just written it).
 int32_t* gnn_error_bits(fpsi_gnn* m) { return m->d_err; }
-int gnn_predict_launch(fpsi_gnn* m, fpsi_ctx* x, double* dx0) {
+int gnn_predict_launch(fpsi_gnn* m, fpsi_ctx* x, double* dx0, bool jacobi_in_iterate) {
   if (!x->have_asm || !x->d_D || x->P.solver == FPSI_SOLVER_LSGS) {
     set_error("learned start: needs an assembled SGS system with the diagonal blocks kept");
     return FPSI_E_STATE;
@@ -1898,7 +1899,7 @@ int gnn_predict_launch(fpsi_gnn* m, fpsi_ctx* x, double* dx0) {
   FPSI_CUDA_TRY(cudaStreamSynchronize(m->stream));  // no training pass in flight
   cudaStream_t s = x->stream;
   // x_J = D^-1 B from the factored blocks (the iterate may hold a solve)
-  if ((rc = launch_jacobi_start(x))) return rc;
+  if (!jacobi_in_iterate && (rc = launch_jacobi_start(x))) return rc;
   // BF16 features [nc][40] in a backward-pass buffer an inference pass does
   // not use ([nc][64] FP32)
   __nv_bfloat16* feat16 = reinterpret_cast<__nv_bfloat16*>(m->d_dz);
