@@ -562,174 +562,6 @@ k_grad_staged(MeshView M, const double* __restrict__ q, const double* __restrict
   }
 }
 
-// The staged kernel with its first pass's gathers made asynchronous: each
-// thread issues `cp.async` copies (8 B each) of every face's neighbour
-// state, rL, rR and normal straight into shared memory, all of them at
-// once, waits for its own copies and then runs the three passes out of
-// shared memory.  The copies hold no registers, so every face of every
-// resident cell is in flight together.  Layout [entry][value][thread].
-constexpr int KA_VALS = 14;  // neighbour state 5, rL 3, rR 3, n 3
-__host__ __device__ inline size_t grad_async_smem(int K, bool wrec) {
-  return size_t(K) * GRAD_THREADS * (KA_VALS * sizeof(double) + sizeof(int32_t)) +
-         (wrec ? size_t(GRAD_THREADS) * GPREC * sizeof(double) : 0);
-}
-__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
-               "l"(src)
-               : "memory");
-}
-template <bool WREC>
-__global__ void __launch_bounds__(GRAD_THREADS, 4)
-k_grad_async(MeshView M, const double* __restrict__ q, const double* __restrict__ qb, int limiter,
-             double Kl, Gas gas, double* __restrict__ grad, double* __restrict__ qf) {
-  extern __shared__ __align__(16) unsigned char gsm[];
-  const int K = M.K;
-  const int t = threadIdx.x;
-  double* sv = reinterpret_cast<double*>(gsm);                                          // [K][14][T]
-  int32_t* se = reinterpret_cast<int32_t*>(sv + size_t(K) * KA_VALS * GRAD_THREADS);  // [K][T]
-  double* sr = WREC ? reinterpret_cast<double*>(gsm + size_t(K) * GRAD_THREADS * (KA_VALS * 8 + 4)) : nullptr;
-  auto V = [&](int j, int v) -> double& { return sv[(size_t(j) * KA_VALS + v) * GRAD_THREADS + t]; };
-  const int64_t c0 = int64_t(blockIdx.x) * GRAD_THREADS;
-  const int64_t c = c0 + t;
-  const int64_t nf = M.nf;
-  if (c < M.nc) {
-    // ---- every face's data on its way into shared memory
-#pragma unroll
-    for (int j = 0; j < KS_MAX; ++j) {
-      if (j >= K) break;
-      const int32_t ent = __ldg(M.ecf + int64_t(j) * M.nc + c);
-      se[size_t(j) * GRAD_THREADS + t] = ent;
-      if (ent < 0) continue;
-      const int64_t f = ent >> 1;
-      const double* p;
-      if (f >= M.nfi) {
-        p = qb + 5 * (f - M.nfi);
-      } else {
-        const int32_t o = __ldg(M.enb + int64_t(j) * M.nc + c);
-        p = q + 5 * int64_t(o);
-      }
-#pragma unroll
-      for (int k = 0; k < 5; ++k) cp_async8(&V(j, k), p + k);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        cp_async8(&V(j, 5 + k), M.rL + k * nf + f);
-        cp_async8(&V(j, 8 + k), M.rR + k * nf + f);
-        cp_async8(&V(j, 11 + k), M.n + k * nf + f);
-      }
-    }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    double qc[5];
-    q_arr(load_q(q, c), qc);
-    const double m0 = M.Minv[c], m1 = M.Minv[M.nc + c], m2 = M.Minv[2 * M.nc + c],
-                 m3 = M.Minv[3 * M.nc + c], m4 = M.Minv[4 * M.nc + c], m5 = M.Minv[5 * M.nc + c];
-    const double vol = M.vol[c];
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
-    // ---- pass 1: gradient sums and bounds, in the cell's face order
-    double b[15], qmax[5], qmin[5];
-#pragma unroll
-    for (int k = 0; k < 15; ++k) b[k] = 0.0;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) qmax[k] = qmin[k] = qc[k];
-    for (int j = 0; j < K; ++j) {
-      const int32_t ent = se[size_t(j) * GRAD_THREADS + t];
-      if (ent < 0) continue;
-      const bool bnd = (ent >> 1) >= M.nfi;
-      const double sg = (ent & 1) ? -1.0 : 1.0;
-      double d[3];
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const double l = V(j, 5 + k), r = V(j, 8 + k);
-        d[k] = bnd ? l : sg * (l - r);
-      }
-#pragma unroll
-      for (int k = 0; k < 5; ++k) {
-        const double qn = V(j, k);
-        const double dq = qn - qc[k];
-        b[3 * k] += d[0] * dq;
-        b[3 * k + 1] += d[1] * dq;
-        b[3 * k + 2] += d[2] * dq;
-        qmax[k] = dmax(qmax[k], qn);
-        qmin[k] = dmin(qmin[k], qn);
-      }
-    }
-    double g[15];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      const double bx = b[3 * k], by = b[3 * k + 1], bz = b[3 * k + 2];
-      g[3 * k] = m0 * bx + m1 * by + m2 * bz;
-      g[3 * k + 1] = m1 * bx + m3 * by + m4 * bz;
-      g[3 * k + 2] = m2 * bx + m4 * by + m5 * bz;
-    }
-    // ---- pass 2: limiter
-    double ph[5];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) ph[k] = limiter == FPSI_LIMITER_ZERO ? 0.0 : 1.0;
-    if (limiter == FPSI_LIMITER_VENKATAKRISHNAN || limiter == FPSI_LIMITER_BARTH) {
-      const double h = cbrt(vol);
-      const double kh = Kl * h;
-      const double eps2 = kh * kh * kh;
-      for (int j = 0; j < K; ++j) {
-        const int32_t ent = se[size_t(j) * GRAD_THREADS + t];
-        if (ent < 0) continue;
-        const int ro = (ent & 1) ? 8 : 5;
-        const double rx = V(j, ro), ry = V(j, ro + 1), rz = V(j, ro + 2);
-#pragma unroll
-        for (int k = 0; k < 5; ++k) {
-          const double d2 = g[3 * k] * rx + g[3 * k + 1] * ry + g[3 * k + 2] * rz;
-          // min(1, a / b) divides only where the ratio is below 1
-          double p = 1.0;
-          if (d2 != 0.0) {
-            const double d1 = d2 > 0 ? qmax[k] - qc[k] : qmin[k] - qc[k];
-            if (limiter == FPSI_LIMITER_BARTH) {
-              if (d2 > 0 ? d1 < d2 : d1 > d2) p = d1 / d2;
-            } else {
-              const double num = (d1 * d1 + eps2) + 2.0 * d2 * d1;
-              const double den = d1 * d1 + 2.0 * d2 * d2 + d1 * d2 + eps2;
-              if (num < den) p = num / den;
-            }
-          }
-          ph[k] = dmin(ph[k], p);
-        }
-      }
-    }
-    // ---- pass 3: face states
-    for (int j = 0; j < K; ++j) {
-      const int32_t ent = se[size_t(j) * GRAD_THREADS + t];
-      if (ent < 0) continue;
-      const int64_t f = ent >> 1;
-      const int side = ent & 1;
-      const int ro = side ? 8 : 5;
-      const double rx = V(j, ro), ry = V(j, ro + 1), rz = V(j, ro + 2);
-      const double nx = V(j, 11), ny = V(j, 12), nz = V(j, 13);
-      const double Tn = V(j, 0), pn = V(j, 4);
-      double l[5];
-#pragma unroll
-      for (int k = 0; k < 5; ++k) l[k] = qc[k] + ph[k] * (g[3 * k] * rx + g[3 * k + 1] * ry + g[3 * k + 2] * rz);
-      l[0] = dmax(l[0], 0.1 * dmin(side ? Tn : qc[0], side ? qc[0] : Tn));
-      l[4] = dmax(l[4], 0.1 * dmin(side ? pn : qc[4], side ? qc[4] : pn) - 0.9 * gas.pamb);
-      double* o = qf + int64_t(QFREC) * f;
-      side_record(o + (QFREC / 2) * side, l, side_maxev(qc, nx, ny, nz, gas));
-      if (f >= M.nfi) {
-        double qbs[5];
-#pragma unroll
-        for (int k = 0; k < 5; ++k) qbs[k] = V(j, k);
-        side_record(o + QFREC / 2, qbs, side_maxev(qbs, nx, ny, nz, gas));
-      }
-    }
-    if (WREC) {
-#pragma unroll
-      for (int k = 0; k < 15; ++k) sr[GPREC * t + k] = g[k];
-#pragma unroll
-      for (int k = 0; k < 5; ++k) sr[GPREC * t + 15 + k] = ph[k];
-    }
-  }
-  if (WREC) {
-    __syncthreads();
-    const int cnt = int(min(int64_t(GRAD_THREADS), M.nc - c0));
-    for (int i = t; i < GPREC * cnt; i += GRAD_THREADS) grad[GPREC * c0 + i] = sr[i];
-  }
-}
-
 // The two reconstructed states of a face and their spectral radii, from
 // the face record the gradient kernel wrote (six aligned 16 B loads).
 struct FaceStates {
