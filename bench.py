@@ -221,6 +221,8 @@ def kernel_bytes(name, nc, nfi, nbf, sweeps, tb, tx, sgs_step_bytes=None, compac
         "face_flux": nf * (qf + 32 + 48),
         "cell_residual": nc * (40 + 8 + 40 + 8) + nf * 48,
         "face_jacobian": nf * (qf + 32) + jac_out,
+        # the inviscid SGS systems' flux and compact Jacobian records in one pass
+        "face_flux_jac": nf * (qf + 32 + 48) + jac_out,
         # q, src, dtau, vol; LU + B slots, pivots, Jacobi start; each face
         # block read once for the diagonal sum, interior ones written once
         # more into the off-diagonal slots

@@ -185,6 +185,8 @@ struct fpsi_ctx {
   // the explicit fjp/fjm are then filled only on request
   void* d_fjc = nullptr;       // [nf][24] TB
   bool asm_compact = false;    // the assembled system's slots are compact
+  int jac_fresh = 0;           // block bytes of compact face records written with the
+                               // current residual (the fused flux kernel), else 0
   bool have_explicit = false;  // fjp/fjm hold the assembled system's blocks
   void* d_D = nullptr;         // [nc][25] TB (only when keep_D)
   // colour-order arrays of the sweeps (see HostMesh)

@@ -716,19 +716,17 @@ struct Lds {
   double comp, dlim, ducros, upwind, nscoeff, nsfactor, filter, ssf;
 };
 
-template <bool VIS, int KIND>
-__global__ void k_face_flux(MeshView M, const double* __restrict__ q,
-                            const double* __restrict__ qb, const double* __restrict__ grad,
-                            const double* __restrict__ qf, Gas g, Visc V, double* __restrict__ F,
-                            const double* __restrict__ adiss, const float* __restrict__ ageom,
-                            Lds P) {
-  const int64_t f = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (f >= M.nf) return;
-  FaceStates s;
-  load_face_states(qf, f, s);
-  const double nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
-  const double A = M.area[f];
-  double fl[5];
+// The inviscid flux of face f from its two face states: the pressure of a
+// viscous wall, the analytic flux of the total-pressure and fixed-mass
+// conditions' boundary state, the low-dissipation fluxes on interior faces
+// (HLLC on boundary faces), or the Riemann solver KIND.
+template <int KIND>
+__device__ __forceinline__ void inviscid_face_flux(const MeshView& M, const double* __restrict__ q,
+                                                   const double* __restrict__ grad, const FaceStates& s,
+                                                   int64_t f, double nx, double ny, double nz, double A,
+                                                   const Gas& g, const double* __restrict__ adiss,
+                                                   const float* __restrict__ ageom, const Lds& P,
+                                                   double fl[5]) {
   const int bk = bc_kind(M, f);
   if (bk == FPSI_BC_VISCOUS_WALL) {
     // pressure only, from the cell-centre pressure (bcViscousWall.loci:220-230),
@@ -760,6 +758,22 @@ __global__ void k_face_flux(MeshView M, const double* __restrict__ q,
   } else {
     riemann1(KIND, s.L, s.R, nx, ny, nz, A, g, fl);
   }
+}
+
+template <bool VIS, int KIND>
+__global__ void k_face_flux(MeshView M, const double* __restrict__ q,
+                            const double* __restrict__ qb, const double* __restrict__ grad,
+                            const double* __restrict__ qf, Gas g, Visc V, double* __restrict__ F,
+                            const double* __restrict__ adiss, const float* __restrict__ ageom,
+                            Lds P) {
+  const int64_t f = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (f >= M.nf) return;
+  FaceStates s;
+  load_face_states(qf, f, s);
+  const double nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
+  const double A = M.area[f];
+  double fl[5];
+  inviscid_face_flux<KIND>(M, q, grad, s, f, nx, ny, nz, A, g, adiss, ageom, P, fl);
   if constexpr (VIS) {
     const VFace v = viscous_face(M, q, qb, grad, V, f);
 #pragma unroll
@@ -1214,6 +1228,36 @@ k_face_jacobian(MeshView M, const double* __restrict__ q, const double* __restri
 // fjp (+) and fjm (-) and the shared U, n (CK_FACE values), staged and
 // written back like the explicit blocks.  A viscous-wall face's pressure
 // block d(p n A)/dpg is c1 = -A with every other coefficient zero.
+// One face's compact Jacobian record (CK_FACE values) from its two states:
+// the fjp direction (zero on viscous walls but -A on c1, zero on the faces
+// whose difference block comes from k_bc_fdjac), the fjm direction on
+// interior faces, then the Roe velocity and the normal.
+template <class TB>
+__device__ __forceinline__ void compact_record(const MeshView& M, int64_t f, const FaceStates& s,
+                                               double nx, double ny, double nz, double A, const Gas& g,
+                                               TB* st) {
+  const RoeAvg ra = roe_average1(s.L, s.R, nx, ny, nz, g);
+  const int bk = bc_kind(M, f);
+  if (bk == FPSI_BC_VISCOUS_WALL) {
+#pragma unroll
+    for (int k = 0; k < CK_DIR; ++k) st[k] = TB(0);
+    st[CK_C1] = TB(-A);
+  } else if (fd_jacobian_kind(bk)) {  // the difference block comes from k_bc_fdjac
+#pragma unroll
+    for (int k = 0; k < CK_DIR; ++k) st[k] = TB(0);
+  } else {
+    jac_roe_compact<TB, true>(ra, A, g, +1, st);
+  }
+  if (f < M.nfi) {
+    jac_roe_compact<TB, true>(ra, A, g, -1, st + CK_DIR);
+  } else {
+#pragma unroll
+    for (int k = 0; k < CK_DIR; ++k) st[CK_DIR + k] = TB(0);
+  }
+  st[2 * CK_DIR] = TB(ra.U), st[2 * CK_DIR + 1] = TB(ra.V), st[2 * CK_DIR + 2] = TB(ra.W);
+  st[2 * CK_DIR + 3] = TB(nx), st[2 * CK_DIR + 4] = TB(ny), st[2 * CK_DIR + 5] = TB(nz);
+}
+
 template <class TB>
 __global__ void __launch_bounds__(JAC_THREADS)
 k_face_jacobian_c(MeshView M, const double* __restrict__ qf, Gas g, TB* __restrict__ fjc) {
@@ -1225,28 +1269,40 @@ k_face_jacobian_c(MeshView M, const double* __restrict__ qf, Gas g, TB* __restri
     FaceStates s;
     load_face_states(qf, f, s);
     const double nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
+    compact_record<TB>(M, f, s, nx, ny, nz, M.area[f], g, stage + CK_FACE * threadIdx.x);
+  }
+  __syncthreads();
+  for (int64_t k = threadIdx.x; k < cnt; k += JAC_THREADS) fjc[CK_FACE * f0 + k] = stage[k];
+}
+
+// The inviscid face flux and the compact Jacobian record of each face in one
+// pass over the face-state records (the SGS systems without viscous terms):
+// the face states, normal and area are read once, and the flux record and
+// the Jacobian record are both written (the latter staged for coalesced
+// stores), so the assembly does not launch k_face_jacobian_c.
+template <int KIND, class TB>
+__global__ void __launch_bounds__(JAC_THREADS)
+k_face_flux_jac(MeshView M, const double* __restrict__ q, const double* __restrict__ grad,
+                const double* __restrict__ qf, Gas g, double* __restrict__ F,
+                const double* __restrict__ adiss, const float* __restrict__ ageom, Lds P,
+                TB* __restrict__ fjc) {
+  __shared__ TB stage[JAC_THREADS * CK_FACE];
+  const int64_t f0 = int64_t(blockIdx.x) * JAC_THREADS;
+  const int64_t f = f0 + threadIdx.x;
+  const int64_t cnt = min(int64_t(JAC_THREADS), M.nf - f0) * CK_FACE;
+  if (f < M.nf) {
+    FaceStates s;
+    load_face_states(qf, f, s);
+    const double nx = M.n[f], ny = M.n[M.nf + f], nz = M.n[2 * M.nf + f];
     const double A = M.area[f];
-    const RoeAvg ra = roe_average1(s.L, s.R, nx, ny, nz, g);
-    TB* st = stage + CK_FACE * threadIdx.x;
-    const int bk = bc_kind(M, f);
-    if (bk == FPSI_BC_VISCOUS_WALL) {
-#pragma unroll
-      for (int k = 0; k < CK_DIR; ++k) st[k] = TB(0);
-      st[CK_C1] = TB(-A);
-    } else if (fd_jacobian_kind(bk)) {  // the difference block comes from k_bc_fdjac
-#pragma unroll
-      for (int k = 0; k < CK_DIR; ++k) st[k] = TB(0);
-    } else {
-      jac_roe_compact<TB, true>(ra, A, g, +1, st);
-    }
-    if (f < M.nfi) {
-      jac_roe_compact<TB, true>(ra, A, g, -1, st + CK_DIR);
-    } else {
-#pragma unroll
-      for (int k = 0; k < CK_DIR; ++k) st[CK_DIR + k] = TB(0);
-    }
-    st[2 * CK_DIR] = TB(ra.U), st[2 * CK_DIR + 1] = TB(ra.V), st[2 * CK_DIR + 2] = TB(ra.W);
-    st[2 * CK_DIR + 3] = TB(nx), st[2 * CK_DIR + 4] = TB(ny), st[2 * CK_DIR + 5] = TB(nz);
+    double fl[5];
+    inviscid_face_flux<KIND>(M, q, grad, s, f, nx, ny, nz, A, g, adiss, ageom, P, fl);
+    const double m = f < M.nfi ? dmax(s.mL, s.mR) : s.mR;
+    double2* o = reinterpret_cast<double2*>(F + FREC * f);
+    o[0] = make_double2(fl[0], fl[1]);
+    o[1] = make_double2(fl[2], fl[3]);
+    o[2] = make_double2(fl[4], m * A);
+    compact_record<TB>(M, f, s, nx, ny, nz, A, g, stage + CK_FACE * threadIdx.x);
   }
   __syncthreads();
   for (int64_t k = threadIdx.x; k < cnt; k += JAC_THREADS) fjc[CK_FACE * f0 + k] = stage[k];
@@ -1976,32 +2032,58 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
     dev::k_alpha_diss<<<blocks_for(M.nc, dev::AD_THREADS), dev::AD_THREADS, 0, s>>>(
         M, x->d_q, x->d_qb, x->d_grad, g, lds(x), x->d_adiss);
   prof_end(x);
+  // an inviscid system relaxed by SGS gets its compact face Jacobian records
+  // from the flux kernel, in the same pass over the face states
+  x->jac_fresh = 0;
+  if (!x->P.viscous && x->P.solver != FPSI_SOLVER_LSGS && x->d_fjc) {
+    prof_begin(x, "face_flux_jac");
+    const unsigned nb = blocks_for(M.nf, dev::JAC_THREADS);
+    const bool f64 = x->P.precision == FPSI_PREC_FP64;
+#define FPSI_FLUXJ(K)                                                                              \
+  do {                                                                                             \
+    if (f64)                                                                                       \
+      dev::k_face_flux_jac<K, double><<<nb, dev::JAC_THREADS, 0, s>>>(                             \
+          M, x->d_q, x->d_grad, x->d_qf, g, x->d_F, x->d_adiss, x->d_ageom, lds(x), (double*)x->d_fjc); \
+    else                                                                                           \
+      dev::k_face_flux_jac<K, float><<<nb, dev::JAC_THREADS, 0, s>>>(                              \
+          M, x->d_q, x->d_grad, x->d_qf, g, x->d_F, x->d_adiss, x->d_ageom, lds(x), (float*)x->d_fjc); \
+  } while (0)
+    if (x->P.flux == FPSI_FLUX_ROE) FPSI_FLUXJ(FPSI_FLUX_ROE);
+    else if (x->P.flux == FPSI_FLUX_HLLE) FPSI_FLUXJ(FPSI_FLUX_HLLE);
+    else if (x->P.flux == FPSI_FLUX_KEC) FPSI_FLUXJ(FPSI_FLUX_KEC);
+    else if (x->P.flux == FPSI_FLUX_SSF) FPSI_FLUXJ(FPSI_FLUX_SSF);
+    else FPSI_FLUXJ(FPSI_FLUX_HLLC);
+#undef FPSI_FLUXJ
+    x->jac_fresh = f64 ? 8 : 4;
+    prof_end(x);
+  } else {
   prof_begin(x, "face_flux");
-  // the viscous terms and each Riemann solver are separate instantiations:
-  // the inviscid Roe kernel does not carry the others' registers
-  {
-    const unsigned nb = blocks_for(M.nf, 128);
-    const dev::Visc Vv = visc(x);
-    double* F = x->d_F;
-#define FPSI_FLUX(VIS, K)                                                                     \
-  dev::k_face_flux<VIS, K><<<nb, 128, 0, s>>>(M, x->d_q, x->d_qb, x->d_grad, x->d_qf, g, Vv, F, \
-                                              x->d_adiss, x->d_ageom, lds(x))
-    if (x->P.viscous) {
-      if (x->P.flux == FPSI_FLUX_ROE) FPSI_FLUX(true, FPSI_FLUX_ROE);
-      else if (x->P.flux == FPSI_FLUX_HLLE) FPSI_FLUX(true, FPSI_FLUX_HLLE);
-      else if (x->P.flux == FPSI_FLUX_KEC) FPSI_FLUX(true, FPSI_FLUX_KEC);
-      else if (x->P.flux == FPSI_FLUX_SSF) FPSI_FLUX(true, FPSI_FLUX_SSF);
-      else FPSI_FLUX(true, FPSI_FLUX_HLLC);
-    } else {
-      if (x->P.flux == FPSI_FLUX_ROE) FPSI_FLUX(false, FPSI_FLUX_ROE);
-      else if (x->P.flux == FPSI_FLUX_HLLE) FPSI_FLUX(false, FPSI_FLUX_HLLE);
-      else if (x->P.flux == FPSI_FLUX_KEC) FPSI_FLUX(false, FPSI_FLUX_KEC);
-      else if (x->P.flux == FPSI_FLUX_SSF) FPSI_FLUX(false, FPSI_FLUX_SSF);
-      else FPSI_FLUX(false, FPSI_FLUX_HLLC);
+    // the viscous terms and each Riemann solver are separate instantiations:
+    // the inviscid Roe kernel does not carry the others' registers
+    {
+      const unsigned nb = blocks_for(M.nf, 128);
+      const dev::Visc Vv = visc(x);
+      double* F = x->d_F;
+  #define FPSI_FLUX(VIS, K)                                                                     \
+    dev::k_face_flux<VIS, K><<<nb, 128, 0, s>>>(M, x->d_q, x->d_qb, x->d_grad, x->d_qf, g, Vv, F, \
+                                                x->d_adiss, x->d_ageom, lds(x))
+      if (x->P.viscous) {
+        if (x->P.flux == FPSI_FLUX_ROE) FPSI_FLUX(true, FPSI_FLUX_ROE);
+        else if (x->P.flux == FPSI_FLUX_HLLE) FPSI_FLUX(true, FPSI_FLUX_HLLE);
+        else if (x->P.flux == FPSI_FLUX_KEC) FPSI_FLUX(true, FPSI_FLUX_KEC);
+        else if (x->P.flux == FPSI_FLUX_SSF) FPSI_FLUX(true, FPSI_FLUX_SSF);
+        else FPSI_FLUX(true, FPSI_FLUX_HLLC);
+      } else {
+        if (x->P.flux == FPSI_FLUX_ROE) FPSI_FLUX(false, FPSI_FLUX_ROE);
+        else if (x->P.flux == FPSI_FLUX_HLLE) FPSI_FLUX(false, FPSI_FLUX_HLLE);
+        else if (x->P.flux == FPSI_FLUX_KEC) FPSI_FLUX(false, FPSI_FLUX_KEC);
+        else if (x->P.flux == FPSI_FLUX_SSF) FPSI_FLUX(false, FPSI_FLUX_SSF);
+        else FPSI_FLUX(false, FPSI_FLUX_HLLC);
+      }
+  #undef FPSI_FLUX
     }
-#undef FPSI_FLUX
+    prof_end(x);
   }
-  prof_end(x);
   prof_begin(x, "cell_residual");
   const bool bdf = x->P.time_accurate != 0;
   if (bdf && !x->have_levels) {
@@ -2070,19 +2152,23 @@ static int launch_assemble_t(fpsi_ctx* x) {
   const bool cpt = compact_blocks(x);
   x->asm_compact = cpt;
   x->have_explicit = !cpt;
-  prof_begin(x, "face_jacobian");
-  if (x->any_fdbc)
-    dev::k_bc_fdjac<TB><<<blocks_for(x->H.nbf, 128), 128, 0, s>>>(M, x->d_q, g, (TB*)x->d_bjac);
-  if (cpt)
-    dev::k_face_jacobian_c<TB><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
-        M, x->d_qf, g, (TB*)x->d_fjc);
-  else if (x->P.viscous)
-    dev::k_face_jacobian<TB, true><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
-        M, x->d_q, x->d_qb, x->d_grad, x->d_qf, g, visc(x), fjp, fjm);
-  else
-    dev::k_face_jacobian<TB, false><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
-        M, x->d_q, x->d_qb, x->d_grad, x->d_qf, g, visc(x), fjp, fjm);
-  prof_end(x);
+  // compact records the flux kernel wrote with this residual are kept
+  const bool fresh = cpt && x->jac_fresh == int(sizeof(TB));
+  if (x->any_fdbc || !fresh) {
+    prof_begin(x, "face_jacobian");
+    if (x->any_fdbc)
+      dev::k_bc_fdjac<TB><<<blocks_for(x->H.nbf, 128), 128, 0, s>>>(M, x->d_q, g, (TB*)x->d_bjac);
+    if (!cpt && x->P.viscous)
+      dev::k_face_jacobian<TB, true><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
+          M, x->d_q, x->d_qb, x->d_grad, x->d_qf, g, visc(x), fjp, fjm);
+    else if (!cpt)
+      dev::k_face_jacobian<TB, false><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
+          M, x->d_q, x->d_qb, x->d_grad, x->d_qf, g, visc(x), fjp, fjm);
+    else if (!fresh)
+      dev::k_face_jacobian_c<TB><<<blocks_for(M.nf, dev::JAC_THREADS), dev::JAC_THREADS, 0, s>>>(
+          M, x->d_qf, g, (TB*)x->d_fjc);
+    prof_end(x);
+  }
   prof_begin(x, "assemble_lu");
   if (cpt)
     launch_assemble_kernel<TB, TX, true>(x, M, g);
