@@ -328,7 +328,11 @@ int fpsi_newton_step(fpsi_ctx* ctx, fpsi_stepinfo* info);
  *               kept whatever its residual (the reference's step).
  *   lin_rtol    > 0: sweep until ||B - A x|| <= lin_rtol ||B||, measured every
  *               check_every sweeps, at most max_sweeps; <= 0: exactly
- *               gauss_seidel_iter sweeps. */
+ *               gauss_seidel_iter sweeps.
+ * The step is queued on the device and synchronises with the host once,
+ * to read its new residual (more often when sweeping to lin_rtol).  A zero
+ * pivot (FPSI_E_SINGULAR) or a model wait that gave up (FPSI_E_TIMEOUT)
+ * leaves the state unchanged: the update kernel reads their error bits. */
 enum fpsi_start_kind {
   FPSI_START_JACOBI = 0,
   FPSI_START_ZERO = 1,
