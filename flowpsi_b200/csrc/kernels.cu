@@ -188,6 +188,10 @@ __global__ void k_bc_state(MeshView M, const double* __restrict__ q, const fpsi_
 // consecutive threads on consecutive addresses.
 // ---------------------------------------------------------------------------
 constexpr int GRAD_THREADS = 128;
+// a cell's gradient-and-limiter record staged in shared memory with a
+// stride of GPREC + 1 doubles, so that the 32 lanes' stores of one value
+// fall into different banks
+constexpr int GPS = GPREC + 1;
 // The cell's faces are taken four at a time from the entry-major lists:
 // the four entries and neighbours are loaded together (entry j of a warp's
 // 32 cells is one coalesced line), then the four neighbour states and face
@@ -385,7 +389,7 @@ template <bool WREC>
 __global__ void __launch_bounds__(GRAD_THREADS, 4)
 k_grad_limiter(MeshView M, const double* __restrict__ q, const double* __restrict__ qb, int limiter,
                double Kl, Gas gas, double* __restrict__ grad, double* __restrict__ qf) {
-  __shared__ double sr[WREC ? GRAD_THREADS * GPREC : 1];
+  __shared__ double sr[WREC ? GRAD_THREADS * GPS : 1];
   const int64_t c0 = int64_t(blockIdx.x) * GRAD_THREADS;
   const int64_t c = c0 + threadIdx.x;
   if (c < M.nc) {
@@ -394,14 +398,15 @@ k_grad_limiter(MeshView M, const double* __restrict__ q, const double* __restric
     face_states_cell(M, q, qb, gas, c, rec, rec + 15, qf);
     if (WREC) {
 #pragma unroll
-      for (int k = 0; k < GPREC; ++k) sr[GPREC * threadIdx.x + k] = rec[k];
+      for (int k = 0; k < GPREC; ++k) sr[GPS * threadIdx.x + k] = rec[k];
     }
   }
   if (WREC) {
     __syncthreads();
     // one record per cell: the gradient (15) then the limiter (5)
     const int cnt = int(min(int64_t(GRAD_THREADS), M.nc - c0));
-    for (int i = threadIdx.x; i < GPREC * cnt; i += GRAD_THREADS) grad[GPREC * c0 + i] = sr[i];
+    for (int i = threadIdx.x; i < GPREC * cnt; i += GRAD_THREADS)
+      grad[GPREC * c0 + i] = sr[GPS * (i / GPREC) + i % GPREC];
   }
 }
 
@@ -418,7 +423,7 @@ constexpr int KS_MAX = 8;
 constexpr int KS_VALS = 8;  // r_own 3, n 3, T and pg across the face
 __host__ __device__ inline size_t grad_staged_smem(int K, bool wrec) {
   return size_t(K) * GRAD_THREADS * (KS_VALS * sizeof(double) + sizeof(int32_t)) +
-         (wrec ? size_t(GRAD_THREADS) * GPREC * sizeof(double) : 0);
+         (wrec ? size_t(GRAD_THREADS) * GPS * sizeof(double) : 0);
 }
 template <bool WREC>
 __global__ void __launch_bounds__(GRAD_THREADS, 4)
@@ -550,15 +555,15 @@ k_grad_staged(MeshView M, const double* __restrict__ q, const double* __restrict
     }
     if (WREC) {
 #pragma unroll
-      for (int k = 0; k < 15; ++k) sr[GPREC * t + k] = g[k];
+      for (int k = 0; k < 15; ++k) sr[GPS * t + k] = g[k];
 #pragma unroll
-      for (int k = 0; k < 5; ++k) sr[GPREC * t + 15 + k] = ph[k];
+      for (int k = 0; k < 5; ++k) sr[GPS * t + 15 + k] = ph[k];
     }
   }
   if (WREC) {
     __syncthreads();
     const int cnt = int(min(int64_t(GRAD_THREADS), M.nc - c0));
-    for (int i = t; i < GPREC * cnt; i += GRAD_THREADS) grad[GPREC * c0 + i] = sr[i];
+    for (int i = t; i < GPREC * cnt; i += GRAD_THREADS) grad[GPREC * c0 + i] = sr[GPS * (i / GPREC) + i % GPREC];
   }
 }
 
@@ -833,6 +838,11 @@ k_alpha_diss(MeshView M, const double* __restrict__ q, const double* __restrict_
   if (c >= M.nc) return;
   const int64_t nf = M.nf;
   double veldiv = 0.0, maxd2 = 0.0;
+  // the cell's own velocity and velocity gradient rows, loaded once
+  double uo[5], go[12];
+  q_arr(load_q(q, c), uo);
+#pragma unroll
+  for (int k = 0; k < 12; ++k) go[k] = grad[GPREC * c + k];
   for (int j0 = 0; j0 < M.K; j0 += ECH) {
     EChunk ch;
     load_chunk(M, c, j0, ch, true);
@@ -850,12 +860,15 @@ k_alpha_diss(MeshView M, const double* __restrict__ q, const double* __restrict_
       const double A = M.area[f];
       double ufn;
       if (f < M.nfi) {
-        const int64_t a = side ? ch.nb[i] : c, b = side ? c : ch.nb[i];
-        double ua[5], ub[5];
-        q_arr(load_q(q, a), ua);
-        q_arr(load_q(q, b), ub);
-        const double* ga = grad + GPREC * a;
-        const double* gb = grad + GPREC * b;
+        // the neighbour's velocity and gradient rows; l is the cl side
+        double qnb[5], gn[12];
+        q_arr(load_q(q, ch.nb[i]), qnb);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) gn[k] = grad[GPREC * int64_t(ch.nb[i]) + k];
+        const double* ua = side ? qnb : uo;
+        const double* ub = side ? uo : qnb;
+        const double* ga = side ? gn : go;
+        const double* gb = side ? go : gn;
         double d[3], d2 = 0.0, dv[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {

@@ -31,9 +31,15 @@ def _pair(case):
     return g, o
 
 
+@pytest.mark.parametrize("flux", [None, 3, 4])
 @pytest.mark.parametrize("visc", [1, 2])
-def test_viscous_residual_matches_oracle(need_gpu, visc):
-    g, o = _pair(_case(visc, "fp64"))
+def test_viscous_residual_matches_oracle(need_gpu, visc, flux):
+    """flux None: the case's Roe flux; 3 and 4: the low-dissipation KEC and
+    SSF fluxes with the viscous terms (fluxLowDiss.loci:320-640)"""
+    case = _case(visc, "fp64")
+    if flux is not None:
+        case.params.flux = flux
+    g, o = _pair(case)
     sg, ng = g.residual()
     so, no = o.residual()
     # flux scale: the inviscid fluxes dominate; measure against max |F| per cell
