@@ -917,12 +917,6 @@ k_alpha_diss(MeshView M, const double* __restrict__ q, const double* __restrict_
 // per-cell residual gather, local time step and norm partials
 // ---------------------------------------------------------------------------
 constexpr int NORM_THREADS = 256;
-// The residual kernel's threads take RES_CPT cells each (stride
-// NORM_THREADS, so the loads stay coalesced); the norm partials are reduced
-// once per RES_CELLS cells, which keeps the shuffles of that reduction a
-// small part of the kernel's shared-memory pipe work.
-constexpr int RES_CPT = 4;
-constexpr int RES_CELLS = NORM_THREADS * RES_CPT;
 
 template <bool BDF>
 __global__ void __launch_bounds__(NORM_THREADS)
@@ -935,117 +929,110 @@ k_cell_residual(MeshView M, const double* __restrict__ q, const double* __restri
                 double cflmax, double vol_tot, const double* __restrict__ qn,
                 const double* __restrict__ qnm1, double* __restrict__ src,
                 double* __restrict__ dtau, double* __restrict__ part) {
+  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   double rt = 0, et = 0, mt = 0, rmax = 0, emax = 0, mmax = 0;
   double rloc = -1, eloc = -1;
-  // signed max-abs with the lowest cell index on ties
-  auto combine = [](double& v, double& loc, double ov, double oloc) {
-    if (fabs(ov) > fabs(v) ||
-        (fabs(ov) == fabs(v) && oloc >= 0 && (loc < 0 || oloc < loc)))
-      v = ov, loc = oloc;
-  };
-  const int64_t cbase = int64_t(blockIdx.x) * RES_CELLS + threadIdx.x;
-#pragma unroll 1
-  for (int r = 0; r < RES_CPT; ++r) {
-    const int64_t c = cbase + int64_t(r) * NORM_THREADS;
-    if (c < M.nc) {
-      // the cell's own state and volume are requested before its face records
-      const Q5 qc = load_q(q, c);
-      const double V = M.vol[c];
-      double s[5] = {0, 0, 0, 0, 0};
-      double meva = 0;
-      // the face records four at a time from the entry-major lists, all four
-      // requested before any is summed, then summed in the cell's face order
-      auto add = [&](int32_t en, const double2* r3) {
-        const double p[5] = {r3[0].x, r3[0].y, r3[1].x, r3[1].y, r3[2].x};
-        if (en & 1) {
+  if (c < M.nc) {
+    // the cell's own state and volume are requested before its face records
+    const Q5 qc = load_q(q, c);
+    const double V = M.vol[c];
+    double s[5] = {0, 0, 0, 0, 0};
+    double meva = 0;
+    // the face records four at a time from the entry-major lists, all four
+    // requested before any is summed, then summed in the cell's face order
+    auto add = [&](int32_t en, const double2* r3) {
+      const double p[5] = {r3[0].x, r3[0].y, r3[1].x, r3[1].y, r3[2].x};
+      if (en & 1) {
 #pragma unroll
-          for (int k = 0; k < 5; ++k) s[k] += p[k];
-        } else {
+        for (int k = 0; k < 5; ++k) s[k] += p[k];
+      } else {
 #pragma unroll
-          for (int k = 0; k < 5; ++k) s[k] -= p[k];
-        }
-        meva += r3[2].y;
-      };
-      for (int j0 = 0; j0 < M.K; j0 += ECH) {
-        int32_t ent[ECH];
-#pragma unroll
-        for (int i = 0; i < ECH; ++i)
-          ent[i] = j0 + i < M.K ? __ldg(M.ecf + int64_t(j0 + i) * M.nc + c) : -1;
-        double2 rec[ECH][3];
-#pragma unroll
-        for (int i = 0; i < ECH; ++i) {
-          const double2* p2 =
-              reinterpret_cast<const double2*>(F + FREC * int64_t(ent[i] >= 0 ? ent[i] >> 1 : 0));
-          rec[i][0] = __ldg(p2), rec[i][1] = __ldg(p2 + 1), rec[i][2] = __ldg(p2 + 2);
-        }
-#pragma unroll
-        for (int i = 0; i < ECH; ++i)
-          if (ent[i] >= 0) add(ent[i], rec[i]);
+        for (int k = 0; k < 5; ++k) s[k] -= p[k];
       }
-      const double cflpdt = 0.5 * meva / V;
-      double dt = dtmax;
-      if (cflmax > 0) dt = dmin(dt, cflmax / cflpdt);
-      // dtau, solverTimestep.loci:302-329 with eta == 1
-      const double rvol = 1.0 / V;
-      const double p = qc.p + g.pamb, T = qc.T;
-      const double rP = 1.0 / (g.Rt * T);
-      const double rho = p * rP;
-      const double rT = -rho / T;
-      const double qk = 0.5 * (qc.u * qc.u + qc.v * qc.v + qc.w * qc.w);
-      const double fT = rT * qk, fP = 1.0 / (g.gamma - 1.0) + rP * qk;
-      const double cterm = fP * rT - fT * rP;
-      const double dsu = s[1] * qc.u + s[2] * qc.v + s[3] * qc.w;
-      const double dtemp =
-          rvol * (s[0] * (fP * rT) + (dsu - s[4] - 2.0 * qk * s[0]) * (rT * rP)) / (cterm * rT);
-      dt = dmin(dt, urelax * T / (fabs(dtemp) + 1e-30));
-      const double dp = rvol * (rT * (2.0 * qk * s[0] - dsu + s[4]) - fT * s[0]);
-      dt = dmin(dt, urelax * p / (fabs(dp) + 1e-30));
-      dtau[c] = dt;
-      if (BDF) {
-        // BDF2: s - 1.5 (Q(n+1) - Q(n)) V/dt + 0.5 (Q(n) - Q(n-1)) V/dt
-        const Q5 a = load_q(qn, c), b = load_q(qnm1, c);
-        const double rdtvol = V / dtmax;
-        const double w1 = 1.5 * rdtvol, w2 = 0.5 * rdtvol;
-        const double rhon = (a.p + g.pamb) / (g.Rt * a.T);
-        const double rhonm1 = (b.p + g.pamb) / (g.Rt * b.T);
-        const double rhonp1 = rho;
-        s[0] = s[0] - w1 * (rhonp1 - rhon) + w2 * (rhon - rhonm1);
-        const double up1[3] = {qc.u, qc.v, qc.w}, un[3] = {a.u, a.v, a.w}, um1[3] = {b.u, b.v, b.w};
+      meva += r3[2].y;
+    };
+    for (int j0 = 0; j0 < M.K; j0 += ECH) {
+      int32_t ent[ECH];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          const double r1 = rhonp1 * up1[i], r0 = rhon * un[i], rm = rhonm1 * um1[i];
-          s[1 + i] = s[1 + i] - w1 * (r1 - r0) + w2 * (r0 - rm);
-        }
-        const double igm1 = 1.0 / (g.gamma - 1.0);
-        const double e1 = rhonp1 * (g.Rt * qc.T * igm1 + qk);
-        const double e0 = rhon * (g.Rt * a.T * igm1 + 0.5 * (a.u * a.u + a.v * a.v + a.w * a.w));
-        const double em = rhonm1 * (g.Rt * b.T * igm1 + 0.5 * (b.u * b.u + b.v * b.v + b.w * b.w));
-        s[4] = s[4] - w1 * (e1 - e0) + w2 * (e0 - em);
+      for (int i = 0; i < ECH; ++i)
+        ent[i] = j0 + i < M.K ? __ldg(M.ecf + int64_t(j0 + i) * M.nc + c) : -1;
+      double2 rec[ECH][3];
+#pragma unroll
+      for (int i = 0; i < ECH; ++i) {
+        const double2* p2 =
+            reinterpret_cast<const double2*>(F + FREC * int64_t(ent[i] >= 0 ? ent[i] >> 1 : 0));
+        rec[i][0] = __ldg(p2), rec[i][1] = __ldg(p2 + 1), rec[i][2] = __ldg(p2 + 2);
       }
-      double* so = src + 5 * c;
 #pragma unroll
-      for (int k = 0; k < 5; ++k) so[k] = s[k];
-      // norms (solverResidual.loci:74-112)
-      const double w = V / vol_tot;
-      const double a0 = rvol * s[0], a4 = rvol * s[4];
-      rt += w * (a0 * a0);
-      et += w * (a4 * a4);
-      double mm = 0;
+      for (int i = 0; i < ECH; ++i)
+        if (ent[i] >= 0) add(ent[i], rec[i]);
+    }
+    const double cflpdt = 0.5 * meva / V;
+    double dt = dtmax;
+    if (cflmax > 0) dt = dmin(dt, cflmax / cflpdt);
+    // dtau, solverTimestep.loci:302-329 with eta == 1
+    const double rvol = 1.0 / V;
+    const double p = qc.p + g.pamb, T = qc.T;
+    const double rP = 1.0 / (g.Rt * T);
+    const double rho = p * rP;
+    const double rT = -rho / T;
+    const double qk = 0.5 * (qc.u * qc.u + qc.v * qc.v + qc.w * qc.w);
+    const double fT = rT * qk, fP = 1.0 / (g.gamma - 1.0) + rP * qk;
+    const double cterm = fP * rT - fT * rP;
+    const double dsu = s[1] * qc.u + s[2] * qc.v + s[3] * qc.w;
+    const double dtemp =
+        rvol * (s[0] * (fP * rT) + (dsu - s[4] - 2.0 * qk * s[0]) * (rT * rP)) / (cterm * rT);
+    dt = dmin(dt, urelax * T / (fabs(dtemp) + 1e-30));
+    const double dp = rvol * (rT * (2.0 * qk * s[0] - dsu + s[4]) - fT * s[0]);
+    dt = dmin(dt, urelax * p / (fabs(dp) + 1e-30));
+    dtau[c] = dt;
+    if (BDF) {
+      // BDF2: s - 1.5 (Q(n+1) - Q(n)) V/dt + 0.5 (Q(n) - Q(n-1)) V/dt
+      const Q5 a = load_q(qn, c), b = load_q(qnm1, c);
+      const double rdtvol = V / dtmax;
+      const double w1 = 1.5 * rdtvol, w2 = 0.5 * rdtvol;
+      const double rhon = (a.p + g.pamb) / (g.Rt * a.T);
+      const double rhonm1 = (b.p + g.pamb) / (g.Rt * b.T);
+      const double rhonp1 = rho;
+      s[0] = s[0] - w1 * (rhonp1 - rhon) + w2 * (rhon - rhonm1);
+      const double up1[3] = {qc.u, qc.v, qc.w}, un[3] = {a.u, a.v, a.w}, um1[3] = {b.u, b.v, b.w};
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
-        const double a = rvol * s[1 + i];
-        if (fabs(mmax) < fabs(a)) mmax = a;
-        mm += a * a;
+        const double r1 = rhonp1 * up1[i], r0 = rhon * un[i], rm = rhonm1 * um1[i];
+        s[1 + i] = s[1 + i] - w1 * (r1 - r0) + w2 * (r0 - rm);
       }
-      mt += mm * (w / 3.0);
-      combine(rmax, rloc, a0, double(c));
-      combine(emax, eloc, a4, double(c));
+      const double igm1 = 1.0 / (g.gamma - 1.0);
+      const double e1 = rhonp1 * (g.Rt * qc.T * igm1 + qk);
+      const double e0 = rhon * (g.Rt * a.T * igm1 + 0.5 * (a.u * a.u + a.v * a.v + a.w * a.w));
+      const double em = rhonm1 * (g.Rt * b.T * igm1 + 0.5 * (b.u * b.u + b.v * b.v + b.w * b.w));
+      s[4] = s[4] - w1 * (e1 - e0) + w2 * (e0 - em);
     }
+    double* so = src + 5 * c;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) so[k] = s[k];
+    // norms (solverResidual.loci:74-112)
+    const double w = V / vol_tot;
+    const double a0 = rvol * s[0], a4 = rvol * s[4];
+    rt = w * (a0 * a0);
+    et = w * (a4 * a4);
+    double mm = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const double a = rvol * s[1 + i];
+      if (fabs(mmax) < fabs(a)) mmax = a;
+      mm += a * a;
+    }
+    mt = mm * (w / 3.0);
+    rmax = a0, emax = a4;
+    rloc = double(c), eloc = double(c);
   }
   // fixed-shape reduction: sums and signed max-abs with lowest-index ties,
   // first across each warp's lanes (shuffles), then across the 8 warps
   const unsigned full = 0xffffffffu;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  auto combine = [&](double& v, double& loc, double ov, double oloc) {
+    if (fabs(ov) > fabs(v) || (fabs(ov) == fabs(v) && loc < 0)) v = ov, loc = oloc;
+  };
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
     rt += __shfl_down_sync(full, rt, off);
@@ -2120,16 +2107,15 @@ int launch_residual(fpsi_ctx* x, double* resid_slot) {
                                   cudaMemcpyDeviceToDevice, s));
     x->have_levels = true;
   }
-  const int nblk = int((M.nc + dev::RES_CELLS - 1) / dev::RES_CELLS);
   if (bdf)
-    dev::k_cell_residual<true><<<nblk, dev::NORM_THREADS, 0, s>>>(
+    dev::k_cell_residual<true><<<x->nblk_norm, dev::NORM_THREADS, 0, s>>>(
         M, x->d_q, x->d_F, g, x->P.urelax, x->P.dtmax, x->P.cflmax, x->H.vol_tot, x->d_qn, x->d_qnm1,
         x->d_src, x->d_dtau, x->d_part);
   else
-    dev::k_cell_residual<false><<<nblk, dev::NORM_THREADS, 0, s>>>(
+    dev::k_cell_residual<false><<<x->nblk_norm, dev::NORM_THREADS, 0, s>>>(
         M, x->d_q, x->d_F, g, x->P.urelax, x->P.dtmax, x->P.cflmax, x->H.vol_tot, nullptr, nullptr,
         x->d_src, x->d_dtau, x->d_part);
-  dev::k_norm_final<<<1, dev::NORM_THREADS, 0, s>>>(x->d_part, nblk, x->d_err + 1, resid_slot);
+  dev::k_norm_final<<<1, dev::NORM_THREADS, 0, s>>>(x->d_part, x->nblk_norm, x->d_err + 1, resid_slot);
   prof_end(x);
   FPSI_CUDA_TRY(cudaGetLastError());
   return FPSI_OK;
