@@ -530,6 +530,13 @@ constexpr int WS_PROD = 8;                         // gathering warps, 16 rows e
 constexpr int WS_EPI = 4;                          // epilogue warps
 constexpr int WS_THREADS = 32 * (WS_PROD + 1 + WS_EPI);
 constexpr int WS_NB = 4;                           // neighbour rows per cell in flight
+// Bytes between the K-chunk blocks of an A tile: the 128 rows' 16 B units
+// of one chunk plus 32 B, so that chunk c starts 2c units (of 16 B) further
+// round the 8 bank groups.  A quarter warp of gathering lanes holds chunks
+// qc + 4i of two rows r, r + 1, whose units then fall into the 8 groups
+// (2 qc + r) mod 8 once each: conflict-free stores.  The MMA reads the skew
+// through its descriptor's K-chunk step (LBO).
+constexpr int WS_ACH = TC_ROWS * 16 + 32;
 
 struct WsSmem {
   size_t a0, a1, b, o, wo, bias, bar, slot, abort, total;
@@ -538,8 +545,8 @@ __host__ __device__ inline WsSmem ws_smem(int fin) {
   const size_t nch = size_t(2 * fin / 8);
   WsSmem s;
   s.a0 = 0;
-  s.a1 = s.a0 + nch * TC_ROWS * 16;
-  s.b = s.a1 + nch * TC_ROWS * 16;
+  s.a1 = s.a0 + nch * WS_ACH;
+  s.b = s.a1 + nch * WS_ACH;
   s.o = s.b + nch * W * 16;
   s.wo = s.o + size_t(WS_EPI) * 32 * TC_OSTRIDE;
   s.bias = s.wo + size_t(NOUT * W + 8) * sizeof(float);
@@ -619,8 +626,8 @@ k_layer_ws(int64_t nc, int fin, const __nv_bfloat16* __restrict__ h, const int32
     // quarter + 4 of its row and of the row's first WS_NB neighbours, all
     // loading at once: four consecutive lanes read 64 contiguous bytes of a
     // row, which costs the L1 less than eight lanes on eight rows (measured:
-    // 314 against 389 us a layer at 64^3 x 6, although the stores of the
-    // latter hit every bank once and these four-way).  The
+    // 314 against 389 us a layer at 64^3 x 6); the A tile's skewed chunk
+    // blocks (WS_ACH) keep this mapping's stores free of bank conflicts.  The
     // neighbours come from the entry-major lists in the cell's face order
     // (boundary entries are -1 and skipped), so the mean sums them in the
     // order of the face graph.
@@ -640,7 +647,7 @@ k_layer_ws(int64_t nc, int fin, const __nv_bfloat16* __restrict__ h, const int32
         for (int j = 0; j < WS_NB; ++j) nbi[j] = cell < nc && j < K ? __ldg(ell + j * nc + cell) : -1;
         if (cell >= nc) {
           for (int c = qc; c < nch; c += 4)
-            *reinterpret_cast<uint4*>(A + (size_t(c) * TC_ROWS + r) * 16) = make_uint4(0, 0, 0, 0);
+            *reinterpret_cast<uint4*>(A + size_t(c) * WS_ACH + size_t(r) * 16) = make_uint4(0, 0, 0, 0);
           continue;
         }
         int deg = 0;
@@ -667,7 +674,7 @@ k_layer_ws(int64_t nc, int fin, const __nv_bfloat16* __restrict__ h, const int32
             if (c >= hch) break;
             float v[8], sum[8];
             own[i].get(v);
-            *reinterpret_cast<uint4*>(A + (size_t(c) * TC_ROWS + r) * 16) = pack8(v);
+            *reinterpret_cast<uint4*>(A + size_t(c) * WS_ACH + size_t(r) * 16) = pack8(v);
 #pragma unroll
             for (int q8 = 0; q8 < 8; ++q8) sum[q8] = 0.f;
 #pragma unroll
@@ -688,7 +695,7 @@ k_layer_ws(int64_t nc, int fin, const __nv_bfloat16* __restrict__ h, const int32
             }
 #pragma unroll
             for (int q8 = 0; q8 < 8; ++q8) sum[q8] *= inv;
-            *reinterpret_cast<uint4*>(A + (size_t(hch + c) * TC_ROWS + r) * 16) = pack8(sum);
+            *reinterpret_cast<uint4*>(A + size_t(hch + c) * WS_ACH + size_t(r) * 16) = pack8(sum);
           }
         }
       }
@@ -708,7 +715,7 @@ k_layer_ws(int64_t nc, int fin, const __nv_bfloat16* __restrict__ h, const int32
         if (*abort_flag) break;
         tc_fence_after();
         for (int st = 0; st < nch / 2; ++st) {
-          const uint64_t ad = umma_desc(sA[b] + size_t(2 * st) * TC_ROWS * 16, TC_ROWS * 16, 128);
+          const uint64_t ad = umma_desc(sA[b] + size_t(2 * st) * WS_ACH, WS_ACH, 128);
           const uint64_t bd = umma_desc(sB + size_t(2 * st) * W * 16, W * 16, 128);
           umma_bf16(tmem + uint32_t(TC_COLS * b), ad, bd, st > 0 ? 1u : 0u);
         }
