@@ -49,6 +49,24 @@ class LearnedStart:
         assert w.size == self.n_params
         N.check(N.lib().fpsi_gnn_set_params(self._h, w.ctypes.data_as(_fp)), "fpsi_gnn_set_params")
 
+    def save(self, path) -> None:
+        """the parameters (BF16 values held as FP32, in the library's
+        packing order) to an .npy file"""
+        np.save(path, self.get_params())
+
+    @classmethod
+    def load(cls, path) -> "LearnedStart":
+        """a model whose parameters are those saved by save(); the training
+        set is not saved"""
+        w = np.load(path)
+        m = cls()
+        if w.dtype != np.float32 or w.ndim != 1 or w.size != m.n_params:
+            m.close()
+            raise ValueError(f"{path}: expected {m.n_params} float32 parameters, got "
+                             f"{w.size} {w.dtype}")
+        m.set_params(w)
+        return m
+
     def add_snapshot(self, solver: FlowPsi, dq) -> None:
         """features of solver's assembled system and its converged update"""
         d = np.ascontiguousarray(dq, np.float64).reshape(-1)

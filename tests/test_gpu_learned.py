@@ -231,6 +231,26 @@ def test_training_is_reproducible(need_gpu):
     assert hs[0][0][-1] < hs[0][0][0]
 
 
+def test_saved_model_predicts_the_same_start(need_gpu, tmp_path):
+    """save() then load() gives the same parameters and the same start"""
+    case, g, _ = _system(n=5)
+    dq = converged_update(g, 1e-10, 400)
+    m = LearnedStart(seed=2)
+    m.add_snapshot(g, dq)
+    m.train(30, batch=g.ncells, lr=3e-3)
+    m.save(tmp_path / "model.npy")
+    m2 = LearnedStart.load(tmp_path / "model.npy")
+    assert np.array_equal(m.get_params(), m2.get_params())
+    x1 = m.predict(g, want=True)
+    x2 = m2.predict(g, want=True)
+    assert np.array_equal(x1, x2)
+    np.save(tmp_path / "short.npy", m.get_params()[:-1])
+    with pytest.raises(ValueError):
+        LearnedStart.load(tmp_path / "short.npy")
+    m.close()
+    m2.close()
+
+
 def test_untrained_model_gives_the_jacobi_start(need_gpu):
     """the head starts at zero: x0 = x_J exactly"""
     case, g, _ = _system(prec="ref")
