@@ -43,6 +43,7 @@ class Params(C.Structure):
         ("lds_ducros_factor", C.c_double), ("lds_use_upwind", C.c_double),
         ("lds_nonsym_coeff", C.c_double), ("lds_nonsym_factor", C.c_double),
         ("lds_miles_filter", C.c_double), ("ssf_coeff", C.c_double),
+        ("step_graphs", C.c_int32), ("reserved2", C.c_int32),
     ]
 
 

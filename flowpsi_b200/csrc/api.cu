@@ -254,6 +254,10 @@ int check_params(const fpsi_params* p) {
     fpsi::set_error("low-dissipation flux switches out of range");
     return FPSI_E_INVALID;
   }
+  if (p->step_graphs < 0 || p->step_graphs > 1) {
+    fpsi::set_error("step_graphs must be 0 or 1");
+    return FPSI_E_INVALID;
+  }
   return FPSI_OK;
 }
 
@@ -331,6 +335,7 @@ void fpsi_default_params(fpsi_params* p) {
   p->lds_nonsym_factor = 1.0;
   p->lds_miles_filter = 0.1;
   p->ssf_coeff = 1.0;
+  p->step_graphs = 1;
 }
 
 const char* fpsi_strerror(int code) {
@@ -1249,17 +1254,71 @@ int fpsi_newton_step_ex(fpsi_ctx* x, fpsi_gnn* model, const fpsi_step_opts* opts
   return FPSI_OK;
 }
 
+// One implicit step's launches on the stream, its norms into slot (device)
+// and, when hdst is given, by a copy queued behind the residual into hdst
+// (pinned host).
+static int launch_step(fpsi_ctx* x, double* slot, double* hdst, bool sa) {
+  int rc = FPSI_OK;
+  if (sa) rc = fpsi::sa_launch_tmu(x);
+  if (!rc) rc = fpsi::launch_residual(x, slot);
+  if (!rc && hdst &&
+      cudaMemcpyAsync(hdst, slot, fpsi::NREC * sizeof(double), cudaMemcpyDeviceToHost, x->stream) !=
+          cudaSuccess)
+    rc = FPSI_E_CUDA;
+  if (!rc && sa) rc = fpsi::sa_launch_residual(x);
+  if (!rc && sa) rc = fpsi::sa_launch_solve(x);
+  if (!rc) rc = fpsi::launch_assemble(x);
+  if (!rc && is_lsgs(x)) {
+    rc = fpsi::lsgs_assemble(x);
+    if (!rc) rc = fpsi::lsgs_solve(x, true);
+  } else if (!rc) {
+    rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter);
+  }
+  if (!rc) rc = fpsi::launch_update(x, slot);
+  if (!rc && sa) rc = fpsi::sa_launch_update(x, slot);
+  return rc;
+}
+
+// The launches of one step captured as a CUDA graph, with its norms going to
+// the fixed slot; null when the capture or the instantiation fails (the
+// caller then launches the step itself).  Nothing of a captured step runs
+// until the graph is launched.
+static cudaGraphExec_t capture_step(fpsi_ctx* x, double* fixed) {
+  if (cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  const int rc = launch_step(x, fixed, nullptr, false);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(x->stream, &g);
+  cudaGraphExec_t ge = nullptr;
+  if (rc == FPSI_OK && e == cudaSuccess && g &&
+      cudaGraphInstantiate(&ge, g, 0) != cudaSuccess)
+    ge = nullptr;
+  if (g) cudaGraphDestroy(g);
+  cudaGetLastError();
+  return ge;
+}
+
 // nsteps implicit steps on the stream; with the SA model nu~ is advanced in
 // each step from the same residual state, after the mean flow's solve.  The
-// norms of step s go to d_hist[8s] and, by a 64-byte copy queued behind the
-// residual, to the pinned h_hist[8s] (whose rtrms slot starts at -1).  Before
-// each launch the host looks at the copies that have landed and stops
+// norms of step s go to d_hist[NREC s] and, by a copy queued behind the
+// residual, to the pinned h_hist[NREC s] (whose rtrms slot starts at -1).
+// Before each launch the host looks at the copies that have landed and stops
 // launching once one holds NaN norms; steps already queued behind it leave
 // the state alone (the update kernels test their step's norms), so the state
-// is the one of the first NaN step.  Returns the number of steps launched.
+// is the one of the first NaN step.  With step_graphs (SGS/FSGS, no SA) step
+// 0 runs as launches, which makes every buffer the step uses, and steps
+// 1.. replay one captured graph whose norms land in d_hist[NREC nsteps]
+// (the history holds nsteps + 1 records) and are copied from there into
+// the step's slots behind the graph.
+// Returns the number of steps launched.
 static int run_steps(fpsi_ctx* x, int32_t nsteps, int32_t* launched) {
   int rc = FPSI_OK;
   const bool sa = fpsi::sa_active(x);
+  const bool graphs = x->P.step_graphs && !sa && !is_lsgs(x) && !x->profiling && nsteps > 2;
+  double* fixed = x->d_hist + fpsi::NREC * int64_t(nsteps);
+  cudaGraphExec_t ge = nullptr;
   volatile double* hh = x->h_hist;
   for (int32_t s = 0; s < nsteps; ++s) hh[fpsi::NREC * int64_t(s)] = -1.0;
   int32_t seen = 0, s = 0;
@@ -1274,23 +1333,20 @@ static int run_steps(fpsi_ctx* x, int32_t nsteps, int32_t* launched) {
     }
     if (nan) break;
     double* slot = x->d_hist + fpsi::NREC * int64_t(s);
-    if (sa) rc = fpsi::sa_launch_tmu(x);
-    if (!rc) rc = fpsi::launch_residual(x, slot);
-    if (!rc && cudaMemcpyAsync(x->h_hist + fpsi::NREC * int64_t(s), slot, fpsi::NREC * sizeof(double),
-                               cudaMemcpyDeviceToHost, x->stream) != cudaSuccess)
-      rc = FPSI_E_CUDA;
-    if (!rc && sa) rc = fpsi::sa_launch_residual(x);
-    if (!rc && sa) rc = fpsi::sa_launch_solve(x);
-    if (!rc) rc = fpsi::launch_assemble(x);
-    if (!rc && is_lsgs(x)) {
-      rc = fpsi::lsgs_assemble(x);
-      if (!rc) rc = fpsi::lsgs_solve(x, true);
-    } else if (!rc) {
-      rc = fpsi::launch_sgs(x, x->P.gauss_seidel_iter);
+    double* hdst = x->h_hist + fpsi::NREC * int64_t(s);
+    if (graphs && s == 1) ge = capture_step(x, fixed);
+    if (ge) {
+      if (cudaGraphLaunch(ge, x->stream) != cudaSuccess ||
+          cudaMemcpyAsync(slot, fixed, fpsi::NREC * sizeof(double), cudaMemcpyDeviceToDevice,
+                          x->stream) != cudaSuccess ||
+          cudaMemcpyAsync(hdst, fixed, fpsi::NREC * sizeof(double), cudaMemcpyDeviceToHost,
+                          x->stream) != cudaSuccess)
+        rc = FPSI_E_CUDA;
+    } else {
+      rc = launch_step(x, slot, hdst, sa);
     }
-    if (!rc) rc = fpsi::launch_update(x, slot);
-    if (!rc && sa) rc = fpsi::sa_launch_update(x, slot);
   }
+  if (ge) cudaGraphExecDestroy(ge);
   *launched = s;
   x->have_sa = x->have_sa_dq = false;
   return rc;
@@ -1325,7 +1381,7 @@ static int finish_run(fpsi_ctx* x, int32_t nsteps, int32_t launched, fpsi_resid*
 int fpsi_run(fpsi_ctx* x, int32_t nsteps, fpsi_resid* norms) {
   if (!x || nsteps < 0) return FPSI_E_INVALID;
   if (nsteps == 0) return FPSI_OK;
-  int rc = ensure_hist(x, nsteps);
+  int rc = ensure_hist(x, nsteps + 1);
   if (rc) return rc;
   int32_t launched = 0;
   rc = run_steps(x, nsteps, &launched);
@@ -1342,7 +1398,7 @@ int fpsi_time_step(fpsi_ctx* x, fpsi_resid* norms) {
     return FPSI_E_STATE;
   }
   const int32_t nit = x->P.newton_iters;
-  int rc = ensure_hist(x, nit);
+  int rc = ensure_hist(x, nit + 1);
   if (rc) return rc;
   int32_t launched = 0;
   rc = run_steps(x, nit, &launched);
@@ -1359,7 +1415,7 @@ int fpsi_time_step(fpsi_ctx* x, fpsi_resid* norms) {
 
 int fpsi_run_timed(fpsi_ctx* x, int32_t nsteps, fpsi_resid* norms, double* device_ms) {
   if (!x || nsteps <= 0 || !device_ms) return FPSI_E_INVALID;
-  int rc = ensure_hist(x, nsteps);
+  int rc = ensure_hist(x, nsteps + 1);
   if (rc) return rc;
   cudaEvent_t a = nullptr, b = nullptr;
   if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) rc = FPSI_E_CUDA;
@@ -1381,7 +1437,7 @@ int fpsi_run_timed(fpsi_ctx* x, int32_t nsteps, fpsi_resid* norms, double* devic
 int fpsi_kernel_times(fpsi_ctx* x, int32_t nsteps, int32_t cap, char* names, double* ms,
                       int64_t* launches, int32_t* count) {
   if (!x || nsteps <= 0 || cap < 0 || !count) return FPSI_E_INVALID;
-  int rc = ensure_hist(x, nsteps);
+  int rc = ensure_hist(x, nsteps + 1);
   if (rc) return rc;
   x->prof.clear();
   x->evnext = 0;

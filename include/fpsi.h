@@ -144,6 +144,14 @@ typedef struct fpsi_params {
   double lds_nonsym_factor;     /* LDS_nonSymmetricFactor 1 */
   double lds_miles_filter;      /* LDS_MILES_filter 0.1 (SSF) */
   double ssf_coeff;             /* SSF_Coeff 1 (SSF) */
+  int32_t step_graphs;     /* 1 (default): fpsi_run, fpsi_run_timed and
+                              fpsi_time_step run the first step of a call
+                              as launches, capture the second as a CUDA
+                              graph and replay it for the rest (same
+                              kernels, same results bit for bit); 0: every
+                              step as launches.  SGS and FSGS systems
+                              without the SA model only */
+  int32_t reserved2;
 } fpsi_params;
 
 typedef struct fpsi_bc {

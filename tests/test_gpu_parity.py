@@ -21,6 +21,7 @@ import numpy as np
 import pytest
 
 from flowpsi_b200 import (FlowPsi, FpsiError, cases, inviscid_riemann_flux, roe_jacobian)
+from flowpsi_b200 import _native as N
 from oracle import Oracle, OracleFunctions
 from tests.helpers import block_rel, face_states, flux_scale, rel_to_scale
 
@@ -290,6 +291,30 @@ def test_run_is_deterministic_and_equals_steps(need_gpu):
         np.testing.assert_array_equal(a, b)
     for a, b in zip(h1, h2):
         assert a["rtrms"] == b["rtrms"] and a["etrms"] == b["etrms"]
+
+
+@pytest.mark.parametrize("name,prec,flux", [("tgv_tets", "mixed", None), ("farfield_hex", "fp64", None),
+                                            ("shock_hex", "ref", None), ("tgv_tets", "mixed", 3)])
+def test_step_graphs_replay_the_launched_steps(need_gpu, name, prec, flux):
+    """fpsi_run replays a captured graph of its second step for the rest:
+    history and state equal those of launching every step, bit for bit"""
+    case = CASES[name](prec)
+    out = []
+    for graphs in (1, 0):
+        p = N.Params.from_buffer_copy(case.params)
+        p.step_graphs = graphs
+        if flux is not None:
+            p.flux = flux
+        g = FlowPsi(case.mesh, p)
+        g.set_state(*case.initial_state(g.geometry()["cellcenter"]))
+        h = g.run(6)
+        h += g.run(3)
+        out.append((h, g.get_state()))
+        g.close()
+    for a, b in zip(out[0][1], out[1][1]):
+        np.testing.assert_array_equal(a, b)
+    for a, b in zip(out[0][0], out[1][0]):
+        assert a == b
 
 
 def test_nan_state_is_reported(need_gpu):
