@@ -646,6 +646,9 @@ def run_fpsi(args, ws, rank, local):
                    "solver": "lsgs" if case.params.solver == 1 else "sgs",
                    "sgs_sweeps": case.params.gauss_seidel_iter,
                    "parallelism": f"replicas{ws}",
+                   "launch": ("CUDA graph of one step, captured at the second step of each run "
+                              "and replayed" if case.params.step_graphs and case.params.solver != 1
+                              else "kernel launches"),
                    "l2": "inputs larger than L2 (%.1f GB resident)" % (solver.device_bytes / 1e9)},
         "roofline": roofline,
         "cpu_baseline": cpu,
