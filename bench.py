@@ -647,8 +647,7 @@ def run_fpsi(args, ws, rank, local):
                    "sgs_sweeps": case.params.gauss_seidel_iter,
                    "parallelism": f"replicas{ws}",
                    "launch": ("CUDA graph of one step, captured at the second step of each run "
-                              "and replayed" if case.params.step_graphs and case.params.solver != 1
-                              else "kernel launches"),
+                              "and replayed" if case.params.step_graphs else "kernel launches"),
                    "l2": "inputs larger than L2 (%.1f GB resident)" % (solver.device_bytes / 1e9)},
         "roofline": roofline,
         "cpu_baseline": cpu,

@@ -1288,7 +1288,7 @@ static cudaGraphExec_t capture_step(fpsi_ctx* x, double* fixed) {
     cudaGetLastError();
     return nullptr;
   }
-  const int rc = launch_step(x, fixed, nullptr, false);
+  const int rc = launch_step(x, fixed, nullptr, fpsi::sa_active(x));
   cudaGraph_t g = nullptr;
   const cudaError_t e = cudaStreamEndCapture(x->stream, &g);
   cudaGraphExec_t ge = nullptr;
@@ -1307,8 +1307,8 @@ static cudaGraphExec_t capture_step(fpsi_ctx* x, double* fixed) {
 // Before each launch the host looks at the copies that have landed and stops
 // launching once one holds NaN norms; steps already queued behind it leave
 // the state alone (the update kernels test their step's norms), so the state
-// is the one of the first NaN step.  With step_graphs (SGS/FSGS, no SA) step
-// 0 runs as launches, which makes every buffer the step uses, and steps
+// is the one of the first NaN step.  With step_graphs step 0 runs as
+// launches, which makes every buffer the step uses, and steps
 // 1.. replay one captured graph whose norms land in d_hist[NREC nsteps]
 // (the history holds nsteps + 1 records) and are copied from there into
 // the step's slots behind the graph.
@@ -1316,7 +1316,7 @@ static cudaGraphExec_t capture_step(fpsi_ctx* x, double* fixed) {
 static int run_steps(fpsi_ctx* x, int32_t nsteps, int32_t* launched) {
   int rc = FPSI_OK;
   const bool sa = fpsi::sa_active(x);
-  const bool graphs = x->P.step_graphs && !sa && !is_lsgs(x) && !x->profiling && nsteps > 2;
+  const bool graphs = x->P.step_graphs && !x->profiling && nsteps > 2;
   double* fixed = x->d_hist + fpsi::NREC * int64_t(nsteps);
   cudaGraphExec_t ge = nullptr;
   volatile double* hh = x->h_hist;

@@ -149,8 +149,7 @@ typedef struct fpsi_params {
                               as launches, capture the second as a CUDA
                               graph and replay it for the rest (same
                               kernels, same results bit for bit); 0: every
-                              step as launches.  SGS and FSGS systems
-                              without the SA model only */
+                              step as launches */
   int32_t reserved2;
 } fpsi_params;
 

@@ -293,12 +293,20 @@ def test_run_is_deterministic_and_equals_steps(need_gpu):
         assert a["rtrms"] == b["rtrms"] and a["etrms"] == b["etrms"]
 
 
+def _bl_sa(prec, solver):
+    return cases.boundary_layer_block(6, 10, 4, dy0=1e-4, growth=1.3, viscous=2, precision=prec,
+                                      solver=solver, sa=True)
+
+
 @pytest.mark.parametrize("name,prec,flux", [("tgv_tets", "mixed", None), ("farfield_hex", "fp64", None),
-                                            ("shock_hex", "ref", None), ("tgv_tets", "mixed", 3)])
+                                            ("shock_hex", "ref", None), ("tgv_tets", "mixed", 3),
+                                            ("bl_sa_sgs", "mixed", None), ("bl_sa_lsgs", "mixed", None),
+                                            ("bl_sa_lsgs", "fp64", None)])
 def test_step_graphs_replay_the_launched_steps(need_gpu, name, prec, flux):
     """fpsi_run replays a captured graph of its second step for the rest:
-    history and state equal those of launching every step, bit for bit"""
-    case = CASES[name](prec)
+    history and state (and nu~ with the SA model) equal those of launching
+    every step, bit for bit"""
+    case = _bl_sa(prec, name[6:]) if name.startswith("bl_sa") else CASES[name](prec)
     out = []
     for graphs in (1, 0):
         p = N.Params.from_buffer_copy(case.params)
@@ -306,15 +314,21 @@ def test_step_graphs_replay_the_launched_steps(need_gpu, name, prec, flux):
         if flux is not None:
             p.flux = flux
         g = FlowPsi(case.mesh, p)
+        if p.solver == 1:
+            g.set_lines(case.lines)
         g.set_state(*case.initial_state(g.geometry()["cellcenter"]))
+        if name.startswith("bl_sa"):
+            g.set_nutilde(case.nut0)
         h = g.run(6)
         h += g.run(3)
-        out.append((h, g.get_state()))
+        out.append((h, g.get_state(), g.nutilde() if name.startswith("bl_sa") else None))
         g.close()
     for a, b in zip(out[0][1], out[1][1]):
         np.testing.assert_array_equal(a, b)
     for a, b in zip(out[0][0], out[1][0]):
         assert a == b
+    if out[0][2] is not None:
+        np.testing.assert_array_equal(out[0][2], out[1][2])
 
 
 def test_nan_state_is_reported(need_gpu):
