@@ -41,6 +41,7 @@ def test_reference_defaults():
     assert p.solver == N.SOLVER["lsgs"]        # solverNewton.loci:223-228
     assert p.gauss_seidel_iter == 6            # linearSolverSGS.loci:39-41
     assert (p.lsgs_relaxation, p.lsgs_abs_tol, p.lsgs_rel_tol, p.lsgs_max_iter) == (0.25, 1e-10, 0.1, 10)
+    assert p.step_graphs == 1                  # fpsi_run replays a captured step graph
 
 
 def test_strerror():
