@@ -24,7 +24,7 @@ SOLVER = {"sgs": 0, "lsgs": 1, "fsgs": 2}
 PRECISION = {"fp64": 0, "ref": 1, "mixed": 2}
 BC = {"farfield": 1, "supersonicInflow": 2, "supersonicOutflow": 3, "extrapolate": 4,
       "reflecting": 5, "viscousWall": 6, "outflow": 7, "outflowMean": 8,
-      "isentropicInflow": 9, "fixedMass": 10, "fixedMassOutflow": 11}
+      "isentropicInflow": 9, "fixedMass": 10, "fixedMassOutflow": 11, "inflow": 12}
 
 
 class Params(C.Structure):

@@ -101,23 +101,27 @@ def farfield_cube(n: int = 32, seed: int = 0, sweeps: int = 5, flux: str = "roe"
 def outflow_duct(n: int = 16, seed: int = 0, sweeps: int = 5, mean: bool = False,
                  back_pressure: float = 1.02e5, flux: str = "roe",
                  limiter: str = "venkatakrishnan", precision: str = "ref",
-                 inflow: str = "farfield", outflow: str = "outflow") -> Case:
+                 inflow: str = "farfield", outflow: str = "outflow", u_sign: float = 1.0) -> Case:
     """Subsonic duct: n^3 hex cube [0,1]^3, inflow at x-min, outflow at
     x-max, periodic in y and z; initial state the freestream (M=0.5 along
     +x, p=1e5 Pa, T=300 K) with 1% noise (farfield_cube).  inflow:
-    'farfield' at the freestream, 'isentropic' at its total pressure and
+    'farfield' or 'inflow' (the subsonic inflow condition) at the
+    freestream, 'isentropic' at its total pressure and
     temperature (bcIsentropic.loci), or 'fixedMass' at its mass flux and
     total temperature (bcFixedMass.loci).  outflow: 'outflow' at a back
     pressure (bcOutflow.loci:174-273; with mean=True the pMean form, where
     the area-weighted mean of the boundary pressure is held instead), or
     'fixedMassOutflow' at 1.01 times the freestream mass flux, massRelax 0.5
-    (bcFixedMassOutflow.loci)."""
+    (bcFixedMassOutflow.loci).  u_sign = -1 starts the flow along -x, so
+    that it leaves through the inflow condition."""
     T0, p0, M = 300.0, 1e5, 0.5
     U0 = M * math.sqrt(GAMMA * RTILDE * T0)
     ff = bc("farfield", T=T0, pg=p0, u=(U0, 0.0, 0.0))
     if inflow == "isentropic":  # total conditions of the freestream
         f = 1.0 + 0.5 * (GAMMA - 1.0) * M * M
         ff = bc("isentropicInflow", T=T0 * f, pg=p0 * f ** (GAMMA / (GAMMA - 1.0)))
+    elif inflow == "inflow":  # subsonic inflow at the freestream (bcInflow.loci:376-431)
+        ff = bc("inflow", T=T0, pg=p0, u=(U0, 0.0, 0.0))
     elif inflow == "fixedMass":  # the freestream's mass flux at its total temperature
         f = 1.0 + 0.5 * (GAMMA - 1.0) * M * M
         ff = bc("fixedMass", T=T0 * f, mass_flux=p0 / (RTILDE * T0) * U0)
@@ -137,13 +141,46 @@ def outflow_duct(n: int = 16, seed: int = 0, sweeps: int = 5, mean: bool = False
         rho = rho0 * (1.0 + 0.01 * normal(seed, 0, nc))
         p = p0 * (1.0 + 0.01 * normal(seed, 1, nc))
         u = np.empty((nc, 3))
-        u[:, 0] = U0 + 0.01 * U0 * normal(seed, 2, nc)
+        u[:, 0] = u_sign * U0 + 0.01 * U0 * normal(seed, 2, nc)
         u[:, 1] = 0.01 * U0 * normal(seed, 3, nc)
         u[:, 2] = 0.01 * U0 * normal(seed, 4, nc)
         T = p / (RTILDE * rho)
         return T, p, u
 
     return Case(f"outflow_duct_{n}", mesh, params, 100, init)
+
+
+def quicktest_duct(spec: dict, n=(12, 3, 3), precision: str = "fp64", sweeps: int = 5) -> Case:
+    """The duct of the reference's uniform-outcome quick tests
+    (quickTest/inviscid/{inflow,isentropic,fixedMass}.vars): unit cross-
+    section, the test's inflow condition at x-min and its pressure outflow at
+    x-max, periodic in y and z (the tests' symmetry sides carry no flux
+    across them either), started from the test's initial state.  spec is
+    one entry of tests/golden/quicktest_uniform.json.  Inviscid, Roe, no
+    limiter (the tests' `limiter: none`), CFL 50: only the converged state,
+    which the two conditions fix, is compared."""
+    i = spec["inflow"]
+    if i["kind"] == "inflow":
+        inb = bc("inflow", T=i["T"], pg=i["p"], u=(i["u"], 0.0, 0.0))
+    elif i["kind"] == "isentropicInflow":
+        inb = bc("isentropicInflow", T=i["T0"], pg=i["p0"])
+    else:
+        inb = bc("fixedMass", T=i["T0"], mdot=i["mdot"])
+    out = bc("outflow", T=spec["init"]["T"], pg=spec["outflow_p"])
+    mesh = GeneratedMesh("hex", n=tuple(n), L=(1.0, 1.0, 1.0), bc_side=(0, 1, -1, -1, -1, -1),
+                         bcs=[inb, out])
+    params = default_params(flux="roe", limiter="none", solver="sgs", gauss_seidel_iter=sweeps,
+                            cflmax=50.0, precision=precision)
+    ic = spec["init"]
+    u0 = ic["u"] if "u" in ic else ic["M"] * math.sqrt(GAMMA * RTILDE * ic["T"])
+
+    def init(cc):
+        nc = cc.shape[0]
+        u = np.zeros((nc, 3))
+        u[:, 0] = u0
+        return np.full(nc, ic["T"]), np.full(nc, ic["p"]), u
+
+    return Case(f"quicktest_duct_{i['kind']}", mesh, params, 400, init)
 
 
 def taylor_green_tets(n: int = 128, seed: int = 0, sweeps: int = 8, jitter: float = 0.1,

@@ -407,7 +407,7 @@ int fpsi_create(fpsi_ctx** out, const fpsi_mesh* mesh, const fpsi_params* params
   }
   x->bcs.assign(mesh->bcs, mesh->bcs + mesh->nbc);
   for (const fpsi_bc& b : x->bcs)
-    if (b.kind < FPSI_BC_FARFIELD || b.kind > FPSI_BC_FIXED_MASS_OUTFLOW) {
+    if (b.kind < FPSI_BC_FARFIELD || b.kind > FPSI_BC_INFLOW) {
       fpsi::set_error("boundary condition kind %d is not on the device path", b.kind);
       delete x;
       return FPSI_E_UNSUPPORTED;

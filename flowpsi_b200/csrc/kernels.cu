@@ -121,6 +121,15 @@ __global__ void k_bc_state(MeshView M, const double* __restrict__ q, const fpsi_
       }
       break;
     }
+    case FPSI_BC_INFLOW: {  // bcInflow.loci:376-401
+      const double uit = qi.u * nx + qi.v * ny + qi.w * nz;
+      const double a0 = sqrt(g.gamma * g.Rt * q0.T);
+      if (uit > 0 || -uit > a0)
+        r = q0;
+      else
+        cv_state(false, qi, q0, nx, ny, nz, 0.0, g, 1.0, r);
+      break;
+    }
     case FPSI_BC_SUPERSONIC_INFLOW:
       r = q0;
       break;

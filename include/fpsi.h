@@ -98,8 +98,12 @@ enum fpsi_bc_kind {
                                       T0 (fpsi_bc.T), bcIsentropic.loci:40-240 */
   FPSI_BC_FIXED_MASS_INFLOW = 10,  /* mass flux (fpsi_bc.mass_flux) at total temperature T0
                                       (fpsi_bc.T), bcFixedMass.loci:84-235 */
-  FPSI_BC_FIXED_MASS_OUTFLOW = 11  /* mass flux (fpsi_bc.mass_flux) relaxed by mass_relax,
+  FPSI_BC_FIXED_MASS_OUTFLOW = 11, /* mass flux (fpsi_bc.mass_flux) relaxed by mass_relax,
                                       bcFixedMassOutflow.loci:72-186 */
+  FPSI_BC_INFLOW = 12              /* subsonic inflow at the reference state (T, pg, u),
+                                      bcInflow.loci:376-431: the farfield's inflow state
+                                      where the flow enters, the reference state itself
+                                      where it leaves */
 };
 /* fpsi_resid.bcErrorCode bits (flowPsiIO.h:212-215) */
 #define FPSI_BCERR_OUTFLOW_BECAME_INFLOW 1

@@ -883,6 +883,17 @@ static uint64_t bc_face_state(const orc_ctx* o, int64_t f, double q[5]) {
       }
       break;
     }
+    case FPSI_BC_INFLOW: {  // bcInflow.loci:376-401: Dirichlet where the flow leaves
+      double uit = dot(ui, n) - us_n;
+      double a0 = std::sqrt(P.gamma * P.Rtilde * bc.T);
+      if (uit > 0 || -uit > a0) {
+        pgb = bc.pg, Tb = bc.T, ub = u0;
+      } else {
+        cv_inflow(pgb, Tb, ub, pgi, Ti, ui, bc.pg, bc.T, u0, n, us_n, P.Pambient, P.gamma,
+                  P.Rtilde, Eta);
+      }
+      break;
+    }
     case FPSI_BC_SUPERSONIC_INFLOW:
       pgb = bc.pg, Tb = bc.T, ub = u0;
       break;

@@ -81,6 +81,8 @@ CASES = {
     "isentropic_in": lambda prec: cases.outflow_duct(6, precision=prec, inflow="isentropic"),
     "fixedmass_in": lambda prec: cases.outflow_duct(6, precision=prec, inflow="fixedMass"),
     "fixedmass_out": lambda prec: cases.outflow_duct(6, precision=prec, outflow="fixedMassOutflow"),
+    "inflow_in": lambda prec: cases.outflow_duct(6, precision=prec, inflow="inflow"),
+    "inflow_leaving": lambda prec: cases.outflow_duct(6, precision=prec, inflow="inflow", u_sign=-1.0),
     "kec_tgv_tets": lambda prec: _kec(cases.taylor_green_tets(5, precision=prec)),
     "kec_farfield_hex": lambda prec: _kec(cases.farfield_cube(6, precision=prec)),
     "kec_shock_hex": lambda prec: _kec(cases.oblique_shock_cube(8, precision=prec)),
@@ -162,7 +164,7 @@ FD_TOL = {"isentropic_in": 1e-8, "fixedmass_in": 1e-3}
 
 @pytest.mark.parametrize("prec", ["fp64", "ref", "mixed"])
 @pytest.mark.parametrize("name", ["farfield_hex", "tgv_tets", "shock_hex", "isentropic_in",
-                                  "fixedmass_in", "fixedmass_out"])
+                                  "fixedmass_in", "fixedmass_out", "inflow_in", "inflow_leaving"])
 def test_blocks_match_oracle(need_gpu, name, prec):
     g, o = _pair(CASES[name](prec))
     g.residual()
@@ -244,7 +246,8 @@ def test_sgs_converges_on_gpu(need_gpu):
 
 @pytest.mark.parametrize("prec", ["fp64", "ref", "mixed"])
 @pytest.mark.parametrize("name", ["farfield_hex", "tgv_tets", "shock_hex", "outflow_pmean",
-                                  "isentropic_in", "fixedmass_in", "fixedmass_out"])
+                                  "isentropic_in", "fixedmass_in", "fixedmass_out", "inflow_in",
+                                  "inflow_leaving"])
 def test_newton_steps_match_oracle(need_gpu, name, prec):
     case = CASES[name](prec)
     g, o = _pair(case)
