@@ -152,26 +152,31 @@ def outflow_duct(n: int = 16, seed: int = 0, sweeps: int = 5, mean: bool = False
 
 def quicktest_duct(spec: dict, n=(12, 3, 3), precision: str = "fp64", sweeps: int = 5) -> Case:
     """The duct of the reference's uniform-outcome quick tests
-    (quickTest/inviscid/{inflow,isentropic,fixedMass}.vars): unit cross-
-    section, the test's inflow condition at x-min and its pressure outflow at
-    x-max, periodic in y and z (the tests' symmetry sides carry no flux
-    across them either), started from the test's initial state.  spec is
-    one entry of tests/golden/quicktest_uniform.json.  Inviscid, Roe, no
-    limiter (the tests' `limiter: none`), CFL 50: only the converged state,
-    which the two conditions fix, is compared."""
-    i = spec["inflow"]
-    if i["kind"] == "inflow":
-        inb = bc("inflow", T=i["T"], pg=i["p"], u=(i["u"], 0.0, 0.0))
+    (quickTest/inviscid/{inflow,isentropic,fixedMass,superSonic}.vars): unit
+    cross-section, the test's inflow condition at x-min and its outflow
+    condition at x-max, periodic in y and z (the tests' symmetry sides carry
+    no flux across them either), started from the test's initial state and
+    stepped as the test is: pseudo-time step dtmax (cflmax unset), its
+    urelax, no limiter.  spec is one entry of
+    tests/golden/quicktest_uniform.json.  Inviscid, Roe: only the converged
+    state, which the two conditions fix, is compared."""
+    i, o = spec["inflow"], spec["outflow"]
+    if i["kind"] in ("inflow", "supersonicInflow"):
+        inb = bc(i["kind"], T=i["T"], pg=i["p"], u=(i["u"], 0.0, 0.0))
     elif i["kind"] == "isentropicInflow":
         inb = bc("isentropicInflow", T=i["T0"], pg=i["p0"])
     else:
         inb = bc("fixedMass", T=i["T0"], mdot=i["mdot"])
-    out = bc("outflow", T=spec["init"]["T"], pg=spec["outflow_p"])
+    ic = spec["init"]
+    if o["kind"] == "outflow":
+        out = bc("outflow", T=ic["T"], pg=o["p"])
+    else:
+        out = bc("supersonicOutflow")
     mesh = GeneratedMesh("hex", n=tuple(n), L=(1.0, 1.0, 1.0), bc_side=(0, 1, -1, -1, -1, -1),
                          bcs=[inb, out])
     params = default_params(flux="roe", limiter="none", solver="sgs", gauss_seidel_iter=sweeps,
-                            cflmax=50.0, precision=precision)
-    ic = spec["init"]
+                            cflmax=0.0, dtmax=spec["dtmax"], urelax=spec["urelax"],
+                            precision=precision)
     u0 = ic["u"] if "u" in ic else ic["M"] * math.sqrt(GAMMA * RTILDE * ic["T"])
 
     def init(cc):
@@ -180,7 +185,7 @@ def quicktest_duct(spec: dict, n=(12, 3, 3), precision: str = "fp64", sweeps: in
         u[:, 0] = u0
         return np.full(nc, ic["T"]), np.full(nc, ic["p"]), u
 
-    return Case(f"quicktest_duct_{i['kind']}", mesh, params, 400, init)
+    return Case(f"quicktest_duct_{i['kind']}", mesh, params, spec["stop_iter"], init)
 
 
 def taylor_green_tets(n: int = 128, seed: int = 0, sweeps: int = 8, jitter: float = 0.1,

@@ -1,13 +1,13 @@
 """Writes tests/golden/quicktest_uniform.json from the flowPsi reference's own
-quick tests (quickTest/inviscid/{inflow,isentropic,fixedMass}.{vars,dat,tol.dat}).
+quick tests (quickTest/inviscid/{inflow,isentropic,fixedMass,superSonic}.{vars,dat,tol.dat}).
 
-Each of these three tests drives a duct of unit cross-section from an
-inflow condition to a pressure outflow and extracts P, T and u at every
+Each of these four tests drives a duct of unit cross-section from an
+inflow condition to an outflow condition and extracts P, T and u at every
 node after it has converged; every node holds the same uniform state, which
 therefore depends only on the two boundary conditions, not on the grid
 (`testGrid.vog`, which is not read here).  The script records, per test, the
-boundary options, the initial state, the expected uniform state and the
-test's tolerances.
+boundary options, the initial state, the pseudo-time step settings, the
+expected uniform state and the test's tolerances.
 
     python tests/golden/make_quicktest_uniform.py /path/to/flowPsi
 """
@@ -16,7 +16,7 @@ import re
 import sys
 from pathlib import Path
 
-TESTS = ("inflow", "isentropic", "fixedMass")
+TESTS = ("inflow", "isentropic", "fixedMass", "superSonic")
 
 
 def number(text: str, key: str) -> float:
@@ -36,7 +36,7 @@ def parse(ref: Path, name: str) -> dict:
     kind = inflow.split("(")[0]
     opts = inflow[len(kind):]
     bc = {"kind": kind}
-    if kind == "inflow":
+    if kind in ("inflow", "supersonicInflow"):
         bc.update(p=number(opts, "p"), T=number(opts, "T"), u=number(opts, "u"))
     elif kind == "isentropicInflow":
         bc.update(p0=number(opts, "p0"), T0=number(opts, "T0"))
@@ -44,7 +44,7 @@ def parse(ref: Path, name: str) -> dict:
         bc.update(mdot=number(opts, "mdot"), T0=number(opts, "T0"))
     else:
         raise ValueError(kind)
-    assert outflow.startswith("outflow(")
+    assert outflow.startswith("outflow(") or outflow == "supersonicOutflow"
     ic = re.search(r"initialConditions\s*:\s*<([^>]*)>", vars_).group(1)
     init = {"p": number(ic, "p"), "T": number(ic, "T")}
     if re.search(r"\bu\s*=", ic):
@@ -55,8 +55,13 @@ def parse(ref: Path, name: str) -> dict:
     assert len(rows) == 1, f"{name}.dat is not uniform"
     P, T, u = (float(v) for v in rows.pop())
     tol = [float(v) for v in (d / f"{name}.tol.dat").read_text().split()]
-    return {"inflow": bc, "outflow_p": number(outflow, "p"), "init": init,
+    return {"inflow": bc, "init": init,
+            "outflow": {"kind": "supersonicOutflow"} if outflow == "supersonicOutflow" else
+                       {"kind": "outflow", "p": number(outflow, "p")},
             "regime": re.search(r"flowRegime\s*:\s*(\w+)", vars_).group(1),
+            "dtmax": number(vars_.replace(":", "="), "dtmax"),
+            "urelax": number(vars_.replace(":", "="), "urelax"),
+            "stop_iter": int(number(vars_.replace(":", "="), "stop_iter")),
             "expect": {"P": P, "T": T, "u": u}, "tol": tol,
             "source": f"quickTest/inviscid/{name}.vars, .dat, .tol.dat"}
 

@@ -1,5 +1,5 @@
 """The device path against the reference's own uniform-outcome quick tests
-(quickTest/inviscid/{inflow,isentropic,fixedMass}; fixture made by
+(quickTest/inviscid/{inflow,isentropic,fixedMass,superSonic}; fixture made by
 tests/golden/make_quicktest_uniform.py): converged in FP64 and in MIXED, the
 duct's state equals the reference's extracted P, T, u within the test's
 relative tolerance, and the oracle's converged state within 1e-8 (the

@@ -1,11 +1,12 @@
 """The oracle against the reference's own uniform-outcome quick tests
-(quickTest/inviscid/{inflow,isentropic,fixedMass}; fixture made by
+(quickTest/inviscid/{inflow,isentropic,fixedMass,superSonic}; fixture made by
 tests/golden/make_quicktest_uniform.py).  Each drives a unit-section duct
-from an inflow condition (bcInflow.loci:376-431, bcIsentropic.loci,
-bcFixedMass.loci) to a pressure outflow (bcOutflow.loci:174-273); the
-converged state is uniform and fixed by the two conditions, so it is
-compared with the reference's extracted P, T, u at the test's own relative
-tolerance."""
+from an inflow condition (bcInflow.loci:270-309 and 376-431,
+bcIsentropic.loci, bcFixedMass.loci) to an outflow condition
+(bcOutflow.loci:127-165 and 174-273), stepped as the test is (its dtmax as
+the pseudo-time step, its urelax); the converged state is uniform and fixed
+by the two conditions, so it is compared with the reference's extracted P,
+T, u at the test's own relative tolerance."""
 import json
 from pathlib import Path
 
